@@ -1,0 +1,168 @@
+/*
+ * vtem_b200 C ABI: the B200 (sm_100a) kernels behind vtem's video
+ * time-encode/decode path.
+ *
+ * The reference (bionet/vtem) has no native ABI: its Python objects launch
+ * inline CUDA strings through PyCUDA.  Each entry point below replaces the
+ * kernel or library call cited beside it (file:line inside the reference
+ * project); the Python package vtem_b200 keeps the reference's class and
+ * function names on top of these.
+ *
+ * Conventions for every entry point:
+ *   - all array arguments are DEVICE pointers owned by the caller (the
+ *     library allocates nothing on the device, except cuSOLVER's own handle);
+ *   - `stream` is a cudaStream_t passed as void*; work is stream-ordered and
+ *     the call returns without synchronising unless stated otherwise;
+ *   - the return value is a status code (VTB_OK = 0); no C++ exception
+ *     crosses the ABI.  A launch failure returns VTB_CUDA_ERR and
+ *     vtb_last_cuda_error() gives the cudaError_t.
+ *   - matrices are row-major with an explicit leading dimension; complex
+ *     arrays are interleaved (re, im) doubles.
+ */
+#ifndef VTEM_B200_H
+#define VTEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VTB_ABI_VERSION 1
+
+enum {
+    VTB_OK = 0,
+    VTB_BAD_ARG = 1,        /* ValueError/TypeError in the reference */
+    VTB_OVERFLOW = 2,       /* spike buffer full: ensemble_encode.py:163-164 */
+    VTB_OOM = 3,
+    VTB_TIMEOUT = 4,
+    VTB_CUDA_ERR = 5,
+    VTB_NOT_CONVERGED = 6,  /* eigensolver failed */
+    VTB_NO_DATA = 7         /* "no spikes to decode": dirichlet.py:39-40 */
+};
+
+int vtb_version(void);
+const char* vtb_status_string(int status);
+int vtb_last_cuda_error(void);
+
+/* ------------------------------------------------------------ RF banks */
+
+/* Gabor RF bank on a pixel grid, out[n*out_ld + py*Px + px].
+ * Replaces gabor_Kernel + generate_visual_receptive_fields
+ * (vtem/vrf.py:1197-1291, :296-331).  h_alpha is the dilation as the user
+ * gives it (the reference uploads 1/h_alpha, vrf.py:258); gain (may be NULL)
+ * scales each RF (extension, 1 = reference). */
+int vtb_rf_gabor(const double* h_alpha, const double* h_l, const double* h_x0, const double* h_y0,
+                 const int32_t* h_ab, const double* gain, int n_filters, int Px, int Py, double Sx,
+                 double Sy, double x_start, double y_start, double KAPPA, double* out, int64_t out_ld,
+                 void* stream);
+
+/* Centre-surround RF bank.  Replaces cs_Kernel (vtem/vrf.py:1120-1193,
+ * :876-913). */
+int vtb_rf_cs(const double* h_alpha, const double* h_x0, const double* h_y0, const double* gain,
+              int n_filters, int Px, int Py, double Sx, double Sy, double x_start, double y_start,
+              double sigma_center, double sigma_surround, double* out, int64_t out_ld, void* stream);
+
+/* RF projection out(f, n) = scale * sum_p video[f*video_ld + p] rf[n*rf_ld + p],
+ * written at out[f*out_t_stride + n*out_n_stride] (either time- or
+ * neuron-major).  Replaces cublasDgemm + .T() of vrf_gabor.filter /
+ * vrf_cs.filter (vtem/vrf.py:264-292, :845-872). */
+int vtb_rf_filter(const double* video, int F, int P, int64_t video_ld, const double* rf, int N,
+                  int64_t rf_ld, double scale, double* out, int64_t out_t_stride, int64_t out_n_stride,
+                  void* stream);
+
+/* Plain FP64 GEMM C(m,n) = alpha sum_k A(m,k) B(n,k) + beta C(m,n), all
+ * element-strided.  Replaces the cuBLAS DGEMM calls of vtem/utils/linalg.py:32-338
+ * (linalg.dot) on this path. */
+int vtb_gemm_f64(int M, int N, int K, const double* A, int64_t a_m, int64_t a_k, const double* B,
+                 int64_t b_n, int64_t b_k, double* C, int64_t c_m, int64_t c_n, double alpha, double beta,
+                 void* stream);
+
+/* ------------------------------------------------------------ IAF encoder */
+
+/* IAF time encoding of input(t, n) = input[t*in_t_stride + n*in_n_stride],
+ * F samples, in blocks of `block_frames` frames sharing one boundary frame
+ * with time_count reset to 0 at each block start (VTEM_IAF's loop,
+ * vtem/vtem.py:165-200; block_frames = F gives one IAF_encode.encode call).
+ * Replaces the IAF kernels of vtem/ensemble_encode.py:438-552 (randn == NULL)
+ * and :555-674 (random thresholds: randn(block, slot, n) holds the N(0,1)
+ * draws, block_cap slots per block, threshold = randn*sigma + delta).
+ * v0, time_count (and delta_value) are read and written back.  Spikes go to
+ * spike_time/spike_step[n*cap + j] (block-relative time, global step index
+ * of the interval that holds the crossing), spike_count[n] their number.
+ * A neuron that fills its `cap` slots stops and *status is set to
+ * VTB_OVERFLOW.  near_count (may be NULL) accumulates the threshold
+ * comparisons whose margin is below near_eps. */
+int vtb_iaf_encode(const double* input, int64_t in_t_stride, int64_t in_n_stride, int N, int F,
+                   int block_frames, double dt, const double* kappa, const double* bias, const double* delta,
+                   double* v0, double* time_count, const double* randn, int64_t randn_block_stride,
+                   int64_t randn_slot_stride, int64_t randn_n_stride, int randn_block_cap, const double* sigma,
+                   double* delta_value, double* spike_time, int32_t* spike_step, int32_t* spike_count, int cap,
+                   unsigned long long* near_count, double near_eps, int32_t* status, void* stream);
+
+/* ------------------------------------------------------------ Dirichlet space */
+
+/* Dirichlet coefficients Ds (N, 2My+1, 2Mx+1) complex from RFs sampled on
+ * an (LPy, LPx) grid over one spatial period.  Replaces compute_Ds + cuFFT +
+ * fft2Ds_kernel (vtem/vrf.py:333-377, :1293-1350). */
+int vtb_dirichlet_coeffs(const double* rf, int N, int LPy, int LPx, int64_t rf_ld, int Mx, int My,
+                         double dxdy, double* Ds, void* stream);
+
+/* Spatial reconstruction functions out (N, Py, Px) from Ds on a (Py1, Px1)
+ * period grid, centre-cropped.  Replaces compute_dirich_space_fft +
+ * Ds2fft_kernel + cuFFT inverse + filter2rec_kernel (vtem/vrf.py:437-499,
+ * :585-677). */
+int vtb_dirich_space(const double* Ds, int N, int Mx, int My, int Px, int Py, int Px1, int Py1,
+                     double* out, void* stream);
+
+/* Dsw[a*ld + b] = Re sum_s conj(Ds[a,s]) Ds[b,s] * norm[a] norm[b].
+ * Replaces compute_Dsw (cublasZgemm + real + put_norm, vtem/vrf.py:502-559). */
+int vtb_dsw(const double* Ds, int N, int Ks, const double* norm, double* Dsw, int64_t ld, void* stream);
+
+/* ------------------------------------------------------------ decoder */
+
+/* q[i] = (kappa delta - bias (tk2-tk1)) norm at neuron ind[i].
+ * Replaces compute_q_Kernel (vtem/dirichlet.py:55-60, :204-222). */
+int vtb_compute_q(const double* tk1, const double* tk2, const int32_t* ind, int n, const double* kappa,
+                  const double* delta, const double* bias, const double* norm, double* q, void* stream);
+
+/* Analytic Gram G[k*G_ld + l] = Gt(k,l) Dsw[ind_k, ind_l] (+ lamb on the
+ * diagonal).  lower_only = 1 writes only l <= k.  Replaces compute_G_Kernel
+ * + diag_add_Kernel (vtem/dirichlet.py:62-85, :272-350). */
+int vtb_compute_G(const double* tk1, const double* tk2, const int32_t* ind, int n, double Wt, int Mt,
+                  const double* Dsw, int64_t dsw_ld, double lamb, int lower_only, double* G, int64_t G_ld,
+                  void* stream);
+
+/* Workspace bytes of vtb_solve_eq_sym for order n. */
+int vtb_solve_eq_sym_workspace(int n, int64_t* bytes);
+
+/* Pseudoinverse solve c = G^+ q keeping |eigenvalues| > rcond * max; G (its
+ * lower triangle is read) is destroyed.  *kept (may be NULL) receives the
+ * number of values kept.  Synchronises the stream once (eigensolver status).
+ * Replaces solve_eq_sym (vtem/utils/linalg.py:591-631, CULA gesvd +
+ * sq_Kernel :791-833). */
+int vtb_solve_eq_sym(double* G, int64_t ld, const double* q, double* c, int n, double rcond, void* work,
+                     int64_t work_bytes, int32_t* kept, void* stream);
+
+/* RNN decoder: c = 0, then steps+1 updates c += dt_alpha (q - G c).  y (may
+ * be NULL) receives the last residual, c_tmp is an n-double scratch vector,
+ * ynorm_trace (may be NULL) the squared residual norm every trace_every
+ * steps.  Replaces rnn3 + rnn3_update (vtem/neural_network.py:15-128). */
+int vtb_rnn(const double* G, int64_t ld, const double* q, double* c, double* y, double* c_tmp, int n,
+            double dt_alpha, int steps, double* ynorm_trace, int trace_every, void* stream);
+
+/* Workspace bytes of vtb_reconstruct. */
+int vtb_reconstruct_workspace(int N, int Nt, int Mt, int64_t* bytes);
+
+/* Reconstruction u (Nt, P) = sum_k c_k norm_{ind_k} dirich[ind_k] psi_k(t)
+ * at the Nt times t[].  The spike list must be sorted by ind.  Replaces
+ * reconstruct + reconstruct_Kernel (vtem/dirichlet.py:165-189, :354-420). */
+int vtb_reconstruct(const double* dirich, int N, int P, const double* tk1, const double* tk2,
+                    const double* c, const int32_t* ind, const double* norm, int nspk, const double* t, int Nt,
+                    int Mt, double WM, double* u, void* work, int64_t work_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VTEM_B200_H */

@@ -1,0 +1,55 @@
+"""The C ABI library loads and exports every symbol include/vtem_b200.h
+declares (CPU: no compute call is made)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from vtem_b200 import _abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, "include", "vtem_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(vtb_\w+)\s*\(", src)))
+
+
+def test_library_loads_and_exports_header():
+    lib = _abi.lib()
+    syms = header_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(lib, s), s
+
+
+def test_every_header_symbol_has_a_binding():
+    bound = set(_abi.SIGNATURES) | {"vtb_status_string"}
+    missing = [s for s in header_symbols() if s not in bound]
+    assert not missing, missing
+
+
+def test_version_and_status_strings():
+    lib = _abi.lib()
+    assert lib.vtb_version() == 1
+    assert _abi.status_string(0) == "ok"
+    assert "overflow" in _abi.status_string(_abi.VTB_OVERFLOW)
+
+
+def test_bad_arguments_rejected_without_gpu():
+    # argument validation happens before any CUDA call
+    lib = _abi.lib()
+    st = lib.vtb_compute_q(None, None, None, -1, None, None, None, None, None, None)
+    assert st == _abi.VTB_BAD_ARG
+    st = lib.vtb_iaf_encode(None, 0, 0, 4, 10, 0, 1e-4, None, None, None, None, None, None, 0, 0, 0, 0, None,
+                            None, None, None, None, 1, None, 0.0, None, None)
+    assert st == _abi.VTB_BAD_ARG
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    monkeypatch.setattr(_abi, "_lib", None)
+    monkeypatch.setattr(_abi, "LIB_PATH", str(tmp_path / "nope.so"))
+    with pytest.raises(RuntimeError, match="not built"):
+        _abi.lib()

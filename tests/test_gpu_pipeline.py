@@ -1,0 +1,115 @@
+"""End-to-end parity on the small configuration (32x32, 2000 samples, 128
+Gabor RFs): VTEM_IAF -> VTDM_prep -> VTDM on the GPU against the oracle's
+restatement of the same calls (GPU)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import vtem_oracle as O
+from vtem_b200 import ensemble_encode, vrf, vtdm, vtem, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small():
+    return workloads.small()
+
+
+def _encode(w, V):
+    g = w.gabor
+    rf = vrf.vrf_gabor((w.Py, w.Px), dx=w.dx, dy=w.dy)
+    rf.load_parameters(num_neurons=w.N, h_alpha=g.h_alpha, h_l=g.h_l, h_x0=g.h_x0, h_y0=g.h_y0, h_ab=g.h_ab,
+                       KAPPA=g.KAPPA, h_gain=g.gain)
+    iaf = ensemble_encode.IAF_encode(w.N, w.dt)
+    iaf.load_parameters(h_kappa=w.kappa, h_bias=w.bias, h_delta=w.delta, h_v0=w.v0)
+    store, sp = vtem.VTEM_IAF(V, None, w.Wt, rf, w.Wx, w.Wy, dx=w.dx, dy=w.dy, fps=1.0 / w.dt, npinput=True,
+                              iaf=iaf, return_spikes=True)
+    return store, sp, rf
+
+
+def test_encode_matches_oracle_on_same_projection(small):
+    w = small
+    V = w.video(device="cuda")
+    store, sp, rf = _encode(w, V)
+    L = rf.filter(V).cpu().numpy()                            # GPU projection
+    g = w.gabor
+    rfo = O.gabor_rf(g.h_alpha, g.h_l, g.h_x0, g.h_y0, g.h_ab, w.Px, w.Py, 1.0, 1.0, -0.5, -0.5, g.KAPPA, g.gain)
+    Lo = O.rf_filter(V.cpu().numpy(), rfo, w.dx, w.dy)
+    assert np.linalg.norm(L - Lo) / np.linalg.norm(Lo) < 1e-13
+    enc = O.vtem_encode(L, w.dt, w.kappa, w.bias, w.delta, w.v0)   # oracle IAF on the same input
+    rd = store
+    assert rd.refresh_interval == len(enc.block_counts)
+    for b in range(len(enc.block_counts)):
+        assert np.array_equal(rd.spike_count[b], enc.block_counts[b])
+        assert np.array_equal(rd.spikes[b], enc.block_spikes[b])       # bit-exact spike times
+    assert sp.near_threshold == enc.near_threshold
+    # oracle IAF on the oracle projection: identical spike counts unless a
+    # crossing sits within rounding of a sample boundary (counted above)
+    enc2 = O.vtem_encode(Lo, w.dt, w.kappa, w.bias, w.delta, w.v0)
+    s1 = np.concatenate(enc.block_steps)
+    s2 = np.concatenate(enc2.block_steps)
+    assert len(s1) == len(s2) and (s1 != s2).sum() <= enc2.near_threshold
+
+
+@pytest.mark.parametrize("rcond", [1e-10, 1e-8])
+def test_decode_matches_oracle(small, rcond):
+    w = small
+    V = w.video(device="cuda")
+    store, sp, rf = _encode(w, V)
+    prep = vtdm.VTDM_prep(store, None, None, w.Mx, w.My)
+    u = vtdm.VTDM(store, None, None, 0.0, w.T, w.dt, w.Mx, Mt=w.Mt, rcond=rcond, output_format=2, prep=prep)
+    # oracle decode of the very same spikes
+    rd = vtem_read(store)
+    rd.select_neurons([-0.5, 0.5, -0.5, 0.5])
+    tk1, tk2, ind, kap, dl, bia, sig = rd.read_select_spikes([0.0, w.T])
+    g = w.gabor
+    norm = np.ones(w.N)
+    Ds, dirich, Dsw = O.prep_decoder_gabor(g.h_alpha, g.h_l, g.h_x0, g.h_y0, g.h_ab, g.KAPPA, g.gain, w.Mx, w.My,
+                                           w.Wx, w.Wy, w.dx, w.dy, w.Px, w.Py, norm)
+    assert np.abs(prep.Ds.cpu().numpy() - Ds).max() < 1e-12 * np.abs(Ds).max()
+    assert np.abs(prep.dirich.cpu().numpy() - dirich).max() < 1e-12 * np.abs(dirich).max()
+    uo, c, q, G, kept = O.decode_window(tk1, tk2, ind, kap, dl, bia, norm, Dsw, dirich, w.Wt, w.Mt, w.T, w.dt,
+                                        rcond=rcond)
+    rel = np.linalg.norm(u - uo) / np.linalg.norm(uo)
+    assert rel <= 1e-8, rel
+    Vh = V.cpu().numpy()
+    snr = -20 * np.log10(np.linalg.norm(u - Vh) / np.linalg.norm(Vh))
+    assert snr > 20  # reference decoder on this RF bank (see the model-mismatch note in DESIGN)
+
+
+def test_rnn_decode_matches_oracle(small):
+    w = small
+    V = w.video(device="cuda")
+    store, sp, rf = _encode(w, V)
+    prep = vtdm.VTDM_prep(store, None, None, w.Mx, w.My)
+    T = 0.05
+    u = vtdm.VTDM(store, None, None, 0.0, T, w.dt, w.Mx, Mt=w.Mt, rnn=True, alpha=5000, steps=200,
+                  output_format=2, prep=prep)
+    rd = vtem_read(store)
+    rd.select_neurons([-0.5, 0.5, -0.5, 0.5])
+    tk1, tk2, ind, kap, dl, bia, sig = rd.read_select_spikes([0.0, T])
+    norm = np.ones(w.N)
+    Dsw = prep.Dsw.cpu().numpy()
+    dirich = prep.dirich.cpu().numpy()
+    uo, *_ = O.decode_window(tk1, tk2, ind, kap, dl, bia, norm, Dsw, dirich, w.Wt, w.Mt, T, w.dt,
+                             rnn=(1e-6, 5000, 200))
+    assert np.linalg.norm(u - uo) / np.linalg.norm(uo) < 1e-10
+
+
+def test_stitched_decode_runs(small):
+    w = small
+    V = w.video(device="cuda")
+    store, sp, rf = _encode(w, V)
+    prep = vtdm.VTDM_prep(store, None, None, w.Mx, w.My)
+    u = vtdm.VTDM(store, None, None, 0.0, 0.1, w.dt, w.Mx, Mt=w.Mt, rcond=1e-10, stitching=True,
+                  stitch_interval=0.04, output_format=2, prep=prep)
+    assert u.shape == (1000, 32, 32) and np.isfinite(u).all()
+
+
+def vtem_read(store):
+    from vtem_b200 import spike_store as ss
+    rd = ss.vtem_storage_read(store)
+    rd.read_vrf_type()
+    rd.read_num_neurons()
+    return rd

@@ -1,0 +1,96 @@
+"""Host-side logic of the path against the oracle (CPU)."""
+import numpy as np
+
+from oracle import vtem_oracle as O
+from vtem_b200 import spike_store as ss
+from vtem_b200 import vtdm, vtem, workloads
+
+
+def _store_from_blocks(counts, spikes, R, N):
+    st = ss.vtem_storage(None, N, "gabor")
+    st.write_video_attributes(1.0, 2.0, 3.0, 8, 8, 0.1, 0.1)
+    st.vrf["alpha"].append(np.ones(N))
+    st.vrf["x0"].append(np.linspace(-0.3, 0.3, N))
+    st.vrf["y0"].append(np.linspace(0.2, -0.2, N))
+    st.vrf["l"].append(np.zeros(N))
+    st.vrf["ab"].append(np.zeros(N, np.int32))
+    st.data["vrf/KAPPA"] = np.array(2.5)
+    st.iaf["kappa"].append(np.ones(N))
+    st.iaf["delta"].append(np.ones(N))
+    st.iaf["bias"].append(np.ones(N))
+    st.iaf["sigma"].append(np.zeros(N))
+    st.write_refresh_interval(R)
+    for c, s in zip(counts, spikes):
+        st.write_spike_in_timebin(c, s)
+    st.close()
+    return st
+
+
+def _random_blocks(rng, N, nb, R):
+    counts, spikes = [], []
+    for b in range(nb):
+        c = rng.integers(0, 5, N).astype(np.int32)
+        s = np.concatenate([np.sort(rng.uniform(0, R, k)) for k in c]) if c.sum() else np.zeros(0)
+        counts.append(c)
+        spikes.append(s)
+    return counts, spikes
+
+
+def test_read_select_spikes_matches_oracle():
+    rng = np.random.default_rng(3)
+    N, nb, R = 7, 9, 0.01
+    counts, spikes = _random_blocks(rng, N, nb, R)
+    st = _store_from_blocks(counts, spikes, R, N)
+    rd = ss.vtem_storage_read(st)
+    rd.read_vrf_type()
+    rd.read_num_neurons()
+    for dom in ([-0.5, 0.5, -0.5, 0.5], [-0.1, 0.35, -0.5, 0.5]):
+        rd.select_neurons(dom)
+        choose, sx, sy = O.select_neurons(rd.d["vrf/x0"], rd.d["vrf/y0"], dom)
+        assert np.array_equal(rd.choose, choose)
+        for tf in ([0.0, 0.09], [0.013, 0.05], [0.02, 0.021]):
+            a = rd.read_select_spikes(tf)
+            b = O.read_select_spikes(counts, spikes, R, choose, tf)
+            for x, y in zip(a[:3], b):
+                assert np.array_equal(x, y)
+
+
+def test_wx_wy_swapped_in_store():
+    st = ss.vtem_storage(None, 1, "cs")
+    st.write_video_attributes(1.0, 2.0, 3.0, 8, 8, 0.1, 0.1)
+    st.close()
+    rd = ss.vtem_storage_read(st)
+    Wt, Wx, Wy = rd.read_video_attributes()[:3]
+    assert (Wt, Wx, Wy) == (1.0, 3.0, 2.0)
+
+
+def test_block_schedule_and_frames():
+    assert vtem.one_time_frames(2000) == 101
+    assert vtem.one_time_frames(50) == 51
+    assert O.block_schedule(2000)[-1] == (1900, 2000)
+    assert len(O.block_schedule(2000)) == 20
+    assert len(O.block_schedule(2001)) == 21
+
+
+def test_norm_and_period_grid():
+    h = vtdm._norm_from_sigma(np.array([1.0, 2.0, 1.0]), np.array([0.0, 0.5, 0.25]))
+    np.testing.assert_allclose(h, O.h_norm_from_sigma(np.array([1.0, 2.0, 1.0]), np.array([0.0, 0.5, 0.25])))
+    assert vtdm.period_grid(3, 3, 2 * np.pi * 3, 2 * np.pi * 3, 1 / 32, 1 / 32) == O.rf_period_grid(
+        3, 3, 2 * np.pi * 3, 2 * np.pi * 3, 1 / 32, 1 / 32)
+    assert O.default_Mt(2 * np.pi * 20) == 40
+
+
+def test_small_workload_video_and_bank():
+    w = workloads.small()
+    V = w.video().numpy()
+    assert V.shape == (2000, 32, 32)
+    assert abs(np.abs(V).max() - 1.0) < 1e-12
+    a = w.coeffs
+    # Hermitian coefficients inside the ellipse give a real video
+    assert np.allclose(a, np.conj(a[::-1, ::-1, ::-1]))
+    Vo = O.bandlimited_video(a * w.scale, w.Mx, w.My, w.Mt, w.Wx, w.Wy, w.Wt, w.Px, w.Py, 1.0, 1.0, 50, w.dt)
+    np.testing.assert_allclose(V[:50], Vo, atol=1e-12)
+    g = w.gabor
+    rf = O.gabor_rf(g.h_alpha, g.h_l, g.h_x0, g.h_y0, g.h_ab, w.Px, w.Py, 1.0, 1.0, -0.5, -0.5, g.KAPPA, g.gain)
+    np.testing.assert_allclose(np.sqrt((rf ** 2).sum((1, 2)) * w.dx * w.dy), 1.0, rtol=1e-12)
+    assert w.N == 128 and (w.delta > 0).all()

@@ -1,0 +1,105 @@
+"""ctypes binding of ``libvtem_b200.so`` (the C ABI in ``include/vtem_b200.h``).
+
+There is no fallback: if the library is missing, importing a compute function
+raises, and every call on a tensor that is not on a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libvtem_b200.so")
+
+VTB_OK = 0
+VTB_BAD_ARG = 1
+VTB_OVERFLOW = 2
+VTB_OOM = 3
+VTB_TIMEOUT = 4
+VTB_CUDA_ERR = 5
+VTB_NOT_CONVERGED = 6
+VTB_NO_DATA = 7
+
+P = ctypes.c_void_p
+I = ctypes.c_int
+L = ctypes.c_int64
+D = ctypes.c_double
+
+# name -> argtypes (restype int)
+SIGNATURES = {
+    "vtb_version": [],
+    "vtb_last_cuda_error": [],
+    "vtb_rf_gabor": [P, P, P, P, P, P, I, I, I, D, D, D, D, D, P, L, P],
+    "vtb_rf_cs": [P, P, P, P, I, I, I, D, D, D, D, D, D, P, L, P],
+    "vtb_rf_filter": [P, I, I, L, P, I, L, D, P, L, L, P],
+    "vtb_gemm_f64": [I, I, I, P, L, L, P, L, L, P, L, L, D, D, P],
+    "vtb_iaf_encode": [P, L, L, I, I, I, D, P, P, P, P, P, P, L, L, L, I, P, P, P, P, P, I, P, D, P, P],
+    "vtb_dirichlet_coeffs": [P, I, I, I, L, I, I, D, P, P],
+    "vtb_dirich_space": [P, I, I, I, I, I, I, I, P, P],
+    "vtb_dsw": [P, I, I, P, P, L, P],
+    "vtb_compute_q": [P, P, P, I, P, P, P, P, P, P],
+    "vtb_compute_G": [P, P, P, I, D, I, P, L, D, I, P, L, P],
+    "vtb_solve_eq_sym_workspace": [I, P],
+    "vtb_solve_eq_sym": [P, L, P, P, I, D, P, L, P, P],
+    "vtb_rnn": [P, L, P, P, P, P, I, D, I, P, I, P],
+    "vtb_reconstruct_workspace": [I, I, I, P],
+    "vtb_reconstruct": [P, I, I, P, P, P, P, P, I, P, I, I, D, P, P, L, P],
+}
+
+_lib = None
+
+
+class VtbError(RuntimeError):
+    def __init__(self, fn, status):
+        self.status = status
+        msg = "%s failed: %s (status %d)" % (fn, status_string(status), status)
+        if status == VTB_CUDA_ERR and _lib is not None:
+            msg += ", cudaError %d" % _lib.vtb_last_cuda_error()
+        super().__init__(msg)
+
+
+def lib():
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "vtem_b200 CUDA library not built (%s); run `python -m vtem_b200.build`" % LIB_PATH)
+        l = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(l, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        l.vtb_status_string.argtypes = [ctypes.c_int]
+        l.vtb_status_string.restype = ctypes.c_char_p
+        _lib = l
+    return _lib
+
+
+def status_string(status: int) -> str:
+    return lib().vtb_status_string(int(status)).decode()
+
+
+def call(name, *args):
+    """Call ``name`` and raise :class:`VtbError` on a nonzero status."""
+    st = getattr(lib(), name)(*args)
+    if st != VTB_OK:
+        raise VtbError(name, st)
+    return st
+
+
+def stream_ptr(device=None):
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def dptr(t: torch.Tensor | None, dtype=None):
+    """Device pointer of a CUDA tensor (None -> NULL)."""
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("vtem_b200 kernels take CUDA tensors (got a %s tensor)" % t.device)
+    if dtype is not None and t.dtype != dtype:
+        raise TypeError("expected %s, got %s" % (dtype, t.dtype))
+    return t.data_ptr()

@@ -1,0 +1,227 @@
+// Ideal IAF time encoder: warp-per-neuron FP64 scan.
+//
+// Semantics follow the reference kernels exactly (vtem/ensemble_encode.py:
+// 438-552 deterministic thresholds, :555-674 random thresholds, including the
+// draw of the next threshold before `area -= (delta - v0)` at :623-627) and
+// VTEM_IAF's block loop (vtem/vtem.py:165-200): frames are grouped in blocks of
+// `block_frames` sharing one boundary frame, time_count restarts at 0 at every
+// block boundary and v0 carries over.  Spike times are block-relative, as the
+// reference stores them.
+//
+// This file is compiled with --fmad=false: every product and sum rounds
+// separately, in the reference's source order, so spike times and sample
+// indices are bit-identical to a non-contracting host execution of the
+// reference kernel.
+//
+// Work split: one warp per neuron.  For each chunk of 32 steps the lanes load
+// 32 samples (coalesced when the input is neuron-major), form y = (x+b)/kappa
+// and the trapezoid area of their own step in parallel, and stage them in
+// shared memory; the warp then walks the 32 steps in order (the membrane
+// recursion is a strict sequential FP64 chain that no reordering may touch).
+// The common step is one add and one compare; steps with a threshold crossing
+// or a negative slope take the reference's full loop.  Spikes are appended by
+// lane 0 to the neuron's slice of the output.  Each neuron stops once its
+// spike count reaches `cap`, which bounds every loop by the buffer size.
+#include "common.cuh"
+
+namespace vtb {
+
+struct IafArgs {
+    const double* in;
+    int64_t ts, ns;          // strides of in(t, n)
+    int N, F, block_frames;
+    double dt;
+    const double* kappa;
+    const double* bias;
+    const double* delta;     // threshold (mean threshold for random thresholds)
+    double* v0;
+    double* time_count;
+    // random thresholds (randn == nullptr: deterministic)
+    const double* randn;
+    int64_t rb, rs, rn;      // strides of randn(block, slot, n)
+    int block_cap;           // slots per block in randn
+    const double* sigma;
+    double* delta_value;
+    // outputs, neuron-major [n * cap + j]
+    double* spike_time;
+    int32_t* spike_step;
+    int32_t* spike_count;
+    int cap;
+    unsigned long long* near_count;
+    double near_eps;
+    int32_t* status;
+};
+
+constexpr int kIafWarps = 4;
+
+template <bool RT>
+__global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
+    __shared__ double s_area[kIafWarps][32];
+    __shared__ double s_y1[kIafWarps][32];
+    __shared__ double s_y2[kIafWarps][32];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const int n = blockIdx.x * kIafWarps + w;
+    if (n >= p.N) return;  // uniform per warp
+
+    const double kap = p.kappa[n];
+    const double bia = p.bias[n];
+    const double dt = p.dt;
+    const double dmean = p.delta[n];
+    const double sg = RT ? p.sigma[n] : 0.0;
+    double delta = RT ? p.delta_value[n] : dmean;
+    double v0 = p.v0[n];
+    double tc = p.time_count[n];
+    int count = 0;
+    int cnt_block = 0;
+    int block = 0;
+    unsigned long long near = 0;
+    bool stop = false;
+
+    const int steps = p.F - 1;
+    const int bstep = p.block_frames - 1;
+    int next_reset = bstep > 0 ? bstep : 0x7fffffff;
+    const double* base = p.in + (int64_t)n * p.ns;
+    auto ld = [&](int t) -> double { return t < p.F ? __ldg(base + (int64_t)t * p.ts) : 0.0; };
+
+    double ycur = (ld(lane) + bia) / kap;
+    double ynext = (ld(32 + lane) + bia) / kap;
+
+    for (int t0 = 0; t0 < steps && !stop; t0 += 32) {
+        const double xpre = ld(t0 + 64 + lane);
+        double y2l = __shfl_down_sync(full, ycur, 1);
+        const double yn0 = __shfl_sync(full, ynext, 0);
+        if (lane == 31) y2l = yn0;
+        const double areal = (ycur + y2l) / 2 * dt;
+        const bool posl = (y2l >= 0 || (y2l < 0 && ycur <= 0));
+        const unsigned posmask = __ballot_sync(full, posl);
+        s_area[w][lane] = areal;
+        s_y1[w][lane] = ycur;
+        s_y2[w][lane] = y2l;
+        __syncwarp();
+        const int nst = min(32, steps - t0);
+        for (int j = 0; j < nst; ++j) {
+            const int g = t0 + j;
+            if (g == next_reset) {  // start of the next frame block
+                tc = 0.0;
+                cnt_block = 0;
+                ++block;
+                next_reset += bstep;
+            }
+            const double area0 = s_area[w][j];
+            const bool pos = (posmask >> j) & 1u;
+            if (pos) {
+                const double s = v0 + area0;
+                near += (fabs(s - delta) < p.near_eps) ? 1ull : 0ull;
+                if (!(s >= delta)) {  // the common step: no crossing
+                    v0 = s;
+                    tc += dt;
+                    continue;
+                }
+                // crossing(s) inside this step: the reference's loop
+                double y1 = s_y1[w][j];
+                const double y2 = s_y2[w][j];
+                double area = area0;
+                double ddt = dt;
+                for (;;) {
+                    const double a = ((y2 - y1) / ddt);
+                    const double remain = (fabs(a) <= 1e-12) ? ((delta - v0) / y1)
+                                                             : (sqrt(y1 * y1 + 2 * (delta - v0) * a) - y1) / (a);
+                    tc += remain;
+                    if (RT) {
+                        const int slot = cnt_block < p.block_cap - 1 ? cnt_block : p.block_cap - 1;
+                        delta = p.randn[(int64_t)block * p.rb + (int64_t)slot * p.rs + (int64_t)n * p.rn] * sg + dmean;
+                    }
+                    if (lane == 0) {
+                        p.spike_time[(int64_t)n * p.cap + count] = tc;
+                        p.spike_step[(int64_t)n * p.cap + count] = g;
+                    }
+                    ++count;
+                    ++cnt_block;
+                    area -= (delta - v0);
+                    v0 = 0;
+                    ddt -= remain;
+                    y1 = y1 + remain * a;
+                    if (count >= p.cap) { stop = true; break; }
+                    const double s2 = v0 + area;
+                    near += (fabs(s2 - delta) < p.near_eps) ? 1ull : 0ull;
+                    if (!(s2 >= delta)) break;
+                }
+                if (stop) break;
+                v0 += area;
+                tc += ddt;
+            } else {
+                // negative slope through zero (ensemble_encode.py:515-535)
+                double y1 = s_y1[w][j];
+                const double y2 = s_y2[w][j];
+                double ddt = dt;
+                double a = ((y2 - y1) / ddt);
+                double remain;
+                for (;;) {
+                    remain = y1 * y1 + 2 * (delta - v0) * a;
+                    near += (fabs(remain) < p.near_eps) ? 1ull : 0ull;
+                    if (!(remain >= 0)) break;
+                    remain = (sqrt(remain) - y1) / a;
+                    tc += remain;
+                    if (RT) {
+                        const int slot = cnt_block < p.block_cap - 1 ? cnt_block : p.block_cap - 1;
+                        delta = p.randn[(int64_t)block * p.rb + (int64_t)slot * p.rs + (int64_t)n * p.rn] * sg + dmean;
+                    }
+                    if (lane == 0) {
+                        p.spike_time[(int64_t)n * p.cap + count] = tc;
+                        p.spike_step[(int64_t)n * p.cap + count] = g;
+                    }
+                    ++count;
+                    ++cnt_block;
+                    v0 = 0;
+                    ddt -= remain;
+                    y1 = y1 + remain * a;
+                    a = ((y2 - y1) / ddt);
+                    if (count >= p.cap) { stop = true; break; }
+                }
+                if (stop) break;
+                v0 += (y1 + y2) / 2 * ddt;
+                tc += ddt;
+            }
+        }
+        __syncwarp();
+        ycur = ynext;
+        ynext = (xpre + bia) / kap;
+    }
+    if (lane == 0) {
+        p.v0[n] = v0;
+        p.time_count[n] = tc;
+        p.spike_count[n] = count;
+        if (RT) p.delta_value[n] = delta;
+        if (p.near_count && near) atomicAdd(p.near_count, near);
+        if (stop && p.status) atomicExch(p.status, VTB_OVERFLOW);
+    }
+}
+
+}  // namespace vtb
+
+using namespace vtb;
+
+VTB_API int vtb_iaf_encode(const double* input, int64_t in_t_stride, int64_t in_n_stride, int N, int F,
+                           int block_frames, double dt, const double* kappa, const double* bias,
+                           const double* delta, double* v0, double* time_count, const double* randn,
+                           int64_t randn_block_stride, int64_t randn_slot_stride, int64_t randn_n_stride,
+                           int randn_block_cap, const double* sigma, double* delta_value, double* spike_time,
+                           int32_t* spike_step, int32_t* spike_count, int cap,
+                           unsigned long long* near_count, double near_eps, int32_t* status, void* stream) {
+    VTB_CHECK_ARG(N >= 0 && F >= 0 && block_frames >= 1 && cap >= 1);
+    if (N == 0) return VTB_OK;
+    VTB_CHECK_ARG(input && kappa && bias && delta && v0 && time_count && spike_time && spike_step &&
+                  spike_count);
+    if (randn) VTB_CHECK_ARG(sigma && delta_value && randn_block_cap >= 1);
+    IafArgs a{input, in_t_stride, in_n_stride, N, F, block_frames, dt, kappa, bias, delta, v0, time_count,
+              randn, randn_block_stride, randn_slot_stride, randn_n_stride, randn_block_cap, sigma,
+              delta_value, spike_time, spike_step, spike_count, cap, near_count, near_eps, status};
+    const int blocks = ceil_div(N, kIafWarps);
+    if (randn)
+        iaf_scan_kernel<true><<<blocks, kIafWarps * 32, 0, as_stream(stream)>>>(a);
+    else
+        iaf_scan_kernel<false><<<blocks, kIafWarps * 32, 0, as_stream(stream)>>>(a);
+    return launch_status();
+}

@@ -1,0 +1,37 @@
+// Status codes, error bookkeeping and version of the C ABI.
+#include "common.cuh"
+
+namespace vtb {
+
+static thread_local int g_last_cuda_error = 0;
+
+void set_last_cuda_error(cudaError_t e) { g_last_cuda_error = (int)e; }
+
+int launch_status() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        g_last_cuda_error = (int)e;
+        return VTB_CUDA_ERR;
+    }
+    return VTB_OK;
+}
+
+}  // namespace vtb
+
+VTB_API int vtb_version(void) { return VTB_ABI_VERSION; }
+
+VTB_API int vtb_last_cuda_error(void) { return vtb::g_last_cuda_error; }
+
+VTB_API const char* vtb_status_string(int status) {
+    switch (status) {
+        case VTB_OK: return "ok";
+        case VTB_BAD_ARG: return "bad argument";
+        case VTB_OVERFLOW: return "spike buffer overflow";
+        case VTB_OOM: return "out of device memory";
+        case VTB_TIMEOUT: return "timed out";
+        case VTB_CUDA_ERR: return "CUDA error";
+        case VTB_NOT_CONVERGED: return "solver did not converge";
+        case VTB_NO_DATA: return "no spikes to decode";
+        default: return "unknown status";
+    }
+}

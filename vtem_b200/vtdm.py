@@ -1,0 +1,227 @@
+"""Video time decoding machines (reference: ``vtem/vtdm.py``).
+
+``VTDM_prep`` (vtdm.py:311-447) builds the decoder's RF bank on one spatial
+period, the Dirichlet coefficients, the spatial reconstruction functions and
+the RF cross-weights.  ``VTDM`` (vtdm.py:450-699) decodes a time range,
+window by window with optional temporal stitching (Hann cross-fade), by
+the pseudoinverse or the RNN solver.
+
+Extensions (keyword-only; defaults are the reference's behaviour):
+``rcond`` (the reference hard-codes 1e-8 through solve_eq_sym's default,
+vtdm.py:648), ``return_device`` (keep the video on the GPU), ``prep``
+(VTDM_prep's in-memory result instead of the two files).  The reference
+writes the video as .avi (output_format 0, needs OpenCV) or .h5 (1); here
+both write ``output + ".npy"``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import dirichlet as dr
+from . import linalg as ls
+from . import neural_network as nn
+from . import simpleio
+from . import spike_store as ss
+from . import vrf
+
+
+@dataclass
+class PrepResult:
+    Ds: torch.Tensor        # (N, 2My+1, 2Mx+1) complex128
+    dirich: torch.Tensor    # (N, decPy, decPx) float64
+    Dsw: torch.Tensor       # (N, N) float64
+    h_norm: np.ndarray
+    Mx: int
+    My: int
+    decPx: int
+    decPy: int
+    Px1: int
+    Py1: int
+
+
+def _norm_from_sigma(h_kappa, h_sigma):
+    """h_norm = 1/(kappa sigma), 1 where sigma == 0, normalised to its max
+    (vtdm.py:408-412, :634-637)."""
+    h_norm = np.ones(len(h_kappa), np.float64)
+    nz = np.nonzero(h_sigma != 0)
+    h_norm[nz] = 1.0 / (h_kappa[nz] * h_sigma[nz])
+    return h_norm / h_norm.max()
+
+
+def _domain(domain, oriSx, oriSy):
+    if domain is None:
+        return [-oriSx / 2, oriSx / 2, -oriSy / 2, oriSy / 2]
+    return [max(float(domain[0]), -oriSx / 2), min(float(domain[1]), oriSx / 2),
+            max(float(domain[2]), -oriSy / 2), min(float(domain[3]), oriSy / 2)]
+
+
+def period_grid(Mx, My, Wx, Wy, dx, dy):
+    """RF grid over one spatial period (vtdm.py:385-388)."""
+    rfSx = (2 * np.pi) * (Mx / Wx)
+    rfSy = (2 * np.pi) * (My / Wy)
+    rfPx = int(np.ceil(rfSx / dx / 16) * 16)
+    rfPy = int(np.ceil(rfSy / dy / 16) * 16)
+    return rfSx, rfSy, rfPx, rfPy
+
+
+def decoder_bank(spfile, Mx, My, Wx, Wy, dx, dy, dtype=np.complex128):
+    """The decoder-side RF object of the selected neurons, sampled at 4x on
+    one spatial period (vtdm.py:423-435)."""
+    rfSx, rfSy, rfPx, rfPy = period_grid(Mx, My, Wx, Wy, dx, dy)
+    if spfile.filter_type == "gabor":
+        gb = vrf.vrf_gabor((rfPy, rfPx), dx=rfSx / rfPx, dy=rfSy / rfPy, scale=4, dtype=dtype)
+        gb.load_parameters(num_neurons=spfile.decode_neurons, h_alpha=spfile.alpha, h_l=spfile.l,
+                           h_x0=spfile.x0, h_y0=spfile.y0, h_ab=spfile.ab, KAPPA=spfile.KAPPA, h_gain=spfile.gain)
+    else:
+        gb = vrf.vrf_cs((rfPy, rfPx), dx=rfSx / rfPx, dy=rfSy / rfPy, scale=4, dtype=dtype)
+        gb.load_parameters(num_neurons=spfile.decode_neurons, h_alpha=spfile.alpha, h_x0=spfile.x0,
+                           h_y0=spfile.y0, sigma_center=spfile.sigma_center, sigma_surround=spfile.sigma_surround,
+                           h_gain=spfile.gain)
+    return gb
+
+
+def prep_from_banks(banks, h_norm, Mx, My, Wx, Wy, decPx, decPy, decSx, decSy):
+    """Ds, phi and Dsw of one or several decoder-side RF objects (each on
+    one spatial period), concatenated in order."""
+    Ds = torch.cat([b.compute_Ds(Mx, My) for b in banks], 0)
+    dirich = banks[0].compute_dirich_space_fft(Ds, Mx, My, decPx, decPy, decSx, decSy, Wx, Wy)
+    Dsw = banks[0].compute_Dsw(Ds, Mx, My, h_norm)
+    dx = decSx / decPx
+    dy = decSy / decPy
+    Px1 = int(np.round(banks[0].Sx / dx))
+    Py1 = int(np.round(banks[0].Sy / dy))
+    return PrepResult(Ds, dirich, Dsw, np.asarray(h_norm), Mx, My, decPx, decPy, Px1, Py1)
+
+
+def VTDM_prep(spikefile, Dswfilename, dirichfilename, Mx, My=None, domain=None, Wx=None, Wy=None,
+              dtype=np.complex128):
+    """Prepare decoding (vtdm.py:311-447).  Writes the spatial functions to
+    ``dirichfilename`` and the cross-weights to ``Dswfilename`` (when not
+    None) and returns a :class:`PrepResult`."""
+    if dtype not in [np.complex128, np.complex64]:
+        raise TypeError("dtype must be complex128 or complex64")
+    spfile = ss.vtem_storage_read(spikefile)
+    spfile.read_vrf_type()
+    spfile.read_num_neurons()
+    Wt, Wx1, Wy1, Px, Py, dx, dy = spfile.read_video_attributes()
+    Wx = Wx1 if Wx is None else float(Wx)
+    Wy = Wy1 if Wy is None else float(Wy)
+    Mx = int(Mx)
+    My = Mx if My is None else int(My)
+    domain = _domain(domain, Px * dx, Py * dy)
+    spfile.select_neurons(domain)
+    h_kappa, h_delta, h_bias, h_sigma = spfile.read_iaf()
+    h_norm = _norm_from_sigma(h_kappa, h_sigma)[spfile.choose]
+    decSx = domain[1] - domain[0]
+    decSy = domain[3] - domain[2]
+    decPx = int(np.round(decSx / dx))
+    decPy = int(np.round(decSy / dy))
+    gb = decoder_bank(spfile, Mx, My, Wx, Wy, dx, dy, np.complex128)
+    prep = prep_from_banks([gb], h_norm, Mx, My, Wx, Wy, decPx, decPy, decSx, decSy)
+    if dirichfilename is not None:
+        simpleio.write_memory_to_file(prep.dirich, dirichfilename)
+    if Dswfilename is not None:
+        simpleio.write_memory_to_file(prep.Dsw, Dswfilename)
+    return prep
+
+
+def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, My=None, Mt=None, domain=None,
+         Wx=None, Wy=None, Wt=None, lamb=0.0, dtype=np.float64, rnn=False, alpha=50000, steps=4000,
+         stitching=False, stitch_interval=None, output_format=0, output="rec", *, rcond=1e-8,
+         return_device=False, prep=None, rnn_dt=1e-6):
+    """Reconstruct a time range of the video (vtdm.py:450-699)."""
+    spfile = ss.vtem_storage_read(spikefile)
+    spfile.read_vrf_type()
+    spfile.read_num_neurons()
+    Wt1, Wx1, Wy1, Px, Py, dx, dy = spfile.read_video_attributes()
+    Wx = Wx1 if Wx is None else float(Wx)
+    Wy = Wy1 if Wy is None else float(Wy)
+    Wt = Wt1 if Wt is None else float(Wt)
+    Mx = int(Mx)
+    My = Mx if My is None else int(My)
+    Mt = int(round(Wt * 2 / 2 / np.pi)) if Mt is None else int(Mt)
+    end = float(end_time)
+    if stitching:
+        if stitch_interval is None:
+            stitch_interval = 20 * dt
+        stitch_interval = min(stitch_interval, end_time)
+        end = round(float(min(start_time + stitch_interval, end_time)) / dt) * dt
+        overlap = 0.2 * stitch_interval
+    else:
+        stitch_interval = float(end_time)
+        overlap = 0
+    domain = _domain(domain, Px * dx, Py * dy)
+    decSx = domain[1] - domain[0]
+    decSy = domain[3] - domain[2]
+    decPx = int(np.round(decSx / dx))
+    decPy = int(np.round(decSy / dy))
+    start = float(start_time)
+    if prep is not None:
+        dirich = prep.dirich
+        Dsw = prep.Dsw
+    else:
+        dirich = torch.as_tensor(simpleio.read_file(dirichfilename), device="cuda")
+        Dsw = torch.as_tensor(simpleio.read_file(Dswfilename), device="cuda")
+    s = dirich.shape
+    total_l = int(round((end_time - start_time) / dt))
+    overlap_l = int(round(overlap / dt))
+    if overlap_l < 3:
+        if round(stitch_interval / dt) >= 8:
+            overlap_l = 4
+            overlap = 4 * dt
+        else:
+            overlap = 0
+            overlap_l = 0
+    interval_l = int(round(stitch_interval / dt))
+    left_window = torch.as_tensor(np.hanning(2 * overlap_l)[0:overlap_l], device="cuda").reshape(-1, 1, 1)
+    right_window = 1.0 - left_window
+    u = torch.empty((total_l, decPy, decPx), dtype=torch.float64, device="cuda")
+    spfile.select_neurons(domain)
+    i = 0
+    prev = None
+    while True:
+        tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_sigma = spfile.read_select_spikes([start, end])
+        h_norm = _norm_from_sigma(spfile.read_iaf()[0], h_sigma)[spfile.choose]
+        cp = dr.dirichlet(spfile.decode_neurons, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm, Wt, Mt,
+                          dtype)
+        cp.compute_q()
+        cp.compute_G(Dsw, float(lamb), lower_only=not rnn)
+        if rnn:
+            cp.d_q = nn.rnn3(cp.d_G, cp.d_q, dt=rnn_dt, alpha=alpha, steps=steps)
+        else:
+            cp.d_q = ls.solve_eq_sym(cp.d_G, cp.d_q, rcond=rcond)
+        cp.freeG()
+        u_rec = cp.reconstruct(dirich, [0, round((end - start) / dt) * dt], dt)
+        if overlap_l:
+            if i == 0:
+                if end_time - end < dt:
+                    u = u_rec
+                    break
+                u[0:(interval_l - overlap_l)] = u_rec[0:-overlap_l]
+                prev = u_rec[-overlap_l:]
+            else:
+                l_ind = i * (interval_l - overlap_l)
+                r_ind = (i + 1) * (interval_l - overlap_l)
+                u[l_ind:(l_ind + overlap_l)] = u_rec[0:overlap_l] * left_window + prev * right_window
+                if end_time - end < dt:
+                    u[(l_ind + overlap_l):] = u_rec[(-u.shape[0] + l_ind + overlap_l):]
+                    break
+                u[(l_ind + overlap_l):r_ind] = u_rec[overlap_l:interval_l - overlap_l]
+                prev = u_rec[-overlap_l:]
+        else:
+            u[(i * interval_l):((i * interval_l) + u_rec.shape[0])] = u_rec
+            if end_time - end < dt:
+                break
+        start = start + round(stitch_interval / dt) * dt - round(overlap / dt) * dt
+        end = min(start + round(stitch_interval / dt) * dt, float(end_time))
+        if float(end_time) - end < overlap:
+            end = end_time
+        i = i + 1
+    if output_format in (0, 1):
+        simpleio.write_memory_to_file(u, output + ".npy")
+    if return_device:
+        return u
+    return u.cpu().numpy()
