@@ -1,0 +1,450 @@
+"""Benchmark of the vtem decode path on the B200.
+
+Workload ("gpu" configuration, vtem_b200.workloads.gpu_scale): a seeded
+Dirichlet-bandlimited video, 64x64 pixels x 10000 samples (1 s at dt=1e-4),
+Mx=My=6, Mt=8, encoded by 768 Gabor + 256 centre-surround RFs feeding IAF
+neurons (~25k spike intervals).  Encoding and decoder preparation happen
+before the timed region.
+
+One step = one decode of the clip: device-resident spike intervals -> the
+float64 video (10000, 64, 64) on the device, by the coefficient-space
+decoder (same reconstruction as the reference's pseudoinverse decode; its
+rel-L2 against the plain n x n path is reported).  value = voxels / s.
+e2e = the same decode through the public API from host spike arrays
+(host->device copy inside the timed region) with the video read back to
+pinned host memory.  The plain float64 n x n path (analytic Gram,
+eigendecomposition pseudoinverse, synthesis) is timed once beside it.
+
+L2: the 328 MB output of every step exceeds the 126 MB L2, and a 256 MB
+buffer is written between timed steps.
+
+--impl reference: the reference's own kernels compiled for the host
+(oracle/_ref) with NumPy for its library calls, on a bounded sample of the
+same workload (a decode window of the same spikes), rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "reconstructed voxels/s at >=40 dB SNR (mixed vs FP64 plain)"
+UNIT = "voxels/s"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- setup
+
+def encode_clip(w, device):
+    """Encode the workload's clip on the GPU and prepare the decoder."""
+    import torch
+    from vtem_b200 import ensemble_encode, spike_store, vrf, vtdm, vtem
+
+    V = w.video(device=device)
+    banks = []
+    g = w.gabor
+    gb = vrf.vrf_gabor((w.Py, w.Px), dx=w.dx, dy=w.dy)
+    gb.load_parameters(num_neurons=len(g.h_alpha), h_alpha=g.h_alpha, h_l=g.h_l, h_x0=g.h_x0, h_y0=g.h_y0,
+                       h_ab=g.h_ab, KAPPA=g.KAPPA, h_gain=g.gain)
+    banks.append(gb)
+    if w.cs is not None:
+        c = w.cs
+        cb = vrf.vrf_cs((w.Py, w.Px), dx=w.dx, dy=w.dy)
+        cb.load_parameters(num_neurons=len(c.h_alpha), h_alpha=c.h_alpha, h_x0=c.h_x0, h_y0=c.h_y0,
+                           sigma_center=c.sigma_center, sigma_surround=c.sigma_surround, h_gain=c.gain)
+        banks.append(cb)
+    bank = vrf.vrf_bank(banks) if len(banks) > 1 else banks[0]
+    iaf = ensemble_encode.IAF_encode(w.N, w.dt)
+    iaf.load_parameters(h_kappa=w.kappa, h_bias=w.bias, h_delta=w.delta, h_v0=w.v0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    store, sp = vtem.VTEM_IAF(V, None, w.Wt, bank, w.Wx, w.Wy, dx=w.dx, dy=w.dy, fps=1.0 / w.dt, npinput=True,
+                              iaf=iaf, return_spikes=True)
+    torch.cuda.synchronize()
+    t_enc = time.perf_counter() - t0
+    # decoder prep: the decoder-side RF banks on one spatial period (vtdm.py:385-435)
+    rfSx, rfSy, rfPx, rfPy = vtdm.period_grid(w.Mx, w.My, w.Wx, w.Wy, w.dx, w.dy)
+    dbanks = []
+    gd = vrf.vrf_gabor((rfPy, rfPx), dx=rfSx / rfPx, dy=rfSy / rfPy, scale=4)
+    gd.load_parameters(num_neurons=len(g.h_alpha), h_alpha=g.h_alpha, h_l=g.h_l, h_x0=g.h_x0, h_y0=g.h_y0,
+                       h_ab=g.h_ab, KAPPA=g.KAPPA, h_gain=g.gain)
+    dbanks.append(gd)
+    if w.cs is not None:
+        c = w.cs
+        cd = vrf.vrf_cs((rfPy, rfPx), dx=rfSx / rfPx, dy=rfSy / rfPy, scale=4)
+        cd.load_parameters(num_neurons=len(c.h_alpha), h_alpha=c.h_alpha, h_x0=c.h_x0, h_y0=c.h_y0,
+                           sigma_center=c.sigma_center, sigma_surround=c.sigma_surround, h_gain=c.gain)
+        dbanks.append(cd)
+    prep = vtdm.prep_from_banks(dbanks, np.ones(w.N), w.Mx, w.My, w.Wx, w.Wy, w.Px, w.Py, 1.0, 1.0)
+    rd = spike_store.vtem_storage_read(store)
+    rd.num_neurons = w.N
+    rd.choose = np.arange(w.N)
+    rd.decode_neurons = w.N
+    rd.d["iaf/kappa"], rd.d["iaf/delta"], rd.d["iaf/bias"] = w.kappa, w.delta, w.bias
+    tk1, tk2, ind, kap, dl, bia, _ = rd.read_select_spikes([0.0, w.T])
+    return V, prep, (tk1, tk2, ind), t_enc, sp, rd
+
+
+def flush_l2(buf):
+    buf.add_(1.0)
+
+
+# ---------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    from vtem_b200 import fast, workloads, dirichlet, linalg
+    from vtem_b200._abi import call, dptr, stream_ptr
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev, timeout=__import__("datetime").timedelta(seconds=600))
+    w = workloads.gpu_scale(seed=rank, frames=args.frames)
+    V, prep, (tk1, tk2, ind), t_enc, sp, rd = encode_clip(w, dev)
+    n = len(tk1)
+    Nt = len(np.arange(0, w.T, w.dt))
+    voxels = Nt * w.Px * w.Py
+    dec = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="auto", refine=2)
+    d_tk1 = torch.as_tensor(tk1, device=dev)
+    d_tk2 = torch.as_tensor(tk2, device=dev)
+    d_ind = torch.as_tensor(ind, device=dev)
+    kap = torch.as_tensor(w.kappa, device=dev)
+    dl = torch.as_tensor(w.delta, device=dev)
+    bia = torch.as_tensor(w.bias, device=dev)
+    u = torch.empty((Nt, w.Py, w.Px), dtype=torch.float64, device=dev)
+    flush = torch.zeros(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
+
+    def step():
+        a = dec.coefficients(d_tk1, d_tk2, d_ind, kap, dl, bia, assume_sorted=True)
+        dec.synthesize(a, w.T, w.dt, out=u)
+
+    for _ in range(args.warmup):
+        step()
+        flush_l2(flush)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    for i in range(args.steps):
+        ev[i][0].record()
+        a = dec.coefficients(d_tk1, d_tk2, d_ind, kap, dl, bia, assume_sorted=True)
+        sev[i][0].record()
+        dec.synthesize(a, w.T, w.dt, out=u)
+        sev[i][1].record()
+        ev[i][1].record()
+        flush_l2(flush)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in ev]
+    synth_ms = [s.elapsed_time(e) for s, e in sev]
+    tot_ms = sum(step_ms)
+    t = torch.tensor([tot_ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tot_ms = float(t.item())
+    value = voxels * world * args.steps / (tot_ms / 1e3)
+
+    # --- end to end through the public API with host buffers
+    h_tk1, h_tk2, h_ind = (torch.as_tensor(x).pin_memory() for x in (tk1, tk2, ind))
+    h_u = torch.empty((Nt, w.Py, w.Px), dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        g1 = h_tk1.to(dev, non_blocking=True)
+        g2 = h_tk2.to(dev, non_blocking=True)
+        gi = h_ind.to(dev, non_blocking=True)
+        uu = dec.decode(g1, g2, gi, kap, dl, bia, w.T, w.dt, out=u, assume_sorted=True)
+        h_u.copy_(uu, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 5))
+    e2e_ms = 0.0
+    for _ in range(e2e_steps):
+        flush_l2(flush)
+        e0.record()
+        e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    te = torch.tensor([e2e_ms], device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = voxels * world * e2e_steps / (float(te.item()) / 1e3)
+    h2d = n * (8 + 8 + 4)
+    d2h = voxels * 8
+
+    # --- accuracy of the fast path: against the plain float64 n x n path (rank 0)
+    result = None
+    if rank == 0:
+        plain = {}
+        if not args.no_plain:
+            plain = run_plain(w, prep, tk1, tk2, ind, u, dev, Nt)
+        synth_bytes = voxels * 8 + Nt * dec.Ks * 16
+        synth_avg = sum(synth_ms) / len(synth_ms) / 1e3
+        peaks = load_peaks()
+        achieved = synth_bytes / synth_avg / 1e9
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Dirichlet-bandlimited video)",
+            "config": {"workload": "gpu: 64x64 px, 10000 samples (1 s, dt=1e-4), Mx=My=6, Mt=8, 768 Gabor + 256 "
+                                   "centre-surround RFs, IAF b~U(2,4) delta~N(0.12,0.012), pinv rcond 1e-8",
+                       "spike_intervals": n, "voxels_per_step": voxels, "K_coeff": dec.K,
+                       "decoder": "coefficient-space (Phi^H Phi, %s solve)" % dec.last_solver,
+                       "l2": "output 328 MB > L2 and a 256 MB flush between steps", "clip_per_rank": True,
+                       "parallelism": "clip-parallel replicas" if world > 1 else "single GPU"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps * launches_per_step(dec),
+            "roofline": {"bound": "hbm", "kernel": "synth (temporal_expand + synth_kernel)",
+                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                         "traffic": measured_traffic(voxels), "algorithmic_bytes": synth_bytes,
+                         "avg_ms": synth_avg * 1e3},
+            "stages_ms": {"coefficients": (tot_ms - sum(synth_ms)) / args.steps, "synthesis": sum(synth_ms) / args.steps,
+                          "encode_once": t_enc * 1e3},
+            "clocks": clk,
+            "plain_fp64": plain,
+            "solver": {"kind": dec.last_solver, "pivots_or_eigs": dec.last_pivots},
+            "near_threshold_events": int(sp.near_threshold),
+        }
+        if not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(w, prep, rd)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def launches_per_step(dec):
+    # temporal_gram 1, kron_gram 1, kron_rhs 1, solve: chol_pivots 1 + 2 per refinement
+    # (cuSOLVER's own kernels not counted), synthesis 2
+    if dec.last_solver == "chol":
+        solve = 1 + 2 * dec.refine
+    else:
+        solve = 3
+    return 1 + 2 + solve + 2
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]), "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def measured_traffic(voxels):
+    """DRAM bytes per synthesis launch from the committed ncu summary, scaled
+    to this workload's output size (null when no capture is committed)."""
+    p = os.path.join(ROOT, "profiles", "synth_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d["dram_bytes"] * voxels / d["voxels"]
+    except Exception:
+        return None
+
+
+def run_plain(w, prep, tk1, tk2, ind, u_fast, dev, Nt):
+    """The plain float64 path of the reference on the whole clip: analytic
+    n x n Gram, eigendecomposition pseudoinverse, synthesis."""
+    import torch
+    from vtem_b200 import dirichlet, linalg
+
+    out = {}
+    try:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cp = dirichlet.dirichlet(w.N, tk1, tk2, ind, w.kappa, w.delta, w.bias, np.ones(w.N), w.Wt, w.Mt)
+        cp.compute_q()
+        cp.compute_G(prep.Dsw, lower_only=True)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        cp.d_q, kept = linalg.solve_eq_sym(cp.d_G, cp.d_q, rcond=w.rcond, return_kept=True)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        cp.freeG()
+        torch.cuda.empty_cache()
+        up = cp.reconstruct(prep.dirich, [0, w.T], w.dt)
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        rel = float((u_fast - up).norm() / up.norm())
+        voxels = Nt * w.Px * w.Py
+        out = {"value": voxels / (t3 - t0), "unit": UNIT, "seconds": t3 - t0,
+               "stages_s": {"q_G": t1 - t0, "pinv_eigh": t2 - t1, "synthesis": t3 - t2},
+               "kept": kept, "n": len(tk1),
+               "fast_vs_plain_rel_l2": rel, "fast_vs_plain_snr_db": -20 * math.log10(max(rel, 1e-300))}
+        del up, cp
+        torch.cuda.empty_cache()
+    except Exception as e:  # report, do not hide
+        out = {"error": repr(e)}
+    return out
+
+
+# ---------------------------------------------------------------- CPU baseline
+
+def cpu_sample(w, prep, rd, window=0.04, frames=None, use_ref=False):
+    """Decode a window [0, window) of the same spikes on the host, with the
+    reference's formulas (oracle port, or the reference's own kernels when
+    use_ref).  Returns (voxels, seconds, description)."""
+    from oracle import vtem_oracle as O
+    Dsw = prep.Dsw.cpu().numpy()
+    dirich = prep.dirich.cpu().numpy()
+    # the window's intervals, as read_select_spikes forms them (one spike either side)
+    t1, t2, ii = rd.read_select_spikes([0.0, window])[:3]
+    norm = np.ones(w.N)
+    Nt = len(np.arange(0, window, w.dt)) if frames is None else frames
+    t0 = time.perf_counter()
+    if use_ref:
+        from oracle import ref_runner as R
+        q = R.compute_q(t1, t2, ii, w.kappa, w.delta, w.bias, norm)
+        G = R.compute_G(t1, t2, ii, Dsw, w.Wt, w.Mt)
+        c = R.solve_eq_sym(G, q, w.rcond)
+        tt = np.arange(Nt) * w.dt
+        R.reconstruct(dirich, t1, t2, c, tt, ii, norm, w.Mt, w.Wt / w.Mt)
+        kind = "reference"
+    else:
+        q = O.compute_q(t1, t2, ii, w.kappa, w.delta, w.bias, norm)
+        G = O.compute_G(t1, t2, ii, Dsw, w.Wt, w.Mt)
+        c, _ = O.solve_eq_sym(G, q, w.rcond)
+        O.reconstruct_factored(dirich, t1, t2, c, np.arange(Nt) * w.dt, ii, norm, w.Mt, w.Wt / w.Mt)
+        kind = "port"
+    sec = time.perf_counter() - t0
+    desc = ("decode window of %d spike intervals (first %.3f s of the clip), %d frames x %dx%d px reconstructed, "
+            "q + analytic G + pseudoinverse + reconstruction" % (len(t1), window, Nt, w.Py, w.Px))
+    return Nt * w.Px * w.Py, sec, desc, kind
+
+
+def cpu_baseline(w, prep, rd):
+    cores = os.cpu_count() or 1
+    vox, sec, desc, kind = cpu_sample(w, prep, rd)
+    return {"value": vox / sec, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc, "seconds": sec}
+
+
+# ---------------------------------------------------------------- reference arm
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    import torch
+    from vtem_b200 import workloads
+    from oracle import ref_runner as R
+    w = workloads.gpu_scale(seed=0, frames=args.frames)
+    dev = torch.device("cuda", 0) if torch.cuda.is_available() else None
+    if dev is None:
+        return {"impl": "reference", "unavailable": "no CUDA device to encode the clip's spikes"}
+    V, prep, (tk1, tk2, ind), t_enc, sp, rd = encode_clip(w, dev)
+    use_ref = R.available()
+    cores = os.cpu_count() or 1
+    # each step: a bounded sample (a 40 ms decode window, 16 frames reconstructed by the reference's kernel)
+    secs, vox = [], 0
+    for i in range(args.warmup + args.steps):
+        v, s, desc, kind = cpu_sample(w, prep, rd, window=0.04, frames=16, use_ref=use_ref)
+        if i >= args.warmup:
+            secs.append(s)
+            vox += v
+    value = vox / sum(secs)
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Dirichlet-bandlimited video)",
+            "config": {"workload": "gpu: 64x64 px, 10000 samples, 1024 RFs (bounded sample per step)"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=10000)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+    else:
+        res = run_ours(args, rank, world, local)
+    if rank == 0 and res is not None:
+        print(json.dumps(res))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -161,6 +161,53 @@ int vtb_reconstruct(const double* dirich, int N, int P, const double* tk1, const
                     const double* c, const int32_t* ind, const double* norm, int nspk, const double* t, int Nt,
                     int Mt, double WM, double* u, void* work, int64_t work_bytes, void* stream);
 
+/* ------------------------------------------------------------ coefficient-space decoder
+ *
+ * The same reconstruction as compute_q + compute_G + solve_eq_sym +
+ * reconstruct (vtem/dirichlet.py:55-85, :165-189; vtem/utils/linalg.py:591-631)
+ * computed in the Dirichlet coefficient space: with Phi[k,(s,m)] =
+ * norm conj(Ds[n_k,s]) T_k(m) and G = Phi Phi^H, the reconstruction's
+ * coefficients are Phi^H G^+ q = M^+ b with M = Phi^H Phi (K x K, K =
+ * ellipse size * (2Mt+1)) and b = Phi^H q; the nonzero spectra of G and M
+ * coincide, so the reference's rcond truncation selects the same subspace.
+ * Spike lists must be sorted by neuron index. */
+
+/* d[n*Ks + s] = norm[n] Ds[n*Kfull + smap[s]] (complex), the ellipse entries. */
+int vtb_coeff_pack(const double* Ds, int N, int Kfull, const int32_t* smap, int Ks, const double* norm, double* d,
+                   void* stream);
+
+/* Per-neuron temporal Gram Wn[n][m][m'] = sum_k conj(T_k(m)) T_k(m') and
+ * gn[n][m] = sum_k conj(T_k(m)) q_k (q_k as compute_q_Kernel), m in [-Mt, Mt],
+ * W = Wt/Mt. */
+int vtb_coeff_temporal_gram(const double* tk1, const double* tk2, const int32_t* ind, int nspk, int N,
+                            const double* kappa, const double* delta, const double* bias, const double* norm, int Mt,
+                            double W, double* Wn, double* gn, void* stream);
+
+/* M = sum_n (d_n d_n^H) kron Wn (column-major, K x K complex, ld ldm) and
+ * b = sum_n d_n kron gn. */
+int vtb_coeff_gram(const double* d, int N, int Ks, const double* Wn, const double* gn, int Kt, double* M,
+                   int64_t ldm, double* b, void* stream);
+
+/* Workspace bytes of vtb_herm_solve (mode 0 eigen, 1 Cholesky). */
+int vtb_herm_solve_workspace(int K, int mode, int64_t* bytes);
+
+/* Solve M a = b for Hermitian PSD M (column-major, destroyed).  mode 0:
+ * pseudoinverse keeping |eigenvalues| > rcond * max (the rule of
+ * solve_eq_sym); mode 1: Cholesky + `refine` float64 refinement sweeps,
+ * VTB_NOT_CONVERGED when the factorisation fails or its pivot spread shows
+ * a condition number beyond 1/rcond.  pivots (HOST, may be NULL) receives
+ * (min, max) eigenvalue (mode 0) or squared Cholesky pivot (mode 1).
+ * Synchronises the stream. */
+int vtb_herm_solve(double* M, int64_t ld, const double* b, double* a, int K, double rcond, int mode, int refine,
+                   void* work, int64_t work_bytes, int32_t* kept, double* pivots, void* stream);
+
+/* u[t][py][px] = Re sum_{s,m} a[s][m] e^{jmW(t0 + t dt)} E_s(px, py) on the
+ * decode grid (the spatial functions of vtb_dirich_space), Nt frames,
+ * float64 (out_f32 = 0) or float32 output.  A_work holds Nt*Ks complex. */
+int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, double W, double t0,
+                         double dt, int Nt, int Px, int Py, int Px1, int Py1, double* A_work, void* u, int out_f32,
+                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

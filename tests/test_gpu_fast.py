@@ -1,0 +1,111 @@
+"""Coefficient-space decoder against the reference decode (GPU).
+
+The coefficient-space path must reproduce the pseudoinverse decode of the
+spike Gram (the oracle's restatement of solve_eq_sym + reconstruct) to the
+same rel-L2 bar as the plain path, and its Gram M = Phi^H Phi must equal the
+explicit product of the spike-by-basis matrix."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import vtem_oracle as O
+from vtem_b200 import ensemble_encode, fast, spike_store, vrf, vtdm, vtem, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def explicit_phi(tk1, tk2, ind, Ds, norm, Mx, My, Mt, W):
+    """Phi[k, (s, m)] = norm conj(Ds[n_k, s]) T_k(m), s over the ellipse."""
+    smap = fast.ellipse_storage_index(Mx, My)
+    D = Ds.reshape(Ds.shape[0], -1)[:, smap]
+    m = np.arange(-Mt, Mt + 1)
+    T = np.empty((len(tk1), len(m)), np.complex128)
+    for j, mm in enumerate(m):
+        if mm == 0:
+            T[:, j] = tk2 - tk1
+        else:
+            T[:, j] = (np.exp(1j * mm * W * tk2) - np.exp(1j * mm * W * tk1)) / (1j * mm * W)
+    Phi = (norm[ind][:, None, None] * np.conj(D[ind])[:, :, None] * T[:, None, :]).reshape(len(tk1), -1)
+    return Phi
+
+
+def test_coeff_gram_matches_explicit_phi():
+    rng = np.random.default_rng(7)
+    N, n, Mx, My, Mt = 11, 400, 3, 2, 3
+    W = 2 * np.pi * 20 / Mt
+    Ds = rng.standard_normal((N, 2 * My + 1, 2 * Mx + 1)) + 1j * rng.standard_normal((N, 2 * My + 1, 2 * Mx + 1))
+    # the coefficients of a real RF: Hermitian (Ds[-m] = conj Ds[m]) and zero outside the ellipse
+    Ds = 0.5 * (Ds + np.conj(Ds[:, ::-1, ::-1])) * O.ellipse_mask(Mx, My)[None]
+    tk1 = rng.uniform(0, 0.3, n)
+    tk2 = tk1 + rng.uniform(0.004, 0.03, n)
+    ind = np.sort(rng.integers(0, N, n)).astype(np.int32)
+    kap, dl, bia = rng.uniform(0.8, 1.2, N), rng.uniform(0.01, 0.05, N), rng.uniform(1, 3, N)
+    norm = rng.uniform(0.5, 1.0, N)
+    dec = fast.CoeffDecoder(torch.as_tensor(Ds, device="cuda"), norm, Mx, My, 2 * np.pi * 20, Mt, 8, 8, 8, 8,
+                            solver="eig")
+    # build W_n, g_n, M, b without solving
+    perm, t1, t2, ii = fast.sort_by_neuron(tk1, tk2, ind)
+    # keep the device copies alive until the kernel has run (the caching
+    # allocator would hand a freed temporary's block to the next one)
+    kap_d, dl_d, bia_d = (torch.as_tensor(a, device="cuda") for a in (kap, dl, bia))
+    from vtem_b200._abi import call, dptr, stream_ptr
+    call("vtb_coeff_temporal_gram", dptr(t1), dptr(t2), dptr(ii), n, N, dptr(kap_d), dptr(dl_d), dptr(bia_d),
+         dptr(dec.norm), Mt, W, dptr(dec.Wn), dptr(dec.gn), stream_ptr())
+    dec._build_M(stream_ptr())
+    Phi = explicit_phi(tk1, tk2, ind, Ds, norm, Mx, My, Mt, W)
+    Mref = Phi.conj().T @ Phi
+    q = O.compute_q(tk1, tk2, ind, kap, dl, bia, norm)
+    bref = Phi.conj().T @ q
+    M = dec.M.cpu().numpy().T                       # stored column-major
+    assert np.abs(M - Mref).max() <= 1e-12 * np.abs(Mref).max()
+    assert np.abs(dec.b.cpu().numpy() - bref).max() <= 1e-12 * np.abs(bref).max()
+    # the spike Gram of the reference is Re(Phi Phi^H)
+    Dsw = (np.conj(Ds.reshape(N, -1)) @ Ds.reshape(N, -1).T).real * np.outer(norm, norm)
+    G = O.compute_G(tk1, tk2, ind, Dsw, 2 * np.pi * 20, Mt)
+    assert np.abs((Phi @ Phi.conj().T).real - G).max() <= 1e-12 * np.abs(G).max()
+
+
+@pytest.fixture(scope="module")
+def small_encoded():
+    w = workloads.small()
+    V = w.video(device="cuda")
+    g = w.gabor
+    rf = vrf.vrf_gabor((w.Py, w.Px), dx=w.dx, dy=w.dy)
+    rf.load_parameters(num_neurons=w.N, h_alpha=g.h_alpha, h_l=g.h_l, h_x0=g.h_x0, h_y0=g.h_y0, h_ab=g.h_ab,
+                       KAPPA=g.KAPPA, h_gain=g.gain)
+    iaf = ensemble_encode.IAF_encode(w.N, w.dt)
+    iaf.load_parameters(h_kappa=w.kappa, h_bias=w.bias, h_delta=w.delta, h_v0=w.v0)
+    store = vtem.VTEM_IAF(V, None, w.Wt, rf, w.Wx, w.Wy, dx=w.dx, dy=w.dy, fps=1.0 / w.dt, npinput=True, iaf=iaf)
+    prep = vtdm.VTDM_prep(store, None, None, w.Mx, w.My)
+    return w, store, prep
+
+
+@pytest.mark.parametrize("solver", ["eig", "chol", "auto"])
+def test_coeff_decode_matches_oracle_pinv(small_encoded, solver):
+    w, store, prep = small_encoded
+    u = vtdm.VTDM(store, None, None, 0.0, w.T, w.dt, w.Mx, Mt=w.Mt, rcond=w.rcond, output_format=2, prep=prep,
+                  decoder="coeff", coeff_solver=solver)
+    rd = spike_store.vtem_storage_read(store)
+    rd.read_vrf_type()
+    rd.read_num_neurons()
+    rd.select_neurons([-0.5, 0.5, -0.5, 0.5])
+    tk1, tk2, ind, kap, dl, bia, sig = rd.read_select_spikes([0.0, w.T])
+    norm = np.ones(w.N)
+    uo, c, q, G, kept = O.decode_window(tk1, tk2, ind, kap, dl, bia, norm, prep.Dsw.cpu().numpy(),
+                                        prep.dirich.cpu().numpy(), w.Wt, w.Mt, w.T, w.dt, rcond=w.rcond)
+    rel = np.linalg.norm(u - uo) / np.linalg.norm(uo)
+    assert rel <= 1e-8, rel
+
+
+def test_coeff_decode_float32_output(small_encoded):
+    w, store, prep = small_encoded
+    rd = spike_store.vtem_storage_read(store)
+    rd.read_vrf_type()
+    rd.read_num_neurons()
+    rd.select_neurons([-0.5, 0.5, -0.5, 0.5])
+    tk1, tk2, ind, kap, dl, bia, sig = rd.read_select_spikes([0.0, w.T])
+    dec = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond)
+    u64 = dec.decode(tk1, tk2, ind, kap, dl, bia, w.T, w.dt)
+    u32 = dec.decode(tk1, tk2, ind, kap, dl, bia, w.T, w.dt, out_dtype=torch.float32)
+    err = (u32.double() - u64).norm() / u64.norm()
+    assert err < 1e-6

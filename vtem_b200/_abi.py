@@ -46,6 +46,12 @@ SIGNATURES = {
     "vtb_rnn": [P, L, P, P, P, P, I, D, I, P, I, P],
     "vtb_reconstruct_workspace": [I, I, I, P],
     "vtb_reconstruct": [P, I, I, P, P, P, P, P, I, P, I, I, D, P, P, L, P],
+    "vtb_coeff_pack": [P, I, I, P, I, P, P, P],
+    "vtb_coeff_temporal_gram": [P, P, P, I, I, P, P, P, P, I, D, P, P, P],
+    "vtb_coeff_gram": [P, I, I, P, P, I, P, L, P, P],
+    "vtb_herm_solve_workspace": [I, I, P],
+    "vtb_herm_solve": [P, L, P, P, I, D, I, I, P, L, P, P, P],
+    "vtb_coeff_synthesize": [P, P, I, I, I, I, D, D, D, I, I, I, I, I, P, P, I, P],
 }
 
 _lib = None

@@ -1,0 +1,360 @@
+// Coefficient-space decoder.
+//
+// The plain decoder solves G c = q with G = Phi Phi^H (n x n, n = spike
+// intervals) and synthesises u = sum_k c_k psi_k phi_{n_k}.  With
+//   Phi[k, (s, m)] = norm_n conj(Ds_n[s]) T_k(m),   T_k(m) = int_{tk1}^{tk2} e^{jmWt} dt,
+// the reconstruction only ever needs a = Phi^H c, and
+//   Phi^H G^+ q = Phi^+ q = M^+ b,   M = Phi^H Phi (K x K),  b = Phi^H q,
+// with the same truncation (the nonzero eigenvalues of Phi Phi^H and
+// Phi^H Phi coincide, so rcond * s_0 selects the same subspace).  K =
+// (ellipse size) * (2 Mt + 1) is independent of the spike count.
+//
+// M has Kronecker structure: with d_n = norm_n Ds_n and the per-neuron
+// temporal Gram W_n[m, m'] = sum_{k in n} conj(T_k(m)) T_k(m'),
+//   M[(s,m),(s',m')] = sum_n d_n[s] conj(d_n[s']) W_n[m, m'],
+//   b[(s,m)]         = sum_n d_n[s] g_n[m],  g_n[m] = sum_{k in n} conj(T_k(m)) q_k,
+// so Phi (n x K) is never formed: one pass over the spikes builds W_n, g_n
+// (temporal_gram_kernel), one tiled pass over the neurons builds M
+// (kron_gram_kernel).  The synthesis expands a on the separable
+// space-time basis: A[t, s] = sum_m a[s, m] e^{jmWt}, then per frame
+// u = Re(ey^T A_t ex) on the decode grid (synth_kernel), whose output write is
+// the one HBM-sized stream of the whole decode.
+#include "common.cuh"
+
+namespace vtb {
+
+__device__ __forceinline__ int lb_i32(const int32_t* a, int n, int v) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
+    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// ------------------------------------------------------------------ W_n, g_n
+// One block per neuron.  Spikes must be sorted by neuron.  T_k(m) for m in
+// [-Mt, Mt] uses the product form (2/(mW)) sin(mW dt/2) e^{jmW tbar}, exact
+// for the integral and free of the cancellation of e^{a} - e^{b}.
+constexpr int kTChunk = 32;
+
+__global__ void __launch_bounds__(256) temporal_gram_kernel(
+    const double* __restrict__ tk1, const double* __restrict__ tk2, const int32_t* __restrict__ ind, int nspk,
+    const double* __restrict__ kappa, const double* __restrict__ delta, const double* __restrict__ bias,
+    const double* __restrict__ norm, int Mt, double W, double2* __restrict__ Wn, double2* __restrict__ gn) {
+    extern __shared__ double2 sT[];  // kTChunk x Kt, then kTChunk q values (as double2.x)
+    const int Kt = 2 * Mt + 1;
+    double2* sq = sT + kTChunk * Kt;
+    const int nr = blockIdx.x;
+    const int lo = lb_i32(ind, nspk, nr), hi = lb_i32(ind, nspk, nr + 1);
+    const int KK = Kt * Kt;
+    const double kd = kappa[nr] * delta[nr], bb = bias[nr], nn = norm[nr];
+    // each thread owns entry e of W_n (grid.y slices the Kt x Kt entries),
+    // and block row 0 also g_n[m] for threads m < Kt
+    const int e = blockIdx.y * blockDim.x + threadIdx.x;
+    const bool own_g = blockIdx.y == 0 && threadIdx.x < Kt;
+    double2 acc = make_double2(0, 0);
+    double2 gacc = make_double2(0, 0);
+    for (int k0 = lo; k0 < hi; k0 += kTChunk) {
+        const int nk = min(kTChunk, hi - k0);
+        __syncthreads();
+        for (int x = threadIdx.x; x < nk * Kt; x += blockDim.x) {
+            const int kk = x / Kt, mi = x % Kt, m = mi - Mt;
+            const double a = tk1[k0 + kk], b = tk2[k0 + kk];
+            const double d = b - a;
+            double2 T;
+            if (m == 0) {
+                T = make_double2(d, 0.0);
+            } else {
+                const double mw = m * W;
+                const double amp = (2.0 / mw) * sin(0.5 * mw * d);
+                double s, c;
+                sincos(mw * (0.5 * (a + b)), &s, &c);
+                T = make_double2(amp * c, amp * s);
+            }
+            sT[kk * Kt + mi] = T;
+            if (mi == 0) sq[kk].x = (kd - bb * d) * nn;  // q_k, compute_q_Kernel's formula
+        }
+        __syncthreads();
+        if (e < KK) {
+            const int m = e / Kt, mp = e % Kt;
+            for (int kk = 0; kk < nk; ++kk) {
+                const double2 a = sT[kk * Kt + m], b = sT[kk * Kt + mp];
+                // conj(a) * b
+                acc.x += a.x * b.x + a.y * b.y;
+                acc.y += a.x * b.y - a.y * b.x;
+            }
+        }
+        if (own_g) {
+            for (int kk = 0; kk < nk; ++kk) {
+                const double2 a = sT[kk * Kt + threadIdx.x];
+                const double q = sq[kk].x;
+                gacc.x += a.x * q;
+                gacc.y -= a.y * q;
+            }
+        }
+    }
+    if (e < KK) Wn[(int64_t)nr * KK + e] = acc;
+    if (own_g) gn[(int64_t)nr * Kt + threadIdx.x] = gacc;
+}
+
+// ------------------------------------------------------------------ M
+// Block = 4 x 4 tile of (s, s') pairs (s-tile <= s'-tile: M is Hermitian and
+// the mirror half is written from the same accumulators); threads own (m, m')
+// entries of the Kt x Kt sub-blocks.  d products for a chunk of neurons are
+// staged in shared memory; W_n entries stream from L2, coalesced.
+constexpr int kKT = 4;
+constexpr int kKN = 32;
+
+__global__ void __launch_bounds__(256) kron_gram_kernel(const double2* __restrict__ d, int N, int Ks,
+                                                        const double2* __restrict__ Wn, int Kt,
+                                                        double2* __restrict__ M, int64_t ldm) {
+    __shared__ double2 sa[kKN][kKT * kKT];
+    // map blockIdx.x to an upper-triangular tile pair (ti <= tj)
+    const int T = (Ks + kKT - 1) / kKT;
+    int b = blockIdx.x, ti = 0;
+    while (b >= T - ti) { b -= T - ti; ++ti; }
+    const int tj = ti + b;
+    const int s0 = ti * kKT, s1 = tj * kKT;
+    const int KK = Kt * Kt;
+    for (int e0 = 0; e0 < KK; e0 += blockDim.x) {
+        const int e = e0 + threadIdx.x;
+        double2 acc[kKT][kKT];
+#pragma unroll
+        for (int i = 0; i < kKT; ++i)
+#pragma unroll
+            for (int j = 0; j < kKT; ++j) acc[i][j] = make_double2(0, 0);
+        for (int n0 = 0; n0 < N; n0 += kKN) {
+            const int nn = min(kKN, N - n0);
+            __syncthreads();
+            for (int x = threadIdx.x; x < nn * kKT * kKT; x += blockDim.x) {
+                const int r = x / (kKT * kKT), ij = x % (kKT * kKT), i = ij / kKT, j = ij % kKT;
+                const int si = s0 + i, sj = s1 + j;
+                double2 v = make_double2(0, 0);
+                if (si < Ks && sj < Ks) v = cmulc(d[(int64_t)(n0 + r) * Ks + si], d[(int64_t)(n0 + r) * Ks + sj]);
+                sa[r][ij] = v;
+            }
+            __syncthreads();
+            if (e < KK) {
+                for (int r = 0; r < nn; ++r) {
+                    const double2 w = Wn[(int64_t)(n0 + r) * KK + e];
+#pragma unroll
+                    for (int i = 0; i < kKT; ++i)
+#pragma unroll
+                        for (int j = 0; j < kKT; ++j) {
+                            const double2 a = sa[r][i * kKT + j];
+                            acc[i][j].x = fma(a.x, w.x, fma(-a.y, w.y, acc[i][j].x));
+                            acc[i][j].y = fma(a.x, w.y, fma(a.y, w.x, acc[i][j].y));
+                        }
+                }
+            }
+        }
+        if (e < KK) {
+            const int m = e / Kt, mp = e % Kt;
+#pragma unroll
+            for (int i = 0; i < kKT; ++i)
+#pragma unroll
+                for (int j = 0; j < kKT; ++j) {
+                    const int si = s0 + i, sj = s1 + j;
+                    if (si >= Ks || sj >= Ks) continue;
+                    const int64_t row = (int64_t)si * Kt + m, col = (int64_t)sj * Kt + mp;
+                    M[col * ldm + row] = acc[i][j];  // column-major
+                    if (ti != tj) M[row * ldm + col] = make_double2(acc[i][j].x, -acc[i][j].y);
+                }
+        }
+    }
+}
+
+// b[(s, m)] = sum_n d[n][s] g[n][m]
+__global__ void kron_rhs_kernel(const double2* __restrict__ d, int N, int Ks, const double2* __restrict__ gn,
+                                int Kt, double2* __restrict__ b) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Ks * Kt) return;
+    const int s = e / Kt, m = e % Kt;
+    double2 acc = make_double2(0, 0);
+    for (int n = 0; n < N; ++n) {
+        const double2 p = cmul(d[(int64_t)n * Ks + s], gn[(int64_t)n * Kt + m]);
+        acc.x += p.x;
+        acc.y += p.y;
+    }
+    b[e] = acc;
+}
+
+// d[n][s] = norm_n * Ds[n][smap[s]]
+__global__ void pack_d_kernel(const double2* __restrict__ Ds, int N, int Kfull, const int32_t* __restrict__ smap,
+                              int Ks, const double* __restrict__ norm, double2* __restrict__ d) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= N * Ks) return;
+    const int n = e / Ks, s = e % Ks;
+    const double2 v = Ds[(int64_t)n * Kfull + smap[s]];
+    d[e] = make_double2(v.x * norm[n], v.y * norm[n]);
+}
+
+// ------------------------------------------------------------------ synthesis
+// A[t][s] = sum_m a[s][m] e^{jmW t_i}, t_i = t0 + i dt
+__global__ void temporal_expand_kernel(const double2* __restrict__ a, int Ks, int Mt, double W, double t0,
+                                       double dt, int Nt, double2* __restrict__ A) {
+    extern __shared__ double2 se[];
+    const int Kt = 2 * Mt + 1;
+    const int it = blockIdx.x;
+    const double tt = t0 + it * dt;
+    for (int mi = threadIdx.x; mi < Kt; mi += blockDim.x) {
+        double s, c;
+        sincos((mi - Mt) * W * tt, &s, &c);
+        se[mi] = make_double2(c, s);
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < Ks; s += blockDim.x) {
+        double2 acc = make_double2(0, 0);
+        for (int mi = 0; mi < Kt; ++mi) {
+            const double2 p = cmul(a[(int64_t)s * Kt + mi], se[mi]);
+            acc.x += p.x;
+            acc.y += p.y;
+        }
+        A[(int64_t)it * Ks + s] = acc;
+    }
+}
+
+// u[t][py][px] = Re sum_{r,c} A_t[(r,c)] ey[r][py] ex[c][px]; one block per
+// group of frames; ex/ey (with the (-1)^{mx+my} signs and the crop offsets of
+// the period grid) are built in shared memory by the block.
+constexpr int kSynthFrames = 8;
+
+template <typename OutT>
+__global__ void __launch_bounds__(256) synth_kernel(const double2* __restrict__ A, const int32_t* __restrict__ smap,
+                                                    int Ks, int Mx, int My, int Px, int Py, int Px1, int Py1, int Nt,
+                                                    OutT* __restrict__ u) {
+    extern __shared__ double2 sm2[];
+    const int Kx = 2 * Mx + 1, Ky = 2 * My + 1;
+    double2* ex = sm2;                 // Kx x Px
+    double2* ey = ex + Kx * Px;        // Ky x Py
+    double2* G = ey + Ky * Py;         // Ky x Kx (frame's coefficients on the grid)
+    double2* B = G + Ky * Kx;          // Ky x Px
+    const int xd = (Px1 - Px) / 2, yd = (Py1 - Py) / 2;
+    for (int e = threadIdx.x; e < Kx * Px; e += blockDim.x) {
+        const int c = e / Px, px = e % Px, mx = c - Mx;
+        const int64_t r = ((((int64_t)mx * (px + xd)) % Px1) + Px1) % Px1;
+        double s, co;
+        sincospi(2.0 * r / Px1, &s, &co);
+        const double sg = (mx & 1) ? -1.0 : 1.0;
+        ex[e] = make_double2(sg * co, sg * s);
+    }
+    for (int e = threadIdx.x; e < Ky * Py; e += blockDim.x) {
+        const int rr = e / Py, py = e % Py, my = My - rr;   // storage row rr holds my = My - rr
+        const int64_t r = ((((int64_t)my * (py + yd)) % Py1) + Py1) % Py1;
+        double s, co;
+        sincospi(2.0 * r / Py1, &s, &co);
+        const double sg = (my & 1) ? -1.0 : 1.0;
+        ey[e] = make_double2(sg * co, sg * s);
+    }
+    const int f0 = blockIdx.x * kSynthFrames;
+    for (int f = f0; f < min(f0 + kSynthFrames, Nt); ++f) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < Ky * Kx; e += blockDim.x) G[e] = make_double2(0, 0);
+        __syncthreads();
+        for (int s = threadIdx.x; s < Ks; s += blockDim.x) G[smap[s]] = A[(int64_t)f * Ks + s];
+        __syncthreads();
+        for (int e = threadIdx.x; e < Ky * Px; e += blockDim.x) {
+            const int rr = e / Px, px = e % Px;
+            double2 acc = make_double2(0, 0);
+            for (int c = 0; c < Kx; ++c) {
+                const double2 p = cmul(G[rr * Kx + c], ex[c * Px + px]);
+                acc.x += p.x;
+                acc.y += p.y;
+            }
+            B[e] = acc;
+        }
+        __syncthreads();
+        OutT* uf = u + (int64_t)f * Px * Py;
+        for (int p = threadIdx.x; p < Px * Py; p += blockDim.x) {
+            const int py = p / Px, px = p % Px;
+            double acc = 0.0;
+            for (int rr = 0; rr < Ky; ++rr) {
+                const double2 b = B[rr * Px + px], e = ey[rr * Py + py];
+                acc = fma(b.x, e.x, fma(-b.y, e.y, acc));
+            }
+            uf[p] = (OutT)acc;
+        }
+    }
+}
+
+}  // namespace vtb
+
+using namespace vtb;
+
+VTB_API int vtb_coeff_temporal_gram(const double* tk1, const double* tk2, const int32_t* ind, int nspk, int N,
+                                    const double* kappa, const double* delta, const double* bias, const double* norm,
+                                    int Mt, double W, double* Wn, double* gn, void* stream) {
+    VTB_CHECK_ARG(nspk >= 0 && N > 0 && Mt >= 1 && Mt <= 128 && Wn && gn && kappa && delta && bias && norm);
+    VTB_CHECK_ARG(nspk == 0 || (tk1 && tk2 && ind));
+    const int Kt = 2 * Mt + 1;
+    const size_t sm = (size_t)kTChunk * (Kt + 1) * sizeof(double2);
+    dim3 grid(N, ceil_div((int64_t)Kt * Kt, 256));
+    temporal_gram_kernel<<<grid, 256, sm, as_stream(stream)>>>(tk1, tk2, ind, nspk, kappa, delta, bias, norm, Mt, W,
+                                                           reinterpret_cast<double2*>(Wn),
+                                                           reinterpret_cast<double2*>(gn));
+    return launch_status();
+}
+
+VTB_API int vtb_coeff_pack(const double* Ds, int N, int Kfull, const int32_t* smap, int Ks, const double* norm,
+                           double* d, void* stream) {
+    VTB_CHECK_ARG(N > 0 && Ks > 0 && Ks <= Kfull && Ds && smap && norm && d);
+    pack_d_kernel<<<ceil_div((int64_t)N * Ks, 256), 256, 0, as_stream(stream)>>>(
+        reinterpret_cast<const double2*>(Ds), N, Kfull, smap, Ks, norm, reinterpret_cast<double2*>(d));
+    return launch_status();
+}
+
+VTB_API int vtb_coeff_gram(const double* d, int N, int Ks, const double* Wn, const double* gn, int Kt, double* M,
+                           int64_t ldm, double* b, void* stream) {
+    VTB_CHECK_ARG(N > 0 && Ks > 0 && Kt > 0 && d && Wn && gn && M && b && ldm >= (int64_t)Ks * Kt);
+    const int T = (Ks + kKT - 1) / kKT;
+    const int tiles = T * (T + 1) / 2;
+    kron_gram_kernel<<<tiles, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(d), N, Ks,
+                                                           reinterpret_cast<const double2*>(Wn), Kt,
+                                                           reinterpret_cast<double2*>(M), ldm);
+    int st = launch_status();
+    if (st) return st;
+    kron_rhs_kernel<<<ceil_div((int64_t)Ks * Kt, 128), 128, 0, as_stream(stream)>>>(
+        reinterpret_cast<const double2*>(d), N, Ks, reinterpret_cast<const double2*>(gn), Kt,
+        reinterpret_cast<double2*>(b));
+    return launch_status();
+}
+
+VTB_API int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, double W,
+                                 double t0, double dt, int Nt, int Px, int Py, int Px1, int Py1, double* A_work,
+                                 void* u, int out_f32, void* stream) {
+    VTB_CHECK_ARG(Ks > 0 && Mx >= 0 && My >= 0 && Mt >= 0 && Nt >= 0 && Px > 0 && Py > 0 && Px1 >= Px && Py1 >= Py);
+    VTB_CHECK_ARG(2 * Mx + 1 <= Px1 && 2 * My + 1 <= Py1);
+    if (Nt == 0) return VTB_OK;
+    VTB_CHECK_ARG(a && smap && A_work && u);
+    cudaStream_t s = as_stream(stream);
+    const int Kt = 2 * Mt + 1;
+    temporal_expand_kernel<<<Nt, 128, Kt * sizeof(double2), s>>>(reinterpret_cast<const double2*>(a), Ks, Mt, W, t0,
+                                                                 dt, Nt, reinterpret_cast<double2*>(A_work));
+    int st = launch_status();
+    if (st) return st;
+    const int Kx = 2 * Mx + 1, Ky = 2 * My + 1;
+    const size_t sm = (size_t)(Kx * Px + Ky * Py + Ky * Kx + Ky * Px) * sizeof(double2);
+    VTB_CHECK_ARG(sm <= 200 * 1024);
+    const int blocks = ceil_div(Nt, kSynthFrames);
+    if (out_f32) {
+        if (sm > 48 * 1024)
+            VTB_CUDA_TRY(cudaFuncSetAttribute(synth_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        synth_kernel<float><<<blocks, 256, sm, s>>>(reinterpret_cast<const double2*>(A_work), smap, Ks, Mx, My, Px,
+                                                   Py, Px1, Py1, Nt, reinterpret_cast<float*>(u));
+    } else {
+        if (sm > 48 * 1024)
+            VTB_CUDA_TRY(cudaFuncSetAttribute(synth_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        synth_kernel<double><<<blocks, 256, sm, s>>>(reinterpret_cast<const double2*>(A_work), smap, Ks, Mx, My, Px,
+                                                    Py, Px1, Py1, Nt, reinterpret_cast<double*>(u));
+    }
+    return launch_status();
+}

@@ -14,6 +14,8 @@
 //      buffered so that every row reads the same previous c.
 #include <cusolverDn.h>
 
+#include <cstdlib>
+
 #include "common.cuh"
 
 namespace vtb {
@@ -120,47 +122,74 @@ __global__ void sumsq_kernel(const double* __restrict__ v, int n, double* __rest
 
 using namespace vtb;
 
-// Workspace layout: [w: n doubles][qq: n doubles][info: 8 bytes][syevd work]
+// Workspace layout (each piece 256-byte aligned): [w: n doubles][qq: n doubles][info][syevd work].
+// The 64-bit cuSOLVER API sizes the eigensolver's workspace (2n^2 doubles at
+// n = 25k is beyond the 32-bit interface); its small host workspace is
+// allocated on the host per call.
+static inline int64_t al256(int64_t x) { return (x + 255) & ~(int64_t)255; }
+
+static cusolverDnParams_t solver_params() {
+    static thread_local cusolverDnParams_t p = nullptr;
+    if (!p && cusolverDnCreateParams(&p) != CUSOLVER_STATUS_SUCCESS) p = nullptr;
+    return p;
+}
+
+static int syevd_sizes(cusolverDnHandle_t h, int n, size_t* dev_bytes, size_t* host_bytes) {
+    cusolverDnParams_t prm = solver_params();
+    if (!prm) return VTB_CUDA_ERR;
+    if (cusolverDnXsyevd_bufferSize(h, prm, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, CUDA_R_64F, nullptr,
+                                    n, CUDA_R_64F, nullptr, CUDA_R_64F, dev_bytes, host_bytes) !=
+        CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    return VTB_OK;
+}
+
 VTB_API int vtb_solve_eq_sym_workspace(int n, int64_t* bytes) {
     VTB_CHECK_ARG(n > 0 && bytes);
     int dev = 0;
     VTB_CUDA_TRY(cudaGetDevice(&dev));
     cusolverDnHandle_t h = solver_handle(dev);
     if (!h) return VTB_CUDA_ERR;
-    int lwork = 0;
-    if (cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, nullptr, n, nullptr,
-                                    &lwork) != CUSOLVER_STATUS_SUCCESS)
-        return VTB_CUDA_ERR;
-    *bytes = (int64_t)(2 * (int64_t)n + 1) * 8 + (int64_t)lwork * 8 + 256;
+    size_t db = 0, hb = 0;
+    int st = syevd_sizes(h, n, &db, &hb);
+    if (st) return st;
+    *bytes = 2 * al256((int64_t)n * 8) + 256 + al256((int64_t)db);
     return VTB_OK;
 }
 
 VTB_API int vtb_solve_eq_sym(double* G, int64_t ld, const double* q, double* c, int n, double rcond, void* work,
                              int64_t work_bytes, int32_t* kept, void* stream) {
     VTB_CHECK_ARG(n > 0 && ld >= n && G && q && c && work);
-    int64_t need = 0;
-    int st = vtb_solve_eq_sym_workspace(n, &need);
-    if (st) return st;
-    VTB_CHECK_ARG(work_bytes >= need);
+    VTB_CHECK_ARG(((uintptr_t)work & 255) == 0);
     int dev = 0;
     VTB_CUDA_TRY(cudaGetDevice(&dev));
     cusolverDnHandle_t h = solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    size_t db = 0, hb = 0;
+    int st = syevd_sizes(h, n, &db, &hb);
+    if (st) return st;
+    VTB_CHECK_ARG(work_bytes >= 2 * al256((int64_t)n * 8) + 256 + al256((int64_t)db));
     cudaStream_t s = as_stream(stream);
     if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
-    double* w = reinterpret_cast<double*>(work);
-    double* qq = w + n;
-    int* info = reinterpret_cast<int*>(qq + n);
-    double* wk = reinterpret_cast<double*>(reinterpret_cast<char*>(info) + 8);
-    const int lwork = (int)((need - (int64_t)(2 * (int64_t)n + 1) * 8 - 256) / 8);
+    char* base = reinterpret_cast<char*>(work);
+    double* w = reinterpret_cast<double*>(base);
+    double* qq = reinterpret_cast<double*>(base + al256((int64_t)n * 8));
+    int* info = reinterpret_cast<int*>(base + 2 * al256((int64_t)n * 8));
+    void* wk = base + 2 * al256((int64_t)n * 8) + 256;
+    void* hwk = hb ? malloc(hb) : nullptr;
+    if (hb && !hwk) return VTB_OOM;
     // Row-major symmetric G is its own column-major transpose.  The row-major
     // lower triangle is the column-major upper one.  On exit the column-major
     // eigenvectors (columns) are the rows of the row-major buffer.
-    if (cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, G, (int)ld, w, wk, lwork, info) !=
-        CUSOLVER_STATUS_SUCCESS)
-        return VTB_CUDA_ERR;
+    const cusolverStatus_t cs = cusolverDnXsyevd(h, solver_params(), CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER,
+                                                 n, CUDA_R_64F, G, ld, CUDA_R_64F, w, CUDA_R_64F, wk, db, hwk, hb, info);
     int hinfo = 0;
-    VTB_CUDA_TRY(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
-    VTB_CUDA_TRY(cudaStreamSynchronize(s));
+    cudaError_t e1 = cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    free(hwk);
+    if (cs != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    VTB_CUDA_TRY(e1);
+    VTB_CUDA_TRY(e2);
     if (hinfo != 0) return VTB_NOT_CONVERGED;
     const int blocks = ceil_div((int64_t)n * 32, 256);
     gemv_rows_kernel<<<blocks, 256, 0, s>>>(G, ld, q, n, qq);  // qq = V^T q
@@ -187,5 +216,264 @@ VTB_API int vtb_rnn(const double* G, int64_t ld, const double* q, double* c, dou
         nxt = t;
     }
     if (cur != c) VTB_CUDA_TRY(cudaMemcpyAsync(c, cur, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    return launch_status();
+}
+
+// ---------------------------------------------------------------------------
+// Hermitian K x K solve of the coefficient-space decoder (M a = b).
+//   mode 0: pseudoinverse by eigendecomposition (cuSOLVER zheevd), the
+//           reference's truncation |w| > rcond * max|w| (same rule as
+//           vtb_solve_eq_sym, the eigenvalues being those of the spike Gram);
+//   mode 1: Cholesky (zpotrf/zpotrs) with `refine` float64 refinement sweeps
+//           against a saved copy of M.  Returns VTB_NOT_CONVERGED when the
+//           factorisation fails or its pivots show a condition number beyond
+//           1/rcond, in which case the caller falls back to mode 0.
+// M is column-major (element (r, c) at c*ld + r), complex interleaved, and is
+// overwritten.
+namespace vtb {
+
+__global__ void zgemv_conj_rows_kernel(const double2* __restrict__ V, int64_t ld, const double2* __restrict__ x,
+                                       int n, double2* __restrict__ y) {
+    // y[i] = sum_j conj(V[i*ld + j]) x[j]   (V row i = column i of the column-major eigenvector matrix)
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const double2* row = V + (int64_t)warp * ld;
+    double sr = 0.0, si = 0.0;
+    for (int j = lane; j < n; j += 32) {
+        const double2 v = row[j], b = x[j];
+        sr += v.x * b.x + v.y * b.y;
+        si += v.x * b.y - v.y * b.x;
+    }
+    for (int o = 16; o; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) y[warp] = make_double2(sr, si);
+}
+
+__global__ void zgemv_cols_kernel(const double2* __restrict__ V, int64_t ld, const double2* __restrict__ x, int n,
+                                  double2* __restrict__ y, const double2* __restrict__ b, int subtract) {
+    // y[j] = sum_i V[i*ld + j] x[i]   (or b[j] - that when subtract)
+    __shared__ double2 part[8][33];
+    const int col = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int g = threadIdx.x >> 5;
+    double sr = 0.0, si = 0.0;
+    if (col < n)
+        for (int i = g; i < n; i += 8) {
+            const double2 v = V[(int64_t)i * ld + col], w = x[i];
+            sr += v.x * w.x - v.y * w.y;
+            si += v.x * w.y + v.y * w.x;
+        }
+    part[g][threadIdx.x & 31] = make_double2(sr, si);
+    __syncthreads();
+    if (g == 0 && col < n) {
+        double tr = 0.0, ti = 0.0;
+        for (int k = 0; k < 8; ++k) {
+            tr += part[k][threadIdx.x & 31].x;
+            ti += part[k][threadIdx.x & 31].y;
+        }
+        y[col] = subtract ? make_double2(b[col].x - tr, b[col].y - ti) : make_double2(tr, ti);
+    }
+}
+
+__global__ void ztruncate_kernel(const double* __restrict__ w, double2* __restrict__ qq, int n, double rcond,
+                                 int32_t* __restrict__ kept) {
+    __shared__ double s0;
+    __shared__ int cnt;
+    if (threadIdx.x == 0) {
+        s0 = fmax(fabs(w[0]), fabs(w[n - 1])) * rcond;
+        cnt = 0;
+    }
+    __syncthreads();
+    int local = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double s = fabs(w[i]);
+        if (s > s0) {
+            qq[i] = make_double2(qq[i].x / s, qq[i].y / s);
+            ++local;
+        } else {
+            qq[i] = make_double2(0.0, 0.0);
+        }
+    }
+    atomicAdd(&cnt, local);
+    __syncthreads();
+    if (threadIdx.x == 0 && kept) *kept = cnt;
+}
+
+// pivots of the Cholesky factor: out[0] = min L_ii^2, out[1] = max L_ii^2
+__global__ void chol_pivots_kernel(const double2* __restrict__ L, int64_t ld, int n, double* __restrict__ out) {
+    __shared__ double smin[32], smax[32];
+    double mn = 1e308, mx = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double d = L[(int64_t)i * ld + i].x;
+        mn = fmin(mn, d * d);
+        mx = fmax(mx, d * d);
+    }
+    for (int o = 16; o; o >>= 1) {
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        smin[threadIdx.x >> 5] = mn;
+        smax[threadIdx.x >> 5] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+            mn = fmin(mn, smin[k]);
+            mx = fmax(mx, smax[k]);
+        }
+        mn = fmin(mn, smin[0]);
+        mx = fmax(mx, smax[0]);
+        out[0] = mn;
+        out[1] = mx;
+    }
+}
+
+__global__ void zaxpy_kernel(double2* __restrict__ a, const double2* __restrict__ d, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = make_double2(a[i].x + d[i].x, a[i].y + d[i].y);
+}
+
+}  // namespace vtb
+
+// Workspace carve-up of vtb_herm_solve; every piece starts on a 256-byte
+// boundary (the complex vectors are read as 16-byte double2).
+namespace vtb {
+struct HermWork {
+    double* w;        // K eigenvalues / pivots
+    double2* v1;      // K
+    double2* v2;      // K
+    int* info;
+    double2* Mc;      // K*K copy of M (mode 1)
+    cuDoubleComplex* wk;
+    int lwork;
+};
+static inline int64_t align256(int64_t x) { return (x + 255) & ~(int64_t)255; }
+static int64_t herm_layout(int K, int mode, int lwork, char* base, HermWork* hw) {
+    int64_t off = 0;
+    auto take = [&](int64_t bytes) {
+        int64_t o = off;
+        off = align256(off + bytes);
+        return o;
+    };
+    const int64_t ow = take((int64_t)K * 8);
+    const int64_t o1 = take((int64_t)K * 16);
+    const int64_t o2 = take((int64_t)K * 16);
+    const int64_t oi = take(64);
+    const int64_t om = mode == 1 ? take((int64_t)K * K * 16) : 0;
+    const int64_t ok = take((int64_t)lwork * 16);
+    if (hw && base) {
+        hw->w = reinterpret_cast<double*>(base + ow);
+        hw->v1 = reinterpret_cast<double2*>(base + o1);
+        hw->v2 = reinterpret_cast<double2*>(base + o2);
+        hw->info = reinterpret_cast<int*>(base + oi);
+        hw->Mc = mode == 1 ? reinterpret_cast<double2*>(base + om) : nullptr;
+        hw->wk = reinterpret_cast<cuDoubleComplex*>(base + ok);
+        hw->lwork = lwork;
+    }
+    return off;
+}
+static int herm_lwork(cusolverDnHandle_t h, int K, int mode, int* lwork) {
+    if (mode == 0)
+        return cusolverDnZheevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, K, nullptr, K, nullptr,
+                                           lwork) == CUSOLVER_STATUS_SUCCESS ? VTB_OK : VTB_CUDA_ERR;
+    return cusolverDnZpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, K, nullptr, K, lwork) == CUSOLVER_STATUS_SUCCESS
+               ? VTB_OK : VTB_CUDA_ERR;
+}
+}  // namespace vtb
+
+VTB_API int vtb_herm_solve_workspace(int K, int mode, int64_t* bytes) {
+    VTB_CHECK_ARG(K > 0 && bytes && (mode == 0 || mode == 1));
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    int lwork = 0;
+    int st = herm_lwork(h, K, mode, &lwork);
+    if (st) return st;
+    *bytes = herm_layout(K, mode, lwork, nullptr, nullptr);
+    return VTB_OK;
+}
+
+VTB_API int vtb_herm_solve(double* M, int64_t ld, const double* b, double* a, int K, double rcond, int mode,
+                           int refine, void* work, int64_t work_bytes, int32_t* kept, double* pivots, void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && M && b && a && work && (mode == 0 || mode == 1));
+    int64_t need = 0;
+    int st = vtb_herm_solve_workspace(K, mode, &need);
+    if (st) return st;
+    VTB_CHECK_ARG(work_bytes >= need);
+    VTB_CHECK_ARG(((uintptr_t)work & 255) == 0 && ((uintptr_t)M & 15) == 0 && ((uintptr_t)b & 15) == 0 &&
+                  ((uintptr_t)a & 15) == 0);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = solver_handle(dev);
+    cudaStream_t s = as_stream(stream);
+    if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    int lwork0 = 0;
+    st = herm_lwork(h, K, mode, &lwork0);
+    if (st) return st;
+    HermWork hw;
+    herm_layout(K, mode, lwork0, reinterpret_cast<char*>(work), &hw);
+    double* w = hw.w;
+    double2* v1 = hw.v1;
+    double2* v2 = hw.v2;
+    int* info = hw.info;
+    double2* Mc = hw.Mc;
+    cuDoubleComplex* wk = hw.wk;
+    const int lwork = hw.lwork;
+    cuDoubleComplex* Mz = reinterpret_cast<cuDoubleComplex*>(M);
+    const double2* bz = reinterpret_cast<const double2*>(b);
+    double2* az = reinterpret_cast<double2*>(a);
+    int hinfo = 0;
+    if (mode == 0) {
+        if (cusolverDnZheevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, K, Mz, (int)ld, w, wk, lwork, info) !=
+            CUSOLVER_STATUS_SUCCESS)
+            return VTB_CUDA_ERR;
+        double ev[2] = {0, 0};
+        VTB_CUDA_TRY(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+        VTB_CUDA_TRY(cudaMemcpyAsync(&ev[0], w, 8, cudaMemcpyDeviceToHost, s));
+        VTB_CUDA_TRY(cudaMemcpyAsync(&ev[1], w + K - 1, 8, cudaMemcpyDeviceToHost, s));
+        VTB_CUDA_TRY(cudaStreamSynchronize(s));
+        if (hinfo != 0) return VTB_NOT_CONVERGED;
+        if (pivots) {
+            pivots[0] = ev[0];
+            pivots[1] = ev[1];
+        }
+        const double2* V = reinterpret_cast<const double2*>(M);  // column c (eigenvector c) at V + c*ld
+        zgemv_conj_rows_kernel<<<ceil_div((int64_t)K * 32, 256), 256, 0, s>>>(V, ld, bz, K, v1);  // V^H b
+        ztruncate_kernel<<<1, 1024, 0, s>>>(w, v1, K, rcond, kept);
+        zgemv_cols_kernel<<<ceil_div(K, 32), 256, 0, s>>>(V, ld, v1, K, az, nullptr, 0);          // V qq
+        return launch_status();
+    }
+    // mode 1: Cholesky + refinement
+    VTB_CUDA_TRY(cudaMemcpy2DAsync(Mc, (size_t)K * 16, M, (size_t)ld * 16, (size_t)K * 16, K, cudaMemcpyDeviceToDevice, s));
+    if (cusolverDnZpotrf(h, CUBLAS_FILL_MODE_LOWER, K, Mz, (int)ld, wk, lwork, info) != CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    chol_pivots_kernel<<<1, 1024, 0, s>>>(reinterpret_cast<const double2*>(M), ld, K, w);
+    double hp[2] = {0, 0};
+    VTB_CUDA_TRY(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+    VTB_CUDA_TRY(cudaMemcpyAsync(hp, w, 16, cudaMemcpyDeviceToHost, s));
+    VTB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (pivots) {
+        pivots[0] = hp[0];
+        pivots[1] = hp[1];
+    }
+    // (max/min pivot) is a lower bound of cond(M): beyond 1/rcond the pseudoinverse would truncate
+    if (hinfo != 0 || !(hp[0] > 0.0) || hp[1] / hp[0] * rcond >= 1.0) return VTB_NOT_CONVERGED;
+    VTB_CUDA_TRY(cudaMemcpyAsync(az, bz, (size_t)K * 16, cudaMemcpyDeviceToDevice, s));
+    if (cusolverDnZpotrs(h, CUBLAS_FILL_MODE_LOWER, K, 1, Mz, (int)ld, reinterpret_cast<cuDoubleComplex*>(az), K,
+                         info) != CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    for (int it = 0; it < refine; ++it) {
+        // r = b - M a with the saved M (column-major: row j of the buffer is column j)
+        zgemv_cols_kernel<<<ceil_div(K, 32), 256, 0, s>>>(Mc, K, az, K, v2, bz, 1);
+        if (cusolverDnZpotrs(h, CUBLAS_FILL_MODE_LOWER, K, 1, Mz, (int)ld, reinterpret_cast<cuDoubleComplex*>(v2), K,
+                             info) != CUSOLVER_STATUS_SUCCESS)
+            return VTB_CUDA_ERR;
+        zaxpy_kernel<<<ceil_div(K, 256), 256, 0, s>>>(az, v2, K);
+    }
+    if (kept) VTB_CUDA_TRY(cudaMemsetAsync(kept, 0xff, sizeof(int32_t), s));
     return launch_status();
 }

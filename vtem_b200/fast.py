@@ -1,0 +1,149 @@
+"""Coefficient-space decoder: the reference's pseudoinverse decode without the
+spike-by-spike Gram.
+
+``CoeffDecoder.decode`` returns the same video as ``dirichlet.compute_q`` +
+``compute_G`` + ``linalg.solve_eq_sym`` + ``dirichlet.reconstruct``
+(vtem/dirichlet.py:55-189, vtem/utils/linalg.py:591-631) for one window:
+with Phi[k,(s,m)] = norm conj(Ds[n_k,s]) T_k(m), G = Phi Phi^H and the
+reconstruction coefficients a = Phi^H G^+ q = M^+ b, M = Phi^H Phi.  M is
+K x K (K = ellipse size * (2Mt+1), 1921 for Mx=My=6, Mt=8) whatever the
+number of spikes, built from per-neuron Kronecker factors on the device; the
+n x n Gram (5 GB at 25k spikes) and its O(n^3) eigendecomposition are never
+formed.  See csrc/coeff.cu for the kernels.
+
+Solver choice: ``"eig"`` applies the reference's truncation rule to the
+eigenvalues of M (identical subspace); ``"chol"`` factorises M by Cholesky
+with float64 refinement and refuses (falls back to ``"eig"`` under
+``"auto"``) when the pivots show a condition number beyond 1/rcond, i.e.
+when the pseudoinverse would truncate.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _abi
+from ._abi import VTB_NOT_CONVERGED, VtbError, call, dptr, stream_ptr
+from .dirichlet import sort_by_neuron
+
+F64 = torch.float64
+C128 = torch.complex128
+
+
+def ellipse_storage_index(Mx, My):
+    """Flat Ds storage indices (row My-my, column mx+Mx) of the spatial
+    ellipse mx^2 My^2 + my^2 Mx^2 <= Mx^2 My^2 (vrf.py:1331), ascending."""
+    idx = []
+    Kx = 2 * Mx + 1
+    for r in range(2 * My + 1):
+        my = My - r
+        for c in range(Kx):
+            mx = c - Mx
+            if mx * mx * My * My + my * my * Mx * Mx <= Mx * Mx * My * My:
+                idx.append(r * Kx + c)
+    return np.array(idx, np.int32)
+
+
+class CoeffDecoder(object):
+    def __init__(self, Ds, h_norm, Mx, My, Wt, Mt, decPx, decPy, Px1, Py1, rcond=1e-8, solver="auto", refine=2,
+                 device="cuda"):
+        self.Mx, self.My, self.Mt = int(Mx), int(My), int(Mt)
+        self.Wt = float(Wt)
+        self.W = self.Wt / self.Mt
+        self.decPx, self.decPy, self.Px1, self.Py1 = int(decPx), int(decPy), int(Px1), int(Py1)
+        self.rcond = float(rcond)
+        self.solver = solver
+        self.refine = int(refine)
+        Ds = Ds.to(device=device, dtype=C128).contiguous()
+        self.N = Ds.shape[0]
+        self.Kfull = Ds[0].numel()
+        self.smap = torch.as_tensor(ellipse_storage_index(self.Mx, self.My), device=device)
+        self.Ks = int(self.smap.numel())
+        self.Kt = 2 * self.Mt + 1
+        self.K = self.Ks * self.Kt
+        self.norm = torch.as_tensor(np.asarray(h_norm, np.float64), device=device)
+        self.d = torch.empty((self.N, self.Ks), dtype=C128, device=device)
+        call("vtb_coeff_pack", dptr(Ds), self.N, self.Kfull, dptr(self.smap), self.Ks, dptr(self.norm),
+             dptr(self.d), stream_ptr())
+        self.Wn = torch.empty((self.N, self.Kt, self.Kt), dtype=C128, device=device)
+        self.gn = torch.empty((self.N, self.Kt), dtype=C128, device=device)
+        self.M = torch.empty((self.K, self.K), dtype=C128, device=device)
+        self.b = torch.empty((self.K,), dtype=C128, device=device)
+        self.a = torch.empty((self.K,), dtype=C128, device=device)
+        self.kept = torch.zeros(1, dtype=torch.int32, device=device)
+        self._work = {}
+        self.last_solver = None
+        self.last_pivots = (0.0, 0.0)
+
+    def _workspace(self, mode):
+        if mode not in self._work:
+            nb = np.zeros(1, np.int64)
+            call("vtb_herm_solve_workspace", self.K, mode, nb.ctypes.data)
+            self._work[mode] = torch.empty(int(nb[0]), dtype=torch.uint8, device=self.M.device)
+        return self._work[mode]
+
+    def coefficients(self, tk1, tk2, neuron_ind, kappa, delta, bias, assume_sorted=False):
+        """Reconstruction coefficients a[(s, m)] (K complex) of one window.
+        ``assume_sorted`` skips the (synchronising) check that the intervals
+        are grouped by neuron, for device-resident inputs already sorted."""
+        if assume_sorted:
+            ind = neuron_ind
+        else:
+            perm, tk1, tk2, ind = sort_by_neuron(tk1, tk2, neuron_ind)
+        n = int(tk1.numel())
+        if n == 0:
+            raise ValueError("no spikes to decode")
+        dev = self.M.device
+        kap = torch.as_tensor(np.asarray(kappa, np.float64), device=dev) if not isinstance(kappa, torch.Tensor) else kappa
+        dl = torch.as_tensor(np.asarray(delta, np.float64), device=dev) if not isinstance(delta, torch.Tensor) else delta
+        bi = torch.as_tensor(np.asarray(bias, np.float64), device=dev) if not isinstance(bias, torch.Tensor) else bias
+        s = stream_ptr()
+        call("vtb_coeff_temporal_gram", dptr(tk1), dptr(tk2), dptr(ind), n, self.N, dptr(kap), dptr(dl), dptr(bi),
+             dptr(self.norm), self.Mt, self.W, dptr(self.Wn), dptr(self.gn), s)
+        self._solve(s)
+        return self.a
+
+    def _build_M(self, s):
+        call("vtb_coeff_gram", dptr(self.d), self.N, self.Ks, dptr(self.Wn), dptr(self.gn), self.Kt, dptr(self.M),
+             self.K, dptr(self.b), s)
+
+    def _solve(self, s):
+        modes = {"eig": [0], "chol": [1], "auto": [1, 0]}[self.solver]
+        piv = np.zeros(2, np.float64)
+        for i, mode in enumerate(modes):
+            self._build_M(s)
+            work = self._workspace(mode)
+            st = _abi.lib().vtb_herm_solve(dptr(self.M), self.K, dptr(self.b), dptr(self.a), self.K, self.rcond,
+                                          mode, self.refine, dptr(work), work.numel(), dptr(self.kept),
+                                          piv.ctypes.data, s)
+            if st == 0:
+                self.last_solver = "eig" if mode == 0 else "chol"
+                self.last_pivots = (float(piv[0]), float(piv[1]))
+                return
+            if st == VTB_NOT_CONVERGED and i + 1 < len(modes):
+                continue
+            raise VtbError("vtb_herm_solve", st)
+
+    def synthesize(self, a, T, dt, t0=0.0, out=None, out_dtype=F64):
+        """Video (Nt, decPy, decPx) at t = t0 + arange(0, T, dt)."""
+        Nt = len(np.arange(0, T, dt))
+        dev = self.M.device
+        if out is None:
+            out = torch.empty((Nt, self.decPy, self.decPx), dtype=out_dtype, device=dev)
+        A = torch.empty((Nt, self.Ks), dtype=C128, device=dev)
+        call("vtb_coeff_synthesize", dptr(a), dptr(self.smap), self.Ks, self.Mx, self.My, self.Mt, self.W, float(t0),
+             float(dt), Nt, self.decPx, self.decPy, self.Px1, self.Py1, dptr(A), dptr(out),
+             int(out.dtype == torch.float32), stream_ptr())
+        return out
+
+    def decode(self, tk1, tk2, neuron_ind, kappa, delta, bias, T, dt, out=None, out_dtype=F64,
+               assume_sorted=False):
+        """The window's video (Nt, decPy, decPx) at t = arange(0, T, dt)."""
+        a = self.coefficients(tk1, tk2, neuron_ind, kappa, delta, bias, assume_sorted=assume_sorted)
+        return self.synthesize(a, T, dt, out=out, out_dtype=out_dtype)
+
+
+def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=2):
+    """A :class:`CoeffDecoder` on the output of ``vtdm.VTDM_prep``."""
+    return CoeffDecoder(prep.Ds, prep.h_norm, prep.Mx, prep.My, Wt, Mt, prep.decPx, prep.decPy, prep.Px1, prep.Py1,
+                        rcond=rcond, solver=solver, refine=refine)

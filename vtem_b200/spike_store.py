@@ -19,9 +19,13 @@ class vtem_storage(object):
         self.title = title
         self.data = {"filter_type": np.array(filter_type)}
         self.vrf = {"alpha": [], "x0": [], "y0": []}
-        if filter_type == "gabor":
+        if filter_type in ("gabor", "mixed"):
             self.vrf["l"] = []
             self.vrf["ab"] = []
+        if filter_type == "mixed":
+            # extension: Gabor and centre-surround neurons in one store, told
+            # apart by vrf/kind (0 Gabor, 1 centre-surround)
+            self.vrf["kind"] = []
         self.iaf = {"kappa": [], "delta": [], "bias": [], "sigma": []}
         self.spike_count = []
         self.spikes = []
@@ -64,8 +68,13 @@ class vtem_storage(object):
         self.vrf["x0"].append(np.asarray(filter.h_x0, np.float64))
         self.vrf["y0"].append(np.asarray(filter.h_y0, np.float64))
         self.vrf["ab"].append(np.asarray(filter.h_ab, np.int32))
-        if filter.h_gain is not None:
-            self.vrf.setdefault("gain", []).append(np.asarray(filter.h_gain, np.float64))
+        if "kind" in self.vrf:
+            self.vrf["kind"].append(np.zeros(len(filter.h_alpha), np.int32))
+        self._gain(filter)
+
+    def _gain(self, filter):
+        g = filter.h_gain if filter.h_gain is not None else np.ones(len(filter.h_alpha))
+        self.vrf.setdefault("gain", []).append(np.asarray(g, np.float64))
 
     def write_cs_parameters(self, filter):
         if "vrf/sigma_center" not in self.data:
@@ -74,8 +83,12 @@ class vtem_storage(object):
         self.vrf["alpha"].append(np.asarray(filter.h_alpha, np.float64))
         self.vrf["x0"].append(np.asarray(filter.h_x0, np.float64))
         self.vrf["y0"].append(np.asarray(filter.h_y0, np.float64))
-        if filter.h_gain is not None:
-            self.vrf.setdefault("gain", []).append(np.asarray(filter.h_gain, np.float64))
+        if "kind" in self.vrf:
+            n = len(filter.h_alpha)
+            self.vrf["l"].append(np.zeros(n))
+            self.vrf["ab"].append(np.zeros(n, np.int32))
+            self.vrf["kind"].append(np.ones(n, np.int32))
+        self._gain(filter)
 
     def write_neuron_parameters(self, iaf):
         self.iaf["kappa"].append(np.asarray(iaf.h_kappa, np.float64))
@@ -116,9 +129,16 @@ class vtem_storage_read(object):
                 int(self.d["vrf/Px"]), int(self.d["vrf/Py"]), float(self.d["vrf/dx"]), float(self.d["vrf/dy"]))
 
     def read_vrf_type(self):
-        self.filter_type = "gabor" if "vrf/ab" in self.d else "cs"
+        if "vrf/kind" in self.d:
+            self.filter_type = "mixed"
+        else:
+            self.filter_type = "gabor" if "vrf/ab" in self.d else "cs"
 
     def read_vrf(self):
+        if self.filter_type == "mixed":
+            return (self.d["vrf/alpha"], self.d["vrf/l"], self.d["vrf/x0"], self.d["vrf/y0"], self.d["vrf/ab"],
+                    float(self.d["vrf/KAPPA"]), float(self.d["vrf/sigma_center"]),
+                    float(self.d["vrf/sigma_surround"]), self.d["vrf/kind"])
         if self.filter_type == "gabor":
             return (self.d["vrf/alpha"], self.d["vrf/l"], self.d["vrf/x0"], self.d["vrf/y0"], self.d["vrf/ab"],
                     float(self.d["vrf/KAPPA"]))
@@ -140,7 +160,10 @@ class vtem_storage_read(object):
     def select_neurons(self, domain):
         """Neurons centred inside ``domain`` = [x0, x1, y0, y1] (+-0.01),
         with centres shifted to the domain centre (spike_store.py:243-277)."""
-        if self.filter_type == "gabor":
+        if self.filter_type == "mixed":
+            (h_alpha, h_l, h_x0, h_y0, h_ab, self.KAPPA, self.sigma_center, self.sigma_surround,
+             h_kind) = self.read_vrf()
+        elif self.filter_type == "gabor":
             h_alpha, h_l, h_x0, h_y0, h_ab, self.KAPPA = self.read_vrf()
         else:
             h_alpha, h_x0, h_y0, self.sigma_center, self.sigma_surround = self.read_vrf()
@@ -156,9 +179,11 @@ class vtem_storage_read(object):
         self.y0 = h_y0[self.choose] - shifty
         g = self.read_gain()
         self.gain = None if g is None else g[self.choose]
-        if self.filter_type == "gabor":
+        if self.filter_type in ("gabor", "mixed"):
             self.l = h_l[self.choose]
             self.ab = h_ab[self.choose]
+        if self.filter_type == "mixed":
+            self.kind = h_kind[self.choose]
         self.decode_neurons = self.choose.size
 
     def read_select_spikes(self, time_frame):

@@ -67,10 +67,25 @@ def period_grid(Mx, My, Wx, Wy, dx, dy):
     return rfSx, rfSy, rfPx, rfPy
 
 
-def decoder_bank(spfile, Mx, My, Wx, Wy, dx, dy, dtype=np.complex128):
+def decoder_bank(spfile, Mx, My, Wx, Wy, dx, dy, dtype=np.complex128, kind=None):
     """The decoder-side RF object of the selected neurons, sampled at 4x on
-    one spatial period (vtdm.py:423-435)."""
+    one spatial period (vtdm.py:423-435).  For a mixed store, ``kind``
+    (0 Gabor, 1 centre-surround) picks one family; returns (bank, indices)."""
     rfSx, rfSy, rfPx, rfPy = period_grid(Mx, My, Wx, Wy, dx, dy)
+    if spfile.filter_type == "mixed":
+        sel = np.nonzero(spfile.kind == kind)[0]
+        g = None if spfile.gain is None else spfile.gain[sel]
+        if kind == 0:
+            gb = vrf.vrf_gabor((rfPy, rfPx), dx=rfSx / rfPx, dy=rfSy / rfPy, scale=4, dtype=dtype)
+            gb.load_parameters(num_neurons=len(sel), h_alpha=spfile.alpha[sel], h_l=spfile.l[sel],
+                               h_x0=spfile.x0[sel], h_y0=spfile.y0[sel], h_ab=spfile.ab[sel], KAPPA=spfile.KAPPA,
+                               h_gain=g)
+        else:
+            gb = vrf.vrf_cs((rfPy, rfPx), dx=rfSx / rfPx, dy=rfSy / rfPy, scale=4, dtype=dtype)
+            gb.load_parameters(num_neurons=len(sel), h_alpha=spfile.alpha[sel], h_x0=spfile.x0[sel],
+                               h_y0=spfile.y0[sel], sigma_center=spfile.sigma_center,
+                               sigma_surround=spfile.sigma_surround, h_gain=g)
+        return gb, sel
     if spfile.filter_type == "gabor":
         gb = vrf.vrf_gabor((rfPy, rfPx), dx=rfSx / rfPx, dy=rfSy / rfPy, scale=4, dtype=dtype)
         gb.load_parameters(num_neurons=spfile.decode_neurons, h_alpha=spfile.alpha, h_l=spfile.l,
@@ -83,10 +98,18 @@ def decoder_bank(spfile, Mx, My, Wx, Wy, dx, dy, dtype=np.complex128):
     return gb
 
 
-def prep_from_banks(banks, h_norm, Mx, My, Wx, Wy, decPx, decPy, decSx, decSy):
+def prep_from_banks(banks, h_norm, Mx, My, Wx, Wy, decPx, decPy, decSx, decSy, order=None):
     """Ds, phi and Dsw of one or several decoder-side RF objects (each on
-    one spatial period), concatenated in order."""
-    Ds = torch.cat([b.compute_Ds(Mx, My) for b in banks], 0)
+    one spatial period), concatenated in order (or scattered to the neuron
+    indices ``order[i]`` of bank i)."""
+    parts = [b.compute_Ds(Mx, My) for b in banks]
+    if order is None:
+        Ds = torch.cat(parts, 0)
+    else:
+        N = sum(len(o) for o in order)
+        Ds = torch.empty((N,) + tuple(parts[0].shape[1:]), dtype=parts[0].dtype, device=parts[0].device)
+        for p, o in zip(parts, order):
+            Ds[torch.as_tensor(o, device=Ds.device)] = p
     dirich = banks[0].compute_dirich_space_fft(Ds, Mx, My, decPx, decPy, decSx, decSy, Wx, Wy)
     Dsw = banks[0].compute_Dsw(Ds, Mx, My, h_norm)
     dx = decSx / decPx
@@ -119,8 +142,14 @@ def VTDM_prep(spikefile, Dswfilename, dirichfilename, Mx, My=None, domain=None, 
     decSy = domain[3] - domain[2]
     decPx = int(np.round(decSx / dx))
     decPy = int(np.round(decSy / dy))
-    gb = decoder_bank(spfile, Mx, My, Wx, Wy, dx, dy, np.complex128)
-    prep = prep_from_banks([gb], h_norm, Mx, My, Wx, Wy, decPx, decPy, decSx, decSy)
+    if spfile.filter_type == "mixed":
+        pairs = [decoder_bank(spfile, Mx, My, Wx, Wy, dx, dy, np.complex128, kind=k) for k in (0, 1)]
+        pairs = [(b, o) for b, o in pairs if len(o)]
+        prep = prep_from_banks([b for b, _ in pairs], h_norm, Mx, My, Wx, Wy, decPx, decPy, decSx, decSy,
+                               order=[o for _, o in pairs])
+    else:
+        gb = decoder_bank(spfile, Mx, My, Wx, Wy, dx, dy, np.complex128)
+        prep = prep_from_banks([gb], h_norm, Mx, My, Wx, Wy, decPx, decPy, decSx, decSy)
     if dirichfilename is not None:
         simpleio.write_memory_to_file(prep.dirich, dirichfilename)
     if Dswfilename is not None:
@@ -131,8 +160,15 @@ def VTDM_prep(spikefile, Dswfilename, dirichfilename, Mx, My=None, domain=None, 
 def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, My=None, Mt=None, domain=None,
          Wx=None, Wy=None, Wt=None, lamb=0.0, dtype=np.float64, rnn=False, alpha=50000, steps=4000,
          stitching=False, stitch_interval=None, output_format=0, output="rec", *, rcond=1e-8,
-         return_device=False, prep=None, rnn_dt=1e-6):
-    """Reconstruct a time range of the video (vtdm.py:450-699)."""
+         return_device=False, prep=None, rnn_dt=1e-6, decoder="plain", coeff_solver="auto"):
+    """Reconstruct a time range of the video (vtdm.py:450-699).
+
+    ``decoder="coeff"`` (extension) decodes each window in the Dirichlet
+    coefficient space (:mod:`vtem_b200.fast`), the same reconstruction
+    without the spike-by-spike Gram; it needs ``prep`` (VTDM_prep's result)
+    and the pseudoinverse solver."""
+    if decoder == "coeff" and (prep is None or rnn):
+        raise ValueError("the coefficient-space decoder needs prep= and the pseudoinverse solver")
     spfile = ss.vtem_storage_read(spikefile)
     spfile.read_vrf_type()
     spfile.read_num_neurons()
@@ -180,21 +216,23 @@ def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, M
     right_window = 1.0 - left_window
     u = torch.empty((total_l, decPy, decPx), dtype=torch.float64, device="cuda")
     spfile.select_neurons(domain)
+    fastdec = None
+    if decoder == "coeff":
+        from . import fast
+        fastdec = fast.from_prep(prep, Wt, Mt, rcond=rcond, solver=coeff_solver)
     i = 0
     prev = None
     while True:
         tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_sigma = spfile.read_select_spikes([start, end])
         h_norm = _norm_from_sigma(spfile.read_iaf()[0], h_sigma)[spfile.choose]
-        cp = dr.dirichlet(spfile.decode_neurons, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm, Wt, Mt,
-                          dtype)
-        cp.compute_q()
-        cp.compute_G(Dsw, float(lamb), lower_only=not rnn)
-        if rnn:
-            cp.d_q = nn.rnn3(cp.d_G, cp.d_q, dt=rnn_dt, alpha=alpha, steps=steps)
+        if fastdec is not None:
+            if len(tk1) == 0:
+                raise ValueError("no spikes to decode")
+            fastdec.norm = torch.as_tensor(h_norm, device="cuda")
+            u_rec = fastdec.decode(tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, round((end - start) / dt) * dt, dt)
         else:
-            cp.d_q = ls.solve_eq_sym(cp.d_G, cp.d_q, rcond=rcond)
-        cp.freeG()
-        u_rec = cp.reconstruct(dirich, [0, round((end - start) / dt) * dt], dt)
+            u_rec = _plain_window(spfile, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm, Wt, Mt, dtype, Dsw,
+                                  lamb, rnn, rnn_dt, alpha, steps, rcond, dirich, start, end, dt)
         if overlap_l:
             if i == 0:
                 if end_time - end < dt:
@@ -225,3 +263,17 @@ def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, M
     if return_device:
         return u
     return u.cpu().numpy()
+
+
+def _plain_window(spfile, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm, Wt, Mt, dtype, Dsw, lamb, rnn,
+                  rnn_dt, alpha, steps, rcond, dirich, start, end, dt):
+    """One window of the reference decoder (vtdm.py:640-652)."""
+    cp = dr.dirichlet(spfile.decode_neurons, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm, Wt, Mt, dtype)
+    cp.compute_q()
+    cp.compute_G(Dsw, float(lamb), lower_only=not rnn)
+    if rnn:
+        cp.d_q = nn.rnn3(cp.d_G, cp.d_q, dt=rnn_dt, alpha=alpha, steps=steps)
+    else:
+        cp.d_q = ls.solve_eq_sym(cp.d_G, cp.d_q, rcond=rcond)
+    cp.freeG()
+    return cp.reconstruct(dirich, [0, round((end - start) / dt) * dt], dt)

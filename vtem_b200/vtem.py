@@ -62,6 +62,9 @@ def VTEM_IAF(videofile, output_filename, Wt, rf, Wx=2 * np.pi * 4, Wy=2 * np.pi 
     else:
         store_type = _rf_type(banks[0])
     spikefile = ss.vtem_storage(output_filename, rf.num_neurons, store_type)
+    if store_type == "mixed":
+        gb0 = next(b for b in banks if _rf_type(b) == "gabor")
+        spikefile.data["vrf/KAPPA"] = np.array(float(gb0.KAPPA))
     spikefile.write_video_attributes(Wt, Wx, Wy, rf.Px, rf.Py, float(dx), float(dy))
     for b in banks:
         if _rf_type(b) == "gabor":
