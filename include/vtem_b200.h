@@ -208,6 +208,24 @@ int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, int Mx, i
                          double dt, int Nt, int Px, int Py, int Px1, int Py1, double* A_work, void* u, int out_f32,
                          void* stream);
 
+/* vtb_coeff_synthesize without the caller's A_work buffer, for callers that
+ * cannot allocate device memory (a plugin confined to another runtime's
+ * memory pool, code that may only use a framework's allocator, replay inside
+ * an already-built execution graph).  No counterpart in the reference: its
+ * reconstruction always allocates through PyCUDA.  The scratch is a fixed
+ * 4 MiB device array inside the library, present on every GPU that loads it
+ * until the process exits; frames are processed in chunks that fit, so Nt is
+ * unbounded but Ks * 16 bytes must be at most 4 MiB (Ks <= 262144), else
+ * VTB_BAD_ARG.  The call allocates nothing (no cudaMalloc/cudaFree, no
+ * allocating library).  The first call on a device looks up the array's
+ * device address with that device current; make that first call before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (other streams, other threads) race, so serialise them.  Output equals
+ * vtb_coeff_synthesize's. */
+int vtb_coeff_synthesize_noalloc(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, double W,
+                                 double t0, double dt, int Nt, int Px, int Py, int Px1, int Py1, void* u,
+                                 int out_f32, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

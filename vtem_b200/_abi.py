@@ -52,6 +52,7 @@ SIGNATURES = {
     "vtb_herm_solve_workspace": [I, I, P],
     "vtb_herm_solve": [P, L, P, P, I, D, I, I, P, L, P, P, P],
     "vtb_coeff_synthesize": [P, P, I, I, I, I, D, D, D, I, I, I, I, I, P, P, I, P],
+    "vtb_coeff_synthesize_noalloc": [P, P, I, I, I, I, D, D, D, I, I, I, I, I, P, I, P],
 }
 
 _lib = None

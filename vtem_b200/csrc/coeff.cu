@@ -358,3 +358,119 @@ VTB_API int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, i
     }
     return launch_status();
 }
+
+// ---------------------------------------------------------------------------
+// Synthesis for callers that cannot allocate device memory.
+//
+// Some hosts of this library cannot call cudaMalloc: a plugin running inside
+// another runtime's fixed memory pool, a process whose allocations all go
+// through a framework allocator it may not bypass, or code replayed inside
+// an already-instantiated execution graph.  For them this variant keeps its
+// temporal-expansion scratch in a fixed file-scope device array instead of a
+// caller-provided buffer.  The array (kNoAllocScratchBytes = 4 MiB) exists on
+// every GPU that loads the library, until the process exits.  Frames are
+// processed in chunks that fit in it, so any clip length works as long as
+// one frame's coefficients (Ks * 16 bytes) fit.
+#include <mutex>
+
+namespace vtb {
+
+constexpr int64_t kNoAllocScratchBytes = 4ll << 20;
+constexpr int64_t kNoAllocScratchElems = kNoAllocScratchBytes / (int64_t)sizeof(double2);
+
+static __device__ __align__(256) double2 g_noalloc_synth_scratch[kNoAllocScratchElems];
+
+// A[i][s] = sum_m a[s][m] e^{jmW t}, t = t0 + (f0 + i) dt, for i < gridDim.x
+__global__ void temporal_expand_chunk_kernel(const double2* __restrict__ a, int Ks, int Mt, double W, double t0,
+                                             double dt, int f0, double2* __restrict__ A) {
+    extern __shared__ double2 se[];
+    const int Kt = 2 * Mt + 1;
+    const int it = f0 + blockIdx.x;
+    const double tt = t0 + it * dt;
+    for (int mi = threadIdx.x; mi < Kt; mi += blockDim.x) {
+        double s, c;
+        sincos((mi - Mt) * W * tt, &s, &c);
+        se[mi] = make_double2(c, s);
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < Ks; s += blockDim.x) {
+        double2 acc = make_double2(0, 0);
+        for (int mi = 0; mi < Kt; ++mi) {
+            const double2 p = cmul(a[(int64_t)s * Kt + mi], se[mi]);
+            acc.x += p.x;
+            acc.y += p.y;
+        }
+        A[(int64_t)blockIdx.x * Ks + s] = acc;
+    }
+}
+
+// Device address of the scratch array, looked up once per device with that
+// device current (in host code the array's name is only a host-side stand-in).
+static double2* noalloc_scratch(int dev, int* status) {
+    static std::mutex mu;
+    static double2* addr[64] = {nullptr};
+    if (dev < 0 || dev >= 64) {
+        *status = VTB_BAD_ARG;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_synth_scratch);
+        if (e != cudaSuccess || !p) {
+            set_last_cuda_error(e);
+            *status = VTB_CUDA_ERR;
+            return nullptr;
+        }
+        addr[dev] = reinterpret_cast<double2*>(p);
+    }
+    return addr[dev];
+}
+
+}  // namespace vtb
+
+VTB_API int vtb_coeff_synthesize_noalloc(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt,
+                                         double W, double t0, double dt, int Nt, int Px, int Py, int Px1, int Py1,
+                                         void* u, int out_f32, void* stream) {
+    VTB_CHECK_ARG(Ks > 0 && Mx >= 0 && My >= 0 && Mt >= 0 && Nt >= 0 && Px > 0 && Py > 0 && Px1 >= Px && Py1 >= Py);
+    VTB_CHECK_ARG(2 * Mx + 1 <= Px1 && 2 * My + 1 <= Py1);
+    // one frame of expanded coefficients must fit in the fixed scratch
+    VTB_CHECK_ARG((int64_t)Ks <= kNoAllocScratchElems);
+    if (Nt == 0) return VTB_OK;
+    VTB_CHECK_ARG(a && smap && u);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    int st = VTB_OK;
+    double2* scratch = noalloc_scratch(dev, &st);
+    if (!scratch) return st;
+    cudaStream_t s = as_stream(stream);
+    const int Kt = 2 * Mt + 1;
+    const int Kx = 2 * Mx + 1, Ky = 2 * My + 1;
+    const size_t sm = (size_t)(Kx * Px + Ky * Py + Ky * Kx + Ky * Px) * sizeof(double2);
+    VTB_CHECK_ARG(sm <= 200 * 1024);
+    if (sm > 48 * 1024) {
+        if (out_f32)
+            VTB_CUDA_TRY(cudaFuncSetAttribute(synth_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        else
+            VTB_CUDA_TRY(cudaFuncSetAttribute(synth_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    }
+    const int chunk = (int)std::min<int64_t>(kNoAllocScratchElems / Ks, (int64_t)Nt);
+    const int64_t frame = (int64_t)Px * Py;
+    for (int f0 = 0; f0 < Nt; f0 += chunk) {
+        const int nf = std::min(chunk, Nt - f0);
+        temporal_expand_chunk_kernel<<<nf, 128, Kt * sizeof(double2), s>>>(reinterpret_cast<const double2*>(a), Ks,
+                                                                            Mt, W, t0, dt, f0, scratch);
+        st = launch_status();
+        if (st) return st;
+        const int blocks = ceil_div(nf, kSynthFrames);
+        if (out_f32)
+            synth_kernel<float><<<blocks, 256, sm, s>>>(scratch, smap, Ks, Mx, My, Px, Py, Px1, Py1, nf,
+                                                       reinterpret_cast<float*>(u) + f0 * frame);
+        else
+            synth_kernel<double><<<blocks, 256, sm, s>>>(scratch, smap, Ks, Mx, My, Px, Py, Px1, Py1, nf,
+                                                        reinterpret_cast<double*>(u) + f0 * frame);
+        st = launch_status();
+        if (st) return st;
+    }
+    return VTB_OK;
+}
