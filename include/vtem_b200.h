@@ -78,6 +78,26 @@ int vtb_gemm_f64(int M, int N, int K, const double* A, int64_t a_m, int64_t a_k,
                  int64_t b_n, int64_t b_k, double* C, int64_t c_m, int64_t c_n, double alpha, double beta,
                  void* stream);
 
+/* ------------------------------------------------------------ tensor cores (tcgen05) */
+
+/* Split a float64 (src_f32 = 0) or float32 matrix src(r, k) = src[r*ld + k*k_stride]
+ * (rows x K, times scale) into bf16 hi/lo parts laid out along K as
+ * dst[r][0:3Kp] = [hi | hi | lo] (pattern 0, the A side) or [hi | lo | hi]
+ * (pattern 1, the B side), Kp = K rounded up to 64, zero padded.  With
+ * vtb_tc_gemm_bf16 over K = 3Kp this gives the split-bf16 product
+ * hi*hi + hi*lo + lo*hi accumulated in fp32.  The mixed-precision form of
+ * the DGEMMs of vtem/vrf.py:291 (RF filter) and the Gram products. */
+int vtb_split_bf16x3(const void* src, int src_f32, int rows, int K, int64_t ld, int64_t k_stride, double scale,
+                     int pattern, void* dst, void* stream);
+
+/* C(m, n) = alpha * sum_k A[m*K + k] B[n*K + k] (+ C when accumulate), A (M x K)
+ * and B (N x K) bf16 row-major (K-major), K a multiple of 64, on the sm_100a
+ * tensor cores (TMA + tcgen05.mma, fp32 accumulator in tensor memory), stored
+ * at C[m*c_m + n*c_n] as float64 (out_f64 = 1) or float32.  *err (device int,
+ * caller-zeroed) receives VTB_TIMEOUT if a pipeline wait ever gave up. */
+int vtb_tc_gemm_bf16(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
+                     int out_f64, double alpha, int accumulate, int32_t* err, void* stream);
+
 /* ------------------------------------------------------------ IAF encoder */
 
 /* IAF time encoding of input(t, n) = input[t*in_t_stride + n*in_n_stride],
@@ -207,6 +227,34 @@ int vtb_herm_solve(double* M, int64_t ld, const double* b, double* a, int K, dou
 int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, double W, double t0,
                          double dt, int Nt, int Px, int Py, int Px1, int Py1, double* A_work, void* u, int out_f32,
                          void* stream);
+
+/* Mixed-precision Kronecker Gram (tensor cores).  ps/ps2 list the npairs
+ * spatial index pairs s <= s'.  L3 receives the RF-bank operand (2*npairs
+ * rows x 3*Kp bf16, Kp = 2N rounded up to 64; once per decoder), R3 the
+ * per-decode operand from Wn (Kt*Kt rows x 3*Kp).  vtb_tc_gemm_bf16(L3, R3)
+ * then gives C[(2p + part)][(m, m')], scattered into the column-major
+ * Hermitian M by vtb_coeff_scatter. */
+int vtb_coeff_lhs_split(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs, void* L3,
+                        void* stream);
+int vtb_coeff_wn_split(const double* Wn, int N, int Kt, void* R3, void* stream);
+int vtb_coeff_scatter(const float* C, int64_t ldc, const int32_t* ps, const int32_t* ps2, int npairs, int Kt, double* M,
+                      int64_t ldm, void* stream);
+
+/* b[(s,m)] = sum_n d[n][s] gn[n][m] (the right-hand side Phi^H q). */
+int vtb_coeff_rhs(const double* d, int N, int Ks, const double* gn, int Kt, double* b, void* stream);
+
+/* Exact float64 residual r = Phi^H (q - Phi a) through the Kronecker factors
+ * (gres: N x (2Mt+1) complex scratch).  Refinement sweeps of the mixed
+ * decoder. */
+int vtb_coeff_residual(const double* tk1, const double* tk2, const int32_t* ind, int nspk, int N, const double* kappa,
+                       const double* delta, const double* bias, const double* norm, int Mt, double W, const double* d,
+                       int Ks, const double* a, double* gres, double* r, void* stream);
+
+/* x = M^-1 x with M factorised in place by vtb_herm_solve(mode 1); work >= 256 bytes. */
+int vtb_herm_potrs(const double* Mfac, int64_t ld, double* x, int K, void* work, int64_t work_bytes, void* stream);
+
+/* a += d (n complex). */
+int vtb_zadd(double* a, const double* d, int n, void* stream);
 
 /* vtb_coeff_synthesize without the caller's A_work buffer, for callers that
  * cannot allocate device memory (a plugin confined to another runtime's

@@ -109,3 +109,24 @@ def test_coeff_decode_float32_output(small_encoded):
     u32 = dec.decode(tk1, tk2, ind, kap, dl, bia, w.T, w.dt, out_dtype=torch.float32)
     err = (u32.double() - u64).norm() / u64.norm()
     assert err < 1e-6
+
+
+def test_mixed_decoder_matches_float64(small_encoded):
+    w, store, prep = small_encoded
+    rd = spike_store.vtem_storage_read(store)
+    rd.read_vrf_type()
+    rd.read_num_neurons()
+    rd.select_neurons([-0.5, 0.5, -0.5, 0.5])
+    tk1, tk2, ind, kap, dl, bia, sig = rd.read_select_spikes([0.0, w.T])
+    ref = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="eig").decode(tk1, tk2, ind, kap, dl, bia, w.T, w.dt)
+    dec0 = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="mixed", mixed_sweeps=0)
+    u0 = dec0.decode(tk1, tk2, ind, kap, dl, bia, w.T, w.dt)
+    dec = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="mixed", mixed_sweeps=3)
+    u = dec.decode(tk1, tk2, ind, kap, dl, bia, w.T, w.dt)
+    assert dec.last_solver == "mixed"
+    e0 = ((u0 - ref).norm() / ref.norm()).item()
+    e = ((u - ref).norm() / ref.norm()).item()
+    # tensor-core Gram alone: >= 40 dB; after float64 refinement: float64-level agreement
+    assert e0 < 1e-2, e0
+    assert e < 1e-9, (e0, e)
+    assert dec.residual_norm(tk1, tk2, ind, kap, dl, bia) < 1e-10

@@ -1,0 +1,60 @@
+"""Tensor-core (tcgen05) GEMM against float64 references (GPU)."""
+import numpy as np
+import pytest
+import torch
+
+from vtem_b200 import tc
+
+pytestmark = pytest.mark.gpu
+
+
+def test_bf16_exact_inputs():
+    # bf16-representable operands with few terms: fp32 accumulation is exact
+    rng = np.random.default_rng(0)
+    M, N, K = 200, 130, 192
+    A = torch.as_tensor(rng.integers(-8, 9, (M, K)).astype(np.float32) / 8, device="cuda").to(torch.bfloat16)
+    B = torch.as_tensor(rng.integers(-8, 9, (N, K)).astype(np.float32) / 8, device="cuda").to(torch.bfloat16)
+    out = torch.zeros((M, N), dtype=torch.float64, device="cuda")
+    out, err = tc.gemm_bf16(A.contiguous(), B.contiguous(), out)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref = A.double() @ B.double().T
+    assert torch.equal(out, ref)
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (300, 257, 1000), (1000, 64, 4096)])
+def test_split_bf16_accuracy(M, N, K):
+    rng = np.random.default_rng(M + N + K)
+    A = torch.as_tensor(rng.standard_normal((M, K)), device="cuda")
+    B = torch.as_tensor(rng.standard_normal((N, K)), device="cuda")
+    C = tc.gemm_split_bf16(A, B, alpha=0.5)
+    ref = 0.5 * (A @ B.T)
+    rel = ((C - ref).norm() / ref.norm()).item()
+    # hi*lo split drops lo*lo: ~2^-16 of the products' scale, plus fp32 accumulation
+    assert rel < 5e-5, rel
+
+
+def test_split_bf16_transposed_output_and_float32():
+    rng = np.random.default_rng(3)
+    A = torch.as_tensor(rng.standard_normal((257, 300)), device="cuda")
+    B = torch.as_tensor(rng.standard_normal((99, 300)), device="cuda")
+    C = tc.gemm_split_bf16(A, B, out_layout="col", out_dtype=torch.float32)
+    ref = (A @ B.T).T
+    assert C.shape == (99, 257)
+    rel = ((C.double() - ref).norm() / ref.norm()).item()
+    assert rel < 5e-5, rel
+
+
+def test_rf_filter_split_bf16_matches_f64():
+    from vtem_b200 import vrf
+    rng = np.random.default_rng(5)
+    V = torch.as_tensor(rng.standard_normal((300, 32, 32)), device="cuda")
+    gb = vrf.vrf_gabor((32, 32), dx=1 / 32, dy=1 / 32)
+    N = 70
+    gb.load_parameters(num_neurons=N, h_alpha=rng.uniform(0.05, 0.2, N), h_l=rng.uniform(0, 3, N),
+                       h_x0=rng.uniform(-.4, .4, N), h_y0=rng.uniform(-.4, .4, N),
+                       h_ab=rng.integers(0, 2, N).astype(np.int32), KAPPA=2.5)
+    ref = gb.filter(V, out_layout="neuron")
+    got = gb.filter(V, out_layout="neuron", precision="bf16x3")
+    rel = ((got - ref).norm() / ref.norm()).item()
+    assert rel < 5e-5, rel

@@ -53,6 +53,15 @@ SIGNATURES = {
     "vtb_herm_solve": [P, L, P, P, I, D, I, I, P, L, P, P, P],
     "vtb_coeff_synthesize": [P, P, I, I, I, I, D, D, D, I, I, I, I, I, P, P, I, P],
     "vtb_coeff_synthesize_noalloc": [P, P, I, I, I, I, D, D, D, I, I, I, I, I, P, I, P],
+    "vtb_split_bf16x3": [P, I, I, I, L, L, D, I, P, P],
+    "vtb_tc_gemm_bf16": [P, I, P, I, I, P, L, L, I, D, I, P, P],
+    "vtb_coeff_lhs_split": [P, I, I, P, P, I, P, P],
+    "vtb_coeff_wn_split": [P, I, I, P, P],
+    "vtb_coeff_scatter": [P, L, P, P, I, I, P, L, P],
+    "vtb_coeff_rhs": [P, I, I, P, I, P, P],
+    "vtb_coeff_residual": [P, P, P, I, I, P, P, P, P, I, D, P, I, P, P, P, P],
+    "vtb_herm_potrs": [P, L, P, I, P, L, P],
+    "vtb_zadd": [P, P, I, P],
 }
 
 _lib = None

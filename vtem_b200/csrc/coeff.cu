@@ -19,6 +19,10 @@
 // space-time basis: A[t, s] = sum_m a[s, m] e^{jmWt}, then per frame
 // u = Re(ey^T A_t ex) on the decode grid (synth_kernel), whose output write is
 // the one HBM-sized stream of the whole decode.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace vtb {
@@ -144,8 +148,10 @@ __global__ void __launch_bounds__(256) kron_gram_kernel(const double2* __restric
             }
             __syncthreads();
             if (e < KK) {
+                double2 wnext = Wn[(int64_t)n0 * KK + e];
                 for (int r = 0; r < nn; ++r) {
-                    const double2 w = Wn[(int64_t)(n0 + r) * KK + e];
+                    const double2 w = wnext;
+                    if (r + 1 < nn) wnext = Wn[(int64_t)(n0 + r + 1) * KK + e];
 #pragma unroll
                     for (int i = 0; i < kKT; ++i)
 #pragma unroll
@@ -173,19 +179,36 @@ __global__ void __launch_bounds__(256) kron_gram_kernel(const double2* __restric
     }
 }
 
-// b[(s, m)] = sum_n d[n][s] g[n][m]
-__global__ void kron_rhs_kernel(const double2* __restrict__ d, int N, int Ks, const double2* __restrict__ gn,
-                                int Kt, double2* __restrict__ b) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= Ks * Kt) return;
-    const int s = e / Kt, m = e % Kt;
-    double2 acc = make_double2(0, 0);
-    for (int n = 0; n < N; ++n) {
-        const double2 p = cmul(d[(int64_t)n * Ks + s], gn[(int64_t)n * Kt + m]);
-        acc.x += p.x;
-        acc.y += p.y;
+// b[(s, m)] = sum_n d[n][s] g[n][m]: one block per spatial index s, the 8
+// warps split the neurons, lanes own temporal indices, partial sums reduced
+// in shared memory.
+__global__ void __launch_bounds__(256) kron_rhs_kernel(const double2* __restrict__ d, int N, int Ks,
+                                                       const double2* __restrict__ gn, int Kt,
+                                                       double2* __restrict__ b) {
+    __shared__ double2 part[8][32];
+    const int s = blockIdx.x;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int m0 = 0; m0 < Kt; m0 += 32) {
+        const int m = m0 + lane;
+        double2 acc = make_double2(0, 0);
+        if (m < Kt)
+            for (int n = w; n < N; n += 8) {
+                const double2 p = cmul(d[(int64_t)n * Ks + s], gn[(int64_t)n * Kt + m]);
+                acc.x += p.x;
+                acc.y += p.y;
+            }
+        part[w][lane] = acc;
+        __syncthreads();
+        if (w == 0 && m < Kt) {
+            double2 t = part[0][lane];
+            for (int k = 1; k < 8; ++k) {
+                t.x += part[k][lane].x;
+                t.y += part[k][lane].y;
+            }
+            b[(int64_t)s * Kt + m] = t;
+        }
+        __syncthreads();
     }
-    b[e] = acc;
 }
 
 // d[n][s] = norm_n * Ds[n][smap[s]]
@@ -225,7 +248,12 @@ __global__ void temporal_expand_kernel(const double2* __restrict__ a, int Ks, in
 
 // u[t][py][px] = Re sum_{r,c} A_t[(r,c)] ey[r][py] ex[c][px]; one block per
 // group of frames; ex/ey (with the (-1)^{mx+my} signs and the crop offsets of
-// the period grid) are built in shared memory by the block.
+// the period grid) are built in shared memory by the block.  Per frame the
+// block forms B[r][px] = sum_c A_t[(r,c)] ex[c][px], then each of the 256
+// threads accumulates a 4 x 4 set of pixels (py = ty + 16i, px = tx + 16j,
+// over 64 x 64 pixel tiles): 32 FMAs per 8 complex shared-memory reads, the
+// strided pixel map keeping those reads free of bank conflicts and the
+// stores in 128-byte rows.
 constexpr int kSynthFrames = 8;
 
 template <typename OutT>
@@ -255,6 +283,7 @@ __global__ void __launch_bounds__(256) synth_kernel(const double2* __restrict__ 
         const double sg = (my & 1) ? -1.0 : 1.0;
         ey[e] = make_double2(sg * co, sg * s);
     }
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int f0 = blockIdx.x * kSynthFrames;
     for (int f = f0; f < min(f0 + kSynthFrames, Nt); ++f) {
         __syncthreads();
@@ -266,22 +295,49 @@ __global__ void __launch_bounds__(256) synth_kernel(const double2* __restrict__ 
             const int rr = e / Px, px = e % Px;
             double2 acc = make_double2(0, 0);
             for (int c = 0; c < Kx; ++c) {
-                const double2 p = cmul(G[rr * Kx + c], ex[c * Px + px]);
-                acc.x += p.x;
-                acc.y += p.y;
+                const double2 g = G[rr * Kx + c], x = ex[c * Px + px];
+                acc.x = fma(g.x, x.x, fma(-g.y, x.y, acc.x));
+                acc.y = fma(g.x, x.y, fma(g.y, x.x, acc.y));
             }
             B[e] = acc;
         }
         __syncthreads();
         OutT* uf = u + (int64_t)f * Px * Py;
-        for (int p = threadIdx.x; p < Px * Py; p += blockDim.x) {
-            const int py = p / Px, px = p % Px;
-            double acc = 0.0;
-            for (int rr = 0; rr < Ky; ++rr) {
-                const double2 b = B[rr * Px + px], e = ey[rr * Py + py];
-                acc = fma(b.x, e.x, fma(-b.y, e.y, acc));
+        for (int y0 = 0; y0 < Py; y0 += 64) {
+            for (int x0 = 0; x0 < Px; x0 += 64) {
+                double acc[4][4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+                for (int rr = 0; rr < Ky; ++rr) {
+                    double2 bv[4], ev[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int px = x0 + tx + 16 * j;
+                        bv[j] = px < Px ? B[rr * Px + px] : make_double2(0, 0);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const int py = y0 + ty + 16 * i;
+                        ev[i] = py < Py ? ey[rr * Py + py] : make_double2(0, 0);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) acc[i][j] = fma(bv[j].x, ev[i].x, fma(-bv[j].y, ev[i].y, acc[i][j]));
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int py = y0 + ty + 16 * i;
+                    if (py >= Py) continue;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int px = x0 + tx + 16 * j;
+                        if (px < Px) uf[(int64_t)py * Px + px] = (OutT)acc[i][j];
+                    }
+                }
             }
-            uf[p] = (OutT)acc;
         }
     }
 }
@@ -322,7 +378,7 @@ VTB_API int vtb_coeff_gram(const double* d, int N, int Ks, const double* Wn, con
                                                            reinterpret_cast<double2*>(M), ldm);
     int st = launch_status();
     if (st) return st;
-    kron_rhs_kernel<<<ceil_div((int64_t)Ks * Kt, 128), 128, 0, as_stream(stream)>>>(
+    kron_rhs_kernel<<<Ks, 256, 0, as_stream(stream)>>>(
         reinterpret_cast<const double2*>(d), N, Ks, reinterpret_cast<const double2*>(gn), Kt,
         reinterpret_cast<double2*>(b));
     return launch_status();
@@ -473,4 +529,226 @@ VTB_API int vtb_coeff_synthesize_noalloc(const double* a, const int32_t* smap, i
         if (st) return st;
     }
     return VTB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-precision pieces of the coefficient-space decoder.
+//
+// (1) The Kronecker Gram as one tensor-core GEMM.  For s <= s' (M is
+//     Hermitian) and a_n = d_n[s] conj(d_n[s']):
+//        Re M((s,m),(s',m')) = sum_n a_n.re W_n.re - a_n.im W_n.im
+//        Im M((s,m),(s',m')) = sum_n a_n.im W_n.re + a_n.re W_n.im
+//     i.e. C = L R^T with L[(pair, part), (n, q)] built from the RF bank
+//     only (split once per decoder) and R[(m, m'), (n, q)] = W_n[m, m'].q
+//     (split per decode).  Split-bf16 products, fp32 accumulation.
+// (2) The exact float64 residual r = Phi^H (q - Phi a) through the same
+//     Kronecker factors (never forming M in float64), for refinement sweeps
+//     on top of a factorisation of the tensor-core M.
+namespace vtb {
+
+// L3[row][seg*Kp + k], row = 2*pair + part, k = 2n + q, Kp = 2N rounded up to 64
+__global__ void kron_lhs_split_kernel(const double2* __restrict__ d, int N, int Ks, const int32_t* __restrict__ ps,
+                                      const int32_t* __restrict__ ps2, int npairs, int Kp,
+                                      __nv_bfloat16* __restrict__ L3) {
+    const int64_t total = (int64_t)npairs * 2 * Kp;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int row = (int)(e / Kp), k = (int)(e % Kp);
+        const int p = row >> 1, part = row & 1;
+        double x = 0.0;
+        if (k < 2 * N) {
+            const int n = k >> 1, q = k & 1;
+            const double2 a = cmulc(d[(int64_t)n * Ks + ps[p]], d[(int64_t)n * Ks + ps2[p]]);
+            // part 0 (real): [a.re, -a.im]; part 1 (imag): [a.im, a.re]
+            x = part == 0 ? (q == 0 ? a.x : -a.y) : (q == 0 ? a.y : a.x);
+        }
+        const __nv_bfloat16 hi = __float2bfloat16_rn((float)x);
+        const __nv_bfloat16 lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
+        __nv_bfloat16* dst = L3 + (int64_t)row * 3 * Kp + k;
+        dst[0] = hi;
+        dst[Kp] = hi;
+        dst[2 * Kp] = lo;
+    }
+}
+
+// R3[e][seg*Kp + k] with e = (m, m'), k = 2n + q: pattern [hi | lo | hi]
+__global__ void kron_rhs_split_kernel(const double2* __restrict__ Wn, int N, int KK, int Kp,
+                                      __nv_bfloat16* __restrict__ R3) {
+    const int64_t total = (int64_t)KK * Kp;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int e = (int)(i / Kp), k = (int)(i % Kp);
+        double x = 0.0;
+        if (k < 2 * N) {
+            const double2 w = Wn[(int64_t)(k >> 1) * KK + e];
+            x = (k & 1) ? w.y : w.x;
+        }
+        const __nv_bfloat16 hi = __float2bfloat16_rn((float)x);
+        const __nv_bfloat16 lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
+        __nv_bfloat16* dst = R3 + (int64_t)e * 3 * Kp + k;
+        dst[0] = hi;
+        dst[Kp] = lo;
+        dst[2 * Kp] = hi;
+    }
+}
+
+// M (column-major, complex float64) from the GEMM result C[(2p + part) * ldc + e]
+__global__ void kron_scatter_kernel(const float* __restrict__ C, int64_t ldc, const int32_t* __restrict__ ps,
+                                    const int32_t* __restrict__ ps2, int npairs, int Kt,
+                                    double2* __restrict__ M, int64_t ldm) {
+    const int KK = Kt * Kt;
+    const int64_t total = (int64_t)npairs * KK;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int p = (int)(i / KK), e = (int)(i % KK);
+        const int m = e / Kt, mp = e % Kt;
+        const int s = ps[p], sp = ps2[p];
+        const double re = C[(int64_t)(2 * p) * ldc + e], im = C[(int64_t)(2 * p + 1) * ldc + e];
+        const int64_t row = (int64_t)s * Kt + m, col = (int64_t)sp * Kt + mp;
+        M[col * ldm + row] = make_double2(re, im);
+        if (s != sp) M[row * ldm + col] = make_double2(re, -im);
+    }
+}
+
+// One block per neuron: v(m) = sum_s conj(d_n[s]) a(s, m); for each of the
+// neuron's spikes y_k = q_k - Re sum_m T_k(m) v(m); g(m) = sum_k conj(T_k(m)) y_k.
+__global__ void __launch_bounds__(256) coeff_residual_kernel(
+    const double* __restrict__ tk1, const double* __restrict__ tk2, const int32_t* __restrict__ ind, int nspk,
+    const double* __restrict__ kappa, const double* __restrict__ delta, const double* __restrict__ bias,
+    const double* __restrict__ norm, int Mt, double W, const double2* __restrict__ d, int Ks,
+    const double2* __restrict__ a, double2* __restrict__ gres) {
+    extern __shared__ double2 sh[];
+    const int Kt = 2 * Mt + 1;
+    double2* v = sh;                 // Kt
+    double2* T = v + Kt;             // kTChunk x Kt
+    double* y = reinterpret_cast<double*>(T + kTChunk * Kt);  // kTChunk
+    const int nr = blockIdx.x;
+    const int lo = lb_i32(ind, nspk, nr), hi = lb_i32(ind, nspk, nr + 1);
+    const double kd = kappa[nr] * delta[nr], bb = bias[nr], nn = norm[nr];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // v(m): warp w handles m = w, w+8, ...
+    for (int m = w; m < Kt; m += 8) {
+        double sr = 0.0, si = 0.0;
+        for (int s = lane; s < Ks; s += 32) {
+            const double2 dd = d[(int64_t)nr * Ks + s], aa = a[(int64_t)s * Kt + m];
+            sr += dd.x * aa.x + dd.y * aa.y;   // conj(dd) * aa
+            si += dd.x * aa.y - dd.y * aa.x;
+        }
+        for (int o = 16; o; o >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            si += __shfl_xor_sync(0xffffffffu, si, o);
+        }
+        if (lane == 0) v[m] = make_double2(sr, si);
+    }
+    double2 gacc = make_double2(0, 0);
+    for (int k0 = lo; k0 < hi; k0 += kTChunk) {
+        const int nk = min(kTChunk, hi - k0);
+        __syncthreads();
+        for (int x = threadIdx.x; x < nk * Kt; x += blockDim.x) {
+            const int kk = x / Kt, mi = x % Kt, m = mi - Mt;
+            const double ta = tk1[k0 + kk], tb = tk2[k0 + kk];
+            const double dtk = tb - ta;
+            double2 Tv;
+            if (m == 0) {
+                Tv = make_double2(dtk, 0.0);
+            } else {
+                const double mw = m * W;
+                const double amp = (2.0 / mw) * sin(0.5 * mw * dtk);
+                double s, c;
+                sincos(mw * (0.5 * (ta + tb)), &s, &c);
+                Tv = make_double2(amp * c, amp * s);
+            }
+            T[kk * Kt + mi] = Tv;
+        }
+        __syncthreads();
+        // y_k, one warp per spike
+        for (int kk = w; kk < nk; kk += 8) {
+            double acc = 0.0;
+            for (int mi = lane; mi < Kt; mi += 32) {
+                const double2 t = T[kk * Kt + mi], vv = v[mi];
+                acc += t.x * vv.x - t.y * vv.y;
+            }
+            for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) {
+                const double qk = (kd - bb * (tk2[k0 + kk] - tk1[k0 + kk])) * nn;
+                y[kk] = qk - acc;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < Kt) {
+            for (int kk = 0; kk < nk; ++kk) {
+                const double2 t = T[kk * Kt + threadIdx.x];
+                gacc.x += t.x * y[kk];
+                gacc.y -= t.y * y[kk];
+            }
+        }
+    }
+    if (threadIdx.x < Kt) gres[(int64_t)nr * Kt + threadIdx.x] = gacc;
+}
+
+__global__ void zadd_kernel(double2* __restrict__ a, const double2* __restrict__ d, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = make_double2(a[i].x + d[i].x, a[i].y + d[i].y);
+}
+
+}  // namespace vtb
+
+VTB_API int vtb_coeff_lhs_split(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs,
+                                void* L3, void* stream) {
+    VTB_CHECK_ARG(N > 0 && Ks > 0 && npairs > 0 && d && ps && ps2 && L3 && ((uintptr_t)L3 & 15) == 0);
+    const int Kp = ceil_div(2 * N, 64) * 64;
+    const int64_t total = (int64_t)npairs * 2 * Kp;
+    kron_lhs_split_kernel<<<(int)std::min<int64_t>(ceil_div(total, 256), 32 * kNumSMs), 256, 0, as_stream(stream)>>>(
+        reinterpret_cast<const double2*>(d), N, Ks, ps, ps2, npairs, Kp, reinterpret_cast<__nv_bfloat16*>(L3));
+    return launch_status();
+}
+
+VTB_API int vtb_coeff_wn_split(const double* Wn, int N, int Kt, void* R3, void* stream) {
+    VTB_CHECK_ARG(N > 0 && Kt > 0 && Wn && R3 && ((uintptr_t)R3 & 15) == 0);
+    const int Kp = ceil_div(2 * N, 64) * 64;
+    const int64_t total = (int64_t)Kt * Kt * Kp;
+    kron_rhs_split_kernel<<<(int)std::min<int64_t>(ceil_div(total, 256), 32 * kNumSMs), 256, 0, as_stream(stream)>>>(
+        reinterpret_cast<const double2*>(Wn), N, Kt * Kt, Kp, reinterpret_cast<__nv_bfloat16*>(R3));
+    return launch_status();
+}
+
+VTB_API int vtb_coeff_scatter(const float* C, int64_t ldc, const int32_t* ps, const int32_t* ps2, int npairs, int Kt,
+                              double* M, int64_t ldm, void* stream) {
+    VTB_CHECK_ARG(npairs > 0 && Kt > 0 && C && ps && ps2 && M);
+    const int64_t total = (int64_t)npairs * Kt * Kt;
+    kron_scatter_kernel<<<(int)std::min<int64_t>(ceil_div(total, 256), 32 * kNumSMs), 256, 0, as_stream(stream)>>>(
+        C, ldc, ps, ps2, npairs, Kt, reinterpret_cast<double2*>(M), ldm);
+    return launch_status();
+}
+
+VTB_API int vtb_coeff_rhs(const double* d, int N, int Ks, const double* gn, int Kt, double* b, void* stream) {
+    VTB_CHECK_ARG(N > 0 && Ks > 0 && Kt > 0 && d && gn && b);
+    kron_rhs_kernel<<<Ks, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(d), N, Ks,
+                                                      reinterpret_cast<const double2*>(gn), Kt,
+                                                      reinterpret_cast<double2*>(b));
+    return launch_status();
+}
+
+VTB_API int vtb_coeff_residual(const double* tk1, const double* tk2, const int32_t* ind, int nspk, int N,
+                               const double* kappa, const double* delta, const double* bias, const double* norm,
+                               int Mt, double W, const double* d, int Ks, const double* a, double* gres, double* r,
+                               void* stream) {
+    VTB_CHECK_ARG(nspk > 0 && N > 0 && Ks > 0 && Mt >= 1 && Mt <= 128 && tk1 && tk2 && ind && kappa && delta &&
+                  bias && norm && d && a && gres && r);
+    const int Kt = 2 * Mt + 1;
+    const size_t sm = (size_t)Kt * sizeof(double2) + (size_t)kTChunk * Kt * sizeof(double2) + kTChunk * sizeof(double);
+    cudaStream_t s = as_stream(stream);
+    coeff_residual_kernel<<<N, 256, sm, s>>>(tk1, tk2, ind, nspk, kappa, delta, bias, norm, Mt, W,
+                                             reinterpret_cast<const double2*>(d), Ks,
+                                             reinterpret_cast<const double2*>(a), reinterpret_cast<double2*>(gres));
+    int st = launch_status();
+    if (st) return st;
+    kron_rhs_kernel<<<Ks, 256, 0, s>>>(reinterpret_cast<const double2*>(d), N, Ks,
+                                       reinterpret_cast<const double2*>(gres), Kt, reinterpret_cast<double2*>(r));
+    return launch_status();
+}
+
+VTB_API int vtb_zadd(double* a, const double* d, int n, void* stream) {
+    VTB_CHECK_ARG(n >= 0 && a && d);
+    if (n == 0) return VTB_OK;
+    zadd_kernel<<<ceil_div(n, 256), 256, 0, as_stream(stream)>>>(reinterpret_cast<double2*>(a),
+                                                                 reinterpret_cast<const double2*>(d), n);
+    return launch_status();
 }

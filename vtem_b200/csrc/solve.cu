@@ -477,3 +477,21 @@ VTB_API int vtb_herm_solve(double* M, int64_t ld, const double* b, double* a, in
     if (kept) VTB_CUDA_TRY(cudaMemsetAsync(kept, 0xff, sizeof(int32_t), s));
     return launch_status();
 }
+
+// Solve with a matrix already factorised by vtb_herm_solve(mode 1): x = M^-1 x
+// in place (two triangular solves).  Used by the refinement sweeps.
+VTB_API int vtb_herm_potrs(const double* Mfac, int64_t ld, double* x, int K, void* work, int64_t work_bytes,
+                           void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && Mfac && x && work && ((uintptr_t)work & 255) == 0 && work_bytes >= 256);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    cudaStream_t s = as_stream(stream);
+    if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    int* info = reinterpret_cast<int*>(work);
+    if (cusolverDnZpotrs(h, CUBLAS_FILL_MODE_LOWER, K, 1, reinterpret_cast<const cuDoubleComplex*>(Mfac), (int)ld,
+                         reinterpret_cast<cuDoubleComplex*>(x), K, info) != CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    return launch_status();
+}

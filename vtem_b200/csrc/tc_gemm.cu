@@ -1,0 +1,316 @@
+// Tensor-core GEMM for sm_100a: C = alpha * A B^T with A (M x K) and B (N x K)
+// in bf16, K-major, accumulated in fp32 in tensor memory (tcgen05).
+//
+// Used with split-bf16 operands: a float64/float32 value x is written as
+// hi = bf16(x), lo = bf16(x - hi), and the operands are laid out along K as
+// A' = [A_hi | A_hi | A_lo], B' = [B_hi | B_lo | B_hi], so one accumulator
+// sums hi*hi + hi*lo + lo*hi (relative error ~2^-16 per product, fp32
+// accumulation), the "split BF16" products of the mixed-precision path.
+//
+// Structure (one 128 x BN output tile per CTA, 128 threads):
+//   thread 0   : TMA producer, 2-D tiled loads with 128-byte swizzle into a
+//                kStages-deep ring of shared-memory stages (no multicast);
+//   thread 32  : MMA issuer, tcgen05.mma.cta_group::1.kind::f16 (M=128,
+//                N=BN, K=16 per instruction), tcgen05.commit to free stages;
+//   warps 0..3 : epilogue, tcgen05.ld 32x32b of their 32 TMEM lanes (rows),
+//                scaled and stored as fp32 or fp64 with arbitrary strides.
+// Every mbarrier wait is bounded; a timeout sets *err and the CTA still
+// drains, releases its tensor memory and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "common.cuh"
+
+namespace vtb {
+
+constexpr int kTcBM = 128;
+constexpr int kTcBK = 64;   // 64 bf16 = 128 bytes = one swizzle row
+constexpr int kTcStages = 4;
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// bounded wait on the phase with the given parity; returns false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major operand tile, 128-byte swizzle: 8-row atoms of 1024 bytes.
+__device__ __forceinline__ uint64_t smem_desc_sw128(const void* base) {
+    const uint64_t addr = smem_u32(base);
+    return ((addr >> 4) & 0x3FFFull) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+template <int BN>
+struct TcIdesc {
+    // c_format f32 (bit 4), a/b bf16 (bits 7, 10), K-major A and B, N>>3 at 17, M>>4 at 24
+    static constexpr uint32_t value = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                      ((uint32_t)(kTcBM >> 4) << 24);
+};
+
+template <int BN>
+struct TcSmem {
+    __nv_bfloat16 a[kTcStages][kTcBM * kTcBK];
+    __nv_bfloat16 b[kTcStages][BN * kTcBK];
+    uint64_t full[kTcStages];
+    uint64_t empty[kTcStages];
+    uint64_t done;
+    uint32_t tmem_base;
+};
+
+template <int BN, typename OutT>
+__global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                         const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
+                                                         OutT* __restrict__ C, int64_t c_m, int64_t c_n, double alpha,
+                                                         int accumulate, int32_t* __restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // 1024-byte alignment of the stage buffers (the swizzle atoms)
+    TcSmem<BN>& sm = *reinterpret_cast<TcSmem<BN>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int m0 = blockIdx.y * kTcBM;
+    const int n0 = blockIdx.x * BN;
+    const int nk = K / kTcBK;
+    constexpr uint32_t kTmemCols = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+
+    if (tid == 0) {
+        for (int s = 0; s < kTcStages; ++s) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 1);
+        }
+        mbar_init(&sm.done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem_base)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = sm.tmem_base;
+    bool ok = true;
+
+    if (tid == 0) {
+        // producer
+        constexpr uint32_t bytes = (kTcBM + BN) * kTcBK * 2;
+        for (int kb = 0; kb < nk && ok; ++kb) {
+            const int s = kb % kTcStages;
+            if (kb >= kTcStages) ok = mbar_wait(&sm.empty[s], ((kb / kTcStages) + 1) & 1);
+            if (!ok) break;
+            mbar_expect_tx(&sm.full[s], bytes);
+            tma_load_2d(sm.a[s], &tmA, &sm.full[s], kb * kTcBK, m0);
+            tma_load_2d(sm.b[s], &tmB, &sm.full[s], kb * kTcBK, n0);
+        }
+        if (!ok) atomicExch(err, VTB_TIMEOUT);
+    } else if (tid == 32) {
+        // MMA issuer
+        constexpr uint32_t idesc = TcIdesc<BN>::value;
+        for (int kb = 0; kb < nk && ok; ++kb) {
+            const int s = kb % kTcStages;
+            ok = mbar_wait(&sm.full[s], (kb / kTcStages) & 1);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint64_t da = smem_desc_sw128(sm.a[s]);
+            const uint64_t db = smem_desc_sw128(sm.b[s]);
+#pragma unroll
+            for (int j = 0; j < kTcBK / 16; ++j) {
+                // advance 16 bf16 (32 bytes) along K inside the swizzle row
+                const uint64_t adv = (uint64_t)(j * 2);
+                const uint32_t acc = (kb > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                    "l"(da + adv), "l"(db + adv), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&sm.empty[s]))
+                         : "memory");
+        }
+        if (ok)
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&sm.done))
+                         : "memory");
+        else
+            atomicExch(err, VTB_TIMEOUT);
+    }
+    __syncwarp();
+    // epilogue: every warp waits for the accumulator (or gives up with the others)
+    bool have = (nk > 0) && mbar_wait(&sm.done, 0);
+    if (!have && nk > 0 && (tid & 31) == 0) atomicExch(err, VTB_TIMEOUT);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int row = m0 + warp * 32 + (tid & 31);
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+        uint32_t v[16];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (have && row < M) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int col = n0 + c0 + j;
+                if (col < N) {
+                    OutT* c = C + (int64_t)row * c_m + (int64_t)col * c_n;
+                    const double x = alpha * (double)__uint_as_float(v[j]);
+                    *c = accumulate ? (OutT)((double)*c + x) : (OutT)x;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------ split-bf16 operands
+// dst[r][seg*Kp + k] for seg in {0,1,2}: pattern 0 = [hi, hi, lo] (A side),
+// pattern 1 = [hi, lo, hi] (B side); zero padding for k >= K.
+template <typename InT>
+__global__ void split_bf16x3_kernel(const InT* __restrict__ src, int rows, int K, int64_t ld, int64_t ks,
+                                    double scale, int Kp, int pattern, __nv_bfloat16* __restrict__ dst) {
+    const int64_t total = (int64_t)rows * Kp;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / Kp), k = (int)(e % Kp);
+        const double x = k < K ? (double)src[(int64_t)r * ld + (int64_t)k * ks] * scale : 0.0;
+        const float xf = (float)x;
+        const __nv_bfloat16 hi = __float2bfloat16_rn(xf);
+        const __nv_bfloat16 lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
+        __nv_bfloat16* d = dst + (int64_t)r * 3 * Kp + k;
+        d[0] = hi;
+        d[Kp] = pattern == 0 ? hi : lo;
+        d[2 * Kp] = pattern == 0 ? lo : hi;
+    }
+}
+
+// ------------------------------------------------------------------ host side
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, []() {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// rows x K bf16 row-major (row pitch ld elements), box = box_rows x 64
+static int make_map(CUtensorMap* map, const void* base, int rows, int K, int64_t ld, int box_rows) {
+    auto fn = encode_fn();
+    if (!fn) return VTB_CUDA_ERR;
+    cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    cuuint32_t box[2] = {(cuuint32_t)kTcBK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? VTB_OK : VTB_BAD_ARG;
+}
+
+template <int BN, typename OutT>
+static int launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, OutT* C, int64_t c_m,
+                     int64_t c_n, double alpha, int accumulate, int32_t* err, cudaStream_t s) {
+    const size_t sm = sizeof(TcSmem<BN>) + 1024;
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [&]() {
+        attr = cudaFuncSetAttribute(tc_gemm_kernel<BN, OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    });
+    if (attr != cudaSuccess) {
+        set_last_cuda_error(attr);
+        return VTB_CUDA_ERR;
+    }
+    dim3 grid(ceil_div(N, BN), ceil_div(M, kTcBM));
+    tc_gemm_kernel<BN, OutT><<<grid, 128, sm, s>>>(ma, mb, M, N, K, C, c_m, c_n, alpha, accumulate, err);
+    return launch_status();
+}
+
+}  // namespace vtb
+
+using namespace vtb;
+
+VTB_API int vtb_split_bf16x3(const void* src, int src_f32, int rows, int K, int64_t ld, int64_t k_stride,
+                             double scale, int pattern, void* dst, void* stream) {
+    VTB_CHECK_ARG(rows >= 0 && K >= 0 && (pattern == 0 || pattern == 1));
+    if (rows == 0) return VTB_OK;
+    VTB_CHECK_ARG(src && dst && ((uintptr_t)dst & 15) == 0);
+    const int Kp = ceil_div(K, kTcBK) * kTcBK;
+    const int64_t total = (int64_t)rows * Kp;
+    const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 16 * kNumSMs);
+    if (src_f32)
+        split_bf16x3_kernel<float><<<blocks, 256, 0, as_stream(stream)>>>(
+            reinterpret_cast<const float*>(src), rows, K, ld, k_stride, scale, Kp, pattern,
+            reinterpret_cast<__nv_bfloat16*>(dst));
+    else
+        split_bf16x3_kernel<double><<<blocks, 256, 0, as_stream(stream)>>>(
+            reinterpret_cast<const double*>(src), rows, K, ld, k_stride, scale, Kp, pattern,
+            reinterpret_cast<__nv_bfloat16*>(dst));
+    return launch_status();
+}
+
+VTB_API int vtb_tc_gemm_bf16(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
+                             int out_f64, double alpha, int accumulate, int32_t* err, void* stream) {
+    VTB_CHECK_ARG(M >= 0 && N >= 0 && K > 0 && (K % kTcBK) == 0);
+    if (M == 0 || N == 0) return VTB_OK;
+    VTB_CHECK_ARG(A && B && C && err && ((uintptr_t)A & 15) == 0 && ((uintptr_t)B & 15) == 0);
+    VTB_CHECK_ARG(ceil_div(M, kTcBM) <= 65535);
+    CUtensorMap ma, mb;
+    int st = make_map(&ma, A, M, K, K, kTcBM);
+    if (st) return st;
+    constexpr int BN = 128;
+    st = make_map(&mb, B, N, K, K, BN);
+    if (st) return st;
+    cudaStream_t s = as_stream(stream);
+    if (out_f64)
+        return launch_tc<BN, double>(ma, mb, M, N, K, reinterpret_cast<double*>(C), c_m, c_n, alpha, accumulate, err, s);
+    return launch_tc<BN, float>(ma, mb, M, N, K, reinterpret_cast<float*>(C), c_m, c_n, alpha, accumulate, err, s);
+}

@@ -15,7 +15,11 @@ Solver choice: ``"eig"`` applies the reference's truncation rule to the
 eigenvalues of M (identical subspace); ``"chol"`` factorises M by Cholesky
 with float64 refinement and refuses (falls back to ``"eig"`` under
 ``"auto"``) when the pivots show a condition number beyond 1/rcond, i.e.
-when the pseudoinverse would truncate.
+when the pseudoinverse would truncate.  ``"mixed"`` builds M on the tensor
+cores from split-bf16 operands (fp32 accumulation, ~1e-5 relative), factors
+it, and recovers float64 accuracy with ``mixed_sweeps`` refinement sweeps
+against the exact float64 residual Phi^H (q - Phi a), which is applied
+through the Kronecker factors without ever forming M in float64.
 """
 from __future__ import annotations
 
@@ -45,8 +49,8 @@ def ellipse_storage_index(Mx, My):
 
 
 class CoeffDecoder(object):
-    def __init__(self, Ds, h_norm, Mx, My, Wt, Mt, decPx, decPy, Px1, Py1, rcond=1e-8, solver="auto", refine=2,
-                 device="cuda"):
+    def __init__(self, Ds, h_norm, Mx, My, Wt, Mt, decPx, decPy, Px1, Py1, rcond=1e-8, solver="auto", refine=0,
+                 device="cuda", mixed_sweeps=2):
         self.Mx, self.My, self.Mt = int(Mx), int(My), int(Mt)
         self.Wt = float(Wt)
         self.W = self.Wt / self.Mt
@@ -74,6 +78,29 @@ class CoeffDecoder(object):
         self._work = {}
         self.last_solver = None
         self.last_pivots = (0.0, 0.0)
+        self.mixed_sweeps = int(mixed_sweeps)
+        self.last_residual = None
+        if solver == "mixed":
+            self._init_mixed(device)
+
+    # ------------------------------------------------------------ mixed
+    def _init_mixed(self, device):
+        iu = np.triu_indices(self.Ks)
+        self.ps = torch.as_tensor(iu[0].astype(np.int32), device=device)
+        self.ps2 = torch.as_tensor(iu[1].astype(np.int32), device=device)
+        self.npairs = int(self.ps.numel())
+        from . import tc
+        self.Kp2 = tc.padded_k(2 * self.N)
+        self.L3 = torch.empty((2 * self.npairs, 3 * self.Kp2), dtype=torch.bfloat16, device=device)
+        call("vtb_coeff_lhs_split", dptr(self.d), self.N, self.Ks, dptr(self.ps), dptr(self.ps2), self.npairs,
+             dptr(self.L3), stream_ptr())
+        KK = self.Kt * self.Kt
+        self.R3 = torch.empty((KK, 3 * self.Kp2), dtype=torch.bfloat16, device=device)
+        self.C = torch.empty((2 * self.npairs, KK), dtype=torch.float32, device=device)
+        self.gres = torch.empty((self.N, self.Kt), dtype=C128, device=device)
+        self.r = torch.empty((self.K,), dtype=C128, device=device)
+        self.tc_err = torch.zeros(1, dtype=torch.int32, device=device)
+        self.potrs_work = torch.empty(256, dtype=torch.uint8, device=device)
 
     def _workspace(self, mode):
         if mode not in self._work:
@@ -100,8 +127,61 @@ class CoeffDecoder(object):
         s = stream_ptr()
         call("vtb_coeff_temporal_gram", dptr(tk1), dptr(tk2), dptr(ind), n, self.N, dptr(kap), dptr(dl), dptr(bi),
              dptr(self.norm), self.Mt, self.W, dptr(self.Wn), dptr(self.gn), s)
-        self._solve(s)
+        if self.solver == "mixed":
+            self._solve_mixed(s, (tk1, tk2, ind, n, kap, dl, bi))
+        else:
+            self._solve(s)
         return self.a
+
+    def _solve_mixed(self, s, spikes):
+        tk1, tk2, ind, n, kap, dl, bi = spikes
+        KK = self.Kt * self.Kt
+        call("vtb_coeff_rhs", dptr(self.d), self.N, self.Ks, dptr(self.gn), self.Kt, dptr(self.b), s)
+        call("vtb_coeff_wn_split", dptr(self.Wn), self.N, self.Kt, dptr(self.R3), s)
+        call("vtb_tc_gemm_bf16", dptr(self.L3), 2 * self.npairs, dptr(self.R3), KK, 3 * self.Kp2, dptr(self.C), KK, 1,
+             0, 1.0, 0, dptr(self.tc_err), s)
+        call("vtb_coeff_scatter", dptr(self.C), KK, dptr(self.ps), dptr(self.ps2), self.npairs, self.Kt,
+             dptr(self.M), self.K, s)
+        work = self._workspace(1)
+        piv = np.zeros(2, np.float64)
+        st = _abi.lib().vtb_herm_solve(dptr(self.M), self.K, dptr(self.b), dptr(self.a), self.K, self.rcond, 1, 0,
+                                      dptr(work), work.numel(), dptr(self.kept), piv.ctypes.data, s)
+        if st != 0:
+            # the pseudoinverse would truncate (or the factorisation failed): float64 path
+            self.solver = "auto"
+            try:
+                self._solve(s)
+            finally:
+                self.solver = "mixed"
+            self.last_solver = "mixed->" + self.last_solver
+            return
+        self.last_pivots = (float(piv[0]), float(piv[1]))
+        for _ in range(self.mixed_sweeps):
+            call("vtb_coeff_residual", dptr(tk1), dptr(tk2), dptr(ind), n, self.N, dptr(kap), dptr(dl), dptr(bi),
+                 dptr(self.norm), self.Mt, self.W, dptr(self.d), self.Ks, dptr(self.a), dptr(self.gres),
+                 dptr(self.r), s)
+            call("vtb_herm_potrs", dptr(self.M), self.K, dptr(self.r), self.K, dptr(self.potrs_work), 256, s)
+            call("vtb_zadd", dptr(self.a), dptr(self.r), self.K, s)
+        self.last_solver = "mixed"
+
+    def residual_norm(self, tk1, tk2, neuron_ind, kappa, delta, bias):
+        """||Phi^H (q - Phi a)|| / ||Phi^H q|| of the current coefficients."""
+        perm, tk1, tk2, ind = sort_by_neuron(tk1, tk2, neuron_ind)
+        dev = self.M.device
+        kap, dl, bi = (torch.as_tensor(np.asarray(x, np.float64), device=dev) if not isinstance(x, torch.Tensor)
+                       else x for x in (kappa, delta, bias))
+        gres = torch.empty((self.N, self.Kt), dtype=C128, device=dev)
+        r = torch.empty((self.K,), dtype=C128, device=dev)
+        s = stream_ptr()
+        call("vtb_coeff_residual", dptr(tk1), dptr(tk2), dptr(ind), int(tk1.numel()), self.N, dptr(kap), dptr(dl),
+             dptr(bi), dptr(self.norm), self.Mt, self.W, dptr(self.d), self.Ks, dptr(self.a), dptr(gres), dptr(r), s)
+        a0 = self.a.clone()
+        self.a.zero_()
+        r0 = torch.empty_like(r)
+        call("vtb_coeff_residual", dptr(tk1), dptr(tk2), dptr(ind), int(tk1.numel()), self.N, dptr(kap), dptr(dl),
+             dptr(bi), dptr(self.norm), self.Mt, self.W, dptr(self.d), self.Ks, dptr(self.a), dptr(gres), dptr(r0), s)
+        self.a.copy_(a0)
+        return float(r.norm() / r0.norm())
 
     def _build_M(self, s):
         call("vtb_coeff_gram", dptr(self.d), self.N, self.Ks, dptr(self.Wn), dptr(self.gn), self.Kt, dptr(self.M),
@@ -143,7 +223,7 @@ class CoeffDecoder(object):
         return self.synthesize(a, T, dt, out=out, out_dtype=out_dtype)
 
 
-def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=2):
+def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=0, mixed_sweeps=2):
     """A :class:`CoeffDecoder` on the output of ``vtdm.VTDM_prep``."""
     return CoeffDecoder(prep.Ds, prep.h_norm, prep.Mx, prep.My, Wt, Mt, prep.decPx, prep.decPy, prep.Px1, prep.Py1,
-                        rcond=rcond, solver=solver, refine=refine)
+                        rcond=rcond, solver=solver, refine=refine, mixed_sweeps=mixed_sweeps)

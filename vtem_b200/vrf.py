@@ -57,12 +57,14 @@ class vrf(object):
             y_start = -self.Syall / 2
         return x_start, y_start
 
-    def filter(self, V, out_layout="time"):
+    def filter(self, V, out_layout="time", precision="f64"):
         """Filter a video ``V`` (frames, Py, Px) with every RF.
 
         Returns the (frames, N) projection ``dx*dy*sum_p V RF`` as a CUDA
         tensor (vrf.py:264-292); ``out_layout="neuron"`` returns the same
         values laid out (N, frames), the layout the IAF scan reads fastest.
+        ``precision="bf16x3"`` (extension) computes it on the tensor cores
+        from split-bf16 operands (relative error ~1e-5) instead of float64.
         """
         V = _dev(V).reshape(V.shape[0], -1)
         F, P = V.shape
@@ -70,6 +72,12 @@ class vrf(object):
             raise ValueError("video frame size does not match the RF grid")
         rf = self._rf_full()
         N = rf.shape[0]
+        if precision == "bf16x3":
+            from . import tc
+            return tc.gemm_split_bf16(V, rf, alpha=self.dx * self.dy,
+                                      out_layout="row" if out_layout == "time" else "col")
+        if precision != "f64":
+            raise ValueError("precision must be 'f64' or 'bf16x3'")
         if out_layout == "time":
             out = torch.empty((F, N), dtype=F64, device=V.device)
             ts, ns = N, 1
@@ -285,6 +293,6 @@ class vrf_bank(object):
             setattr(self, k, getattr(b0, k))
         self.num_neurons = sum(b.num_neurons for b in self.banks)
 
-    def filter(self, V, out_layout="time"):
-        outs = [b.filter(V, out_layout) for b in self.banks]
+    def filter(self, V, out_layout="time", precision="f64"):
+        outs = [b.filter(V, out_layout, precision) for b in self.banks]
         return torch.cat(outs, dim=1 if out_layout == "time" else 0)
