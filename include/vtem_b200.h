@@ -214,8 +214,10 @@ int vtb_herm_solve_workspace(int K, int mode, int64_t* bytes);
 /* Solve M a = b for Hermitian PSD M (column-major, destroyed).  mode 0:
  * pseudoinverse keeping |eigenvalues| > rcond * max (the rule of
  * solve_eq_sym); mode 1: Cholesky + `refine` float64 refinement sweeps,
- * VTB_NOT_CONVERGED when the factorisation fails or its pivot spread shows
- * a condition number beyond 1/rcond.  pivots (HOST, may be NULL) receives
+ * VTB_NOT_CONVERGED when the factorisation fails or the spread of its
+ * squared pivots (only a lower bound of the condition number) reaches
+ * 1/rcond; mode 1 uses rcond only as that acceptance threshold, and callers
+ * pass one well below the pseudoinverse's own rcond.  pivots (HOST, may be NULL) receives
  * (min, max) eigenvalue (mode 0) or squared Cholesky pivot (mode 1).
  * Synchronises the stream. */
 int vtb_herm_solve(double* M, int64_t ld, const double* b, double* a, int K, double rcond, int mode, int refine,
@@ -252,6 +254,15 @@ int vtb_coeff_residual(const double* tk1, const double* tk2, const int32_t* ind,
 
 /* x = M^-1 x with M factorised in place by vtb_herm_solve(mode 1); work >= 256 bytes. */
 int vtb_herm_potrs(const double* Mfac, int64_t ld, double* x, int K, void* work, int64_t work_bytes, void* stream);
+
+/* Batched Cholesky solve of `batch` equally sized Hermitian systems (a group
+ * of clips with the same K): Mptrs/bptrs are device arrays of device
+ * pointers (column-major M factorised in place, b overwritten by the
+ * solution), infos[i] != 0 flags a clip whose factorisation failed or whose
+ * pivot spread exceeds 1/rcond (it then needs vtb_herm_solve mode 0).  The
+ * batched form of the per-window solve of vtem/vtdm.py:645-648. */
+int vtb_herm_chol_batched(double** Mptrs, int64_t ld, double** bptrs, int K, int batch, double rcond,
+                          int32_t* infos, int32_t* solve_info, void* stream);
 
 /* a += d (n complex). */
 int vtb_zadd(double* a, const double* d, int n, void* stream);

@@ -1,0 +1,68 @@
+"""Batched decoding of uneven clips (GPU): every clip of the batch equals its
+stand-alone decode, and the whole-clip device pairing equals the reference's
+spike reader."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import vtem_oracle as O
+from vtem_b200 import batch, ensemble_encode, fast, spike_store, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def problems():
+    clips = workloads.batch_clips(count=256, seed=2)
+    # short clips with few RFs; two (M, Mt) groups of three clips each form
+    # batched Cholesky groups, two more clips are groups of one
+    small = [c for c in clips if c.F <= 2500 and c.N <= 400]
+    keys = {}
+    for c in small:
+        keys.setdefault((c.Mx, c.Mt), []).append(c)
+    groups = sorted(keys.values(), key=len, reverse=True)
+    pick = groups[0][:3] + groups[1][:3] + [g[0] for g in groups[2:4]]
+    assert len(pick) == 8
+    return [batch.encode_clip_problem(c) for c in pick]
+
+
+def test_batch_equals_alone(problems):
+    bd = batch.BatchDecoder(problems, streams=4)
+    outs = [o.clone() for o in bd.run()]
+    torch.cuda.synchronize()
+    for p, u, db in zip(problems, outs, bd.decs):
+        d = fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver="auto")
+        ua = d.decode(p.tk1, p.tk2, p.ind, p.kappa, p.delta, p.bias, p.T, p.dt)
+        assert db.last_solver == d.last_solver
+        rel = ((u - ua).norm() / ua.norm()).item()
+        assert rel < 1e-11, rel
+        # and both equal the reference's pseudoinverse semantics (eigen path)
+        de = fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver="eig")
+        ue = de.decode(p.tk1, p.tk2, p.ind, p.kappa, p.delta, p.bias, p.T, p.dt)
+        assert ((u - ue).norm() / ue.norm()).item() < 1e-8
+    # a second run on the same decoder gives the same videos
+    outs2 = bd.run()
+    for a, b in zip(outs, outs2):
+        assert torch.equal(a, b)
+
+
+def test_device_pairs_match_reader():
+    rng = np.random.default_rng(9)
+    N, F = 12, 1234
+    L = rng.standard_normal((F, N)) * 0.3
+    e = ensemble_encode.IAF_encode(N, 1e-4)
+    e.load_parameters(h_kappa=np.ones(N), h_bias=np.full(N, 3.0), h_delta=np.full(N, 0.01),
+                      h_v0=rng.uniform(0, 0.01, N))
+    sp = e.encode_blocks(L, block_frames=101)
+    T = F * 1e-4
+    tk1, tk2, ind = spike_store.device_pairs(sp, T)
+    times, steps, cnt = sp.to_host_lists()
+    bc, bs = [], []
+    for b in range(len(range(0, F, 100))):
+        c = np.array([np.sum(s // 100 == b) for s in steps], np.int32)
+        bc.append(c)
+        bs.append(np.concatenate([t[s // 100 == b] for t, s in zip(times, steps)]))
+    r1, r2, ri = O.read_select_spikes(bc, bs, 100 * 1e-4, np.arange(N), [0.0, T])
+    assert np.array_equal(tk1.cpu().numpy(), r1)
+    assert np.array_equal(tk2.cpu().numpy(), r2)
+    assert np.array_equal(ind.cpu().numpy(), ri)

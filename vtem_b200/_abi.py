@@ -62,6 +62,7 @@ SIGNATURES = {
     "vtb_coeff_residual": [P, P, P, I, I, P, P, P, P, I, D, P, I, P, P, P, P],
     "vtb_herm_potrs": [P, L, P, I, P, L, P],
     "vtb_zadd": [P, P, I, P],
+    "vtb_herm_chol_batched": [P, L, P, I, I, D, P, P, P],
 }
 
 _lib = None

@@ -495,3 +495,63 @@ VTB_API int vtb_herm_potrs(const double* Mfac, int64_t ld, double* x, int K, voi
         return VTB_CUDA_ERR;
     return launch_status();
 }
+
+// Batched Cholesky solve of `batch` Hermitian K x K systems (one group of
+// equally sized clips): cusolverDnZpotrfBatched then ZpotrsBatched.  Mptrs
+// and bptrs are DEVICE arrays of device pointers (column-major M, lower
+// factor in place; b overwritten by the solution).  infos (device, batch
+// ints) receives each clip's status: the factorisation's own, or -1 when the
+// pivot spread shows a condition number beyond 1/rcond (the same test as
+// vtb_herm_solve mode 1); a nonzero entry means that clip needs the
+// eigen-pseudoinverse instead (its b is then meaningless).
+namespace vtb {
+__global__ void batched_pivot_check_kernel(double2* const* __restrict__ Mptrs, int64_t ld, int K, double rcond,
+                                           int32_t* __restrict__ infos) {
+    __shared__ double smin[32], smax[32];
+    const double2* L = Mptrs[blockIdx.x];
+    double mn = 1e308, mx = 0.0;
+    for (int i = threadIdx.x; i < K; i += blockDim.x) {
+        const double d = L[(int64_t)i * ld + i].x;
+        mn = fmin(mn, d * d);
+        mx = fmax(mx, d * d);
+    }
+    for (int o = 16; o; o >>= 1) {
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        smin[threadIdx.x >> 5] = mn;
+        smax[threadIdx.x >> 5] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+            mn = fmin(mn, smin[k]);
+            mx = fmax(mx, smax[k]);
+        }
+        if (infos[blockIdx.x] == 0 && (!(mn > 0.0) || mx / mn * rcond >= 1.0)) infos[blockIdx.x] = -1;
+    }
+}
+}  // namespace vtb
+
+VTB_API int vtb_herm_chol_batched(double** Mptrs, int64_t ld, double** bptrs, int K, int batch, double rcond,
+                                  int32_t* infos, int32_t* solve_info, void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && batch > 0 && Mptrs && bptrs && infos && solve_info);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    cudaStream_t s = as_stream(stream);
+    if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    if (cusolverDnZpotrfBatched(h, CUBLAS_FILL_MODE_LOWER, K, reinterpret_cast<cuDoubleComplex**>(Mptrs), (int)ld,
+                                infos, batch) != CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    batched_pivot_check_kernel<<<batch, 256, 0, s>>>(reinterpret_cast<double2* const*>(Mptrs), ld, K, rcond, infos);
+    int st = launch_status();
+    if (st) return st;
+    if (cusolverDnZpotrsBatched(h, CUBLAS_FILL_MODE_LOWER, K, 1, reinterpret_cast<cuDoubleComplex**>(Mptrs), (int)ld,
+                                reinterpret_cast<cuDoubleComplex**>(bptrs), K, solve_info, batch) !=
+        CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    return launch_status();
+}

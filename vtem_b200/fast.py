@@ -13,9 +13,11 @@ formed.  See csrc/coeff.cu for the kernels.
 
 Solver choice: ``"eig"`` applies the reference's truncation rule to the
 eigenvalues of M (identical subspace); ``"chol"`` factorises M by Cholesky
-with float64 refinement and refuses (falls back to ``"eig"`` under
-``"auto"``) when the pivots show a condition number beyond 1/rcond, i.e.
-when the pseudoinverse would truncate.  ``"mixed"`` builds M on the tensor
+and is used (under ``"auto"``) only when the pseudoinverse cannot truncate:
+the window must have at least K intervals, and the spread of the squared
+Cholesky pivots, a lower bound of the condition number that can
+underestimate it by orders of magnitude on badly sampled windows, must stay
+below 1 / (rcond * CHOL_MARGIN); otherwise the eigen-pseudoinverse runs.  ``"mixed"`` builds M on the tensor
 cores from split-bf16 operands (fp32 accumulation, ~1e-5 relative), factors
 it, and recovers float64 accuracy with ``mixed_sweeps`` refinement sweeps
 against the exact float64 residual Phi^H (q - Phi a), which is applied
@@ -32,6 +34,10 @@ from .dirichlet import sort_by_neuron
 
 F64 = torch.float64
 C128 = torch.complex128
+
+# Cholesky is trusted only when the pivot spread is this far below 1/rcond
+# (a window with pivot spread 1.6e5 had condition number 1.2e10).
+CHOL_MARGIN = 1e4
 
 
 def ellipse_storage_index(Mx, My):
@@ -130,7 +136,7 @@ class CoeffDecoder(object):
         if self.solver == "mixed":
             self._solve_mixed(s, (tk1, tk2, ind, n, kap, dl, bi))
         else:
-            self._solve(s)
+            self._solve(s, n)
         return self.a
 
     def _solve_mixed(self, s, spikes):
@@ -144,13 +150,14 @@ class CoeffDecoder(object):
              dptr(self.M), self.K, s)
         work = self._workspace(1)
         piv = np.zeros(2, np.float64)
-        st = _abi.lib().vtb_herm_solve(dptr(self.M), self.K, dptr(self.b), dptr(self.a), self.K, self.rcond, 1, 0,
-                                      dptr(work), work.numel(), dptr(self.kept), piv.ctypes.data, s)
+        st = 1 if n < self.K else _abi.lib().vtb_herm_solve(
+            dptr(self.M), self.K, dptr(self.b), dptr(self.a), self.K, self.rcond * CHOL_MARGIN, 1, 0, dptr(work),
+            work.numel(), dptr(self.kept), piv.ctypes.data, s)
         if st != 0:
             # the pseudoinverse would truncate (or the factorisation failed): float64 path
             self.solver = "auto"
             try:
-                self._solve(s)
+                self._solve(s, n)
             finally:
                 self.solver = "mixed"
             self.last_solver = "mixed->" + self.last_solver
@@ -187,13 +194,16 @@ class CoeffDecoder(object):
         call("vtb_coeff_gram", dptr(self.d), self.N, self.Ks, dptr(self.Wn), dptr(self.gn), self.Kt, dptr(self.M),
              self.K, dptr(self.b), s)
 
-    def _solve(self, s):
+    def _solve(self, s, n=None):
         modes = {"eig": [0], "chol": [1], "auto": [1, 0]}[self.solver]
+        if self.solver == "auto" and n is not None and n < self.K:
+            modes = [0]          # fewer intervals than unknowns: M is singular
         piv = np.zeros(2, np.float64)
         for i, mode in enumerate(modes):
             self._build_M(s)
             work = self._workspace(mode)
-            st = _abi.lib().vtb_herm_solve(dptr(self.M), self.K, dptr(self.b), dptr(self.a), self.K, self.rcond,
+            thr = self.rcond * CHOL_MARGIN if mode == 1 else self.rcond
+            st = _abi.lib().vtb_herm_solve(dptr(self.M), self.K, dptr(self.b), dptr(self.a), self.K, thr,
                                           mode, self.refine, dptr(work), work.numel(), dptr(self.kept),
                                           piv.ctypes.data, s)
             if st == 0:

@@ -240,3 +240,28 @@ class vtem_storage_read(object):
         tk2 = np.concatenate(tk2l) if tk2l else np.zeros(0)
         ind = np.concatenate(indl) if indl else np.zeros(0, np.int32)
         return tk1, tk2, ind, self.kappa, self.delta, self.bias, h_sigma
+
+
+def device_pairs(spikes, T, t0=0.0):
+    """Device-side form of ``read_select_spikes`` for a window that holds the
+    whole clip, [t0, T) with t0 = 0 (spike_store.py:279-351): absolute times
+    ``t + block * refresh_interval - t0`` (the reference's expression), then
+    consecutive pairs of every neuron, grouped by neuron.  ``spikes`` is the
+    :class:`~vtem_b200.ensemble_encode.DeviceSpikes` of one encode.  Only valid
+    when every spike lies inside (t0, T) (true for a whole-clip window), which
+    is checked."""
+    import torch
+    if t0 != 0.0:
+        raise ValueError("device_pairs covers the whole-clip window only")
+    N, cap = spikes.time.shape
+    bstep = spikes.block_frames - 1
+    R = spikes.refresh_interval
+    valid = torch.arange(cap, device=spikes.time.device)[None, :] < spikes.count[:, None]
+    blk = (spikes.step.long() // bstep).double()
+    t = spikes.time + blk * R - t0
+    tv = torch.where(valid, t, torch.full_like(t, 0.5 * T))
+    if bool(((tv <= 0) | (tv >= T)).any()):
+        raise ValueError("spikes outside the window: use read_select_spikes")
+    pv = valid[:, 1:]
+    nid = torch.arange(N, device=t.device, dtype=torch.int32)[:, None].expand(N, cap - 1)
+    return t[:, :-1][pv].contiguous(), t[:, 1:][pv].contiguous(), nid[pv].contiguous()

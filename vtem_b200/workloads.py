@@ -86,8 +86,11 @@ class Workload:
 
     def video(self, device="cpu"):
         """(F, Py, Px) float64 video, max|u| = 1."""
-        return bandlimited_video(self.coeffs, self.Mx, self.My, self.Mt, self.Wx, self.Wy, self.Wt, self.Px,
-                                 self.Py, self.F, self.dt, device) * self.scale
+        u = bandlimited_video(self.coeffs, self.Mx, self.My, self.Mt, self.Wx, self.Wy, self.Wt, self.Px,
+                              self.Py, self.F, self.dt, device)
+        if self.scale is None:
+            self.scale = 1.0 / float(u.abs().max())
+        return u * self.scale
 
 
 def ellipse_mask(Mx, My):
@@ -233,3 +236,40 @@ def gpu_scale(seed=0, rf_seed=1, frames=10000):
                  cs, np.ones(N), bias, delta, v0, 1e-8)
     w.scale = 1.0 / float(w.video().abs().max())
     return w
+
+
+def batch_clips(count=256, seed=2, rf_scale=1.0):
+    """Independent clips of uneven size for batched decoding: frame side in
+    {16, 32, 48, 64}, duration U(0.05, 0.5) s at dt=1e-4, Mt in {3..8},
+    Mx=My in {2..6}, RF count in {32..1024} (3/4 Gabor, 1/4 centre-surround
+    as in the GPU configuration), IAF b~U(2,4), delta~N(0.075, 0.0075) (~40 Hz).
+    The video scale (max|u| = 1) is set on the device at encode time."""
+    rng = np.random.default_rng(seed)
+    clips = []
+    for i in range(count):
+        side = int(rng.choice([16, 32, 48, 64]))
+        dur = float(rng.uniform(0.05, 0.5))
+        F = int(round(dur / 1e-4))
+        Mt = int(rng.integers(3, 9))
+        M = int(rng.integers(2, 7))
+        N = int(rng.integers(32, 1025))
+        Ng = max(1, (3 * N) // 4)
+        Nc = N - Ng
+        sub = np.random.default_rng(rng.integers(1 << 62))
+        a = bandlimited_coeffs(M, M, Mt, int(sub.integers(1 << 31)))
+        sig = sub.choice([0.05, 0.1, 0.2], Ng)
+        g = GaborParams(sig, sub.uniform(0, np.pi, Ng), sub.uniform(-0.5, 0.5, Ng), sub.uniform(-0.5, 0.5, Ng),
+                        (np.arange(Ng) % 2).astype(np.int32), 2.5, np.ones(Ng))
+        g.gain = _unit_gain(gabor_grid_values(g, side, side, gain=False), 1.0 / side, 1.0 / side)
+        cs = None
+        if Nc > 0:
+            c = sub.uniform(-0.5, 0.5, (Nc, 2))
+            cs = CSParams(np.ones(Nc), c[:, 0].copy(), c[:, 1].copy(), 0.05, 0.15, np.ones(Nc))
+            cs.gain = _unit_gain(cs_grid_values(cs, side, side, gain=False), 1.0 / side, 1.0 / side)
+        bias = sub.uniform(2, 4, N)
+        delta = np.abs(sub.normal(0.075, 0.0075, N))
+        v0 = sub.uniform(0, 1, N) * delta
+        w = Workload("batch%03d" % i, side, side, F, 1e-4, M, M, Mt, 2 * np.pi * M, 2 * np.pi * M, 2 * np.pi * 20, a,
+                     None, g, cs, np.ones(N), bias, delta, v0, 1e-8)
+        clips.append(w)
+    return clips
