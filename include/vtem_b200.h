@@ -252,6 +252,14 @@ int vtb_coeff_residual(const double* tk1, const double* tk2, const int32_t* ind,
                        const double* delta, const double* bias, const double* norm, int Mt, double W, const double* d,
                        int Ks, const double* a, double* gres, double* r, void* stream);
 
+/* a = Phi^H w for per-interval weights w (g: N x (2Mt+1) complex scratch):
+ * the reconstruction coefficients of a spike-space solution c = w, e.g.
+ * vtb_solve_eq_sym's pseudoinverse of the n x n Gram (vtem/dirichlet.py:165-189
+ * regrouped) when a window has fewer intervals than coefficients. */
+int vtb_coeff_from_spike_weights(const double* tk1, const double* tk2, const int32_t* ind, int nspk, int N,
+                                 const double* w, int Mt, double W, const double* d, int Ks, double* g, double* a,
+                                 void* stream);
+
 /* x = M^-1 x with M factorised in place by vtb_herm_solve(mode 1); work >= 256 bytes. */
 int vtb_herm_potrs(const double* Mfac, int64_t ld, double* x, int K, void* work, int64_t work_bytes, void* stream);
 

@@ -63,6 +63,7 @@ SIGNATURES = {
     "vtb_herm_potrs": [P, L, P, I, P, L, P],
     "vtb_zadd": [P, P, I, P],
     "vtb_herm_chol_batched": [P, L, P, I, I, D, P, P, P],
+    "vtb_coeff_from_spike_weights": [P, P, P, I, I, P, I, D, P, I, P, P, P],
 }
 
 _lib = None

@@ -50,8 +50,9 @@ class BatchDecoder(object):
         dev = self.decs[0].M.device
         self.streams = [torch.cuda.Stream(device=dev) for _ in range(streams)]
         self.groups = defaultdict(list)
-        for i, d in enumerate(self.decs):
-            self.groups[d.K].append(i)
+        for i, (p, d) in enumerate(zip(self.problems, self.decs)):
+            if int(p.tk1.numel()) >= d.K:
+                self.groups[d.K].append(i)
         self.ptrs = {}
         for K, idx in self.groups.items():
             mp = torch.as_tensor([self.decs[i].M.data_ptr() for i in idx], dtype=torch.int64, device=dev)
@@ -69,16 +70,22 @@ class BatchDecoder(object):
         start.record(main)
         for s in self.streams:
             s.wait_event(start)
-        # phase 1: per-clip Gram and right-hand side, round-robin over the streams
+        # phase 1: per-clip Gram and right-hand side, round-robin over the
+        # streams; clips with fewer intervals than coefficients are solved in
+        # the (smaller) spike space right away
         for i, (p, d) in enumerate(zip(self.problems, self.decs)):
             st = self.streams[i % len(self.streams)]
             with torch.cuda.stream(st):
                 s = stream_ptr()
                 n = int(p.tk1.numel())
+                if n < d.K:
+                    d._solve_spike_space(s, (p.tk1, p.tk2, p.ind, n, p.kappa, p.delta, p.bias))
+                    continue
                 call("vtb_coeff_temporal_gram", dptr(p.tk1), dptr(p.tk2), dptr(p.ind), n, d.N, dptr(p.kappa),
                      dptr(p.delta), dptr(p.bias), dptr(d.norm), d.Mt, d.W, dptr(d.Wn), dptr(d.gn), s)
                 d._build_M(s)
                 d.a.copy_(d.b)
+                d.last_solver = "chol-batched"
         joins = []
         for st in self.streams:
             e = torch.cuda.Event()
@@ -94,9 +101,6 @@ class BatchDecoder(object):
             rc = self.problems[idx[0]].rcond * fast.CHOL_MARGIN
             call("vtb_herm_chol_batched", mp.data_ptr(), K, bp.data_ptr(), K, len(idx), rc, dptr(infos), dptr(sinfo),
                  s)
-            for j, i in enumerate(idx):
-                if int(self.problems[i].tk1.numel()) < K:
-                    infos[j] = 1
         # clips whose factorisation failed: eigen-pseudoinverse alone (rare; needs a host check)
         for K, idx in self.groups.items():
             infos = self.ptrs[K][2]

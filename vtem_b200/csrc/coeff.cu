@@ -752,3 +752,52 @@ VTB_API int vtb_zadd(double* a, const double* d, int n, void* stream) {
                                                                  reinterpret_cast<const double2*>(d), n);
     return launch_status();
 }
+
+// g[n][m] = sum_{k in n} conj(T_k(m)) w_k for per-interval weights w (the
+// coefficients c of the spike-space solve): with vtb_coeff_rhs this gives
+// a = Phi^H c, the reconstruction coefficients of the reference's n x n
+// pseudoinverse solution (used when a window has fewer intervals than
+// coefficients, where the n x n system is the smaller one).
+namespace vtb {
+__global__ void __launch_bounds__(256) temporal_weighted_kernel(const double* __restrict__ tk1,
+                                                                const double* __restrict__ tk2,
+                                                                const int32_t* __restrict__ ind, int nspk,
+                                                                const double* __restrict__ wk, int Mt, double W,
+                                                                double2* __restrict__ g) {
+    const int Kt = 2 * Mt + 1;
+    const int nr = blockIdx.x;
+    const int lo = lb_i32(ind, nspk, nr), hi = lb_i32(ind, nspk, nr + 1);
+    for (int mi = threadIdx.x; mi < Kt; mi += blockDim.x) {
+        const int m = mi - Mt;
+        double gr = 0.0, gi = 0.0;
+        for (int k = lo; k < hi; ++k) {
+            const double a = tk1[k], b = tk2[k], d = b - a, w = wk[k];
+            if (m == 0) {
+                gr += d * w;
+            } else {
+                const double mw = m * W;
+                const double amp = (2.0 / mw) * sin(0.5 * mw * d);
+                double s, c;
+                sincos(mw * (0.5 * (a + b)), &s, &c);
+                gr += amp * c * w;   // conj(T) = amp e^{-j mW tbar}
+                gi -= amp * s * w;
+            }
+        }
+        g[(int64_t)nr * Kt + mi] = make_double2(gr, gi);
+    }
+}
+}  // namespace vtb
+
+VTB_API int vtb_coeff_from_spike_weights(const double* tk1, const double* tk2, const int32_t* ind, int nspk, int N,
+                                         const double* w, int Mt, double W, const double* d, int Ks, double* g,
+                                         double* a, void* stream) {
+    VTB_CHECK_ARG(nspk > 0 && N > 0 && Ks > 0 && Mt >= 1 && tk1 && tk2 && ind && w && d && g && a);
+    const int Kt = 2 * Mt + 1;
+    cudaStream_t s = as_stream(stream);
+    temporal_weighted_kernel<<<N, 64, 0, s>>>(tk1, tk2, ind, nspk, w, Mt, W, reinterpret_cast<double2*>(g));
+    int st = launch_status();
+    if (st) return st;
+    kron_rhs_kernel<<<Ks, 256, 0, s>>>(reinterpret_cast<const double2*>(d), N, Ks, reinterpret_cast<const double2*>(g),
+                                       Kt, reinterpret_cast<double2*>(a));
+    return launch_status();
+}

@@ -65,6 +65,8 @@ class CoeffDecoder(object):
         self.solver = solver
         self.refine = int(refine)
         Ds = Ds.to(device=device, dtype=C128).contiguous()
+        self.Ds = Ds
+        self._dsw = None
         self.N = Ds.shape[0]
         self.Kfull = Ds[0].numel()
         self.smap = torch.as_tensor(ellipse_storage_index(self.Mx, self.My), device=device)
@@ -133,11 +135,37 @@ class CoeffDecoder(object):
         s = stream_ptr()
         call("vtb_coeff_temporal_gram", dptr(tk1), dptr(tk2), dptr(ind), n, self.N, dptr(kap), dptr(dl), dptr(bi),
              dptr(self.norm), self.Mt, self.W, dptr(self.Wn), dptr(self.gn), s)
-        if self.solver == "mixed":
+        if self.solver in ("auto", "mixed") and n < self.K:
+            # fewer intervals than coefficients: the reference's n x n system is
+            # the smaller one (its pseudoinverse, then a = Phi^H c)
+            self._solve_spike_space(s, (tk1, tk2, ind, n, kap, dl, bi))
+        elif self.solver == "mixed":
             self._solve_mixed(s, (tk1, tk2, ind, n, kap, dl, bi))
         else:
             self._solve(s, n)
         return self.a
+
+    def _solve_spike_space(self, s, spikes):
+        tk1, tk2, ind, n, kap, dl, bi = spikes
+        dev = self.M.device
+        if self._dsw is None:
+            self._dsw = torch.empty((self.N, self.N), dtype=torch.float64, device=dev)
+            call("vtb_dsw", dptr(self.Ds), self.N, self.Kfull, dptr(self.norm), dptr(self._dsw), self.N, s)
+        G = torch.empty((n, n), dtype=torch.float64, device=dev)
+        q = torch.empty((n,), dtype=torch.float64, device=dev)
+        call("vtb_compute_q", dptr(tk1), dptr(tk2), dptr(ind), n, dptr(kap), dptr(dl), dptr(bi), dptr(self.norm),
+             dptr(q), s)
+        call("vtb_compute_G", dptr(tk1), dptr(tk2), dptr(ind), n, self.Wt, self.Mt, dptr(self._dsw), self.N, 0.0, 1,
+             dptr(G), n, s)
+        nb = np.zeros(1, np.int64)
+        call("vtb_solve_eq_sym_workspace", n, nb.ctypes.data)
+        work = torch.empty(int(nb[0]), dtype=torch.uint8, device=dev)
+        c = torch.empty((n,), dtype=torch.float64, device=dev)
+        call("vtb_solve_eq_sym", dptr(G), n, dptr(q), dptr(c), n, self.rcond, dptr(work), int(nb[0]),
+             dptr(self.kept), s)
+        call("vtb_coeff_from_spike_weights", dptr(tk1), dptr(tk2), dptr(ind), n, self.N, dptr(c), self.Mt, self.W,
+             dptr(self.d), self.Ks, dptr(self.gn), dptr(self.a), s)
+        self.last_solver = "spike-space eig"
 
     def _solve_mixed(self, s, spikes):
         tk1, tk2, ind, n, kap, dl, bi = spikes
