@@ -38,7 +38,8 @@ enum {
     VTB_TIMEOUT = 4,
     VTB_CUDA_ERR = 5,
     VTB_NOT_CONVERGED = 6,  /* eigensolver failed */
-    VTB_NO_DATA = 7         /* "no spikes to decode": dirichlet.py:39-40 */
+    VTB_NO_DATA = 7,        /* "no spikes to decode": dirichlet.py:39-40 */
+    VTB_BLOCK_LIMIT = 8     /* a frame block reached the per-call spike limit: ensemble_encode.py:163-164 */
 };
 
 int vtb_version(void);
@@ -111,14 +112,32 @@ int vtb_tc_gemm_bf16(const void* A, int M, const void* B, int N, int K, void* C,
  * spike_time/spike_step[n*cap + j] (block-relative time, global step index
  * of the interval that holds the crossing), spike_count[n] their number.
  * A neuron that fills its `cap` slots stops and *status is set to
- * VTB_OVERFLOW.  near_count (may be NULL) accumulates the threshold
- * comparisons whose margin is below near_eps. */
+ * VTB_OVERFLOW.  With block_rate > 0, a neuron whose spike count inside
+ * frame block b (starting at frame s = b*(block_frames-1)) reaches
+ * ceil(min(block_frames, F - s) / block_rate) sets *status to
+ * VTB_BLOCK_LIMIT: the reference's per-call buffer limit of each block's
+ * IAF_encode.encode (ensemble_encode.py:163-164, avg_rate = block_rate).
+ * near_count (may be NULL) accumulates the threshold comparisons whose
+ * margin is below near_eps. */
 int vtb_iaf_encode(const double* input, int64_t in_t_stride, int64_t in_n_stride, int N, int F,
                    int block_frames, double dt, const double* kappa, const double* bias, const double* delta,
                    double* v0, double* time_count, const double* randn, int64_t randn_block_stride,
                    int64_t randn_slot_stride, int64_t randn_n_stride, int randn_block_cap, const double* sigma,
                    double* delta_value, double* spike_time, int32_t* spike_step, int32_t* spike_count, int cap,
-                   unsigned long long* near_count, double near_eps, int32_t* status, void* stream);
+                   unsigned long long* near_count, double near_eps, int32_t* status, double block_rate,
+                   void* stream);
+
+/* Consecutive spike pairs of every neuron over the whole encoded clip, the
+ * window [t0, T) of read_select_spikes (vtem/spike_store.py:279-351) when it
+ * holds every spike: absolute time t = spike_time + (spike_step /
+ * (block_frames-1)) * refresh_interval - t0 (the reference's expression,
+ * same rounding), then tk1/tk2 = (t_j, t_{j+1}) and ind = n, grouped by
+ * neuron.  offsets[n] = sum over m < n of max(spike_count[m] - 1, 0) (the
+ * caller's exclusive scan).  *outside is set to 1 when a spike lies outside
+ * (0, T), in which case the caller must use the general reader. */
+int vtb_spike_pairs(const double* spike_time, const int32_t* spike_step, const int32_t* spike_count, int N, int cap,
+                    int block_frames, double refresh_interval, double t0, double T, const int64_t* offsets,
+                    double* tk1, double* tk2, int32_t* ind, int32_t* outside, void* stream);
 
 /* ------------------------------------------------------------ Dirichlet space */
 
@@ -271,6 +290,20 @@ int vtb_herm_potrs(const double* Mfac, int64_t ld, double* x, int K, void* work,
  * batched form of the per-window solve of vtem/vtdm.py:645-648. */
 int vtb_herm_chol_batched(double** Mptrs, int64_t ld, double** bptrs, int K, int batch, double rcond,
                           int32_t* infos, int32_t* solve_info, void* stream);
+
+/* Batched pseudoinverse solve of `batch` Hermitian systems of one size K by
+ * eigendecomposition (cuSOLVER XsyevBatched): a_z = V diag(1/w_i if
+ * |w_i| > rcond*max|w| else 0) V^H b_z, the truncation of solve_eq_sym
+ * (vtem/utils/linalg.py:591-631) applied per system, as vtb_herm_solve
+ * mode 0 does for one.  M holds the column-major matrices contiguously
+ * (stride K*K complex) and is overwritten; b and a are contiguous (stride K);
+ * kept[z] (optional) receives the number of kept eigenvalues and infos[z]
+ * the eigensolver's status per system.  The grouped counterpart of the
+ * per-window solve of vtem/vtdm.py:645-648 for systems whose pseudoinverse
+ * truncates. */
+int vtb_herm_pinv_batched_workspace(int K, int batch, int64_t* bytes);
+int vtb_herm_pinv_batched(double* M, const double* b, double* a, int K, int batch, double rcond, void* work,
+                          int64_t work_bytes, int32_t* kept, int32_t* infos, void* stream);
 
 /* a += d (n complex). */
 int vtb_zadd(double* a, const double* d, int n, void* stream);

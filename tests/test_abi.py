@@ -43,8 +43,10 @@ def test_bad_arguments_rejected_without_gpu():
     lib = _abi.lib()
     st = lib.vtb_compute_q(None, None, None, -1, None, None, None, None, None, None)
     assert st == _abi.VTB_BAD_ARG
+    st = lib.vtb_spike_pairs(None, None, None, 4, 10, 1, 0.01, 0.0, 1.0, None, None, None, None, None, None)
+    assert st == _abi.VTB_BAD_ARG
     st = lib.vtb_iaf_encode(None, 0, 0, 4, 10, 0, 1e-4, None, None, None, None, None, None, 0, 0, 0, 0, None,
-                            None, None, None, None, 1, None, 0.0, None, None)
+                            None, None, None, None, 1, None, 0.0, None, 0.0, None)
     assert st == _abi.VTB_BAD_ARG
 
 

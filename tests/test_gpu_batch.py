@@ -33,7 +33,7 @@ def test_batch_equals_alone(problems):
     for p, u, db in zip(problems, outs, bd.decs):
         d = fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver="auto")
         ua = d.decode(p.tk1, p.tk2, p.ind, p.kappa, p.delta, p.bias, p.T, p.dt)
-        assert db.last_solver == d.last_solver
+        assert {"chol-batched": "chol", "eig-batched": "eig"}.get(db.last_solver, db.last_solver) == d.last_solver
         rel = ((u - ua).norm() / ua.norm()).item()
         assert rel < 1e-11, rel
         # and both equal the reference's pseudoinverse semantics (eigen path)
@@ -66,3 +66,51 @@ def test_device_pairs_match_reader():
     assert np.array_equal(tk1.cpu().numpy(), r1)
     assert np.array_equal(tk2.cpu().numpy(), r2)
     assert np.array_equal(ind.cpu().numpy(), ri)
+
+
+def test_pinv_batched_equals_single():
+    """Batched eigen-pseudoinverse (rank-deficient and full-rank Hermitian
+    systems of one size) equals the single-system mode 0 solve."""
+    from vtem_b200._abi import call, dptr, lib, stream_ptr
+    rng = np.random.default_rng(11)
+    K, B = 72, 5
+    Ms, bs = [], []
+    for z in range(B):
+        r = K if z % 2 else K // 2 + 3 * z          # rank-deficient for even z
+        X = rng.standard_normal((K, r)) + 1j * rng.standard_normal((K, r))
+        Ms.append(X @ X.conj().T)
+        bs.append(rng.standard_normal(K) + 1j * rng.standard_normal(K))
+    dev = torch.device("cuda")
+    # column-major storage of Hermitian M is its conjugate transpose row-major
+    Mb = torch.as_tensor(np.stack([m.T for m in Ms]), device=dev).contiguous()
+    bb = torch.as_tensor(np.stack(bs), device=dev)
+    ab = torch.empty_like(bb)
+    nb = np.zeros(1, np.int64)
+    call("vtb_herm_pinv_batched_workspace", K, B, nb.ctypes.data)
+    work = torch.empty(int(nb[0]), dtype=torch.uint8, device=dev)
+    kept = torch.empty(B, dtype=torch.int32, device=dev)
+    infos = torch.empty(B, dtype=torch.int32, device=dev)
+    rcond = 1e-8
+    call("vtb_herm_pinv_batched", dptr(Mb), dptr(bb), dptr(ab), K, B, rcond, dptr(work), int(nb[0]), dptr(kept),
+         dptr(infos), stream_ptr())
+    torch.cuda.synchronize()
+    assert infos.cpu().tolist() == [0] * B
+    for z in range(B):
+        M1 = torch.as_tensor(Ms[z].T.copy(), device=dev)
+        a1 = torch.empty(K, dtype=torch.complex128, device=dev)
+        call("vtb_herm_solve_workspace", K, 0, nb.ctypes.data)
+        w1 = torch.empty(int(nb[0]), dtype=torch.uint8, device=dev)
+        k1 = torch.zeros(1, dtype=torch.int32, device=dev)
+        piv = np.zeros(2)
+        st = lib().vtb_herm_solve(dptr(M1), K, dptr(bb[z]), dptr(a1), K, rcond, 0, 0, dptr(w1), w1.numel(),
+                                  dptr(k1), piv.ctypes.data, stream_ptr())
+        assert st == 0
+        torch.cuda.synchronize()
+        assert int(kept[z]) == int(k1[0])
+        rel = ((ab[z] - a1).norm() / a1.norm()).item()
+        assert rel < 1e-10, (z, rel)
+        # the truncated solution in numpy's pseudoinverse semantics
+        w, V = np.linalg.eigh(Ms[z])
+        keep = np.abs(w) > rcond * np.abs(w).max()
+        ref = V[:, keep] @ ((V[:, keep].conj().T @ bs[z]) / w[keep])
+        assert np.linalg.norm(ab[z].cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-8

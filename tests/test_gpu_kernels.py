@@ -235,3 +235,56 @@ def test_bad_shapes_raise():
     with pytest.raises(TypeError):
         linalg.solve_eq_sym(torch.zeros((3, 3), dtype=torch.float32, device=dev),
                             torch.zeros((3, 1), dtype=torch.float64, device=dev))
+
+
+def _block_counts_oracle(L, dt, kap, bia, dl, v0, B):
+    r = O.vtem_encode(L, dt, kap, bia, dl, v0, block_frames=B, max_spike_per_block=100000)
+    return np.array(r.block_counts)          # (blocks, N)
+
+
+@pytest.mark.parametrize("rate_scale", [0.9, 1.1])
+def test_iaf_block_limit_matches_reference_rule(rate_scale):
+    """The kernel's per-block spike limit raises exactly when a block's count
+    reaches ceil(block length / avg_rate) (ensemble_encode.py:163-164)."""
+    rng = np.random.default_rng(5)
+    N, F, B, dt = 6, 1210, 101, 1e-4
+    L = rng.standard_normal((F, N)) * 0.2
+    kap, bia = np.ones(N), np.full(N, 2.0)
+    dl = np.full(N, 2.0 * dt * 3)            # about one spike every 3 samples
+    v0 = rng.uniform(0, 1, N) * dl
+    cnt = _block_counts_oracle(L, dt, kap, bia, dl, v0, B)
+    sizes = np.array([min(B, F - s) for s in range(0, F, B - 1)])[:cnt.shape[0]]
+    # an avg_rate whose limit sits just above / below the busiest block
+    worst = np.max(cnt.max(axis=1) / sizes)
+    avg_rate = 1.0 / (worst * rate_scale)
+    expect_raise = bool((cnt.max(axis=1) >= np.ceil(sizes / avg_rate)).any())
+    enc = _iaf(N, dt, kap, bia, dl, v0)
+    if expect_raise:
+        with pytest.raises(ValueError):
+            enc.encode_blocks(L, block_frames=B, avg_rate=avg_rate)
+    else:
+        sp = enc.encode_blocks(L, block_frames=B, avg_rate=avg_rate)
+        assert np.array_equal(ensemble_encode.spikes_per_block(sp, F), cnt)
+
+
+def test_iaf_small_buffer_retry_is_exact():
+    """A neuron that outgrows the first-try buffer triggers the full-buffer
+    rerun from the saved state: same spikes, same v0 as one full-buffer run."""
+    rng = np.random.default_rng(8)
+    N, F, B, dt = 40, 3000, 101, 1e-4
+    L = rng.standard_normal((F, N)) * 0.3
+    kap, bia = np.ones(N), np.full(N, 3.0)
+    dl = np.full(N, 0.02)
+    dl[7] = 3.0 * dt * 4                     # ~750 spikes: beyond the first-try buffer
+    v0 = rng.uniform(0, 1, N) * dl
+    small = 64 + -(-F // ensemble_encode.SMALL_CAP_STRIDE)
+    a = _iaf(N, dt, kap, bia, dl, v0)
+    sa = a.encode_blocks(L, block_frames=B)
+    b = _iaf(N, dt, kap, bia, dl, v0)
+    sb = b.encode_blocks(L, block_frames=B, cap=int(np.ceil(F / 0.1)))
+    ca, cb = sa.count.cpu().numpy(), sb.count.cpu().numpy()
+    assert ca[7] > small and np.array_equal(ca, cb)
+    ta, tb = sa.to_host_lists(), sb.to_host_lists()
+    for n in range(N):
+        assert np.array_equal(ta[0][n], tb[0][n]) and np.array_equal(ta[1][n], tb[1][n])
+    assert torch.equal(a.d_v0, b.d_v0)

@@ -21,6 +21,7 @@ VTB_TIMEOUT = 4
 VTB_CUDA_ERR = 5
 VTB_NOT_CONVERGED = 6
 VTB_NO_DATA = 7
+VTB_BLOCK_LIMIT = 8
 
 P = ctypes.c_void_p
 I = ctypes.c_int
@@ -35,7 +36,8 @@ SIGNATURES = {
     "vtb_rf_cs": [P, P, P, P, I, I, I, D, D, D, D, D, D, P, L, P],
     "vtb_rf_filter": [P, I, I, L, P, I, L, D, P, L, L, P],
     "vtb_gemm_f64": [I, I, I, P, L, L, P, L, L, P, L, L, D, D, P],
-    "vtb_iaf_encode": [P, L, L, I, I, I, D, P, P, P, P, P, P, L, L, L, I, P, P, P, P, P, I, P, D, P, P],
+    "vtb_iaf_encode": [P, L, L, I, I, I, D, P, P, P, P, P, P, L, L, L, I, P, P, P, P, P, I, P, D, P, D, P],
+    "vtb_spike_pairs": [P, P, P, I, I, I, D, D, D, P, P, P, P, P, P],
     "vtb_dirichlet_coeffs": [P, I, I, I, L, I, I, D, P, P],
     "vtb_dirich_space": [P, I, I, I, I, I, I, I, P, P],
     "vtb_dsw": [P, I, I, P, P, L, P],
@@ -64,6 +66,8 @@ SIGNATURES = {
     "vtb_zadd": [P, P, I, P],
     "vtb_herm_chol_batched": [P, L, P, I, I, D, P, P, P],
     "vtb_coeff_from_spike_weights": [P, P, P, I, I, P, I, D, P, I, P, P, P],
+    "vtb_herm_pinv_batched_workspace": [I, I, P],
+    "vtb_herm_pinv_batched": [P, P, P, I, I, D, P, L, P, P, P],
 }
 
 _lib = None

@@ -64,9 +64,12 @@ class BatchDecoder(object):
                      for p in self.problems]
         self.fallbacks = 0
 
-    def run(self):
+    def run(self, timing=False):
+        """Decode every clip; returns the list of videos.  With ``timing`` the
+        device time of the three phases is left in ``self.phase_ms`` (the
+        caller synchronises before reading it)."""
         main = torch.cuda.current_stream()
-        start = torch.cuda.Event()
+        start = torch.cuda.Event(enable_timing=timing)
         start.record(main)
         for s in self.streams:
             s.wait_event(start)
@@ -93,6 +96,8 @@ class BatchDecoder(object):
             joins.append(e)
         for e in joins:
             main.wait_event(e)
+        t1 = torch.cuda.Event(enable_timing=timing)
+        t1.record(main)
         # phase 2: one batched Cholesky per group of equally sized systems
         # (clips with fewer intervals than unknowns are singular: eigen path)
         s = stream_ptr()
@@ -101,19 +106,21 @@ class BatchDecoder(object):
             rc = self.problems[idx[0]].rcond * fast.CHOL_MARGIN
             call("vtb_herm_chol_batched", mp.data_ptr(), K, bp.data_ptr(), K, len(idx), rc, dptr(infos), dptr(sinfo),
                  s)
-        # clips whose factorisation failed: eigen-pseudoinverse alone (rare; needs a host check)
-        for K, idx in self.groups.items():
-            infos = self.ptrs[K][2]
-            bad = torch.nonzero(infos).flatten().tolist()
-            for j in bad:
-                i = idx[j]
-                d = self.decs[i]
-                d.solver = "eig"
-                d._solve(s)     # rebuilds M (the batched call factorised it in place)
-                d.solver = "chol"
-                d.last_solver = "eig"
-                self.fallbacks += 1
-        done = torch.cuda.Event()
+        # clips whose factorisation was refused (their pseudoinverse truncates):
+        # batched eigen-pseudoinverse per system size (one host check)
+        keys = list(self.groups)
+        if keys:
+            flags = torch.cat([self.ptrs[K][2] for K in keys]).ne(0).cpu().tolist()
+            bad_by_K, o = defaultdict(list), 0
+            for K in keys:
+                idx = self.groups[K]
+                bad_by_K[K] = [self.decs[idx[j]] for j in range(len(idx)) if flags[o + j]]
+                o += len(idx)
+            eig_infos = [fast.pinv_batched(ds) for ds in bad_by_K.values() if ds]
+            self.fallbacks = sum(len(ds) for ds in bad_by_K.values())
+            if eig_infos and int(torch.cat(eig_infos).ne(0).sum()) != 0:
+                raise fast.VtbError("vtb_herm_pinv_batched", fast.VTB_NOT_CONVERGED)
+        done = torch.cuda.Event(enable_timing=timing)
         done.record(main)
         # phase 3: synthesis
         for i, (p, d) in enumerate(zip(self.problems, self.decs)):
@@ -125,15 +132,28 @@ class BatchDecoder(object):
             e = torch.cuda.Event()
             e.record(st)
             main.wait_event(e)
+        if timing:
+            end = torch.cuda.Event(enable_timing=True)
+            end.record(main)
+            self._phase_events = (start, t1, done, end)
         return self.outs
 
+    @property
+    def phase_ms(self):
+        """(Gram/right-hand sides, solves, synthesis) device milliseconds of
+        the last ``run(timing=True)``."""
+        e = self._phase_events
+        return tuple(e[i].elapsed_time(e[i + 1]) for i in range(3))
 
-def encode_clip_problem(w, device="cuda", keep_video=False):
+
+def encode_clip_problem(w, device="cuda", keep_video=False, video=None, precision="f64"):
     """Encode workload ``w`` on the GPU (RF projection + IAF block loop) and
     prepare its coefficient-space decode: the ClipProblem of the clip (and
-    the video when ``keep_video``)."""
+    the video when ``keep_video``).  ``video`` (a device tensor, float64 or
+    float32) replaces the clip's generated video; ``precision`` is the RF
+    projection's ("f64", or "bf16x3" on the tensor cores)."""
     from . import ensemble_encode, spike_store, vrf, vtdm
-    V = w.video(device=device)
+    V = w.video(device=device) if video is None else video
     banks, dbanks = [], []
     rfSx, rfSy, rfPx, rfPy = vtdm.period_grid(w.Mx, w.My, w.Wx, w.Wy, w.dx, w.dy)
     if w.gabor is not None:
@@ -153,7 +173,7 @@ def encode_clip_problem(w, device="cuda", keep_video=False):
                               sigma_center=c.sigma_center, sigma_surround=c.sigma_surround, h_gain=c.gain)
             lst.append(b)
     bank = vrf.vrf_bank(banks) if len(banks) > 1 else banks[0]
-    L = bank.filter(V, out_layout="neuron")
+    L = bank.filter(V, out_layout="neuron", precision=precision)
     iaf = ensemble_encode.IAF_encode(w.N, w.dt)
     iaf.load_parameters(h_kappa=w.kappa, h_bias=w.bias, h_delta=w.delta, h_v0=w.v0)
     B = min(101, w.F + 1)

@@ -50,6 +50,7 @@ struct IafArgs {
     unsigned long long* near_count;
     double near_eps;
     int32_t* status;
+    double block_rate;       // > 0: per-block spike limit ceil(block length / block_rate)
 };
 
 constexpr int kIafWarps = 4;
@@ -82,6 +83,15 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
     const int steps = p.F - 1;
     const int bstep = p.block_frames - 1;
     int next_reset = bstep > 0 ? bstep : 0x7fffffff;
+    // spike limit of the current frame block (the reference's per-call buffer)
+    auto block_limit = [&](int b) -> int {
+        if (!(p.block_rate > 0.0)) return 0x7fffffff;
+        const int len = min(p.block_frames, p.F - b * bstep);
+        const double lim = ceil((double)len / p.block_rate);
+        return lim < 2147483647.0 ? (int)lim : 0x7fffffff;
+    };
+    int lim_block = block_limit(0);
+    bool limit_hit = false;
     const double* base = p.in + (int64_t)n * p.ns;
     auto ld = [&](int t) -> double { return t < p.F ? __ldg(base + (int64_t)t * p.ts) : 0.0; };
 
@@ -108,6 +118,7 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
                 cnt_block = 0;
                 ++block;
                 next_reset += bstep;
+                lim_block = block_limit(block);
             }
             const double area0 = s_area[w][j];
             const bool pos = (posmask >> j) & 1u;
@@ -139,6 +150,7 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
                     }
                     ++count;
                     ++cnt_block;
+                    limit_hit |= cnt_block >= lim_block;
                     area -= (delta - v0);
                     v0 = 0;
                     ddt -= remain;
@@ -174,6 +186,7 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
                     }
                     ++count;
                     ++cnt_block;
+                    limit_hit |= cnt_block >= lim_block;
                     v0 = 0;
                     ddt -= remain;
                     y1 = y1 + remain * a;
@@ -195,8 +208,41 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
         p.spike_count[n] = count;
         if (RT) p.delta_value[n] = delta;
         if (p.near_count && near) atomicAdd(p.near_count, near);
-        if (stop && p.status) atomicExch(p.status, VTB_OVERFLOW);
+        if (p.status) {
+            if (limit_hit) atomicExch(p.status, VTB_BLOCK_LIMIT);
+            else if (stop) atomicCAS(p.status, 0, VTB_OVERFLOW);
+        }
     }
+}
+
+// Consecutive pairs of each neuron's spikes, one warp per neuron (this file
+// is compiled without FMA contraction, so t rounds as the reference's
+// expression time + block * refresh - t0 does).
+__global__ void __launch_bounds__(256) spike_pairs_kernel(const double* __restrict__ time,
+                                                          const int32_t* __restrict__ step,
+                                                          const int32_t* __restrict__ count, int N, int cap,
+                                                          int bstep, double R, double t0, double T,
+                                                          const int64_t* __restrict__ offs, double* __restrict__ tk1,
+                                                          double* __restrict__ tk2, int32_t* __restrict__ ind,
+                                                          int32_t* __restrict__ outside) {
+    const int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (n >= N) return;
+    const int c = min(count[n], cap);
+    const int64_t o = offs[n];
+    bool bad = false;
+    for (int j = lane; j < c; j += 32) {
+        const int64_t k = (int64_t)n * cap + j;
+        const double blk = (double)(step[k] / bstep);
+        const double t = time[k] + blk * R - t0;
+        bad |= !(t > 0.0 && t < T);
+        if (j + 1 < c) {
+            tk1[o + j] = t;
+            ind[o + j] = n;
+        }
+        if (j > 0) tk2[o + j - 1] = t;
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicExch(outside, 1);
 }
 
 }  // namespace vtb
@@ -209,7 +255,8 @@ VTB_API int vtb_iaf_encode(const double* input, int64_t in_t_stride, int64_t in_
                            int64_t randn_block_stride, int64_t randn_slot_stride, int64_t randn_n_stride,
                            int randn_block_cap, const double* sigma, double* delta_value, double* spike_time,
                            int32_t* spike_step, int32_t* spike_count, int cap,
-                           unsigned long long* near_count, double near_eps, int32_t* status, void* stream) {
+                           unsigned long long* near_count, double near_eps, int32_t* status, double block_rate,
+                           void* stream) {
     VTB_CHECK_ARG(N >= 0 && F >= 0 && block_frames >= 1 && cap >= 1);
     if (N == 0) return VTB_OK;
     VTB_CHECK_ARG(input && kappa && bias && delta && v0 && time_count && spike_time && spike_step &&
@@ -217,11 +264,24 @@ VTB_API int vtb_iaf_encode(const double* input, int64_t in_t_stride, int64_t in_
     if (randn) VTB_CHECK_ARG(sigma && delta_value && randn_block_cap >= 1);
     IafArgs a{input, in_t_stride, in_n_stride, N, F, block_frames, dt, kappa, bias, delta, v0, time_count,
               randn, randn_block_stride, randn_slot_stride, randn_n_stride, randn_block_cap, sigma,
-              delta_value, spike_time, spike_step, spike_count, cap, near_count, near_eps, status};
+              delta_value, spike_time, spike_step, spike_count, cap, near_count, near_eps, status, block_rate};
     const int blocks = ceil_div(N, kIafWarps);
     if (randn)
         iaf_scan_kernel<true><<<blocks, kIafWarps * 32, 0, as_stream(stream)>>>(a);
     else
         iaf_scan_kernel<false><<<blocks, kIafWarps * 32, 0, as_stream(stream)>>>(a);
+    return launch_status();
+}
+
+VTB_API int vtb_spike_pairs(const double* spike_time, const int32_t* spike_step, const int32_t* spike_count, int N,
+                            int cap, int block_frames, double refresh_interval, double t0, double T,
+                            const int64_t* offsets, double* tk1, double* tk2, int32_t* ind, int32_t* outside,
+                            void* stream) {
+    VTB_CHECK_ARG(N >= 0 && cap >= 1 && block_frames >= 2);
+    if (N == 0) return VTB_OK;
+    VTB_CHECK_ARG(spike_time && spike_step && spike_count && offsets && outside);
+    spike_pairs_kernel<<<ceil_div((int64_t)N * 32, 256), 256, 0, as_stream(stream)>>>(
+        spike_time, spike_step, spike_count, N, cap, block_frames - 1, refresh_interval, t0, T, offsets, tk1, tk2,
+        ind, outside);
     return launch_status();
 }

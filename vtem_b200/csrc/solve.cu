@@ -232,12 +232,18 @@ VTB_API int vtb_rnn(const double* G, int64_t ld, const double* q, double* c, dou
 // overwritten.
 namespace vtb {
 
+// The GEMV and truncation kernels take a batch index from blockIdx.y (the
+// truncation from blockIdx.x): matrix z at V + z*mstride, vectors at
+// x/y + z*vstride (strides 0 for a single system).
 __global__ void zgemv_conj_rows_kernel(const double2* __restrict__ V, int64_t ld, const double2* __restrict__ x,
-                                       int n, double2* __restrict__ y) {
+                                       int n, double2* __restrict__ y, int64_t mstride = 0, int64_t vstride = 0) {
     // y[i] = sum_j conj(V[i*ld + j]) x[j]   (V row i = column i of the column-major eigenvector matrix)
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
+    V += blockIdx.y * mstride;
+    x += blockIdx.y * vstride;
+    y += blockIdx.y * vstride;
     const double2* row = V + (int64_t)warp * ld;
     double sr = 0.0, si = 0.0;
     for (int j = lane; j < n; j += 32) {
@@ -253,9 +259,14 @@ __global__ void zgemv_conj_rows_kernel(const double2* __restrict__ V, int64_t ld
 }
 
 __global__ void zgemv_cols_kernel(const double2* __restrict__ V, int64_t ld, const double2* __restrict__ x, int n,
-                                  double2* __restrict__ y, const double2* __restrict__ b, int subtract) {
+                                  double2* __restrict__ y, const double2* __restrict__ b, int subtract,
+                                  int64_t mstride = 0, int64_t vstride = 0) {
     // y[j] = sum_i V[i*ld + j] x[i]   (or b[j] - that when subtract)
     __shared__ double2 part[8][33];
+    V += blockIdx.y * mstride;
+    x += blockIdx.y * vstride;
+    y += blockIdx.y * vstride;
+    if (b) b += blockIdx.y * vstride;
     const int col = blockIdx.x * 32 + (threadIdx.x & 31);
     const int g = threadIdx.x >> 5;
     double sr = 0.0, si = 0.0;
@@ -281,6 +292,9 @@ __global__ void ztruncate_kernel(const double* __restrict__ w, double2* __restri
                                  int32_t* __restrict__ kept) {
     __shared__ double s0;
     __shared__ int cnt;
+    w += (int64_t)blockIdx.x * n;
+    qq += (int64_t)blockIdx.x * n;
+    if (kept) kept += blockIdx.x;
     if (threadIdx.x == 0) {
         s0 = fmax(fabs(w[0]), fabs(w[n - 1])) * rcond;
         cnt = 0;
@@ -553,5 +567,100 @@ VTB_API int vtb_herm_chol_batched(double** Mptrs, int64_t ld, double** bptrs, in
                                 reinterpret_cast<cuDoubleComplex**>(bptrs), K, solve_info, batch) !=
         CUSOLVER_STATUS_SUCCESS)
         return VTB_CUDA_ERR;
+    return launch_status();
+}
+
+// Batched pseudoinverse of Hermitian systems of one size K by
+// eigendecomposition (cuSOLVER XsyevBatched): for every matrix z,
+// a_z = V diag(1/w_i if |w_i| > rcond max|w| else 0) V^H b_z, the truncation
+// of vtb_herm_solve mode 0.  The matrices are contiguous, column-major, at
+// stride ld*K; b and a at stride K.  M is overwritten by the eigenvectors.
+namespace vtb {
+struct PinvBatchedWork {
+    double* w;        // batch*K eigenvalues
+    double2* v1;      // batch*K
+    int* info;        // batch
+    void* wk;
+    size_t wk_bytes;
+};
+static int pinv_batched_sizes(cusolverDnHandle_t h, int K, int64_t ld, int batch, size_t* db, size_t* hb) {
+    cusolverDnParams_t prm = solver_params();
+    if (!prm) return VTB_CUDA_ERR;
+    if (cusolverDnXsyevBatched_bufferSize(h, prm, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, K, CUDA_C_64F,
+                                          nullptr, ld, CUDA_R_64F, nullptr, CUDA_C_64F, db, hb, batch) !=
+        CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    return VTB_OK;
+}
+static int64_t pinv_batched_layout(int K, int batch, size_t db, char* base, PinvBatchedWork* pw) {
+    int64_t off = 0;
+    auto take = [&](int64_t bytes) {
+        int64_t o = off;
+        off = al256(off + bytes);
+        return o;
+    };
+    const int64_t ow = take((int64_t)batch * K * 8);
+    const int64_t o1 = take((int64_t)batch * K * 16);
+    const int64_t oi = take((int64_t)batch * 4);
+    const int64_t ok = take((int64_t)db);
+    if (pw && base) {
+        pw->w = reinterpret_cast<double*>(base + ow);
+        pw->v1 = reinterpret_cast<double2*>(base + o1);
+        pw->info = reinterpret_cast<int*>(base + oi);
+        pw->wk = base + ok;
+        pw->wk_bytes = db;
+    }
+    return off;
+}
+}  // namespace vtb
+
+VTB_API int vtb_herm_pinv_batched_workspace(int K, int batch, int64_t* bytes) {
+    VTB_CHECK_ARG(K > 0 && batch > 0 && bytes);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    size_t db = 0, hb = 0;
+    int st = pinv_batched_sizes(h, K, K, batch, &db, &hb);
+    if (st) return st;
+    *bytes = pinv_batched_layout(K, batch, db, nullptr, nullptr);
+    return VTB_OK;
+}
+
+VTB_API int vtb_herm_pinv_batched(double* M, const double* b, double* a, int K, int batch, double rcond, void* work,
+                                  int64_t work_bytes, int32_t* kept, int32_t* infos, void* stream) {
+    VTB_CHECK_ARG(K > 0 && batch > 0 && M && b && a && work && infos);
+    VTB_CHECK_ARG(((uintptr_t)work & 255) == 0 && ((uintptr_t)M & 15) == 0 && ((uintptr_t)b & 15) == 0 &&
+                  ((uintptr_t)a & 15) == 0);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    size_t db = 0, hb = 0;
+    int st = pinv_batched_sizes(h, K, K, batch, &db, &hb);
+    if (st) return st;
+    VTB_CHECK_ARG(work_bytes >= pinv_batched_layout(K, batch, db, nullptr, nullptr));
+    PinvBatchedWork pw;
+    pinv_batched_layout(K, batch, db, reinterpret_cast<char*>(work), &pw);
+    cudaStream_t s = as_stream(stream);
+    if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    void* hwk = hb ? malloc(hb) : nullptr;
+    if (hb && !hwk) return VTB_OOM;
+    const cusolverStatus_t cs = cusolverDnXsyevBatched(h, solver_params(), CUSOLVER_EIG_MODE_VECTOR,
+                                                       CUBLAS_FILL_MODE_LOWER, K, CUDA_C_64F, M, K, CUDA_R_64F, pw.w,
+                                                       CUDA_C_64F, pw.wk, pw.wk_bytes, hwk, hb, pw.info, batch);
+    // the host workspace must outlive the call's use of it
+    cudaError_t e1 = cudaStreamSynchronize(s);
+    free(hwk);
+    if (cs != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    VTB_CUDA_TRY(e1);
+    VTB_CUDA_TRY(cudaMemcpyAsync(infos, pw.info, (size_t)batch * 4, cudaMemcpyDeviceToDevice, s));
+    const double2* V = reinterpret_cast<const double2*>(M);
+    const int64_t ms = (int64_t)K * K;
+    zgemv_conj_rows_kernel<<<dim3(ceil_div((int64_t)K * 32, 256), batch), 256, 0, s>>>(
+        V, K, reinterpret_cast<const double2*>(b), K, pw.v1, ms, K);
+    ztruncate_kernel<<<batch, 1024, 0, s>>>(pw.w, pw.v1, K, rcond, kept);
+    zgemv_cols_kernel<<<dim3(ceil_div(K, 32), batch), 256, 0, s>>>(V, K, pw.v1, K, reinterpret_cast<double2*>(a),
+                                                                 nullptr, 0, ms, K);
     return launch_status();
 }

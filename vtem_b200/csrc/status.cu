@@ -32,6 +32,7 @@ VTB_API const char* vtb_status_string(int status) {
         case VTB_CUDA_ERR: return "CUDA error";
         case VTB_NOT_CONVERGED: return "solver did not converge";
         case VTB_NO_DATA: return "no spikes to decode";
+        case VTB_BLOCK_LIMIT: return "spikes in a frame block reached the buffer limit";
         default: return "unknown status";
     }
 }

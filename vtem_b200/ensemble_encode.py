@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from ._abi import VtbError, call, dptr, stream_ptr, VTB_OVERFLOW
+from ._abi import VTB_BLOCK_LIMIT, VTB_OVERFLOW, VtbError, call, dptr, stream_ptr
 
 F64 = torch.float64
 
@@ -25,6 +25,11 @@ def _dev(a, dtype=F64):
     if isinstance(a, torch.Tensor):
         return a.to(device="cuda", dtype=dtype).contiguous()
     return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+# First-try spike buffer of encode_blocks: one slot per this many samples
+# (plus 64) per neuron, i.e. up to 625 spikes/s at dt = 1e-4.
+SMALL_CAP_STRIDE = 16
 
 
 @dataclass
@@ -115,7 +120,7 @@ class IAF_encode(pop_encode):
 
     # ------------------------------------------------------------------
     def _launch(self, x, ts, ns, N, F, block_frames, cap, startbias, randn=None, block_cap=0,
-                near_eps=1e-12):
+                near_eps=1e-12, block_rate=0.0):
         sl = slice(startbias, startbias + N)
         st = torch.empty((N, cap), dtype=F64, device=x.device)
         ss = torch.empty((N, cap), dtype=torch.int32, device=x.device)
@@ -129,7 +134,8 @@ class IAF_encode(pop_encode):
             rargs = (None, 0, 0, 0, 0, None, None)
         call("vtb_iaf_encode", dptr(x), ts, ns, N, F, block_frames, self.dt, dptr(self.d_kappa[sl]),
              dptr(self.d_bias[sl]), dptr(self.d_delta[sl]), dptr(self.d_v0[sl]), dptr(self.d_time_count[sl]),
-             *rargs, dptr(st), dptr(ss), dptr(cnt), cap, dptr(near), near_eps, dptr(status), stream_ptr())
+             *rargs, dptr(st), dptr(ss), dptr(cnt), cap, dptr(near), near_eps, dptr(status), float(block_rate),
+             stream_ptr())
         return st, ss, cnt, near, status
 
     @staticmethod
@@ -168,31 +174,49 @@ class IAF_encode(pop_encode):
         ``block_frames`` frames stepping by block_frames-1, time_count reset
         at each block start, v0 carried.  Returns :class:`DeviceSpikes`; the
         reference's per-block overflow rule (ensemble_encode.py:163-164) is
-        checked when ``check``.  time_count is left as the reference leaves
-        it after its loop: reset to 0."""
+        checked by the kernel and raised here when ``check``.  time_count is
+        left as the reference leaves it after its loop: reset to 0.
+
+        The reference's buffer holds ceil(F / avg_rate) spikes per neuron.
+        With ``check`` (and no explicit ``cap``) the scan first runs with
+        room for one spike every SMALL_CAP_STRIDE samples and, only if a
+        neuron fills that, runs again from the saved state with the full
+        buffer; the spikes are the same either way."""
         x, ts, ns, N, F = self._as_input(neural_inputs, layout)
         if N != self.num_neurons:
             raise ValueError("input size should match number of neurons")
         nblocks = max(1, len(range(0, F, block_frames - 1)))
         block_cap = int(np.ceil(block_frames / avg_rate))
-        if cap is None:
-            cap = max(16, int(np.ceil(F / avg_rate)))
+        full = max(16, int(np.ceil(F / avg_rate)))
+        caps = [full] if cap is not None or not check else [min(full, 64 + -(-F // SMALL_CAP_STRIDE)), full]
+        if cap is not None:
+            caps = [int(cap)]
         randn = self._draw_randn(nblocks, block_cap, N)
-        st, ss, cnt, near, status = self._launch(x, ts, ns, N, F, block_frames, cap, 0, randn=randn,
-                                                 block_cap=block_cap, near_eps=near_eps)
+        saved = None
+        if len(caps) > 1:
+            saved = [self.d_v0.clone(), self.d_time_count.clone()]
+            if self.random_thresholds:
+                saved.append(self.d_delta_value.clone())
+        for i, c in enumerate(caps):
+            st, ss, cnt, near, status = self._launch(x, ts, ns, N, F, block_frames, c, 0, randn=randn,
+                                                     block_cap=block_cap, near_eps=near_eps,
+                                                     block_rate=avg_rate if check else 0.0)
+            if not check:
+                break
+            code = int(status.item())
+            if code == VTB_BLOCK_LIMIT or (code == VTB_OVERFLOW and i + 1 == len(caps)):
+                self.reset_timer()
+                raise ValueError("number of spikes exceeded the limit of buffer")
+            if code != VTB_OVERFLOW:
+                break
+            # a neuron filled the small buffer: rerun from the saved state
+            self.d_v0.copy_(saved[0])
+            self.d_time_count.copy_(saved[1])
+            if self.random_thresholds:
+                self.d_delta_value.copy_(saved[2])
         self.reset_timer()
         out = DeviceSpikes(st, ss, cnt, block_frames, self.dt)
-        if check:
-            if status.item() == VTB_OVERFLOW:
-                raise ValueError("number of spikes exceeded the limit of buffer")
-            out.near_threshold = int(near.item())
-            per_block = spikes_per_block(out, F)
-            lim = np.array([np.ceil(min(block_frames, F - s) / avg_rate)
-                            for s in range(0, F, block_frames - 1)])
-            if per_block.size and (per_block.max(axis=1) >= lim[:per_block.shape[0]]).any():
-                raise ValueError("number of spikes exceeded the limit of buffer")
-        else:
-            out.near_threshold = near
+        out.near_threshold = int(near.item()) if check else near
         return out
 
     def _draw_randn(self, nblocks, block_cap, N):

@@ -251,17 +251,22 @@ def device_pairs(spikes, T, t0=0.0):
     when every spike lies inside (t0, T) (true for a whole-clip window), which
     is checked."""
     import torch
+    from ._abi import call, dptr, stream_ptr
     if t0 != 0.0:
         raise ValueError("device_pairs covers the whole-clip window only")
     N, cap = spikes.time.shape
-    bstep = spikes.block_frames - 1
-    R = spikes.refresh_interval
-    valid = torch.arange(cap, device=spikes.time.device)[None, :] < spikes.count[:, None]
-    blk = (spikes.step.long() // bstep).double()
-    t = spikes.time + blk * R - t0
-    tv = torch.where(valid, t, torch.full_like(t, 0.5 * T))
-    if bool(((tv <= 0) | (tv >= T)).any()):
+    dev = spikes.time.device
+    c1 = (spikes.count.long() - 1).clamp_(min=0)
+    incl = torch.cumsum(c1, 0)
+    n = int(incl[-1]) if N else 0
+    offs = incl - c1
+    tk1 = torch.empty(n, dtype=torch.float64, device=dev)
+    tk2 = torch.empty(n, dtype=torch.float64, device=dev)
+    ind = torch.empty(n, dtype=torch.int32, device=dev)
+    outside = torch.zeros(1, dtype=torch.int32, device=dev)
+    call("vtb_spike_pairs", dptr(spikes.time), dptr(spikes.step), dptr(spikes.count), N, cap, spikes.block_frames,
+         spikes.refresh_interval, float(t0), float(T), dptr(offs), dptr(tk1) if n else None,
+         dptr(tk2) if n else None, dptr(ind) if n else None, dptr(outside), stream_ptr())
+    if int(outside.item()):
         raise ValueError("spikes outside the window: use read_select_spikes")
-    pv = valid[:, 1:]
-    nid = torch.arange(N, device=t.device, dtype=torch.int32)[:, None].expand(N, cap - 1)
-    return t[:, :-1][pv].contiguous(), t[:, 1:][pv].contiguous(), nid[pv].contiguous()
+    return tk1, tk2, ind

@@ -78,6 +78,8 @@ class vrf(object):
                                       out_layout="row" if out_layout == "time" else "col")
         if precision != "f64":
             raise ValueError("precision must be 'f64' or 'bf16x3'")
+        if V.dtype != F64:
+            V = V.to(F64)
         if out_layout == "time":
             out = torch.empty((F, N), dtype=F64, device=V.device)
             ts, ns = N, 1
