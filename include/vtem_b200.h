@@ -308,6 +308,52 @@ int vtb_herm_pinv_batched(double* M, const double* b, double* a, int K, int batc
 /* a += d (n complex). */
 int vtb_zadd(double* a, const double* d, int n, void* stream);
 
+/* ------------------------------------------------------------ real form
+ *
+ * A real video has Hermitian-symmetric coefficients (a[K-1-j] = conj a[j]
+ * for the index j = s*(2Mt+1) + m + Mt), and on those vectors the unitary map
+ * x_j = sqrt2 Re a_j, x_{h+1+j} = sqrt2 Im a_j (j < h = (K-1)/2), x_h = a_h
+ * turns the Hermitian M a = b into the real symmetric Mr x = br with the same
+ * eigenvalues: the solve of vtem/vtdm.py:645-648 (solve_eq_sym,
+ * vtem/utils/linalg.py:591-631) in a quarter of the complex arithmetic.
+ * Mr is written row-major and full (it is symmetric, so also column-major). */
+
+/* Mr (K x K, K = Ks*Kt, float32 or float64 when out_f64) from the tensor-core
+ * Gram output C of vtb_coeff_lhs_split/vtb_coeff_wn_split/vtb_tc_gemm_bf16
+ * (pairs s <= s' in row-major upper-triangular order). */
+int vtb_coeff_real_scatter(const float* C, int64_t ldc, int Ks, int Kt, void* Mr, int64_t ldr, int out_f64,
+                           void* stream);
+/* Mr from the complex column-major M of vtb_coeff_gram. */
+int vtb_coeff_realify(const double* M, int64_t ldm, int K, void* Mr, int64_t ldr, int out_f64, void* stream);
+/* br from b, and a (= or += when accumulate) from x; `batch` vectors at stride K. */
+int vtb_coeff_realify_vec(const double* b, int K, int batch, double* br, void* stream);
+int vtb_coeff_unrealify_vec(const double* x, int K, int batch, double* a, int accumulate, void* stream);
+
+/* Workspace bytes of the real symmetric solver: mode 0 eigen-pseudoinverse
+ * (float64), 1 float64 Cholesky, 2 float32 Cholesky. */
+int vtb_sym_workspace(int K, int mode, int64_t* bytes);
+/* Cholesky factorisation in place (lower factor), mode 1 (double M) or 2
+ * (float M).  Does not synchronise: flag (device int32) receives 0, 1 when
+ * the factorisation failed, or 2 when the spread of the squared pivots (a
+ * lower bound of cond(M)) times rcond reaches 1; pivots (device, 2 doubles,
+ * may be NULL) the (min, max) squared pivot. */
+int vtb_sym_factor(void* M, int64_t ld, int K, int mode, double rcond, void* work, int64_t work_bytes,
+                   int32_t* flag, double* pivots, void* stream);
+/* x = M^-1 x (float64 x) with a factor of vtb_sym_factor of the same mode. */
+int vtb_sym_potrs(const void* Mfac, int64_t ld, double* x, int K, int mode, void* work, int64_t work_bytes,
+                  void* stream);
+/* Pseudoinverse solve x = V diag(1/w if |w| > rcond*max|w| else 0) V^T b of
+ * a float64 symmetric M (destroyed), the rule of solve_eq_sym
+ * (vtem/utils/linalg.py:591-631, sq_Kernel :791-833).  kept (device) the
+ * number of kept eigenvalues; eig_range (HOST, may be NULL) the smallest
+ * and largest eigenvalue.  Synchronises the stream. */
+int vtb_sym_pinv(double* M, int64_t ld, const double* b, double* x, int K, double rcond, void* work,
+                 int64_t work_bytes, int32_t* kept, double* eig_range, void* stream);
+/* out (device) = ||dx|| / ||x||: the relative size of a refinement correction. */
+int vtb_norm_ratio(const double* dx, const double* x, int n, double* out, void* stream);
+/* y += x (n doubles). */
+int vtb_daxpy1(double* y, const double* x, int n, void* stream);
+
 /* vtb_coeff_synthesize without the caller's A_work buffer, for callers that
  * cannot allocate device memory (a plugin confined to another runtime's
  * memory pool, code that may only use a framework's allocator, replay inside

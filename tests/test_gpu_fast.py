@@ -130,3 +130,68 @@ def test_mixed_decoder_matches_float64(small_encoded):
     assert e0 < 1e-2, e0
     assert e < 1e-9, (e0, e)
     assert dec.residual_norm(tk1, tk2, ind, kap, dl, bia) < 1e-10
+
+
+def test_real_form_matches_hermitian_system():
+    """The real symmetric form (csrc/realsys.cu) of M a = b has the
+    eigenvalues of M and the same solution; the tensor-core Gram scattered
+    straight into the real form equals the float64 one to its precision."""
+    from vtem_b200._abi import call, dptr, stream_ptr
+    rng = np.random.default_rng(11)
+    # enough neurons and intervals that M is nonsingular (rank <= N * Kt)
+    N, n, Mx, My, Mt = 40, 1500, 3, 2, 3
+    W = 2 * np.pi * 20 / Mt
+    Ds = rng.standard_normal((N, 2 * My + 1, 2 * Mx + 1)) + 1j * rng.standard_normal((N, 2 * My + 1, 2 * Mx + 1))
+    Ds = 0.5 * (Ds + np.conj(Ds[:, ::-1, ::-1])) * O.ellipse_mask(Mx, My)[None]
+    tk1 = rng.uniform(0, 0.3, n)
+    tk2 = tk1 + rng.uniform(0.004, 0.03, n)
+    ind = np.sort(rng.integers(0, N, n)).astype(np.int32)
+    kap, dl, bia = (torch.as_tensor(x, device="cuda") for x in
+                    (rng.uniform(0.8, 1.2, N), rng.uniform(0.01, 0.05, N), rng.uniform(1, 3, N)))
+    dec = fast.CoeffDecoder(torch.as_tensor(Ds, device="cuda"), rng.uniform(0.5, 1.0, N), Mx, My, 2 * np.pi * 20,
+                            Mt, 8, 8, 8, 8, solver="mixed")
+    t1, t2, ii = (torch.as_tensor(x, device="cuda") for x in (tk1, tk2, ind))
+    s = stream_ptr()
+    K, KK = dec.K, dec.Kt * dec.Kt
+    call("vtb_coeff_temporal_gram", dptr(t1), dptr(t2), dptr(ii), n, N, dptr(kap), dptr(dl), dptr(bia),
+         dptr(dec.norm), Mt, W, dptr(dec.Wn), dptr(dec.gn), s)
+    dec._build_M(s)
+    call("vtb_coeff_realify", dptr(dec.M), K, K, dptr(dec.Mr), K, 1, s)
+    call("vtb_coeff_realify_vec", dptr(dec.b), K, 1, dptr(dec.br), s)
+    M = dec.M.cpu().numpy().T
+    b = dec.b.cpu().numpy()
+    Mr = dec.Mr.cpu().numpy()
+    br = dec.br.cpu().numpy()
+    assert np.abs(Mr - Mr.T).max() <= 1e-13 * np.abs(Mr).max()
+    ev_c = np.linalg.eigvalsh(M)
+    ev_r = np.linalg.eigvalsh(Mr)
+    assert np.abs(ev_c - ev_r).max() <= 1e-11 * ev_c.max()
+    a = np.linalg.solve(M, b)
+    x = torch.as_tensor(np.linalg.solve(Mr, br), device="cuda")
+    call("vtb_coeff_unrealify_vec", dptr(x), K, 1, dptr(dec.a), 0, s)
+    assert np.abs(dec.a.cpu().numpy() - a).max() <= 1e-9 * np.abs(a).max()
+    # tensor-core Gram -> real form in float32
+    call("vtb_coeff_wn_split", dptr(dec.Wn), N, dec.Kt, dptr(dec.R3), s)
+    call("vtb_tc_gemm_bf16", dptr(dec.L3), 2 * dec.npairs, dptr(dec.R3), KK, 3 * dec.Kp2, dptr(dec.C), KK, 1, 0, 1.0,
+         0, dec._stat_ptr(7), s)
+    call("vtb_coeff_real_scatter", dptr(dec.C), KK, dec.Ks, dec.Kt, dptr(dec.Mr32), K, 0, s)
+    M32 = dec.Mr32.double().cpu().numpy()
+    assert np.abs(M32 - Mr).max() <= 2e-5 * np.abs(Mr).max()
+    # float32 Cholesky + solve, then a float64 Cholesky solve, against numpy
+    work = dec._workspace(2)
+    dec.stat.zero_()
+    call("vtb_sym_factor", dptr(dec.Mr32), K, K, 2, 1e-12, dptr(work), work.numel(), dec._stat_ptr(0),
+         dec._stat_ptr(1), s)
+    x32 = torch.as_tensor(br, device="cuda")
+    call("vtb_sym_potrs", dptr(dec.Mr32), K, dptr(x32), K, 2, dptr(work), work.numel(), s)
+    flag, piv, _, tc_err = dec._read_stat()
+    assert flag == 0 and tc_err == 0 and piv[0] > 0
+    xr = np.linalg.solve(Mr, br)
+    assert np.linalg.norm(x32.cpu().numpy() - xr) <= 1e-2 * np.linalg.norm(xr)
+    w1 = dec._workspace(1)
+    dec.stat.zero_()
+    call("vtb_sym_factor", dptr(dec.Mr), K, K, 1, 1e-12, dptr(w1), w1.numel(), dec._stat_ptr(0), dec._stat_ptr(1), s)
+    x64 = torch.as_tensor(br, device="cuda")
+    call("vtb_sym_potrs", dptr(dec.Mr), K, dptr(x64), K, 1, dptr(w1), w1.numel(), s)
+    assert dec._read_stat()[0] == 0
+    assert np.linalg.norm(x64.cpu().numpy() - xr) <= 1e-9 * np.linalg.norm(xr)

@@ -68,6 +68,16 @@ SIGNATURES = {
     "vtb_coeff_from_spike_weights": [P, P, P, I, I, P, I, D, P, I, P, P, P],
     "vtb_herm_pinv_batched_workspace": [I, I, P],
     "vtb_herm_pinv_batched": [P, P, P, I, I, D, P, L, P, P, P],
+    "vtb_coeff_real_scatter": [P, L, I, I, P, L, I, P],
+    "vtb_coeff_realify": [P, L, I, P, L, I, P],
+    "vtb_coeff_realify_vec": [P, I, I, P, P],
+    "vtb_coeff_unrealify_vec": [P, I, I, P, I, P],
+    "vtb_sym_workspace": [I, I, P],
+    "vtb_sym_factor": [P, L, I, I, D, P, L, P, P, P],
+    "vtb_sym_potrs": [P, L, P, I, I, P, L, P],
+    "vtb_norm_ratio": [P, P, I, P, P],
+    "vtb_daxpy1": [P, P, I, P],
+    "vtb_sym_pinv": [P, L, P, P, I, D, P, L, P, P, P],
 }
 
 _lib = None

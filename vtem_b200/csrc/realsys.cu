@@ -1,0 +1,502 @@
+// Real form of the coefficient-space system.
+//
+// The video is real, so its Dirichlet coefficients are Hermitian-symmetric:
+// with the complex index j = s*Kt + (m + Mt) (s over the ascending storage
+// indices of the spatial ellipse, which is symmetric about its centre), the
+// mirrored index (-mx, -my, -m) is jb = K-1-j and a[jb] = conj(a[j]).  The
+// system M a = b keeps that symmetry (M[jb][kb] = conj(M[j][k]) because
+// Ds[n][-s] = conj(Ds[n][s]) for a real RF and T_k(-m) = conj(T_k(m))).  On
+// the Hermitian-symmetric vectors the unitary change of variables
+//     x_j = sqrt2 Re a_j,  x_{h+1+j} = sqrt2 Im a_j   (j < h = (K-1)/2),
+//     x_h = a_h                                       (the centre, real)
+// turns M a = b into a REAL symmetric K x K system Mr x = br with the same
+// eigenvalues (the reference's truncation rule picks the same subspace), at a
+// quarter of the arithmetic of the complex factorisation or eigensolver and
+// half the storage.  With A = M[j][k], B = M[j][kb] (parts p, q of the real
+// row/column indices; 0 = real part or centre, 1 = imaginary part):
+//     Mr = s_r s_c * { A.re + B.re,  -A.im + B.im,  A.im + B.im,  A.re - B.re }
+// for (p, q) = (0,0), (0,1), (1,0), (1,1), with s = 1/sqrt2 on the centre
+// row/column and 1 elsewhere.
+//
+// Factorisations (cuSOLVER, the vendor library for dense LAPACK; the decoder
+// keeps everything else in these kernels):
+//   mode 1: float64 Cholesky (dpotrf) of a float64 Mr;
+//   mode 2: float32 Cholesky (spotrf) of a float32 Mr (the mixed-precision
+//           path: the tensor-core Gram and a float32 factor, with float64
+//           refinement sweeps against the exact residual).
+// Neither synchronises: a device flag receives 1 when the factorisation fails
+// and 2 when the spread of the squared pivots, a lower bound of cond(Mr),
+// reaches 1/rcond (the pseudoinverse might then truncate), so that a
+// sequence of launches can be captured and checked once at its end.
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cstdlib>
+
+#include "common.cuh"
+
+namespace vtb {
+
+constexpr double kInvSqrt2 = 0.70710678118654752440;
+constexpr double kSqrt2 = 1.41421356237309504880;
+
+// complex index and part of real index R (h = (K-1)/2)
+__device__ __forceinline__ void real_split(int R, int h, int& j, int& part) {
+    if (R <= h) {
+        j = R;
+        part = 0;
+    } else {
+        j = R - h - 1;
+        part = 1;
+    }
+}
+
+__device__ __forceinline__ double real_entry(double2 A, double2 B, int p, int q) {
+    if (p == 0) return q == 0 ? A.x + B.x : -A.y + B.y;
+    return q == 0 ? A.y + B.y : A.x - B.x;
+}
+
+// Element M[j][k] of the Hermitian M from the tensor-core Gram output
+// C[(2p + part) * ldc + m*Kt + m'] (pairs p of spatial indices s <= s' in
+// row-major upper-triangular order).
+__device__ __forceinline__ double2 gram_from_pairs(const float* __restrict__ C, int64_t ldc, int Ks, int Kt, int j,
+                                                   int k) {
+    int s = j / Kt, m = j - s * Kt, s2 = k / Kt, m2 = k - s2 * Kt;
+    bool conj = false;
+    if (s > s2) {
+        int t = s; s = s2; s2 = t;
+        t = m; m = m2; m2 = t;
+        conj = true;
+    }
+    const int64_t p = (int64_t)s * Ks - (int64_t)s * (s - 1) / 2 + (s2 - s);
+    const int e = m * Kt + m2;
+    const double re = C[(2 * p) * ldc + e], im = C[(2 * p + 1) * ldc + e];
+    return make_double2(re, conj ? -im : im);
+}
+
+template <typename OutT>
+__global__ void __launch_bounds__(256) real_scatter_kernel(const float* __restrict__ C, int64_t ldc, int Ks, int Kt,
+                                                           OutT* __restrict__ Mr, int64_t ldr) {
+    const int K = Ks * Kt, h = (K - 1) / 2;
+    const int64_t total = (int64_t)K * K;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int R = (int)(i / K), Q = (int)(i - (int64_t)R * K);
+        int j, p, k, q;
+        real_split(R, h, j, p);
+        real_split(Q, h, k, q);
+        const double2 A = gram_from_pairs(C, ldc, Ks, Kt, j, k);
+        const double2 B = gram_from_pairs(C, ldc, Ks, Kt, j, K - 1 - k);
+        double v = real_entry(A, B, p, q);
+        if (R == h) v *= kInvSqrt2;
+        if (Q == h) v *= kInvSqrt2;
+        Mr[(int64_t)R * ldr + Q] = (OutT)v;
+    }
+}
+
+// From the complex column-major M (element (j, k) at k*ldm + j).
+template <typename OutT>
+__global__ void __launch_bounds__(256) realify_kernel(const double2* __restrict__ M, int64_t ldm, int K,
+                                                      OutT* __restrict__ Mr, int64_t ldr) {
+    const int h = (K - 1) / 2;
+    const int64_t total = (int64_t)K * K;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int R = (int)(i / K), Q = (int)(i - (int64_t)R * K);
+        int j, p, k, q;
+        real_split(R, h, j, p);
+        real_split(Q, h, k, q);
+        const double2 A = M[(int64_t)k * ldm + j];
+        const double2 B = M[(int64_t)(K - 1 - k) * ldm + j];
+        double v = real_entry(A, B, p, q);
+        if (R == h) v *= kInvSqrt2;
+        if (Q == h) v *= kInvSqrt2;
+        Mr[(int64_t)R * ldr + Q] = (OutT)v;
+    }
+}
+
+// br from the Hermitian-symmetric complex b (batch index from blockIdx.y)
+__global__ void realify_vec_kernel(const double2* __restrict__ b, int K, double* __restrict__ br) {
+    const int h = (K - 1) / 2;
+    b += (int64_t)blockIdx.y * K;
+    br += (int64_t)blockIdx.y * K;
+    for (int R = blockIdx.x * blockDim.x + threadIdx.x; R < K; R += gridDim.x * blockDim.x) {
+        if (R < h) br[R] = kSqrt2 * b[R].x;
+        else if (R == h) br[R] = b[h].x;
+        else br[R] = kSqrt2 * b[R - h - 1].y;
+    }
+}
+
+// a (=, or += when accumulate) the Hermitian-symmetric complex vector of x
+__global__ void unrealify_vec_kernel(const double* __restrict__ x, int K, double2* __restrict__ a, int accumulate) {
+    const int h = (K - 1) / 2;
+    x += (int64_t)blockIdx.y * K;
+    a += (int64_t)blockIdx.y * K;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j <= h; j += gridDim.x * blockDim.x) {
+        if (j == h) {
+            const double2 v = make_double2(x[h], 0.0);
+            a[h] = accumulate ? make_double2(a[h].x + v.x, a[h].y) : v;
+        } else {
+            const double2 v = make_double2(x[j] * kInvSqrt2, x[h + 1 + j] * kInvSqrt2);
+            const int jb = K - 1 - j;
+            if (accumulate) {
+                a[j] = make_double2(a[j].x + v.x, a[j].y + v.y);
+                a[jb] = make_double2(a[jb].x + v.x, a[jb].y - v.y);
+            } else {
+                a[j] = v;
+                a[jb] = make_double2(v.x, -v.y);
+            }
+        }
+    }
+}
+
+__global__ void f64_to_f32_kernel(const double* __restrict__ x, float* __restrict__ y, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = (float)x[i];
+}
+__global__ void f32_to_f64_kernel(const float* __restrict__ x, double* __restrict__ y, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = (double)x[i];
+}
+__global__ void daxpy1_kernel(double* __restrict__ y, const double* __restrict__ x, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] += x[i];
+}
+
+// Squared pivots of a Cholesky factor (diagonal of L, row-major or
+// column-major alike) -> piv[0] = min, piv[1] = max; flag = 1 if the
+// factorisation reported a failure, 2 if max/min * rcond >= 1.
+template <typename T>
+__global__ void pivot_flag_kernel(const T* __restrict__ L, int64_t ld, int K, const int* __restrict__ info,
+                                  double rcond, double* __restrict__ piv, int32_t* __restrict__ flag) {
+    __shared__ double smin[32], smax[32];
+    double mn = 1e308, mx = 0.0;
+    for (int i = threadIdx.x; i < K; i += blockDim.x) {
+        const double d = (double)L[(int64_t)i * ld + i];
+        mn = fmin(mn, d * d);
+        mx = fmax(mx, d * d);
+    }
+    for (int o = 16; o; o >>= 1) {
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        smin[threadIdx.x >> 5] = mn;
+        smax[threadIdx.x >> 5] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+            mn = fmin(mn, smin[k]);
+            mx = fmax(mx, smax[k]);
+        }
+        if (piv) {
+            piv[0] = mn;
+            piv[1] = mx;
+        }
+        int f = 0;
+        if (*info != 0 || !(mn > 0.0)) f = 1;
+        else if (mx / mn * rcond >= 1.0) f = 2;
+        *flag = f;
+    }
+}
+
+// out = ||dx|| / ||x|| (the relative size of a refinement correction)
+__global__ void norm_ratio_kernel(const double* __restrict__ dx, const double* __restrict__ x, int n,
+                                  double* __restrict__ out) {
+    __shared__ double sd[32], sx[32];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a = fma(dx[i], dx[i], a);
+        b = fma(x[i], x[i], b);
+    }
+    for (int o = 16; o; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sd[threadIdx.x >> 5] = a;
+        sx[threadIdx.x >> 5] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+            a += sd[k];
+            b += sx[k];
+        }
+        *out = sqrt(a) / fmax(sqrt(b), 1e-300);
+    }
+}
+
+static cusolverDnHandle_t real_solver_handle(int dev) {
+    static thread_local cusolverDnHandle_t h[64] = {nullptr};
+    if (dev < 0 || dev >= 64) return nullptr;
+    if (!h[dev]) {
+        if (cusolverDnCreate(&h[dev]) != CUSOLVER_STATUS_SUCCESS) h[dev] = nullptr;
+    }
+    return h[dev];
+}
+
+static int64_t al256r(int64_t x) { return (x + 255) & ~(int64_t)255; }
+
+// Workspace: [info 256][vec f32: K floats][w: K doubles][v1: K doubles][lapack work]
+struct RealWork {
+    int* info;
+    float* vf;
+    double* w;
+    double* v1;
+    void* wk;
+    int lwork;   // elements of the factorisation's / eigensolver's work type
+};
+
+static int real_lwork(cusolverDnHandle_t h, int K, int mode, int* lwork) {
+    cusolverStatus_t cs;
+    if (mode == 0)
+        cs = cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, K, nullptr, K, nullptr,
+                                         lwork);
+    else if (mode == 1)
+        cs = cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, K, nullptr, K, lwork);
+    else
+        cs = cusolverDnSpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, K, nullptr, K, lwork);
+    return cs == CUSOLVER_STATUS_SUCCESS ? VTB_OK : VTB_CUDA_ERR;
+}
+
+static int64_t real_layout(int K, int mode, int lwork, char* base, RealWork* rw) {
+    int64_t off = 0;
+    auto take = [&](int64_t bytes) {
+        const int64_t o = off;
+        off = al256r(off + bytes);
+        return o;
+    };
+    const int64_t oi = take(256);
+    const int64_t of = take((int64_t)K * 4);
+    const int64_t ow = take((int64_t)K * 8);
+    const int64_t o1 = take((int64_t)K * 8);
+    const int64_t ok = take((int64_t)lwork * (mode == 2 ? 4 : 8));
+    if (base && rw) {
+        rw->info = reinterpret_cast<int*>(base + oi);
+        rw->vf = reinterpret_cast<float*>(base + of);
+        rw->w = reinterpret_cast<double*>(base + ow);
+        rw->v1 = reinterpret_cast<double*>(base + o1);
+        rw->wk = base + ok;
+        rw->lwork = lwork;
+    }
+    return off;
+}
+
+static int real_setup(int K, int mode, void* work, int64_t work_bytes, void* stream, cusolverDnHandle_t* ph,
+                      RealWork* rw) {
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = real_solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    int lwork = 0;
+    int st = real_lwork(h, K, mode, &lwork);
+    if (st) return st;
+    const int64_t need = real_layout(K, mode, lwork, nullptr, nullptr);
+    VTB_CHECK_ARG(work_bytes >= need && ((uintptr_t)work & 255) == 0);
+    real_layout(K, mode, lwork, reinterpret_cast<char*>(work), rw);
+    if (cusolverDnSetStream(h, as_stream(stream)) != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    *ph = h;
+    return VTB_OK;
+}
+
+// x = V diag(1/w if |w| > rcond*max|w| else 0) V^T b for the column-major
+// eigenvector matrix V (columns = eigenvectors): v1 = V^T b (one warp per
+// column), truncation, x = V v1 (column blocks).
+__global__ void dgemv_t_kernel(const double* __restrict__ V, int64_t ld, const double* __restrict__ x, int n,
+                               double* __restrict__ y) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const double* col = V + (int64_t)warp * ld;
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) s = fma(col[i], x[i], s);
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[warp] = s;
+}
+
+__global__ void dgemv_n_kernel(const double* __restrict__ V, int64_t ld, const double* __restrict__ x, int n,
+                               double* __restrict__ y) {
+    __shared__ double part[8][33];
+    const int row = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int g = threadIdx.x >> 5;
+    double s = 0.0;
+    if (row < n)
+        for (int c = g; c < n; c += 8) s = fma(V[(int64_t)c * ld + row], x[c], s);
+    part[g][threadIdx.x & 31] = s;
+    __syncthreads();
+    if (g == 0 && row < n) {
+        double t = 0.0;
+        for (int k = 0; k < 8; ++k) t += part[k][threadIdx.x & 31];
+        y[row] = t;
+    }
+}
+
+__global__ void dtruncate_kernel(const double* __restrict__ w, double* __restrict__ v, int n, double rcond,
+                                 int32_t* __restrict__ kept) {
+    __shared__ double s0;
+    __shared__ int cnt;
+    if (threadIdx.x == 0) {
+        s0 = fmax(fabs(w[0]), fabs(w[n - 1])) * rcond;
+        cnt = 0;
+    }
+    __syncthreads();
+    int local = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double s = fabs(w[i]);
+        if (s > s0) {
+            v[i] = v[i] / s;
+            ++local;
+        } else {
+            v[i] = 0.0;
+        }
+    }
+    atomicAdd(&cnt, local);
+    __syncthreads();
+    if (threadIdx.x == 0 && kept) *kept = cnt;
+}
+
+}  // namespace vtb
+
+using namespace vtb;
+
+VTB_API int vtb_coeff_real_scatter(const float* C, int64_t ldc, int Ks, int Kt, void* Mr, int64_t ldr, int out_f64,
+                                   void* stream) {
+    VTB_CHECK_ARG(Ks > 0 && (Ks & 1) && Kt > 0 && (Kt & 1) && C && Mr && ldr >= (int64_t)Ks * Kt);
+    const int64_t total = (int64_t)Ks * Kt * Ks * Kt;
+    const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 16 * kNumSMs);
+    if (out_f64)
+        real_scatter_kernel<double><<<blocks, 256, 0, as_stream(stream)>>>(C, ldc, Ks, Kt,
+                                                                           reinterpret_cast<double*>(Mr), ldr);
+    else
+        real_scatter_kernel<float><<<blocks, 256, 0, as_stream(stream)>>>(C, ldc, Ks, Kt, reinterpret_cast<float*>(Mr),
+                                                                          ldr);
+    return launch_status();
+}
+
+VTB_API int vtb_coeff_realify(const double* M, int64_t ldm, int K, void* Mr, int64_t ldr, int out_f64, void* stream) {
+    VTB_CHECK_ARG(K > 0 && (K & 1) && M && Mr && ldm >= K && ldr >= K);
+    const int64_t total = (int64_t)K * K;
+    const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 16 * kNumSMs);
+    if (out_f64)
+        realify_kernel<double><<<blocks, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(M), ldm, K,
+                                                                      reinterpret_cast<double*>(Mr), ldr);
+    else
+        realify_kernel<float><<<blocks, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(M), ldm, K,
+                                                                     reinterpret_cast<float*>(Mr), ldr);
+    return launch_status();
+}
+
+VTB_API int vtb_coeff_realify_vec(const double* b, int K, int batch, double* br, void* stream) {
+    VTB_CHECK_ARG(K > 0 && (K & 1) && batch > 0 && b && br);
+    realify_vec_kernel<<<dim3(ceil_div(K, 256), batch), 256, 0, as_stream(stream)>>>(
+        reinterpret_cast<const double2*>(b), K, br);
+    return launch_status();
+}
+
+VTB_API int vtb_coeff_unrealify_vec(const double* x, int K, int batch, double* a, int accumulate, void* stream) {
+    VTB_CHECK_ARG(K > 0 && (K & 1) && batch > 0 && x && a);
+    unrealify_vec_kernel<<<dim3(ceil_div((K + 1) / 2, 256), batch), 256, 0, as_stream(stream)>>>(
+        x, K, reinterpret_cast<double2*>(a), accumulate);
+    return launch_status();
+}
+
+VTB_API int vtb_sym_workspace(int K, int mode, int64_t* bytes) {
+    VTB_CHECK_ARG(K > 0 && bytes && mode >= 0 && mode <= 2);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = real_solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    int lwork = 0;
+    int st = real_lwork(h, K, mode, &lwork);
+    if (st) return st;
+    *bytes = real_layout(K, mode, lwork, nullptr, nullptr);
+    return VTB_OK;
+}
+
+VTB_API int vtb_sym_factor(void* M, int64_t ld, int K, int mode, double rcond, void* work, int64_t work_bytes,
+                           int32_t* flag, double* pivots, void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && M && work && flag && (mode == 1 || mode == 2));
+    cusolverDnHandle_t h;
+    RealWork rw;
+    int st = real_setup(K, mode, work, work_bytes, stream, &h, &rw);
+    if (st) return st;
+    cudaStream_t s = as_stream(stream);
+    cusolverStatus_t cs;
+    if (mode == 1)
+        cs = cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, K, reinterpret_cast<double*>(M), (int)ld,
+                              reinterpret_cast<double*>(rw.wk), rw.lwork, rw.info);
+    else
+        cs = cusolverDnSpotrf(h, CUBLAS_FILL_MODE_LOWER, K, reinterpret_cast<float*>(M), (int)ld,
+                              reinterpret_cast<float*>(rw.wk), rw.lwork, rw.info);
+    if (cs != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    if (mode == 1)
+        pivot_flag_kernel<double><<<1, 1024, 0, s>>>(reinterpret_cast<const double*>(M), ld, K, rw.info, rcond, pivots,
+                                                     flag);
+    else
+        pivot_flag_kernel<float><<<1, 1024, 0, s>>>(reinterpret_cast<const float*>(M), ld, K, rw.info, rcond, pivots,
+                                                    flag);
+    return launch_status();
+}
+
+VTB_API int vtb_sym_potrs(const void* Mfac, int64_t ld, double* x, int K, int mode, void* work, int64_t work_bytes,
+                          void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && Mfac && x && work && (mode == 1 || mode == 2));
+    cusolverDnHandle_t h;
+    RealWork rw;
+    int st = real_setup(K, mode, work, work_bytes, stream, &h, &rw);
+    if (st) return st;
+    cudaStream_t s = as_stream(stream);
+    if (mode == 1) {
+        if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, K, 1, reinterpret_cast<const double*>(Mfac), (int)ld, x, K,
+                             rw.info) != CUSOLVER_STATUS_SUCCESS)
+            return VTB_CUDA_ERR;
+        return launch_status();
+    }
+    f64_to_f32_kernel<<<ceil_div(K, 256), 256, 0, s>>>(x, rw.vf, K);
+    if (cusolverDnSpotrs(h, CUBLAS_FILL_MODE_LOWER, K, 1, reinterpret_cast<const float*>(Mfac), (int)ld, rw.vf, K,
+                         rw.info) != CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    f32_to_f64_kernel<<<ceil_div(K, 256), 256, 0, s>>>(rw.vf, x, K);
+    return launch_status();
+}
+
+VTB_API int vtb_norm_ratio(const double* dx, const double* x, int n, double* out, void* stream) {
+    VTB_CHECK_ARG(n > 0 && dx && x && out);
+    norm_ratio_kernel<<<1, 1024, 0, as_stream(stream)>>>(dx, x, n, out);
+    return launch_status();
+}
+
+VTB_API int vtb_daxpy1(double* y, const double* x, int n, void* stream) {
+    VTB_CHECK_ARG(n >= 0 && y && x);
+    if (n == 0) return VTB_OK;
+    daxpy1_kernel<<<ceil_div(n, 256), 256, 0, as_stream(stream)>>>(y, x, n);
+    return launch_status();
+}
+
+VTB_API int vtb_sym_pinv(double* M, int64_t ld, const double* b, double* x, int K, double rcond, void* work,
+                         int64_t work_bytes, int32_t* kept, double* eig_range, void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && M && b && x && work);
+    cusolverDnHandle_t h;
+    RealWork rw;
+    int st = real_setup(K, 0, work, work_bytes, stream, &h, &rw);
+    if (st) return st;
+    cudaStream_t s = as_stream(stream);
+    if (cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, K, M, (int)ld, rw.w,
+                         reinterpret_cast<double*>(rw.wk), rw.lwork, rw.info) != CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    int hinfo = 0;
+    double ev[2] = {0, 0};
+    VTB_CUDA_TRY(cudaMemcpyAsync(&hinfo, rw.info, sizeof(int), cudaMemcpyDeviceToHost, s));
+    VTB_CUDA_TRY(cudaMemcpyAsync(&ev[0], rw.w, 8, cudaMemcpyDeviceToHost, s));
+    VTB_CUDA_TRY(cudaMemcpyAsync(&ev[1], rw.w + K - 1, 8, cudaMemcpyDeviceToHost, s));
+    VTB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hinfo != 0) return VTB_NOT_CONVERGED;
+    if (eig_range) {
+        eig_range[0] = ev[0];
+        eig_range[1] = ev[1];
+    }
+    dgemv_t_kernel<<<ceil_div((int64_t)K * 32, 256), 256, 0, s>>>(M, ld, b, K, rw.v1);
+    dtruncate_kernel<<<1, 1024, 0, s>>>(rw.w, rw.v1, K, rcond, kept);
+    dgemv_n_kernel<<<ceil_div(K, 32), 256, 0, s>>>(M, ld, rw.v1, K, x);
+    return launch_status();
+}

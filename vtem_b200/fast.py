@@ -11,17 +11,25 @@ number of spikes, built from per-neuron Kronecker factors on the device; the
 n x n Gram (5 GB at 25k spikes) and its O(n^3) eigendecomposition are never
 formed.  See csrc/coeff.cu for the kernels.
 
+Real form: the coefficients of a real video are Hermitian-symmetric, so the
+K x K Hermitian system is solved as the equivalent REAL symmetric system
+(csrc/realsys.cu; same eigenvalues, a quarter of the arithmetic).
+
 Solver choice: ``"eig"`` applies the reference's truncation rule to the
-eigenvalues of M (identical subspace); ``"chol"`` factorises M by Cholesky
-and is used (under ``"auto"``) only when the pseudoinverse cannot truncate:
-the window must have at least K intervals, and the spread of the squared
-Cholesky pivots, a lower bound of the condition number that can
+eigenvalues of M (identical subspace); ``"chol"`` factorises M by float64
+Cholesky and is used (under ``"auto"``) only when the pseudoinverse cannot
+truncate: the window must have at least K intervals, and the spread of the
+squared Cholesky pivots, a lower bound of the condition number that can
 underestimate it by orders of magnitude on badly sampled windows, must stay
-below 1 / (rcond * CHOL_MARGIN); otherwise the eigen-pseudoinverse runs.  ``"mixed"`` builds M on the tensor
-cores from split-bf16 operands (fp32 accumulation, ~1e-5 relative), factors
-it, and recovers float64 accuracy with ``mixed_sweeps`` refinement sweeps
-against the exact float64 residual Phi^H (q - Phi a), which is applied
-through the Kronecker factors without ever forming M in float64.
+below 1 / (rcond * CHOL_MARGIN); otherwise the eigen-pseudoinverse runs.
+``"mixed"`` builds M on the tensor cores from split-bf16 operands (fp32
+accumulation), factorises it by float32 Cholesky, and recovers float64
+accuracy with ``mixed_sweeps`` refinement sweeps against the exact float64
+residual Phi^H (q - Phi a), applied through the Kronecker factors without
+forming M in float64.  A mixed solve is accepted when the factorisation
+succeeds, its pivots pass the same test, and the refinement contracts
+(estimated remaining error below MIXED_TOL); otherwise the float64 path
+decodes the window.
 """
 from __future__ import annotations
 
@@ -38,6 +46,8 @@ C128 = torch.complex128
 # Cholesky is trusted only when the pivot spread is this far below 1/rcond
 # (a window with pivot spread 1.6e5 had condition number 1.2e10).
 CHOL_MARGIN = 1e4
+# accepted mixed solves: estimated relative error left after the last sweep
+MIXED_TOL = 1e-8
 
 
 def ellipse_storage_index(Mx, My):
@@ -83,6 +93,15 @@ class CoeffDecoder(object):
         self.b = torch.empty((self.K,), dtype=C128, device=device)
         self.a = torch.empty((self.K,), dtype=C128, device=device)
         self.kept = torch.zeros(1, dtype=torch.int32, device=device)
+        # real form: Mr (float64), right-hand side, iterate, correction
+        self.Mr = torch.empty((self.K, self.K), dtype=F64, device=device)
+        self.br = torch.empty((self.K,), dtype=F64, device=device)
+        self.xr = torch.empty((self.K,), dtype=F64, device=device)
+        self.rr = torch.empty((self.K,), dtype=F64, device=device)
+        # status words read once per solve: [flag (int32), min pivot^2, max
+        # pivot^2, sweep correction ratios x4, tensor-core error (int32)]
+        self.stat = torch.zeros(8, dtype=F64, device=device)
+        self.last_ratios = []
         self._work = {}
         self.last_solver = None
         self.last_pivots = (0.0, 0.0)
@@ -107,15 +126,25 @@ class CoeffDecoder(object):
         self.C = torch.empty((2 * self.npairs, KK), dtype=torch.float32, device=device)
         self.gres = torch.empty((self.N, self.Kt), dtype=C128, device=device)
         self.r = torch.empty((self.K,), dtype=C128, device=device)
-        self.tc_err = torch.zeros(1, dtype=torch.int32, device=device)
-        self.potrs_work = torch.empty(256, dtype=torch.uint8, device=device)
+        self.Mr32 = torch.empty((self.K, self.K), dtype=torch.float32, device=device)
 
     def _workspace(self, mode):
+        """Workspace of the real-form solver: mode 0 eigen, 1 float64
+        Cholesky, 2 float32 Cholesky."""
         if mode not in self._work:
             nb = np.zeros(1, np.int64)
-            call("vtb_herm_solve_workspace", self.K, mode, nb.ctypes.data)
+            call("vtb_sym_workspace", self.K, mode, nb.ctypes.data)
             self._work[mode] = torch.empty(int(nb[0]), dtype=torch.uint8, device=self.M.device)
         return self._work[mode]
+
+    def _stat_ptr(self, i):
+        return self.stat.data_ptr() + 8 * i
+
+    def _read_stat(self):
+        """(flag, (min, max) squared pivots, sweep ratios, tensor-core error): one synchronising read."""
+        h = self.stat.cpu().numpy()
+        iv = h.view(np.int32)
+        return int(iv[0]), (float(h[1]), float(h[2])), [float(x) for x in h[3:7]], int(iv[14])
 
     def coefficients(self, tk1, tk2, neuron_ind, kappa, delta, bias, assume_sorted=False):
         """Reconstruction coefficients a[(s, m)] (K complex) of one window.
@@ -169,20 +198,36 @@ class CoeffDecoder(object):
 
     def _solve_mixed(self, s, spikes):
         tk1, tk2, ind, n, kap, dl, bi = spikes
-        KK = self.Kt * self.Kt
+        K, KK = self.K, self.Kt * self.Kt
+        self.stat.zero_()
         call("vtb_coeff_rhs", dptr(self.d), self.N, self.Ks, dptr(self.gn), self.Kt, dptr(self.b), s)
+        call("vtb_coeff_realify_vec", dptr(self.b), K, 1, dptr(self.br), s)
         call("vtb_coeff_wn_split", dptr(self.Wn), self.N, self.Kt, dptr(self.R3), s)
         call("vtb_tc_gemm_bf16", dptr(self.L3), 2 * self.npairs, dptr(self.R3), KK, 3 * self.Kp2, dptr(self.C), KK, 1,
-             0, 1.0, 0, dptr(self.tc_err), s)
-        call("vtb_coeff_scatter", dptr(self.C), KK, dptr(self.ps), dptr(self.ps2), self.npairs, self.Kt,
-             dptr(self.M), self.K, s)
-        work = self._workspace(1)
-        piv = np.zeros(2, np.float64)
-        st = 1 if n < self.K else _abi.lib().vtb_herm_solve(
-            dptr(self.M), self.K, dptr(self.b), dptr(self.a), self.K, self.rcond * CHOL_MARGIN, 1, 0, dptr(work),
-            work.numel(), dptr(self.kept), piv.ctypes.data, s)
-        if st != 0:
-            # the pseudoinverse would truncate (or the factorisation failed): float64 path
+             0, 1.0, 0, self._stat_ptr(7), s)
+        call("vtb_coeff_real_scatter", dptr(self.C), KK, self.Ks, self.Kt, dptr(self.Mr32), K, 0, s)
+        work = self._workspace(2)
+        call("vtb_sym_factor", dptr(self.Mr32), K, K, 2, self.rcond * CHOL_MARGIN, dptr(work), work.numel(),
+             self._stat_ptr(0), self._stat_ptr(1), s)
+        self.xr.copy_(self.br)
+        call("vtb_sym_potrs", dptr(self.Mr32), K, dptr(self.xr), K, 2, dptr(work), work.numel(), s)
+        for i in range(self.mixed_sweeps):
+            call("vtb_coeff_unrealify_vec", dptr(self.xr), K, 1, dptr(self.a), 0, s)
+            call("vtb_coeff_residual", dptr(tk1), dptr(tk2), dptr(ind), n, self.N, dptr(kap), dptr(dl), dptr(bi),
+                 dptr(self.norm), self.Mt, self.W, dptr(self.d), self.Ks, dptr(self.a), dptr(self.gres),
+                 dptr(self.r), s)
+            call("vtb_coeff_realify_vec", dptr(self.r), K, 1, dptr(self.rr), s)
+            call("vtb_sym_potrs", dptr(self.Mr32), K, dptr(self.rr), K, 2, dptr(work), work.numel(), s)
+            call("vtb_norm_ratio", dptr(self.rr), dptr(self.xr), K, self._stat_ptr(3 + min(i, 3)), s)
+            call("vtb_daxpy1", dptr(self.xr), dptr(self.rr), K, s)
+        call("vtb_coeff_unrealify_vec", dptr(self.xr), K, 1, dptr(self.a), 0, s)
+        flag, piv, ratios, tc_err = self._read_stat()
+        self.last_pivots = piv
+        self.last_ratios = ratios[:min(self.mixed_sweeps, 4)]
+        if tc_err != 0:
+            raise VtbError("vtb_tc_gemm_bf16", tc_err)
+        if flag != 0 or not self._mixed_converged(self.last_ratios):
+            # the pseudoinverse might truncate, or float32 is not enough: float64 path
             self.solver = "auto"
             try:
                 self._solve(s, n)
@@ -190,14 +235,22 @@ class CoeffDecoder(object):
                 self.solver = "mixed"
             self.last_solver = "mixed->" + self.last_solver
             return
-        self.last_pivots = (float(piv[0]), float(piv[1]))
-        for _ in range(self.mixed_sweeps):
-            call("vtb_coeff_residual", dptr(tk1), dptr(tk2), dptr(ind), n, self.N, dptr(kap), dptr(dl), dptr(bi),
-                 dptr(self.norm), self.Mt, self.W, dptr(self.d), self.Ks, dptr(self.a), dptr(self.gres),
-                 dptr(self.r), s)
-            call("vtb_herm_potrs", dptr(self.M), self.K, dptr(self.r), self.K, dptr(self.potrs_work), 256, s)
-            call("vtb_zadd", dptr(self.a), dptr(self.r), self.K, s)
         self.last_solver = "mixed"
+
+    @staticmethod
+    def _mixed_converged(r):
+        """Refinement acceptance from the relative sizes of the sweeps'
+        corrections: with two or more sweeps the last must shrink and the
+        error it leaves (about r_last^2 / r_prev) must be below MIXED_TOL;
+        with one sweep its correction alone must be below sqrt(MIXED_TOL)."""
+        if not r:
+            return True
+        if len(r) == 1:
+            return r[0] <= MIXED_TOL ** 0.5
+        a, b = r[-2], r[-1]
+        if b == 0.0:
+            return True
+        return b < 0.5 * a and b * b / a <= MIXED_TOL
 
     def residual_norm(self, tk1, tk2, neuron_ind, kappa, delta, bias):
         """||Phi^H (q - Phi a)|| / ||Phi^H q|| of the current coefficients."""
@@ -223,24 +276,40 @@ class CoeffDecoder(object):
              self.K, dptr(self.b), s)
 
     def _solve(self, s, n=None):
+        """Float64 solve in real form: Cholesky (accepted by the pivot test)
+        and/or the eigen-pseudoinverse, by solver mode."""
         modes = {"eig": [0], "chol": [1], "auto": [1, 0]}[self.solver]
         if self.solver == "auto" and n is not None and n < self.K:
             modes = [0]          # fewer intervals than unknowns: M is singular
-        piv = np.zeros(2, np.float64)
+        K = self.K
+        self._build_M(s)
+        call("vtb_coeff_realify_vec", dptr(self.b), K, 1, dptr(self.br), s)
         for i, mode in enumerate(modes):
-            self._build_M(s)
+            call("vtb_coeff_realify", dptr(self.M), K, K, dptr(self.Mr), K, 1, s)
             work = self._workspace(mode)
-            thr = self.rcond * CHOL_MARGIN if mode == 1 else self.rcond
-            st = _abi.lib().vtb_herm_solve(dptr(self.M), self.K, dptr(self.b), dptr(self.a), self.K, thr,
-                                          mode, self.refine, dptr(work), work.numel(), dptr(self.kept),
-                                          piv.ctypes.data, s)
-            if st == 0:
-                self.last_solver = "eig" if mode == 0 else "chol"
-                self.last_pivots = (float(piv[0]), float(piv[1]))
-                return
-            if st == VTB_NOT_CONVERGED and i + 1 < len(modes):
-                continue
-            raise VtbError("vtb_herm_solve", st)
+            if mode == 1:
+                self.stat.zero_()
+                call("vtb_sym_factor", dptr(self.Mr), K, K, 1, self.rcond * CHOL_MARGIN, dptr(work), work.numel(),
+                     self._stat_ptr(0), self._stat_ptr(1), s)
+                self.xr.copy_(self.br)
+                call("vtb_sym_potrs", dptr(self.Mr), K, dptr(self.xr), K, 1, dptr(work), work.numel(), s)
+                flag, piv, _, _ = self._read_stat()
+                self.last_pivots = piv
+                if flag == 0:
+                    call("vtb_coeff_unrealify_vec", dptr(self.xr), K, 1, dptr(self.a), 0, s)
+                    self.kept.fill_(-1)
+                    self.last_solver = "chol"
+                    return
+                if i + 1 < len(modes):
+                    continue
+                raise VtbError("vtb_sym_factor", VTB_NOT_CONVERGED)
+            rng = np.zeros(2, np.float64)
+            call("vtb_sym_pinv", dptr(self.Mr), K, dptr(self.br), dptr(self.xr), K, self.rcond, dptr(work),
+                 work.numel(), dptr(self.kept), rng.ctypes.data, s)
+            call("vtb_coeff_unrealify_vec", dptr(self.xr), K, 1, dptr(self.a), 0, s)
+            self.last_pivots = (float(rng[0]), float(rng[1]))
+            self.last_solver = "eig"
+            return
 
     def synthesize(self, a, T, dt, t0=0.0, out=None, out_dtype=F64):
         """Video (Nt, decPy, decPx) at t = t0 + arange(0, T, dt)."""
