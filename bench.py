@@ -297,16 +297,20 @@ def run_ours(args, rank, world, local):
 
 
 def launches_mixed(dec):
-    # temporal_gram 1, rhs 1, wn split 1, tc gemm 1, scatter 1, herm_solve(chol): chol_pivots 1,
-    # per sweep: residual 2 + zadd 1, synthesis 2 (cuSOLVER's own kernels not counted)
-    return 1 + 1 + 1 + 1 + 1 + 1 + 3 * dec.mixed_sweeps + 2
+    # own kernels per decode: temporal_gram, rhs, realify_vec, wn split, tc gemm, real scatter (6); factor:
+    # pivot test + diagonal-block inverses (2); solve: f64<->f32 conversions (2); per sweep: unrealify,
+    # residual (2), realify_vec, conversions (2), norm ratio, axpy (8); final unrealify (1); synthesis (2).
+    # cuSOLVER's own kernels (spotrf, strsv) are not counted.
+    return 6 + 2 + 2 + 8 * dec.mixed_sweeps + 1 + 2
 
 
 def run_batch(args, rank, world, local):
     """Many-clip workload: 256 independent clips of uneven size (seed 2).
-    One step = decoding every clip of the batch (grouped batched Cholesky,
-    multi-stream Gram and synthesis); compared with decoding the same clips
-    one after another with the single-clip decoder."""
+    One step = decoding every clip of the batch (mixed precision: grouped
+    float32 Cholesky, batched triangular solves and float64 refinement,
+    replayed as CUDA graphs; float64 fallbacks on worker threads); compared
+    with decoding the same clips one after another with the stand-alone
+    decoders (mixed, and float64)."""
     import torch
     from vtem_b200 import batch, fast, workloads
     torch.cuda.set_device(local)
@@ -318,48 +322,58 @@ def run_batch(args, rank, world, local):
     t_setup = time.perf_counter() - t0
     voxels = sum(p.voxels for p in probs)
     spikes = [int(p.tk1.numel()) for p in probs]
-    bd = batch.BatchDecoder(probs, streams=8)
+    bd = batch.BatchDecoder(probs, streams=8, sweeps=args.sweeps, graph=True)
     flush = torch.zeros(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
     for _ in range(args.warmup):
         bd.run()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
-    ms = 0.0
+    ms, phases = 0.0, np.zeros(3)
     for _ in range(args.steps):
         flush_l2(flush)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        bd.run()
+        bd.run(timing=True)
         e1.record()
         torch.cuda.synchronize()
         ms += e0.elapsed_time(e1)
+        phases += np.array(bd.phase_ms)
     clk = clocks.stop()
-    # one clip at a time, same decoders and solver rule
-    singles = [fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver="auto") for p in probs]
-    for d, p in zip(singles, probs):
-        d.decode(p.tk1, p.tk2, p.ind, p.kappa, p.delta, p.bias, p.T, p.dt, assume_sorted=True)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for d, p in zip(singles, probs):
-        d.decode(p.tk1, p.tk2, p.ind, p.kappa, p.delta, p.bias, p.T, p.dt, assume_sorted=True)
-    e1.record()
-    torch.cuda.synchronize()
-    seq_ms = e0.elapsed_time(e1)
-    solvers = {}
-    for d in bd.decs:
-        solvers[d.last_solver] = solvers.get(d.last_solver, 0) + 1
+    solvers = bd.solver_counts()
+
+    def sequential(solver):
+        decs = [fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver=solver, mixed_sweeps=args.sweeps)
+                for p in probs]
+        for d, p in zip(decs, probs):
+            d.decode(p.tk1, p.tk2, p.ind, p.kappa, p.delta, p.bias, p.T, p.dt, assume_sorted=True)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for d, p in zip(decs, probs):
+            d.decode(p.tk1, p.tk2, p.ind, p.kappa, p.delta, p.bias, p.T, p.dt, assume_sorted=True)
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    seq_mixed = sequential("mixed")
+    seq_f64 = sequential("auto")
+    step_ms = ms / args.steps
     return {"metric": METRIC + " [batch of %d clips]" % len(probs), "value": voxels * args.steps / (ms / 1e3),
-            "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (split-bf16 tensor-core Gram, f32 Cholesky, f64 refinement)",
             "data": "synthetic (seeded Dirichlet-bandlimited video)",
             "config": {"workload": "batch: %d clips, side {16,32,48,64}, 0.05-0.5 s, Mt 3..8, M 2..6, 32..1024 RFs"
                                    % len(probs), "voxels_per_step": voxels, "spikes_min": min(spikes),
                        "spikes_max": max(spikes), "groups": len(bd.groups), "solvers": solvers,
-                       "setup_s": t_setup},
-            "sequential_ms": seq_ms, "batched_speedup": seq_ms / (ms / args.steps),
+                       "cuda_graphs": bd.use_graph, "graph_error": bd.graph_error, "setup_s": t_setup,
+                       "l2": "256 MB flush between steps"},
+            "phases_ms": {"grouped_mixed_solve": phases[0] / args.steps, "f64_fallbacks": phases[1] / args.steps,
+                          "synthesis": phases[2] / args.steps},
+            "sequential_ms": {"mixed": seq_mixed, "f64": seq_f64},
+            "batched_speedup": {"vs_sequential_mixed": seq_mixed / step_ms, "vs_sequential_f64": seq_f64 / step_ms},
             "clips_per_s": len(probs) * args.steps / (ms / 1e3), "clocks": clk}
 
 

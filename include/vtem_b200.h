@@ -349,6 +349,30 @@ int vtb_sym_potrs(const void* Mfac, int64_t ld, double* x, int K, int mode, void
  * and largest eigenvalue.  Synchronises the stream. */
 int vtb_sym_pinv(double* M, int64_t ld, const double* b, double* x, int K, double rcond, void* work,
                  int64_t work_bytes, int32_t* kept, double* eig_range, void* stream);
+/* Batched float32 Cholesky of `batch` real systems of one size K (a group of
+ * clips with equal K; Mptrs: device array of device pointers, factorised in
+ * place): cusolverDnSpotrfBatched, the pivot test of vtb_sym_factor per
+ * system (flags[z]; pivots, may be NULL, 2 doubles per system) and the
+ * inverses of each factor's 32 x 32 diagonal blocks for vtb_sym_potrs_batched
+ * (Dinv + z * vtb_sym_dinv_floats(K)).  infos (device) receives cuSOLVER's
+ * per-system status.  The grouped counterpart of the per-window solve of
+ * vtem/vtdm.py:645-648.  Does not synchronise. */
+int vtb_sym_factor_batched(float** Mptrs, int64_t ld, int K, int batch, double rcond, float* Dinv, int32_t* infos,
+                           int32_t* flags, double* pivots, void* stream);
+int64_t vtb_sym_dinv_floats(int K);
+
+/* One system of vtb_sym_potrs_batched: x = L^-T L^-1 x (x float64, in place). */
+typedef struct vtb_trsv_desc {
+    const float* L;     /* float32 factor, column-major, leading dimension ld */
+    const float* Dinv;  /* inverses of its 32 x 32 diagonal blocks */
+    double* x;
+    int64_t ld;
+    int32_t K;
+    int32_t pad;
+} vtb_trsv_desc;
+/* Solves of `batch` systems (descs: device array), one CTA each; Kmax >= every K. */
+int vtb_sym_potrs_batched(const void* descs, int batch, int Kmax, void* stream);
+
 /* out (device) = ||dx|| / ||x||: the relative size of a refinement correction. */
 int vtb_norm_ratio(const double* dx, const double* x, int n, double* out, void* stream);
 /* y += x (n doubles). */

@@ -78,6 +78,9 @@ SIGNATURES = {
     "vtb_norm_ratio": [P, P, I, P, P],
     "vtb_daxpy1": [P, P, I, P],
     "vtb_sym_pinv": [P, L, P, P, I, D, P, L, P, P, P],
+    "vtb_sym_factor_batched": [P, L, I, I, D, P, P, P, P, P],
+    "vtb_sym_potrs_batched": [P, I, I, P],
+    "vtb_sym_dinv_floats": [I],  # restype int64, set in lib()
 }
 
 _lib = None
@@ -104,6 +107,8 @@ def lib():
             f = getattr(l, name)
             f.argtypes = args
             f.restype = ctypes.c_int
+        l.vtb_sym_dinv_floats.argtypes = [ctypes.c_int]
+        l.vtb_sym_dinv_floats.restype = ctypes.c_int64
         l.vtb_status_string.argtypes = [ctypes.c_int]
         l.vtb_status_string.restype = ctypes.c_char_p
         _lib = l

@@ -1,30 +1,45 @@
 """Batched decoding of many independent clips (uneven durations, RF counts
-and Dirichlet orders) on one GPU.
+and Dirichlet orders) on one GPU, in mixed precision.
 
-Each clip is decoded in the Dirichlet coefficient space exactly as
-:class:`vtem_b200.fast.CoeffDecoder` does alone; the batch only changes how
-the work is scheduled:
+Each clip is decoded in the Dirichlet coefficient space as
+:class:`vtem_b200.fast.CoeffDecoder` (``solver="mixed"``) does alone; the
+batch changes how the work is scheduled:
 
-* per-clip temporal/Kronecker Gram kernels are issued round-robin on
-  several CUDA streams so that small clips overlap on the device;
-* clips whose systems have the same size K are factorised and solved by one
-  batched Cholesky call per group (``vtb_herm_chol_batched``), the grouped
-  counterpart of the reference's per-window ``solve_eq_sym``
-  (vtem/vtdm.py:645-648); a clip whose factorisation fails (its
-  pseudoinverse would truncate) is solved alone by the eigen-pseudoinverse;
-* synthesis kernels are again spread over the streams.
+* per clip, the temporal Gram, the right-hand side and the tensor-core
+  Kronecker Gram (scattered into the real symmetric float32 system) are
+  issued round-robin on several CUDA streams;
+* clips whose systems have the same size K are factorised by one batched
+  float32 Cholesky per group (``vtb_sym_factor_batched``), and every clip's
+  triangular solves run in one launch (``vtb_sym_potrs_batched``, one CTA per
+  clip), the grouped counterpart of the reference's per-window solve
+  (vtem/vtdm.py:645-648); float64 refinement sweeps against each clip's
+  exact residual follow;
+* that whole sequence, up to the acceptance check, is captured once as a
+  CUDA graph and replayed per run (``graph=True``);
+* one host check then reads every clip's flags: a clip whose pseudoinverse
+  might truncate (factorisation refused, or refinement not contracting) is
+  decoded by the float64 path -- Cholesky, else the eigen-pseudoinverse --
+  on a pool of host threads with their own streams, so that the
+  latency-bound eigensolvers of different clips overlap on the device;
+  clips with fewer intervals than coefficients take the spike-space
+  pseudoinverse the same way;
+* synthesis kernels are again spread over the streams (a second graph).
 
-The result of every clip equals its stand-alone decode (tests check it).
+The result of every clip equals its stand-alone decode within the mixed
+decoder's tolerance, and the reference's pseudoinverse within 1e-8 (tests).
 """
 from __future__ import annotations
 
 from collections import defaultdict
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import torch
 
 from . import fast
-from ._abi import call, dptr, stream_ptr
+from ._abi import call, dptr, lib, stream_ptr
+
+TRSV_DESC = np.dtype([("L", "<u8"), ("Dinv", "<u8"), ("x", "<u8"), ("ld", "<i8"), ("K", "<i4"), ("pad", "<i4")])
 
 
 class ClipProblem(object):
@@ -42,108 +57,321 @@ class ClipProblem(object):
     def voxels(self):
         return self.Nt * self.prep.decPx * self.prep.decPy
 
+    @property
+    def spikes(self):
+        return (self.tk1, self.tk2, self.ind, int(self.tk1.numel()), self.kappa, self.delta, self.bias)
+
+
+def stage_mixed(d, p, s):
+    """Device work of one clip up to its factorisation (no synchronisation):
+    W_n, g_n, b and its real form br, the tensor-core Gram scattered into the
+    float32 real system Mr32, and xr = br."""
+    tk1, tk2, ind, n, kap, dl, bi = p.spikes
+    K, KK = d.K, d.Kt * d.Kt
+    d.stat.zero_()
+    call("vtb_coeff_temporal_gram", dptr(tk1), dptr(tk2), dptr(ind), n, d.N, dptr(kap), dptr(dl), dptr(bi),
+         dptr(d.norm), d.Mt, d.W, dptr(d.Wn), dptr(d.gn), s)
+    call("vtb_coeff_rhs", dptr(d.d), d.N, d.Ks, dptr(d.gn), d.Kt, dptr(d.b), s)
+    call("vtb_coeff_realify_vec", dptr(d.b), K, 1, dptr(d.br), s)
+    call("vtb_coeff_wn_split", dptr(d.Wn), d.N, d.Kt, dptr(d.R3), s)
+    call("vtb_tc_gemm_bf16", dptr(d.L3), 2 * d.npairs, dptr(d.R3), KK, 3 * d.Kp2, dptr(d.C), KK, 1, 0, 1.0, 0,
+         d._stat_ptr(7), s)
+    call("vtb_coeff_real_scatter", dptr(d.C), KK, d.Ks, d.Kt, dptr(d.Mr32), K, 0, s)
+    d.xr.copy_(d.br)
+
+
+def sweep_residual(d, p, s):
+    """One clip's part of a refinement sweep before its solve: a from xr, the
+    exact float64 residual, and its real form rr."""
+    tk1, tk2, ind, n, kap, dl, bi = p.spikes
+    K = d.K
+    call("vtb_coeff_unrealify_vec", dptr(d.xr), K, 1, dptr(d.a), 0, s)
+    call("vtb_coeff_residual", dptr(tk1), dptr(tk2), dptr(ind), n, d.N, dptr(kap), dptr(dl), dptr(bi),
+         dptr(d.norm), d.Mt, d.W, dptr(d.d), d.Ks, dptr(d.a), dptr(d.gres), dptr(d.r), s)
+    call("vtb_coeff_realify_vec", dptr(d.r), K, 1, dptr(d.rr), s)
+
+
+def sweep_update(d, i, s):
+    """After the solve of rr: record ||rr|| / ||xr|| and xr += rr."""
+    call("vtb_norm_ratio", dptr(d.rr), dptr(d.xr), d.K, d._stat_ptr(3 + min(i, 3)), s)
+    call("vtb_daxpy1", dptr(d.xr), dptr(d.rr), d.K, s)
+
+
+def trsv_descs(entries, device):
+    """Device array of vtb_trsv_desc for (L, Dinv, x, ld, K) tuples."""
+    a = np.zeros(len(entries), TRSV_DESC)
+    for i, (L, Dinv, x, ld, K) in enumerate(entries):
+        a[i] = (L, Dinv, x, ld, K, 0)
+    return torch.as_tensor(np.frombuffer(a.tobytes(), np.uint8).copy()).to(device)
+
+
+class MixedSolvePlan(object):
+    """Grouped float32 Cholesky, batched triangular solves and float64
+    refinement sweeps of a set of mixed decoders whose systems were staged by
+    :func:`stage_mixed` (each with at least K intervals).  ``launch`` only
+    enqueues device work (capturable in a CUDA graph); ``check`` reads every
+    system's flags and correction ratios in one synchronising copy and
+    returns the indices (into ``decs``) that need the float64 path."""
+
+    def __init__(self, decs, probs, sweeps, streams):
+        self.decs, self.probs = list(decs), list(probs)
+        self.sweeps = int(sweeps)
+        self.streams = streams
+        dev = self.decs[0].M.device
+        self.device = dev
+        by_K = defaultdict(list)
+        for i, d in enumerate(self.decs):
+            by_K[d.K].append(i)
+        self.groups = []
+        l = lib()
+        dinv_of = {}
+        for K, idx in sorted(by_K.items()):
+            B = len(idx)
+            nf = int(l.vtb_sym_dinv_floats(K))
+            g = {
+                "K": K, "idx": idx,
+                "mptrs": torch.as_tensor([self.decs[i].Mr32.data_ptr() for i in idx], dtype=torch.int64, device=dev),
+                "dinv": torch.empty((B, nf), dtype=torch.float32, device=dev),
+                "infos": torch.zeros(B, dtype=torch.int32, device=dev),
+                "flags": torch.zeros(B, dtype=torch.int32, device=dev),
+                "piv": torch.zeros(2 * B, dtype=torch.float64, device=dev),
+            }
+            for j, i in enumerate(idx):
+                dinv_of[i] = g["dinv"][j]
+            self.groups.append(g)
+        self.Kmax = max(d.K for d in self.decs)
+        self.desc_x = trsv_descs([(d.Mr32.data_ptr(), dinv_of[i].data_ptr(), d.xr.data_ptr(), d.K, d.K)
+                                  for i, d in enumerate(self.decs)], dev)
+        self.desc_r = trsv_descs([(d.Mr32.data_ptr(), dinv_of[i].data_ptr(), d.rr.data_ptr(), d.K, d.K)
+                                  for i, d in enumerate(self.decs)], dev)
+        self.order = [i for g in self.groups for i in g["idx"]]
+
+    def _fork(self):
+        main = torch.cuda.current_stream(self.device)
+        ev = torch.cuda.Event()
+        ev.record(main)
+        for st in self.streams:
+            st.wait_event(ev)
+        return main
+
+    def _join(self, main):
+        for st in self.streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+
+    def launch(self):
+        s = stream_ptr()
+        for g in self.groups:
+            rc = self.probs[g["idx"][0]].rcond * fast.CHOL_MARGIN
+            call("vtb_sym_factor_batched", g["mptrs"].data_ptr(), g["K"], g["K"], len(g["idx"]), rc,
+                 dptr(g["dinv"]), dptr(g["infos"]), dptr(g["flags"]), dptr(g["piv"]), s)
+        n = len(self.decs)
+        call("vtb_sym_potrs_batched", dptr(self.desc_x), n, self.Kmax, s)
+        for i in range(self.sweeps):
+            main = self._fork()
+            for c, (d, p) in enumerate(zip(self.decs, self.probs)):
+                with torch.cuda.stream(self.streams[c % len(self.streams)]):
+                    sweep_residual(d, p, stream_ptr())
+            self._join(main)
+            call("vtb_sym_potrs_batched", dptr(self.desc_r), n, self.Kmax, stream_ptr())
+            main = self._fork()
+            for c, d in enumerate(self.decs):
+                with torch.cuda.stream(self.streams[c % len(self.streams)]):
+                    sweep_update(d, i, stream_ptr())
+            self._join(main)
+        s = stream_ptr()
+        for d in self.decs:
+            call("vtb_coeff_unrealify_vec", dptr(d.xr), d.K, 1, dptr(d.a), 0, s)
+
+    def check(self):
+        """Indices of the systems the float64 path must decode (one
+        synchronising read); records pivots and ratios on each decoder."""
+        flags = torch.cat([g["flags"] for g in self.groups])
+        piv = torch.cat([g["piv"] for g in self.groups])
+        stats = torch.stack([d.stat for d in self.decs])
+        flags, piv, stats = flags.cpu().numpy(), piv.cpu().numpy(), stats.cpu().numpy()
+        bad = []
+        fl = dict(zip(self.order, flags))
+        pv = {i: (float(piv[2 * j]), float(piv[2 * j + 1])) for j, i in enumerate(self.order)}
+        for i, d in enumerate(self.decs):
+            tc_err = int(stats[i].view(np.int32)[14])
+            if tc_err != 0:
+                raise fast.VtbError("vtb_tc_gemm_bf16", tc_err)
+            d.last_pivots = pv[i]
+            d.last_ratios = [float(x) for x in stats[i][3:3 + min(self.sweeps, 4)]]
+            if fl[i] != 0 or not d._mixed_converged(d.last_ratios):
+                bad.append(i)
+            else:
+                d.last_solver = "mixed-batched"
+        return bad
+
 
 class BatchDecoder(object):
-    def __init__(self, problems, streams=8):
+    """Decode many clips per ``run()``: mixed-precision grouped solves as
+    described in the module docstring.  ``graph`` captures the staging,
+    factorisation and refinement (and, separately, the synthesis) as CUDA
+    graphs on the first run and replays them afterwards; inputs are read
+    from the problems' device tensors, so new spikes of the same sizes are
+    decoded by copying them into those tensors.  ``workers`` host threads
+    run the float64 fallbacks and spike-space solves concurrently."""
+
+    def __init__(self, problems, streams=8, sweeps=1, graph=True, workers=8):
         self.problems = list(problems)
-        self.decs = [fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver="chol") for p in self.problems]
+        self.decs = [fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver="mixed", mixed_sweeps=sweeps)
+                     for p in self.problems]
         dev = self.decs[0].M.device
+        self.device = dev
         self.streams = [torch.cuda.Stream(device=dev) for _ in range(streams)]
-        self.groups = defaultdict(list)
-        for i, (p, d) in enumerate(zip(self.problems, self.decs)):
-            if int(p.tk1.numel()) >= d.K:
-                self.groups[d.K].append(i)
-        self.ptrs = {}
-        for K, idx in self.groups.items():
-            mp = torch.as_tensor([self.decs[i].M.data_ptr() for i in idx], dtype=torch.int64, device=dev)
-            bp = torch.as_tensor([self.decs[i].a.data_ptr() for i in idx], dtype=torch.int64, device=dev)
-            infos = torch.zeros(len(idx), dtype=torch.int32, device=dev)
-            sinfo = torch.zeros(1, dtype=torch.int32, device=dev)
-            self.ptrs[K] = (mp, bp, infos, sinfo)
+        self.coeff = [i for i, (p, d) in enumerate(zip(self.problems, self.decs)) if int(p.tk1.numel()) >= d.K]
+        self.spike = [i for i in range(len(self.problems)) if i not in set(self.coeff)]
+        self.plan = MixedSolvePlan([self.decs[i] for i in self.coeff], [self.problems[i] for i in self.coeff], sweeps,
+                                   self.streams) if self.coeff else None
+        self.groups = self.plan.groups if self.plan else []
         self.outs = [torch.empty((p.Nt, p.prep.decPy, p.prep.decPx), dtype=torch.float64, device=dev)
                      for p in self.problems]
+        self.use_graph = bool(graph)
+        self.graph_error = None
+        self._g1 = self._g2 = None
+        self._pool = ThreadPoolExecutor(max_workers=max(1, workers))
+        self._worker_streams = {}
         self.fallbacks = 0
+        self._phase_events = None
 
-    def run(self, timing=False):
-        """Decode every clip; returns the list of videos.  With ``timing`` the
-        device time of the three phases is left in ``self.phase_ms`` (the
-        caller synchronises before reading it)."""
-        main = torch.cuda.current_stream()
-        start = torch.cuda.Event(enable_timing=timing)
-        start.record(main)
-        for s in self.streams:
-            s.wait_event(start)
-        # phase 1: per-clip Gram and right-hand side, round-robin over the
-        # streams; clips with fewer intervals than coefficients are solved in
-        # the (smaller) spike space right away
-        for i, (p, d) in enumerate(zip(self.problems, self.decs)):
-            st = self.streams[i % len(self.streams)]
-            with torch.cuda.stream(st):
-                s = stream_ptr()
-                n = int(p.tk1.numel())
-                if n < d.K:
-                    d._solve_spike_space(s, (p.tk1, p.tk2, p.ind, n, p.kappa, p.delta, p.bias))
-                    continue
-                call("vtb_coeff_temporal_gram", dptr(p.tk1), dptr(p.tk2), dptr(p.ind), n, d.N, dptr(p.kappa),
-                     dptr(p.delta), dptr(p.bias), dptr(d.norm), d.Mt, d.W, dptr(d.Wn), dptr(d.gn), s)
-                d._build_M(s)
-                d.a.copy_(d.b)
-                d.last_solver = "chol-batched"
-        joins = []
+    # ---------------------------------------------------------- device work
+    def _fork(self):
+        main = torch.cuda.current_stream(self.device)
+        ev = torch.cuda.Event()
+        ev.record(main)
         for st in self.streams:
-            e = torch.cuda.Event()
-            e.record(st)
-            joins.append(e)
-        for e in joins:
-            main.wait_event(e)
-        t1 = torch.cuda.Event(enable_timing=timing)
-        t1.record(main)
-        # phase 2: one batched Cholesky per group of equally sized systems
-        # (clips with fewer intervals than unknowns are singular: eigen path)
-        s = stream_ptr()
-        for K, idx in self.groups.items():
-            mp, bp, infos, sinfo = self.ptrs[K]
-            rc = self.problems[idx[0]].rcond * fast.CHOL_MARGIN
-            call("vtb_herm_chol_batched", mp.data_ptr(), K, bp.data_ptr(), K, len(idx), rc, dptr(infos), dptr(sinfo),
-                 s)
-        # clips whose factorisation was refused (their pseudoinverse truncates):
-        # batched eigen-pseudoinverse per system size (one host check)
-        keys = list(self.groups)
-        if keys:
-            flags = torch.cat([self.ptrs[K][2] for K in keys]).ne(0).cpu().tolist()
-            bad_by_K, o = defaultdict(list), 0
-            for K in keys:
-                idx = self.groups[K]
-                bad_by_K[K] = [self.decs[idx[j]] for j in range(len(idx)) if flags[o + j]]
-                o += len(idx)
-            eig_infos = [fast.pinv_batched(ds) for ds in bad_by_K.values() if ds]
-            self.fallbacks = sum(len(ds) for ds in bad_by_K.values())
-            if eig_infos and int(torch.cat(eig_infos).ne(0).sum()) != 0:
-                raise fast.VtbError("vtb_herm_pinv_batched", fast.VTB_NOT_CONVERGED)
-        done = torch.cuda.Event(enable_timing=timing)
-        done.record(main)
-        # phase 3: synthesis
+            st.wait_event(ev)
+        return main
+
+    def _join(self, main):
+        for st in self.streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+
+    def _stage_and_solve(self):
+        main = self._fork()
+        for c, i in enumerate(self.coeff):
+            with torch.cuda.stream(self.streams[c % len(self.streams)]):
+                stage_mixed(self.decs[i], self.problems[i], stream_ptr())
+        self._join(main)
+        self.plan.launch()
+
+    def _synthesize(self):
+        main = self._fork()
         for i, (p, d) in enumerate(zip(self.problems, self.decs)):
-            st = self.streams[i % len(self.streams)]
-            st.wait_event(done)
-            with torch.cuda.stream(st):
+            with torch.cuda.stream(self.streams[i % len(self.streams)]):
                 d.synthesize(d.a, p.T, p.dt, out=self.outs[i])
-        for st in self.streams:
-            e = torch.cuda.Event()
-            e.record(st)
-            main.wait_event(e)
-        if timing:
-            end = torch.cuda.Event(enable_timing=True)
-            end.record(main)
-            self._phase_events = (start, t1, done, end)
+        self._join(main)
+
+    def _capture(self, fn):
+        fn()                      # eager warm-up: library handles, kernel attributes, allocations
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            fn()
+        return g
+
+    def _ensure_graphs(self):
+        if not self.use_graph or self._g2 is not None:
+            return
+        try:
+            if self.plan is not None:
+                self._g1 = self._capture(self._stage_and_solve)
+            self._g2 = self._capture(self._synthesize)
+        except Exception as e:  # graphs unavailable: the same launches, issued eagerly
+            self.graph_error = repr(e)
+            self.use_graph = False
+            self._g1 = self._g2 = None
+            torch.cuda.synchronize(self.device)
+
+    # ---------------------------------------------------------- float64 path
+    def _worker_stream(self):
+        import threading
+        tid = threading.get_ident()
+        st = self._worker_streams.get(tid)
+        if st is None:
+            st = torch.cuda.Stream(device=self.device)
+            self._worker_streams[tid] = st
+        return st
+
+    def _float64(self, i, after=None):
+        """Float64 decode of clip i (spike-space pseudoinverse, or Cholesky /
+        eigen-pseudoinverse of its real system) on a worker thread."""
+        torch.cuda.set_device(self.device)
+        st = self._worker_stream()
+        with torch.cuda.stream(st):
+            if after is not None:
+                st.wait_event(after)
+            d, p = self.decs[i], self.problems[i]
+            n = int(p.tk1.numel())
+            s = stream_ptr()
+            if n < d.K:
+                d._solve_spike_space(s, p.spikes)
+            else:
+                d.solver = "auto"
+                try:
+                    d._solve(s, n)
+                finally:
+                    d.solver = "mixed"
+                d.last_solver = "mixed->" + d.last_solver
+            ev = torch.cuda.Event()
+            ev.record(st)
+        return ev
+
+    # ---------------------------------------------------------- run
+    def run(self, timing=False):
+        """Decode every clip; returns the list of videos (device).  With
+        ``timing`` the device time of (staging + grouped solves, float64
+        fallbacks, synthesis) is left in ``self.phase_ms``."""
+        self._ensure_graphs()
+        main = torch.cuda.current_stream(self.device)
+        ev = [torch.cuda.Event(enable_timing=timing) for _ in range(4)]
+        ev[0].record(main)
+        futs = [self._pool.submit(self._float64, i, ev[0]) for i in self.spike]
+        bad = []
+        if self.plan is not None:
+            if self._g1 is not None:
+                self._g1.replay()
+            else:
+                self._stage_and_solve()
+            ev[1].record(main)
+            bad = [self.coeff[j] for j in self.plan.check()]
+            futs += [self._pool.submit(self._float64, i, ev[1]) for i in bad]
+        else:
+            ev[1].record(main)
+        for f in futs:
+            main.wait_event(f.result())
+        self.fallbacks = len(bad)
+        ev[2].record(main)
+        if self._g2 is not None:
+            self._g2.replay()
+        else:
+            self._synthesize()
+        ev[3].record(main)
+        self._phase_events = ev
         return self.outs
 
     @property
     def phase_ms(self):
-        """(Gram/right-hand sides, solves, synthesis) device milliseconds of
-        the last ``run(timing=True)``."""
+        """(staging + grouped solves, float64 fallbacks, synthesis) device
+        milliseconds of the last ``run(timing=True)`` (synchronise first)."""
         e = self._phase_events
         return tuple(e[i].elapsed_time(e[i + 1]) for i in range(3))
+
+    def solver_counts(self):
+        c = {}
+        for d in self.decs:
+            c[d.last_solver] = c.get(d.last_solver, 0) + 1
+        return c
+
+    def close(self):
+        self._pool.shutdown(wait=True)
+        self._g1 = self._g2 = None
 
 
 def encode_clip_problem(w, device="cuda", keep_video=False, video=None, precision="f64"):

@@ -165,8 +165,8 @@ __global__ void daxpy1_kernel(double* __restrict__ y, const double* __restrict__
 // column-major alike) -> piv[0] = min, piv[1] = max; flag = 1 if the
 // factorisation reported a failure, 2 if max/min * rcond >= 1.
 template <typename T>
-__global__ void pivot_flag_kernel(const T* __restrict__ L, int64_t ld, int K, const int* __restrict__ info,
-                                  double rcond, double* __restrict__ piv, int32_t* __restrict__ flag) {
+__device__ void pivot_flag_body(const T* __restrict__ L, int64_t ld, int K, const int* __restrict__ info,
+                                double rcond, double* __restrict__ piv, int32_t* __restrict__ flag) {
     __shared__ double smin[32], smax[32];
     double mn = 1e308, mx = 0.0;
     for (int i = threadIdx.x; i < K; i += blockDim.x) {
@@ -197,6 +197,12 @@ __global__ void pivot_flag_kernel(const T* __restrict__ L, int64_t ld, int K, co
         else if (mx / mn * rcond >= 1.0) f = 2;
         *flag = f;
     }
+}
+
+template <typename T>
+__global__ void pivot_flag_kernel(const T* __restrict__ L, int64_t ld, int K, const int* __restrict__ info,
+                                  double rcond, double* __restrict__ piv, int32_t* __restrict__ flag) {
+    pivot_flag_body<T>(L, ld, K, info, rcond, piv, flag);
 }
 
 // out = ||dx|| / ||x|| (the relative size of a refinement correction)
@@ -237,12 +243,183 @@ static cusolverDnHandle_t real_solver_handle(int dev) {
 
 static int64_t al256r(int64_t x) { return (x + 255) & ~(int64_t)255; }
 
-// Workspace: [info 256][vec f32: K floats][w: K doubles][v1: K doubles][lapack work]
+// ------------------------------------------------------------------ float32 triangular solves
+// x = L^-T L^-1 x for the lower float32 Cholesky factor L (column-major,
+// element (i, j) at j*ld + i, as spotrf leaves it), for BATCHES of systems:
+// one CTA of 1024 threads solves one system with the right-hand side in
+// shared memory (many systems keep every SM busy; a single system is left to
+// cuSOLVER's multi-CTA spotrs, since one CTA is bound by one SM's share of
+// L2 bandwidth), in 32-wide block steps:
+//   forward  (L y = b):  y_J = Dinv_J r_J (one warp), then every row below
+//            the block subtracts L(i, J) y_J (the thread's rows of column
+//            block J are loaded before the block barrier, hiding L2 latency);
+//   backward (L^T x = y): warp w forms the dot product of column J*32+w below
+//            the block with the solved tail, then x_J = Dinv_J^T (y_J - s).
+// Dinv_J = L_JJ^-1 (32 x 32, row-major) is formed once per factorisation by
+// diag_inv_kernel.  Every read of L is a coalesced column segment.
+constexpr int kTrsvThreads = 1024;
+constexpr int kTrsvPrefetchRows = 1;
+
+// One warp per diagonal block: lane c solves L_JJ X[:, c] = e_c; padding
+// beyond K is the identity.
+__device__ void diag_inv_body(const float* __restrict__ L, int64_t ld, int K, float* __restrict__ Dinv) {
+    __shared__ float sL[4][32][33];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int J = blockIdx.x * 4 + w;
+    const int nt = (K + 31) >> 5;
+    if (J >= nt) return;
+    const int base = J * 32;
+    for (int r = 0; r < 32; ++r) {
+        const int gr = base + r, gc = base + lane;
+        float v = 0.f;
+        if (gr < K && gc < K) {
+            if (lane <= r) v = L[(int64_t)gc * ld + gr];
+        } else if (r == lane) {
+            v = 1.f;
+        }
+        sL[w][r][lane] = v;
+    }
+    __syncwarp();
+    float X[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+        float s = (r == lane) ? 1.f : 0.f;
+#pragma unroll
+        for (int k = 0; k < r; ++k) s = fmaf(-sL[w][r][k], X[k], s);
+        X[r] = s / sL[w][r][r];
+    }
+#pragma unroll
+    for (int r = 0; r < 32; ++r) Dinv[(int64_t)J * 1024 + r * 32 + lane] = X[r];
+}
+
+__global__ void __launch_bounds__(128) diag_inv_kernel(const float* __restrict__ L, int64_t ld, int K,
+                                                       float* __restrict__ Dinv) {
+    diag_inv_body(L, ld, K, Dinv);
+}
+
+// Solves in place on the float32 vector r (shared memory, K entries); part
+// is 32 floats of shared scratch.  Requires blockDim.x == kTrsvThreads.
+__device__ void trsv_pair(const float* __restrict__ L, int64_t ld, const float* __restrict__ Dinv, int K,
+                          float* __restrict__ r, float* __restrict__ part) {
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int nt = (K + 31) >> 5;
+    // forward: L y = b
+    for (int J = 0; J < nt; ++J) {
+        const int c0 = J * 32, rs = c0 + 32;
+        float Lr[kTrsvPrefetchRows][32];
+#pragma unroll
+        for (int m = 0; m < kTrsvPrefetchRows; ++m) {
+            const int i = rs + t + m * kTrsvThreads;
+            if (i < K) {
+#pragma unroll
+                for (int k = 0; k < 32; ++k) Lr[m][k] = L[(int64_t)(c0 + k) * ld + i];
+            }
+        }
+        if (w == 0) {
+            const float* D = Dinv + (int64_t)J * 1024 + lane * 32;
+            float acc = 0.f;
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                const float rk = (c0 + k < K) ? r[c0 + k] : 0.f;
+                acc = fmaf(D[k], rk, acc);
+            }
+            __syncwarp();
+            if (c0 + lane < K) r[c0 + lane] = acc;
+        }
+        __syncthreads();
+        // rows below the block exist only when c0 + 32 <= K - 1, so every
+        // column of the block is in range here
+#pragma unroll
+        for (int m = 0; m < kTrsvPrefetchRows; ++m) {
+            const int i = rs + t + m * kTrsvThreads;
+            if (i < K) {
+                float s = 0.f;
+#pragma unroll
+                for (int k = 0; k < 32; ++k) s = fmaf(Lr[m][k], r[c0 + k], s);
+                r[i] -= s;
+            }
+        }
+        for (int i = rs + t + kTrsvPrefetchRows * kTrsvThreads; i < K; i += kTrsvThreads) {
+            float s = 0.f;
+            for (int k = 0; k < 32; ++k) s = fmaf(L[(int64_t)(c0 + k) * ld + i], r[c0 + k], s);
+            r[i] -= s;
+        }
+        __syncthreads();
+    }
+    // backward: L^T x = y
+    for (int J = nt - 1; J >= 0; --J) {
+        const int c0 = J * 32, rs = c0 + 32;
+        const int c = c0 + w;
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+        if (c < K) {
+            const float* col = L + (int64_t)c * ld;
+            int i = rs + lane;
+            for (; i + 96 < K; i += 128) {
+                s0 = fmaf(col[i], r[i], s0);
+                s1 = fmaf(col[i + 32], r[i + 32], s1);
+                s2 = fmaf(col[i + 64], r[i + 64], s2);
+                s3 = fmaf(col[i + 96], r[i + 96], s3);
+            }
+            for (; i < K; i += 32) s0 = fmaf(col[i], r[i], s0);
+        }
+        float s = (s0 + s1) + (s2 + s3);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) part[w] = s;
+        __syncthreads();
+        if (w == 0) {
+            const float* D = Dinv + (int64_t)J * 1024;
+            float acc = 0.f;
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                const float yk = (c0 + k < K) ? r[c0 + k] - part[k] : 0.f;
+                acc = fmaf(D[k * 32 + lane], yk, acc);
+            }
+            __syncwarp();
+            if (c0 + lane < K) r[c0 + lane] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+using TrsvDesc = vtb_trsv_desc;
+static_assert(sizeof(TrsvDesc) == 40, "vtb_trsv_desc layout");
+
+// one CTA per system of a batch (descriptors in device memory)
+__global__ void __launch_bounds__(kTrsvThreads) trsv_pair_batched_kernel(const TrsvDesc* __restrict__ descs) {
+    extern __shared__ float trsv_sm[];
+    const TrsvDesc d = descs[blockIdx.x];
+    float* part = trsv_sm;
+    float* r = trsv_sm + 32;
+    for (int i = threadIdx.x; i < d.K; i += blockDim.x) r[i] = (float)d.x[i];
+    __syncthreads();
+    trsv_pair(d.L, d.ld, d.Dinv, d.K, r, part);
+    for (int i = threadIdx.x; i < d.K; i += blockDim.x) d.x[i] = (double)r[i];
+}
+
+// Per-system pivot test of a batch of float32 factors (blockIdx.x = system).
+__global__ void pivot_flag_batched_kernel(float* const* __restrict__ Mptrs, int64_t ld, int K,
+                                          const int* __restrict__ infos, double rcond, double* __restrict__ piv,
+                                          int32_t* __restrict__ flags) {
+    const int z = blockIdx.x;
+    pivot_flag_body<float>(Mptrs[z], ld, K, infos + z, rcond, piv ? piv + 2 * z : nullptr, flags + z);
+}
+
+__global__ void __launch_bounds__(128) diag_inv_batched_kernel(float* const* __restrict__ Mptrs, int64_t ld, int K,
+                                                               float* __restrict__ Dinv, int64_t dinv_stride) {
+    diag_inv_body(Mptrs[blockIdx.y], ld, K, Dinv + blockIdx.y * dinv_stride);
+}
+
+static int64_t dinv_floats(int K) { return (int64_t)((K + 31) / 32) * 1024; }
+
+// Workspace: [info 256][vec f32: K floats][w: K doubles][v1: K doubles][Dinv (mode 2)][lapack work]
+
 struct RealWork {
     int* info;
     float* vf;
     double* w;
     double* v1;
+    float* dinv;  // mode 2: inverses of the factor's 32 x 32 diagonal blocks
     void* wk;
     int lwork;   // elements of the factorisation's / eigensolver's work type
 };
@@ -270,12 +447,14 @@ static int64_t real_layout(int K, int mode, int lwork, char* base, RealWork* rw)
     const int64_t of = take((int64_t)K * 4);
     const int64_t ow = take((int64_t)K * 8);
     const int64_t o1 = take((int64_t)K * 8);
+    const int64_t od = take(mode == 2 ? dinv_floats(K) * 4 : 0);
     const int64_t ok = take((int64_t)lwork * (mode == 2 ? 4 : 8));
     if (base && rw) {
         rw->info = reinterpret_cast<int*>(base + oi);
         rw->vf = reinterpret_cast<float*>(base + of);
         rw->w = reinterpret_cast<double*>(base + ow);
         rw->v1 = reinterpret_cast<double*>(base + o1);
+        rw->dinv = reinterpret_cast<float*>(base + od);
         rw->wk = base + ok;
         rw->lwork = lwork;
     }
@@ -432,9 +611,11 @@ VTB_API int vtb_sym_factor(void* M, int64_t ld, int K, int mode, double rcond, v
     if (mode == 1)
         pivot_flag_kernel<double><<<1, 1024, 0, s>>>(reinterpret_cast<const double*>(M), ld, K, rw.info, rcond, pivots,
                                                      flag);
-    else
+    else {
         pivot_flag_kernel<float><<<1, 1024, 0, s>>>(reinterpret_cast<const float*>(M), ld, K, rw.info, rcond, pivots,
                                                     flag);
+        diag_inv_kernel<<<ceil_div((K + 31) / 32, 4), 128, 0, s>>>(reinterpret_cast<const float*>(M), ld, K, rw.dinv);
+    }
     return launch_status();
 }
 
@@ -452,11 +633,58 @@ VTB_API int vtb_sym_potrs(const void* Mfac, int64_t ld, double* x, int K, int mo
             return VTB_CUDA_ERR;
         return launch_status();
     }
+    // one system: cuSOLVER's multi-CTA solves (a single CTA is bound by one
+    // SM's share of L2 bandwidth); batches use trsv_pair_batched_kernel
     f64_to_f32_kernel<<<ceil_div(K, 256), 256, 0, s>>>(x, rw.vf, K);
     if (cusolverDnSpotrs(h, CUBLAS_FILL_MODE_LOWER, K, 1, reinterpret_cast<const float*>(Mfac), (int)ld, rw.vf, K,
                          rw.info) != CUSOLVER_STATUS_SUCCESS)
         return VTB_CUDA_ERR;
     f32_to_f64_kernel<<<ceil_div(K, 256), 256, 0, s>>>(rw.vf, x, K);
+    return launch_status();
+}
+
+// Batched float32 Cholesky of `batch` systems of one size K (a group of clips
+// with equal K): cusolverDnSpotrfBatched, then per system the pivot test of
+// vtb_sym_factor (flags[z]) and the diagonal-block inverses used by
+// vtb_sym_potrs_batched (Dinv + z * vtb_sym_dinv_floats(K)).  infos (device,
+// batch ints) receives cuSOLVER's per-system status.  Does not synchronise.
+VTB_API int vtb_sym_factor_batched(float** Mptrs, int64_t ld, int K, int batch, double rcond, float* Dinv,
+                                   int32_t* infos, int32_t* flags, double* pivots, void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && batch >= 0);
+    if (batch == 0) return VTB_OK;
+    VTB_CHECK_ARG(Mptrs && Dinv && infos && flags);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = real_solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    cudaStream_t s = as_stream(stream);
+    if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    if (cusolverDnSpotrfBatched(h, CUBLAS_FILL_MODE_LOWER, K, Mptrs, (int)ld, infos, batch) != CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    pivot_flag_batched_kernel<<<batch, 1024, 0, s>>>(Mptrs, ld, K, infos, rcond, pivots, flags);
+    int st = launch_status();
+    if (st) return st;
+    diag_inv_batched_kernel<<<dim3(ceil_div((K + 31) / 32, 4), batch), 128, 0, s>>>(Mptrs, ld, K, Dinv,
+                                                                                   dinv_floats(K));
+    return launch_status();
+}
+
+VTB_API int64_t vtb_sym_dinv_floats(int K) { return K > 0 ? dinv_floats(K) : 0; }
+
+// Batched float32 solves x_z = L_z^-T L_z^-1 x_z, one CTA per system.  descs
+// (device) holds per system {L (column-major float32 factor of
+// vtb_sym_factor mode 2 or vtb_sym_factor_batched), Dinv (the inverses of its
+// 32 x 32 diagonal blocks), x (float64, in place), ld, K}; Kmax bounds K.
+VTB_API int vtb_sym_potrs_batched(const void* descs, int batch, int Kmax, void* stream) {
+    VTB_CHECK_ARG(batch >= 0 && Kmax > 0);
+    if (batch == 0) return VTB_OK;
+    VTB_CHECK_ARG(descs);
+    const size_t sm = (size_t)(Kmax + 32) * sizeof(float);
+    VTB_CHECK_ARG(sm <= 200 * 1024);
+    if (sm > 48 * 1024)
+        VTB_CUDA_TRY(
+            cudaFuncSetAttribute(trsv_pair_batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    trsv_pair_batched_kernel<<<batch, kTrsvThreads, sm, as_stream(stream)>>>(reinterpret_cast<const TrsvDesc*>(descs));
     return launch_status();
 }
 
