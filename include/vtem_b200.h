@@ -373,6 +373,16 @@ typedef struct vtb_trsv_desc {
 /* Solves of `batch` systems (descs: device array), one CTA each; Kmax >= every K. */
 int vtb_sym_potrs_batched(const void* descs, int batch, int Kmax, void* stream);
 
+/* Batched eigen-pseudoinverse of `batch` real symmetric systems of one size K
+ * (cuSOLVER XsyevBatched): per system the rule of vtb_sym_pinv.  M holds the
+ * matrices contiguously (stride K*K, destroyed), b and x at stride K; kept
+ * (device, may be NULL) and infos (device) per system.  The grouped
+ * counterpart of solve_eq_sym (vtem/utils/linalg.py:591-631) for windows whose
+ * pseudoinverse truncates.  Synchronises the stream. */
+int vtb_sym_pinv_batched_workspace(int K, int batch, int64_t* bytes);
+int vtb_sym_pinv_batched(double* M, const double* b, double* x, int K, int batch, double rcond, void* work,
+                         int64_t work_bytes, int32_t* kept, int32_t* infos, void* stream);
+
 /* out (device) = ||dx|| / ||x||: the relative size of a refinement correction. */
 int vtb_norm_ratio(const double* dx, const double* x, int n, double* out, void* stream);
 /* y += x (n doubles). */

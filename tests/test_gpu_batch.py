@@ -129,3 +129,62 @@ def test_pinv_batched_equals_single():
         keep = np.abs(w) > rcond * np.abs(w).max()
         ref = V[:, keep] @ ((V[:, keep].conj().T @ bs[z]) / w[keep])
         assert np.linalg.norm(ab[z].cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-8
+
+
+def test_pinv_bucketed_equals_single():
+    """Eigen-pseudoinverses of systems of different sizes, padded into one
+    batched call, equal each system's stand-alone vtb_sym_pinv (same kept
+    count, same solution), full-rank and rank-deficient alike."""
+    from vtem_b200._abi import call, dptr, stream_ptr
+
+    class Sys(object):
+        pass
+
+    rng = np.random.default_rng(5)
+    dev = torch.device("cuda")
+    systems = []
+    # full rank (r > K, well conditioned) and rank-deficient (r < K) systems
+    for K, r in ((61, 80), (55, 30), (49, 70), (45, 20), (23, 40)):
+        X = rng.standard_normal((K, r))
+        A = X @ X.T
+        bc = np.zeros(K, np.complex128)
+        d = Sys()
+        d.K, d.rcond = K, 1e-8
+        # pinv_bucketed realifies d.M (complex column-major); give it a real
+        # Hermitian-symmetric system through the inverse map of the real form
+        d.Mr = torch.empty((K, K), dtype=torch.float64, device=dev)
+        d.br = torch.as_tensor(rng.standard_normal(K), device=dev)
+        d.xr = torch.empty(K, dtype=torch.float64, device=dev)
+        d.a = torch.empty(K, dtype=torch.complex128, device=dev)
+        d.kept = torch.zeros(1, dtype=torch.int32, device=dev)
+        d.A = A
+        systems.append(d)
+    # complex M whose real form is A: M = U^H A U for the unitary map of the real form
+    for d in systems:
+        K, h = d.K, (d.K - 1) // 2
+        U = np.zeros((K, K), np.complex128)       # x = U a on Hermitian-symmetric a
+        for j in range(h):
+            U[j, j] = U[j, K - 1 - j] = 1 / np.sqrt(2)
+            U[h + 1 + j, j] = -1j / np.sqrt(2)
+            U[h + 1 + j, K - 1 - j] = 1j / np.sqrt(2)
+        U[h, h] = 1.0
+        M = U.conj().T @ d.A @ U
+        d.M = torch.as_tensor(M.T.copy(), device=dev)     # column-major
+    batch.pinv_bucketed(systems, stream_ptr())
+    torch.cuda.synchronize()
+    for d in systems:
+        K = d.K
+        assert np.abs(d.Mr.cpu().numpy() - d.A).max() <= 1e-12 * np.abs(d.A).max()
+        nb = np.zeros(1, np.int64)
+        call("vtb_sym_workspace", K, 0, nb.ctypes.data)
+        w1 = torch.empty(int(nb[0]), dtype=torch.uint8, device=dev)
+        A1 = torch.as_tensor(d.A.copy(), device=dev)
+        x1 = torch.empty(K, dtype=torch.float64, device=dev)
+        k1 = torch.zeros(1, dtype=torch.int32, device=dev)
+        rng2 = np.zeros(2)
+        call("vtb_sym_pinv", dptr(A1), K, dptr(d.br), dptr(x1), K, 1e-8, dptr(w1), int(nb[0]), dptr(k1),
+             rng2.ctypes.data, stream_ptr())
+        torch.cuda.synchronize()
+        assert int(d.kept[0]) == int(k1[0])
+        rel = ((d.xr - x1).norm() / x1.norm()).item()
+        assert rel < 1e-9, (K, rel)

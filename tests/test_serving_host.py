@@ -71,7 +71,7 @@ class FakeServer(serving.Server):
             raise RuntimeError("eigensolver failed")
         self.eig_groups.append(sorted(j.req.rid for j in jobs))
         for j in jobs:
-            assert len({x.dec.K for x in jobs}) == 1
+            # systems of any size: the solver thread groups them by padded size
             j.req.solver = "eig"
 
     def _phase_b(self, job):

@@ -80,6 +80,8 @@ SIGNATURES = {
     "vtb_sym_pinv": [P, L, P, P, I, D, P, L, P, P, P],
     "vtb_sym_factor_batched": [P, L, I, I, D, P, P, P, P, P],
     "vtb_sym_potrs_batched": [P, I, I, P],
+    "vtb_sym_pinv_batched_workspace": [I, I, P],
+    "vtb_sym_pinv_batched": [P, P, P, I, I, D, P, L, P, P, P],
     "vtb_sym_dinv_floats": [I],  # restype int64, set in lib()
 }
 

@@ -184,13 +184,20 @@ class MixedSolvePlan(object):
         for d in self.decs:
             call("vtb_coeff_unrealify_vec", dptr(d.xr), d.K, 1, dptr(d.a), 0, s)
 
-    def check(self):
-        """Indices of the systems the float64 path must decode (one
-        synchronising read); records pivots and ratios on each decoder."""
+    def gather(self):
+        """Device tensors (flags, pivots, per-system status words) for
+        :meth:`evaluate`; copying them to the host is the caller's choice
+        (synchronous in :meth:`check`, asynchronous in the serving loop)."""
         flags = torch.cat([g["flags"] for g in self.groups])
         piv = torch.cat([g["piv"] for g in self.groups])
         stats = torch.stack([d.stat for d in self.decs])
-        flags, piv, stats = flags.cpu().numpy(), piv.cpu().numpy(), stats.cpu().numpy()
+        return flags, piv, stats
+
+    def evaluate(self, flags, piv, stats):
+        """Indices of the systems the float64 path must decode, from host
+        copies of :meth:`gather`'s tensors; records pivots and correction
+        ratios on each decoder."""
+        flags, piv, stats = (np.asarray(x) for x in (flags, piv, stats))
         bad = []
         fl = dict(zip(self.order, flags))
         pv = {i: (float(piv[2 * j]), float(piv[2 * j + 1])) for j, i in enumerate(self.order)}
@@ -205,6 +212,80 @@ class MixedSolvePlan(object):
             else:
                 d.last_solver = "mixed-batched"
         return bad
+
+    def check(self):
+        """Indices of the systems the float64 path must decode (one
+        synchronising read)."""
+        return self.evaluate(*(t.cpu().numpy() for t in self.gather()))
+
+
+# Eigen-pseudoinverses of systems of different sizes are grouped into batches
+# of one padded size: a system of size K joins a batch of size K' >= K when
+# K >= PINV_BUCKET_RATIO * K'.  Scratch per batched call is bounded.
+PINV_BUCKET_RATIO = 0.7
+PINV_BATCH_BYTES = 2 << 30
+
+
+def pinv_buckets(Ks, ratio=PINV_BUCKET_RATIO):
+    """Greedy grouping of system sizes (indices into Ks) by padded size."""
+    order = sorted(range(len(Ks)), key=lambda i: -Ks[i])
+    out = []
+    while order:
+        top = Ks[order[0]]
+        take = [i for i in order if Ks[i] >= ratio * top]
+        out.append((top, take))
+        order = [i for i in order if Ks[i] < ratio * top]
+    return out
+
+
+def pinv_bucketed(decs, s):
+    """Truncated eigen-pseudoinverse (float64, the rule of solve_eq_sym) of
+    the real systems of ``decs`` (their complex M and b already built), in
+    batched eigensolver calls of one padded size.  A system of size K is
+    embedded in a K' x K' matrix whose extra diagonal entries equal Mr's
+    largest diagonal entry d: the padded eigenvalues (= d, with
+    lambda_max / K <= d <= lambda_max) change neither lambda_max nor which of
+    the system's own eigenvalues pass rcond * lambda_max, and with a zero
+    right-hand side there the solution is zero in the padding, so every
+    system gets exactly its stand-alone pseudoinverse."""
+    if not decs:
+        return
+    if len({d.rcond for d in decs}) > 1:
+        by_r = defaultdict(list)
+        for d in decs:
+            by_r[d.rcond].append(d)
+        for group in by_r.values():
+            pinv_bucketed(group, s)
+        return
+    dev = decs[0].M.device
+    for Kp, idx in pinv_buckets([d.K for d in decs]):
+        per = max(1, int(PINV_BATCH_BYTES // (Kp * Kp * 8)))
+        for c0 in range(0, len(idx), per):
+            chunk = [decs[i] for i in idx[c0:c0 + per]]
+            B = len(chunk)
+            Mb = torch.zeros((B, Kp, Kp), dtype=torch.float64, device=dev)
+            bb = torch.zeros((B, Kp), dtype=torch.float64, device=dev)
+            for z, d in enumerate(chunk):
+                K = d.K
+                call("vtb_coeff_realify", dptr(d.M), K, K, dptr(d.Mr), K, 1, s)
+                Mb[z, :K, :K].copy_(d.Mr)
+                if K < Kp:
+                    Mb[z].diagonal()[K:] = d.Mr.diagonal().max()
+                bb[z, :K].copy_(d.br)
+            xb = torch.empty_like(bb)
+            nb = np.zeros(1, np.int64)
+            call("vtb_sym_pinv_batched_workspace", Kp, B, nb.ctypes.data)
+            work = torch.empty(int(nb[0]), dtype=torch.uint8, device=dev)
+            kept = torch.zeros(B, dtype=torch.int32, device=dev)
+            infos = torch.zeros(B, dtype=torch.int32, device=dev)
+            call("vtb_sym_pinv_batched", dptr(Mb), dptr(bb), dptr(xb), Kp, B, chunk[0].rcond, dptr(work),
+                 int(nb[0]), dptr(kept), dptr(infos), s)
+            if int(infos.ne(0).sum()) != 0:
+                raise fast.VtbError("vtb_sym_pinv_batched", fast.VTB_NOT_CONVERGED)
+            for z, d in enumerate(chunk):
+                d.xr.copy_(xb[z, :d.K])
+                call("vtb_coeff_unrealify_vec", dptr(d.xr), d.K, 1, dptr(d.a), 0, s)
+                d.kept.copy_(kept[z:z + 1] - (Kp - d.K))
 
 
 class BatchDecoder(object):
@@ -299,11 +380,14 @@ class BatchDecoder(object):
             self._worker_streams[tid] = st
         return st
 
-    def _float64(self, i, after=None):
-        """Float64 decode of clip i (spike-space pseudoinverse, or Cholesky /
-        eigen-pseudoinverse of its real system) on a worker thread."""
+    def _float64(self, i, after=None, eig=True):
+        """Float64 decode of clip i on a worker thread: the spike-space
+        pseudoinverse (fewer intervals than coefficients), else Cholesky of
+        its real system and, when ``eig``, the eigen-pseudoinverse if the
+        Cholesky is refused.  Returns (solved, event)."""
         torch.cuda.set_device(self.device)
         st = self._worker_stream()
+        ok = True
         with torch.cuda.stream(st):
             if after is not None:
                 st.wait_event(after)
@@ -313,15 +397,19 @@ class BatchDecoder(object):
             if n < d.K:
                 d._solve_spike_space(s, p.spikes)
             else:
-                d.solver = "auto"
+                d.solver = "auto" if eig else "chol"
                 try:
                     d._solve(s, n)
+                    d.last_solver = "mixed->" + d.last_solver
+                except fast.VtbError as e:
+                    if eig or e.status != fast.VTB_NOT_CONVERGED:
+                        raise
+                    ok = False
                 finally:
                     d.solver = "mixed"
-                d.last_solver = "mixed->" + d.last_solver
             ev = torch.cuda.Event()
             ev.record(st)
-        return ev
+        return ok, ev
 
     # ---------------------------------------------------------- run
     def run(self, timing=False):
@@ -333,7 +421,7 @@ class BatchDecoder(object):
         ev = [torch.cuda.Event(enable_timing=timing) for _ in range(4)]
         ev[0].record(main)
         futs = [self._pool.submit(self._float64, i, ev[0]) for i in self.spike]
-        bad = []
+        bad, chol = [], []
         if self.plan is not None:
             if self._g1 is not None:
                 self._g1.replay()
@@ -341,11 +429,23 @@ class BatchDecoder(object):
                 self._stage_and_solve()
             ev[1].record(main)
             bad = [self.coeff[j] for j in self.plan.check()]
-            futs += [self._pool.submit(self._float64, i, ev[1]) for i in bad]
+            # float64 Cholesky first (concurrently); the systems it refuses are
+            # eigen-solved together, grouped by padded size
+            chol = [(i, self._pool.submit(self._float64, i, ev[1], False)) for i in bad]
         else:
             ev[1].record(main)
+        rest = []
+        for i, f in chol:
+            ok, e = f.result()
+            main.wait_event(e)
+            if not ok:
+                rest.append(i)
+        if rest:
+            pinv_bucketed([self.decs[i] for i in rest], stream_ptr())
+            for i in rest:
+                self.decs[i].last_solver = "mixed->eig-batched"
         for f in futs:
-            main.wait_event(f.result())
+            main.wait_event(f.result()[1])
         self.fallbacks = len(bad)
         ev[2].record(main)
         if self._g2 is not None:

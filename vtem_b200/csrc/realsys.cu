@@ -510,8 +510,8 @@ __global__ void dgemv_n_kernel(const double* __restrict__ V, int64_t ld, const d
     }
 }
 
-__global__ void dtruncate_kernel(const double* __restrict__ w, double* __restrict__ v, int n, double rcond,
-                                 int32_t* __restrict__ kept) {
+__device__ void dtruncate_body(const double* __restrict__ w, double* __restrict__ v, int n, double rcond,
+                               int32_t* __restrict__ kept) {
     __shared__ double s0;
     __shared__ int cnt;
     if (threadIdx.x == 0) {
@@ -532,6 +532,11 @@ __global__ void dtruncate_kernel(const double* __restrict__ w, double* __restric
     atomicAdd(&cnt, local);
     __syncthreads();
     if (threadIdx.x == 0 && kept) *kept = cnt;
+}
+
+__global__ void dtruncate_kernel(const double* __restrict__ w, double* __restrict__ v, int n, double rcond,
+                                 int32_t* __restrict__ kept) {
+    dtruncate_body(w, v, n, rcond, kept);
 }
 
 }  // namespace vtb
@@ -726,5 +731,120 @@ VTB_API int vtb_sym_pinv(double* M, int64_t ld, const double* b, double* x, int 
     dgemv_t_kernel<<<ceil_div((int64_t)K * 32, 256), 256, 0, s>>>(M, ld, b, K, rw.v1);
     dtruncate_kernel<<<1, 1024, 0, s>>>(rw.w, rw.v1, K, rcond, kept);
     dgemv_n_kernel<<<ceil_div(K, 32), 256, 0, s>>>(M, ld, rw.v1, K, x);
+    return launch_status();
+}
+
+// Batched eigen-pseudoinverse of `batch` real symmetric systems of one size K
+// (cuSOLVER XsyevBatched): x_z = V diag(1/w if |w| > rcond*max|w| else 0)
+// V^T b_z, the rule of vtb_sym_pinv per system.  M holds the matrices
+// contiguously (stride K*K, overwritten by the eigenvectors), b and x at
+// stride K; kept[z] (device, may be NULL) the kept counts, infos[z] (device)
+// the eigensolver's status.  Synchronises the stream (the host workspace of
+// the eigensolver must outlive the call).
+namespace vtb {
+static cusolverDnParams_t real_params() {
+    static thread_local cusolverDnParams_t p = nullptr;
+    if (!p && cusolverDnCreateParams(&p) != CUSOLVER_STATUS_SUCCESS) p = nullptr;
+    return p;
+}
+static int pinv_batched_real_sizes(cusolverDnHandle_t h, int K, int batch, size_t* db, size_t* hb) {
+    cusolverDnParams_t prm = real_params();
+    if (!prm) return VTB_CUDA_ERR;
+    if (cusolverDnXsyevBatched_bufferSize(h, prm, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, K, CUDA_R_64F,
+                                          nullptr, K, CUDA_R_64F, nullptr, CUDA_R_64F, db, hb, batch) !=
+        CUSOLVER_STATUS_SUCCESS)
+        return VTB_CUDA_ERR;
+    return VTB_OK;
+}
+// [w: batch*K][v: batch*K][info: batch][eigensolver work]
+static int64_t pinv_batched_real_layout(int K, int batch, size_t db) {
+    return al256r((int64_t)batch * K * 8) * 2 + al256r((int64_t)batch * 4) + al256r((int64_t)db);
+}
+
+__global__ void dgemv_t_batched_kernel(const double* __restrict__ V, int K, const double* __restrict__ x,
+                                       double* __restrict__ y) {
+    const int z = blockIdx.y;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= K) return;
+    const double* col = V + (int64_t)z * K * K + (int64_t)warp * K;
+    const double* xz = x + (int64_t)z * K;
+    double s = 0.0;
+    for (int i = lane; i < K; i += 32) s = fma(col[i], xz[i], s);
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[(int64_t)z * K + warp] = s;
+}
+
+__global__ void dgemv_n_batched_kernel(const double* __restrict__ V, int K, const double* __restrict__ x,
+                                       double* __restrict__ y) {
+    __shared__ double part[8][33];
+    const int z = blockIdx.y;
+    const double* Vz = V + (int64_t)z * K * K;
+    const double* xz = x + (int64_t)z * K;
+    const int row = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int g = threadIdx.x >> 5;
+    double s = 0.0;
+    if (row < K)
+        for (int c = g; c < K; c += 8) s = fma(Vz[(int64_t)c * K + row], xz[c], s);
+    part[g][threadIdx.x & 31] = s;
+    __syncthreads();
+    if (g == 0 && row < K) {
+        double t = 0.0;
+        for (int k = 0; k < 8; ++k) t += part[k][threadIdx.x & 31];
+        y[(int64_t)z * K + row] = t;
+    }
+}
+
+__global__ void dtruncate_batched_kernel(const double* __restrict__ w, double* __restrict__ v, int K, double rcond,
+                                         int32_t* __restrict__ kept) {
+    const int z = blockIdx.x;
+    dtruncate_body(w + (int64_t)z * K, v + (int64_t)z * K, K, rcond, kept ? kept + z : nullptr);
+}
+}  // namespace vtb
+
+VTB_API int vtb_sym_pinv_batched_workspace(int K, int batch, int64_t* bytes) {
+    VTB_CHECK_ARG(K > 0 && batch > 0 && bytes);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = real_solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    size_t db = 0, hb = 0;
+    int st = pinv_batched_real_sizes(h, K, batch, &db, &hb);
+    if (st) return st;
+    *bytes = pinv_batched_real_layout(K, batch, db);
+    return VTB_OK;
+}
+
+VTB_API int vtb_sym_pinv_batched(double* M, const double* b, double* x, int K, int batch, double rcond, void* work,
+                                 int64_t work_bytes, int32_t* kept, int32_t* infos, void* stream) {
+    VTB_CHECK_ARG(K > 0 && batch > 0 && M && b && x && work && infos && ((uintptr_t)work & 255) == 0);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    cusolverDnHandle_t h = real_solver_handle(dev);
+    if (!h) return VTB_CUDA_ERR;
+    size_t db = 0, hb = 0;
+    int st = pinv_batched_real_sizes(h, K, batch, &db, &hb);
+    if (st) return st;
+    VTB_CHECK_ARG(work_bytes >= pinv_batched_real_layout(K, batch, db));
+    char* base = reinterpret_cast<char*>(work);
+    double* w = reinterpret_cast<double*>(base);
+    double* v = reinterpret_cast<double*>(base + al256r((int64_t)batch * K * 8));
+    int* info = reinterpret_cast<int*>(base + 2 * al256r((int64_t)batch * K * 8));
+    void* wk = base + 2 * al256r((int64_t)batch * K * 8) + al256r((int64_t)batch * 4);
+    cudaStream_t s = as_stream(stream);
+    if (cusolverDnSetStream(h, s) != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    void* hwk = hb ? malloc(hb) : nullptr;
+    if (hb && !hwk) return VTB_OOM;
+    const cusolverStatus_t cs = cusolverDnXsyevBatched(h, real_params(), CUSOLVER_EIG_MODE_VECTOR,
+                                                       CUBLAS_FILL_MODE_LOWER, K, CUDA_R_64F, M, K, CUDA_R_64F, w,
+                                                       CUDA_R_64F, wk, db, hwk, hb, info, batch);
+    cudaError_t e1 = cudaStreamSynchronize(s);
+    free(hwk);
+    if (cs != CUSOLVER_STATUS_SUCCESS) return VTB_CUDA_ERR;
+    VTB_CUDA_TRY(e1);
+    VTB_CUDA_TRY(cudaMemcpyAsync(infos, info, (size_t)batch * 4, cudaMemcpyDeviceToDevice, s));
+    dgemv_t_batched_kernel<<<dim3(ceil_div((int64_t)K * 32, 256), batch), 256, 0, s>>>(M, K, b, v);
+    dtruncate_batched_kernel<<<batch, 1024, 0, s>>>(w, v, K, rcond, kept);
+    dgemv_n_batched_kernel<<<dim3(ceil_div(K, 32), batch), 256, 0, s>>>(M, K, v, x);
     return launch_status();
 }

@@ -64,6 +64,11 @@ def ellipse_storage_index(Mx, My):
     return np.array(idx, np.int32)
 
 
+def coefficient_count(Mx, My, Mt):
+    """K = (ellipse size) * (2 Mt + 1), the size of the coefficient system."""
+    return len(ellipse_storage_index(Mx, My)) * (2 * int(Mt) + 1)
+
+
 class CoeffDecoder(object):
     def __init__(self, Ds, h_norm, Mx, My, Wt, Mt, decPx, decPy, Px1, Py1, rcond=1e-8, solver="auto", refine=0,
                  device="cuda", mixed_sweeps=2):

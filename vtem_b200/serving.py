@@ -11,11 +11,15 @@ runs in ticks of ``tick_s`` (2 ms):
    an admitted request runs its first phase on a worker thread with its own
    CUDA stream: upload, RF projection on the tensor cores (split-bf16 from
    the float32 video), IAF block loop, spike pairing, Dirichlet coefficients
-   and the Kronecker Gram of its coefficient-space system;
+   and the tensor-core Kronecker Gram of its real coefficient system;
 2. at each tick the systems of every request whose first phase has finished
-   are solved together: requests with equal system size K share one batched
-   Cholesky call; a request whose pseudoinverse would truncate, or with fewer
-   intervals than coefficients, is solved alone by the eigen-pseudoinverse;
+   are solved together in mixed precision (vtem_b200.batch.MixedSolvePlan):
+   requests with equal system size K share one batched float32 Cholesky,
+   all share one batched triangular-solve launch per refinement sweep; a
+   request whose pseudoinverse might truncate goes to the solver thread
+   (float64 Cholesky, else the eigen-pseudoinverse batched over padded
+   sizes), and one with fewer intervals than coefficients was solved in the
+   spike space by its encoder;
 3. solved requests run their synthesis and the download of the video on
    their own stream; a request completes when its download has finished,
    and its memory returns to the budget.
@@ -111,16 +115,17 @@ class _InFlight(object):
 
 
 class _CholBatch(object):
-    """Handle of the batched Cholesky calls launched at one tick."""
+    """Handle of the grouped mixed solve launched at one tick."""
 
-    def __init__(self, jobs, flags_host, event):
-        self.jobs, self._flags, self._event = jobs, flags_host, event
+    def __init__(self, jobs, plan, host, event):
+        self.jobs, self._plan, self._host, self._event = jobs, plan, host, event
 
     def query(self):
         return self._event.query()
 
     def flags(self):
-        return self._flags.tolist()
+        bad = set(self._plan.evaluate(*(h.numpy() for h in self._host)))
+        return [i in bad for i in range(len(self.jobs))]
 
     @property
     def event(self):
@@ -131,7 +136,7 @@ class Server(object):
     """Request loop over one GPU (see the module docstring)."""
 
     def __init__(self, budget_bytes=120 * 10 ** 9, workers=2, tick_s=0.002, device="cuda", precision="bf16x3",
-                 switch_interval=2e-4):
+                 switch_interval=2e-4, sweeps=1):
         self.budget = int(budget_bytes)
         self.workers = int(workers)
         self.tick_s = float(tick_s)
@@ -140,6 +145,7 @@ class Server(object):
             dev = torch.device("cuda", torch.cuda.current_device())
         self.device = dev
         self.precision = precision
+        self.sweeps = int(sweeps)
         # the interpreter's thread switch interval while serving: shorter
         # than a kernel launch sequence, so that a thread with device work to
         # issue does not wait behind another thread's Python
@@ -162,69 +168,70 @@ class Server(object):
         with torch.cuda.stream(job.stream):
             V = req.video.to(self.device, non_blocking=True)
             p = batch.encode_clip_problem(req.workload, self.device, video=V, precision=self.precision)
-            d = fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver="chol")
-            s = stream_ptr()
             n = int(p.tk1.numel())
+            mixed = n >= fast.coefficient_count(p.prep.Mx, p.prep.My, p.Mt)
+            d = fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver="mixed" if mixed else "auto",
+                               mixed_sweeps=self.sweeps)
+            s = stream_ptr()
             if n < d.K:
-                d._solve_spike_space(s, (p.tk1, p.tk2, p.ind, n, p.kappa, p.delta, p.bias))
+                d._solve_spike_space(s, p.spikes)
                 req.solver = d.last_solver
             else:
-                call("vtb_coeff_temporal_gram", dptr(p.tk1), dptr(p.tk2), dptr(p.ind), n, d.N, dptr(p.kappa),
-                     dptr(p.delta), dptr(p.bias), dptr(d.norm), d.Mt, d.W, dptr(d.Wn), dptr(d.gn), s)
-                d._build_M(s)
-                d.a.copy_(d.b)
+                batch.stage_mixed(d, p, s)
             job.problem, job.dec = p, d
             job.ev_a = torch.cuda.Event()
             job.ev_a.record(job.stream)
 
     # -- phase 2: batched Cholesky (loop thread, solve stream) --------------
     def _launch_chol(self, jobs):
-        """Launch one batched Cholesky per system size over ``jobs`` (all with
-        a coefficient-space system) and return a handle whose ``query()``
-        tells when the factorisations are done and ``flags()`` then lists,
-        per job, whether its factorisation was refused."""
+        """Launch the grouped mixed-precision solve of ``jobs`` (all with a
+        coefficient-space system staged by the encoder): one batched float32
+        Cholesky per system size, batched triangular solves, float64
+        refinement sweeps; returns a handle whose ``query()`` tells when it
+        is done and ``flags()`` then lists, per job, whether the float64 path
+        must solve it instead."""
         with torch.cuda.stream(self._solve_stream):
             main = torch.cuda.current_stream(self.device)
             for j in jobs:
                 main.wait_event(j.ev_a)
-            s = stream_ptr()
-            groups = defaultdict(list)
-            for j in jobs:
-                groups[j.dec.K].append(j)
-            order, infos = [], []
-            for K, js in groups.items():
-                dev = self.device
-                mp = torch.as_tensor([j.dec.M.data_ptr() for j in js], dtype=torch.int64).to(dev,
-                                                                                             non_blocking=True)
-                bp = torch.as_tensor([j.dec.a.data_ptr() for j in js], dtype=torch.int64).to(dev,
-                                                                                             non_blocking=True)
-                inf = torch.zeros(len(js), dtype=torch.int32, device=dev)
-                sinfo = torch.zeros(1, dtype=torch.int32, device=dev)
-                call("vtb_herm_chol_batched", mp.data_ptr(), K, bp.data_ptr(), K, len(js),
-                     js[0].problem.rcond * fast.CHOL_MARGIN, dptr(inf), dptr(sinfo), s)
-                order.extend(js)
-                infos.append(inf)
-                self.batched_solves += 1
-                self.max_batch = max(self.max_batch, len(js))
-            flags_dev = torch.cat(infos).ne(0)
-            flags_host = torch.empty(flags_dev.shape, dtype=torch.bool, pin_memory=True)
-            flags_host.copy_(flags_dev, non_blocking=True)
+            plan = batch.MixedSolvePlan([j.dec for j in jobs], [j.problem for j in jobs], self.sweeps,
+                                        [self._solve_stream])
+            plan.launch()
+            host = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in plan.gather()]
+            for h, t in zip(host, plan.gather()):
+                h.copy_(t, non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(main)
-        return _CholBatch(order, flags_host, ev)
+            self.batched_solves += len(plan.groups)
+            self.max_batch = max([self.max_batch] + [len(g["idx"]) for g in plan.groups])
+        return _CholBatch(jobs, plan, host, ev)
 
     # -- phase 2b: eigen-pseudoinverse of refused systems (solver thread) ----
     def _eig(self, jobs):
-        """Truncated eigen-pseudoinverse of systems of one size (their
-        Cholesky was refused); runs on the solver thread and returns when
-        the solutions are on the device."""
+        """Float64 path for systems the mixed solve refused (solver thread):
+        float64 Cholesky where its pivot test passes, else the truncated
+        eigen-pseudoinverse, batched over padded sizes.  Returns when the
+        solutions are on the device."""
         with torch.cuda.stream(self._eig_stream):
             st = torch.cuda.current_stream(self.device)
             for j in jobs:
                 st.wait_event(j.ev_s)
-            info = fast.pinv_batched([j.dec for j in jobs])
-            if int(info.ne(0).sum()) != 0:
-                raise fast.VtbError("vtb_herm_pinv_batched", fast.VTB_NOT_CONVERGED)
+            s = stream_ptr()
+            rest = []
+            for j in jobs:
+                d = j.dec
+                d.solver = "chol"
+                try:
+                    d._solve(s, int(j.problem.tk1.numel()))
+                    d.last_solver = "mixed->chol"
+                except fast.VtbError as e:
+                    if e.status != fast.VTB_NOT_CONVERGED:
+                        raise
+                    rest.append(d)
+                    d.last_solver = "mixed->eig-batched"
+                finally:
+                    d.solver = "mixed"
+            batch.pinv_bucketed(rest, s)
             ev = torch.cuda.Event()
             ev.record(st)
         for j in jobs:
@@ -377,16 +384,16 @@ class Server(object):
                     if not cb.query():
                         still.append(cb)
                         continue
-                    refused = defaultdict(list)
+                    refused = []
                     for j, bad in zip(cb.jobs, cb.flags()):
                         j.ev_s = cb.event
                         if bad:
-                            refused[j.dec.K].append(j)
+                            refused.append(j)
                         else:
-                            j.req.solver = "chol-batched"
+                            j.req.solver = "mixed-batched"
                             to_synthesis(j)
-                    for js in refused.values():
-                        eig_q.put(js)
+                    if refused:
+                        eig_q.put(refused)
                 checking = still
                 for j in new_eig:
                     if j.req.error is not None:
