@@ -250,6 +250,7 @@ def run_ours(args, rank, world, local):
         plain = {}
         if not args.no_plain:
             plain = run_plain(w, prep, tk1, tk2, ind, {"mixed": umix, "coeff_f64": u64}, dev, Nt)
+        rnn = None if args.no_rnn else run_rnn(w, prep, tk1, tk2, ind, dev, Nt, steps=args.rnn_steps)
         snr_mix = plain.get("snr_db", {}).get("mixed")
         headline_mixed = snr_mix is None or snr_mix >= 40.0
         tot_ms = mix_ms if headline_mixed else f64_ms
@@ -285,6 +286,7 @@ def run_ours(args, rank, world, local):
                           "synthesis": sum(synth_ms) / args.steps, "encode_once": t_enc * 1e3},
             "clocks": clk,
             "plain_fp64": plain,
+            "rnn": rnn,
             "solver": {"mixed": decmix.last_solver, "f64": dec64.last_solver, "pivots": dec64.last_pivots},
             "near_threshold_events": int(sp.near_threshold),
         }
@@ -541,6 +543,49 @@ def run_plain(w, prep, tk1, tk2, ind, u_fast_variants, dev, Nt):
     return out
 
 
+def run_rnn(w, prep, tk1, tk2, ind, dev, Nt, steps=2000):
+    """The RNN decoder (rnn3, step 1/lambda_max, steps+1 updates) on the
+    whole clip: on the coefficient system (one cooperative launch) and on the
+    reference's n x n spike Gram, same step and updates; device seconds of
+    each (coefficients + synthesis) and the rel-L2 between the videos."""
+    import torch
+    from vtem_b200 import dirichlet, fast, neural_network
+    out = {"steps": steps}
+    try:
+        inputs = tuple(torch.as_tensor(x, device=dev) for x in (tk1, tk2, ind, w.kappa, w.delta, w.bias))
+        dec = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="auto")
+        dec.rnn_coefficients(*inputs, steps=10, assume_sorted=True)       # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a, dta = dec.rnn_coefficients(*inputs, steps=steps, assume_sorted=True)
+        u = dec.synthesize(a, w.T, w.dt)
+        e1.record()
+        torch.cuda.synchronize()
+        out["coeff_ms"] = e0.elapsed_time(e1)
+        out["dt_alpha"] = dta
+        out["coeff_voxels_per_s"] = Nt * w.Px * w.Py / (out["coeff_ms"] / 1e3)
+        cp = dirichlet.dirichlet(w.N, tk1, tk2, ind, w.kappa, w.delta, w.bias, np.ones(w.N), w.Wt, w.Mt)
+        torch.cuda.synchronize()
+        e0.record()
+        cp.compute_q()
+        cp.compute_G(prep.Dsw)
+        cp.d_q = neural_network.rnn3(cp.d_G, cp.d_q, dt=dta, alpha=1.0, steps=steps)
+        cp.freeG()
+        up = cp.reconstruct(prep.dirich, [0, w.T], w.dt)
+        e1.record()
+        torch.cuda.synchronize()
+        out["plain_ms"] = e0.elapsed_time(e1)
+        out["plain_voxels_per_s"] = Nt * w.Px * w.Py / (out["plain_ms"] / 1e3)
+        out["rel_l2_coeff_vs_plain"] = float((u - up.reshape(u.shape)).norm() / up.norm())
+        out["speedup"] = out["plain_ms"] / out["coeff_ms"]
+        del cp, up, u
+        torch.cuda.empty_cache()
+    except Exception as e:  # report, do not hide
+        out["error"] = repr(e)
+    return out
+
+
 # ---------------------------------------------------------------- CPU baseline
 
 def cpu_sample(w, prep, rd, window=0.04, frames=None, use_ref=False):
@@ -622,6 +667,8 @@ def main():
     ap.add_argument("--frames", type=int, default=10000)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-rnn", action="store_true")
+    ap.add_argument("--rnn-steps", type=int, default=2000)
     ap.add_argument("--sweeps", type=int, default=1)
     ap.add_argument("--workload", default="gpu", choices=["gpu", "batch", "serve"])
     ap.add_argument("--clips", type=int, default=256)

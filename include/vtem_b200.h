@@ -383,6 +383,18 @@ int vtb_sym_pinv_batched_workspace(int K, int batch, int64_t* bytes);
 int vtb_sym_pinv_batched(double* M, const double* b, double* x, int K, int batch, double rcond, void* work,
                          int64_t work_bytes, int32_t* kept, int32_t* infos, void* stream);
 
+/* RNN decoder on the real coefficient system: from x = 0, steps+1 updates
+ * x <- x + dt_alpha (br - Mr x), float64.  The same iterates as rnn3 on the
+ * spike Gram (vtem/neural_network.py:15-128) mapped by a = Phi^H c
+ * (Phi^H c_{i+1} = Phi^H c_i + dt_alpha (Phi^H q - Phi^H Phi Phi^H c_i)), on
+ * K x K instead of n x n.  One cooperative launch runs every update (rows of
+ * Mr cached in shared memory); x_tmp (K doubles) and bar (16 bytes) are
+ * scratch.  After the stream reaches the call's end, the int32 at byte
+ * offset 8 of bar is nonzero if a grid-barrier wait exceeded its limit (the
+ * result is then invalid). */
+int vtb_rnn_coeff(const double* Mr, int64_t ld, const double* br, double* x, double* x_tmp, int K, double dt_alpha,
+                  int steps, void* bar, void* stream);
+
 /* out (device) = ||dx|| / ||x||: the relative size of a refinement correction. */
 int vtb_norm_ratio(const double* dx, const double* x, int n, double* out, void* stream);
 /* y += x (n doubles). */

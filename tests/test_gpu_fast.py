@@ -195,3 +195,41 @@ def test_real_form_matches_hermitian_system():
     call("vtb_sym_potrs", dptr(dec.Mr), K, dptr(x64), K, 1, dptr(w1), w1.numel(), s)
     assert dec._read_stat()[0] == 0
     assert np.linalg.norm(x64.cpu().numpy() - xr) <= 1e-9 * np.linalg.norm(xr)
+
+
+def test_coefficient_rnn_matches_spike_rnn(small_encoded):
+    """The RNN decoder on the coefficient system gives the reconstruction of
+    the reference's rnn3 on the n x n spike Gram (same step, same number of
+    updates), and the float64 oracle's rnn3 + reconstruction."""
+    from vtem_b200 import dirichlet, neural_network
+    w, store, prep = small_encoded
+    rd = spike_store.vtem_storage_read(store)
+    rd.read_vrf_type()
+    rd.read_num_neurons()
+    rd.select_neurons([-0.5, 0.5, -0.5, 0.5])
+    tk1, tk2, ind, kap, dl, bia, sig = rd.read_select_spikes([0.0, w.T])
+    steps = 300
+    dec = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond)
+    a, dta = dec.rnn_coefficients(tk1, tk2, ind, kap, dl, bia, steps=steps)
+    u = dec.synthesize(a, w.T, w.dt)
+    norm = np.ones(w.N)
+    cp = dirichlet.dirichlet(w.N, tk1, tk2, ind, kap, dl, bia, norm, w.Wt, w.Mt)
+    cp.compute_q()
+    cp.compute_G(prep.Dsw)
+    G = cp.d_G
+    lam = torch.linalg.eigvalsh(G)[-1].item()
+    # the power-iteration estimate of lambda_max (shared by G and M) is a
+    # lower bound close to it: a stable step below 2 / lambda_max
+    assert 0.5 < 1.0 / (lam * dta) <= 1.0 + 1e-9
+    cp.d_q = neural_network.rnn3(G, cp.d_q, dt=dta, alpha=1.0, steps=steps)
+    up = cp.reconstruct(prep.dirich, [0, w.T], w.dt)
+    rel = ((u - up.reshape(u.shape)).norm() / up.norm()).item()
+    assert rel < 1e-9, rel
+    # oracle: rnn3 and the reference's reconstruction formula in float64 numpy
+    q = O.compute_q(tk1, tk2, ind, kap, dl, bia, norm)
+    Go = O.compute_G(tk1, tk2, ind, prep.Dsw.cpu().numpy(), w.Wt, w.Mt)
+    co = O.rnn3(Go, q, dta, 1.0, steps)
+    t = np.arange(0, w.T, w.dt)
+    uo = O.reconstruct_factored(prep.dirich.cpu().numpy(), tk1, tk2, co.ravel(), t, ind, norm, w.Mt, w.Wt / w.Mt)
+    rel_o = np.linalg.norm(u.cpu().numpy().ravel() - uo.ravel()) / np.linalg.norm(uo)
+    assert rel_o < 1e-8, rel_o

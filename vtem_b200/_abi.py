@@ -82,6 +82,7 @@ SIGNATURES = {
     "vtb_sym_potrs_batched": [P, I, I, P],
     "vtb_sym_pinv_batched_workspace": [I, I, P],
     "vtb_sym_pinv_batched": [P, P, P, I, I, D, P, L, P, P, P],
+    "vtb_rnn_coeff": [P, L, P, P, P, I, D, I, P, P],
     "vtb_sym_dinv_floats": [I],  # restype int64, set in lib()
 }
 

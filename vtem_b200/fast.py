@@ -316,6 +316,56 @@ class CoeffDecoder(object):
             self.last_solver = "eig"
             return
 
+    def lambda_max(self, iters=40):
+        """Largest eigenvalue of the float64 real system Mr (that of the
+        spike Gram G = Phi Phi^H as well) by power iteration from a fixed
+        start; Mr must be built (``_build_real``)."""
+        v = torch.ones(self.K, dtype=F64, device=self.Mr.device)
+        lam = torch.zeros((), dtype=F64, device=v.device)
+        for _ in range(iters):
+            w = torch.mv(self.Mr, v)
+            lam = torch.dot(v, w) / torch.dot(v, v)
+            v = w / w.norm()
+        return float(lam)
+
+    def _build_real(self, s):
+        """Float64 M, b and their real forms Mr, br."""
+        self._build_M(s)
+        call("vtb_coeff_realify_vec", dptr(self.b), self.K, 1, dptr(self.br), s)
+        call("vtb_coeff_realify", dptr(self.M), self.K, self.K, dptr(self.Mr), self.K, 1, s)
+
+    def rnn_coefficients(self, tk1, tk2, neuron_ind, kappa, delta, bias, dt_alpha=None, steps=4000,
+                         assume_sorted=False):
+        """Reconstruction coefficients of the RNN decoder (rnn3,
+        vtem/neural_network.py:15-99: steps+1 gradient-flow updates from
+        c = 0 with step dt*alpha) run on the coefficient system: the same
+        iterates mapped by a = Phi^H c.  ``dt_alpha`` None takes
+        1 / lambda_max (power iteration).  Returns (a, dt_alpha)."""
+        if assume_sorted:
+            ind = neuron_ind
+        else:
+            perm, tk1, tk2, ind = sort_by_neuron(tk1, tk2, neuron_ind)
+        n = int(tk1.numel())
+        if n == 0:
+            raise ValueError("no spikes to decode")
+        dev = self.M.device
+        kap, dl, bi = (torch.as_tensor(np.asarray(x, np.float64), device=dev) if not isinstance(x, torch.Tensor)
+                       else x for x in (kappa, delta, bias))
+        s = stream_ptr()
+        call("vtb_coeff_temporal_gram", dptr(tk1), dptr(tk2), dptr(ind), n, self.N, dptr(kap), dptr(dl), dptr(bi),
+             dptr(self.norm), self.Mt, self.W, dptr(self.Wn), dptr(self.gn), s)
+        self._build_real(s)
+        if dt_alpha is None:
+            dt_alpha = 1.0 / self.lambda_max()
+        bar = torch.zeros(4, dtype=torch.int32, device=dev)
+        call("vtb_rnn_coeff", dptr(self.Mr), self.K, dptr(self.br), dptr(self.xr), dptr(self.rr), self.K,
+             float(dt_alpha), int(steps), dptr(bar), s)
+        call("vtb_coeff_unrealify_vec", dptr(self.xr), self.K, 1, dptr(self.a), 0, s)
+        if int(bar[2].item()) != 0:
+            raise VtbError("vtb_rnn_coeff", _abi.VTB_TIMEOUT)
+        self.last_solver = "rnn"
+        return self.a, float(dt_alpha)
+
     def synthesize(self, a, T, dt, t0=0.0, out=None, out_dtype=F64):
         """Video (Nt, decPy, decPx) at t = t0 + arange(0, T, dt)."""
         Nt = len(np.arange(0, T, dt))
