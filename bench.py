@@ -251,6 +251,7 @@ def run_ours(args, rank, world, local):
         if not args.no_plain:
             plain = run_plain(w, prep, tk1, tk2, ind, {"mixed": umix, "coeff_f64": u64}, dev, Nt)
         rnn = None if args.no_rnn else run_rnn(w, prep, tk1, tk2, ind, dev, Nt, steps=args.rnn_steps)
+        encode = run_encode(w, V, dev)
         snr_mix = plain.get("snr_db", {}).get("mixed")
         headline_mixed = snr_mix is None or snr_mix >= 40.0
         tot_ms = mix_ms if headline_mixed else f64_ms
@@ -287,6 +288,7 @@ def run_ours(args, rank, world, local):
             "clocks": clk,
             "plain_fp64": plain,
             "rnn": rnn,
+            "encode": encode,
             "solver": {"mixed": decmix.last_solver, "f64": dec64.last_solver, "pivots": dec64.last_pivots},
             "near_threshold_events": int(sp.near_threshold),
         }
@@ -543,6 +545,75 @@ def run_plain(w, prep, tk1, tk2, ind, u_fast_variants, dev, Nt):
     return out
 
 
+def run_encode(w, V, dev, reps=5):
+    """Encoder stages on the clip, device-timed: the RF projection
+    L = dx dy V RF^T in float64 and on the tensor cores (split-bf16 operands,
+    fp32 accumulation), and the IAF block scan (float64) on the float64
+    projection; the rel. error of the tensor-core projection and how many
+    spikes its scan changes."""
+    import torch
+    from vtem_b200 import ensemble_encode, vrf
+    g = w.gabor
+    banks = []
+    gb = vrf.vrf_gabor((w.Py, w.Px), dx=w.dx, dy=w.dy)
+    gb.load_parameters(num_neurons=len(g.h_alpha), h_alpha=g.h_alpha, h_l=g.h_l, h_x0=g.h_x0, h_y0=g.h_y0,
+                       h_ab=g.h_ab, KAPPA=g.KAPPA, h_gain=g.gain)
+    banks.append(gb)
+    if w.cs is not None:
+        c = w.cs
+        cb = vrf.vrf_cs((w.Py, w.Px), dx=w.dx, dy=w.dy)
+        cb.load_parameters(num_neurons=len(c.h_alpha), h_alpha=c.h_alpha, h_x0=c.h_x0, h_y0=c.h_y0,
+                           sigma_center=c.sigma_center, sigma_surround=c.sigma_surround, h_gain=c.gain)
+        banks.append(cb)
+    bank = vrf.vrf_bank(banks) if len(banks) > 1 else banks[0]
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / reps
+
+    L64, t64 = timed(lambda: bank.filter(V, out_layout="neuron", precision="f64"))
+    Ltc, ttc = timed(lambda: bank.filter(V, out_layout="neuron", precision="bf16x3"))
+    flop = 2.0 * w.F * w.Px * w.Py * w.N
+
+    def scan(L):
+        iaf = ensemble_encode.IAF_encode(w.N, w.dt)
+        iaf.load_parameters(h_kappa=w.kappa, h_bias=w.bias, h_delta=w.delta, h_v0=w.v0)
+        return iaf.encode_blocks(L, block_frames=min(101, w.F + 1), layout="neuron")
+
+    sp64, tscan = timed(lambda: scan(L64))
+    sptc = scan(Ltc)
+    n64, ntc = int(sp64.count.sum()), int(sptc.count.sum())
+    peaks = load_peaks()
+    return {"rf_projection": {"f64_ms": t64, "tensor_core_ms": ttc, "algorithmic_gflop": flop / 1e9,
+                              "f64_tflops": flop / t64 / 1e9, "tensor_core_tflops": flop / ttc / 1e9,
+                              "tensor_core_frac_of_bf16_peak": 3 * flop / ttc / 1e9 / peaks["bf16_tflops"],
+                              "tensor_core_rel_err": float((Ltc - L64).norm() / L64.norm())},
+            "iaf_scan": {"ms": tscan, "bytes_read": 8 * w.F * w.N, "gbs": 8.0 * w.F * w.N / tscan / 1e6,
+                         "frac_of_hbm": 8.0 * w.F * w.N / tscan / 1e6 / peaks["hbm_gbs"],
+                         "spikes": n64, "near_threshold": int(sp64.near_threshold)},
+            "spikes_tensor_core_projection": ntc}
+
+
+def run_encode_only(args, rank, world, local):
+    """Encoder stages alone on the GPU configuration's clip (run_encode)."""
+    import torch
+    from vtem_b200 import workloads
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = workloads.gpu_scale(seed=rank, frames=args.frames)
+    V = w.video(device=dev)
+    res = run_encode(w, V, dev, reps=max(1, args.steps))
+    res["config"] = {"workload": "encode: 64x64 px, %d samples, 768 Gabor + 256 centre-surround RFs" % w.F}
+    return res
+
+
 def run_rnn(w, prep, tk1, tk2, ind, dev, Nt, steps=2000):
     """The RNN decoder (rnn3, step 1/lambda_max, steps+1 updates) on the
     whole clip: on the coefficient system (one cooperative launch) and on the
@@ -670,7 +741,7 @@ def main():
     ap.add_argument("--no-rnn", action="store_true")
     ap.add_argument("--rnn-steps", type=int, default=2000)
     ap.add_argument("--sweeps", type=int, default=1)
-    ap.add_argument("--workload", default="gpu", choices=["gpu", "batch", "serve"])
+    ap.add_argument("--workload", default="gpu", choices=["gpu", "batch", "serve", "encode"])
     ap.add_argument("--clips", type=int, default=256)
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=200.0)
@@ -686,6 +757,8 @@ def main():
         res = run_batch(args, rank, world, local)
     elif args.workload == "serve":
         res = run_serve(args, rank, world, local)
+    elif args.workload == "encode":
+        res = run_encode_only(args, rank, world, local)
     else:
         res = run_ours(args, rank, world, local)
     if rank == 0 and res is not None:

@@ -58,3 +58,33 @@ def test_rf_filter_split_bf16_matches_f64():
     got = gb.filter(V, out_layout="neuron", precision="bf16x3")
     rel = ((got - ref).norm() / ref.norm()).item()
     assert rel < 5e-5, rel
+
+
+@pytest.mark.parametrize("bn", [64, 96, 128, 160, 192, 256])
+def test_every_tile_width_is_exact_on_bf16_inputs(bn):
+    """Each tile width the autotuner may pick computes the same product
+    (bf16-exact operands: fp32 accumulation is exact), with partial edge tiles
+    in both directions."""
+    from vtem_b200._abi import call, dptr, stream_ptr
+    rng = np.random.default_rng(bn)
+    M, N, K = 300, 289, 256
+    A = torch.as_tensor(rng.integers(-8, 9, (M, K)).astype(np.float32) / 8, device="cuda").to(torch.bfloat16)
+    B = torch.as_tensor(rng.integers(-8, 9, (N, K)).astype(np.float32) / 8, device="cuda").to(torch.bfloat16)
+    out = torch.zeros((M, N), dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    call("vtb_tc_gemm_bf16_bn", dptr(A), M, dptr(B), N, K, dptr(out), N, 1, 0, 1.0, 0, dptr(err), bn, stream_ptr())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(out.double(), A.double() @ B.double().T)
+
+
+def test_autotuner_picks_a_candidate_and_caches_it():
+    from vtem_b200 import autotune
+    rng = np.random.default_rng(1)
+    A = torch.as_tensor(rng.standard_normal((513, 200)), device="cuda")
+    B = torch.as_tensor(rng.standard_normal((289, 200)), device="cuda")
+    C1 = tc.gemm_split_bf16(A, B)
+    key = autotune._key(513, 289, tc.padded_k(200) * 3, True)
+    assert autotune._cache[key] in autotune.CANDIDATES
+    C2 = tc.gemm_split_bf16(A, B)           # cached choice: same result
+    assert torch.equal(C1, C2)

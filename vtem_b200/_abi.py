@@ -57,6 +57,7 @@ SIGNATURES = {
     "vtb_coeff_synthesize_noalloc": [P, P, I, I, I, I, D, D, D, I, I, I, I, I, P, I, P],
     "vtb_split_bf16x3": [P, I, I, I, L, L, D, I, P, P],
     "vtb_tc_gemm_bf16": [P, I, P, I, I, P, L, L, I, D, I, P, P],
+    "vtb_tc_gemm_bf16_bn": [P, I, P, I, I, P, L, L, I, D, I, P, I, P],
     "vtb_coeff_lhs_split": [P, I, I, P, P, I, P, P],
     "vtb_coeff_wn_split": [P, I, I, P, P],
     "vtb_coeff_scatter": [P, L, P, P, I, I, P, L, P],

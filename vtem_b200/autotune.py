@@ -1,0 +1,109 @@
+"""Autotuner for the tensor-core GEMM's output tile width.
+
+``vtb_tc_gemm_bf16_bn`` is built for output tiles of 128 rows by BN columns
+with BN in :data:`CANDIDATES`.  The best BN depends on the problem: the
+Kronecker Gram of the decoder has only (2 Mt + 1)^2 columns (289 at Mt = 8),
+where a width that divides them evenly wastes no tensor-core work, while the
+RF projection has hundreds of RF columns and many rows.  ``tile_for`` times
+every candidate on the caller's own operands (CUDA events, a few launches
+each) the first time a shape is seen, and reuses the choice afterwards; the
+choices are kept per process and, when ``VTB_AUTOTUNE_CACHE`` names a file,
+in that JSON file across processes.  ``VTB_AUTOTUNE=0`` disables tuning
+(BN = 128).  Tuning launches and synchronises, so it must not run inside a
+CUDA graph capture: callers run once eagerly before capturing.
+"""
+from __future__ import annotations
+
+import json
+import os
+import threading
+
+import torch
+
+from ._abi import call
+
+CANDIDATES = (64, 96, 128, 160, 192, 256)
+DEFAULT_BN = 128
+
+_lock = threading.Lock()
+_cache = {}
+_loaded = False
+timings = {}      # shape -> {bn: ms}, for reports
+
+
+def _key(M, N, K, out_f64):
+    return "%d,%d,%d,%d" % (M, N, K, int(bool(out_f64)))
+
+
+def _load():
+    global _loaded
+    if _loaded:
+        return
+    _loaded = True
+    path = os.environ.get("VTB_AUTOTUNE_CACHE")
+    if path and os.path.exists(path):
+        try:
+            with open(path) as f:
+                _cache.update({k: int(v) for k, v in json.load(f).items()})
+        except (OSError, ValueError):
+            pass
+
+
+def _save():
+    path = os.environ.get("VTB_AUTOTUNE_CACHE")
+    if not path:
+        return
+    try:
+        with open(path, "w") as f:
+            json.dump(_cache, f, indent=1, sort_keys=True)
+    except OSError:
+        pass
+
+
+def tile_for(M, N, K, out_f64, launch, reps=3):
+    """BN for the GEMM (M x K) @ (N x K)^T; ``launch(bn)`` issues one GEMM
+    with tile width bn on the current stream (raising on a bad status)."""
+    if os.environ.get("VTB_AUTOTUNE", "1") == "0":
+        return DEFAULT_BN
+    key = _key(M, N, K, out_f64)
+    with _lock:
+        _load()
+        if key in _cache:
+            return _cache[key]
+    if torch.cuda.is_current_stream_capturing():
+        return DEFAULT_BN
+    res = {}
+    for bn in CANDIDATES:
+        if bn > 2 * max(N, 64) and bn != DEFAULT_BN:
+            continue          # wider than twice the problem: only padding
+        launch(bn)            # warm-up (kernel attributes, instruction cache)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            launch(bn)
+        e1.record()
+        e1.synchronize()
+        res[bn] = e0.elapsed_time(e1) / reps
+    best = min(res, key=res.get)
+    with _lock:
+        _cache[key] = best
+        timings[key] = res
+        _save()
+    return best
+
+
+def gemm_bf16_tuned(A3, M, B3, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err_ptr, stream):
+    """vtb_tc_gemm_bf16_bn with the tuned tile width for this shape."""
+    def launch(bn):
+        call("vtb_tc_gemm_bf16_bn", A3, M, B3, N, K, C, c_m, c_n, int(out_f64), float(alpha), int(accumulate),
+             err_ptr, int(bn), stream)
+
+    if accumulate:
+        # tuning launches repeatedly: only a non-accumulating GEMM may be tuned
+        with _lock:
+            _load()
+            bn = _cache.get(_key(M, N, K, out_f64), DEFAULT_BN)
+    else:
+        bn = tile_for(M, N, K, out_f64, launch)
+    launch(bn)
+    return bn

@@ -36,7 +36,7 @@ from concurrent.futures import ThreadPoolExecutor
 import numpy as np
 import torch
 
-from . import fast
+from . import autotune, fast
 from ._abi import call, dptr, lib, stream_ptr
 
 TRSV_DESC = np.dtype([("L", "<u8"), ("Dinv", "<u8"), ("x", "<u8"), ("ld", "<i8"), ("K", "<i4"), ("pad", "<i4")])
@@ -74,8 +74,8 @@ def stage_mixed(d, p, s):
     call("vtb_coeff_rhs", dptr(d.d), d.N, d.Ks, dptr(d.gn), d.Kt, dptr(d.b), s)
     call("vtb_coeff_realify_vec", dptr(d.b), K, 1, dptr(d.br), s)
     call("vtb_coeff_wn_split", dptr(d.Wn), d.N, d.Kt, dptr(d.R3), s)
-    call("vtb_tc_gemm_bf16", dptr(d.L3), 2 * d.npairs, dptr(d.R3), KK, 3 * d.Kp2, dptr(d.C), KK, 1, 0, 1.0, 0,
-         d._stat_ptr(7), s)
+    autotune.gemm_bf16_tuned(dptr(d.L3), 2 * d.npairs, dptr(d.R3), KK, 3 * d.Kp2, dptr(d.C), KK, 1, 0, 1.0, 0,
+                             d._stat_ptr(7), s)
     call("vtb_coeff_real_scatter", dptr(d.C), KK, d.Ks, d.Kt, dptr(d.Mr32), K, 0, s)
     d.xr.copy_(d.br)
 

@@ -191,12 +191,26 @@ __global__ void __launch_bounds__(256) kron_rhs_kernel(const double2* __restrict
     for (int m0 = 0; m0 < Kt; m0 += 32) {
         const int m = m0 + lane;
         double2 acc = make_double2(0, 0);
-        if (m < Kt)
-            for (int n = w; n < N; n += 8) {
-                const double2 p = cmul(d[(int64_t)n * Ks + s], gn[(int64_t)n * Kt + m]);
-                acc.x += p.x;
-                acc.y += p.y;
+        if (m < Kt) {
+            // four independent partial sums keep eight loads in flight per lane
+            double2 a4[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+            int n = w;
+            for (; n + 24 < N; n += 32) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int nu = n + 8 * u;
+                    const double2 p = cmul(d[(int64_t)nu * Ks + s], gn[(int64_t)nu * Kt + m]);
+                    a4[u].x += p.x;
+                    a4[u].y += p.y;
+                }
             }
+            for (; n < N; n += 8) {
+                const double2 p = cmul(d[(int64_t)n * Ks + s], gn[(int64_t)n * Kt + m]);
+                a4[0].x += p.x;
+                a4[0].y += p.y;
+            }
+            acc = make_double2((a4[0].x + a4[1].x) + (a4[2].x + a4[3].x), (a4[0].y + a4[1].y) + (a4[2].y + a4[3].y));
+        }
         part[w][lane] = acc;
         __syncthreads();
         if (w == 0 && m < Kt) {

@@ -256,7 +256,7 @@ static int64_t al256r(int64_t x) { return (x + 255) & ~(int64_t)255; }
 //   backward (L^T x = y): warp w forms the dot product of column J*32+w below
 //            the block with the solved tail, then x_J = Dinv_J^T (y_J - s).
 // Dinv_J = L_JJ^-1 (32 x 32, row-major) is formed once per factorisation by
-// diag_inv_kernel.  Every read of L is a coalesced column segment.
+// diag_inv_batched_kernel.  Every read of L is a coalesced column segment.
 constexpr int kTrsvThreads = 1024;
 constexpr int kTrsvPrefetchRows = 1;
 
@@ -292,10 +292,6 @@ __device__ void diag_inv_body(const float* __restrict__ L, int64_t ld, int K, fl
     for (int r = 0; r < 32; ++r) Dinv[(int64_t)J * 1024 + r * 32 + lane] = X[r];
 }
 
-__global__ void __launch_bounds__(128) diag_inv_kernel(const float* __restrict__ L, int64_t ld, int K,
-                                                       float* __restrict__ Dinv) {
-    diag_inv_body(L, ld, K, Dinv);
-}
 
 // Solves in place on the float32 vector r (shared memory, K entries); part
 // is 32 floats of shared scratch.  Requires blockDim.x == kTrsvThreads.
@@ -412,14 +408,13 @@ __global__ void __launch_bounds__(128) diag_inv_batched_kernel(float* const* __r
 
 static int64_t dinv_floats(int K) { return (int64_t)((K + 31) / 32) * 1024; }
 
-// Workspace: [info 256][vec f32: K floats][w: K doubles][v1: K doubles][Dinv (mode 2)][lapack work]
+// Workspace: [info 256][vec f32: K floats][w: K doubles][v1: K doubles][lapack work]
 
 struct RealWork {
     int* info;
     float* vf;
     double* w;
     double* v1;
-    float* dinv;  // mode 2: inverses of the factor's 32 x 32 diagonal blocks
     void* wk;
     int lwork;   // elements of the factorisation's / eigensolver's work type
 };
@@ -447,14 +442,12 @@ static int64_t real_layout(int K, int mode, int lwork, char* base, RealWork* rw)
     const int64_t of = take((int64_t)K * 4);
     const int64_t ow = take((int64_t)K * 8);
     const int64_t o1 = take((int64_t)K * 8);
-    const int64_t od = take(mode == 2 ? dinv_floats(K) * 4 : 0);
     const int64_t ok = take((int64_t)lwork * (mode == 2 ? 4 : 8));
     if (base && rw) {
         rw->info = reinterpret_cast<int*>(base + oi);
         rw->vf = reinterpret_cast<float*>(base + of);
         rw->w = reinterpret_cast<double*>(base + ow);
         rw->v1 = reinterpret_cast<double*>(base + o1);
-        rw->dinv = reinterpret_cast<float*>(base + od);
         rw->wk = base + ok;
         rw->lwork = lwork;
     }
@@ -619,7 +612,6 @@ VTB_API int vtb_sym_factor(void* M, int64_t ld, int K, int mode, double rcond, v
     else {
         pivot_flag_kernel<float><<<1, 1024, 0, s>>>(reinterpret_cast<const float*>(M), ld, K, rw.info, rcond, pivots,
                                                     flag);
-        diag_inv_kernel<<<ceil_div((K + 31) / 32, 4), 128, 0, s>>>(reinterpret_cast<const float*>(M), ld, K, rw.dinv);
     }
     return launch_status();
 }

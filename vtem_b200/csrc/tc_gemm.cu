@@ -297,20 +297,40 @@ VTB_API int vtb_split_bf16x3(const void* src, int src_f32, int rows, int K, int6
     return launch_status();
 }
 
-VTB_API int vtb_tc_gemm_bf16(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
-                             int out_f64, double alpha, int accumulate, int32_t* err, void* stream) {
+template <int BN>
+static int tc_dispatch(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
+                       int out_f64, double alpha, int accumulate, int32_t* err, cudaStream_t s) {
+    CUtensorMap ma, mb;
+    int st = make_map(&ma, A, M, K, K, kTcBM);
+    if (st) return st;
+    st = make_map(&mb, B, N, K, K, BN);
+    if (st) return st;
+    if (out_f64)
+        return launch_tc<BN, double>(ma, mb, M, N, K, reinterpret_cast<double*>(C), c_m, c_n, alpha, accumulate, err, s);
+    return launch_tc<BN, float>(ma, mb, M, N, K, reinterpret_cast<float*>(C), c_m, c_n, alpha, accumulate, err, s);
+}
+
+// Output tile widths the kernel is built for (M tile = 128): the autotuner
+// of vtem_b200.autotune picks one per problem shape.
+VTB_API int vtb_tc_gemm_bf16_bn(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
+                                int out_f64, double alpha, int accumulate, int32_t* err, int bn, void* stream) {
     VTB_CHECK_ARG(M >= 0 && N >= 0 && K > 0 && (K % kTcBK) == 0);
     if (M == 0 || N == 0) return VTB_OK;
     VTB_CHECK_ARG(A && B && C && err && ((uintptr_t)A & 15) == 0 && ((uintptr_t)B & 15) == 0);
     VTB_CHECK_ARG(ceil_div(M, kTcBM) <= 65535);
-    CUtensorMap ma, mb;
-    int st = make_map(&ma, A, M, K, K, kTcBM);
-    if (st) return st;
-    constexpr int BN = 128;
-    st = make_map(&mb, B, N, K, K, BN);
-    if (st) return st;
     cudaStream_t s = as_stream(stream);
-    if (out_f64)
-        return launch_tc<BN, double>(ma, mb, M, N, K, reinterpret_cast<double*>(C), c_m, c_n, alpha, accumulate, err, s);
-    return launch_tc<BN, float>(ma, mb, M, N, K, reinterpret_cast<float*>(C), c_m, c_n, alpha, accumulate, err, s);
+    switch (bn) {
+        case 64: return tc_dispatch<64>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 96: return tc_dispatch<96>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 128: return tc_dispatch<128>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 160: return tc_dispatch<160>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 192: return tc_dispatch<192>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 256: return tc_dispatch<256>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        default: return VTB_BAD_ARG;
+    }
+}
+
+VTB_API int vtb_tc_gemm_bf16(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
+                             int out_f64, double alpha, int accumulate, int32_t* err, void* stream) {
+    return vtb_tc_gemm_bf16_bn(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, 128, stream);
 }

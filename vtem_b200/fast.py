@@ -36,7 +36,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import _abi
+from . import _abi, autotune
 from ._abi import VTB_NOT_CONVERGED, VtbError, call, dptr, stream_ptr
 from .dirichlet import sort_by_neuron
 
@@ -133,6 +133,19 @@ class CoeffDecoder(object):
         self.r = torch.empty((self.K,), dtype=C128, device=device)
         self.Mr32 = torch.empty((self.K, self.K), dtype=torch.float32, device=device)
 
+    def set_norm(self, h_norm):
+        """Per-neuron weights norm (vtem/vtdm.py:634-638, 1/(kappa sigma) for
+        random-threshold encoders): repacks d = norm * Ds and the operands
+        derived from it."""
+        dev = self.M.device
+        self.norm = torch.as_tensor(np.asarray(h_norm, np.float64), device=dev).contiguous()
+        call("vtb_coeff_pack", dptr(self.Ds), self.N, self.Kfull, dptr(self.smap), self.Ks, dptr(self.norm),
+             dptr(self.d), stream_ptr())
+        self._dsw = None
+        if self.solver == "mixed":
+            call("vtb_coeff_lhs_split", dptr(self.d), self.N, self.Ks, dptr(self.ps), dptr(self.ps2), self.npairs,
+                 dptr(self.L3), stream_ptr())
+
     def _workspace(self, mode):
         """Workspace of the real-form solver: mode 0 eigen, 1 float64
         Cholesky, 2 float32 Cholesky."""
@@ -208,8 +221,8 @@ class CoeffDecoder(object):
         call("vtb_coeff_rhs", dptr(self.d), self.N, self.Ks, dptr(self.gn), self.Kt, dptr(self.b), s)
         call("vtb_coeff_realify_vec", dptr(self.b), K, 1, dptr(self.br), s)
         call("vtb_coeff_wn_split", dptr(self.Wn), self.N, self.Kt, dptr(self.R3), s)
-        call("vtb_tc_gemm_bf16", dptr(self.L3), 2 * self.npairs, dptr(self.R3), KK, 3 * self.Kp2, dptr(self.C), KK, 1,
-             0, 1.0, 0, self._stat_ptr(7), s)
+        autotune.gemm_bf16_tuned(dptr(self.L3), 2 * self.npairs, dptr(self.R3), KK, 3 * self.Kp2, dptr(self.C), KK, 1,
+                                 0, 1.0, 0, self._stat_ptr(7), s)
         call("vtb_coeff_real_scatter", dptr(self.C), KK, self.Ks, self.Kt, dptr(self.Mr32), K, 0, s)
         work = self._workspace(2)
         call("vtb_sym_factor", dptr(self.Mr32), K, K, 2, self.rcond * CHOL_MARGIN, dptr(work), work.numel(),

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import torch
 
+from . import autotune
 from ._abi import VtbError, call, dptr, stream_ptr
 
 KB = 64
@@ -41,8 +42,8 @@ def gemm_bf16(A3, B3, out, alpha=1.0, accumulate=False, out_layout="row"):
         cm, cn = out.stride(0), out.stride(1)
     else:
         cm, cn = out.stride(1), out.stride(0)
-    call("vtb_tc_gemm_bf16", dptr(A3), M, dptr(B3), N, K, dptr(out), cm, cn, int(out.dtype == torch.float64),
-         float(alpha), int(bool(accumulate)), dptr(err), stream_ptr())
+    autotune.gemm_bf16_tuned(dptr(A3), M, dptr(B3), N, K, dptr(out), cm, cn, out.dtype == torch.float64, alpha,
+                             bool(accumulate), dptr(err), stream_ptr())
     return out, err
 
 

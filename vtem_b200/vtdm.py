@@ -165,10 +165,11 @@ def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, M
 
     ``decoder="coeff"`` (extension) decodes each window in the Dirichlet
     coefficient space (:mod:`vtem_b200.fast`), the same reconstruction
-    without the spike-by-spike Gram; it needs ``prep`` (VTDM_prep's result)
-    and the pseudoinverse solver."""
-    if decoder == "coeff" and (prep is None or rnn):
-        raise ValueError("the coefficient-space decoder needs prep= and the pseudoinverse solver")
+    without the spike-by-spike Gram, by the pseudoinverse or (``rnn``) the
+    RNN's gradient flow run on the coefficient system; it needs ``prep``
+    (VTDM_prep's result) and no Gram regularisation (``lamb`` = 0)."""
+    if decoder == "coeff" and (prep is None or lamb):
+        raise ValueError("the coefficient-space decoder needs prep= and lamb=0")
     spfile = ss.vtem_storage_read(spikefile)
     spfile.read_vrf_type()
     spfile.read_num_neurons()
@@ -228,8 +229,14 @@ def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, M
         if fastdec is not None:
             if len(tk1) == 0:
                 raise ValueError("no spikes to decode")
-            fastdec.norm = torch.as_tensor(h_norm, device="cuda")
-            u_rec = fastdec.decode(tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, round((end - start) / dt) * dt, dt)
+            fastdec.set_norm(h_norm)
+            T = round((end - start) / dt) * dt
+            if rnn:
+                a, _ = fastdec.rnn_coefficients(tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias,
+                                                dt_alpha=rnn_dt * alpha, steps=steps)
+                u_rec = fastdec.synthesize(a, T, dt)
+            else:
+                u_rec = fastdec.decode(tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, T, dt)
         else:
             u_rec = _plain_window(spfile, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm, Wt, Mt, dtype, Dsw,
                                   lamb, rnn, rnn_dt, alpha, steps, rcond, dirich, start, end, dt)
