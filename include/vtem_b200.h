@@ -244,7 +244,10 @@ int vtb_herm_solve(double* M, int64_t ld, const double* b, double* a, int K, dou
 
 /* u[t][py][px] = Re sum_{s,m} a[s][m] e^{jmW(t0 + t dt)} E_s(px, py) on the
  * decode grid (the spatial functions of vtb_dirich_space), Nt frames,
- * float64 (out_f32 = 0) or float32 output.  A_work holds Nt*Ks complex. */
+ * float64 (out_f32 = 0) or float32 output.  For 2My+1 <= 13 one fused kernel
+ * pairs each spatial frequency with its mirror (the real part of the sum over
+ * half the spectrum) and A_work may be NULL; otherwise A_work holds Nt*Ks
+ * complex (the per-frame temporal expansion). */
 int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, double W, double t0,
                          double dt, int Nt, int Px, int Py, int Px1, int Py1, double* A_work, void* u, int out_f32,
                          void* stream);

@@ -179,49 +179,62 @@ __global__ void __launch_bounds__(256) kron_gram_kernel(const double2* __restric
     }
 }
 
-// b[(s, m)] = sum_n d[n][s] g[n][m]: one block per spatial index s, the 8
-// warps split the neurons, lanes own temporal indices, partial sums reduced
-// in shared memory.
+// b[(s, m)] = sum_n d[n][s] g[n][m]: one block per spatial index s; warp w
+// owns the temporal indices m = w, w+8, ..., its lanes stride over the
+// neurons (each d[n][s] loaded once for all of the warp's m), four
+// independent partial sums per m keep the loads in flight, then a warp
+// reduction.  Deterministic (fixed summation order).
+constexpr int kRhsMaxM = 4;   // m per warp: Kt <= 32
+
 __global__ void __launch_bounds__(256) kron_rhs_kernel(const double2* __restrict__ d, int N, int Ks,
                                                        const double2* __restrict__ gn, int Kt,
                                                        double2* __restrict__ b) {
-    __shared__ double2 part[8][32];
     const int s = blockIdx.x;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int m0 = 0; m0 < Kt; m0 += 32) {
-        const int m = m0 + lane;
-        double2 acc = make_double2(0, 0);
-        if (m < Kt) {
-            // four independent partial sums keep eight loads in flight per lane
-            double2 a4[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-            int n = w;
-            for (; n + 24 < N; n += 32) {
+    for (int mbase = 0; mbase < Kt; mbase += 8 * kRhsMaxM) {
+        double2 acc[kRhsMaxM][2];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int nu = n + 8 * u;
-                    const double2 p = cmul(d[(int64_t)nu * Ks + s], gn[(int64_t)nu * Kt + m]);
-                    a4[u].x += p.x;
-                    a4[u].y += p.y;
+        for (int q = 0; q < kRhsMaxM; ++q) acc[q][0] = acc[q][1] = make_double2(0, 0);
+        int n = lane;
+        for (; n + 32 < N; n += 64) {
+#pragma unroll
+            for (int u2 = 0; u2 < 2; ++u2) {
+                const int nu = n + 32 * u2;
+                const double2 dv = d[(int64_t)nu * Ks + s];
+#pragma unroll
+                for (int q = 0; q < kRhsMaxM; ++q) {
+                    const int m = mbase + w + 8 * q;
+                    if (m < Kt) {
+                        const double2 p = cmul(dv, gn[(int64_t)nu * Kt + m]);
+                        acc[q][u2].x += p.x;
+                        acc[q][u2].y += p.y;
+                    }
                 }
             }
-            for (; n < N; n += 8) {
-                const double2 p = cmul(d[(int64_t)n * Ks + s], gn[(int64_t)n * Kt + m]);
-                a4[0].x += p.x;
-                a4[0].y += p.y;
-            }
-            acc = make_double2((a4[0].x + a4[1].x) + (a4[2].x + a4[3].x), (a4[0].y + a4[1].y) + (a4[2].y + a4[3].y));
         }
-        part[w][lane] = acc;
-        __syncthreads();
-        if (w == 0 && m < Kt) {
-            double2 t = part[0][lane];
-            for (int k = 1; k < 8; ++k) {
-                t.x += part[k][lane].x;
-                t.y += part[k][lane].y;
+        for (; n < N; n += 32) {
+            const double2 dv = d[(int64_t)n * Ks + s];
+#pragma unroll
+            for (int q = 0; q < kRhsMaxM; ++q) {
+                const int m = mbase + w + 8 * q;
+                if (m < Kt) {
+                    const double2 p = cmul(dv, gn[(int64_t)n * Kt + m]);
+                    acc[q][0].x += p.x;
+                    acc[q][0].y += p.y;
+                }
             }
-            b[(int64_t)s * Kt + m] = t;
         }
-        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kRhsMaxM; ++q) {
+            double x = acc[q][0].x + acc[q][1].x, y = acc[q][0].y + acc[q][1].y;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                x += __shfl_xor_sync(0xffffffffu, x, o);
+                y += __shfl_xor_sync(0xffffffffu, y, o);
+            }
+            const int m = mbase + w + 8 * q;
+            if (lane == 0 && m < Kt) b[(int64_t)s * Kt + m] = make_double2(x, y);
+        }
     }
 }
 
@@ -356,6 +369,169 @@ __global__ void __launch_bounds__(256) synth_kernel(const double2* __restrict__ 
     }
 }
 
+// Fused synthesis over half the spectrum.  The spatial factors are
+// Hermitian (ey[-my] = conj ey[my], ex[-mx] = conj ex[mx]), so the real part
+// of the full sum pairs every (my, mx) with (-my, -mx):
+//     u[py][px] = Re B[0][px] + sum_{my >= 1} Re(ey[my][py] B'[my][px]),
+//     B'[my][px] = sum_mx (A_t[my][mx] + conj A_t[-my][-mx]) ex[mx][px]
+//               = sum_k Y[k][py] X[k][px],  k < 2My+1 real rows
+// (Y[0] = 1, Y[2my-1] = Re ey, Y[2my] = -Im ey; X[0] = Re B[0],
+// X[2my-1] = Re B'[my], X[2my] = Im B'[my]); for the Hermitian-symmetric
+// coefficients every decoder produces, B' = 2 B.  Per frame: the temporal
+// expansion of the ellipse (a[s][m] staged in shared memory once per block),
+// B for my >= 0, then the rank-(2My+1) real product, each thread a 4 x 4
+// pixel block (8 shared-memory reads per 16 FMAs, two blocks per SM): 13 FMAs
+// per voxel at Mx = My = 6, no intermediate buffer in HBM, streaming stores.
+constexpr int kHalfMaxRows = 13;   // 2My+1 served by the fused kernel (My <= 6)
+
+constexpr int kHalfFrames = 2;     // frames per iteration: more threads busy in the per-frame setup
+
+template <typename OutT>
+__global__ void __launch_bounds__(256, 2) synth_half_kernel(const double2* __restrict__ a,
+                                                            const int32_t* __restrict__ smap, int Ks, int Mx, int My,
+                                                            int Mt, double W, double t0, double dt, int Nt, int Px,
+                                                            int Py, int Px1, int Py1, OutT* __restrict__ u) {
+    extern __shared__ double2 hs[];
+    const int Kx = 2 * Mx + 1, Ky = 2 * My + 1, Kt = 2 * Mt + 1, R = Ky, H = My + 1, KG = Ky * Kx;
+    double2* ex = hs;                               // Kx x Px
+    double2* as = ex + Kx * Px;                     // Ks x Kt
+    double2* E = as + Ks * Kt;                      // kHalfFrames x Kt
+    double2* G = E + kHalfFrames * Kt;              // kHalfFrames x Ky x Kx (zero outside the ellipse)
+    double* X = reinterpret_cast<double*>(G + kHalfFrames * KG);   // kHalfFrames x R x Px
+    double* Ys = X + kHalfFrames * R * Px;          // R x Py
+    const int xd = (Px1 - Px) / 2, yd = (Py1 - Py) / 2;
+    // spatial factors from one sincospi per pixel column / row and powers of
+    // it (a few ulp per power; a per-entry sincospi here would cost more than
+    // the frames a block renders)
+    for (int px = threadIdx.x; px < Px; px += blockDim.x) {
+        double sn, co;
+        sincospi(2.0 * ((px + xd) % Px1) / Px1, &sn, &co);
+        const double2 base = make_double2(co, sn);
+        double2 pw = make_double2(1.0, 0.0);
+        ex[Mx * Px + px] = pw;
+        for (int mx = 1; mx <= Mx; ++mx) {
+            pw = cmul(pw, base);
+            const double sg = (mx & 1) ? -1.0 : 1.0;
+            ex[(Mx + mx) * Px + px] = make_double2(sg * pw.x, sg * pw.y);
+            ex[(Mx - mx) * Px + px] = make_double2(sg * pw.x, -sg * pw.y);
+        }
+    }
+    for (int py = threadIdx.x; py < Py; py += blockDim.x) {
+        double sn, co;
+        sincospi(2.0 * ((py + yd) % Py1) / Py1, &sn, &co);
+        const double2 base = make_double2(co, sn);
+        double2 pw = make_double2(1.0, 0.0);
+        Ys[py] = 1.0;
+        for (int my = 1; my <= My; ++my) {
+            pw = cmul(pw, base);
+            const double sg = (my & 1) ? -1.0 : 1.0;
+            Ys[(2 * my - 1) * Py + py] = sg * pw.x;
+            Ys[(2 * my) * Py + py] = -sg * pw.y;
+        }
+    }
+    // transposed, as[m][s]: the expansion's threads (consecutive s) read consecutive entries
+    for (int e = threadIdx.x; e < Ks * Kt; e += blockDim.x) as[(e % Kt) * Ks + e / Kt] = a[e];
+    for (int e = threadIdx.x; e < kHalfFrames * KG; e += blockDim.x) G[e] = make_double2(0, 0);
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    for (int f0 = blockIdx.x * kHalfFrames; f0 < Nt; f0 += gridDim.x * kHalfFrames) {
+        const int nf = min(kHalfFrames, Nt - f0);
+        __syncthreads();
+        for (int q = threadIdx.x; q < nf; q += blockDim.x) {
+            double sn, co;
+            sincos(W * (t0 + (f0 + q) * dt), &sn, &co);
+            const double2 base = make_double2(co, sn);
+            double2 pw = make_double2(1.0, 0.0);
+            E[q * Kt + Mt] = pw;
+            for (int m = 1; m <= Mt; ++m) {
+                pw = cmul(pw, base);
+                E[q * Kt + Mt + m] = pw;
+                E[q * Kt + Mt - m] = make_double2(pw.x, -pw.y);
+            }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < nf * Ks; e += blockDim.x) {
+            const int q = e / Ks, sidx = e % Ks;
+            double2 acc = make_double2(0, 0);
+            for (int mi = 0; mi < Kt; ++mi) {
+                const double2 p = cmul(as[mi * Ks + sidx], E[q * Kt + mi]);
+                acc.x += p.x;
+                acc.y += p.y;
+            }
+            G[q * KG + smap[sidx]] = acc;
+        }
+        __syncthreads();
+        // storage row rr holds my = My - rr: rows rr <= My are my >= 0
+        for (int e = threadIdx.x; e < nf * H * Px; e += blockDim.x) {
+            const int q = e / (H * Px), r2 = e % (H * Px);
+            const int my = r2 / Px, px = r2 % Px, rr = My - my;
+            const double2* Gq = G + q * KG;
+            double2 acc = make_double2(0, 0);
+            for (int c = 0; c < Kx; ++c) {
+                double2 g = Gq[rr * Kx + c];
+                if (my > 0) {
+                    const double2 gm = Gq[KG - 1 - (rr * Kx + c)];   // (-my, -mx)
+                    g = make_double2(g.x + gm.x, g.y - gm.y);
+                }
+                const double2 x = ex[c * Px + px];
+                acc.x = fma(g.x, x.x, fma(-g.y, x.y, acc.x));
+                acc.y = fma(g.x, x.y, fma(g.y, x.x, acc.y));
+            }
+            double* Xq = X + q * R * Px;
+            if (my == 0) {
+                Xq[px] = acc.x;
+            } else {
+                Xq[(2 * my - 1) * Px + px] = acc.x;
+                Xq[(2 * my) * Px + px] = acc.y;
+            }
+        }
+        __syncthreads();
+        // each thread: pixels (y0 + ty + 16i, x0 + tx + 16j), i, j < 4: the X
+        // reads of a warp are 16 consecutive doubles, the Y reads two, both
+        // free of bank conflicts, and the stores 128-byte rows
+        for (int y0 = 0; y0 < Py; y0 += 64) {
+            for (int q = 0; q < nf; ++q) {
+                const double* Xq = X + q * R * Px;
+                OutT* uf = u + (int64_t)(f0 + q) * Px * Py;
+                for (int x0 = 0; x0 < Px; x0 += 64) {
+                    double acc[4][4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#pragma unroll 1
+                    for (int k = 0; k < R; ++k) {
+                        double xv[4], yv[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int px = x0 + tx + 16 * j;
+                            xv[j] = px < Px ? Xq[k * Px + px] : 0.0;
+                        }
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const int py = y0 + ty + 16 * i;
+                            yv[i] = py < Py ? Ys[k * Py + py] : 0.0;
+                        }
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) acc[i][j] = fma(yv[i], xv[j], acc[i][j]);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const int py = y0 + ty + 16 * i;
+                        if (py >= Py) continue;
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int px = x0 + tx + 16 * j;
+                            if (px < Px) __stcs(uf + (int64_t)py * Px + px, (OutT)acc[i][j]);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
 }  // namespace vtb
 
 using namespace vtb;
@@ -404,14 +580,38 @@ VTB_API int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, i
     VTB_CHECK_ARG(Ks > 0 && Mx >= 0 && My >= 0 && Mt >= 0 && Nt >= 0 && Px > 0 && Py > 0 && Px1 >= Px && Py1 >= Py);
     VTB_CHECK_ARG(2 * Mx + 1 <= Px1 && 2 * My + 1 <= Py1);
     if (Nt == 0) return VTB_OK;
-    VTB_CHECK_ARG(a && smap && A_work && u);
+    VTB_CHECK_ARG(a && smap && u);
     cudaStream_t s = as_stream(stream);
     const int Kt = 2 * Mt + 1;
+    const int Kx = 2 * Mx + 1, Ky = 2 * My + 1;
+    if (Ky <= kHalfMaxRows) {
+        // fused half-spectrum kernel (A_work unused)
+        const size_t smh = (size_t)(Kx * Px + Ks * Kt + kHalfFrames * (Kt + Ky * Kx)) * sizeof(double2) +
+                           (size_t)(kHalfFrames * Ky * Px + Ky * Py) * sizeof(double);
+        VTB_CHECK_ARG(smh <= 200 * 1024);
+        const int blocks = (int)std::min<int64_t>(ceil_div(Nt, kHalfFrames), 2 * kNumSMs);
+        if (out_f32) {
+            if (smh > 48 * 1024)
+                VTB_CUDA_TRY(cudaFuncSetAttribute(synth_half_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)smh));
+            synth_half_kernel<float><<<blocks, 256, smh, s>>>(reinterpret_cast<const double2*>(a), smap, Ks, Mx, My, Mt,
+                                                              W, t0, dt, Nt, Px, Py, Px1, Py1,
+                                                              reinterpret_cast<float*>(u));
+        } else {
+            if (smh > 48 * 1024)
+                VTB_CUDA_TRY(cudaFuncSetAttribute(synth_half_kernel<double>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smh));
+            synth_half_kernel<double><<<blocks, 256, smh, s>>>(reinterpret_cast<const double2*>(a), smap, Ks, Mx, My,
+                                                               Mt, W, t0, dt, Nt, Px, Py, Px1, Py1,
+                                                               reinterpret_cast<double*>(u));
+        }
+        return launch_status();
+    }
+    VTB_CHECK_ARG(A_work);
     temporal_expand_kernel<<<Nt, 128, Kt * sizeof(double2), s>>>(reinterpret_cast<const double2*>(a), Ks, Mt, W, t0,
                                                                  dt, Nt, reinterpret_cast<double2*>(A_work));
     int st = launch_status();
     if (st) return st;
-    const int Kx = 2 * Mx + 1, Ky = 2 * My + 1;
     const size_t sm = (size_t)(Kx * Px + Ky * Py + Ky * Kx + Ky * Px) * sizeof(double2);
     VTB_CHECK_ARG(sm <= 200 * 1024);
     const int blocks = ceil_div(Nt, kSynthFrames);

@@ -385,7 +385,8 @@ class CoeffDecoder(object):
         dev = self.M.device
         if out is None:
             out = torch.empty((Nt, self.decPy, self.decPx), dtype=out_dtype, device=dev)
-        A = torch.empty((Nt, self.Ks), dtype=C128, device=dev)
+        # the fused kernel (2My+1 <= 13) needs no expansion buffer
+        A = None if 2 * self.My + 1 <= 13 else torch.empty((Nt, self.Ks), dtype=C128, device=dev)
         call("vtb_coeff_synthesize", dptr(a), dptr(self.smap), self.Ks, self.Mx, self.My, self.Mt, self.W, float(t0),
              float(dt), Nt, self.decPx, self.decPy, self.Px1, self.Py1, dptr(A), dptr(out),
              int(out.dtype == torch.float32), stream_ptr())
