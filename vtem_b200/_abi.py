@@ -111,8 +111,9 @@ def lib():
             f = getattr(l, name)
             f.argtypes = args
             f.restype = ctypes.c_int
-        l.vtb_sym_dinv_floats.argtypes = [ctypes.c_int]
-        l.vtb_sym_dinv_floats.restype = ctypes.c_int64
+        for name in ("vtb_sym_dinv_floats",):
+            getattr(l, name).argtypes = [ctypes.c_int]
+            getattr(l, name).restype = ctypes.c_int64
         l.vtb_status_string.argtypes = [ctypes.c_int]
         l.vtb_status_string.restype = ctypes.c_char_p
         _lib = l
