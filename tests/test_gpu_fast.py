@@ -233,3 +233,20 @@ def test_coefficient_rnn_matches_spike_rnn(small_encoded):
     uo = O.reconstruct_factored(prep.dirich.cpu().numpy(), tk1, tk2, co.ravel(), t, ind, norm, w.Mt, w.Wt / w.Mt)
     rel_o = np.linalg.norm(u.cpu().numpy().ravel() - uo.ravel()) / np.linalg.norm(uo)
     assert rel_o < 1e-8, rel_o
+
+
+def test_decode_to_host_matches_device_decode(small_encoded):
+    """The overlapped end-to-end decode into pinned host memory returns the
+    device decode's video (frame ranges synthesised separately)."""
+    w, store, prep = small_encoded
+    rd = spike_store.vtem_storage_read(store)
+    rd.read_vrf_type()
+    rd.read_num_neurons()
+    rd.select_neurons([-0.5, 0.5, -0.5, 0.5])
+    tk1, tk2, ind, kap, dl, bia, sig = rd.read_select_spikes([0.0, w.T])
+    dec = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="mixed", mixed_sweeps=2)
+    u = dec.decode(tk1, tk2, ind, kap, dl, bia, w.T, w.dt).cpu()
+    h = torch.empty(u.shape, dtype=torch.float64).pin_memory()
+    dec.decode_to_host(tk1, tk2, ind, kap, dl, bia, w.T, w.dt, h, chunks=5)
+    torch.cuda.synchronize()
+    assert ((h - u).norm() / u.norm()).item() < 1e-13

@@ -288,3 +288,34 @@ def test_iaf_small_buffer_retry_is_exact():
     for n in range(N):
         assert np.array_equal(ta[0][n], tb[0][n]) and np.array_equal(ta[1][n], tb[1][n])
     assert torch.equal(a.d_v0, b.d_v0)
+
+
+@pytest.mark.parametrize("N,F,seed,dmin,dmax", [(64, 10000, 5, 0.01, 0.04), (40, 4000, 6, 0.002, 0.01),
+                                                (96, 10000, 7, 0.03, 0.2)])
+def test_iaf_long_scan_bitexact(N, F, seed, dmin, dmax):
+    """Long scans at dt = 1e-4 with sparse spiking: whole 32-step chunks
+    without a crossing (the register-chain path, with frame-block
+    boundaries inside chunks) and chunks with crossings; spike times, steps,
+    final membrane values and near-threshold counts bit-exact against the
+    reference-order C oracle."""
+    rng = np.random.default_rng(seed)
+    L = rng.standard_normal((F, N)) * 0.5
+    kap = rng.uniform(0.7, 1.3, N)
+    bia = rng.uniform(2.0, 4.0, N)
+    dl = rng.uniform(dmin, dmax, N)
+    v0 = rng.uniform(0, 1, N) * dl
+    dt = 1e-4
+    enc = O.vtem_encode(L, dt, kap, bia, dl, v0, block_frames=101)
+    e = _iaf(N, dt, kap, bia, dl, v0)
+    sp = e.encode_blocks(L, block_frames=101)
+    times, steps, cnt = sp.to_host_lists()
+    got_t, got_s = [], []
+    for b in range(len(enc.block_counts)):
+        for n in range(N):
+            sel = (steps[n] // 100) == b
+            got_t.append(times[n][sel])
+            got_s.append(steps[n][sel])
+    assert np.array_equal(np.concatenate(got_s), np.concatenate(enc.block_steps))
+    assert np.array_equal(np.concatenate(got_t), np.concatenate(enc.block_spikes))
+    assert np.array_equal(e.d_v0.cpu().numpy(), enc.v0)
+    assert sp.near_threshold == enc.near_threshold

@@ -111,7 +111,47 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
         s_y2[w][lane] = y2l;
         __syncwarp();
         const int nst = min(32, steps - t0);
-        for (int j = 0; j < nst; ++j) {
+        // Fast chunk: every step of the 32 has the positive-slope form and at
+        // most one frame-block boundary falls inside.  All lanes run the
+        // membrane and time recursions v += area_j, tc += dt in the
+        // reference's order as one register chain (the areas arrive by
+        // shuffle, off the chain's critical path), lane j keeping the value
+        // after step j; a ballot then finds the first crossing.  Steps before
+        // it are final as computed (the same float64 operations in the same
+        // order as the step loop below); the crossing step and the rest of
+        // the chunk run through the step loop from the exact state.
+        int jstart = 0;
+        if (nst == 32 && posmask == full && (bstep >= 32 || bstep <= 0)) {
+            const int rpos = (next_reset >= t0 && next_reset < t0 + 32) ? next_reset - t0 : -1;
+            double v = v0, tt = tc, s_l = 0.0, t_l = 0.0;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const double aj = __shfl_sync(full, areal, j);
+                if (j == rpos) tt = 0.0;
+                v = v + aj;
+                tt = tt + dt;
+                if (lane == j) {
+                    s_l = v;
+                    t_l = tt;
+                }
+            }
+            const unsigned cross = __ballot_sync(full, s_l >= delta);
+            const unsigned nearm = __ballot_sync(full, fabs(s_l - delta) < p.near_eps);
+            const int f = cross ? __ffs(cross) - 1 : 32;
+            near += (unsigned long long)__popc(f < 32 ? (nearm & ((1u << f) - 1u)) : nearm);
+            if (f > 0) {
+                v0 = __shfl_sync(full, s_l, f - 1);
+                tc = __shfl_sync(full, t_l, f - 1);
+                if (rpos >= 0 && rpos < f) {
+                    cnt_block = 0;
+                    ++block;
+                    next_reset += bstep;
+                    lim_block = block_limit(block);
+                }
+            }
+            jstart = f;
+        }
+        for (int j = jstart; j < nst; ++j) {
             const int g = t0 + j;
             if (g == next_reset) {  // start of the next frame block
                 tc = 0.0;

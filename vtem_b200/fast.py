@@ -399,6 +399,47 @@ class CoeffDecoder(object):
         return self.synthesize(a, T, dt, out=out, out_dtype=out_dtype)
 
 
+    def decode_to_host(self, tk1, tk2, neuron_ind, kappa, delta, bias, T, dt, host_out, chunks=8,
+                       assume_sorted=False):
+        """Decode into ``host_out`` (pinned host tensor (Nt, decPy, decPx)):
+        the synthesis runs in ``chunks`` frame ranges on the current stream
+        and each finished range is copied to the host on a copy stream, so
+        the download of one range overlaps the synthesis of the next.  The
+        current stream waits for the last copy (synchronise it, or an event
+        recorded on it, before reading ``host_out``)."""
+        a = self.coefficients(tk1, tk2, neuron_ind, kappa, delta, bias, assume_sorted=assume_sorted)
+        Nt = int(host_out.shape[0])
+        if tuple(host_out.shape) != (Nt, self.decPy, self.decPx) or not host_out.is_pinned():
+            raise ValueError("host_out must be a pinned (Nt, decPy, decPx) tensor")
+        f32 = host_out.dtype == torch.float32
+        dev = self.M.device
+        key = (Nt, host_out.dtype)
+        if getattr(self, "_e2e_key", None) != key:
+            self._e2e_out = torch.empty(host_out.shape, dtype=host_out.dtype, device=dev)
+            self._e2e_key = key
+            self._copy_stream = torch.cuda.Stream(device=dev)
+        out = self._e2e_out
+        main = torch.cuda.current_stream(dev)
+        cs = self._copy_stream
+        bounds = np.linspace(0, Nt, max(1, int(chunks)) + 1).astype(np.int64)
+        A = None if 2 * self.My + 1 <= 13 else torch.empty((Nt, self.Ks), dtype=C128, device=dev)
+        for f0, f1 in zip(bounds[:-1], bounds[1:]):
+            if f1 <= f0:
+                continue
+            call("vtb_coeff_synthesize", dptr(a), dptr(self.smap), self.Ks, self.Mx, self.My, self.Mt, self.W,
+                 float(f0 * dt), float(dt), int(f1 - f0), self.decPx, self.decPy, self.Px1, self.Py1, dptr(A),
+                 dptr(out[f0:f1]), int(f32), main.cuda_stream)
+            ev = torch.cuda.Event()
+            ev.record(main)
+            cs.wait_event(ev)
+            with torch.cuda.stream(cs):
+                host_out[f0:f1].copy_(out[f0:f1], non_blocking=True)
+        done = torch.cuda.Event()
+        done.record(cs)
+        main.wait_event(done)
+        return host_out
+
+
 def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=0, mixed_sweeps=2):
     """A :class:`CoeffDecoder` on the output of ``vtdm.VTDM_prep``."""
     return CoeffDecoder(prep.Ds, prep.h_norm, prep.Mx, prep.My, Wt, Mt, prep.decPx, prep.decPy, prep.Px1, prep.Py1,
