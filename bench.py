@@ -43,6 +43,24 @@ METRIC = "reconstructed voxels/s at >=40 dB SNR (mixed vs FP64 plain)"
 UNIT = "voxels/s"
 
 
+def reduce_max(values, device, world):
+    """Element-wise maximum over ranks of per-rank timings (the job's time is
+    its slowest rank's): an all-reduce MAX on ``device`` (CUDA for NCCL, CPU
+    for gloo); a no-op with one rank."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def weak_value(units_per_rank, world, steps, ms):
+    """Whole-job throughput of clip-parallel ranks: every rank processes
+    ``units_per_rank`` per step, the job takes the slowest rank's ``ms``."""
+    return units_per_rank * world * steps / (ms / 1e3)
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -206,10 +224,7 @@ def run_ours(args, rank, world, local):
     mix_ms, mix_synth = time_decoder(decmix, inputs, w, umix, flush, args.steps, args.warmup)
     clk = clocks.stop()
     f64_ms, f64_synth = time_decoder(dec64, inputs, w, u64, flush, args.steps, args.warmup)
-    t = torch.tensor([mix_ms, f64_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    mix_ms, f64_ms = (float(x) for x in t.tolist())
+    mix_ms, f64_ms = reduce_max([mix_ms, f64_ms], dev, world)
     rel_mix_f64 = float(((umix - u64).norm() / u64.norm()).item())
     resid = decmix.residual_norm(*inputs)
 
@@ -238,10 +253,8 @@ def run_ours(args, rank, world, local):
         e1.record()
         torch.cuda.synchronize()
         e2e_ms += e0.elapsed_time(e1)
-    te = torch.tensor([e2e_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = voxels * world * e2e_steps / (float(te.item()) / 1e3)
+    e2e_ms = reduce_max([e2e_ms], dev, world)[0]
+    e2e_value = weak_value(voxels, world, e2e_steps, e2e_ms)
     h2d = n * (8 + 8 + 4)
     d2h = voxels * 8
 
@@ -256,7 +269,7 @@ def run_ours(args, rank, world, local):
         headline_mixed = snr_mix is None or snr_mix >= 40.0
         tot_ms = mix_ms if headline_mixed else f64_ms
         synth_ms = mix_synth if headline_mixed else f64_synth
-        value = voxels * world * args.steps / (tot_ms / 1e3)
+        value = weak_value(voxels, world, args.steps, tot_ms)
         # the fused synthesis writes the video and reads only the K coefficients
         synth_bytes = voxels * 8 + dec64.K * 16
         synth_avg = sum(synth_ms) / len(synth_ms) / 1e3
