@@ -252,6 +252,20 @@ int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, int Mx, i
                          double dt, int Nt, int Px, int Py, int Px1, int Py1, double* A_work, void* u, int out_f32,
                          void* stream);
 
+/* Grouped tensor-core GEMM: nprob independent problems C_p = A_p B_p^T (bf16
+ * K-major operands as vtb_tc_gemm_bf16's, float32 row-major C_p with leading
+ * dimension ldc_p, alpha 1) in ONE launch, the Gram GEMMs of a batch of clips
+ * of uneven size.  vtb_tc_group_build fills a HOST descriptor array
+ * (vtb_tc_group_bytes(nprob) bytes; the arrays passed are host arrays of the
+ * problems' device pointers and sizes) and returns the grid size; the caller
+ * copies it to 64-byte-aligned device memory and launches
+ * vtb_tc_gemm_grouped with the same tile width bn (64, 128 or 256). */
+int64_t vtb_tc_group_bytes(int nprob);
+int vtb_tc_group_build(void* host_desc, int nprob, const uint64_t* A, const int* M, const uint64_t* B, const int* N,
+                       const int* K, const uint64_t* C, const int64_t* ldc, const uint64_t* err, int bn,
+                       int* total_tiles);
+int vtb_tc_gemm_grouped(const void* dev_desc, int nprob, int total_tiles, int bn, void* stream);
+
 /* Mixed-precision Kronecker Gram (tensor cores).  ps/ps2 list the npairs
  * spatial index pairs s <= s'.  L3 receives the RF-bank operand (2*npairs
  * rows x 3*Kp bf16, Kp = 2N rounded up to 64; once per decoder), R3 the

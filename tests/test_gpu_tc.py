@@ -88,3 +88,38 @@ def test_autotuner_picks_a_candidate_and_caches_it():
     assert autotune._cache[key] in autotune.CANDIDATES
     C2 = tc.gemm_split_bf16(A, B)           # cached choice: same result
     assert torch.equal(C1, C2)
+
+
+@pytest.mark.parametrize("bn", [64, 128, 256])
+def test_grouped_gemm_equals_single_launches(bn):
+    """One grouped launch over problems of uneven sizes gives each problem's
+    single-launch result bit for bit (same tiles, same accumulation order)."""
+    from vtem_b200._abi import call, dptr, lib, stream_ptr
+    rng = np.random.default_rng(bn + 1)
+    shapes = [(300, 289, 384), (97, 49, 128), (513, 121, 192), (128, 225, 64), (40, 81, 256)]
+    As, Bs, Cs, Cref, errs = [], [], [], [], []
+    for (M, N, K) in shapes:
+        A = torch.as_tensor(rng.standard_normal((M, K)), device="cuda").to(torch.bfloat16).contiguous()
+        B = torch.as_tensor(rng.standard_normal((N, K)), device="cuda").to(torch.bfloat16).contiguous()
+        As.append(A)
+        Bs.append(B)
+        Cs.append(torch.full((M, N), float("nan"), dtype=torch.float32, device="cuda"))
+        Cref.append(torch.zeros((M, N), dtype=torch.float32, device="cuda"))
+        errs.append(torch.zeros(1, dtype=torch.int32, device="cuda"))
+        call("vtb_tc_gemm_bf16_bn", dptr(A), M, dptr(B), N, K, dptr(Cref[-1]), N, 1, 0, 1.0, 0, dptr(errs[-1]), bn,
+             stream_ptr())
+    n = len(shapes)
+    u64 = np.uint64
+    arr = [np.array([a.data_ptr() for a in As], u64), np.array([s[0] for s in shapes], np.int32),
+           np.array([b.data_ptr() for b in Bs], u64), np.array([s[1] for s in shapes], np.int32),
+           np.array([s[2] for s in shapes], np.int32), np.array([c.data_ptr() for c in Cs], u64),
+           np.array([s[1] for s in shapes], np.int64), np.array([e.data_ptr() for e in errs], u64)]
+    host = np.zeros(int(lib().vtb_tc_group_bytes(n)), np.uint8)
+    tiles = np.zeros(1, np.int32)
+    call("vtb_tc_group_build", host.ctypes.data, n, *[a.ctypes.data for a in arr], bn, tiles.ctypes.data)
+    desc = torch.as_tensor(host).cuda()
+    call("vtb_tc_gemm_grouped", dptr(desc), n, int(tiles[0]), bn, stream_ptr())
+    torch.cuda.synchronize()
+    assert all(int(e.item()) == 0 for e in errs)
+    for C, R in zip(Cs, Cref):
+        assert torch.equal(C, R)

@@ -84,6 +84,9 @@ SIGNATURES = {
     "vtb_sym_pinv_batched_workspace": [I, I, P],
     "vtb_sym_pinv_batched": [P, P, P, I, I, D, P, L, P, P, P],
     "vtb_rnn_coeff": [P, L, P, P, P, I, D, I, P, P],
+    "vtb_tc_group_bytes": [I],  # restype int64, set in lib()
+    "vtb_tc_group_build": [P, I, P, P, P, P, P, P, P, P, I, P],
+    "vtb_tc_gemm_grouped": [P, I, I, I, P],
     "vtb_sym_dinv_floats": [I],  # restype int64, set in lib()
 }
 
@@ -111,7 +114,7 @@ def lib():
             f = getattr(l, name)
             f.argtypes = args
             f.restype = ctypes.c_int
-        for name in ("vtb_sym_dinv_floats",):
+        for name in ("vtb_sym_dinv_floats", "vtb_tc_group_bytes"):
             getattr(l, name).argtypes = [ctypes.c_int]
             getattr(l, name).restype = ctypes.c_int64
         l.vtb_status_string.argtypes = [ctypes.c_int]

@@ -5,9 +5,10 @@ Each clip is decoded in the Dirichlet coefficient space as
 :class:`vtem_b200.fast.CoeffDecoder` (``solver="mixed"``) does alone; the
 batch changes how the work is scheduled:
 
-* per clip, the temporal Gram, the right-hand side and the tensor-core
-  Kronecker Gram (scattered into the real symmetric float32 system) are
-  issued round-robin on several CUDA streams;
+* per clip, the temporal Gram and the right-hand side are issued
+  round-robin on several CUDA streams; the tensor-core Kronecker Grams of all
+  clips run as ONE grouped GEMM launch (``GroupedGram``, tile width chosen by
+  timing), then each is scattered into its real symmetric float32 system;
 * clips whose systems have the same size K are factorised by one batched
   float32 Cholesky per group (``vtb_sym_factor_batched``), and every clip's
   triangular solves run in one launch (``vtb_sym_potrs_batched``, one CTA per
@@ -60,6 +61,81 @@ class ClipProblem(object):
     @property
     def spikes(self):
         return (self.tk1, self.tk2, self.ind, int(self.tk1.numel()), self.kappa, self.delta, self.bias)
+
+
+class GroupedGram(object):
+    """The tensor-core Kronecker Gram GEMMs of many mixed decoders
+    (C_p = L3_p R3_p^T, uneven sizes) as ONE grouped launch
+    (``vtb_tc_gemm_grouped``); its tile width is chosen by timing the
+    candidates on the first eager run (``autotune``)."""
+
+    WIDTHS = (64, 128, 256)
+
+    def __init__(self, decs):
+        self.decs = list(decs)
+        self.n = len(self.decs)
+        dev = self.decs[0].M.device
+        u64 = np.uint64
+        self.args = [
+            np.array([d.L3.data_ptr() for d in self.decs], u64), np.array([2 * d.npairs for d in self.decs], np.int32),
+            np.array([d.R3.data_ptr() for d in self.decs], u64), np.array([d.Kt * d.Kt for d in self.decs], np.int32),
+            np.array([3 * d.Kp2 for d in self.decs], np.int32), np.array([d.C.data_ptr() for d in self.decs], u64),
+            np.array([d.Kt * d.Kt for d in self.decs], np.int64),
+            np.array([d._stat_ptr(7) for d in self.decs], u64)]
+        self.desc = {}
+        self.tiles = {}
+        nbytes = int(lib().vtb_tc_group_bytes(self.n))
+        for bn in self.WIDTHS:
+            host = np.zeros(nbytes, np.uint8)
+            tiles = np.zeros(1, np.int32)
+            a = self.args
+            call("vtb_tc_group_build", host.ctypes.data, self.n, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data,
+                 a[3].ctypes.data, a[4].ctypes.data, a[5].ctypes.data, a[6].ctypes.data, a[7].ctypes.data, bn,
+                 tiles.ctypes.data)
+            self.desc[bn] = torch.as_tensor(host).to(dev)
+            self.tiles[bn] = int(tiles[0])
+        self.bn = None
+
+    def _launch(self, bn, s):
+        call("vtb_tc_gemm_grouped", dptr(self.desc[bn]), self.n, self.tiles[bn], bn, s)
+
+    def launch(self, s):
+        if self.bn is None:
+            if torch.cuda.is_current_stream_capturing():
+                self.bn = 64
+            else:
+                times = {}
+                for bn in self.WIDTHS:
+                    self._launch(bn, s)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    for _ in range(3):
+                        self._launch(bn, s)
+                    e1.record()
+                    e1.synchronize()
+                    times[bn] = e0.elapsed_time(e1) / 3
+                self.bn = min(times, key=times.get)
+                self.timings = times
+        self._launch(self.bn, s)
+
+
+def stage_mixed_pre(d, p, s):
+    """Device work of one clip before its Gram GEMM: W_n, g_n, b and its real
+    form br, and the split-bf16 operand of the temporal Grams."""
+    tk1, tk2, ind, n, kap, dl, bi = p.spikes
+    d.stat.zero_()
+    call("vtb_coeff_temporal_gram", dptr(tk1), dptr(tk2), dptr(ind), n, d.N, dptr(kap), dptr(dl), dptr(bi),
+         dptr(d.norm), d.Mt, d.W, dptr(d.Wn), dptr(d.gn), s)
+    call("vtb_coeff_rhs", dptr(d.d), d.N, d.Ks, dptr(d.gn), d.Kt, dptr(d.b), s)
+    call("vtb_coeff_realify_vec", dptr(d.b), d.K, 1, dptr(d.br), s)
+    call("vtb_coeff_wn_split", dptr(d.Wn), d.N, d.Kt, dptr(d.R3), s)
+
+
+def stage_mixed_post(d, s):
+    """After the Gram GEMM: the float32 real system and xr = br."""
+    KK = d.Kt * d.Kt
+    call("vtb_coeff_real_scatter", dptr(d.C), KK, d.Ks, d.Kt, dptr(d.Mr32), d.K, 0, s)
+    d.xr.copy_(d.br)
 
 
 def stage_mixed(d, p, s):
@@ -309,6 +385,7 @@ class BatchDecoder(object):
         self.plan = MixedSolvePlan([self.decs[i] for i in self.coeff], [self.problems[i] for i in self.coeff], sweeps,
                                    self.streams) if self.coeff else None
         self.groups = self.plan.groups if self.plan else []
+        self.gram = GroupedGram([self.decs[i] for i in self.coeff]) if self.coeff else None
         self.outs = [torch.empty((p.Nt, p.prep.decPy, p.prep.decPx), dtype=torch.float64, device=dev)
                      for p in self.problems]
         self.use_graph = bool(graph)
@@ -338,7 +415,14 @@ class BatchDecoder(object):
         main = self._fork()
         for c, i in enumerate(self.coeff):
             with torch.cuda.stream(self.streams[c % len(self.streams)]):
-                stage_mixed(self.decs[i], self.problems[i], stream_ptr())
+                stage_mixed_pre(self.decs[i], self.problems[i], stream_ptr())
+        self._join(main)
+        # every clip's Kronecker Gram in one grouped tensor-core launch
+        self.gram.launch(stream_ptr())
+        main = self._fork()
+        for c, i in enumerate(self.coeff):
+            with torch.cuda.stream(self.streams[c % len(self.streams)]):
+                stage_mixed_post(self.decs[i], stream_ptr())
         self._join(main)
         self.plan.launch()
 

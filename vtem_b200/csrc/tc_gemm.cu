@@ -20,6 +20,7 @@
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
+#include <cstring>
 #include <mutex>
 
 #include "common.cuh"
@@ -92,18 +93,16 @@ struct TcSmem {
     uint32_t tmem_base;
 };
 
+// One 128 x BN output tile (rows m0.., columns n0..) of C = alpha A B^T; the
+// tensor maps may live in kernel parameters or in global memory.
 template <int BN, typename OutT>
-__global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
-                                                         const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
-                                                         OutT* __restrict__ C, int64_t c_m, int64_t c_n, double alpha,
-                                                         int accumulate, int32_t* __restrict__ err) {
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
+__device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMap* tmB, int M, int N, int K, int m0,
+                                        int n0, OutT* __restrict__ C, int64_t c_m, int64_t c_n, double alpha,
+                                        int accumulate, int32_t* __restrict__ err, uint8_t* smem_raw) {
     // 1024-byte alignment of the stage buffers (the swizzle atoms)
     TcSmem<BN>& sm = *reinterpret_cast<TcSmem<BN>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
-    const int m0 = blockIdx.y * kTcBM;
-    const int n0 = blockIdx.x * BN;
     const int nk = K / kTcBK;
     constexpr uint32_t kTmemCols = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
 
@@ -135,8 +134,8 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
             if (kb >= kTcStages) ok = mbar_wait(&sm.empty[s], ((kb / kTcStages) + 1) & 1);
             if (!ok) break;
             mbar_expect_tx(&sm.full[s], bytes);
-            tma_load_2d(sm.a[s], &tmA, &sm.full[s], kb * kTcBK, m0);
-            tma_load_2d(sm.b[s], &tmB, &sm.full[s], kb * kTcBK, n0);
+            tma_load_2d(sm.a[s], tmA, &sm.full[s], kb * kTcBK, m0);
+            tma_load_2d(sm.b[s], tmB, &sm.full[s], kb * kTcBK, n0);
         }
         if (!ok) atomicExch(err, VTB_TIMEOUT);
     } else if (tid == 32) {
@@ -206,6 +205,54 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
     if (warp == 0) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
+}
+
+template <int BN, typename OutT>
+__global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                         const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
+                                                         OutT* __restrict__ C, int64_t c_m, int64_t c_n, double alpha,
+                                                         int accumulate, int32_t* __restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    tc_tile<BN, OutT>(&tmA, &tmB, M, N, K, blockIdx.y * kTcBM, blockIdx.x * BN, C, c_m, c_n, alpha, accumulate, err,
+                      smem_raw);
+}
+
+// Grouped GEMM: many independent problems C_p = A_p B_p^T (float32 output,
+// row-major, leading dimension ldc) in one launch.  Problem p owns the tiles
+// [tile_start, tile_start + ceil(M/128) * ceil(N/BN)); a CTA finds its
+// problem by binary search and runs the same tile pipeline, its tensor maps
+// read from global memory (written by the host before the launch).
+struct TcGroupProblem {
+    CUtensorMap ma;
+    CUtensorMap mb;
+    float* C;
+    int64_t ldc;
+    int M, N, K, tile_start;
+    int32_t* err;
+    int pad[6];
+};
+
+template <int BN>
+__global__ void __launch_bounds__(128, 1) tc_gemm_grouped_kernel(const TcGroupProblem* __restrict__ probs, int nprob) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    const int tile = blockIdx.x;
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (probs[mid].tile_start <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    const TcGroupProblem* p = probs + lo;
+    if (threadIdx.x == 0) {
+        // the TMA unit reads the maps through the tensor-map proxy: order
+        // it after the generic-proxy writes that placed them
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&p->ma) : "memory");
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&p->mb) : "memory");
+    }
+    const int ntn = (p->N + BN - 1) / BN;
+    const int t = tile - p->tile_start;
+    tc_tile<BN, float>(&p->ma, &p->mb, p->M, p->N, p->K, (t / ntn) * kTcBM, (t % ntn) * BN, p->C, p->ldc, 1, 1.0, 0,
+                       p->err, smem_raw);
 }
 
 // ------------------------------------------------------------------ split-bf16 operands
@@ -333,4 +380,68 @@ VTB_API int vtb_tc_gemm_bf16_bn(const void* A, int M, const void* B, int N, int 
 VTB_API int vtb_tc_gemm_bf16(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
                              int out_f64, double alpha, int accumulate, int32_t* err, void* stream) {
     return vtb_tc_gemm_bf16_bn(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, 128, stream);
+}
+
+VTB_API int64_t vtb_tc_group_bytes(int nprob) { return nprob > 0 ? (int64_t)nprob * (int64_t)sizeof(TcGroupProblem) : 0; }
+
+// Fill the HOST descriptor array of a grouped GEMM (nprob problems C_p =
+// A_p B_p^T, A_p M_p x K_p and B_p N_p x K_p bf16 K-major, C_p float32
+// row-major with leading dimension ldc_p; all arrays are host arrays of the
+// problems' device pointers and sizes); *total_tiles receives the grid size.
+// The caller copies the array to device memory (vtb_tc_group_bytes bytes,
+// 64-byte aligned) before vtb_tc_gemm_grouped.
+VTB_API int vtb_tc_group_build(void* host_desc, int nprob, const uint64_t* A, const int* M, const uint64_t* B,
+                               const int* N, const int* K, const uint64_t* C, const int64_t* ldc, const uint64_t* err,
+                               int bn, int* total_tiles) {
+    VTB_CHECK_ARG(host_desc && nprob > 0 && A && M && B && N && K && C && ldc && err && total_tiles);
+    VTB_CHECK_ARG(bn == 64 || bn == 128 || bn == 256);
+    TcGroupProblem* d = reinterpret_cast<TcGroupProblem*>(host_desc);
+    int tiles = 0;
+    for (int p = 0; p < nprob; ++p) {
+        VTB_CHECK_ARG(M[p] > 0 && N[p] > 0 && K[p] > 0 && (K[p] % kTcBK) == 0 && A[p] && B[p] && C[p] && err[p]);
+        VTB_CHECK_ARG((A[p] & 15) == 0 && (B[p] & 15) == 0);
+        memset(&d[p], 0, sizeof(TcGroupProblem));
+        int st = make_map(&d[p].ma, reinterpret_cast<const void*>(A[p]), M[p], K[p], K[p], kTcBM);
+        if (st) return st;
+        st = make_map(&d[p].mb, reinterpret_cast<const void*>(B[p]), N[p], K[p], K[p], bn);
+        if (st) return st;
+        d[p].C = reinterpret_cast<float*>(C[p]);
+        d[p].ldc = ldc[p];
+        d[p].M = M[p];
+        d[p].N = N[p];
+        d[p].K = K[p];
+        d[p].tile_start = tiles;
+        d[p].err = reinterpret_cast<int32_t*>(err[p]);
+        tiles += ceil_div(M[p], kTcBM) * ceil_div(N[p], bn);
+    }
+    *total_tiles = tiles;
+    return VTB_OK;
+}
+
+template <int BN>
+static int launch_grouped(const void* desc, int nprob, int tiles, cudaStream_t s) {
+    const size_t sm = sizeof(TcSmem<BN>) + 1024;
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [&]() {
+        attr = cudaFuncSetAttribute(tc_gemm_grouped_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    });
+    if (attr != cudaSuccess) {
+        set_last_cuda_error(attr);
+        return VTB_CUDA_ERR;
+    }
+    tc_gemm_grouped_kernel<BN><<<tiles, 128, sm, s>>>(reinterpret_cast<const TcGroupProblem*>(desc), nprob);
+    return launch_status();
+}
+
+// One launch over all problems of a descriptor array built with the same bn.
+VTB_API int vtb_tc_gemm_grouped(const void* dev_desc, int nprob, int total_tiles, int bn, void* stream) {
+    VTB_CHECK_ARG(dev_desc && nprob > 0 && total_tiles > 0 && ((uintptr_t)dev_desc & 63) == 0);
+    cudaStream_t s = as_stream(stream);
+    switch (bn) {
+        case 64: return launch_grouped<64>(dev_desc, nprob, total_tiles, s);
+        case 128: return launch_grouped<128>(dev_desc, nprob, total_tiles, s);
+        case 256: return launch_grouped<256>(dev_desc, nprob, total_tiles, s);
+        default: return VTB_BAD_ARG;
+    }
 }
