@@ -454,7 +454,8 @@ def run_serve(args, rank, world, local):
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
-    srv = serving.Server(budget_bytes=args.budget_gb * 10 ** 9, workers=args.workers, device=dev)
+    srv = serving.Server(budget_bytes=args.budget_gb * 10 ** 9, workers=args.workers, device=dev,
+                         solvers=args.solvers)
     done = srv.run(reqs, keep_result=lambda r: r.rid < args.plain_sample)
     clk = clocks.stop()
     st = serving.summary(done, srv.wall_s)
@@ -477,8 +478,8 @@ def run_serve(args, rank, world, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (bf16x3 projection, split-bf16 Gram, f32 Cholesky, f64 refinement)",
             "data": "synthetic (seeded Dirichlet-bandlimited video, float32 input)",
             "config": {"workload": "serve: %d requests, Poisson %.0f/s (seed 3), batch-clip sizes (seed 3), "
-                                   "budget %d GB, tick 2 ms, %d workers"
-                                   % (len(reqs), args.rate, args.budget_gb, args.workers)},
+                                   "budget %d GB, tick 2 ms, %d encode workers, %d solver threads"
+                                   % (len(reqs), args.rate, args.budget_gb, args.workers, args.solvers)},
             "latency_ms": {"p50": st["p50_ms"], "p95": st["p95_ms"], "p99": st["p99_ms"], "mean": st["mean_ms"]},
             "phases_mean_ms": st["phases_mean_ms"],
             "completed": st["completed"], "failed": st["failed"], "solvers": solvers,
@@ -760,7 +761,8 @@ def main():
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=200.0)
     ap.add_argument("--budget-gb", type=int, default=120)
-    ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--workers", type=int, default=3)
+    ap.add_argument("--solvers", type=int, default=2)
     ap.add_argument("--plain-sample", type=int, default=8)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -6,8 +6,9 @@ Kronecker Gram of the decoder has only (2 Mt + 1)^2 columns (289 at Mt = 8),
 where a width that divides them evenly wastes no tensor-core work, while the
 RF projection has hundreds of RF columns and many rows.  ``tile_for`` times
 every candidate on the caller's own operands (CUDA events, a few launches
-each) the first time a shape is seen, and reuses the choice afterwards; the
-choices are kept per process and, when ``VTB_AUTOTUNE_CACHE`` names a file,
+each) the first time a shape class (exact column count, row and reduction
+lengths rounded to powers of two) is seen, and reuses the choice afterwards;
+the choices are kept per process and, when ``VTB_AUTOTUNE_CACHE`` names a file,
 in that JSON file across processes.  ``VTB_AUTOTUNE=0`` disables tuning
 (BN = 128).  Tuning launches and synchronises, so it must not run inside a
 CUDA graph capture: callers run once eagerly before capturing.
@@ -31,8 +32,33 @@ _loaded = False
 timings = {}      # shape -> {bn: ms}, for reports
 
 
+def _bucket(x):
+    return max(0, int(x - 1).bit_length())
+
+
 def _key(M, N, K, out_f64):
-    return "%d,%d,%d,%d" % (M, N, K, int(bool(out_f64)))
+    """Shape class: the exact column count (the tile waste depends on it) and
+    the row and reduction lengths rounded up to powers of two."""
+    return "%d,%d,%d,%d" % (_bucket(M), N, _bucket(K), int(bool(out_f64)))
+
+
+_frozen = threading.local()
+
+
+class frozen(object):
+    """Within this context (per thread) no tuning runs: shapes already tuned
+    keep their width, others get DEFAULT_BN.  For concurrent users such as a
+    serving loop, where timing launches would both stall and be distorted by
+    the other threads' work."""
+
+    def __enter__(self):
+        self._prev = getattr(_frozen, "on", False)
+        _frozen.on = True
+        return self
+
+    def __exit__(self, *exc):
+        _frozen.on = self._prev
+        return False
 
 
 def _load():
@@ -70,7 +96,7 @@ def tile_for(M, N, K, out_f64, launch, reps=3):
         _load()
         if key in _cache:
             return _cache[key]
-    if torch.cuda.is_current_stream_capturing():
+    if torch.cuda.is_current_stream_capturing() or getattr(_frozen, "on", False):
         return DEFAULT_BN
     res = {}
     for bn in CANDIDATES:

@@ -16,7 +16,7 @@ runs in ticks of ``tick_s`` (2 ms):
    are solved together in mixed precision (vtem_b200.batch.MixedSolvePlan):
    requests with equal system size K share one batched float32 Cholesky,
    all share one batched triangular-solve launch per refinement sweep; a
-   request whose pseudoinverse might truncate goes to the solver thread
+   request whose pseudoinverse might truncate goes to a solver thread
    (float64 Cholesky, else the eigen-pseudoinverse batched over padded
    sizes), and one with fewer intervals than coefficients was solved in the
    spike space by its encoder;
@@ -40,7 +40,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from . import batch, fast
+from . import autotune, batch, fast
 from ._abi import call, dptr, stream_ptr
 from .workloads import ellipse_mask
 
@@ -136,7 +136,7 @@ class Server(object):
     """Request loop over one GPU (see the module docstring)."""
 
     def __init__(self, budget_bytes=120 * 10 ** 9, workers=2, tick_s=0.002, device="cuda", precision="bf16x3",
-                 switch_interval=2e-4, sweeps=1):
+                 switch_interval=2e-4, sweeps=1, solvers=2):
         self.budget = int(budget_bytes)
         self.workers = int(workers)
         self.tick_s = float(tick_s)
@@ -146,6 +146,7 @@ class Server(object):
         self.device = dev
         self.precision = precision
         self.sweeps = int(sweeps)
+        self.solvers = max(1, int(solvers))   # threads for the float64 fallbacks
         # the interpreter's thread switch interval while serving: shorter
         # than a kernel launch sequence, so that a thread with device work to
         # issue does not wait behind another thread's Python
@@ -159,13 +160,22 @@ class Server(object):
     def _new_stream(self):
         return torch.cuda.Stream(device=self.device)
 
+    def _solver_stream(self):
+        tid = threading.get_ident()
+        st = self._eig_streams.get(tid)
+        if st is None:
+            st = self._eig_streams[tid] = self._new_stream()
+        return st
+
     def _bind_thread(self):
         torch.cuda.set_device(self.device)
 
     # -- phase 1 (worker thread, own stream) -------------------------------
     def _phase_a(self, job):
         req = job.req
-        with torch.cuda.stream(job.stream):
+        # no GEMM tile tuning inside the loop (it would time launches under
+        # the other threads' load and stall this worker)
+        with torch.cuda.stream(job.stream), autotune.frozen():
             V = req.video.to(self.device, non_blocking=True)
             p = batch.encode_clip_problem(req.workload, self.device, video=V, precision=self.precision)
             n = int(p.tk1.numel())
@@ -212,7 +222,7 @@ class Server(object):
         float64 Cholesky where its pivot test passes, else the truncated
         eigen-pseudoinverse, batched over padded sizes.  Returns when the
         solutions are on the device."""
-        with torch.cuda.stream(self._eig_stream):
+        with torch.cuda.stream(self._solver_stream()):
             st = torch.cuda.current_stream(self.device)
             for j in jobs:
                 st.wait_event(j.ev_s)
@@ -264,7 +274,7 @@ class Server(object):
 
         The loop thread never waits on the device: it launches work and
         polls events.  Encoding runs on ``workers`` threads, eigen-
-        pseudoinverses on one solver thread."""
+        pseudoinverses on ``solvers`` solver threads (own streams)."""
         pending = sorted(requests, key=lambda r: r.arrival)
         for r in pending:
             if r.bytes > self.budget:
@@ -272,12 +282,12 @@ class Server(object):
         waiting, ready, checking, in_b = [], [], [], []
         done = []
         lock = threading.Lock()
-        encoded, solved = [], []            # filled by the encode workers / the solver thread
+        encoded, solved = [], []            # filled by the encode workers / the solver threads
         work_q, eig_q = queue.Queue(), queue.Queue()
         thread_errors = []
         streams = [self._new_stream() for _ in range(self.workers)]
         self._solve_stream = self._new_stream()
-        self._eig_stream = self._new_stream()
+        self._eig_streams = {}
 
         def encoder(st):
             try:
@@ -299,6 +309,7 @@ class Server(object):
                     encoded.append(job)
 
         def solver():
+            # one stream per solver thread
             try:
                 self._bind_thread()
             except Exception as e:
@@ -321,7 +332,7 @@ class Server(object):
             sys.setswitchinterval(self.switch_interval)
         t0 = time.perf_counter()
         threads = [threading.Thread(target=encoder, args=(st,), daemon=True) for st in streams]
-        threads.append(threading.Thread(target=solver, daemon=True))
+        threads.extend(threading.Thread(target=solver, daemon=True) for _ in range(self.solvers))
         for t in threads:
             t.start()
         nreq = len(pending)
@@ -378,7 +389,7 @@ class Server(object):
                             j.req.state = "solving"
                         checking.append(self._launch_chol(coeff))
                 # 3. finished factorisations: accepted -> synthesis, refused ->
-                # the solver thread (grouped by size)
+                # a solver thread (grouped by padded size there)
                 still = []
                 for cb in checking:
                     if not cb.query():
@@ -417,7 +428,8 @@ class Server(object):
         finally:
             for _ in range(self.workers):
                 work_q.put(None)
-            eig_q.put(None)
+            for _ in range(self.solvers):
+                eig_q.put(None)
             for t in threads:
                 t.join()
             sys.setswitchinterval(old_switch)
