@@ -19,6 +19,7 @@
 // space-time basis: A[t, s] = sum_m a[s, m] e^{jmWt}, then per frame
 // u = Re(ey^T A_t ex) on the decode grid (synth_kernel), whose output write is
 // the one HBM-sized stream of the whole decode.
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -179,24 +180,32 @@ __global__ void __launch_bounds__(256) kron_gram_kernel(const double2* __restric
     }
 }
 
-// b[(s, m)] = sum_n d[n][s] g[n][m]: one block per spatial index s; warp w
-// owns the temporal indices m = w, w+8, ..., its lanes stride over the
-// neurons (each d[n][s] loaded once for all of the warp's m), four
-// independent partial sums per m keep the loads in flight, then a warp
-// reduction.  Deterministic (fixed summation order).
-constexpr int kRhsMaxM = 4;   // m per warp: Kt <= 32
+// b[(s, m)] = sum_n d[n][s] g[n][m]: a cluster of kRhsSplit CTAs per spatial
+// index s, each summing a contiguous quarter of the neurons: warp w owns the
+// temporal indices m = w, w+8, ..., its lanes stride over the neurons (each
+// d[n][s] loaded once for all of the warp's m) with two partial sums per m,
+// then a warp reduction; the cluster's first CTA adds the others' partial
+// sums through distributed shared memory in rank order (deterministic).
+constexpr int kRhsMaxM = 4;   // m per warp per pass: 32 per pass
+constexpr int kRhsSplit = 4;  // CTAs per cluster (neuron quarters)
 
-__global__ void __launch_bounds__(256) kron_rhs_kernel(const double2* __restrict__ d, int N, int Ks,
-                                                       const double2* __restrict__ gn, int Kt,
-                                                       double2* __restrict__ b) {
-    const int s = blockIdx.x;
+__global__ void __cluster_dims__(kRhsSplit, 1, 1) __launch_bounds__(256)
+    kron_rhs_kernel(const double2* __restrict__ d, int N, int Ks, const double2* __restrict__ gn, int Kt,
+                    double2* __restrict__ b) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    __shared__ double2 part[32];
+    const int rank = (int)cluster.block_rank();
+    const int s = blockIdx.x / kRhsSplit;
+    const int nq = (N + kRhsSplit - 1) / kRhsSplit;
+    const int n_lo = rank * nq, n_hi = min(N, n_lo + nq);
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int mbase = 0; mbase < Kt; mbase += 8 * kRhsMaxM) {
         double2 acc[kRhsMaxM][2];
 #pragma unroll
         for (int q = 0; q < kRhsMaxM; ++q) acc[q][0] = acc[q][1] = make_double2(0, 0);
-        int n = lane;
-        for (; n + 32 < N; n += 64) {
+        int n = n_lo + lane;
+        for (; n + 32 < n_hi; n += 64) {
 #pragma unroll
             for (int u2 = 0; u2 < 2; ++u2) {
                 const int nu = n + 32 * u2;
@@ -212,7 +221,7 @@ __global__ void __launch_bounds__(256) kron_rhs_kernel(const double2* __restrict
                 }
             }
         }
-        for (; n < N; n += 32) {
+        for (; n < n_hi; n += 32) {
             const double2 dv = d[(int64_t)n * Ks + s];
 #pragma unroll
             for (int q = 0; q < kRhsMaxM; ++q) {
@@ -232,9 +241,23 @@ __global__ void __launch_bounds__(256) kron_rhs_kernel(const double2* __restrict
                 x += __shfl_xor_sync(0xffffffffu, x, o);
                 y += __shfl_xor_sync(0xffffffffu, y, o);
             }
-            const int m = mbase + w + 8 * q;
-            if (lane == 0 && m < Kt) b[(int64_t)s * Kt + m] = make_double2(x, y);
+            if (lane == 0) part[w + 8 * q] = make_double2(x, y);
         }
+        cluster.sync();
+        if (rank == 0 && threadIdx.x < 32) {
+            const int m = mbase + threadIdx.x;
+            if (m < Kt) {
+                double2 t = part[threadIdx.x];
+#pragma unroll
+                for (int r = 1; r < kRhsSplit; ++r) {
+                    const double2 o = cluster.map_shared_rank(part, r)[threadIdx.x];
+                    t.x += o.x;
+                    t.y += o.y;
+                }
+                b[(int64_t)s * Kt + m] = t;
+            }
+        }
+        cluster.sync();   // the partial sums stay valid until rank 0 has read them
     }
 }
 
@@ -568,7 +591,7 @@ VTB_API int vtb_coeff_gram(const double* d, int N, int Ks, const double* Wn, con
                                                            reinterpret_cast<double2*>(M), ldm);
     int st = launch_status();
     if (st) return st;
-    kron_rhs_kernel<<<Ks, 256, 0, as_stream(stream)>>>(
+    kron_rhs_kernel<<<Ks * kRhsSplit, 256, 0, as_stream(stream)>>>(
         reinterpret_cast<const double2*>(d), N, Ks, reinterpret_cast<const double2*>(gn), Kt,
         reinterpret_cast<double2*>(b));
     return launch_status();
@@ -934,7 +957,7 @@ VTB_API int vtb_coeff_scatter(const float* C, int64_t ldc, const int32_t* ps, co
 
 VTB_API int vtb_coeff_rhs(const double* d, int N, int Ks, const double* gn, int Kt, double* b, void* stream) {
     VTB_CHECK_ARG(N > 0 && Ks > 0 && Kt > 0 && d && gn && b);
-    kron_rhs_kernel<<<Ks, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(d), N, Ks,
+    kron_rhs_kernel<<<Ks * kRhsSplit, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(d), N, Ks,
                                                       reinterpret_cast<const double2*>(gn), Kt,
                                                       reinterpret_cast<double2*>(b));
     return launch_status();
@@ -954,7 +977,7 @@ VTB_API int vtb_coeff_residual(const double* tk1, const double* tk2, const int32
                                              reinterpret_cast<const double2*>(a), reinterpret_cast<double2*>(gres));
     int st = launch_status();
     if (st) return st;
-    kron_rhs_kernel<<<Ks, 256, 0, s>>>(reinterpret_cast<const double2*>(d), N, Ks,
+    kron_rhs_kernel<<<Ks * kRhsSplit, 256, 0, s>>>(reinterpret_cast<const double2*>(d), N, Ks,
                                        reinterpret_cast<const double2*>(gres), Kt, reinterpret_cast<double2*>(r));
     return launch_status();
 }
@@ -1011,7 +1034,7 @@ VTB_API int vtb_coeff_from_spike_weights(const double* tk1, const double* tk2, c
     temporal_weighted_kernel<<<N, 64, 0, s>>>(tk1, tk2, ind, nspk, w, Mt, W, reinterpret_cast<double2*>(g));
     int st = launch_status();
     if (st) return st;
-    kron_rhs_kernel<<<Ks, 256, 0, s>>>(reinterpret_cast<const double2*>(d), N, Ks, reinterpret_cast<const double2*>(g),
+    kron_rhs_kernel<<<Ks * kRhsSplit, 256, 0, s>>>(reinterpret_cast<const double2*>(d), N, Ks, reinterpret_cast<const double2*>(g),
                                        Kt, reinterpret_cast<double2*>(a));
     return launch_status();
 }
