@@ -217,7 +217,7 @@ int vtb_coeff_pack(const double* Ds, int N, int Kfull, const int32_t* smap, int 
 
 /* Per-neuron temporal Gram Wn[n][m][m'] = sum_k conj(T_k(m)) T_k(m') and
  * gn[n][m] = sum_k conj(T_k(m)) q_k (q_k as compute_q_Kernel), m in [-Mt, Mt],
- * W = Wt/Mt. */
+ * W = Wt/Mt, Mt <= 21. */
 int vtb_coeff_temporal_gram(const double* tk1, const double* tk2, const int32_t* ind, int nspk, int N,
                             const double* kappa, const double* delta, const double* bias, const double* norm, int Mt,
                             double W, double* Wn, double* gn, void* stream);

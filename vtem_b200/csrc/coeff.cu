@@ -28,14 +28,44 @@
 
 namespace vtb {
 
-__device__ __forceinline__ int lb_i32(const int32_t* a, int n, int v) {
+// lower_bound of v in the sorted a[0..n) by one full warp: 32-way probes
+// (three dependent rounds for 25k entries instead of fifteen), the same
+// result on every lane.
+__device__ int warp_lower_bound(const int32_t* __restrict__ a, int n, int v) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     int lo = 0, hi = n;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (a[mid] < v) lo = mid + 1;
-        else hi = mid;
+    while (hi - lo > 32) {
+        const int step = (hi - lo + 31) / 32;
+        const int pos = lo + lane * step;
+        const int c = __popc(__ballot_sync(full, pos < hi && a[pos] < v));
+        if (c == 0) {
+            hi = lo;
+        } else {
+            const int nlo = lo + (c - 1) * step + 1;
+            hi = min(hi, lo + c * step);
+            lo = nlo;
+        }
     }
-    return lo;
+    const int pos = lo + lane;
+    return lo + __popc(__ballot_sync(full, pos < hi && a[pos] < v));
+}
+
+// [lo, hi) of neuron nr in the neuron-sorted index array, found by warp 0 and
+// shared with the block (all threads must call it).
+__device__ __forceinline__ void neuron_range(const int32_t* __restrict__ ind, int nspk, int nr, int& lo, int& hi) {
+    __shared__ int s_range[2];
+    if (threadIdx.x < 32) {
+        const int a = warp_lower_bound(ind, nspk, nr);
+        const int b = warp_lower_bound(ind, nspk, nr + 1);
+        if (threadIdx.x == 0) {
+            s_range[0] = a;
+            s_range[1] = b;
+        }
+    }
+    __syncthreads();
+    lo = s_range[0];
+    hi = s_range[1];
 }
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -48,8 +78,32 @@ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
 // ------------------------------------------------------------------ W_n, g_n
 // One block per neuron.  Spikes must be sorted by neuron.  T_k(m) for m in
 // [-Mt, Mt] uses the product form (2/(mW)) sin(mW dt/2) e^{jmW tbar}, exact
-// for the integral and free of the cancellation of e^{a} - e^{b}.
+// for the integral and free of the cancellation of e^{a} - e^{b}; its
+// harmonics come from powers of e^{jW tbar} and e^{jW dt/2} (two sincos per
+// interval; a few ulp per power).
 constexpr int kTChunk = 32;
+
+__device__ __forceinline__ void spike_T(double a, double b, int Mt, double W, double2* __restrict__ T) {
+    const double d = b - a;
+    double s1, c1, sh, ch;
+    sincos(W * (0.5 * (a + b)), &s1, &c1);
+    sincos(0.5 * W * d, &sh, &ch);
+    T[Mt] = make_double2(d, 0.0);
+    const double2 e1 = make_double2(c1, s1), h1 = make_double2(ch, sh);
+    double2 pe = make_double2(1.0, 0.0), ph = make_double2(1.0, 0.0);
+    for (int m = 1; m <= Mt; ++m) {
+        pe = cmul(pe, e1);
+        ph = cmul(ph, h1);
+        const double amp = (2.0 / (m * W)) * ph.y;   // (2/(mW)) sin(mW d/2), even in m
+        T[Mt + m] = make_double2(amp * pe.x, amp * pe.y);
+        T[Mt - m] = make_double2(amp * pe.x, -amp * pe.y);
+    }
+}
+
+// Thread t owns the entries e = t, t+256, ... (at most kTgEntries) of the
+// upper triangle (m <= m') of the Hermitian W_n (the mirror is written from
+// the same sum); threads m < Kt also g_n[m].
+constexpr int kTgEntries = 4;   // Kt(Kt+1)/2 <= 1024: Mt <= 21
 
 __global__ void __launch_bounds__(256) temporal_gram_kernel(
     const double* __restrict__ tk1, const double* __restrict__ tk2, const int32_t* __restrict__ ind, int nspk,
@@ -59,43 +113,46 @@ __global__ void __launch_bounds__(256) temporal_gram_kernel(
     const int Kt = 2 * Mt + 1;
     double2* sq = sT + kTChunk * Kt;
     const int nr = blockIdx.x;
-    const int lo = lb_i32(ind, nspk, nr), hi = lb_i32(ind, nspk, nr + 1);
-    const int KK = Kt * Kt;
+    int lo, hi;
+    neuron_range(ind, nspk, nr, lo, hi);
+    const int KK = Kt * Kt, nup = Kt * (Kt + 1) / 2;
     const double kd = kappa[nr] * delta[nr], bb = bias[nr], nn = norm[nr];
-    // each thread owns entry e of W_n (grid.y slices the Kt x Kt entries),
-    // and block row 0 also g_n[m] for threads m < Kt
-    const int e = blockIdx.y * blockDim.x + threadIdx.x;
-    const bool own_g = blockIdx.y == 0 && threadIdx.x < Kt;
-    double2 acc = make_double2(0, 0);
+    int em[kTgEntries], emp[kTgEntries];
+    double2 acc[kTgEntries];
+#pragma unroll
+    for (int u = 0; u < kTgEntries; ++u) {
+        int e = threadIdx.x + u * blockDim.x, m = 0;
+        em[u] = -1;
+        emp[u] = 0;
+        acc[u] = make_double2(0, 0);
+        if (e < nup) {
+            while (e >= Kt - m) {
+                e -= Kt - m;
+                ++m;
+            }
+            em[u] = m;
+            emp[u] = m + e;
+        }
+    }
+    const bool own_g = threadIdx.x < Kt;
     double2 gacc = make_double2(0, 0);
     for (int k0 = lo; k0 < hi; k0 += kTChunk) {
         const int nk = min(kTChunk, hi - k0);
         __syncthreads();
-        for (int x = threadIdx.x; x < nk * Kt; x += blockDim.x) {
-            const int kk = x / Kt, mi = x % Kt, m = mi - Mt;
-            const double a = tk1[k0 + kk], b = tk2[k0 + kk];
-            const double d = b - a;
-            double2 T;
-            if (m == 0) {
-                T = make_double2(d, 0.0);
-            } else {
-                const double mw = m * W;
-                const double amp = (2.0 / mw) * sin(0.5 * mw * d);
-                double s, c;
-                sincos(mw * (0.5 * (a + b)), &s, &c);
-                T = make_double2(amp * c, amp * s);
-            }
-            sT[kk * Kt + mi] = T;
-            if (mi == 0) sq[kk].x = (kd - bb * d) * nn;  // q_k, compute_q_Kernel's formula
+        if (threadIdx.x < nk) {
+            const double a = tk1[k0 + threadIdx.x], b = tk2[k0 + threadIdx.x];
+            spike_T(a, b, Mt, W, sT + threadIdx.x * Kt);
+            sq[threadIdx.x].x = (kd - bb * (b - a)) * nn;  // q_k, compute_q_Kernel's formula
         }
         __syncthreads();
-        if (e < KK) {
-            const int m = e / Kt, mp = e % Kt;
+#pragma unroll
+        for (int u = 0; u < kTgEntries; ++u) {
+            if (em[u] < 0) continue;
             for (int kk = 0; kk < nk; ++kk) {
-                const double2 a = sT[kk * Kt + m], b = sT[kk * Kt + mp];
+                const double2 a = sT[kk * Kt + em[u]], b = sT[kk * Kt + emp[u]];
                 // conj(a) * b
-                acc.x += a.x * b.x + a.y * b.y;
-                acc.y += a.x * b.y - a.y * b.x;
+                acc[u].x += a.x * b.x + a.y * b.y;
+                acc[u].y += a.x * b.y - a.y * b.x;
             }
         }
         if (own_g) {
@@ -107,7 +164,13 @@ __global__ void __launch_bounds__(256) temporal_gram_kernel(
             }
         }
     }
-    if (e < KK) Wn[(int64_t)nr * KK + e] = acc;
+#pragma unroll
+    for (int u = 0; u < kTgEntries; ++u) {
+        if (em[u] < 0) continue;
+        const int m = em[u], mp = emp[u];
+        Wn[(int64_t)nr * KK + m * Kt + mp] = acc[u];
+        if (m != mp) Wn[(int64_t)nr * KK + mp * Kt + m] = make_double2(acc[u].x, -acc[u].y);
+    }
     if (own_g) gn[(int64_t)nr * Kt + threadIdx.x] = gacc;
 }
 
@@ -566,8 +629,8 @@ VTB_API int vtb_coeff_temporal_gram(const double* tk1, const double* tk2, const 
     VTB_CHECK_ARG(nspk == 0 || (tk1 && tk2 && ind));
     const int Kt = 2 * Mt + 1;
     const size_t sm = (size_t)kTChunk * (Kt + 1) * sizeof(double2);
-    dim3 grid(N, ceil_div((int64_t)Kt * Kt, 256));
-    temporal_gram_kernel<<<grid, 256, sm, as_stream(stream)>>>(tk1, tk2, ind, nspk, kappa, delta, bias, norm, Mt, W,
+    VTB_CHECK_ARG(Kt * (Kt + 1) / 2 <= 256 * kTgEntries);
+    temporal_gram_kernel<<<N, 256, sm, as_stream(stream)>>>(tk1, tk2, ind, nspk, kappa, delta, bias, norm, Mt, W,
                                                            reinterpret_cast<double2*>(Wn),
                                                            reinterpret_cast<double2*>(gn));
     return launch_status();
@@ -857,7 +920,8 @@ __global__ void __launch_bounds__(256) coeff_residual_kernel(
     double2* T = v + Kt;             // kTChunk x Kt
     double* y = reinterpret_cast<double*>(T + kTChunk * Kt);  // kTChunk
     const int nr = blockIdx.x;
-    const int lo = lb_i32(ind, nspk, nr), hi = lb_i32(ind, nspk, nr + 1);
+    int lo, hi;
+    neuron_range(ind, nspk, nr, lo, hi);
     const double kd = kappa[nr] * delta[nr], bb = bias[nr], nn = norm[nr];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // v(m): warp w handles m = w, w+8, ...
@@ -878,22 +942,7 @@ __global__ void __launch_bounds__(256) coeff_residual_kernel(
     for (int k0 = lo; k0 < hi; k0 += kTChunk) {
         const int nk = min(kTChunk, hi - k0);
         __syncthreads();
-        for (int x = threadIdx.x; x < nk * Kt; x += blockDim.x) {
-            const int kk = x / Kt, mi = x % Kt, m = mi - Mt;
-            const double ta = tk1[k0 + kk], tb = tk2[k0 + kk];
-            const double dtk = tb - ta;
-            double2 Tv;
-            if (m == 0) {
-                Tv = make_double2(dtk, 0.0);
-            } else {
-                const double mw = m * W;
-                const double amp = (2.0 / mw) * sin(0.5 * mw * dtk);
-                double s, c;
-                sincos(mw * (0.5 * (ta + tb)), &s, &c);
-                Tv = make_double2(amp * c, amp * s);
-            }
-            T[kk * Kt + mi] = Tv;
-        }
+        if (threadIdx.x < nk) spike_T(tk1[k0 + threadIdx.x], tk2[k0 + threadIdx.x], Mt, W, T + threadIdx.x * Kt);
         __syncthreads();
         // y_k, one warp per spike
         for (int kk = w; kk < nk; kk += 8) {
@@ -1003,7 +1052,8 @@ __global__ void __launch_bounds__(256) temporal_weighted_kernel(const double* __
                                                                 double2* __restrict__ g) {
     const int Kt = 2 * Mt + 1;
     const int nr = blockIdx.x;
-    const int lo = lb_i32(ind, nspk, nr), hi = lb_i32(ind, nspk, nr + 1);
+    int lo, hi;
+    neuron_range(ind, nspk, nr, lo, hi);
     for (int mi = threadIdx.x; mi < Kt; mi += blockDim.x) {
         const int m = mi - Mt;
         double gr = 0.0, gi = 0.0;
