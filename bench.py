@@ -295,6 +295,7 @@ def run_ours(args, rank, world, local):
                          "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                          "traffic": measured_traffic(voxels), "algorithmic_bytes": synth_bytes,
                          "avg_ms": synth_avg * 1e3},
+            "roofline_tensor": gram_gemm_roofline(decmix, peaks),
             "variants_ms_per_step": {"mixed": mix_ms / args.steps, "coeff_f64": f64_ms / args.steps},
             "mixed_vs_coeff_f64_rel_l2": rel_mix_f64, "mixed_residual_rel": resid,
             "stages_ms": {"coefficients": (tot_ms - sum(synth_ms)) / args.steps,
@@ -312,6 +313,38 @@ def run_ours(args, rank, world, local):
         dist.barrier()
         dist.destroy_process_group()
     return result
+
+
+def gram_gemm_roofline(dec, peaks, reps=20):
+    """The mixed decoder's tensor-core Kronecker Gram (the decode's tensor-
+    bound kernel) timed alone with CUDA events on its own operands, at its
+    autotuned tile width, against the measured bf16 peak.  Tensor work counts
+    the three split-bf16 products; the 158 MB RF-bank operand exceeds L2, so
+    repeated launches read it from HBM as a decode does."""
+    import torch
+    from vtem_b200 import autotune
+    from vtem_b200._abi import dptr, stream_ptr
+    KK, M, K = dec.Kt * dec.Kt, 2 * dec.npairs, 3 * dec.Kp2
+    s = stream_ptr()
+
+    def once():
+        return autotune.gemm_bf16_tuned(dptr(dec.L3), M, dptr(dec.R3), KK, K, dptr(dec.C), KK, 1, 0, 1.0, 0,
+                                        dec._stat_ptr(7), s)
+    bn = once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        once()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    flop = 2.0 * M * KK * K
+    achieved = flop / (ms / 1e3) / 1e12
+    return {"bound": "tensor", "kernel": "tc_gemm_kernel<%d, float> (Kronecker Gram, split-bf16)" % bn,
+            "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+            "frac": achieved / peaks["bf16_tflops"], "peak_source": peaks["source"], "avg_ms": ms,
+            "tensor_flop": flop, "shape": [M, KK, K], "operand_bytes": M * K * 2 + KK * K * 2}
 
 
 def launches_mixed(dec):

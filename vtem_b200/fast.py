@@ -444,59 +444,3 @@ def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=0, mixed_sweeps=2)
     """A :class:`CoeffDecoder` on the output of ``vtdm.VTDM_prep``."""
     return CoeffDecoder(prep.Ds, prep.h_norm, prep.Mx, prep.My, Wt, Mt, prep.decPx, prep.decPy, prep.Px1, prep.Py1,
                         rcond=rcond, solver=solver, refine=refine, mixed_sweeps=mixed_sweeps)
-
-
-# Largest device scratch of one batched eigen-pseudoinverse call (matrices);
-# bigger groups are split into calls of at most this size.  Groups smaller
-# than PINV_BATCH_MIN are solved one system at a time (vtb_herm_solve mode 0).
-PINV_BATCH_BYTES = 2 << 30
-PINV_BATCH_MIN = 4
-
-
-def pinv_batched(decs, stream=None):
-    """Eigen-pseudoinverse of several decoders' systems of one size K in
-    batched eigensolver calls (``vtb_herm_pinv_batched``): each decoder's M
-    and b are rebuilt from its W_n, g_n (a previous Cholesky attempt may have
-    factorised M in place) into contiguous scratch, and its ``a`` receives
-    the truncated solution, exactly as ``solver="eig"`` gives alone.
-    Returns the device int32 tensor of per-system eigensolver statuses."""
-    if not decs:
-        return None
-    K = decs[0].K
-    if any(d.K != K or d.rcond != decs[0].rcond for d in decs):
-        raise ValueError("pinv_batched needs systems of one size and one rcond")
-    s = stream_ptr() if stream is None else stream
-    dev = decs[0].M.device
-    if len(decs) < PINV_BATCH_MIN:
-        for d in decs:
-            saved = d.solver
-            d.solver = "eig"
-            try:
-                d._solve(s)
-            finally:
-                d.solver = saved
-        return torch.zeros(len(decs), dtype=torch.int32, device=dev)
-    per = max(1, int(PINV_BATCH_BYTES // (K * K * 16)))
-    all_infos = []
-    for c0 in range(0, len(decs), per):
-        chunk = decs[c0:c0 + per]
-        B = len(chunk)
-        Mb = torch.empty((B, K, K), dtype=C128, device=dev)
-        bb = torch.empty((B, K), dtype=C128, device=dev)
-        for i, d in enumerate(chunk):
-            call("vtb_coeff_gram", dptr(d.d), d.N, d.Ks, dptr(d.Wn), dptr(d.gn), d.Kt, dptr(Mb[i]), K, dptr(bb[i]), s)
-        ab = torch.empty_like(bb)
-        nb = np.zeros(1, np.int64)
-        call("vtb_herm_pinv_batched_workspace", K, B, nb.ctypes.data)
-        work = torch.empty(int(nb[0]), dtype=torch.uint8, device=dev)
-        kept = torch.empty(B, dtype=torch.int32, device=dev)
-        infos = torch.empty(B, dtype=torch.int32, device=dev)
-        call("vtb_herm_pinv_batched", dptr(Mb), dptr(bb), dptr(ab), K, B, decs[0].rcond, dptr(work), int(nb[0]),
-             dptr(kept), dptr(infos), s)
-        for i, d in enumerate(chunk):
-            d.a.copy_(ab[i])
-            d.b.copy_(bb[i])
-            d.kept.copy_(kept[i:i + 1])
-            d.last_solver = "eig-batched"
-        all_infos.append(infos)
-    return torch.cat(all_infos)
