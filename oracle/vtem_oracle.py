@@ -600,3 +600,128 @@ def decode_window(tk1, tk2, ind, kappa, delta, bias, norm, Dsw, dirich, Wt, Mt, 
     t = np.arange(0, T, dt)
     u = reconstruct_factored(dirich, tk1, tk2, c, t, ind, norm, Mt, Wt / Mt)
     return u, c, q, G, kept
+
+
+# ---------------------------------------------------------------------------
+# Stitching  (vtem/vtdm.py)
+# ---------------------------------------------------------------------------
+
+
+def temporal_stitch(decode, start_time, end_time, dt, stitching, stitch_interval):
+    """VTDM's window loop (vtdm.py:573-699): ``decode(start, end)`` returns
+    the (frames, Py, Px) reconstruction of one window; consecutive windows
+    overlap by 20 % of the interval (at least 4 samples when the interval has
+    8 or more) and are cross-faded with a Hann ramp.  Returns the video and
+    the list of (start, end) windows decoded."""
+    end = float(end_time)
+    if stitching:
+        if stitch_interval is None:
+            stitch_interval = 20 * dt
+        stitch_interval = min(stitch_interval, end_time)
+        end = round(float(min(start_time + stitch_interval, end_time)) / dt) * dt
+        overlap = 0.2 * stitch_interval
+    else:
+        stitch_interval = float(end_time)
+        overlap = 0
+    start = float(start_time)
+    total_l = round((end_time - start_time) / dt)
+    overlap_l = round(overlap / dt)
+    if overlap_l < 3:
+        if round(stitch_interval / dt) >= 8:
+            overlap_l, overlap = 4, 4 * dt
+        else:
+            overlap_l, overlap = 0, 0
+    interval_l = round(stitch_interval / dt)
+    lw = np.hanning(2 * overlap_l)[:overlap_l].reshape(-1, 1, 1)
+    u = None
+    prev = None
+    windows = []
+    i = 0
+    while True:
+        windows.append((start, end))
+        ur = np.asarray(decode(start, end))
+        if u is None:
+            u = np.empty((total_l,) + ur.shape[1:], np.float64)
+        if overlap_l:
+            if i == 0:
+                if end_time - end < dt:
+                    u = ur
+                    break
+                u[:interval_l - overlap_l] = ur[:-overlap_l]
+                prev = ur[-overlap_l:]
+            else:
+                a = i * (interval_l - overlap_l)
+                b = (i + 1) * (interval_l - overlap_l)
+                u[a:a + overlap_l] = ur[:overlap_l] * lw + prev * (1.0 - lw)
+                if end_time - end < dt:
+                    u[a + overlap_l:] = ur[-u.shape[0] + a + overlap_l:]
+                    break
+                u[a + overlap_l:b] = ur[overlap_l:interval_l - overlap_l]
+                prev = ur[-overlap_l:]
+        else:
+            u[i * interval_l:i * interval_l + ur.shape[0]] = ur
+            if end_time - end < dt:
+                break
+        start = start + round(stitch_interval / dt) * dt - round(overlap / dt) * dt
+        end = min(start + round(stitch_interval / dt) * dt, float(end_time))
+        if float(end_time) - end < overlap:
+            end = end_time
+        i += 1
+    return u, windows
+
+
+def _edge_window(n, lo_edge, hi_edge, over):
+    """1-D tile weight of decode_video (vtdm.py:246-262): a rising Hann half
+    over the first ``over`` pixels unless the tile starts on the domain edge,
+    a falling one over the last ``over`` unless it ends there."""
+    left = 0 if lo_edge else over
+    right = 0 if hi_edge else over
+    return np.concatenate((np.hanning(2 * left)[:left], np.ones(n - left - right),
+                           1 - np.hanning(2 * right)[:right]))
+
+
+def spatial_tile_walk(domain, decPx, decPy, spatial_interval, dx, dy):
+    """decode_video's tile walk (vtdm.py:214-302), row by row from the top
+    (pixel row 0 = the domain's largest y), each row from the right edge.
+    Returns [(tile domain, row0, row1, col0, col1, weight)]."""
+    ivx = min(spatial_interval[0], decPx)
+    ivy = min(spatial_interval[1], decPy)
+    ovx, ovy = round(.2 * ivx), round(.2 * ivy)
+    tiles = []
+    start_y = max(domain[3] - ivy * dy, domain[2])
+    end_y = domain[3]
+    sy, ey = 0, ivy
+    while True:
+        start_x = max(domain[1] - ivx * dx, domain[0])
+        end_x = domain[1]
+        sx, ex = decPx - ivx, decPx
+        while True:
+            wy = _edge_window(ey - sy, sy == 0, ey == decPy, ovy)
+            wx = _edge_window(ex - sx, sx == 0, ex == decPx, ovx)
+            tiles.append(([start_x, end_x, start_y, end_y], sy, ey, sx, ex, np.outer(wy, wx)))
+            if start_x == domain[0]:
+                break
+            start_x = max(start_x - ivx * dx + ovx * dx, domain[0])
+            end_x = end_x - ivx * dx + ovx * dx
+            sx = max(sx - ivx + ovx, 0)
+            ex = ex - ivx + ovx
+        if start_y == domain[2]:
+            break
+        start_y = max(start_y - ivy * dy + ovy * dy, domain[2])
+        end_y = end_y - ivy * dy + ovy * dy
+        sy = ey - ovy
+        ey = min(sy + ivy, decPy)
+    return tiles
+
+
+def spatial_stitch(decode_tile, domain, decPx, decPy, spatial_interval, dx, dy):
+    """decode_video with spatial stitching (vtdm.py:181-309): the sum over
+    tiles of ``decode_tile(tile domain)`` (frames, rows, cols) times the
+    tile's weight."""
+    u = None
+    for dom, sy, ey, sx, ex, w in spatial_tile_walk(domain, decPx, decPy, spatial_interval, dx, dy):
+        ut = np.asarray(decode_tile(dom))
+        if u is None:
+            u = np.zeros((ut.shape[0], decPy, decPx), np.float64)
+        u[:, sy:ey, sx:ex] += ut * w
+    return u

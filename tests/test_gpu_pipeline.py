@@ -97,14 +97,71 @@ def test_rnn_decode_matches_oracle(small):
     assert np.linalg.norm(u - uo) / np.linalg.norm(uo) < 1e-10
 
 
-def test_stitched_decode_runs(small):
+@pytest.mark.parametrize("decoder", ["plain", "coeff", "batch"])
+def test_stitched_decode_matches_oracle(small, decoder):
+    """Temporal stitching (vtdm.py:573-699): three overlapping windows, each
+    decoded alone and cross-faded, against the oracle's window loop.  The
+    pseudoinverse cut is the reference's own (rcond 1e-8, vtdm.py:648): the
+    short windows' Grams are ill-conditioned enough that a 1e-10 cut lets
+    rounding through at the 1e-7 level."""
     w = small
     V = w.video(device="cuda")
     store, sp, rf = _encode(w, V)
     prep = vtdm.VTDM_prep(store, None, None, w.Mx, w.My)
-    u = vtdm.VTDM(store, None, None, 0.0, 0.1, w.dt, w.Mx, Mt=w.Mt, rcond=1e-10, stitching=True,
-                  stitch_interval=0.04, output_format=2, prep=prep)
-    assert u.shape == (1000, 32, 32) and np.isfinite(u).all()
+    u = vtdm.VTDM(store, None, None, 0.0, 0.1, w.dt, w.Mx, Mt=w.Mt, stitching=True, stitch_interval=0.04,
+                  output_format=2, prep=prep, decoder=decoder)
+    rd = vtem_read(store)
+    rd.select_neurons([-0.5, 0.5, -0.5, 0.5])
+    norm = np.ones(w.N)
+    Dsw = prep.Dsw.cpu().numpy()
+    dirich = prep.dirich.cpu().numpy()
+
+    def window(s, e):
+        tk1, tk2, ind, kap, dl, bia, sig = rd.read_select_spikes([s, e])
+        return O.decode_window(tk1, tk2, ind, kap, dl, bia, norm, Dsw, dirich, w.Wt, w.Mt,
+                               round((e - s) / w.dt) * w.dt, w.dt, rcond=1e-8)[0]
+
+    uo, wins = O.temporal_stitch(window, 0.0, 0.1, w.dt, True, 0.04)
+    assert len(wins) == 3 and u.shape == uo.shape == (1000, 32, 32)
+    rel = np.linalg.norm(u - uo) / np.linalg.norm(uo)
+    assert rel <= 1e-8, rel
+
+
+@pytest.mark.parametrize("decoder", ["plain", "coeff", "batch"])
+def test_spatial_stitching_matches_oracle(small, decoder):
+    """decode_video with spatial stitching (vtdm.py:181-309): 2 x 2 tiles of
+    20 x 20 pixels over the 32 x 32 frame, each prepared on its own domain
+    (neurons centred in it, positions relative to its centre) and decoded
+    alone, blended with the tiles' Hann weights; against the oracle's tile
+    walk over the oracle's per-tile preparation and decode."""
+    w = small
+    V = w.video(device="cuda")
+    store, sp, rf = _encode(w, V)
+    T = 0.05
+    u = vtdm.decode_video(store, None, None, 0.0, T, w.dt, w.Mx, Mt=w.Mt, spatial_stitching=True,
+                          spatial_interval=[20, 20], output_format=2, decoder=decoder)
+    rd = vtem_read(store)
+    g = w.gabor
+    dom = [-0.5, 0.5, -0.5, 0.5]
+
+    def tile(d):
+        choose, sx, sy = O.select_neurons(g.h_x0, g.h_y0, d)
+        tPx = int(np.round((d[1] - d[0]) / w.dx))
+        tPy = int(np.round((d[3] - d[2]) / w.dy))
+        norm = np.ones(len(choose))
+        Ds, dirich, Dsw = O.prep_decoder_gabor(g.h_alpha[choose], g.h_l[choose], g.h_x0[choose] - sx,
+                                               g.h_y0[choose] - sy, g.h_ab[choose], g.KAPPA, g.gain[choose],
+                                               w.Mx, w.My, w.Wx, w.Wy, w.dx, w.dy, tPx, tPy, norm)
+        rd.select_neurons(d)
+        assert np.array_equal(rd.choose, choose)
+        tk1, tk2, ind, kap, dl, bia, sig = rd.read_select_spikes([0.0, T])
+        return O.decode_window(tk1, tk2, ind, kap, dl, bia, norm, Dsw, dirich, w.Wt, w.Mt, T, w.dt,
+                               rcond=1e-8)[0]
+
+    uo = O.spatial_stitch(tile, dom, 32, 32, [20, 20], w.dx, w.dy)
+    assert u.shape == uo.shape == (500, 32, 32)
+    rel = np.linalg.norm(u - uo) / np.linalg.norm(uo)
+    assert rel <= 1e-8, rel
 
 
 def vtem_read(store):

@@ -94,3 +94,57 @@ def test_small_workload_video_and_bank():
     rf = O.gabor_rf(g.h_alpha, g.h_l, g.h_x0, g.h_y0, g.h_ab, w.Px, w.Py, 1.0, 1.0, -0.5, -0.5, g.KAPPA, g.gain)
     np.testing.assert_allclose(np.sqrt((rf ** 2).sum((1, 2)) * w.dx * w.dy), 1.0, rtol=1e-12)
     assert w.N == 128 and (w.delta > 0).all()
+
+
+TEMPORAL_CASES = [
+    (0.0, 1.0, 0.001, True, 0.2),
+    (0.0, 0.1, 0.001, True, 0.04),
+    (0.0, 0.1, 0.001, False, None),     # one window (4-sample overlap unused)
+    (0.0, 0.5, 0.01, True, None),       # default interval 20 dt
+    (0.1, 0.7, 0.001, True, 0.13),      # offset start, ragged last window
+    (0.0, 0.05, 0.01, True, 0.05),      # 5-sample interval: no overlap
+    (0.0, 0.2, 0.01, True, 0.07),
+    (0.0, 0.33, 0.001, True, 0.1),
+]
+
+
+def test_temporal_plan_matches_oracle():
+    """Window schedule and Hann cross-fade of VTDM's temporal stitching
+    (vtdm.py:573-699) against the oracle's loop, on random window contents."""
+    import torch
+    rng = np.random.default_rng(3)
+    for st, et, dt, stitching, si in TEMPORAL_CASES:
+        recs = {}
+
+        def dec(s, e):
+            if (s, e) not in recs:
+                recs[(s, e)] = rng.standard_normal((int(round((e - s) / dt)), 3, 2))
+            return recs[(s, e)]
+
+        uo, wins = O.temporal_stitch(dec, st, et, dt, stitching, si)
+        plan = vtdm.temporal_plan(st, et, dt, stitching, si)
+        assert plan.windows == wins
+        u = torch.empty((plan.total_l, 3, 2), dtype=torch.float64)
+        prev = None
+        for i, (s, e) in enumerate(plan.windows):
+            u, prev = vtdm.place_window(u, plan, i, torch.as_tensor(dec(s, e)), prev)
+        np.testing.assert_allclose(u.numpy(), uo, rtol=0, atol=1e-15)
+
+
+def test_spatial_tiles_match_oracle():
+    """decode_video's tile walk and 2-D Hann weights (vtdm.py:214-302)
+    against the oracle's, and the weights' partition of unity over the
+    domain, including tiles wider than the domain and ragged last tiles."""
+    for Px, Py, ix, iy in [(32, 32, 20, 20), (64, 48, 30, 20), (97, 33, 30, 7), (128, 100, 96, 96),
+                           (48, 24, 200, 8), (33, 100, 30, 96), (64, 64, 64, 64)]:
+        dx = dy = 1.0 / Px
+        dom = [-Px * dx / 2, Px * dx / 2, -Py * dy / 2, Py * dy / 2]
+        a = O.spatial_tile_walk(dom, Px, Py, [ix, iy], dx, dy)
+        b = vtdm.spatial_tiles(Px, Py, (ix, iy), dom, dx, dy)
+        assert len(a) == len(b)
+        cover = np.zeros((Py, Px))
+        for (da, r0, r1, c0, c1, wa), (db, rows, wb) in zip(a, b):
+            assert da == db and (r0, r1, c0, c1) == rows
+            np.testing.assert_array_equal(wa, wb)
+            cover[r0:r1, c0:c1] += wa
+        np.testing.assert_allclose(cover, 1.0, rtol=0, atol=1e-12)

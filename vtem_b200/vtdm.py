@@ -167,9 +167,12 @@ def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, M
     coefficient space (:mod:`vtem_b200.fast`), the same reconstruction
     without the spike-by-spike Gram, by the pseudoinverse or (``rnn``) the
     RNN's gradient flow run on the coefficient system; it needs ``prep``
-    (VTDM_prep's result) and no Gram regularisation (``lamb`` = 0)."""
-    if decoder == "coeff" and (prep is None or lamb):
+    (VTDM_prep's result) and no Gram regularisation (``lamb`` = 0).
+    ``decoder="batch"`` decodes all windows at once (:func:`decode_windows_batched`)."""
+    if decoder in ("coeff", "batch") and (prep is None or lamb):
         raise ValueError("the coefficient-space decoder needs prep= and lamb=0")
+    if decoder == "batch" and rnn:
+        raise ValueError("the batched decoder solves by the pseudoinverse only")
     spfile = ss.vtem_storage_read(spikefile)
     spfile.read_vrf_type()
     spfile.read_num_neurons()
@@ -180,50 +183,31 @@ def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, M
     Mx = int(Mx)
     My = Mx if My is None else int(My)
     Mt = int(round(Wt * 2 / 2 / np.pi)) if Mt is None else int(Mt)
-    end = float(end_time)
-    if stitching:
-        if stitch_interval is None:
-            stitch_interval = 20 * dt
-        stitch_interval = min(stitch_interval, end_time)
-        end = round(float(min(start_time + stitch_interval, end_time)) / dt) * dt
-        overlap = 0.2 * stitch_interval
-    else:
-        stitch_interval = float(end_time)
-        overlap = 0
+    plan = temporal_plan(start_time, end_time, dt, stitching, stitch_interval)
     domain = _domain(domain, Px * dx, Py * dy)
     decSx = domain[1] - domain[0]
     decSy = domain[3] - domain[2]
     decPx = int(np.round(decSx / dx))
     decPy = int(np.round(decSy / dy))
-    start = float(start_time)
     if prep is not None:
         dirich = prep.dirich
         Dsw = prep.Dsw
     else:
         dirich = torch.as_tensor(simpleio.read_file(dirichfilename), device="cuda")
         Dsw = torch.as_tensor(simpleio.read_file(Dswfilename), device="cuda")
-    s = dirich.shape
-    total_l = int(round((end_time - start_time) / dt))
-    overlap_l = int(round(overlap / dt))
-    if overlap_l < 3:
-        if round(stitch_interval / dt) >= 8:
-            overlap_l = 4
-            overlap = 4 * dt
-        else:
-            overlap = 0
-            overlap_l = 0
-    interval_l = int(round(stitch_interval / dt))
-    left_window = torch.as_tensor(np.hanning(2 * overlap_l)[0:overlap_l], device="cuda").reshape(-1, 1, 1)
-    right_window = 1.0 - left_window
-    u = torch.empty((total_l, decPy, decPx), dtype=torch.float64, device="cuda")
+    u = torch.empty((plan.total_l, decPy, decPx), dtype=torch.float64, device="cuda")
     spfile.select_neurons(domain)
+    if decoder == "batch":
+        u = decode_windows_batched([(spfile, prep, plan)], Wt, Mt, dt, rcond)[0]
+        if output_format in (0, 1):
+            simpleio.write_memory_to_file(u, output + ".npy")
+        return u if return_device else u.cpu().numpy()
     fastdec = None
     if decoder == "coeff":
         from . import fast
         fastdec = fast.from_prep(prep, Wt, Mt, rcond=rcond, solver=coeff_solver)
-    i = 0
     prev = None
-    while True:
+    for i, (start, end) in enumerate(plan.windows):
         tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_sigma = spfile.read_select_spikes([start, end])
         h_norm = _norm_from_sigma(spfile.read_iaf()[0], h_sigma)[spfile.choose]
         if fastdec is not None:
@@ -240,31 +224,7 @@ def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, M
         else:
             u_rec = _plain_window(spfile, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm, Wt, Mt, dtype, Dsw,
                                   lamb, rnn, rnn_dt, alpha, steps, rcond, dirich, start, end, dt)
-        if overlap_l:
-            if i == 0:
-                if end_time - end < dt:
-                    u = u_rec
-                    break
-                u[0:(interval_l - overlap_l)] = u_rec[0:-overlap_l]
-                prev = u_rec[-overlap_l:]
-            else:
-                l_ind = i * (interval_l - overlap_l)
-                r_ind = (i + 1) * (interval_l - overlap_l)
-                u[l_ind:(l_ind + overlap_l)] = u_rec[0:overlap_l] * left_window + prev * right_window
-                if end_time - end < dt:
-                    u[(l_ind + overlap_l):] = u_rec[(-u.shape[0] + l_ind + overlap_l):]
-                    break
-                u[(l_ind + overlap_l):r_ind] = u_rec[overlap_l:interval_l - overlap_l]
-                prev = u_rec[-overlap_l:]
-        else:
-            u[(i * interval_l):((i * interval_l) + u_rec.shape[0])] = u_rec
-            if end_time - end < dt:
-                break
-        start = start + round(stitch_interval / dt) * dt - round(overlap / dt) * dt
-        end = min(start + round(stitch_interval / dt) * dt, float(end_time))
-        if float(end_time) - end < overlap:
-            end = end_time
-        i = i + 1
+        u, prev = place_window(u, plan, i, u_rec, prev)
     if output_format in (0, 1):
         simpleio.write_memory_to_file(u, output + ".npy")
     if return_device:
@@ -284,3 +244,227 @@ def _plain_window(spfile, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm
         cp.d_q = ls.solve_eq_sym(cp.d_G, cp.d_q, rcond=rcond)
     cp.freeG()
     return cp.reconstruct(dirich, [0, round((end - start) / dt) * dt], dt)
+
+
+@dataclass
+class TemporalPlan:
+    """Window schedule of VTDM: the (start, end) of each decoded window, the
+    samples two neighbours share (cross-faded), the samples per window and
+    in the whole range."""
+    windows: list
+    overlap_l: int
+    interval_l: int
+    total_l: int
+
+
+def temporal_plan(start_time, end_time, dt, stitching=False, stitch_interval=None):
+    """Windows of VTDM's temporal stitching (vtdm.py:573-605, :674-694):
+    intervals of ``stitch_interval`` (20 dt by default) that overlap by 20 %
+    of it, rounded to samples (at least 4 samples when an interval has 8 or
+    more, none below that); the last window reaches end_time.  Without
+    stitching one window covers the range.  The schedule depends on the
+    times only, so it is computed before any window is decoded."""
+    end = float(end_time)
+    if stitching:
+        if stitch_interval is None:
+            stitch_interval = 20 * dt
+        stitch_interval = min(stitch_interval, end_time)
+        end = round(float(min(start_time + stitch_interval, end_time)) / dt) * dt
+        overlap = 0.2 * stitch_interval
+    else:
+        stitch_interval = float(end_time)
+        overlap = 0
+    overlap_l = int(round(overlap / dt))
+    if overlap_l < 3:
+        if round(stitch_interval / dt) >= 8:
+            overlap_l, overlap = 4, 4 * dt
+        else:
+            overlap_l, overlap = 0, 0
+    start = float(start_time)
+    windows = [(start, end)]
+    while not end_time - end < dt:
+        start = start + round(stitch_interval / dt) * dt - round(overlap / dt) * dt
+        end = min(start + round(stitch_interval / dt) * dt, float(end_time))
+        if float(end_time) - end < overlap:
+            end = end_time
+        windows.append((start, end))
+    return TemporalPlan(windows, overlap_l, int(round(stitch_interval / dt)),
+                        int(round((end_time - start_time) / dt)))
+
+
+def place_window(u, plan, i, u_rec, prev):
+    """Write window i's reconstruction into the video u (vtdm.py:656-680):
+    outside the overlaps the samples are copied, over an overlap the previous
+    window's tail fades out under a Hann ramp while this one fades in.  A
+    single window with overlap replaces u.  Returns (u, tail to blend into
+    the next window)."""
+    ol, il = plan.overlap_l, plan.interval_l
+    last = i == len(plan.windows) - 1
+    if not ol:
+        u[i * il:i * il + u_rec.shape[0]] = u_rec
+        return u, None
+    if i == 0:
+        if last:
+            return u_rec, None
+        u[:il - ol] = u_rec[:-ol]
+        return u, u_rec[-ol:]
+    lw = torch.as_tensor(np.hanning(2 * ol)[:ol], dtype=u.dtype, device=u.device).reshape(-1, 1, 1)
+    a = i * (il - ol)
+    u[a:a + ol] = u_rec[:ol] * lw + prev * (1.0 - lw)
+    if last:
+        u[a + ol:] = u_rec[-u.shape[0] + a + ol:]
+        return u, None
+    u[a + ol:(i + 1) * (il - ol)] = u_rec[ol:il - ol]
+    return u, u_rec[-ol:]
+
+
+def decode_windows_batched(jobs, Wt, Mt, dt, rcond=1e-8):
+    """Decode every window of several decodes as one batch.  ``jobs`` is a
+    list of (spike reader with its neurons selected, VTDM_prep result,
+    TemporalPlan); all windows of all jobs become the clips of one
+    :class:`vtem_b200.batch.BatchDecoder` (grouped tensor-core Grams, one
+    batched Cholesky per system size, float64 fallbacks where the
+    pseudoinverse truncates), then each job's windows are stitched on the
+    device.  Returns one (frames, decPy, decPx) float64 device video per
+    job."""
+    from .batch import BatchDecoder, ClipProblem
+    probs, spans = [], []
+    for spfile, prep, plan in jobs:
+        dev = prep.Ds.device
+        first = len(probs)
+        for start, end in plan.windows:
+            tk1, tk2, ind, kap, dl, bia, _ = spfile.read_select_spikes([start, end])
+            if len(tk1) == 0:
+                raise ValueError("no spikes to decode")
+            f = lambda x: torch.as_tensor(np.asarray(x, np.float64), device=dev)
+            probs.append(ClipProblem(prep, Wt, Mt, f(tk1), f(tk2),
+                                     torch.as_tensor(np.asarray(ind, np.int32), device=dev), f(kap), f(dl), f(bia),
+                                     round((end - start) / dt) * dt, dt, rcond))
+        spans.append((first, len(probs)))
+    bd = BatchDecoder(probs, graph=False)
+    try:
+        outs = bd.run()
+    finally:
+        bd.close()
+    vids = []
+    for (spfile, prep, plan), (a, b) in zip(jobs, spans):
+        u = torch.empty((plan.total_l, prep.decPy, prep.decPx), dtype=torch.float64, device=outs[a].device)
+        prev = None
+        for i in range(a, b):
+            u, prev = place_window(u, plan, i - a, outs[i], prev)
+        vids.append(u)
+    return vids
+
+
+def spatial_tiles(decPx, decPy, spatial_interval, domain, dx, dy, dtype=np.float64):
+    """Tiles of the spatial stitching of decode_video (vtdm.py:216-302): tiles
+    of spatial_interval pixels (clipped to the domain) with a 20 % overlap,
+    the x tiles from the right edge leftwards, the y tiles from the top edge
+    (pixel row 0) downwards; each tile's weight is 1 inside and Hann ramps
+    over the overlaps it shares with a neighbour.  Returns a list of
+    (tile domain [x0, x1, y0, y1], (row0, row1, col0, col1), weight)."""
+    ix = min(int(spatial_interval[0]), decPx)
+    iy = min(int(spatial_interval[1]), decPy)
+    ox, oy = int(round(0.2 * ix)), int(round(0.2 * iy))
+
+    def ramp(n, rising):
+        h = np.hanning(2 * n)[:n] if n else np.zeros(0)
+        return h if rising else 1.0 - h
+
+    def axis_window(lo_i, hi_i, n_total, over):
+        a = 0 if lo_i == 0 else over
+        b = 0 if hi_i == n_total else over
+        return np.concatenate((ramp(a, True), np.ones(hi_i - lo_i - a - b), ramp(b, False)))
+
+    tiles = []
+    y1, y0 = domain[3], max(domain[3] - iy * dy, domain[2])
+    r0, r1 = 0, iy
+    while True:
+        x1, x0 = domain[1], max(domain[1] - ix * dx, domain[0])
+        c0, c1 = decPx - ix, decPx
+        while True:
+            wy = axis_window(r0, r1, decPy, oy).reshape(-1, 1)
+            wx = axis_window(c0, c1, decPx, ox).reshape(1, -1)
+            tiles.append(([x0, x1, y0, y1], (r0, r1, c0, c1), (wy @ wx).astype(dtype)))
+            if x0 == domain[0]:
+                break
+            x0 = max(x0 - ix * dx + ox * dx, domain[0])
+            x1 = x1 - ix * dx + ox * dx
+            c0 = max(c0 - ix + ox, 0)
+            c1 = c1 - ix + ox
+        if y0 == domain[2]:
+            break
+        y0 = max(y0 - iy * dy + oy * dy, domain[2])
+        y1 = y1 - iy * dy + oy * dy
+        r0 = r1 - oy
+        r1 = min(r0 + iy, decPy)
+    return tiles
+
+
+def decode_video(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, My=None, Mt=None,
+                 domain=None, Wx=None, Wy=None, Wt=None, lamb=0.0, dtype=np.float64, rnn=False, alpha=50000,
+                 steps=4000, stitching=False, stitch_interval=None, spatial_stitching=False,
+                 spatial_interval=(96, 96), precompute=True, write_blocks=False, output_format=0, output="rec",
+                 *, rcond=1e-8, decoder="plain", coeff_solver="auto"):
+    """Reconstruct a time range of the video (vtdm.py:18-309): VTDM_prep +
+    VTDM on the whole domain, or with ``spatial_stitching`` on overlapping
+    tiles (:func:`spatial_tiles`), each tile prepared and decoded alone
+    (temporal stitching inside VTDM as requested) and blended with its 2-D
+    Hann weight.  ``decoder="batch"`` (extension) decodes every window of
+    every tile as one batch (:func:`decode_windows_batched`): all tiles
+    share the Dirichlet orders, so their systems are factorised together.
+    ``precompute`` selects the reference's two preparation
+    variants, which compute the same cross-weights; both use VTDM_prep here.
+    The reference's call without spatial stitching passes VTDM an extra
+    positional argument (vtdm.py:165-169 vs :450-453) and raises; here it
+    decodes.  Videos are written as .npy (output_format 0 or 1)."""
+    extra = dict(rcond=rcond, decoder=decoder, coeff_solver=coeff_solver)
+    if not spatial_stitching:
+        prep = VTDM_prep(spikefile, Dswfilename, dirichfilename, Mx, My, domain, Wx, Wy, dtype=np.complex128)
+        return VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, My, Mt, domain, Wx, Wy,
+                    Wt, lamb, dtype, rnn, alpha, steps, stitching, stitch_interval, output_format, output,
+                    prep=prep, **extra)
+    spfile = ss.vtem_storage_read(spikefile)
+    Wt1, Wx1, Wy1, Px, Py, dx, dy = spfile.read_video_attributes()
+    Wx = Wx1 if Wx is None else float(Wx)
+    Wy = Wy1 if Wy is None else float(Wy)
+    Mx = int(Mx)
+    My = Mx if My is None else int(My)
+    domain = _domain(domain, Px * dx, Py * dy)
+    decPx = int(np.round((domain[1] - domain[0]) / dx))
+    decPy = int(np.round((domain[3] - domain[2]) / dy))
+    total_l = int(round((end_time - start_time) / dt))
+    tiles = spatial_tiles(decPx, decPy, spatial_interval, domain, dx, dy, dtype)
+    if decoder == "batch":
+        if rnn or lamb:
+            raise ValueError("the batched decoder solves by the pseudoinverse without regularisation")
+        Wt = Wt1 if Wt is None else float(Wt)
+        Mt = int(round(Wt * 2 / 2 / np.pi)) if Mt is None else int(Mt)
+        plan = temporal_plan(start_time, end_time, dt, stitching, stitch_interval)
+        jobs = []
+        for cdom, _, _ in tiles:
+            prep = VTDM_prep(spikefile, Dswfilename, dirichfilename, Mx, My, cdom, Wx, Wy, dtype=np.complex128)
+            rd = ss.vtem_storage_read(spikefile)
+            rd.read_vrf_type()
+            rd.read_num_neurons()
+            rd.select_neurons(cdom)
+            jobs.append((rd, prep, plan))
+        vids = decode_windows_batched(jobs, Wt, Mt, dt, rcond)
+        ud = torch.zeros((total_l, decPy, decPx), dtype=torch.float64, device=vids[0].device)
+        for (_, (r0, r1, c0, c1), wgt), ut in zip(tiles, vids):
+            ud[:, r0:r1, c0:c1] += ut * torch.as_tensor(wgt, dtype=torch.float64, device=ut.device)
+        u = ud.cpu().numpy().astype(dtype, copy=False)
+        if output_format in (0, 1):
+            simpleio.write_memory_to_file(u, output + ".npy")
+        return u
+    u = np.zeros((total_l, decPy, decPx), dtype=dtype)
+    fmt = (1 if output_format == 1 else 0) if write_blocks else 2
+    for i, (cdom, (r0, r1, c0, c1), wgt) in enumerate(tiles):
+        prep = VTDM_prep(spikefile, Dswfilename, dirichfilename, Mx, My, cdom, Wx, Wy, dtype=np.complex128)
+        ut = VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, My, Mt, cdom, Wx, Wy, Wt,
+                  lamb, dtype, rnn, alpha, steps, stitching, stitch_interval, fmt, output + str(i), prep=prep,
+                  **extra)
+        u[:, r0:r1, c0:c1] += np.multiply(ut, wgt)
+    if output_format in (0, 1):
+        simpleio.write_memory_to_file(u, output + ".npy")
+    return u
