@@ -164,6 +164,28 @@ def test_spatial_stitching_matches_oracle(small, decoder):
     assert rel <= 1e-8, rel
 
 
+def test_vtdmb_matches_vtdm(small, tmp_path):
+    """VTDM_prepb + VTDMb (vtdm.py:701-1071: Ds written by the prep, the
+    cross-weights formed per window by compute_Gb) reproduce VTDM_prep +
+    VTDM, through the files the preps write; decode_video's precompute=False
+    takes that path."""
+    w = small
+    V = w.video(device="cuda")
+    store, sp, rf = _encode(w, V)
+    T = 0.05
+    prep = vtdm.VTDM_prep(store, str(tmp_path / "dsw.npy"), str(tmp_path / "dirich.npy"), w.Mx, w.My)
+    u = vtdm.VTDM(store, str(tmp_path / "dsw.npy"), str(tmp_path / "dirich.npy"), 0.0, T, w.dt, w.Mx, Mt=w.Mt,
+                  output_format=2)
+    vtdm.VTDM_prepb(store, str(tmp_path / "ds.npy"), str(tmp_path / "dirich_b.npy"), w.Mx, w.My)
+    ub = vtdm.VTDMb(store, str(tmp_path / "ds.npy"), str(tmp_path / "dirich_b.npy"), 0.0, T, w.dt, w.Mx, Mt=w.Mt,
+                    output_format=2)
+    assert np.abs(ub - u).max() <= 1e-12 * np.abs(u).max()
+    kw = dict(Mt=w.Mt, spatial_stitching=True, spatial_interval=[24, 24], output_format=2)
+    ua = vtdm.decode_video(store, None, None, 0.0, T, w.dt, w.Mx, **kw)
+    uc = vtdm.decode_video(store, None, None, 0.0, T, w.dt, w.Mx, precompute=False, **kw)
+    assert np.abs(uc - ua).max() <= 1e-12 * np.abs(ua).max()
+
+
 def vtem_read(store):
     from vtem_b200 import spike_store as ss
     rd = ss.vtem_storage_read(store)

@@ -160,7 +160,7 @@ def VTDM_prep(spikefile, Dswfilename, dirichfilename, Mx, My=None, domain=None, 
 def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, My=None, Mt=None, domain=None,
          Wx=None, Wy=None, Wt=None, lamb=0.0, dtype=np.float64, rnn=False, alpha=50000, steps=4000,
          stitching=False, stitch_interval=None, output_format=0, output="rec", *, rcond=1e-8,
-         return_device=False, prep=None, rnn_dt=1e-6, decoder="plain", coeff_solver="auto"):
+         return_device=False, prep=None, rnn_dt=1e-6, decoder="plain", coeff_solver="auto", _from_ds=False):
     """Reconstruct a time range of the video (vtdm.py:450-699).
 
     ``decoder="coeff"`` (extension) decodes each window in the Dirichlet
@@ -191,7 +191,7 @@ def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, M
     decPy = int(np.round(decSy / dy))
     if prep is not None:
         dirich = prep.dirich
-        Dsw = prep.Dsw
+        Dsw = prep.Ds if _from_ds else prep.Dsw
     else:
         dirich = torch.as_tensor(simpleio.read_file(dirichfilename), device="cuda")
         Dsw = torch.as_tensor(simpleio.read_file(Dswfilename), device="cuda")
@@ -223,7 +223,7 @@ def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, M
                 u_rec = fastdec.decode(tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, T, dt)
         else:
             u_rec = _plain_window(spfile, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm, Wt, Mt, dtype, Dsw,
-                                  lamb, rnn, rnn_dt, alpha, steps, rcond, dirich, start, end, dt)
+                                  lamb, rnn, rnn_dt, alpha, steps, rcond, dirich, start, end, dt, _from_ds)
         u, prev = place_window(u, plan, i, u_rec, prev)
     if output_format in (0, 1):
         simpleio.write_memory_to_file(u, output + ".npy")
@@ -233,17 +233,51 @@ def VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, M
 
 
 def _plain_window(spfile, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm, Wt, Mt, dtype, Dsw, lamb, rnn,
-                  rnn_dt, alpha, steps, rcond, dirich, start, end, dt):
-    """One window of the reference decoder (vtdm.py:640-652)."""
+                  rnn_dt, alpha, steps, rcond, dirich, start, end, dt, from_ds=False):
+    """One window of the reference decoder (vtdm.py:640-652; with
+    ``from_ds`` the Gram of VTDMb, vtdm.py:1015-1020, whose cross-weights
+    come from the Dirichlet coefficients)."""
     cp = dr.dirichlet(spfile.decode_neurons, tk1, tk2, neuron_ind, h_kappa, h_delta, h_bias, h_norm, Wt, Mt, dtype)
     cp.compute_q()
-    cp.compute_G(Dsw, float(lamb), lower_only=not rnn)
+    if from_ds:
+        cp.compute_Gb(Dsw, float(lamb), lower_only=not rnn)
+    else:
+        cp.compute_G(Dsw, float(lamb), lower_only=not rnn)
     if rnn:
         cp.d_q = nn.rnn3(cp.d_G, cp.d_q, dt=rnn_dt, alpha=alpha, steps=steps)
     else:
         cp.d_q = ls.solve_eq_sym(cp.d_G, cp.d_q, rcond=rcond)
     cp.freeG()
     return cp.reconstruct(dirich, [0, round((end - start) / dt) * dt], dt)
+
+
+def VTDM_prepb(spikefile, Dsfilename, dirichfilename, Mx, My=None, domain=None, Wx=None, Wy=None,
+               dtype=np.complex128):
+    """Prepare decoding for VTDMb (vtdm.py:701-827): as VTDM_prep, but the
+    Dirichlet coefficients Ds are written to ``Dsfilename`` (when not None)
+    in place of the cross-weights, which VTDMb forms per window."""
+    prep = VTDM_prep(spikefile, None, dirichfilename, Mx, My, domain, Wx, Wy, dtype=dtype)
+    if Dsfilename is not None:
+        simpleio.write_memory_to_file(prep.Ds, Dsfilename)
+    return prep
+
+
+def VTDMb(spikefile, Dsfilename, dirichfilename, start_time, end_time, dt, Mx, My=None, Mt=None, domain=None,
+          Wx=None, Wy=None, Wt=None, lamb=0.0, dtype=np.float64, rnn=False, alpha=50000, steps=4000,
+          stitching=False, stitch_interval=None, output_format=0, output="rec", *, rcond=1e-8,
+          return_device=False, prep=None, rnn_dt=1e-6):
+    """VTDM with the Gram built from the Dirichlet coefficients
+    (vtdm.py:830-1071, dirichlet.compute_Gb): each window forms
+    Re(Ds Ds^H) with its norm, then the same Gram, solve and
+    reconstruction as VTDM."""
+    if prep is None:
+        Ds = torch.as_tensor(simpleio.read_file(Dsfilename), device="cuda")
+        dirich = torch.as_tensor(simpleio.read_file(dirichfilename), device="cuda")
+        prep = PrepResult(Ds, dirich, None, None, int(Mx), int(Mx if My is None else My), dirich.shape[2],
+                          dirich.shape[1], 0, 0)
+    return VTDM(spikefile, None, dirichfilename, start_time, end_time, dt, Mx, My, Mt, domain, Wx, Wy, Wt, lamb,
+                dtype, rnn, alpha, steps, stitching, stitch_interval, output_format, output, rcond=rcond,
+                return_device=return_device, prep=prep, rnn_dt=rnn_dt, _from_ds=True)
 
 
 @dataclass
@@ -413,17 +447,30 @@ def decode_video(spikefile, Dswfilename, dirichfilename, start_time, end_time, d
     Hann weight.  ``decoder="batch"`` (extension) decodes every window of
     every tile as one batch (:func:`decode_windows_batched`): all tiles
     share the Dirichlet orders, so their systems are factorised together.
-    ``precompute`` selects the reference's two preparation
-    variants, which compute the same cross-weights; both use VTDM_prep here.
-    The reference's call without spatial stitching passes VTDM an extra
-    positional argument (vtdm.py:165-169 vs :450-453) and raises; here it
-    decodes.  Videos are written as .npy (output_format 0 or 1)."""
+    ``precompute=False`` takes the reference's second variant, VTDM_prepb
+    + VTDMb (cross-weights formed per window from the Dirichlet
+    coefficients), with the plain decoder.  The reference's call without
+    spatial stitching passes VTDM an extra positional argument
+    (vtdm.py:165-169 vs :450-453) and raises; here it decodes.  Videos are
+    written as .npy (output_format 0 or 1)."""
     extra = dict(rcond=rcond, decoder=decoder, coeff_solver=coeff_solver)
+    b = not precompute and decoder == "plain"
+
+    def prep_of(dom):
+        if b:
+            return VTDM_prepb(spikefile, Dswfilename, dirichfilename, Mx, My, dom, Wx, Wy, dtype=np.complex128)
+        return VTDM_prep(spikefile, Dswfilename, dirichfilename, Mx, My, dom, Wx, Wy, dtype=np.complex128)
+
+    def vtdm_of(dom, prep, fmt, out):
+        if b:
+            return VTDMb(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, My, Mt, dom, Wx, Wy,
+                         Wt, lamb, dtype, rnn, alpha, steps, stitching, stitch_interval, fmt, out, rcond=rcond,
+                         prep=prep)
+        return VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, My, Mt, dom, Wx, Wy, Wt,
+                    lamb, dtype, rnn, alpha, steps, stitching, stitch_interval, fmt, out, prep=prep, **extra)
+
     if not spatial_stitching:
-        prep = VTDM_prep(spikefile, Dswfilename, dirichfilename, Mx, My, domain, Wx, Wy, dtype=np.complex128)
-        return VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, My, Mt, domain, Wx, Wy,
-                    Wt, lamb, dtype, rnn, alpha, steps, stitching, stitch_interval, output_format, output,
-                    prep=prep, **extra)
+        return vtdm_of(domain, prep_of(domain), output_format, output)
     spfile = ss.vtem_storage_read(spikefile)
     Wt1, Wx1, Wy1, Px, Py, dx, dy = spfile.read_video_attributes()
     Wx = Wx1 if Wx is None else float(Wx)
@@ -460,10 +507,7 @@ def decode_video(spikefile, Dswfilename, dirichfilename, start_time, end_time, d
     u = np.zeros((total_l, decPy, decPx), dtype=dtype)
     fmt = (1 if output_format == 1 else 0) if write_blocks else 2
     for i, (cdom, (r0, r1, c0, c1), wgt) in enumerate(tiles):
-        prep = VTDM_prep(spikefile, Dswfilename, dirichfilename, Mx, My, cdom, Wx, Wy, dtype=np.complex128)
-        ut = VTDM(spikefile, Dswfilename, dirichfilename, start_time, end_time, dt, Mx, My, Mt, cdom, Wx, Wy, Wt,
-                  lamb, dtype, rnn, alpha, steps, stitching, stitch_interval, fmt, output + str(i), prep=prep,
-                  **extra)
+        ut = vtdm_of(cdom, prep_of(cdom), fmt, output + str(i))
         u[:, r0:r1, c0:c1] += np.multiply(ut, wgt)
     if output_format in (0, 1):
         simpleio.write_memory_to_file(u, output + ".npy")
