@@ -291,7 +291,7 @@ def run_ours(args, rank, world, local):
                        "parallelism": "clip-parallel replicas" if world > 1 else "single GPU"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps * (launches_mixed(decmix) if headline_mixed else launches_per_step(dec64)),
-            "roofline": {"bound": "hbm", "kernel": "synth_half_kernel (fused synthesis)",
+            "roofline": {"bound": "hbm", "kernel": "synth_ws_kernel (warp-specialised synthesis)",
                          "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                          "traffic": measured_traffic(voxels), "algorithmic_bytes": synth_bytes,

@@ -1,0 +1,69 @@
+"""Coefficient-space synthesis against the direct sum (GPU).
+
+vtb_coeff_synthesize renders u[f][py][px] = Re sum_s A_t[s] ey_s[py] ex_s[px]
+with A_t[s] = sum_m a[s][m] e^{j m W t_f} over the reference's spatial
+ellipse (the Dirichlet reconstruction of dirichlet.py:354-420 and
+vrf.py:437-499 in coefficient form).  It has three kernels: the
+warp-specialised one (frames up to 64 px wide, Mx, My <= 6), the
+half-spectrum one (2 My + 1 <= 13) and the general two-pass one; each is
+checked on odd sizes, crop offsets, frame counts that leave partial chunks,
+and non-Hermitian coefficients (the kernels may not assume the symmetry the
+decoders produce)."""
+import numpy as np
+import pytest
+import torch
+
+from vtem_b200 import _abi
+from vtem_b200.fast import ellipse_storage_index
+
+pytestmark = pytest.mark.gpu
+
+
+def _direct(a, Mx, My, Mt, W, t0, dt, Nt, Px, Py, Px1, Py1):
+    smap = ellipse_storage_index(Mx, My)
+    Kx, Kt = 2 * Mx + 1, 2 * Mt + 1
+    my = My - smap // Kx
+    mx = smap % Kx - Mx
+    px = (np.arange(Px) + (Px1 - Px) // 2) % Px1
+    py = (np.arange(Py) + (Py1 - Py) // 2) % Py1
+    ex = ((-1.0) ** mx)[:, None] * np.exp(2j * np.pi * np.outer(mx, px) / Px1)
+    ey = ((-1.0) ** my)[:, None] * np.exp(2j * np.pi * np.outer(my, py) / Py1)
+    E = np.exp(1j * W * np.outer(t0 + np.arange(Nt) * dt, np.arange(-Mt, Mt + 1)))
+    A = E @ a.reshape(len(smap), Kt).T
+    return np.einsum("fs,sy,sx->fyx", A, ey, ex).real
+
+
+CASES = [
+    # Mx, My, Mt, Px, Py, Px1, Py1, Nt          kernel
+    (6, 6, 8, 64, 64, 64, 64, 37),              # warp-specialised (the decoder's configuration)
+    (3, 3, 4, 32, 32, 32, 32, 16),              # warp-specialised, whole chunks
+    (2, 5, 3, 17, 70, 20, 75, 53),              # warp-specialised, odd sizes, crop offsets, two row tiles
+    (0, 2, 1, 9, 5, 9, 5, 3),                   # warp-specialised, Mx = 0
+    (7, 4, 2, 40, 24, 48, 30, 21),              # half-spectrum (Mx > 6)
+    (3, 3, 4, 80, 50, 96, 60, 19),              # half-spectrum (wider than 64)
+    (4, 7, 2, 20, 20, 20, 20, 11),              # general (2 My + 1 > 13)
+]
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_synthesis_matches_direct_sum(case, dtype):
+    Mx, My, Mt, Px, Py, Px1, Py1, Nt = case
+    rng = np.random.default_rng(Mx * 100 + My * 10 + Mt)
+    smap = torch.as_tensor(ellipse_storage_index(Mx, My), device="cuda")
+    Ks, Kt = int(smap.numel()), 2 * Mt + 1
+    a = rng.standard_normal(Ks * Kt) + 1j * rng.standard_normal(Ks * Kt)
+    W, t0, dt = 2 * np.pi * 20 / Mt, 0.013, 1e-3
+    ad = torch.as_tensor(a, dtype=torch.complex128, device="cuda")
+    A = torch.empty((Nt, Ks), dtype=torch.complex128, device="cuda")
+    u = torch.full((Nt, Py, Px), float("nan"), dtype=dtype, device="cuda")
+    st = _abi.lib().vtb_coeff_synthesize(ad.data_ptr(), smap.data_ptr(), Ks, Mx, My, Mt, W, t0, dt, Nt, Px, Py, Px1,
+                                         Py1, A.data_ptr(), u.data_ptr(), int(dtype == torch.float32),
+                                         _abi.stream_ptr())
+    assert st == 0, _abi.status_string(st)
+    ref = _direct(a, Mx, My, Mt, W, t0, dt, Nt, Px, Py, Px1, Py1)
+    got = u.double().cpu().numpy()
+    assert np.isfinite(got).all()
+    tol = 1e-12 if dtype == torch.float64 else 1e-6
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    assert err <= tol, err

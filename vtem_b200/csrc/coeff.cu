@@ -618,6 +618,311 @@ __global__ void __launch_bounds__(256, 2) synth_half_kernel(const double2* __res
     }
 }
 
+// Warp-specialised synthesis for frames up to 64 pixels wide with Mx, My <= 6
+// (the decoder's usual orders).  Same sum as synth_half_kernel:
+//     u[py][px] = sum_k Y[k][py] X_f[k][px],  k < 2My+1 real rows,
+// with the per-frame rows X_f built from the expanded, Hermitian-folded
+// coefficients.  Each 384-thread block renders a contiguous range of frames
+// (balanced to one frame) with two roles that run concurrently:
+//  * producer warps (4): per chunk of kFoldFrames frames, E = e^{j m W t} by
+//    powers, A_t[s] = sum_m a[s][m] E[m] (consecutive threads on consecutive
+//    s: contiguous coefficient reads, E broadcast) scattered into a zeroed
+//    (2My+1) x (2Mx+1) grid, the fold
+//        g[c] = A_t[my][c] + conj A_t[-my][-c]   (g = A_t[0] for my = 0),
+//        Re = g0.x + sum_m (S.x exr - D.y exi),  Im = g0.y + sum_m (S.y exr + D.x exi),
+//    S = g[m] + g[-m], D = g[m] - g[-m] (4 FMAs per |m|; exr/exi of the
+//    thread's pixel column in registers), and per frame the X rows into one
+//    of kWsSlots shared-memory slots;
+//  * consumer warps (8): per frame, u = Y^T X on the float64 tensor cores
+//    (mma.sync m8n8k4, k padded to a multiple of 4 with zero rows), warp w
+//    rows 8w..8w+7 of a 64-row tile, all 64 columns; column pairs written
+//    with streaming stores.
+// The slots are handed over with named barriers (bar.arrive by the side that
+// fills or frees a slot, bar.sync by the side that waits): both sides walk
+// the same frame list, so every arrive has its matching sync and no wait is
+// open-ended.  Row strides 68 (X) and 64k + 4 (Y) put the four k rows of an
+// mma fragment on distinct banks.
+constexpr int kFoldMaxM = 6;
+constexpr int kFoldFrames = 8;
+constexpr int kFoldXS = 68;
+constexpr int kWsSlots = 3;
+constexpr int kWsConsumers = 256;   // 8 warps
+constexpr int kWsProducers = 128;   // 4 warps
+constexpr int kWsThreads = kWsConsumers + kWsProducers;
+// named barrier ids: 0 = __syncthreads, 1 = producers only, then FULL and EMPTY per slot
+constexpr int kBarProd = 1, kBarFull = 2, kBarEmpty = 2 + kWsSlots;
+
+// Barrier ids as immediates (so that only the ids used are reserved).
+template <int ID>
+__device__ __forceinline__ void named_sync(int n) {
+    asm volatile("bar.sync %0, %1;\n" ::"n"(ID), "r"(n) : "memory");
+}
+template <int ID>
+__device__ __forceinline__ void named_arrive(int n) {
+    asm volatile("bar.arrive %0, %1;\n" ::"n"(ID), "r"(n) : "memory");
+}
+template <int BASE>
+__device__ __forceinline__ void slot_sync(int slot, int n) {
+    static_assert(kWsSlots == 3, "one case per slot");
+    if (slot == 0) named_sync<BASE>(n);
+    else if (slot == 1) named_sync<BASE + 1>(n);
+    else named_sync<BASE + 2>(n);
+}
+template <int BASE>
+__device__ __forceinline__ void slot_arrive(int slot, int n) {
+    if (slot == 0) named_arrive<BASE>(n);
+    else if (slot == 1) named_arrive<BASE + 1>(n);
+    else named_arrive<BASE + 2>(n);
+}
+
+// D (8x8) += A (8x4) B (4x8) on the float64 tensor cores: lane l holds
+// A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0,1}].
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void store_pair(double* p, double x, double y) {
+    __stcs(reinterpret_cast<double2*>(p), make_double2(x, y));
+}
+__device__ __forceinline__ void store_pair(float* p, double x, double y) {
+    __stcs(reinterpret_cast<float2*>(p), make_float2((float)x, (float)y));
+}
+
+template <typename OutT, int MY>
+__global__ void __launch_bounds__(kWsThreads, 2) synth_ws_kernel(const double2* __restrict__ a,
+                                                                 const int32_t* __restrict__ smap, int Ks, int Mx,
+                                                                 int Mt, double W, double t0, double dt, int Nt,
+                                                                 int Px, int Py, int Px1, int Py1, int YS,
+                                                                 OutT* __restrict__ u) {
+    constexpr int R = 2 * MY + 1, H = MY + 1, KS = (R + 3) / 4;
+    extern __shared__ double2 fs[];
+    const int Kx = 2 * Mx + 1, Kt = 2 * Mt + 1, KG = R * Kx;
+    const int RS = 2 + 4 * Mx;                              // doubles per folded row
+    double2* as = fs;                                       // Kt x Ks (transposed)
+    double2* E = as + Ks * Kt;                              // kFoldFrames x Kt
+    double2* Ag = E + kFoldFrames * Kt;                     // kFoldFrames x KG (zero outside the ellipse)
+    double* Fold = reinterpret_cast<double*>(Ag + kFoldFrames * KG);   // kFoldFrames x H x RS
+    double* X = Fold + kFoldFrames * H * RS;                // kWsSlots x 16 x kFoldXS (rows >= R zero)
+    double* Ys = X + kWsSlots * 16 * kFoldXS;               // 16 x YS (zero beyond Py and R)
+    const int tid = threadIdx.x;
+    for (int e = tid; e < 16 * YS; e += blockDim.x) Ys[e] = 0.0;
+    for (int e = tid; e < kFoldFrames * KG; e += blockDim.x) Ag[e] = make_double2(0.0, 0.0);
+    for (int e = tid; e < kWsSlots * 16 * kFoldXS; e += blockDim.x) X[e] = 0.0;
+    __syncthreads();
+    {
+        const int yd = (Py1 - Py) / 2;
+        for (int py = tid; py < Py; py += blockDim.x) {
+            double sn, co;
+            sincospi(2.0 * ((py + yd) % Py1) / Py1, &sn, &co);
+            const double2 base = make_double2(co, sn);
+            double2 pw = make_double2(1.0, 0.0);
+            Ys[py] = 1.0;
+            for (int my = 1; my <= MY; ++my) {
+                pw = cmul(pw, base);
+                const double sg = (my & 1) ? -1.0 : 1.0;
+                Ys[(2 * my - 1) * YS + py] = sg * pw.x;
+                Ys[(2 * my) * YS + py] = -sg * pw.y;
+            }
+        }
+    }
+    for (int e = tid; e < Ks * Kt; e += blockDim.x) as[(e % Kt) * Ks + e / Kt] = a[e];
+    __syncthreads();
+    const int fb = (int)((int64_t)blockIdx.x * Nt / gridDim.x);
+    const int fe = (int)((int64_t)(blockIdx.x + 1) * Nt / gridDim.x);
+    const int n = fe - fb;
+    if (tid < kWsConsumers) {
+        // ---- consumer: u = Y^T X per frame on the tensor cores
+        const int warp = tid >> 5, lane = tid & 31;
+        const bool vec2 = (Px % 2) == 0;                    // pair stores stay aligned
+        for (int i = 0; i < n; ++i) {
+            const int slot = i % kWsSlots;
+            slot_sync<kBarFull>(slot, kWsThreads);
+            const double* Xq = X + slot * 16 * kFoldXS;
+            OutT* uf = u + (int64_t)(fb + i) * Px * Py;
+            for (int y0 = 0; y0 < Py; y0 += 64) {
+                const int r0 = y0 + 8 * warp;               // this warp's 8 rows
+                if (r0 >= Py) continue;                     // warp-uniform
+                double af[KS];                              // A = Y^T (8 rows x 4 k) fragments
+#pragma unroll
+                for (int ks = 0; ks < KS; ++ks) af[ks] = Ys[(4 * ks + (lane & 3)) * YS + r0 + (lane >> 2)];
+                double acc[8][2];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) acc[t][0] = acc[t][1] = 0.0;
+#pragma unroll
+                for (int ks = 0; ks < KS; ++ks) {
+                    const double* Xk = Xq + (4 * ks + (lane & 3)) * kFoldXS + (lane >> 2);
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) dmma_8x8x4(acc[t], af[ks], Xk[8 * t]);
+                }
+                const int py = r0 + (lane >> 2);
+                if (py < Py) {
+                    OutT* ur = uf + (int64_t)py * Px;
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const int px = 8 * t + 2 * (lane & 3);
+                        if (px + 1 < Px && vec2) {
+                            store_pair(ur + px, acc[t][0], acc[t][1]);
+                        } else {
+                            if (px < Px) __stcs(ur + px, (OutT)acc[t][0]);
+                            if (px + 1 < Px) __stcs(ur + px + 1, (OutT)acc[t][1]);
+                        }
+                    }
+                }
+            }
+            if (i + kWsSlots < n) slot_arrive<kBarEmpty>(slot, kWsThreads);
+        }
+        return;
+    }
+    // ---- producer: expansion, fold and X rows, kWsSlots frames ahead at most
+    const int ptid = tid - kWsConsumers;
+    const int cpx = ptid & 63;
+    double exr[kFoldMaxM], exi[kFoldMaxM];
+    {
+        const int xd = (Px1 - Px) / 2;
+        double sn = 0.0, co = 1.0;
+        if (cpx < Px) sincospi(2.0 * ((cpx + xd) % Px1) / Px1, &sn, &co);
+        const double2 base = make_double2(co, sn);
+        double2 pw = make_double2(1.0, 0.0);
+#pragma unroll
+        for (int m = 0; m < kFoldMaxM; ++m) {
+            pw = cmul(pw, base);
+            const double sg = (m & 1) ? 1.0 : -1.0;         // (-1)^(m+1)
+            exr[m] = sg * pw.x;
+            exi[m] = sg * pw.y;
+        }
+    }
+    int i = 0;
+    for (int c0 = fb; c0 < fe; c0 += kFoldFrames) {
+        const int nf = min(kFoldFrames, fe - c0);
+        if (ptid < nf) {
+            double sn, co;
+            sincos(W * (t0 + (c0 + ptid) * dt), &sn, &co);
+            const double2 base = make_double2(co, sn);
+            double2 pw = make_double2(1.0, 0.0);
+            double2* Eq = E + ptid * Kt;
+            Eq[Mt] = pw;
+            for (int m = 1; m <= Mt; ++m) {
+                pw = cmul(pw, base);
+                Eq[Mt + m] = pw;
+                Eq[Mt - m] = make_double2(pw.x, -pw.y);
+            }
+        }
+        named_sync<kBarProd>(kWsProducers);
+        // temporal expansion: thread per (frame, ellipse entry)
+        // two entries per thread at a time: four independent FMA chains
+        for (int e0 = ptid; e0 < nf * Ks; e0 += 2 * kWsProducers) {
+            const int e1 = min(e0 + kWsProducers, nf * Ks - 1);   // a duplicate of e0's work when past the end
+            const int q0 = e0 / Ks, s0 = e0 - q0 * Ks, q1 = e1 / Ks, s1 = e1 - q1 * Ks;
+            const double2 *E0 = E + q0 * Kt, *E1 = E + q1 * Kt;
+            double ax0 = 0.0, ay0 = 0.0, ax1 = 0.0, ay1 = 0.0;
+            for (int mi = 0; mi < Kt; ++mi) {
+                const double2 c0 = as[mi * Ks + s0], v0 = E0[mi];
+                const double2 c1 = as[mi * Ks + s1], v1 = E1[mi];
+                ax0 = fma(c0.x, v0.x, fma(-c0.y, v0.y, ax0));
+                ay0 = fma(c0.x, v0.y, fma(c0.y, v0.x, ay0));
+                ax1 = fma(c1.x, v1.x, fma(-c1.y, v1.y, ax1));
+                ay1 = fma(c1.x, v1.y, fma(c1.y, v1.x, ay1));
+            }
+            Ag[q0 * KG + __ldg(smap + s0)] = make_double2(ax0, ay0);
+            if (e0 + kWsProducers < nf * Ks) Ag[q1 * KG + __ldg(smap + s1)] = make_double2(ax1, ay1);
+        }
+        named_sync<kBarProd>(kWsProducers);
+        // fold: task (q, my, m), my in [0, My], m in [0, Mx]; grid row My - my'
+        for (int e = ptid; e < nf * H * (Mx + 1); e += kWsProducers) {
+            const int q = e / (H * (Mx + 1)), r = e % (H * (Mx + 1));
+            const int my = r / (Mx + 1), m = r % (Mx + 1);
+            const double2* Aq = Ag + q * KG;
+            const double2* up = Aq + (MY - my) * Kx + Mx;   // row my, column 0
+            const double2* dn = Aq + (MY + my) * Kx + Mx;   // row -my, column 0
+            double* row = Fold + (q * H + my) * RS;
+            if (m == 0) {
+                double2 g = up[0];
+                if (my > 0) g = make_double2(g.x + dn[0].x, g.y - dn[0].y);
+                row[0] = g.x;
+                row[1] = g.y;
+            } else {
+                double2 gp = up[m], gm = up[-m];
+                if (my > 0) {
+                    const double2 hp = dn[-m], hm = dn[m];
+                    gp = make_double2(gp.x + hp.x, gp.y - hp.y);
+                    gm = make_double2(gm.x + hm.x, gm.y - hm.y);
+                }
+                double* v = row + 2 + 4 * (m - 1);
+                v[0] = gp.x + gm.x;
+                v[1] = -(gp.y - gm.y);
+                v[2] = gp.y + gm.y;
+                v[3] = gp.x - gm.x;
+            }
+        }
+        named_sync<kBarProd>(kWsProducers);
+        for (int q = 0; q < nf; ++q, ++i) {
+            const int slot = i % kWsSlots;
+            if (i >= kWsSlots) slot_sync<kBarEmpty>(slot, kWsThreads);
+            double* Xq = X + slot * 16 * kFoldXS;
+            if (cpx < Px) {
+                // this thread's rows my = g, g + 2, ... together: independent FMA chains
+                constexpr int NR = (MY + 2) / 2;
+                const int g = ptid >> 6;
+                double re[NR], im[NR];
+#pragma unroll
+                for (int j = 0; j < NR; ++j) {
+                    const int my = min(g + 2 * j, MY);
+                    const double* row = Fold + (q * H + my) * RS;
+                    re[j] = row[0];
+                    im[j] = row[1];
+                }
+#pragma unroll
+                for (int m = 0; m < kFoldMaxM; ++m) {
+                    if (m < Mx) {
+#pragma unroll
+                        for (int j = 0; j < NR; ++j) {
+                            const double* row = Fold + (q * H + min(g + 2 * j, MY)) * RS;
+                            const double2 v01 = *reinterpret_cast<const double2*>(row + 2 + 4 * m);
+                            const double2 v23 = *reinterpret_cast<const double2*>(row + 4 + 4 * m);
+                            re[j] = fma(v01.x, exr[m], fma(v01.y, exi[m], re[j]));
+                            im[j] = fma(v23.x, exr[m], fma(v23.y, exi[m], im[j]));
+                        }
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < NR; ++j) {
+                    const int my = g + 2 * j;
+                    if (my > MY) continue;
+                    if (my == 0) {
+                        Xq[cpx] = re[j];
+                    } else {
+                        Xq[(2 * my - 1) * kFoldXS + cpx] = re[j];
+                        Xq[(2 * my) * kFoldXS + cpx] = im[j];
+                    }
+                }
+            }
+            slot_arrive<kBarFull>(slot, kWsThreads);
+        }
+    }
+}
+
+template <typename OutT>
+static void launch_ws(int My, int blocks, size_t smf, cudaStream_t s, const double2* a, const int32_t* smap, int Ks,
+                      int Mx, int Mt, double W, double t0, double dt, int Nt, int Px, int Py, int Px1, int Py1, int YS,
+                      OutT* u, cudaError_t* err) {
+    auto go = [&](auto kern) {
+        *err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smf);
+        if (*err == cudaSuccess)
+            kern<<<blocks, kWsThreads, smf, s>>>(a, smap, Ks, Mx, Mt, W, t0, dt, Nt, Px, Py, Px1, Py1, YS, u);
+    };
+    switch (My) {
+        case 0: go(synth_ws_kernel<OutT, 0>); break;
+        case 1: go(synth_ws_kernel<OutT, 1>); break;
+        case 2: go(synth_ws_kernel<OutT, 2>); break;
+        case 3: go(synth_ws_kernel<OutT, 3>); break;
+        case 4: go(synth_ws_kernel<OutT, 4>); break;
+        case 5: go(synth_ws_kernel<OutT, 5>); break;
+        default: go(synth_ws_kernel<OutT, 6>); break;
+    }
+}
+
 }  // namespace vtb
 
 using namespace vtb;
@@ -670,6 +975,24 @@ VTB_API int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, i
     cudaStream_t s = as_stream(stream);
     const int Kt = 2 * Mt + 1;
     const int Kx = 2 * Mx + 1, Ky = 2 * My + 1;
+    if (Px <= 64 && Mx <= kFoldMaxM && My <= kFoldMaxM && Py <= 256) {
+        // warp-specialised kernel (A_work unused)
+        const int H = My + 1, YS = ceil_div(Py, 64) * 64 + 4;   // padded: A fragments hit distinct banks
+        const size_t smf = (size_t)(Ks * Kt + kFoldFrames * (Kt + Ky * Kx)) * sizeof(double2) +
+                           (size_t)(kFoldFrames * H * (2 + 4 * Mx) + kWsSlots * 16 * kFoldXS + 16 * YS) *
+                               sizeof(double);
+        VTB_CHECK_ARG(smf <= 200 * 1024);
+        const int blocks = (int)std::min<int64_t>(Nt, 2 * kNumSMs);
+        cudaError_t err = cudaSuccess;
+        if (out_f32)
+            launch_ws<float>(My, blocks, smf, s, reinterpret_cast<const double2*>(a), smap, Ks, Mx, Mt, W, t0, dt, Nt,
+                             Px, Py, Px1, Py1, YS, reinterpret_cast<float*>(u), &err);
+        else
+            launch_ws<double>(My, blocks, smf, s, reinterpret_cast<const double2*>(a), smap, Ks, Mx, Mt, W, t0, dt, Nt,
+                              Px, Py, Px1, Py1, YS, reinterpret_cast<double*>(u), &err);
+        VTB_CUDA_TRY(err);
+        return launch_status();
+    }
     if (Ky <= kHalfMaxRows) {
         // fused half-spectrum kernel (A_work unused)
         const size_t smh = (size_t)(Kx * Px + Ks * Kt + kHalfFrames * (Kt + Ky * Kx)) * sizeof(double2) +
