@@ -350,10 +350,10 @@ def gram_gemm_roofline(dec, peaks, reps=20):
 
 def launches_mixed(dec):
     # own kernels per decode: temporal_gram, rhs, realify_vec, wn split, tc gemm, real scatter (6); factor:
-    # pivot test + diagonal-block inverses (2); solve: f64<->f32 conversions (2); per sweep: unrealify,
-    # residual (2), realify_vec, conversions (2), norm ratio, axpy (8); final unrealify (1); synthesis (2).
+    # pivot test (1); solve: f64<->f32 conversions (2); per sweep: unrealify, residual (2), realify_vec,
+    # conversions (2), norm ratio, axpy (8); final unrealify (1); synthesis (1, warp-specialised).
     # cuSOLVER's own kernels (spotrf, strsv) are not counted.
-    return 6 + 2 + 2 + 8 * dec.mixed_sweeps + 1 + 2
+    return 6 + 1 + 2 + 8 * dec.mixed_sweeps + 1 + 1
 
 
 def run_batch(args, rank, world, local):

@@ -186,6 +186,42 @@ def test_vtdmb_matches_vtdm(small, tmp_path):
     assert np.abs(uc - ua).max() <= 1e-12 * np.abs(ua).max()
 
 
+@pytest.mark.parametrize("decoder", ["plain", "coeff"])
+def test_random_threshold_decode_matches_oracle(small, decoder):
+    """Random-threshold IAF (ensemble_encode.py:175-333) with per-neuron
+    sigma, decoded with the reference's weighting norm = 1/(kappa sigma)
+    normalised to its maximum (vtdm.py:408-413, :634-638): the decoder's
+    cross-weights and q carry the non-uniform norm; against the oracle's
+    decode of the same spikes with the oracle's norm."""
+    w = small
+    V = w.video(device="cuda")
+    g = w.gabor
+    rf = vrf.vrf_gabor((w.Py, w.Px), dx=w.dx, dy=w.dy)
+    rf.load_parameters(num_neurons=w.N, h_alpha=g.h_alpha, h_l=g.h_l, h_x0=g.h_x0, h_y0=g.h_y0, h_ab=g.h_ab,
+                       KAPPA=g.KAPPA, h_gain=g.gain)
+    rng = np.random.default_rng(11)
+    sigma = w.delta * rng.uniform(0.01, 0.03, w.N)
+    iaf = ensemble_encode.IAF_encode_rt(w.N, w.dt)
+    iaf.randn_source = lambda shape: rng.standard_normal(shape)
+    iaf.load_parameters(h_kappa=w.kappa, h_bias=w.bias, h_delta=w.delta, h_sigma=sigma,
+                        h_delta_value=w.delta + sigma * rng.standard_normal(w.N), h_v0=w.v0)
+    store = vtem.VTEM_IAF(V, None, w.Wt, rf, w.Wx, w.Wy, dx=w.dx, dy=w.dy, fps=1.0 / w.dt, npinput=True, iaf=iaf)
+    T = 0.05
+    prep = vtdm.VTDM_prep(store, None, None, w.Mx, w.My)
+    u = vtdm.VTDM(store, None, None, 0.0, T, w.dt, w.Mx, Mt=w.Mt, output_format=2, prep=prep, decoder=decoder)
+    norm = O.h_norm_from_sigma(w.kappa, sigma)
+    assert norm.min() < 0.9                       # the weighting is not uniform
+    np.testing.assert_allclose(prep.h_norm, norm, rtol=1e-15)
+    rd = vtem_read(store)
+    rd.select_neurons([-0.5, 0.5, -0.5, 0.5])
+    tk1, tk2, ind, kap, dl, bia, sig = rd.read_select_spikes([0.0, T])
+    Ds, dirich, Dsw = O.prep_decoder_gabor(g.h_alpha, g.h_l, g.h_x0, g.h_y0, g.h_ab, g.KAPPA, g.gain, w.Mx, w.My,
+                                           w.Wx, w.Wy, w.dx, w.dy, w.Px, w.Py, norm)
+    uo = O.decode_window(tk1, tk2, ind, kap, dl, bia, norm, Dsw, dirich, w.Wt, w.Mt, T, w.dt, rcond=1e-8)[0]
+    rel = np.linalg.norm(u - uo) / np.linalg.norm(uo)
+    assert rel <= 1e-8, rel
+
+
 def vtem_read(store):
     from vtem_b200 import spike_store as ss
     rd = ss.vtem_storage_read(store)
