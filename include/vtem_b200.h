@@ -359,6 +359,19 @@ int vtb_sym_factor(void* M, int64_t ld, int K, int mode, double rcond, void* wor
 /* x = M^-1 x (float64 x) with a factor of vtb_sym_factor of the same mode. */
 int vtb_sym_potrs(const void* Mfac, int64_t ld, double* x, int K, int mode, void* work, int64_t work_bytes,
                   void* stream);
+/* One system, multi-CTA: x = L^-T L^-1 x (x float64, float32 arithmetic) with
+ * a float32 factor of vtb_sym_factor (mode 2).  CTA j owns rows 64j..64j+63;
+ * the forward and backward solves hand rows on through per-CTA flags
+ * (bounded waits; err (device int32) is set to 3 if one runs out, and the
+ * result is then invalid).  Cooperative launch of ceil(K/64) CTAs, which must
+ * all be resident (else VTB_BAD_ARG).  Replaces cusolverDnSpotrs in the
+ * mixed decoder's solve; the reference's counterpart is the solve of
+ * linalg.py:591-631.  Dinv: vtb_sym_dinv (vtb_sym_dinv_floats(K) floats);
+ * work: vtb_sym_potrs_flags_bytes(K) bytes. */
+int vtb_sym_dinv(const float* L, int64_t ld, int K, float* Dinv, void* stream);
+int64_t vtb_sym_potrs_flags_bytes(int K);
+int vtb_sym_potrs_flags(const float* L, int64_t ld, const float* Dinv, int K, double* x, void* work,
+                        int64_t work_bytes, int32_t* err, void* stream);
 /* Pseudoinverse solve x = V diag(1/w if |w| > rcond*max|w| else 0) V^T b of
  * a float64 symmetric M (destroyed), the rule of solve_eq_sym
  * (vtem/utils/linalg.py:591-631, sq_Kernel :791-833).  kept (device) the

@@ -250,3 +250,38 @@ def test_decode_to_host_matches_device_decode(small_encoded):
     dec.decode_to_host(tk1, tk2, ind, kap, dl, bia, w.T, w.dt, h, chunks=5)
     torch.cuda.synchronize()
     assert ((h - u).norm() / u.norm()).item() < 1e-13
+
+
+@pytest.mark.parametrize("K", [1, 17, 32, 33, 64, 65, 100, 257, 1000, 1921])
+def test_flag_solve_matches_cusolver(K):
+    """The multi-CTA flag hand-off solve (vtb_sym_potrs_flags) against
+    cuSOLVER's spotrs on the same float32 factor and against a float64 solve,
+    for sizes that leave partial 32- and 64-row blocks; twice in a row (the
+    flags are reset per call)."""
+    from vtem_b200._abi import call, dptr, lib, stream_ptr
+    rng = np.random.default_rng(K)
+    Q, _ = np.linalg.qr(rng.standard_normal((K, K)))
+    A = (Q * rng.uniform(1.0, 100.0, K)) @ Q.T
+    A = 0.5 * (A + A.T)
+    M = torch.as_tensor(A, dtype=torch.float32, device="cuda").contiguous()
+    s = stream_ptr()
+    nb = np.zeros(1, np.int64)
+    call("vtb_sym_workspace", K, 2, nb.ctypes.data)
+    work = torch.empty(int(nb[0]), dtype=torch.uint8, device="cuda")
+    stat = torch.zeros(4, dtype=torch.float64, device="cuda")
+    call("vtb_sym_factor", dptr(M), K, K, 2, 1e-12, dptr(work), work.numel(), stat.data_ptr(), stat.data_ptr() + 8, s)
+    dinv = torch.empty(int(lib().vtb_sym_dinv_floats(K)), dtype=torch.float32, device="cuda")
+    fw = torch.empty(int(lib().vtb_sym_potrs_flags_bytes(K)), dtype=torch.uint8, device="cuda")
+    call("vtb_sym_dinv", dptr(M), K, K, dptr(dinv), s)
+    for _ in range(2):
+        b = rng.standard_normal(K)
+        x1 = torch.as_tensor(b, device="cuda")
+        x2 = torch.as_tensor(b, device="cuda")
+        call("vtb_sym_potrs_flags", dptr(M), K, dptr(dinv), K, dptr(x1), dptr(fw), fw.numel(), stat.data_ptr(), s)
+        call("vtb_sym_potrs", dptr(M), K, dptr(x2), K, 2, dptr(work), work.numel(), s)
+        flag = int(stat[:1].view(torch.int32)[0].item())
+        assert flag == 0, flag
+        xr = np.linalg.solve(A, b)
+        a1, a2 = x1.cpu().numpy(), x2.cpu().numpy()
+        assert np.linalg.norm(a1 - a2) <= 1e-4 * np.linalg.norm(xr)
+        assert np.linalg.norm(a1 - xr) <= 1e-4 * np.linalg.norm(xr)

@@ -76,6 +76,9 @@ SIGNATURES = {
     "vtb_sym_workspace": [I, I, P],
     "vtb_sym_factor": [P, L, I, I, D, P, L, P, P, P],
     "vtb_sym_potrs": [P, L, P, I, I, P, L, P],
+    "vtb_sym_dinv": [P, L, I, P, P],
+    "vtb_sym_potrs_flags_bytes": [I],  # restype int64, set in lib()
+    "vtb_sym_potrs_flags": [P, L, P, I, P, P, L, P, P],
     "vtb_norm_ratio": [P, P, I, P, P],
     "vtb_daxpy1": [P, P, I, P],
     "vtb_sym_pinv": [P, L, P, P, I, D, P, L, P, P, P],
@@ -114,7 +117,7 @@ def lib():
             f = getattr(l, name)
             f.argtypes = args
             f.restype = ctypes.c_int
-        for name in ("vtb_sym_dinv_floats", "vtb_tc_group_bytes"):
+        for name in ("vtb_sym_dinv_floats", "vtb_tc_group_bytes", "vtb_sym_potrs_flags_bytes"):
             getattr(l, name).argtypes = [ctypes.c_int]
             getattr(l, name).restype = ctypes.c_int64
         l.vtb_status_string.argtypes = [ctypes.c_int]

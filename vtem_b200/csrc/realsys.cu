@@ -408,6 +408,229 @@ __global__ void __launch_bounds__(128) diag_inv_batched_kernel(float* const* __r
 
 static int64_t dinv_floats(int K) { return (int64_t)((K + 31) / 32) * 1024; }
 
+// ---------------------------------------------------------------------------
+// Multi-CTA triangular solves for ONE system: x = L^-T L^-1 x.
+//
+// cuSOLVER's spotrs at K = 1921 is two chains of ~60 dependent 32-wide block
+// steps (0.12-0.14 ms per triangle), each step a kernel-internal barrier.
+// Here CTA j owns rows 64j..64j+63 (two 32-row sub-blocks A, B) and works
+// left-looking: in the forward solve it accumulates L(rows, i) y_i for every
+// earlier sub-block i as soon as that sub-block's owner has published y_i
+// (a per-CTA flag), then solves its own two sub-blocks with the inverses of
+// the 32 x 32 diagonal blocks (Dinv, from diag_inv_body) and publishes; the
+// backward solve mirrors it from the last CTA down, reading column panels.
+// The chain is 2 x ceil(K/64) flag hand-offs instead of 4 x ceil(K/32) block
+// steps, and every CTA streams only its own panels of L.  The loads of a
+// panel do not depend on the flag, so they are issued before the wait.
+// All CTAs are co-resident (cooperative launch, one CTA per 64 rows, at
+// most one per SM); each wait is bounded: after kTrsvSpinLimit polls the CTA
+// sets *err = 3 and carries on (it still publishes, so no other CTA waits
+// on it forever), and the caller treats the solve as failed.
+constexpr int kTrsvFlagThreads = 256;
+constexpr unsigned kTrsvSpinLimit = 1u << 21;   // x ~40 ns: well under a second
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// lane 0 polls, the warp learns the outcome; false after the limit
+__device__ bool warp_wait_flag(const unsigned* f, int* err) {
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) {
+        unsigned it = 0;
+        while (ld_acquire_u32(f) == 0u) {
+            if (++it > kTrsvSpinLimit || *(volatile int*)err == 3) {
+                atomicExch(err, 3);
+                ok = 0;
+                break;
+            }
+        }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok != 0;
+}
+
+// publish: the warp's stores precede lane 0's release store of the flag
+__device__ __forceinline__ void warp_publish(unsigned* f) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(f), "r"(1u) : "memory");
+}
+
+// v[r] summed over the 32 lanes; lane r receives the total of v[r]
+__device__ __forceinline__ float warp_transpose_reduce(float (&v)[32]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int k = 0; k < o; ++k) {
+            const float send = up ? v[k] : v[k + o];
+            const float keep = up ? v[k + o] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    return v[0];
+}
+
+// sum_k a[k] v[k], v in shared memory (broadcast reads), four chains
+__device__ __forceinline__ float dot32(const float (&a)[32], const float* v) {
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 32; k += 4) {
+        const float4 q = *reinterpret_cast<const float4*>(v + k);
+        s0 = fmaf(a[k], q.x, s0);
+        s1 = fmaf(a[k + 1], q.y, s1);
+        s2 = fmaf(a[k + 2], q.z, s2);
+        s3 = fmaf(a[k + 3], q.w, s3);
+    }
+    return (s0 + s1) + (s2 + s3);
+}
+
+__global__ void __launch_bounds__(kTrsvFlagThreads) trsv_flags_kernel(const float* __restrict__ L, int64_t ld,
+                                                                      const float* __restrict__ Dinv, int K,
+                                                                      double* x, float* ybuf, float* zbuf,
+                                                                      unsigned* flags, int* err) {
+    __shared__ float part[2][8][32];
+    __shared__ __align__(16) float sv[2][32];
+    const int j = blockIdx.x, nc = gridDim.x;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rA = 64 * j, rB = rA + 32;                 // first rows of sub-blocks A, B
+    const int sA = 2 * j, sB = 2 * j + 1;                // their sub-block indices
+    const bool hasB = rB < K;
+    unsigned* ff = flags;                                // forward flags, one per CTA
+    unsigned* fb = flags + nc;                           // backward flags
+    const int ra = rA + lane, rb = rB + lane;
+    // ---- forward: contributions of the sub-blocks i < 2j
+    float accA = 0.f, accB = 0.f;
+    for (int i = w; i < sA; i += 8) {
+        float la[32], lb[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+            const float* col = L + (int64_t)(32 * i + c) * ld;
+            la[c] = ra < K ? col[ra] : 0.f;
+            lb[c] = rb < K ? col[rb] : 0.f;
+        }
+        warp_wait_flag(ff + (i >> 1), err);
+        const float yv = __ldcg(ybuf + 32 * i + lane);   // sub-block i < 2j is full
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+            const float yc = __shfl_sync(0xffffffffu, yv, c);
+            accA = fmaf(la[c], yc, accA);
+            accB = fmaf(lb[c], yc, accB);
+        }
+    }
+    part[0][w][lane] = accA;
+    part[1][w][lane] = accB;
+    // warp 0's operands, loaded before the barrier: rows of Dinv_A, Dinv_B and of L(B, A)
+    float dA[32], dB[32], lba[32];
+    if (w == 0) {
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            dA[k] = Dinv[(int64_t)sA * 1024 + lane * 32 + k];
+            dB[k] = hasB ? Dinv[(int64_t)sB * 1024 + lane * 32 + k] : 0.f;
+            lba[k] = (hasB && rb < K && rA + k < K) ? L[(int64_t)(rA + k) * ld + rb] : 0.f;
+        }
+    }
+    __syncthreads();
+    float yA = 0.f, yB = 0.f;
+    if (w == 0) {
+        float s = ra < K ? (float)x[ra] : 0.f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) s -= part[0][q][lane];
+        sv[0][lane] = s;
+        __syncwarp();
+        yA = dot32(dA, sv[0]);
+        sv[1][lane] = yA;
+        __syncwarp();
+        if (hasB) {
+            float t = rb < K ? (float)x[rb] : 0.f;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) t -= part[1][q][lane];
+            t -= dot32(lba, sv[1]);
+            sv[0][lane] = t;
+            __syncwarp();
+            yB = dot32(dB, sv[0]);
+        }
+        if (ra < K) __stcg(ybuf + ra, yA);
+        if (hasB && rb < K) __stcg(ybuf + rb, yB);
+        warp_publish(ff + j);
+    }
+    __syncthreads();
+    // ---- backward: contributions of the sub-blocks i > 2j+1, last first
+    float cA[32], cB[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) cA[r] = cB[r] = 0.f;
+    const int nsub = (K + 31) >> 5;
+    const int first = sB + 1;
+    // warp w takes i = first + w + 8m, visited from the largest m down
+    const int cnt = nsub > first + w ? (nsub - 1 - first - w) / 8 + 1 : 0;
+    for (int m = cnt - 1; m >= 0; --m) {
+        const int i = first + w + 8 * m;
+        const int ri = 32 * i + lane;                    // row of L this lane reads
+        float va[32], vb[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) {
+            va[r] = (ri < K && rA + r < K) ? L[(int64_t)(rA + r) * ld + ri] : 0.f;
+            vb[r] = (ri < K && rB + r < K) ? L[(int64_t)(rB + r) * ld + ri] : 0.f;
+        }
+        warp_wait_flag(fb + (i >> 1), err);
+        const float xv = ri < K ? __ldcg(zbuf + ri) : 0.f;
+#pragma unroll
+        for (int r = 0; r < 32; ++r) {
+            cA[r] = fmaf(va[r], xv, cA[r]);
+            cB[r] = fmaf(vb[r], xv, cB[r]);
+        }
+    }
+    part[0][w][lane] = warp_transpose_reduce(cA);
+    part[1][w][lane] = warp_transpose_reduce(cB);
+    // warp 0: columns of Dinv_A, Dinv_B (rows of their transposes)
+    if (w == 0) {
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            dA[k] = Dinv[(int64_t)sA * 1024 + k * 32 + lane];
+            dB[k] = hasB ? Dinv[(int64_t)sB * 1024 + k * 32 + lane] : 0.f;
+        }
+    }
+    __syncthreads();
+    if (w == 0) {
+        float xB = 0.f;
+        if (hasB) {
+            float t = yB;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) t -= part[1][q][lane];
+            sv[0][lane] = t;
+            __syncwarp();
+            xB = dot32(dB, sv[0]);
+        }
+        // L(B, A)^T x_B: lane c holds row c of L(B, A) in lba
+        float pr[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) pr[r] = lba[r] * xB;
+        const float lt = warp_transpose_reduce(pr);
+        float t = yA - lt;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) t -= part[0][q][lane];
+        sv[1][lane] = t;
+        __syncwarp();
+        const float xA = dot32(dA, sv[1]);
+        if (ra < K) __stcg(zbuf + ra, xA);
+        if (hasB && rb < K) __stcg(zbuf + rb, xB);
+        warp_publish(fb + j);
+        if (ra < K) x[ra] = (double)xA;
+        if (hasB && rb < K) x[rb] = (double)xB;
+    }
+}
+
+__global__ void __launch_bounds__(128) diag_inv_kernel(const float* __restrict__ L, int64_t ld, int K,
+                                                       float* __restrict__ Dinv) {
+    diag_inv_body(L, ld, K, Dinv);
+}
+
+static int flag_ctas(int K) { return (K + 63) / 64; }
+
 // Workspace: [info 256][vec f32: K floats][w: K doubles][v1: K doubles][lapack work]
 
 struct RealWork {
@@ -637,6 +860,53 @@ VTB_API int vtb_sym_potrs(const void* Mfac, int64_t ld, double* x, int K, int mo
                          rw.info) != CUSOLVER_STATUS_SUCCESS)
         return VTB_CUDA_ERR;
     f32_to_f64_kernel<<<ceil_div(K, 256), 256, 0, s>>>(rw.vf, x, K);
+    return launch_status();
+}
+
+// Inverses of the 32 x 32 diagonal blocks of one float32 factor (lower,
+// column-major) for vtb_sym_potrs_flags: Dinv receives vtb_sym_dinv_floats(K)
+// floats.
+VTB_API int vtb_sym_dinv(const float* L, int64_t ld, int K, float* Dinv, void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && L && Dinv);
+    const int nt = (K + 31) / 32;
+    diag_inv_kernel<<<ceil_div(nt, 4), 128, 0, as_stream(stream)>>>(L, ld, K, Dinv);
+    return launch_status();
+}
+
+VTB_API int64_t vtb_sym_potrs_flags_bytes(int K) {
+    if (K <= 0) return 0;
+    const int64_t nsub = (K + 31) / 32;
+    return al256r(2 * (int64_t)flag_ctas(K) * 4) + 2 * al256r(nsub * 32 * 4);
+}
+
+// x = L^-T L^-1 x (float64 x, float32 arithmetic) for one system with the
+// multi-CTA flag hand-off solve (trsv_flags_kernel); Dinv from vtb_sym_dinv.
+// work: vtb_sym_potrs_flags_bytes(K).  err (device int32): set to 3 if a
+// wait exceeded its limit (the result is then invalid).  VTB_BAD_ARG when
+// the ceil(K/64) CTAs cannot all be resident (K above ~9400 on a B200).
+VTB_API int vtb_sym_potrs_flags(const float* L, int64_t ld, const float* Dinv, int K, double* x, void* work,
+                                int64_t work_bytes, int32_t* err, void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && L && Dinv && x && work && err);
+    VTB_CHECK_ARG(work_bytes >= vtb_sym_potrs_flags_bytes(K));
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    int coop = 0, nsm = 0, per_sm = 0;
+    VTB_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    VTB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    VTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_flags_kernel, kTrsvFlagThreads, 0));
+    int nc = flag_ctas(K);
+    VTB_CHECK_ARG(coop && nc <= nsm * per_sm);
+    const int64_t nsub = (K + 31) / 32;
+    char* wb = reinterpret_cast<char*>(work);
+    unsigned* flags = reinterpret_cast<unsigned*>(wb);
+    float* ybuf = reinterpret_cast<float*>(wb + al256r(2 * (int64_t)nc * 4));
+    float* zbuf = reinterpret_cast<float*>(reinterpret_cast<char*>(ybuf) + al256r(nsub * 32 * 4));
+    cudaStream_t s = as_stream(stream);
+    VTB_CUDA_TRY(cudaMemsetAsync(flags, 0, 2 * (size_t)nc * 4, s));
+    int* errp = reinterpret_cast<int*>(err);
+    void* args[] = {(void*)&L, (void*)&ld, (void*)&Dinv, (void*)&K, (void*)&x, (void*)&ybuf, (void*)&zbuf,
+                    (void*)&flags, (void*)&errp};
+    VTB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)trsv_flags_kernel, dim3(nc), dim3(kTrsvFlagThreads), args, 0, s));
     return launch_status();
 }
 

@@ -37,7 +37,7 @@ import numpy as np
 import torch
 
 from . import _abi, autotune
-from ._abi import VTB_NOT_CONVERGED, VtbError, call, dptr, stream_ptr
+from ._abi import VTB_NOT_CONVERGED, VtbError, call, dptr, lib, stream_ptr
 from .dirichlet import sort_by_neuron
 
 F64 = torch.float64
@@ -227,15 +227,16 @@ class CoeffDecoder(object):
         work = self._workspace(2)
         call("vtb_sym_factor", dptr(self.Mr32), K, K, 2, self.rcond * CHOL_MARGIN, dptr(work), work.numel(),
              self._stat_ptr(0), self._stat_ptr(1), s)
+        solve = self._mixed_solver(s, work)
         self.xr.copy_(self.br)
-        call("vtb_sym_potrs", dptr(self.Mr32), K, dptr(self.xr), K, 2, dptr(work), work.numel(), s)
+        solve(self.xr)
         for i in range(self.mixed_sweeps):
             call("vtb_coeff_unrealify_vec", dptr(self.xr), K, 1, dptr(self.a), 0, s)
             call("vtb_coeff_residual", dptr(tk1), dptr(tk2), dptr(ind), n, self.N, dptr(kap), dptr(dl), dptr(bi),
                  dptr(self.norm), self.Mt, self.W, dptr(self.d), self.Ks, dptr(self.a), dptr(self.gres),
                  dptr(self.r), s)
             call("vtb_coeff_realify_vec", dptr(self.r), K, 1, dptr(self.rr), s)
-            call("vtb_sym_potrs", dptr(self.Mr32), K, dptr(self.rr), K, 2, dptr(work), work.numel(), s)
+            solve(self.rr)
             call("vtb_norm_ratio", dptr(self.rr), dptr(self.xr), K, self._stat_ptr(3 + min(i, 3)), s)
             call("vtb_daxpy1", dptr(self.xr), dptr(self.rr), K, s)
         call("vtb_coeff_unrealify_vec", dptr(self.xr), K, 1, dptr(self.a), 0, s)
@@ -254,6 +255,24 @@ class CoeffDecoder(object):
             self.last_solver = "mixed->" + self.last_solver
             return
         self.last_solver = "mixed"
+
+    def _mixed_solver(self, s, work):
+        """The solve with the float32 factor in Mr32: the multi-CTA flag
+        hand-off solve (diagonal-block inverses formed here, once per
+        factor), or cuSOLVER's spotrs where its CTAs cannot all be resident.
+        A wait that runs out sets the factor's flag, which sends the window
+        to the float64 path."""
+        K = self.K
+        if getattr(self, "_flag_work", None) is None:
+            dev = self.M.device
+            self._dinv = torch.empty(int(lib().vtb_sym_dinv_floats(K)), dtype=torch.float32, device=dev)
+            self._flag_work = torch.empty(int(lib().vtb_sym_potrs_flags_bytes(K)), dtype=torch.uint8, device=dev)
+            self._flags_ok = (K + 63) // 64 <= torch.cuda.get_device_properties(dev).multi_processor_count
+        if not self._flags_ok:
+            return lambda x: call("vtb_sym_potrs", dptr(self.Mr32), K, dptr(x), K, 2, dptr(work), work.numel(), s)
+        call("vtb_sym_dinv", dptr(self.Mr32), K, K, dptr(self._dinv), s)
+        return lambda x: call("vtb_sym_potrs_flags", dptr(self.Mr32), K, dptr(self._dinv), K, dptr(x),
+                              dptr(self._flag_work), self._flag_work.numel(), self._stat_ptr(0), s)
 
     @staticmethod
     def _mixed_converged(r):
