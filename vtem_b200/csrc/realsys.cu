@@ -247,9 +247,9 @@ static int64_t al256r(int64_t x) { return (x + 255) & ~(int64_t)255; }
 // x = L^-T L^-1 x for the lower float32 Cholesky factor L (column-major,
 // element (i, j) at j*ld + i, as spotrf leaves it), for BATCHES of systems:
 // one CTA of 1024 threads solves one system with the right-hand side in
-// shared memory (many systems keep every SM busy; a single system is left to
-// cuSOLVER's multi-CTA spotrs, since one CTA is bound by one SM's share of
-// L2 bandwidth), in 32-wide block steps:
+// shared memory (many systems keep every SM busy; a single system goes to
+// the multi-CTA trsv_flags_kernel below, since one CTA is bound by one SM's
+// share of L2 bandwidth), in 32-wide block steps:
 //   forward  (L y = b):  y_J = Dinv_J r_J (one warp), then every row below
 //            the block subtracts L(i, J) y_J (the thread's rows of column
 //            block J are loaded before the block barrier, hiding L2 latency);
@@ -853,8 +853,8 @@ VTB_API int vtb_sym_potrs(const void* Mfac, int64_t ld, double* x, int K, int mo
             return VTB_CUDA_ERR;
         return launch_status();
     }
-    // one system: cuSOLVER's multi-CTA solves (a single CTA is bound by one
-    // SM's share of L2 bandwidth); batches use trsv_pair_batched_kernel
+    // one system: cuSOLVER's multi-CTA solves (the mixed decoder uses
+    // vtb_sym_potrs_flags instead); batches use trsv_pair_batched_kernel
     f64_to_f32_kernel<<<ceil_div(K, 256), 256, 0, s>>>(x, rw.vf, K);
     if (cusolverDnSpotrs(h, CUBLAS_FILL_MODE_LOWER, K, 1, reinterpret_cast<const float*>(Mfac), (int)ld, rw.vf, K,
                          rw.info) != CUSOLVER_STATUS_SUCCESS)
