@@ -55,3 +55,28 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_abi, "LIB_PATH", str(tmp_path / "nope.so"))
     with pytest.raises(RuntimeError, match="not built"):
         _abi.lib()
+
+
+def header_arities():
+    src = open(os.path.join(ROOT, "include", "vtem_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for name, params in re.findall(r"\b(vtb_\w+)\s*\(([^;{]*?)\)\s*;", src):
+        p = params.strip()
+        out[name] = 0 if p in ("", "void") else p.count(",") + 1
+    return out
+
+
+def test_bindings_match_header_arity():
+    """Every ctypes binding passes as many arguments as the C declaration
+    takes (a drift between the two would pass garbage through the ABI)."""
+    ar = header_arities()
+    bad = {n: (len(a), ar[n]) for n, a in _abi.SIGNATURES.items() if n in ar and len(a) != ar[n]}
+    assert not bad, bad
+
+
+def test_solver_entry_points_reject_bad_sizes_without_gpu():
+    lib = _abi.lib()
+    assert lib.vtb_sym_dinv(None, 0, 0, None, None) == _abi.VTB_BAD_ARG
+    assert lib.vtb_sym_potrs_flags(None, 0, None, 0, None, None, 0, None, None) == _abi.VTB_BAD_ARG
+    assert lib.vtb_sym_potrs_flags_bytes(0) == 0
