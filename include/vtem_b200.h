@@ -98,6 +98,11 @@ int vtb_split_bf16x3(const void* src, int src_f32, int rows, int K, int64_t ld, 
  * caller-zeroed) receives VTB_TIMEOUT if a pipeline wait ever gave up. */
 int vtb_tc_gemm_bf16(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
                      int out_f64, double alpha, int accumulate, int32_t* err, void* stream);
+/* vtb_tc_gemm_bf16 with output tiles 128 x bn, bn in {64, 96, 128, 160, 192,
+ * 256} (vtb_tc_gemm_bf16 is bn = 128); the autotuner picks bn per problem
+ * shape.  VTB_BAD_ARG for any other bn. */
+int vtb_tc_gemm_bf16_bn(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
+                        int out_f64, double alpha, int accumulate, int32_t* err, int bn, void* stream);
 
 /* ------------------------------------------------------------ IAF encoder */
 

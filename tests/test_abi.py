@@ -31,6 +31,12 @@ def test_every_header_symbol_has_a_binding():
     assert not missing, missing
 
 
+def test_every_binding_is_declared_in_the_header():
+    declared = set(header_symbols())
+    undeclared = [s for s in _abi.SIGNATURES if s not in declared]
+    assert not undeclared, undeclared
+
+
 def test_version_and_status_strings():
     lib = _abi.lib()
     assert lib.vtb_version() == 1
