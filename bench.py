@@ -228,6 +228,18 @@ def run_ours(args, rank, world, local):
     mix_ms, f64_ms = reduce_max([mix_ms, f64_ms], dev, world)
     rel_mix_f64 = float(((umix - u64).norm() / u64.norm()).item())
     resid = decmix.residual_norm(*inputs)
+    mix_ratios = list(decmix.last_ratios)
+    gram_err = decmix.gram_error()
+    # BASELINE configuration 2 as specified: the same mixed decoder with 3 float64 refinement sweeps
+    dec3 = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="mixed", mixed_sweeps=3)
+    u3 = torch.empty_like(u64)
+    mix3_ms, _ = time_decoder(dec3, inputs, w, u3, flush, args.steps, args.warmup)
+    mix3_ms = reduce_max([mix3_ms], dev, world)[0]
+    config2 = {"sweeps": 3, "ms_per_step": mix3_ms / args.steps, "solver": dec3.last_solver,
+               "sweep_ratios": list(dec3.last_ratios),
+               "rel_l2_vs_coeff_f64": float(((u3 - u64).norm() / u64.norm()).item()),
+               "residual_rel": dec3.residual_norm(*inputs), "gram_rel_frobenius": gram_err}
+    del u3, dec3
 
     # --- end to end through the public API with host buffers (mixed decoder)
     h_tk1, h_tk2, h_ind = (torch.as_tensor(x).pin_memory() for x in (tk1, tk2, ind))
@@ -282,13 +294,11 @@ def run_ours(args, rank, world, local):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 (split-bf16 tensor-core Gram, f64 refinement)"
             if headline_mixed else "f64",
             "data": "synthetic (seeded Dirichlet-bandlimited video)",
-            "config": {"workload": "gpu: 64x64 px, 10000 samples (1 s, dt=1e-4), Mx=My=6, Mt=8, 768 Gabor + 256 "
-                                   "centre-surround RFs, IAF b~U(2,4) delta~N(0.12,0.012), pinv rcond 1e-8",
-                       "spike_intervals": n, "voxels_per_step": voxels, "K_coeff": dec64.K,
-                       "decoder": ("mixed: tensor-core Gram + %d f64 refinement sweeps" % args.sweeps)
-                       if headline_mixed else "coefficient-space float64",
-                       "l2": "output 328 MB > L2 and a 256 MB flush between steps", "clip_per_rank": True,
-                       "parallelism": "clip-parallel replicas" if world > 1 else "single GPU"},
+            "config": workload_config(w),
+            "config_detail": {"spike_intervals": n, "voxels_per_step": voxels, "K_coeff": dec64.K,
+                              "decoder": ("mixed: tensor-core Gram + %d f64 refinement sweeps" % args.sweeps)
+                              if headline_mixed else "coefficient-space float64", "clip_per_rank": True,
+                              "parallelism": "clip-parallel replicas" if world > 1 else "single GPU"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps * (launches_mixed(decmix) if headline_mixed else launches_per_step(dec64)),
             "roofline": {"bound": "hbm", "kernel": "synth_ws_kernel (warp-specialised synthesis)",
@@ -308,8 +318,13 @@ def run_ours(args, rank, world, local):
             "solver": {"mixed": decmix.last_solver, "f64": dec64.last_solver, "pivots": dec64.last_pivots},
             "near_threshold_events": int(sp.near_threshold),
         }
+        result["config2"] = config2
+        result["mixed_sweep_ratios"] = mix_ratios
+        result["gram_rel_frobenius"] = gram_err
+        if not args.no_serve:
+            result["serving"] = serve_short(dev, args.serve_requests, args.rate)
         if not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline(w, prep, rd)
+            result["cpu_baseline"] = cpu_baseline(host_clip_from_device(w, prep, rd), windows=2, window=0.1)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -346,6 +361,33 @@ def gram_gemm_roofline(dec, peaks, reps=20):
             "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
             "frac": achieved / peaks["bf16_tflops"], "peak_source": peaks["source"], "avg_ms": ms,
             "tensor_flop": flop, "shape": [M, KK, K], "operand_bytes": M * K * 2 + KK * K * 2}
+
+
+def serve_short(dev, requests=64, rate=200.0, seed=3):
+    """A short serving run for the default bench line (BASELINE configuration
+    4's request mix): ``requests`` encode+decode jobs sized like the batch
+    clips (seed 3), Poisson arrivals at ``rate``/s, 120 GB admission budget,
+    2 ms ticks; latency is arrival to result on the host (wall clock)."""
+    import torch
+    from vtem_b200 import serving, workloads
+    clips = workloads.batch_clips(count=requests, seed=seed)
+    reqs = serving.make_requests(clips, rate=rate, seed=seed, device=dev)
+    warm = serving.make_requests(workloads.batch_clips(count=8, seed=1000), rate=rate, seed=7, device=dev)
+    serving.Server(device=dev).run(warm)
+    torch.cuda.synchronize()
+    srv = serving.Server(budget_bytes=120 * 10 ** 9, workers=3, device=dev, solvers=2)
+    done = srv.run(reqs)
+    st = serving.summary(done, srv.wall_s)
+    solvers = {}
+    for r in done:
+        solvers[r.solver] = solvers.get(r.solver, 0) + 1
+    out = {"requests": len(reqs), "rate_per_s": rate, "p50_ms": st["p50_ms"], "p95_ms": st["p95_ms"],
+           "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "voxels_per_s": st["voxels_per_s"],
+           "completed": st["completed"], "failed": st["failed"], "wall_s": srv.wall_s, "solvers": solvers,
+           "max_batch": srv.max_batch}
+    del reqs, done, srv
+    torch.cuda.empty_cache()
+    return out
 
 
 def launches_mixed(dec):
@@ -764,76 +806,216 @@ def run_rnn(w, prep, tk1, tk2, ind, dev, Nt, steps=2000):
     return out
 
 
-# ---------------------------------------------------------------- CPU baseline
+# ---------------------------------------------------------------- CPU baseline / reference arm
 
-def cpu_sample(w, prep, rd, window=0.04, frames=None, use_ref=False):
-    """Decode a window [0, window) of the same spikes on the host, with the
-    reference's formulas (oracle port, or the reference's own kernels when
-    use_ref).  Returns (voxels, seconds, description)."""
+def load_workloads():
+    """``vtem_b200/workloads.py`` loaded by path: the seeded workload
+    definitions only (NumPy and torch, no kernels), so that the reference arm
+    never imports the ``vtem_b200`` package or loads its library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_vtem_workloads", os.path.join(ROOT, "vtem_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+class HostClip(object):
+    """A clip encoded and prepared on the host: spike store contents (block
+    counts and block-relative times, as vtem_storage keeps them) and the
+    decoder preparation (Ds, phi, Dsw)."""
+
+    def __init__(self, w, block_counts, block_spikes, refresh, Ds, dirich, Dsw, seconds):
+        self.w, self.block_counts, self.block_spikes, self.refresh = w, block_counts, block_spikes, refresh
+        self.Ds, self.dirich, self.Dsw, self.setup_s = Ds, dirich, Dsw, seconds
+
+    def window(self, t0, t1):
+        """Spike intervals of [t0, t1), relative to t0 (read_select_spikes)."""
+        from oracle import vtem_oracle as O
+        return O.read_select_spikes(self.block_counts, self.block_spikes, self.refresh, np.arange(self.w.N),
+                                    [t0, t1])
+
+
+def reference_encode(w):
+    """VTEM_IAF + VTDM_prep of the workload's clip with the reference's own
+    kernels compiled for the host (oracle/_ref: gabor/cs RFs, the IAF scan,
+    fft2Ds, Ds2fft, filter2rec, put_norm) and NumPy for the library calls the
+    reference makes (cuBLAS GEMM for the projection and Dsw, cuFFT); the
+    stimulus is the seeded video evaluated by NumPy."""
+    from oracle import ref_runner as R
     from oracle import vtem_oracle as O
-    Dsw = prep.Dsw.cpu().numpy()
-    dirich = prep.dirich.cpu().numpy()
-    # the window's intervals, as read_select_spikes forms them (one spike either side)
-    t1, t2, ii = rd.read_select_spikes([0.0, window])[:3]
-    norm = np.ones(w.N)
-    Nt = len(np.arange(0, window, w.dt)) if frames is None else frames
     t0 = time.perf_counter()
+    V = O.bandlimited_video(w.coeffs, w.Mx, w.My, w.Mt, w.Wx, w.Wy, w.Wt, w.Px, w.Py, 1.0, 1.0, w.F, w.dt)
+    V *= w.scale
+    g, c = w.gabor, w.cs
+    rf = [R.gabor(g.h_alpha, g.h_l, g.h_x0, g.h_y0, g.h_ab, w.Px, w.Py, 1.0, 1.0, -0.5, -0.5, g.KAPPA)
+          * g.gain[:, None, None]]
+    if c is not None:
+        rf.append(R.cs(c.h_alpha, c.h_x0, c.h_y0, w.Px, w.Py, 1.0, 1.0, -0.5, -0.5, c.sigma_center,
+                       c.sigma_surround) * c.gain[:, None, None])
+    rf = np.concatenate(rf, 0)
+    L = (w.dx * w.dy) * (V.reshape(w.F, -1) @ rf.reshape(w.N, -1).T)       # vrf.py:291 (cuBLAS)
+    del V
+    B = min(101, w.F + 1)
+    v0, tc = w.v0.copy(), np.zeros(w.N)
+    counts, spikes = [], []
+    for s, e in O.block_schedule(w.F, B):
+        sp, cnt = R.iaf_encode(L[s:e], w.dt, w.kappa, w.bias, w.delta, v0, tc)
+        tc[:] = 0.0                                                      # reset_timer, vtem.py:197
+        counts.append(cnt)
+        spikes.append(np.concatenate(sp))
+    del L
+    # decoder side: RFs at 4x over one spatial period (vtdm.py:385-435)
+    rfSx, rfSy, rfPx, rfPy = O.rf_period_grid(w.Mx, w.My, w.Wx, w.Wy, w.dx, w.dy)
+    LPx, LPy = rfPx * 4, rfPy * 4
+    fdx, fdy = (rfSx / rfPx) / 4, (rfSy / rfPy) / 4
+    Sx, Sy = LPx * fdx, LPy * fdy
+    fine = [R.gabor(g.h_alpha, g.h_l, g.h_x0, g.h_y0, g.h_ab, LPx, LPy, Sx, Sy, -Sx / 2, -Sy / 2, g.KAPPA)
+            * g.gain[:, None, None]]
+    if c is not None:
+        fine.append(R.cs(c.h_alpha, c.h_x0, c.h_y0, LPx, LPy, Sx, Sy, -Sx / 2, -Sy / 2, c.sigma_center,
+                         c.sigma_surround) * c.gain[:, None, None])
+    fine = np.concatenate(fine, 0)
+    Ds = R.compute_Ds(fine, w.Mx, w.My, fdx * fdy)
+    del fine
+    Px1 = int(np.round(Sx / w.dx))
+    Py1 = int(np.round(Sy / w.dy))
+    dirich = R.dirich_space_fft(Ds, w.Mx, w.My, w.Px, w.Py, Px1, Py1)
+    Dsw = R.compute_Dsw(Ds, np.ones(w.N))
+    return HostClip(w, counts, spikes, (B - 1) * w.dt, Ds, dirich, Dsw, time.perf_counter() - t0)
+
+
+def window_decode(clip, t0, window, use_ref):
+    """One VTDM window of the clip (vtdm.py:630-652) on the host, every frame
+    of the window reconstructed: q, the analytic Gram, the pseudoinverse and
+    the reconstruction, by the reference's own kernels (q, G, sq,
+    reconstruct; NumPy SVD for CULA's gesvd) when ``use_ref``, else by the
+    oracle's NumPy restatement (eigh pseudoinverse, factored reconstruction)
+    on all host threads.  The spike read is outside the timing.  Returns
+    (voxels, seconds, intervals, frames)."""
+    from oracle import vtem_oracle as O
+    w = clip.w
+    t1, t2, ii = clip.window(t0, t0 + window)
+    norm = np.ones(w.N)
+    tt = np.arange(0, window, w.dt)
+    tt = tt[:int(round(window / w.dt))]
+    s = time.perf_counter()
     if use_ref:
         from oracle import ref_runner as R
         q = R.compute_q(t1, t2, ii, w.kappa, w.delta, w.bias, norm)
-        G = R.compute_G(t1, t2, ii, Dsw, w.Wt, w.Mt)
-        c = R.solve_eq_sym(G, q, w.rcond)
-        tt = np.arange(Nt) * w.dt
-        R.reconstruct(dirich, t1, t2, c, tt, ii, norm, w.Mt, w.Wt / w.Mt)
-        kind = "reference"
+        G = R.compute_G(t1, t2, ii, clip.Dsw, w.Wt, w.Mt)
+        cc = R.solve_eq_sym(G, q, w.rcond)
+        R.reconstruct(clip.dirich, t1, t2, cc, tt, ii, norm, w.Mt, w.Wt / w.Mt)
     else:
-        q = O.compute_q(t1, t2, ii, w.kappa, w.delta, w.bias, norm)
-        G = O.compute_G(t1, t2, ii, Dsw, w.Wt, w.Mt)
-        c, _ = O.solve_eq_sym(G, q, w.rcond)
-        O.reconstruct_factored(dirich, t1, t2, c, np.arange(Nt) * w.dt, ii, norm, w.Mt, w.Wt / w.Mt)
-        kind = "port"
-    sec = time.perf_counter() - t0
-    desc = ("decode window of %d spike intervals (first %.3f s of the clip), %d frames x %dx%d px reconstructed, "
-            "q + analytic G + pseudoinverse + reconstruction" % (len(t1), window, Nt, w.Py, w.Px))
-    return Nt * w.Px * w.Py, sec, desc, kind
+        O.decode_window(t1, t2, ii, w.kappa, w.delta, w.bias, norm, clip.Dsw, clip.dirich, w.Wt, w.Mt,
+                        len(tt) * w.dt, w.dt, rcond=w.rcond, threads=os.cpu_count())
+    sec = time.perf_counter() - s
+    return len(tt) * w.Px * w.Py, sec, len(t1), len(tt)
 
 
-def cpu_baseline(w, prep, rd):
-    cores = os.cpu_count() or 1
-    vox, sec, desc, kind = cpu_sample(w, prep, rd)
-    return {"value": vox / sec, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc, "seconds": sec}
+def sample_desc(window, intervals, frames, w, kind):
+    what = ("reference kernels q/G/sq/reconstruct + NumPy SVD (CULA gesvd)" if kind == "reference" else
+            "NumPy restatement: q, analytic G, eigh pseudoinverse, factored reconstruction")
+    return ("consecutive %.3g s decode windows of the clip's spikes (%d-%d intervals each), all %d frames x "
+            "%dx%d px of each window reconstructed; %s" % (window, min(intervals), max(intervals), frames,
+                                                          w.Py, w.Px, what))
 
 
-# ---------------------------------------------------------------- reference arm
+def cpu_baseline(clip, windows=3, window=0.04, use_ref=False):
+    """The oracle port on consecutive windows of the clip (host threads)."""
+    vox, sec, ns = 0, 0.0, []
+    for i in range(windows):
+        v, s, n, f = window_decode(clip, i * window, window, use_ref)
+        vox, sec = vox + v, sec + s
+        ns.append(n)
+    kind = "reference" if use_ref else "port"
+    return {"value": vox / sec, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": kind,
+            "sample": sample_desc(window, ns, f, clip.w, kind), "seconds": sec}
+
+
+def host_clip_from_device(w, prep, rd):
+    """The GPU-encoded clip's spike store and preparation as a HostClip."""
+    return HostClip(w, [np.asarray(c) for c in rd.source.spike_count], [np.asarray(s) for s in rd.source.spikes],
+                    float(rd.source.data["iaf/refresh_interval"]), prep.Ds.cpu().numpy(), prep.dirich.cpu().numpy(),
+                    prep.Dsw.cpu().numpy(), 0.0)
+
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's own kernels compiled for the host
+    (oracle/_ref), NumPy for its library calls, all host threads.  The clip
+    is encoded and prepared by those kernels before the timed steps; each
+    step decodes the next window of the clip (its every frame) as VTDM does
+    for one window.  Rank 0 only; the package under test is never imported."""
     if rank != 0:
         return None
-    import torch
-    from vtem_b200 import workloads
     from oracle import ref_runner as R
-    w = workloads.gpu_scale(seed=0, frames=args.frames)
-    dev = torch.device("cuda", 0) if torch.cuda.is_available() else None
-    if dev is None:
-        return {"impl": "reference", "unavailable": "no CUDA device to encode the clip's spikes"}
-    V, prep, (tk1, tk2, ind), t_enc, sp, rd = encode_clip(w, dev)
-    use_ref = R.available()
-    cores = os.cpu_count() or 1
-    # each step: a bounded sample (a 40 ms decode window, 16 frames reconstructed by the reference's kernel)
-    secs, vox = [], 0
+    if not R.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref (the reference's kernels built for the host) "
+                                                    "is missing: run python oracle/build_ref.py"}
+    W = load_workloads()
+    w = W.gpu_scale(seed=0, frames=args.frames)
+    clip = reference_encode(w)
+    nwin = max(1, int(w.T / args.ref_window))
+    secs, vox, ns = [], 0, []
     for i in range(args.warmup + args.steps):
-        v, s, desc, kind = cpu_sample(w, prep, rd, window=0.04, frames=16, use_ref=use_ref)
+        v, s, n, f = window_decode(clip, (i % nwin) * args.ref_window, args.ref_window, True)
         if i >= args.warmup:
             secs.append(s)
             vox += v
+            ns.append(n)
     value = vox / sum(secs)
+    desc = sample_desc(args.ref_window, ns, f, w, "reference")
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Dirichlet-bandlimited video)",
-            "config": {"workload": "gpu: 64x64 px, 10000 samples, 1024 RFs (bounded sample per step)"},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Dirichlet-bandlimited video)", "config": workload_config(w),
             "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference",
+                             "sample": desc, "setup_s": clip.setup_s},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def workload_config(w):
+    """The ``config`` object both arms print for the GPU configuration."""
+    return {"workload": "gpu: %dx%d px, %d samples (%.3g s, dt=1e-4), Mx=My=%d, Mt=%d, 768 Gabor + 256 "
+                        "centre-surround RFs, IAF b~U(2,4) delta~N(0.12,0.012), pinv rcond %g"
+                        % (w.Px, w.Py, w.F, w.T, w.Mx, w.Mt, w.rcond),
+            "l2": "output 328 MB > L2 and a 256 MB flush between steps"}
+
+
+def run_cpu_full(args):
+    """The whole clip decoded on the host by the oracle's NumPy restatement
+    (all host threads), as ONE window, the way the GPU decodes it: q and the
+    analytic n x n Gram in full, the eigh pseudoinverse in full, and the
+    reconstruction of ``--cpu-frames`` frames spread over the clip,
+    extrapolated linearly to all frames (reported as such).  The spikes are
+    the reference-kernel encode of the clip (``reference_encode``)."""
+    from oracle import vtem_oracle as O
+    W = load_workloads()
+    w = W.gpu_scale(seed=0, frames=args.frames)
+    clip = reference_encode(w)
+    t1, t2, ii = clip.window(0.0, w.T)
+    norm = np.ones(w.N)
+    s0 = time.perf_counter()
+    q = O.compute_q(t1, t2, ii, w.kappa, w.delta, w.bias, norm)
+    G = O.compute_G_threaded(t1, t2, ii, clip.Dsw, w.Wt, w.Mt)
+    s1 = time.perf_counter()
+    c, kept = O.solve_eq_sym(G, q, w.rcond)
+    s2 = time.perf_counter()
+    del G
+    tt = np.arange(w.F) * w.dt
+    pick = np.linspace(0, w.F - 1, args.cpu_frames).astype(np.int64)
+    O.reconstruct_factored_threaded(clip.dirich, t1, t2, c, tt[pick], ii, norm, w.Mt, w.Wt / w.Mt)
+    s3 = time.perf_counter()
+    rec_full = (s3 - s2) * w.F / len(pick)
+    total = (s2 - s0) + rec_full
+    voxels = w.F * w.Px * w.Py
+    return {"metric": METRIC + " [whole clip on the host, one window]", "value": voxels / total, "unit": UNIT,
+            "kind": "port", "cores": os.cpu_count() or 1, "intervals": len(t1), "kept": kept,
+            "stages_s": {"q_G": s1 - s0, "pinv_eigh": s2 - s1,
+                         "reconstruction_extrapolated": rec_full,
+                         "reconstruction_measured": {"frames": len(pick), "seconds": s3 - s2}},
+            "seconds_total": total, "encode_setup_s": clip.setup_s, "config": workload_config(w)}
 
 
 def main():
@@ -848,7 +1030,7 @@ def main():
     ap.add_argument("--no-rnn", action="store_true")
     ap.add_argument("--rnn-steps", type=int, default=2000)
     ap.add_argument("--sweeps", type=int, default=1)
-    ap.add_argument("--workload", default="gpu", choices=["gpu", "batch", "serve", "encode", "stitch"])
+    ap.add_argument("--workload", default="gpu", choices=["gpu", "batch", "serve", "encode", "stitch", "cpu-full"])
     ap.add_argument("--tile", type=int, default=48)
     ap.add_argument("--window", type=float, default=0.5)
     ap.add_argument("--clips", type=int, default=256)
@@ -858,6 +1040,12 @@ def main():
     ap.add_argument("--workers", type=int, default=3)
     ap.add_argument("--solvers", type=int, default=2)
     ap.add_argument("--plain-sample", type=int, default=8)
+    ap.add_argument("--no-serve", action="store_true", help="skip the short serving run of the default line")
+    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--ref-window", type=float, default=0.025,
+                    help="decode window (s) of one reference-arm step")
+    ap.add_argument("--cpu-frames", type=int, default=40,
+                    help="frames reconstructed by --workload cpu-full (the rest extrapolated)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()
@@ -871,6 +1059,8 @@ def main():
         res = run_encode_only(args, rank, world, local)
     elif args.workload == "stitch":
         res = run_stitch(args, rank, world, local)
+    elif args.workload == "cpu-full":
+        res = run_cpu_full(args) if rank == 0 else None
     else:
         res = run_ours(args, rank, world, local)
     if rank == 0 and res is not None:

@@ -46,6 +46,16 @@ int vtb_version(void);
 const char* vtb_status_string(int status);
 int vtb_last_cuda_error(void);
 
+/* Every spin-wait inside this library's kernels (flag hand-offs between
+ * CTAs, grid barriers, mbarrier waits) is bounded: after a number of polls
+ * the waiting CTA records VTB_TIMEOUT in the call's status word, stops
+ * waiting and returns.  polls > 0 makes every kernel launched afterwards (by
+ * any thread of the process) give up after `polls` polls; 0 restores each
+ * kernel's default (well under a second).  *previous (may be NULL) receives
+ * the value replaced.  No counterpart in the reference (its kernels never
+ * wait on one another); meant for tests and diagnostics. */
+int vtb_set_wait_limit(int64_t polls, int64_t* previous);
+
 /* ------------------------------------------------------------ RF banks */
 
 /* Gabor RF bank on a pixel grid, out[n*out_ld + py*Px + px].
@@ -377,6 +387,35 @@ int vtb_sym_dinv(const float* L, int64_t ld, int K, float* Dinv, void* stream);
 int64_t vtb_sym_potrs_flags_bytes(int K);
 int vtb_sym_potrs_flags(const float* L, int64_t ld, const float* Dinv, int K, double* x, void* work,
                         int64_t work_bytes, int32_t* err, void* stream);
+/* Float32 Cholesky of ONE symmetric positive definite K x K matrix A
+ * (column-major, leading dimension ld; the factor L overwrites the lower
+ * triangle), written for the B200: one cooperative launch, 64 x 64 tiles as
+ * a data-flow graph (one CTA walks the diagonal: POTRF, inverse, TRSM of the
+ * sub-diagonal tile, SYRK of the next diagonal tile; every other CTA
+ * accumulates the trailing updates of its tiles in registers and runs their
+ * TRSMs), release/acquire flags between CTAs with bounded waits.  Dinv
+ * (vtb_chol_dinv_floats(K) floats) receives the inverses of the 64 x 64
+ * diagonal tiles of L; work: vtb_chol_work_bytes(K) bytes, 256-byte aligned.
+ * status (device int32, zeroed by the caller) receives 1 (a pivot <= 0), 2
+ * (max/min squared pivot times rcond >= 1: the pseudoinverse might truncate)
+ * or 3 (a wait between CTAs ran out; the factor is then invalid); pivots
+ * (device, 2 doubles, may be NULL) the (min, max) squared pivot.  Replaces
+ * cuSOLVER's spotrf in the mixed decoder's solve of G c = q, whose
+ * reference counterpart is solve_eq_sym (vtem/utils/linalg.py:591-631) as
+ * called per window at vtem/vtdm.py:645-648. */
+int64_t vtb_chol_dinv_floats(int K);
+int64_t vtb_chol_work_bytes(int K);
+int vtb_chol_factor(float* A, int64_t ld, int K, float* Dinv, void* work, int64_t work_bytes, int32_t* status,
+                    double* pivots, double rcond, void* stream);
+/* x = L^-T L^-1 x (x float64 in and out, float32 arithmetic) with the factor
+ * and Dinv of vtb_chol_factor, in one thread-block cluster (16 CTAs where the
+ * GPU can schedule them, else 8): block-row substitution over the 64-row
+ * tiles, each solved block handed to every CTA through distributed shared
+ * memory, one cluster barrier per block.  K <= 10240.  Replaces spotrs in the
+ * same solve (linalg.py:591-631).  vtb_chol_solve_cluster() gives the
+ * cluster size in use (0 before the first call). */
+int vtb_chol_solve(const float* L, int64_t ld, const float* Dinv, int K, double* x, void* stream);
+int vtb_chol_solve_cluster(void);
 /* Pseudoinverse solve x = V diag(1/w if |w| > rcond*max|w| else 0) V^T b of
  * a float64 symmetric M (destroyed), the rule of solve_eq_sym
  * (vtem/utils/linalg.py:591-631, sq_Kernel :791-833).  kept (device) the

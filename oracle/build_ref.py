@@ -10,6 +10,7 @@ the reference applies, and compiles each kernel with g++ against
 ``oracle/_ref/`` (git-ignored, never committed).
 
 Usage:  python oracle/build_ref.py [--reference /path/to/reference]
+        (default: $VTEM_REFERENCE_ROOT, else the container's mount point)
 Needs the reference tree; on a machine without it, the prebuilt
 ``oracle/_ref/libvtem_ref.so`` is used as is.
 """
@@ -24,7 +25,14 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+# where the read-only reference tree is mounted in the build container;
+# VTEM_REFERENCE_ROOT or --reference override it
 DEFAULT_REF = "/root/reference"
+
+
+def reference_root() -> str:
+    """The reference tree to read the kernel strings from."""
+    return os.environ.get("VTEM_REFERENCE_ROOT", DEFAULT_REF)
 
 
 class _Types(dict):
@@ -128,7 +136,7 @@ def compile_all(sources):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=DEFAULT_REF)
+    ap.add_argument("--reference", default=reference_root())
     a = ap.parse_args(argv)
     if not os.path.isdir(os.path.join(a.reference, "vtem")):
         print("reference tree not found at %s; keeping prebuilt oracle/_ref" % a.reference)

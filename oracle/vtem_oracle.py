@@ -450,6 +450,44 @@ def compute_G(tk1, tk2, ind, Dsw, Wt, Mt, lamb=0.0, rows=None):
     return G
 
 
+def _threads(threads):
+    return max(1, int(threads or os.cpu_count() or 1))
+
+
+def compute_G_threaded(tk1, tk2, ind, Dsw, Wt, Mt, lamb=0.0, threads=None, rows_per_task=256):
+    """:func:`compute_G` with its rows split over host threads: the same
+    entries, each computed by the same expression (NumPy releases the GIL
+    inside the element-wise ufuncs)."""
+    from concurrent.futures import ThreadPoolExecutor
+    n = len(tk1)
+    G = np.empty((n, n))
+    starts = list(range(0, n, rows_per_task))
+
+    def task(r0):
+        r = np.arange(r0, min(n, r0 + rows_per_task))
+        G[r0:r0 + len(r)] = compute_G(tk1, tk2, ind, Dsw, Wt, Mt, lamb, rows=r)
+
+    with ThreadPoolExecutor(_threads(threads)) as ex:
+        list(ex.map(task, starts))
+    return G
+
+
+def reconstruct_factored_threaded(dirich, tk1, tk2, c, t, ind, norm, Mt, WM, threads=None, frames_per_task=64):
+    """:func:`reconstruct_factored` with the frames split over host threads."""
+    from concurrent.futures import ThreadPoolExecutor
+    t = np.asarray(t, np.float64)
+    out = np.empty((len(t),) + tuple(dirich.shape[1:]))
+    starts = list(range(0, len(t), frames_per_task))
+
+    def task(f0):
+        f1 = min(len(t), f0 + frames_per_task)
+        out[f0:f1] = reconstruct_factored(dirich, tk1, tk2, c, t[f0:f1], ind, norm, Mt, WM)
+
+    with ThreadPoolExecutor(_threads(threads)) as ex:
+        list(ex.map(task, starts))
+    return out
+
+
 def solve_eq_sym(G, q, rcond=1e-8):
     """Pseudoinverse solve of ``G c = q`` for symmetric PSD G with singular
     values below ``rcond * s_0`` dropped (solve_eq_sym + sq_Kernel,
@@ -587,18 +625,25 @@ def prep_decoder_gabor(h_alpha, h_l, h_x0, h_y0, h_ab, KAPPA, gain, Mx, My, Wx, 
 
 
 def decode_window(tk1, tk2, ind, kappa, delta, bias, norm, Dsw, dirich, Wt, Mt, T, dt, rcond=1e-8,
-                  lamb=0.0, rnn=None):
+                  lamb=0.0, rnn=None, threads=1):
     """One VTDM window (vtdm.py:631-652): q, G, pinv (or rnn3 with
-    ``rnn = (dt, alpha, steps)``), reconstruction at t = arange(0, T, dt)."""
+    ``rnn = (dt, alpha, steps)``), reconstruction at t = arange(0, T, dt).
+    ``threads`` > 1 splits the Gram's rows and the frames over host threads."""
     q = compute_q(tk1, tk2, ind, kappa, delta, bias, norm)
-    G = compute_G(tk1, tk2, ind, Dsw, Wt, Mt, lamb)
+    if threads == 1:
+        G = compute_G(tk1, tk2, ind, Dsw, Wt, Mt, lamb)
+    else:
+        G = compute_G_threaded(tk1, tk2, ind, Dsw, Wt, Mt, lamb, threads=threads)
     if rnn is None:
         c, kept = solve_eq_sym(G, q, rcond)
     else:
         c = rnn3(G, q, *rnn)
         kept = None
     t = np.arange(0, T, dt)
-    u = reconstruct_factored(dirich, tk1, tk2, c, t, ind, norm, Mt, Wt / Mt)
+    if threads == 1:
+        u = reconstruct_factored(dirich, tk1, tk2, c, t, ind, norm, Mt, Wt / Mt)
+    else:
+        u = reconstruct_factored_threaded(dirich, tk1, tk2, c, t, ind, norm, Mt, Wt / Mt, threads=threads)
     return u, c, q, G, kept
 
 

@@ -86,3 +86,18 @@ def test_solver_entry_points_reject_bad_sizes_without_gpu():
     assert lib.vtb_sym_dinv(None, 0, 0, None, None) == _abi.VTB_BAD_ARG
     assert lib.vtb_sym_potrs_flags(None, 0, None, 0, None, None, 0, None, None) == _abi.VTB_BAD_ARG
     assert lib.vtb_sym_potrs_flags_bytes(0) == 0
+
+
+def test_chol_and_wait_limit_entry_points_without_gpu():
+    lib = _abi.lib()
+    assert lib.vtb_chol_work_bytes(0) == 0 and lib.vtb_chol_dinv_floats(0) == 0
+    assert lib.vtb_chol_dinv_floats(1921) == 31 * 4096
+    assert lib.vtb_chol_factor(None, 0, 0, None, None, 0, None, None, 1e-8, None) == _abi.VTB_BAD_ARG
+    assert lib.vtb_chol_solve(None, 0, None, 0, None, None) == _abi.VTB_BAD_ARG
+    assert lib.vtb_set_wait_limit(-1, None) == _abi.VTB_BAD_ARG
+    with _abi.wait_limit(7):
+        import numpy as np
+        prev = np.zeros(1, np.int64)
+        assert lib.vtb_set_wait_limit(7, prev.ctypes.data) == 0 and prev[0] == 7
+    prev = np.zeros(1, np.int64)
+    assert lib.vtb_set_wait_limit(0, prev.ctypes.data) == 0 and prev[0] == 0

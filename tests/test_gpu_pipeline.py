@@ -75,7 +75,9 @@ def test_decode_matches_oracle(small, rcond):
     assert rel <= 1e-8, rel
     Vh = V.cpu().numpy()
     snr = -20 * np.log10(np.linalg.norm(u - Vh) / np.linalg.norm(Vh))
-    assert snr > 20  # reference decoder on this RF bank (see the model-mismatch note in DESIGN)
+    # the encoder samples the RFs on the video grid, the decoder on a 4x grid over one period; RFs
+    # touching the domain edge differ by a few percent between the two sums, which caps the SNR
+    assert snr > 20
 
 
 def test_rnn_decode_matches_oracle(small):

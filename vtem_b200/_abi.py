@@ -32,6 +32,7 @@ D = ctypes.c_double
 SIGNATURES = {
     "vtb_version": [],
     "vtb_last_cuda_error": [],
+    "vtb_set_wait_limit": [L, P],
     "vtb_rf_gabor": [P, P, P, P, P, P, I, I, I, D, D, D, D, D, P, L, P],
     "vtb_rf_cs": [P, P, P, P, I, I, I, D, D, D, D, D, D, P, L, P],
     "vtb_rf_filter": [P, I, I, L, P, I, L, D, P, L, L, P],
@@ -91,6 +92,11 @@ SIGNATURES = {
     "vtb_tc_group_build": [P, I, P, P, P, P, P, P, P, P, I, P],
     "vtb_tc_gemm_grouped": [P, I, I, I, P],
     "vtb_sym_dinv_floats": [I],  # restype int64, set in lib()
+    "vtb_chol_dinv_floats": [I],  # restype int64, set in lib()
+    "vtb_chol_work_bytes": [I],  # restype int64, set in lib()
+    "vtb_chol_factor": [P, L, I, P, P, L, P, P, D, P],
+    "vtb_chol_solve": [P, L, P, I, P, P],
+    "vtb_chol_solve_cluster": [],
 }
 
 _lib = None
@@ -117,7 +123,8 @@ def lib():
             f = getattr(l, name)
             f.argtypes = args
             f.restype = ctypes.c_int
-        for name in ("vtb_sym_dinv_floats", "vtb_tc_group_bytes", "vtb_sym_potrs_flags_bytes"):
+        for name in ("vtb_sym_dinv_floats", "vtb_tc_group_bytes", "vtb_sym_potrs_flags_bytes", "vtb_chol_dinv_floats",
+                     "vtb_chol_work_bytes"):
             getattr(l, name).argtypes = [ctypes.c_int]
             getattr(l, name).restype = ctypes.c_int64
         l.vtb_status_string.argtypes = [ctypes.c_int]
@@ -136,6 +143,26 @@ def call(name, *args):
     if st != VTB_OK:
         raise VtbError(name, st)
     return st
+
+
+class wait_limit(object):
+    """Context manager: inside it, every bounded device wait of the kernels
+    launched (by any thread) gives up after ``polls`` polls and reports
+    VTB_TIMEOUT (vtb_set_wait_limit); the previous limit is restored on exit."""
+
+    def __init__(self, polls):
+        self.polls = int(polls)
+
+    def __enter__(self):
+        import numpy as np
+        prev = np.zeros(1, np.int64)
+        call("vtb_set_wait_limit", self.polls, prev.ctypes.data)
+        self.prev = int(prev[0])
+        return self
+
+    def __exit__(self, *exc):
+        call("vtb_set_wait_limit", self.prev, None)
+        return False
 
 
 def stream_ptr(device=None):

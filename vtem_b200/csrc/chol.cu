@@ -1,0 +1,778 @@
+// Float32 Cholesky factorisation of ONE symmetric positive definite system
+// (the mixed decoder's real-form coefficient system, K = 1921 at the GPU
+// configuration), written for the B200 instead of cuSOLVER's spotrf.
+//
+// spotrf at K = 1921 is latency-bound (a chain of dependent panel steps, 0.67
+// ms for 2.4 GFLOP).  Here one cooperative launch factorises the matrix in
+// 64 x 64 tiles (T = ceil(K/64) tile rows) as a data-flow graph:
+//
+//   CTA 0 ("diagonal") walks the critical path, step k = 0..T-1:
+//     POTRF + inverse of the diagonal tile (k,k) (two 32 x 32 register
+//     factorisations in one warp each, the rest as small shared-memory
+//     products), publishes L_kk^-1 (Dinv) and L_kk;
+//     TRSM of the sub-diagonal tile L_{k+1,k} = A_{k+1,k} L_kk^-T;
+//     SYRK of the next diagonal tile A_{k+1,k+1} -= L_{k+1,k} L_{k+1,k}^T,
+//     which it keeps in shared memory for step k+1.
+//   CTAs 1.. ("workers") run every other piece: for tile (I,J) the updates
+//     A_IJ -= sum_{k'} L_Ik' L_Jk'^T (the 4 x 4 register block of each thread
+//     stays in registers across all of them), then for I >= J+2 the TRSM
+//     with the published Dinv_J.  Diagonal and sub-diagonal tiles receive
+//     from the workers all updates but the last (the diagonal CTA applies
+//     that one), so the diagonal CTA never waits on a round trip through a
+//     worker for data its own previous step produced.
+//
+// Worker tasks are ordered by the step whose outputs they need ("group" g:
+// the TRSM tiles (I, g) for I >= g+2, then the sub-diagonal (g+2, g+1), then
+// the diagonal (g+2, g+2), pre-updated through g) and dealt round-robin; each
+// worker runs its tasks in that order.  Every dependency of a task lies in
+// an earlier position or in a diagonal step that depends only on earlier
+// groups, so with all CTAs co-resident (cooperative launch) the graph cannot
+// deadlock.
+//
+// Hand-offs: a tile's producer stores it, then (after a CTA barrier) thread
+// 0 makes the stores visible (__threadfence) and release-stores the tile's
+// flag; a consumer's thread 0 acquire-polls the flag, the CTA barrier
+// follows, and the tile is read through L2 (ld.global.cg).  Every wait is
+// bounded: after the limit the CTA marks the call aborted (status 3) and all
+// CTAs stop waiting and return.
+//
+// Rows and columns beyond K behave as the identity (0 off the diagonal, 1
+// on it), so K needs no padding.  The factor L is written over the lower
+// triangle of A (column-major, element (i, j) at j*ld + i, as spotrf leaves
+// it); Dinv receives T tiles of 64 x 64 (column-major, tile k at k*4096)
+// holding L_kk^-1 for the triangular solves.  A failed pivot (<= 0 or not a
+// number) or a spread of the squared pivots max/min >= 1/rcond sets the
+// status word to 1 or 2, as vtb_sym_factor's pivot test does.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace vtb {
+
+constexpr int kCT = 64;               // tile
+constexpr int kCTE = kCT * kCT;       // tile elements
+constexpr int kCThreads = 256;
+constexpr unsigned kCholSpin = 1u << 22;
+
+__device__ __forceinline__ unsigned c_ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void c_st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+struct CholCtx {
+    float* A;
+    int64_t ld;
+    int K, T;
+    float* Dinv;
+    unsigned* tflag;     // T*T tile flags: 1 = worker part done, 2 = final L tile published
+    int* abort_word;     // nonzero: some CTA gave up
+    int32_t* status;     // caller's status word
+    double* piv;         // caller's [min, max] squared pivots (may be null)
+    double rcond;
+    unsigned limit;
+};
+
+// thread 0 waits until *f >= v; every thread learns the outcome
+__device__ bool cta_wait(const CholCtx& c, const unsigned* f, unsigned v, int* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned it = 0;
+        while (c_ld_acquire(f) < v) {
+            if (++it > c.limit || *(volatile int*)c.abort_word != 0) {
+                atomicExch(c.abort_word, 1);
+                atomicMax(c.status, 3);
+                ok = 0;
+                break;
+            }
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+__device__ __forceinline__ void cta_publish(unsigned* f, unsigned v) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        c_st_release(f, v);
+    }
+}
+
+// tile (I, J) of A into shared memory s (column-major, 64 x 64); entries
+// beyond K are the identity's
+__device__ void load_tile(const CholCtx& c, float* s, int I, int J) {
+    const int r0 = I * kCT, c0 = J * kCT;
+    const bool full = r0 + kCT <= c.K && c0 + kCT <= c.K;
+    for (int e = threadIdx.x; e < kCTE; e += kCThreads) {
+        const int cc = e >> 6, r = e & 63;
+        const int gr = r0 + r, gc = c0 + cc;
+        float v;
+        if (full || (gr < c.K && gc < c.K)) v = __ldcg(c.A + (int64_t)gc * c.ld + gr);
+        else v = gr == gc ? 1.f : 0.f;
+        s[e] = v;
+    }
+}
+
+// shared tile s into tile (I, J) of A (rows and columns below K; for a
+// diagonal tile the lower triangle only)
+__device__ void store_tile(const CholCtx& c, const float* s, int I, int J) {
+    const int r0 = I * kCT, c0 = J * kCT;
+    for (int e = threadIdx.x; e < kCTE; e += kCThreads) {
+        const int cc = e >> 6, r = e & 63;
+        const int gr = r0 + r, gc = c0 + cc;
+        if (gr < c.K && gc < c.K && (I != J || r >= cc)) __stcg(c.A + (int64_t)gc * c.ld + gr, s[e]);
+    }
+}
+
+// acc[i][j] -= sum_{t0 <= t < t1} P[t][4tr+i] Q[t][4tc+j]  (P, Q column-major 64 x 64)
+__device__ __forceinline__ void sub_ptq(float (&acc)[4][4], const float* P, const float* Q, int tr, int tc, int t0,
+                                        int t1) {
+#pragma unroll 4
+    for (int t = t0; t < t1; ++t) {
+        const float4 p = *reinterpret_cast<const float4*>(P + t * kCT + 4 * tr);
+        const float4 q = *reinterpret_cast<const float4*>(Q + t * kCT + 4 * tc);
+        const float pv[4] = {p.x, p.y, p.z, p.w};
+        const float qv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(-pv[i], qv[j], acc[i][j]);
+    }
+}
+
+__device__ __forceinline__ void acc_from(float (&acc)[4][4], const float* s, int tr, int tc) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = s[(4 * tc + j) * kCT + 4 * tr + i];
+}
+
+__device__ __forceinline__ void acc_to(const float (&acc)[4][4], float* s, int tr, int tc) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) s[(4 * tc + j) * kCT + 4 * tr + i] = acc[i][j];
+}
+
+// X = X L^-T in place: X (column-major 64 x 64, shared), Li = L^-1 (lower,
+// column-major: Li[t*64 + c] = (L^-1)[c][t], zero for t > c)
+__device__ void trsm_right(float* X, const float* Li) {
+    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+    // acc = -(sum_t X[r][t] Li[c][t]) with t <= c
+    sub_ptq(acc, X, Li, tr, tc, 0, 4 * tc + 4);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = -acc[i][j];
+    acc_to(acc, X, tr, tc);
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------- 32 x 32 in one warp
+// Lane r holds row r of the symmetric positive definite block in a[0..31]
+// (a[c] = A[r][c]).  On return a[c] = L[r][c] and x[c] = (L^-1)[r][c] for
+// c <= r (zero above the diagonal).  Right-looking: at step j the pivot is
+// broadcast from lane j, column j of L is formed, the trailing columns and
+// the rows of the inverse (Gauss-Jordan on [L | I]) are updated.  pmin/pmax
+// track the pivots (squared diagonal of L) of the first nvalid rows (the
+// rest are the identity's padding beyond K); a pivot <= 0 or NaN sets bad.
+__device__ __forceinline__ void potrf_inv32(float (&a)[32], float (&x)[32], float& pmin, float& pmax, int& bad,
+                                            int nvalid) {
+    const int r = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < 32; ++c) x[c] = c == r ? 1.f : 0.f;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        float p = __shfl_sync(0xffffffffu, a[j], j);
+        if (!(p > 0.f)) {
+            bad = 1;
+            p = 1.f;
+        }
+        if (j < nvalid) {
+            pmin = fminf(pmin, p);
+            pmax = fmaxf(pmax, p);
+        }
+        const float rs = rsqrtf(p);
+        const float l = r >= j ? a[j] * rs : 0.f;
+        a[j] = l;
+#pragma unroll
+        for (int c = j + 1; c < 32; ++c) a[c] = fmaf(-l, __shfl_sync(0xffffffffu, l, c), a[c]);
+#pragma unroll
+        for (int c = 0; c <= j; ++c) {
+            const float xj = __shfl_sync(0xffffffffu, x[c] * rs, j);
+            x[c] = r == j ? xj : fmaf(-l, xj, x[c]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 32; ++c)
+        if (c > r) a[c] = 0.f;
+}
+
+// The 32 x 32 block at (o, o) of the column-major 64 x 64 tile S: lane r
+// reads row r; writes L into S and L^-1 into the same block of Li.
+__device__ __forceinline__ void warp_block_potrf(float* S, float* Li, int o, float& pmin, float& pmax, int& bad,
+                                                 int nvalid) {
+    const int r = threadIdx.x & 31;
+    float a[32], x[32];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) a[c] = S[(o + c) * kCT + o + r];
+    potrf_inv32(a, x, pmin, pmax, bad, nvalid - o);
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+        S[(o + c) * kCT + o + r] = a[c];
+        Li[(o + c) * kCT + o + r] = c <= r ? x[c] : 0.f;
+    }
+}
+
+// POTRF + inverse of the 64 x 64 tile S (column-major, symmetric positive
+// definite) by 2 x 2 blocks of 32: S <- L (upper triangle zeroed), Li <-
+// L^-1 (lower, upper zero).  Tmp: 32 x 32 scratch (column-major, ld 32).
+// nvalid: rows of the tile below K.
+__device__ void potrf_inv64(float* S, float* Li, float* Tmp, float& pmin, float& pmax, int& bad, int nvalid) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // (1) L11, L11^-1
+    if (w == 0) warp_block_potrf(S, Li, 0, pmin, pmax, bad, nvalid);
+    __syncthreads();
+    // (2) L21 = A21 L11^-T: lane = row r (32 + r), warp w: columns 4w..4w+3
+    {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int t = 0; t < 32; ++t) {
+            const float av = S[t * kCT + 32 + lane];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[j] = fmaf(av, Li[t * kCT + 4 * w + j], acc[j]);   // Li[c][t], t <= c
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 4; ++j) S[(4 * w + j) * kCT + 32 + lane] = acc[j];
+    }
+    __syncthreads();
+    // (3) A22 -= L21 L21^T
+    {
+        float acc[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[j] = S[(32 + 4 * w + j) * kCT + 32 + lane];
+        for (int t = 0; t < 32; ++t) {
+            const float lv = S[t * kCT + 32 + lane];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[j] = fmaf(-lv, S[t * kCT + 32 + 4 * w + j], acc[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) S[(32 + 4 * w + j) * kCT + 32 + lane] = acc[j];
+    }
+    __syncthreads();
+    // (4) warp 0: L22, L22^-1; warps 1..7 meanwhile: Tmp = L21 L11^-1
+    if (w == 0) {
+        warp_block_potrf(S, Li, 32, pmin, pmax, bad, nvalid);
+    } else {
+        for (int e = threadIdx.x - 32; e < 1024; e += kCThreads - 32) {
+            const int rr = e & 31, cc = e >> 5;
+            float s = 0.f;
+            for (int t = cc; t < 32; ++t) s = fmaf(S[t * kCT + 32 + rr], Li[cc * kCT + t], s);   // L21[rr][t] Li11[t][cc]
+            Tmp[cc * 32 + rr] = s;
+        }
+    }
+    __syncthreads();
+    // (5) Li21 = -L22^-1 Tmp: lane = row r, warp w: columns 4w..4w+3
+    {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int t = 0; t <= lane; ++t) {
+            const float lv = Li[(32 + t) * kCT + 32 + lane];   // Li22[lane][t]
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[j] = fmaf(-lv, Tmp[(4 * w + j) * 32 + t], acc[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            Li[(4 * w + j) * kCT + 32 + lane] = acc[j];
+            S[(32 + 4 * w + j) * kCT + lane] = 0.f;            // upper block of L
+            Li[(32 + 4 * w + j) * kCT + lane] = 0.f;           // upper block of L^-1
+        }
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------- worker tasks
+// Group g (0 <= g <= T-3) holds T-g tasks: (I, g) for I = g+2..T-1 (type 0),
+// then (g+2, g+1) (type 1), then (g+2, g+2) (type 2).
+__device__ __forceinline__ void task_of(int T, int t, int& I, int& J, int& type) {
+    int g = 0, base = 0;
+    while (base + (T - g) <= t) {
+        base += T - g;
+        ++g;
+    }
+    const int o = t - base, n0 = T - g - 2;
+    if (o < n0) {
+        I = g + 2 + o;
+        J = g;
+        type = 0;
+    } else if (o == n0) {
+        I = g + 2;
+        J = g + 1;
+        type = 1;
+    } else {
+        I = g + 2;
+        J = g + 2;
+        type = 2;
+    }
+}
+
+struct CholSmem {
+    float a[kCTE];
+    float b[kCTE];
+    float x[kCTE];
+    float tmp[1024];
+    int ok;
+    float pmin[8], pmax[8];
+    int bad;
+};
+
+__device__ void worker(const CholCtx& c, CholSmem& sm) {
+    const int W = gridDim.x - 1, wid = blockIdx.x - 1;
+    const int T = c.T;
+    const int ntask = T >= 3 ? T * (T + 1) / 2 - 3 : 0;
+    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+    for (int t = wid; t < ntask; t += W) {
+        int I, J, type;
+        task_of(T, t, I, J, type);
+        // updates k' < kend, kend = J for type 0, I-1 for types 1 and 2
+        const int kend = type == 0 ? J : I - 1;
+        __syncthreads();
+        load_tile(c, sm.x, I, J);
+        __syncthreads();
+        float acc[4][4];
+        acc_from(acc, sm.x, tr, tc);
+        for (int k = 0; k < kend; ++k) {
+            if (!cta_wait(c, c.tflag + I * T + k, 2u, &sm.ok)) return;
+            if (I != J && !cta_wait(c, c.tflag + J * T + k, 2u, &sm.ok)) return;
+            load_tile(c, sm.a, I, k);
+            if (I != J) load_tile(c, sm.b, J, k);
+            __syncthreads();
+            sub_ptq(acc, sm.a, I != J ? sm.b : sm.a, tr, tc, 0, kCT);
+        }
+        if (type == 0) {
+            if (!cta_wait(c, c.tflag + J * T + J, 2u, &sm.ok)) return;
+            for (int e = threadIdx.x; e < kCTE; e += kCThreads) sm.b[e] = __ldcg(c.Dinv + (int64_t)J * kCTE + e);
+            acc_to(acc, sm.x, tr, tc);
+            __syncthreads();
+            trsm_right(sm.x, sm.b);
+        } else {
+            __syncthreads();
+            acc_to(acc, sm.x, tr, tc);
+            __syncthreads();
+        }
+        store_tile(c, sm.x, I, J);
+        cta_publish(c.tflag + I * T + J, type == 0 ? 2u : 1u);
+    }
+}
+
+__device__ void diagonal(const CholCtx& c, CholSmem& sm) {
+    const int T = c.T;
+    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float pmin = 3.4e38f, pmax = 0.f;
+    int bad = 0;
+    load_tile(c, sm.a, 0, 0);
+    __syncthreads();
+    for (int k = 0; k < T; ++k) {
+        // sm.a holds A_kk with every update applied
+        potrf_inv64(sm.a, sm.b, sm.tmp, pmin, pmax, bad, c.K - k * kCT);
+        for (int e = threadIdx.x; e < kCTE; e += kCThreads) __stcg(c.Dinv + (int64_t)k * kCTE + e, sm.b[e]);
+        store_tile(c, sm.a, k, k);
+        cta_publish(c.tflag + k * T + k, 2u);
+        if (k + 1 >= T) break;
+        // sub-diagonal tile: the workers applied updates k' < k (none when k = 0)
+        if (k >= 1 && !cta_wait(c, c.tflag + (k + 1) * T + k, 1u, &sm.ok)) return;
+        load_tile(c, sm.x, k + 1, k);
+        __syncthreads();
+        trsm_right(sm.x, sm.b);
+        store_tile(c, sm.x, k + 1, k);
+        cta_publish(c.tflag + (k + 1) * T + k, 2u);
+        // next diagonal tile: the workers applied updates k' < k; this CTA applies k
+        if (k >= 1 && !cta_wait(c, c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok)) return;
+        load_tile(c, sm.a, k + 1, k + 1);
+        __syncthreads();
+        float acc[4][4];
+        acc_from(acc, sm.a, tr, tc);
+        sub_ptq(acc, sm.x, sm.x, tr, tc, 0, kCT);
+        __syncthreads();
+        acc_to(acc, sm.a, tr, tc);
+        __syncthreads();
+    }
+    // pivot test (pivots of warp 0, which ran every 32 x 32 factorisation)
+    if (w == 0 && lane == 0) {
+        int f = 0;
+        if (bad) f = 1;
+        else if ((double)pmax / (double)pmin * c.rcond >= 1.0) f = 2;
+        if (f) atomicMax(c.status, f);
+        if (c.piv) {
+            c.piv[0] = (double)pmin;
+            c.piv[1] = (double)pmax;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kCThreads, 1) chol_tiles_kernel(CholCtx c) {
+    extern __shared__ __align__(16) uint8_t chol_smem[];
+    CholSmem& sm = *reinterpret_cast<CholSmem*>(chol_smem);
+    if (blockIdx.x == 0) diagonal(c, sm);
+    else worker(c, sm);
+}
+
+static int chol_tiles(int K) { return (K + kCT - 1) / kCT; }
+
+}  // namespace vtb
+
+using namespace vtb;
+
+VTB_API int64_t vtb_chol_dinv_floats(int K) { return K > 0 ? (int64_t)chol_tiles(K) * kCTE : 0; }
+
+VTB_API int64_t vtb_chol_work_bytes(int K) {
+    if (K <= 0) return 0;
+    const int64_t T = chol_tiles(K);
+    return ((T * T * 4 + 255) & ~(int64_t)255) + 256;
+}
+
+// Float32 Cholesky of the symmetric positive definite K x K matrix A
+// (column-major, leading dimension ld; only the lower triangle is written:
+// A = L L^T with L over the lower triangle).  Dinv (vtb_chol_dinv_floats(K)
+// floats) receives the inverses of the 64 x 64 diagonal tiles of L for
+// vtb_chol_solve.  work: vtb_chol_work_bytes(K) bytes of scratch (cleared
+// here).  status (device int32, cleared by the caller) receives 1 when a
+// pivot fails, 2 when max/min of the squared pivots reaches 1/rcond, 3 when
+// a wait between CTAs ran out; pivots (device, may be NULL) receives [min,
+// max] squared pivots.  Replaces spotrf (cuSOLVER) in the mixed decoder's
+// solve of G c = q (vtem/utils/linalg.py:591-631 as called at
+// vtem/vtdm.py:645-648).  Stream-ordered; does not synchronise.
+VTB_API int vtb_chol_factor(float* A, int64_t ld, int K, float* Dinv, void* work, int64_t work_bytes, int32_t* status,
+                            double* pivots, double rcond, void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && A && Dinv && work && status);
+    VTB_CHECK_ARG(work_bytes >= vtb_chol_work_bytes(K) && ((uintptr_t)work & 255) == 0);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    int coop = 0, nsm = 0;
+    VTB_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    VTB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (!coop) return VTB_CUDA_ERR;
+    const size_t sm = sizeof(CholSmem);
+    VTB_CUDA_TRY(cudaFuncSetAttribute(chol_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int per_sm = 0;
+    VTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chol_tiles_kernel, kCThreads, sm));
+    if (per_sm < 1) return VTB_CUDA_ERR;
+    const int T = chol_tiles(K);
+    const int ntask = T >= 3 ? T * (T + 1) / 2 - 3 : 0;
+    const int grid = 1 + std::max(1, std::min(nsm - 1, ntask));
+    cudaStream_t s = as_stream(stream);
+    const int64_t fbytes = ((int64_t)T * T * 4 + 255) & ~(int64_t)255;
+    VTB_CUDA_TRY(cudaMemsetAsync(work, 0, (size_t)(fbytes + 256), s));
+    CholCtx c;
+    c.A = A;
+    c.ld = ld;
+    c.K = K;
+    c.T = T;
+    c.Dinv = Dinv;
+    c.tflag = reinterpret_cast<unsigned*>(work);
+    c.abort_word = reinterpret_cast<int*>(reinterpret_cast<char*>(work) + fbytes);
+    c.status = status;
+    c.piv = pivots;
+    c.rcond = rcond;
+    c.limit = wait_limit(kCholSpin);
+    void* args[] = {(void*)&c};
+    VTB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)chol_tiles_kernel, dim3(grid), dim3(kCThreads), args, sm, s));
+    return launch_status();
+}
+
+namespace vtb {
+
+// ---------------------------------------------------------------------------
+// x = L^-T L^-1 x for the factor of vtb_chol_factor, in ONE thread-block
+// cluster (C CTAs on one GPC): block-row substitution over the 64-row tiles,
+// the diagonal blocks applied through Dinv (L_kk^-1).  CTA q owns the tile
+// rows k = q, q + C, ...; every CTA keeps the whole solved vector in its
+// shared memory.  Forward step j (one cluster barrier each):
+//   owner(j):  y_j = Dinv_j (b_j - s_j - L_{j,j-1} y_{j-1}), then stores y_j
+//              into every CTA's shared memory (distributed shared memory);
+//   every CTA: s_k += L_{k,j-1} y_{j-1} for its rows k > j
+// (s_k: the running sum of the already solved blocks), so the chain between
+// two barriers is one 64 x 64 product and one application of Dinv.  The
+// backward pass is the mirror image with L^T.  Each step's tiles are loaded
+// into registers BEFORE the barrier that releases the previous block, so
+// their L2 latency overlaps the wait.  No spin-wait: the cluster barrier is
+// the hardware's, and every CTA takes every step.
+constexpr int kSThreads = 256;
+constexpr int kSPre = 4;          // own tiles per step loaded ahead in registers
+constexpr int kSMaxT = 160;       // K <= 10240
+
+struct SolveSmem {
+    float v[kSMaxT * kCT];        // y (forward), then x (backward)
+    float s[24][kCT];             // running sums of own rows (ceil(T/C) <= 24)
+    float red[kSPre + 1][4][kCT]; // partial products of one step
+    float t[kCT + 1];             // the owner's block before Dinv
+    float tile[kCT * (kCT + 1)];  // padded tile for the transposed products
+};
+
+__device__ __forceinline__ void dsm_store(float* local_addr, unsigned rank, float v) {
+    uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(local_addr)), r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(r), "f"(v) : "memory");
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// this thread's 16 elements of tile (I, J): rows r = t & 63, columns 16q..16q+15
+__device__ __forceinline__ void load16(const float* A, int64_t ld, int K, int I, int J, float (&v)[16]) {
+    const int r = threadIdx.x & 63, q = threadIdx.x >> 6;
+    const int gr = I * kCT + r;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+        const int gc = J * kCT + 16 * q + c;
+        v[c] = (gr < K && gc < K) ? __ldcg(A + (int64_t)gc * ld + gr) : (gr == gc ? 1.f : 0.f);
+    }
+}
+
+__global__ void __launch_bounds__(kSThreads, 1) chol_solve_kernel(const float* __restrict__ A, int64_t ld,
+                                                                  const float* __restrict__ Dinv, int K, double* x) {
+    extern __shared__ __align__(16) uint8_t solve_smem[];
+    SolveSmem& sm = *reinterpret_cast<SolveSmem*>(solve_smem);
+    const int T = (K + kCT - 1) / kCT;
+    unsigned C, q;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(C));
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(q));
+    const int tid = threadIdx.x, r = tid & 63, qq = tid >> 6;
+    const int nown = ((int)T - (int)q + (int)C - 1) / (int)C;   // own rows k = q + C m
+    for (int e = tid; e < 24 * kCT; e += kSThreads) (&sm.s[0][0])[e] = 0.f;
+    cluster_sync_all();
+
+    // ------------------------------------------------ forward: L y = b
+    for (int j = 0; j < T; ++j) {
+        const bool own = (j % (int)C) == (int)q;
+        // own rows k > j with a term from block j-1, in order: the first kSPre
+        // tiles ahead in registers
+        float crit[16], dv[16], pre[kSPre][16];
+        if (own && j >= 1) load16(A, ld, K, j, j - 1, crit);
+        if (own) {
+#pragma unroll
+            for (int c = 0; c < 16; ++c) dv[c] = __ldcg(Dinv + (int64_t)j * kCTE + (16 * qq + c) * kCT + r);
+        }
+        const int m0 = (j + 1 - (int)q + (int)C - 1) / (int)C;    // first own row index k = q + C m > j
+        const int mstart = m0 < 0 ? 0 : m0;
+        if (j >= 1) {
+#pragma unroll
+            for (int p = 0; p < kSPre; ++p) {
+                const int m = mstart + p;
+                if (m < nown) load16(A, ld, K, (int)q + (int)C * m, j - 1, pre[p]);
+            }
+        }
+        cluster_sync_all();                     // y_{j-1} is in every CTA's v
+        const float* yp = sm.v + (j - 1) * kCT;
+        if (own) {
+            float acc = 0.f;
+            if (j >= 1) {
+#pragma unroll
+                for (int c = 0; c < 16; ++c) acc = fmaf(crit[c], yp[16 * qq + c], acc);
+            }
+            sm.red[kSPre][qq][r] = acc;
+            __syncthreads();
+            if (tid < kCT) {
+                const int gr = j * kCT + tid;
+                const float b = gr < K ? (float)x[gr] : 0.f;
+                const int mj = (j - (int)q) / (int)C;
+                sm.t[tid] = b - sm.s[mj][tid] - ((sm.red[kSPre][0][tid] + sm.red[kSPre][1][tid]) +
+                                                 (sm.red[kSPre][2][tid] + sm.red[kSPre][3][tid]));
+            }
+            __syncthreads();
+            float y = 0.f;
+#pragma unroll
+            for (int c = 0; c < 16; ++c) y = fmaf(dv[c], sm.t[16 * qq + c], y);   // Dinv[r][16qq+c]
+            sm.red[kSPre][qq][r] = y;
+            __syncthreads();
+            if (tid < kCT) {
+                const float yj = (sm.red[kSPre][0][tid] + sm.red[kSPre][1][tid]) +
+                                 (sm.red[kSPre][2][tid] + sm.red[kSPre][3][tid]);
+                for (unsigned d = 0; d < C; ++d) dsm_store(sm.v + j * kCT + tid, d, yj);
+            }
+        }
+        // non-critical: s_k += L_{k,j-1} y_{j-1} for own k > j
+        if (j >= 1) {
+            for (int m = mstart; m < nown; m += kSPre) {
+#pragma unroll
+                for (int p = 0; p < kSPre; ++p) {
+                    const int mm = m + p;
+                    float acc = 0.f;
+                    if (mm < nown) {
+                        float w[16];
+                        if (m == mstart) {
+#pragma unroll
+                            for (int c = 0; c < 16; ++c) w[c] = pre[p][c];
+                        } else {
+                            load16(A, ld, K, (int)q + (int)C * mm, j - 1, w);
+                        }
+#pragma unroll
+                        for (int c = 0; c < 16; ++c) acc = fmaf(w[c], yp[16 * qq + c], acc);
+                    }
+                    sm.red[p][qq][r] = acc;
+                }
+                __syncthreads();
+                if (tid < kCT) {
+                    for (int p = 0; p < kSPre && m + p < nown; ++p)
+                        sm.s[m + p][tid] += (sm.red[p][0][tid] + sm.red[p][1][tid]) +
+                                            (sm.red[p][2][tid] + sm.red[p][3][tid]);
+                }
+                __syncthreads();
+            }
+        }
+    }
+    cluster_sync_all();                         // y complete everywhere
+    for (int e = tid; e < 24 * kCT; e += kSThreads) (&sm.s[0][0])[e] = 0.f;
+    __syncthreads();
+
+    // ------------------------------------------------ backward: L^T x = y
+    // step j = T-1 .. 0: owner(j): x_j = Dinv_j^T (y_j - s_j - L_{j+1,j}^T x_{j+1});
+    // every CTA: s_k += L_{j+1,k}^T x_{j+1} for own k < j
+    for (int j = T - 1; j >= 0; --j) {
+        const bool own = (j % (int)C) == (int)q;
+        float crit[16], dv[16];
+        if (own && j + 1 < T) load16(A, ld, K, j + 1, j, crit);
+        if (own) {
+#pragma unroll
+            for (int c = 0; c < 16; ++c) dv[c] = __ldcg(Dinv + (int64_t)j * kCTE + (16 * qq + c) * kCT + r);
+        }
+        cluster_sync_all();                     // x_{j+1} is in every CTA's v
+        const float* xp = sm.v + (j + 1) * kCT;
+        if (own) {
+            const int mj = (j - (int)q) / (int)C;
+            // tile L_{j+1,j} (rows of block j+1, columns of block j) transposed: padded shared copy
+            if (j + 1 < T) {
+#pragma unroll
+                for (int c = 0; c < 16; ++c) sm.tile[(16 * qq + c) * (kCT + 1) + r] = crit[c];
+            }
+            __syncthreads();
+            // thread (r, qq): column c = r of the tile, rows 16qq..16qq+15
+            float acc = 0.f;
+            if (j + 1 < T) {
+#pragma unroll
+                for (int k = 0; k < 16; ++k) acc = fmaf(sm.tile[r * (kCT + 1) + 16 * qq + k], xp[16 * qq + k], acc);
+            }
+            sm.red[kSPre][qq][r] = acc;
+            __syncthreads();
+            if (tid < kCT)
+                sm.t[tid] = sm.v[j * kCT + tid] - sm.s[mj][tid] -
+                            ((sm.red[kSPre][0][tid] + sm.red[kSPre][1][tid]) +
+                             (sm.red[kSPre][2][tid] + sm.red[kSPre][3][tid]));
+            // Dinv_j^T: x[c] = sum_{r >= c} Dinv[r][c] t[r]
+#pragma unroll
+            for (int c = 0; c < 16; ++c) sm.tile[(16 * qq + c) * (kCT + 1) + r] = dv[c];
+            __syncthreads();
+            float xv = 0.f;
+#pragma unroll
+            for (int k = 0; k < 16; ++k) xv = fmaf(sm.tile[r * (kCT + 1) + 16 * qq + k], sm.t[16 * qq + k], xv);
+            sm.red[kSPre][qq][r] = xv;
+            __syncthreads();
+            if (tid < kCT) {
+                const float xj = (sm.red[kSPre][0][tid] + sm.red[kSPre][1][tid]) +
+                                 (sm.red[kSPre][2][tid] + sm.red[kSPre][3][tid]);
+                for (unsigned d = 0; d < C; ++d) dsm_store(sm.v + j * kCT + tid, d, xj);
+            }
+        }
+        // non-critical: s_k += L_{j+1,k}^T x_{j+1} for own k < j
+        if (j + 1 < T) {
+            for (int m = 0; m < nown; ++m) {
+                const int k = (int)q + (int)C * m;
+                if (k >= j) break;
+                float w[16];
+                load16(A, ld, K, j + 1, k, w);
+                __syncthreads();
+#pragma unroll
+                for (int c = 0; c < 16; ++c) sm.tile[(16 * qq + c) * (kCT + 1) + r] = w[c];
+                __syncthreads();
+                float acc = 0.f;
+#pragma unroll
+                for (int kk = 0; kk < 16; ++kk)
+                    acc = fmaf(sm.tile[r * (kCT + 1) + 16 * qq + kk], xp[16 * qq + kk], acc);
+                sm.red[0][qq][r] = acc;
+                __syncthreads();
+                if (tid < kCT)
+                    sm.s[m][tid] += (sm.red[0][0][tid] + sm.red[0][1][tid]) + (sm.red[0][2][tid] + sm.red[0][3][tid]);
+            }
+        }
+    }
+    cluster_sync_all();
+    if (q == 0)
+        for (int i = tid; i < K; i += kSThreads) x[i] = (double)sm.v[i];
+    cluster_sync_all();                         // no CTA leaves while its shared memory may be written
+}
+
+// cluster size: 16 CTAs where the non-portable size can be scheduled, else 8
+static int g_solve_cs = 0;
+
+static cudaError_t launch_solve(int cs, const float* L, int64_t ld, const float* Dinv, int K, double* x,
+                                cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(kSThreads);
+    cfg.dynamicSmemBytes = sizeof(SolveSmem);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, chol_solve_kernel, L, ld, Dinv, K, x);
+}
+
+}  // namespace vtb
+
+// x = L^-T L^-1 x (x float64 in and out, float32 arithmetic) with the factor
+// and the diagonal-tile inverses of vtb_chol_factor, in one thread-block
+// cluster.  K <= 10240.  Replaces spotrs (cuSOLVER) in the mixed decoder.
+// Stream-ordered; does not synchronise.
+VTB_API int vtb_chol_solve(const float* L, int64_t ld, const float* Dinv, int K, double* x, void* stream) {
+    VTB_CHECK_ARG(K > 0 && K <= kSMaxT * kCT && ld >= K && L && Dinv && x);
+    if (g_solve_cs == 0) {
+        VTB_CUDA_TRY(cudaFuncSetAttribute(chol_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)sizeof(SolveSmem)));
+        int cs = 8;
+        if (cudaFuncSetAttribute(chol_solve_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+            cudaSuccess) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(16);
+            cfg.blockDim = dim3(kSThreads);
+            cfg.dynamicSmemBytes = sizeof(SolveSmem);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = 16;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, chol_solve_kernel, &cfg) == cudaSuccess && nclusters > 0)
+                cs = 16;
+        }
+        cudaGetLastError();
+        g_solve_cs = cs;
+    }
+    VTB_CUDA_TRY(launch_solve(g_solve_cs, L, ld, Dinv, K, x, as_stream(stream)));
+    return launch_status();
+}
+
+// CTAs of the cluster vtb_chol_solve launches (0 before its first call).
+VTB_API int vtb_chol_solve_cluster(void) { return vtb::g_solve_cs; }

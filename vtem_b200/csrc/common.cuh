@@ -18,6 +18,10 @@ int launch_status();
 
 void set_last_cuda_error(cudaError_t e);
 
+// Polls after which a bounded device wait gives up: the process-wide value
+// set by vtb_set_wait_limit, else the kernel's default.
+uint32_t wait_limit(uint32_t default_polls);
+
 constexpr int kNumSMs = 148;
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }

@@ -436,12 +436,12 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 }
 
 // lane 0 polls, the warp learns the outcome; false after the limit
-__device__ bool warp_wait_flag(const unsigned* f, int* err) {
+__device__ bool warp_wait_flag(const unsigned* f, int* err, unsigned limit) {
     int ok = 1;
     if ((threadIdx.x & 31) == 0) {
         unsigned it = 0;
         while (ld_acquire_u32(f) == 0u) {
-            if (++it > kTrsvSpinLimit || *(volatile int*)err == 3) {
+            if (++it > limit || *(volatile int*)err == 3) {
                 atomicExch(err, 3);
                 ok = 0;
                 break;
@@ -492,7 +492,7 @@ __device__ __forceinline__ float dot32(const float (&a)[32], const float* v) {
 __global__ void __launch_bounds__(kTrsvFlagThreads) trsv_flags_kernel(const float* __restrict__ L, int64_t ld,
                                                                       const float* __restrict__ Dinv, int K,
                                                                       double* x, float* ybuf, float* zbuf,
-                                                                      unsigned* flags, int* err) {
+                                                                      unsigned* flags, int* err, unsigned limit) {
     __shared__ float part[2][8][32];
     __shared__ __align__(16) float sv[2][32];
     const int j = blockIdx.x, nc = gridDim.x;
@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(kTrsvFlagThreads) trsv_flags_kernel(const floa
             la[c] = ra < K ? col[ra] : 0.f;
             lb[c] = rb < K ? col[rb] : 0.f;
         }
-        warp_wait_flag(ff + (i >> 1), err);
+        warp_wait_flag(ff + (i >> 1), err, limit);
         const float yv = __ldcg(ybuf + 32 * i + lane);   // sub-block i < 2j is full
 #pragma unroll
         for (int c = 0; c < 32; ++c) {
@@ -576,7 +576,7 @@ __global__ void __launch_bounds__(kTrsvFlagThreads) trsv_flags_kernel(const floa
             va[r] = (ri < K && rA + r < K) ? L[(int64_t)(rA + r) * ld + ri] : 0.f;
             vb[r] = (ri < K && rB + r < K) ? L[(int64_t)(rB + r) * ld + ri] : 0.f;
         }
-        warp_wait_flag(fb + (i >> 1), err);
+        warp_wait_flag(fb + (i >> 1), err, limit);
         const float xv = ri < K ? __ldcg(zbuf + ri) : 0.f;
 #pragma unroll
         for (int r = 0; r < 32; ++r) {
@@ -904,8 +904,9 @@ VTB_API int vtb_sym_potrs_flags(const float* L, int64_t ld, const float* Dinv, i
     cudaStream_t s = as_stream(stream);
     VTB_CUDA_TRY(cudaMemsetAsync(flags, 0, 2 * (size_t)nc * 4, s));
     int* errp = reinterpret_cast<int*>(err);
+    unsigned limit = wait_limit(kTrsvSpinLimit);
     void* args[] = {(void*)&L, (void*)&ld, (void*)&Dinv, (void*)&K, (void*)&x, (void*)&ybuf, (void*)&zbuf,
-                    (void*)&flags, (void*)&errp};
+                    (void*)&flags, (void*)&errp, (void*)&limit};
     VTB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)trsv_flags_kernel, dim3(nc), dim3(kTrsvFlagThreads), args, 0, s));
     return launch_status();
 }

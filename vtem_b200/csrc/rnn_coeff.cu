@@ -27,7 +27,7 @@ constexpr int kRnnThreads = 256;
 
 // Generation barrier over all CTAs of the launch (cooperative launch: all
 // co-resident).  count/gen live in global memory, zeroed before the launch.
-__device__ bool rnn_grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, int* err) {
+__device__ bool rnn_grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, int* err, unsigned limit) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -42,7 +42,7 @@ __device__ bool rnn_grid_barrier(unsigned* count, unsigned* gen, unsigned nblock
         } else {
             unsigned it = 0;
             while (*vgen == g) {
-                if (++it > kRnnSpinLimit || *(volatile int*)err) {
+                if (++it > limit || *(volatile int*)err) {
                     atomicExch(err, 1);
                     ok = 0;
                     break;
@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(kRnnThreads) rnn_coeff_kernel(const double* __
                                                                 const double* __restrict__ br, double* xa,
                                                                 double* xb, int K, double dta, int updates,
                                                                 int rows_per_block, int cache_rows,
-                                                                unsigned* bar, int* err) {
+                                                                unsigned* bar, int* err, unsigned limit) {
     extern __shared__ double rnn_sm[];
     double* sx = rnn_sm;                 // K: previous iterate
     double* sM = rnn_sm + K;             // rows_per_block x K (when cache_rows)
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(kRnnThreads) rnn_coeff_kernel(const double* __
             for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             if (lane == 0) __stcg(nxt + r, sx[r] + dta * (br[r] - s));
         }
-        if (!rnn_grid_barrier(bar, bar + 1, gridDim.x, err)) return;
+        if (!rnn_grid_barrier(bar, bar + 1, gridDim.x, err, limit)) return;
     }
 }
 
@@ -130,8 +130,9 @@ VTB_API int vtb_rnn_coeff(const double* Mr, int64_t ld, const double* br, double
     int* err = reinterpret_cast<int*>(b + 2);
     double* xa = x;
     double* xb = x_tmp;
+    unsigned limit = wait_limit(kRnnSpinLimit);
     void* args[] = {(void*)&Mr, (void*)&ld, (void*)&br, (void*)&xa, (void*)&xb, (void*)&K, (void*)&dt_alpha,
-                    (void*)&updates, (void*)&rows, (void*)&cache, (void*)&b, (void*)&err};
+                    (void*)&updates, (void*)&rows, (void*)&cache, (void*)&b, (void*)&err, (void*)&limit};
     VTB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)rnn_coeff_kernel, dim3(blocks), dim3(kRnnThreads), args, sm, s));
     // the result is in xa after an even number of updates, else in xb
     if (updates & 1) VTB_CUDA_TRY(cudaMemcpyAsync(x, x_tmp, (size_t)K * 8, cudaMemcpyDeviceToDevice, s));

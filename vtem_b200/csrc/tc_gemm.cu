@@ -31,6 +31,9 @@ constexpr int kTcBM = 128;
 constexpr int kTcBK = 64;   // 64 bf16 = 128 bytes = one swizzle row
 constexpr int kTcStages = 4;
 constexpr uint32_t kWaitLimit = 1u << 22;
+// drain of a CTA that gave up: its own TMA loads and MMAs complete without
+// depending on anything else, so this bound is only a backstop
+constexpr uint32_t kDrainLimit = 1u << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -46,9 +49,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 }
 
 // bounded wait on the phase with the given parity; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -98,7 +101,8 @@ struct TcSmem {
 template <int BN, typename OutT>
 __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMap* tmB, int M, int N, int K, int m0,
                                         int n0, OutT* __restrict__ C, int64_t c_m, int64_t c_n, double alpha,
-                                        int accumulate, int32_t* __restrict__ err, uint8_t* smem_raw) {
+                                        int accumulate, int32_t* __restrict__ err, uint32_t limit,
+                                        uint8_t* smem_raw) {
     // 1024-byte alignment of the stage buffers (the swizzle atoms)
     TcSmem<BN>& sm = *reinterpret_cast<TcSmem<BN>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     const int tid = threadIdx.x;
@@ -126,16 +130,18 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
     const uint32_t tmem = sm.tmem_base;
     bool ok = true;
 
+    int issued = 0;   // TMA stages the producer issued
     if (tid == 0) {
         // producer
         constexpr uint32_t bytes = (kTcBM + BN) * kTcBK * 2;
         for (int kb = 0; kb < nk && ok; ++kb) {
             const int s = kb % kTcStages;
-            if (kb >= kTcStages) ok = mbar_wait(&sm.empty[s], ((kb / kTcStages) + 1) & 1);
+            if (kb >= kTcStages) ok = mbar_wait(&sm.empty[s], ((kb / kTcStages) + 1) & 1, limit);
             if (!ok) break;
             mbar_expect_tx(&sm.full[s], bytes);
             tma_load_2d(sm.a[s], tmA, &sm.full[s], kb * kTcBK, m0);
             tma_load_2d(sm.b[s], tmB, &sm.full[s], kb * kTcBK, n0);
+            issued = kb + 1;
         }
         if (!ok) atomicExch(err, VTB_TIMEOUT);
     } else if (tid == 32) {
@@ -143,7 +149,7 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
         constexpr uint32_t idesc = TcIdesc<BN>::value;
         for (int kb = 0; kb < nk && ok; ++kb) {
             const int s = kb % kTcStages;
-            ok = mbar_wait(&sm.full[s], (kb / kTcStages) & 1);
+            ok = mbar_wait(&sm.full[s], (kb / kTcStages) & 1, limit);
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint64_t da = smem_desc_sw128(sm.a[s]);
@@ -164,17 +170,21 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
                              smem_u32(&sm.empty[s]))
                          : "memory");
         }
-        if (ok)
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&sm.done))
-                         : "memory");
-        else
-            atomicExch(err, VTB_TIMEOUT);
+        // committed also after a timeout: `done` then tracks the MMAs that
+        // were issued, so the tensor memory is freed only after they finish
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&sm.done))
+                     : "memory");
+        if (!ok) atomicExch(err, VTB_TIMEOUT);
     }
     __syncwarp();
     // epilogue: every warp waits for the accumulator (or gives up with the others)
-    bool have = (nk > 0) && mbar_wait(&sm.done, 0);
-    if (!have && nk > 0 && (tid & 31) == 0) atomicExch(err, VTB_TIMEOUT);
+    bool have = (nk > 0) && mbar_wait(&sm.done, 0, limit);
+    if (!have && nk > 0) {
+        if ((tid & 31) == 0) atomicExch(err, VTB_TIMEOUT);
+        // the issued MMAs finish before the accumulator is touched or freed
+        mbar_wait(&sm.done, 0, kDrainLimit);
+    }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int row = m0 + warp * 32 + (tid & 31);
 #pragma unroll 1
@@ -200,6 +210,10 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
             }
         }
     }
+    // a CTA that gave up drains its producer's issued TMA loads before it exits
+    if (tid == 0)
+        for (int kb = issued > kTcStages ? issued - kTcStages : 0; kb < issued; ++kb)
+            mbar_wait(&sm.full[kb % kTcStages], (kb / kTcStages) & 1, kDrainLimit);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
@@ -211,10 +225,10 @@ template <int BN, typename OutT>
 __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
                                                          const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
                                                          OutT* __restrict__ C, int64_t c_m, int64_t c_n, double alpha,
-                                                         int accumulate, int32_t* __restrict__ err) {
+                                                         int accumulate, int32_t* __restrict__ err, uint32_t limit) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     tc_tile<BN, OutT>(&tmA, &tmB, M, N, K, blockIdx.y * kTcBM, blockIdx.x * BN, C, c_m, c_n, alpha, accumulate, err,
-                      smem_raw);
+                      limit, smem_raw);
 }
 
 // Grouped GEMM: many independent problems C_p = A_p B_p^T (float32 output,
@@ -233,7 +247,8 @@ struct TcGroupProblem {
 };
 
 template <int BN>
-__global__ void __launch_bounds__(128, 1) tc_gemm_grouped_kernel(const TcGroupProblem* __restrict__ probs, int nprob) {
+__global__ void __launch_bounds__(128, 1) tc_gemm_grouped_kernel(const TcGroupProblem* __restrict__ probs, int nprob,
+                                                                  uint32_t limit) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const int tile = blockIdx.x;
     int lo = 0, hi = nprob - 1;
@@ -252,7 +267,7 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_grouped_kernel(const TcGroupPr
     const int ntn = (p->N + BN - 1) / BN;
     const int t = tile - p->tile_start;
     tc_tile<BN, float>(&p->ma, &p->mb, p->M, p->N, p->K, (t / ntn) * kTcBM, (t % ntn) * BN, p->C, p->ldc, 1, 1.0, 0,
-                       p->err, smem_raw);
+                       p->err, limit, smem_raw);
 }
 
 // ------------------------------------------------------------------ split-bf16 operands
@@ -317,7 +332,8 @@ static int launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N,
         return VTB_CUDA_ERR;
     }
     dim3 grid(ceil_div(N, BN), ceil_div(M, kTcBM));
-    tc_gemm_kernel<BN, OutT><<<grid, 128, sm, s>>>(ma, mb, M, N, K, C, c_m, c_n, alpha, accumulate, err);
+    tc_gemm_kernel<BN, OutT><<<grid, 128, sm, s>>>(ma, mb, M, N, K, C, c_m, c_n, alpha, accumulate, err,
+                                                   wait_limit(kWaitLimit));
     return launch_status();
 }
 
@@ -430,7 +446,8 @@ static int launch_grouped(const void* desc, int nprob, int tiles, cudaStream_t s
         set_last_cuda_error(attr);
         return VTB_CUDA_ERR;
     }
-    tc_gemm_grouped_kernel<BN><<<tiles, 128, sm, s>>>(reinterpret_cast<const TcGroupProblem*>(desc), nprob);
+    tc_gemm_grouped_kernel<BN><<<tiles, 128, sm, s>>>(reinterpret_cast<const TcGroupProblem*>(desc), nprob,
+                                                       wait_limit(kWaitLimit));
     return launch_status();
 }
 

@@ -23,7 +23,9 @@ squared Cholesky pivots, a lower bound of the condition number that can
 underestimate it by orders of magnitude on badly sampled windows, must stay
 below 1 / (rcond * CHOL_MARGIN); otherwise the eigen-pseudoinverse runs.
 ``"mixed"`` builds M on the tensor cores from split-bf16 operands (fp32
-accumulation), factorises it by float32 Cholesky, and recovers float64
+accumulation), factorises it by float32 Cholesky (this library's tile
+Cholesky, ``mixed_factor="tiles"``, or cuSOLVER's spotrf, ``"cusolver"``),
+and recovers float64
 accuracy with ``mixed_sweeps`` refinement sweeps against the exact float64
 residual Phi^H (q - Phi a), applied through the Kronecker factors without
 forming M in float64.  A mixed solve is accepted when the factorisation
@@ -71,7 +73,7 @@ def coefficient_count(Mx, My, Mt):
 
 class CoeffDecoder(object):
     def __init__(self, Ds, h_norm, Mx, My, Wt, Mt, decPx, decPy, Px1, Py1, rcond=1e-8, solver="auto", refine=0,
-                 device="cuda", mixed_sweeps=2):
+                 device="cuda", mixed_sweeps=2, mixed_factor="tiles"):
         self.Mx, self.My, self.Mt = int(Mx), int(My), int(Mt)
         self.Wt = float(Wt)
         self.W = self.Wt / self.Mt
@@ -111,7 +113,11 @@ class CoeffDecoder(object):
         self.last_solver = None
         self.last_pivots = (0.0, 0.0)
         self.mixed_sweeps = int(mixed_sweeps)
+        if mixed_factor not in ("tiles", "cusolver"):
+            raise ValueError("mixed_factor must be 'tiles' or 'cusolver'")
+        self.mixed_factor = mixed_factor
         self.last_residual = None
+        self.last_status = {}
         if solver == "mixed":
             self._init_mixed(device)
 
@@ -132,6 +138,9 @@ class CoeffDecoder(object):
         self.gres = torch.empty((self.N, self.Kt), dtype=C128, device=device)
         self.r = torch.empty((self.K,), dtype=C128, device=device)
         self.Mr32 = torch.empty((self.K, self.K), dtype=torch.float32, device=device)
+        # the tile Cholesky's diagonal-tile inverses and flag scratch
+        self._cdinv = torch.empty(int(lib().vtb_chol_dinv_floats(self.K)), dtype=torch.float32, device=device)
+        self._cwork = torch.empty(int(lib().vtb_chol_work_bytes(self.K)), dtype=torch.uint8, device=device)
 
     def set_norm(self, h_norm):
         """Per-neuron weights norm (vtem/vtdm.py:634-638, 1/(kappa sigma) for
@@ -224,10 +233,16 @@ class CoeffDecoder(object):
         autotune.gemm_bf16_tuned(dptr(self.L3), 2 * self.npairs, dptr(self.R3), KK, 3 * self.Kp2, dptr(self.C), KK, 1,
                                  0, 1.0, 0, self._stat_ptr(7), s)
         call("vtb_coeff_real_scatter", dptr(self.C), KK, self.Ks, self.Kt, dptr(self.Mr32), K, 0, s)
-        work = self._workspace(2)
-        call("vtb_sym_factor", dptr(self.Mr32), K, K, 2, self.rcond * CHOL_MARGIN, dptr(work), work.numel(),
-             self._stat_ptr(0), self._stat_ptr(1), s)
-        solve = self._mixed_solver(s, work)
+        if self.mixed_factor == "tiles":
+            # float32 tile Cholesky (one cooperative launch) and cluster solves
+            call("vtb_chol_factor", dptr(self.Mr32), K, K, dptr(self._cdinv), dptr(self._cwork),
+                 self._cwork.numel(), self._stat_ptr(0), self._stat_ptr(1), self.rcond * CHOL_MARGIN, s)
+            solve = lambda x: call("vtb_chol_solve", dptr(self.Mr32), K, dptr(self._cdinv), K, dptr(x), s)
+        else:
+            work = self._workspace(2)
+            call("vtb_sym_factor", dptr(self.Mr32), K, K, 2, self.rcond * CHOL_MARGIN, dptr(work), work.numel(),
+                 self._stat_ptr(0), self._stat_ptr(1), s)
+            solve = self._mixed_solver(s, work)
         self.xr.copy_(self.br)
         solve(self.xr)
         for i in range(self.mixed_sweeps):
@@ -243,10 +258,10 @@ class CoeffDecoder(object):
         flag, piv, ratios, tc_err = self._read_stat()
         self.last_pivots = piv
         self.last_ratios = ratios[:min(self.mixed_sweeps, 4)]
-        if tc_err != 0:
-            raise VtbError("vtb_tc_gemm_bf16", tc_err)
-        if flag != 0 or not self._mixed_converged(self.last_ratios):
-            # the pseudoinverse might truncate, or float32 is not enough: float64 path
+        self.last_status = {"factor_flag": flag, "tensor_core_status": tc_err}
+        if tc_err != 0 or flag != 0 or not self._mixed_converged(self.last_ratios):
+            # a tensor-core or factorisation wait ran out, the pseudoinverse
+            # might truncate, or float32 is not enough: float64 path
             self.solver = "auto"
             try:
                 self._solve(s, n)
@@ -307,6 +322,20 @@ class CoeffDecoder(object):
              dptr(bi), dptr(self.norm), self.Mt, self.W, dptr(self.d), self.Ks, dptr(self.a), dptr(gres), dptr(r0), s)
         self.a.copy_(a0)
         return float(r.norm() / r0.norm())
+
+    def gram_error(self):
+        """||M_tc - M||_F / ||M||_F of the last mixed solve: the tensor-core
+        Gram (split-bf16 operands, fp32 accumulation) scattered into its real
+        form again, against the float64 real system built from the same
+        temporal Grams.  Overwrites the float64 system buffers (M, Mr)."""
+        if self.solver != "mixed":
+            raise ValueError("gram_error needs the mixed decoder")
+        s = stream_ptr()
+        K, KK = self.K, self.Kt * self.Kt
+        mtc = torch.empty((K, K), dtype=torch.float32, device=self.M.device)
+        call("vtb_coeff_real_scatter", dptr(self.C), KK, self.Ks, self.Kt, dptr(mtc), K, 0, s)
+        self._build_real(s)
+        return float((mtc.double() - self.Mr).norm() / self.Mr.norm())
 
     def _build_M(self, s):
         call("vtb_coeff_gram", dptr(self.d), self.N, self.Ks, dptr(self.Wn), dptr(self.gn), self.Kt, dptr(self.M),
@@ -459,7 +488,8 @@ class CoeffDecoder(object):
         return host_out
 
 
-def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=0, mixed_sweeps=2):
+def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=0, mixed_sweeps=2, mixed_factor="tiles"):
     """A :class:`CoeffDecoder` on the output of ``vtdm.VTDM_prep``."""
     return CoeffDecoder(prep.Ds, prep.h_norm, prep.Mx, prep.My, Wt, Mt, prep.decPx, prep.decPy, prep.Px1, prep.Py1,
-                        rcond=rcond, solver=solver, refine=refine, mixed_sweeps=mixed_sweeps)
+                        rcond=rcond, solver=solver, refine=refine, mixed_sweeps=mixed_sweeps,
+                        mixed_factor=mixed_factor)
