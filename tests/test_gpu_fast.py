@@ -174,16 +174,17 @@ def test_real_form_matches_hermitian_system():
     call("vtb_coeff_wn_split", dptr(dec.Wn), N, dec.Kt, dptr(dec.R3), s)
     call("vtb_tc_gemm_bf16", dptr(dec.L3), 2 * dec.npairs, dptr(dec.R3), KK, 3 * dec.Kp2, dptr(dec.C), KK, 1, 0, 1.0,
          0, dec._stat_ptr(7), s)
-    call("vtb_coeff_real_scatter", dptr(dec.C), KK, dec.Ks, dec.Kt, dptr(dec.Mr32), K, 0, s)
-    M32 = dec.Mr32.double().cpu().numpy()
+    ld = dec.ld32
+    call("vtb_coeff_real_scatter", dptr(dec.C), KK, dec.Ks, dec.Kt, dptr(dec.Mr32), ld, 0, s)
+    M32 = dec.Mr32[:, :K].double().cpu().numpy()
     assert np.abs(M32 - Mr).max() <= 2e-5 * np.abs(Mr).max()
     # float32 Cholesky + solve, then a float64 Cholesky solve, against numpy
     work = dec._workspace(2)
     dec.stat.zero_()
-    call("vtb_sym_factor", dptr(dec.Mr32), K, K, 2, 1e-12, dptr(work), work.numel(), dec._stat_ptr(0),
+    call("vtb_sym_factor", dptr(dec.Mr32), ld, K, 2, 1e-12, dptr(work), work.numel(), dec._stat_ptr(0),
          dec._stat_ptr(1), s)
     x32 = torch.as_tensor(br, device="cuda")
-    call("vtb_sym_potrs", dptr(dec.Mr32), K, dptr(x32), K, 2, dptr(work), work.numel(), s)
+    call("vtb_sym_potrs", dptr(dec.Mr32), ld, dptr(x32), K, 2, dptr(work), work.numel(), s)
     flag, piv, _, tc_err = dec._read_stat()
     assert flag == 0 and tc_err == 0 and piv[0] > 0
     xr = np.linalg.solve(Mr, br)

@@ -134,7 +134,7 @@ def stage_mixed_pre(d, p, s):
 def stage_mixed_post(d, s):
     """After the Gram GEMM: the float32 real system and xr = br."""
     KK = d.Kt * d.Kt
-    call("vtb_coeff_real_scatter", dptr(d.C), KK, d.Ks, d.Kt, dptr(d.Mr32), d.K, 0, s)
+    call("vtb_coeff_real_scatter", dptr(d.C), KK, d.Ks, d.Kt, dptr(d.Mr32), d.ld32, 0, s)
     d.xr.copy_(d.br)
 
 
@@ -152,7 +152,7 @@ def stage_mixed(d, p, s):
     call("vtb_coeff_wn_split", dptr(d.Wn), d.N, d.Kt, dptr(d.R3), s)
     autotune.gemm_bf16_tuned(dptr(d.L3), 2 * d.npairs, dptr(d.R3), KK, 3 * d.Kp2, dptr(d.C), KK, 1, 0, 1.0, 0,
                              d._stat_ptr(7), s)
-    call("vtb_coeff_real_scatter", dptr(d.C), KK, d.Ks, d.Kt, dptr(d.Mr32), K, 0, s)
+    call("vtb_coeff_real_scatter", dptr(d.C), KK, d.Ks, d.Kt, dptr(d.Mr32), d.ld32, 0, s)
     d.xr.copy_(d.br)
 
 
@@ -205,7 +205,7 @@ class MixedSolvePlan(object):
             B = len(idx)
             nf = int(l.vtb_sym_dinv_floats(K))
             g = {
-                "K": K, "idx": idx,
+                "K": K, "idx": idx, "ld": self.decs[idx[0]].ld32,
                 "mptrs": torch.as_tensor([self.decs[i].Mr32.data_ptr() for i in idx], dtype=torch.int64, device=dev),
                 "dinv": torch.empty((B, nf), dtype=torch.float32, device=dev),
                 "infos": torch.zeros(B, dtype=torch.int32, device=dev),
@@ -216,9 +216,9 @@ class MixedSolvePlan(object):
                 dinv_of[i] = g["dinv"][j]
             self.groups.append(g)
         self.Kmax = max(d.K for d in self.decs)
-        self.desc_x = trsv_descs([(d.Mr32.data_ptr(), dinv_of[i].data_ptr(), d.xr.data_ptr(), d.K, d.K)
+        self.desc_x = trsv_descs([(d.Mr32.data_ptr(), dinv_of[i].data_ptr(), d.xr.data_ptr(), d.ld32, d.K)
                                   for i, d in enumerate(self.decs)], dev)
-        self.desc_r = trsv_descs([(d.Mr32.data_ptr(), dinv_of[i].data_ptr(), d.rr.data_ptr(), d.K, d.K)
+        self.desc_r = trsv_descs([(d.Mr32.data_ptr(), dinv_of[i].data_ptr(), d.rr.data_ptr(), d.ld32, d.K)
                                   for i, d in enumerate(self.decs)], dev)
         self.order = [i for g in self.groups for i in g["idx"]]
 
@@ -240,7 +240,7 @@ class MixedSolvePlan(object):
         s = stream_ptr()
         for g in self.groups:
             rc = self.probs[g["idx"][0]].rcond * fast.CHOL_MARGIN
-            call("vtb_sym_factor_batched", g["mptrs"].data_ptr(), g["K"], g["K"], len(g["idx"]), rc,
+            call("vtb_sym_factor_batched", g["mptrs"].data_ptr(), g["ld"], g["K"], len(g["idx"]), rc,
                  dptr(g["dinv"]), dptr(g["infos"]), dptr(g["flags"]), dptr(g["piv"]), s)
         n = len(self.decs)
         call("vtb_sym_potrs_batched", dptr(self.desc_x), n, self.Kmax, s)

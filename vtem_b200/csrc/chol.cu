@@ -54,7 +54,7 @@ namespace vtb {
 constexpr int kCT = 64;               // tile
 constexpr int kCTE = kCT * kCT;       // tile elements
 constexpr int kCThreads = 256;
-constexpr unsigned kCholSpin = 1u << 22;
+constexpr unsigned kCholSpin = 1u << 20;
 
 __device__ __forceinline__ unsigned c_ld_acquire(const unsigned* p) {
     unsigned v;
@@ -108,10 +108,30 @@ __device__ __forceinline__ void cta_publish(unsigned* f, unsigned v) {
 }
 
 // tile (I, J) of A into shared memory s (column-major, 64 x 64); entries
-// beyond K are the identity's
+// beyond K are the identity's.  A tile inside K whose columns start on 16
+// bytes (ld % 4 == 0, A aligned) is copied asynchronously (cp.async, 16-byte
+// chunks, L2 only): the caller waits with cp.async.wait_group and a CTA
+// barrier before reading it.  Other tiles are loaded synchronously.  Every
+// call commits exactly one cp.async group (empty for a synchronous load), so
+// callers can count groups.
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 __device__ void load_tile(const CholCtx& c, float* s, int I, int J) {
     const int r0 = I * kCT, c0 = J * kCT;
     const bool full = r0 + kCT <= c.K && c0 + kCT <= c.K;
+    if (full && (c.ld & 3) == 0 && ((uintptr_t)c.A & 15) == 0) {
+        for (int e = threadIdx.x; e < kCTE / 4; e += kCThreads) {
+            const int cc = e >> 4, r = (e & 15) * 4;
+            cp_async16(s + cc * kCT + r, c.A + (int64_t)(c0 + cc) * c.ld + r0 + r);
+        }
+        cp_async_commit();
+        return;
+    }
     for (int e = threadIdx.x; e < kCTE; e += kCThreads) {
         const int cc = e >> 6, r = e & 63;
         const int gr = r0 + r, gc = c0 + cc;
@@ -120,6 +140,15 @@ __device__ void load_tile(const CholCtx& c, float* s, int I, int J) {
         else v = gr == gc ? 1.f : 0.f;
         s[e] = v;
     }
+    cp_async_commit();   // an empty group: every call commits exactly one
+}
+
+// thread 0 checks *f >= v once (no wait); every thread learns the answer
+__device__ bool cta_ready(const unsigned* f, unsigned v, int* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) *s_ok = c_ld_acquire(f) >= v;
+    __syncthreads();
+    return *s_ok != 0;
 }
 
 // shared tile s into tile (I, J) of A (rows and columns below K; for a
@@ -331,13 +360,11 @@ __device__ __forceinline__ void task_of(int T, int t, int& I, int& J, int& type)
 }
 
 struct CholSmem {
-    float a[kCTE];
-    float b[kCTE];
-    float x[kCTE];
+    float a[2][kCTE];     // worker: operand L_Ik' (double buffer); diagonal CTA: current and next diagonal tile
+    float b[2][kCTE];     // worker: operand L_Jk' (double buffer); diagonal CTA: L_kk^-1, sub-diagonal tile
+    float x[kCTE];        // worker: the task's tile (staging)
     float tmp[1024];
     int ok;
-    float pmin[8], pmax[8];
-    int bad;
 };
 
 __device__ void worker(const CholCtx& c, CholSmem& sm) {
@@ -352,23 +379,50 @@ __device__ void worker(const CholCtx& c, CholSmem& sm) {
         const int kend = type == 0 ? J : I - 1;
         __syncthreads();
         load_tile(c, sm.x, I, J);
+        cp_async_wait_all();
         __syncthreads();
         float acc[4][4];
         acc_from(acc, sm.x, tr, tc);
+        // operands of update k in buffer k & 1; the next update's operands are
+        // requested before this one's product when their flags are already set
+        if (kend > 0) {
+            if (!cta_wait(c, c.tflag + I * T + 0, 2u, &sm.ok)) return;
+            if (I != J && !cta_wait(c, c.tflag + J * T + 0, 2u, &sm.ok)) return;
+            load_tile(c, sm.a[0], I, 0);
+            if (I != J) load_tile(c, sm.b[0], J, 0);
+        }
         for (int k = 0; k < kend; ++k) {
-            if (!cta_wait(c, c.tflag + I * T + k, 2u, &sm.ok)) return;
-            if (I != J && !cta_wait(c, c.tflag + J * T + k, 2u, &sm.ok)) return;
-            load_tile(c, sm.a, I, k);
-            if (I != J) load_tile(c, sm.b, J, k);
+            const int nb = (k + 1) & 1;
+            bool next = false;
+            if (k + 1 < kend) {
+                next = cta_ready(c.tflag + I * T + k + 1, 2u, &sm.ok) &&
+                       (I == J || cta_ready(c.tflag + J * T + k + 1, 2u, &sm.ok));
+                if (next) {
+                    // the buffers of update k-1 are free: every thread passed the barriers above
+                    load_tile(c, sm.a[nb], I, k + 1);
+                    if (I != J) load_tile(c, sm.b[nb], J, k + 1);
+                }
+            }
+            // this update's groups complete; the next update's (one per operand) may stay in flight
+            if (next && I != J) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+            else if (next) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+            else cp_async_wait_all();
             __syncthreads();
-            sub_ptq(acc, sm.a, I != J ? sm.b : sm.a, tr, tc, 0, kCT);
+            const float* pa = sm.a[k & 1];
+            sub_ptq(acc, pa, I != J ? sm.b[k & 1] : pa, tr, tc, 0, kCT);
+            if (k + 1 < kend && !next) {
+                if (!cta_wait(c, c.tflag + I * T + k + 1, 2u, &sm.ok)) return;
+                if (I != J && !cta_wait(c, c.tflag + J * T + k + 1, 2u, &sm.ok)) return;
+                load_tile(c, sm.a[nb], I, k + 1);
+                if (I != J) load_tile(c, sm.b[nb], J, k + 1);
+            }
         }
         if (type == 0) {
             if (!cta_wait(c, c.tflag + J * T + J, 2u, &sm.ok)) return;
-            for (int e = threadIdx.x; e < kCTE; e += kCThreads) sm.b[e] = __ldcg(c.Dinv + (int64_t)J * kCTE + e);
+            for (int e = threadIdx.x; e < kCTE; e += kCThreads) sm.b[0][e] = __ldcg(c.Dinv + (int64_t)J * kCTE + e);
             acc_to(acc, sm.x, tr, tc);
             __syncthreads();
-            trsm_right(sm.x, sm.b);
+            trsm_right(sm.x, sm.b[0]);
         } else {
             __syncthreads();
             acc_to(acc, sm.x, tr, tc);
@@ -385,32 +439,53 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float pmin = 3.4e38f, pmax = 0.f;
     int bad = 0;
-    load_tile(c, sm.a, 0, 0);
+    int cur = 0;                         // sm.a[cur]: the diagonal tile of this step
+    float* Li = sm.b[0];
+    float* X = sm.b[1];
+    load_tile(c, sm.a[0], 0, 0);
+    cp_async_wait_all();
     __syncthreads();
     for (int k = 0; k < T; ++k) {
-        // sm.a holds A_kk with every update applied
-        potrf_inv64(sm.a, sm.b, sm.tmp, pmin, pmax, bad, c.K - k * kCT);
-        for (int e = threadIdx.x; e < kCTE; e += kCThreads) __stcg(c.Dinv + (int64_t)k * kCTE + e, sm.b[e]);
-        store_tile(c, sm.a, k, k);
+        float* D = sm.a[cur];
+        float* Y = sm.a[cur ^ 1];
+        // the next two tiles, requested now when the workers have published
+        // them, arrive during the factorisation of this one
+        bool hx = false, hy = false;
+        if (k + 1 < T) {
+            hx = k < 1 || cta_ready(c.tflag + (k + 1) * T + k, 1u, &sm.ok);
+            if (hx) load_tile(c, X, k + 1, k);
+            hy = k < 1 || cta_ready(c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok);
+            if (hy) load_tile(c, Y, k + 1, k + 1);
+        }
+        potrf_inv64(D, Li, sm.tmp, pmin, pmax, bad, c.K - k * kCT);
+        for (int e = threadIdx.x; e < kCTE; e += kCThreads) __stcg(c.Dinv + (int64_t)k * kCTE + e, Li[e]);
+        store_tile(c, D, k, k);
         cta_publish(c.tflag + k * T + k, 2u);
         if (k + 1 >= T) break;
         // sub-diagonal tile: the workers applied updates k' < k (none when k = 0)
-        if (k >= 1 && !cta_wait(c, c.tflag + (k + 1) * T + k, 1u, &sm.ok)) return;
-        load_tile(c, sm.x, k + 1, k);
+        if (!hx) {
+            if (!cta_wait(c, c.tflag + (k + 1) * T + k, 1u, &sm.ok)) return;
+            load_tile(c, X, k + 1, k);
+        }
+        cp_async_wait_all();
         __syncthreads();
-        trsm_right(sm.x, sm.b);
-        store_tile(c, sm.x, k + 1, k);
+        trsm_right(X, Li);
+        store_tile(c, X, k + 1, k);
         cta_publish(c.tflag + (k + 1) * T + k, 2u);
         // next diagonal tile: the workers applied updates k' < k; this CTA applies k
-        if (k >= 1 && !cta_wait(c, c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok)) return;
-        load_tile(c, sm.a, k + 1, k + 1);
+        if (!hy) {
+            if (!cta_wait(c, c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok)) return;
+            load_tile(c, Y, k + 1, k + 1);
+        }
+        cp_async_wait_all();
         __syncthreads();
         float acc[4][4];
-        acc_from(acc, sm.a, tr, tc);
-        sub_ptq(acc, sm.x, sm.x, tr, tc, 0, kCT);
+        acc_from(acc, Y, tr, tc);
+        sub_ptq(acc, X, X, tr, tc, 0, kCT);
         __syncthreads();
-        acc_to(acc, sm.a, tr, tc);
+        acc_to(acc, Y, tr, tc);
         __syncthreads();
+        cur ^= 1;
     }
     // pivot test (pivots of warp 0, which ran every 32 x 32 factorisation)
     if (w == 0 && lane == 0) {

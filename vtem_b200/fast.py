@@ -137,7 +137,9 @@ class CoeffDecoder(object):
         self.C = torch.empty((2 * self.npairs, KK), dtype=torch.float32, device=device)
         self.gres = torch.empty((self.N, self.Kt), dtype=C128, device=device)
         self.r = torch.empty((self.K,), dtype=C128, device=device)
-        self.Mr32 = torch.empty((self.K, self.K), dtype=torch.float32, device=device)
+        # float32 real system, rows padded to 16 bytes (the tile Cholesky copies 16-byte chunks)
+        self.ld32 = (self.K + 3) // 4 * 4
+        self.Mr32 = torch.empty((self.K, self.ld32), dtype=torch.float32, device=device)
         # the tile Cholesky's diagonal-tile inverses and flag scratch
         self._cdinv = torch.empty(int(lib().vtb_chol_dinv_floats(self.K)), dtype=torch.float32, device=device)
         self._cwork = torch.empty(int(lib().vtb_chol_work_bytes(self.K)), dtype=torch.uint8, device=device)
@@ -232,15 +234,16 @@ class CoeffDecoder(object):
         call("vtb_coeff_wn_split", dptr(self.Wn), self.N, self.Kt, dptr(self.R3), s)
         autotune.gemm_bf16_tuned(dptr(self.L3), 2 * self.npairs, dptr(self.R3), KK, 3 * self.Kp2, dptr(self.C), KK, 1,
                                  0, 1.0, 0, self._stat_ptr(7), s)
-        call("vtb_coeff_real_scatter", dptr(self.C), KK, self.Ks, self.Kt, dptr(self.Mr32), K, 0, s)
+        ld = self.ld32
+        call("vtb_coeff_real_scatter", dptr(self.C), KK, self.Ks, self.Kt, dptr(self.Mr32), ld, 0, s)
         if self.mixed_factor == "tiles":
             # float32 tile Cholesky (one cooperative launch) and cluster solves
-            call("vtb_chol_factor", dptr(self.Mr32), K, K, dptr(self._cdinv), dptr(self._cwork),
+            call("vtb_chol_factor", dptr(self.Mr32), ld, K, dptr(self._cdinv), dptr(self._cwork),
                  self._cwork.numel(), self._stat_ptr(0), self._stat_ptr(1), self.rcond * CHOL_MARGIN, s)
-            solve = lambda x: call("vtb_chol_solve", dptr(self.Mr32), K, dptr(self._cdinv), K, dptr(x), s)
+            solve = lambda x: call("vtb_chol_solve", dptr(self.Mr32), ld, dptr(self._cdinv), K, dptr(x), s)
         else:
             work = self._workspace(2)
-            call("vtb_sym_factor", dptr(self.Mr32), K, K, 2, self.rcond * CHOL_MARGIN, dptr(work), work.numel(),
+            call("vtb_sym_factor", dptr(self.Mr32), ld, K, 2, self.rcond * CHOL_MARGIN, dptr(work), work.numel(),
                  self._stat_ptr(0), self._stat_ptr(1), s)
             solve = self._mixed_solver(s, work)
         self.xr.copy_(self.br)
@@ -284,9 +287,10 @@ class CoeffDecoder(object):
             self._flag_work = torch.empty(int(lib().vtb_sym_potrs_flags_bytes(K)), dtype=torch.uint8, device=dev)
             self._flags_ok = (K + 63) // 64 <= torch.cuda.get_device_properties(dev).multi_processor_count
         if not self._flags_ok:
-            return lambda x: call("vtb_sym_potrs", dptr(self.Mr32), K, dptr(x), K, 2, dptr(work), work.numel(), s)
-        call("vtb_sym_dinv", dptr(self.Mr32), K, K, dptr(self._dinv), s)
-        return lambda x: call("vtb_sym_potrs_flags", dptr(self.Mr32), K, dptr(self._dinv), K, dptr(x),
+            return lambda x: call("vtb_sym_potrs", dptr(self.Mr32), self.ld32, dptr(x), K, 2, dptr(work), work.numel(),
+                                  s)
+        call("vtb_sym_dinv", dptr(self.Mr32), self.ld32, K, dptr(self._dinv), s)
+        return lambda x: call("vtb_sym_potrs_flags", dptr(self.Mr32), self.ld32, dptr(self._dinv), K, dptr(x),
                               dptr(self._flag_work), self._flag_work.numel(), self._stat_ptr(0), s)
 
     @staticmethod
