@@ -40,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "reconstructed voxels/s at >=40 dB SNR (mixed vs FP64 plain)"
+SYNTH_KERNEL = "harmonics_kernel<double, 17>"
 UNIT = "voxels/s"
 
 
@@ -240,6 +241,15 @@ def run_ours(args, rank, world, local):
                "rel_l2_vs_coeff_f64": float(((u3 - u64).norm() / u64.norm()).item()),
                "residual_rel": dec3.residual_norm(*inputs), "gram_rel_frobenius": gram_err}
     del u3, dec3
+    # the same decoder on cuSOLVER's spotrf/spotrs and the warp-specialised per-frame synthesis, for comparison
+    decv = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="mixed", mixed_sweeps=args.sweeps,
+                          mixed_factor="cusolver", synth="fused")
+    uv = torch.empty_like(u64)
+    alt_ms, alt_synth = time_decoder(decv, inputs, w, uv, flush, args.steps, args.warmup)
+    alt_ms = reduce_max([alt_ms], dev, world)[0]
+    alt = {"ms_per_step": alt_ms / args.steps, "synthesis_ms": sum(alt_synth) / len(alt_synth),
+           "solver": decv.last_solver, "rel_l2_vs_headline": float(((uv - umix).norm() / umix.norm()).item())}
+    del uv, decv
 
     # --- end to end through the public API with host buffers (mixed decoder)
     h_tk1, h_tk2, h_ind = (torch.as_tensor(x).pin_memory() for x in (tk1, tk2, ind))
@@ -283,8 +293,8 @@ def run_ours(args, rank, world, local):
         tot_ms = mix_ms if headline_mixed else f64_ms
         synth_ms = mix_synth if headline_mixed else f64_synth
         value = weak_value(voxels, world, args.steps, tot_ms)
-        # the fused synthesis writes the video and reads only the K coefficients
-        synth_bytes = voxels * 8 + dec64.K * 16
+        # the synthesis writes the video and reads the K coefficients and the per-pixel weights (P x Kt)
+        synth_bytes = voxels * 8 + dec64.K * 16 + 2 * w.Px * w.Py * dec64.Kt * 8
         synth_avg = sum(synth_ms) / len(synth_ms) / 1e3
         peaks = load_peaks()
         achieved = synth_bytes / synth_avg / 1e9
@@ -301,13 +311,16 @@ def run_ours(args, rank, world, local):
                               "parallelism": "clip-parallel replicas" if world > 1 else "single GPU"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps * (launches_mixed(decmix) if headline_mixed else launches_per_step(dec64)),
-            "roofline": {"bound": "hbm", "kernel": "synth_ws_kernel (warp-specialised synthesis)",
+            "roofline": {"bound": "hbm", "kernel": SYNTH_KERNEL + " (rank-%d synthesis; timed with its weights "
+                                                                 "kernel)" % dec64.Kt,
                          "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
-                         "traffic": measured_traffic(voxels), "algorithmic_bytes": synth_bytes,
+                         "traffic": measured_traffic(voxels, SYNTH_KERNEL), "algorithmic_bytes": synth_bytes,
                          "avg_ms": synth_avg * 1e3},
             "roofline_tensor": gram_gemm_roofline(decmix, peaks),
-            "variants_ms_per_step": {"mixed": mix_ms / args.steps, "coeff_f64": f64_ms / args.steps},
+            "variants_ms_per_step": {"mixed": mix_ms / args.steps, "coeff_f64": f64_ms / args.steps,
+                                     "mixed_cusolver_factor_fused_synthesis": alt["ms_per_step"]},
+            "variant_cusolver_fused": alt,
             "mixed_vs_coeff_f64_rel_l2": rel_mix_f64, "mixed_residual_rel": resid,
             "stages_ms": {"coefficients": (tot_ms - sum(synth_ms)) / args.steps,
                           "synthesis": sum(synth_ms) / args.steps, "encode_once": t_enc * 1e3},
@@ -391,11 +404,11 @@ def serve_short(dev, requests=64, rate=200.0, seed=3):
 
 
 def launches_mixed(dec):
-    # own kernels per decode: temporal_gram, rhs, realify_vec, wn split, tc gemm, real scatter (6); factor:
-    # pivot test (1); solve: f64<->f32 conversions (2); per sweep: unrealify, residual (2), realify_vec,
-    # conversions (2), norm ratio, axpy (8); final unrealify (1); synthesis (1, warp-specialised).
-    # cuSOLVER's own kernels (spotrf, strsv) are not counted.
-    return 6 + 1 + 2 + 8 * dec.mixed_sweeps + 1 + 1
+    # this library's kernels per decode: temporal Gram (1); right-hand side, realify, W_n split, tensor-core
+    # Gram, real scatter (5); tile Cholesky (1); initial solve (1); per sweep: unrealify, residual and its
+    # reduction (2), realify, solve, norm ratio, axpy (7); final unrealify (1); synthesis: per-pixel weights
+    # and the harmonics product (2).  With mixed_factor="cusolver", cuSOLVER's kernels are not counted.
+    return 1 + 5 + 1 + 1 + 7 * dec.mixed_sweeps + 1 + 2
 
 
 def run_batch(args, rank, world, local):
@@ -588,13 +601,16 @@ def load_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
-def measured_traffic(voxels):
-    """DRAM bytes per synthesis launch from the committed ncu summary, scaled
-    to this workload's output size (null when no capture is committed)."""
+def measured_traffic(voxels, kernel):
+    """DRAM bytes per synthesis launch from the committed ncu summary of the
+    same kernel, scaled to this workload's output size (null when no capture
+    of that kernel is committed)."""
     p = os.path.join(ROOT, "profiles", "synth_traffic.json")
     try:
         with open(p) as f:
             d = json.load(f)
+        if d.get("kernel") != kernel:
+            return None
         return d["dram_bytes"] * voxels / d["voxels"]
     except Exception:
         return None

@@ -266,6 +266,19 @@ int vtb_herm_solve(double* M, int64_t ld, const double* b, double* a, int K, dou
 int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, double W, double t0,
                          double dt, int Nt, int Px, int Py, int Px1, int Py1, double* A_work, void* u, int out_f32,
                          void* stream);
+/* The same video as a rank-(2Mt+1) product: u[f][p] = sum_k C[f][k] H[p][k]
+ * with C[f] = [1, cos(mWt), sin(mWt) for m = 1..Mt] at t = t0 + f dt and the
+ * per-pixel weights H of vtb_coeff_basis (column 0 = Re B_0, 2m-1 = Re P_m,
+ * 2m = -Im P_m, where B_m(p) = sum_s a[s][m] E_s(p) and P_m = B_m +
+ * conj B_{-m}): 2Mt+1 float64 FMAs per voxel, the coefficients' spatial sum
+ * done once per window instead of once per frame.  H: P x ldh doubles, P =
+ * Px*Py pixels in row-major frame order, ldh >= 2Mt+1 <= 33 (basis) or <= 21
+ * (harmonics).  Replaces reconstruct_Kernel (vtem/dirichlet.py:354-420) on
+ * the coefficient space, as vtb_coeff_synthesize does. */
+int vtb_coeff_basis(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, int Px, int Py, int Px1,
+                    int Py1, double* H, int ldh, void* stream);
+int vtb_synth_harmonics(const double* H, int ldh, int P, int Mt, double W, double t0, double dt, int Nt, void* u,
+                        int out_f32, void* stream);
 
 /* Grouped tensor-core GEMM: nprob independent problems C_p = A_p B_p^T (bf16
  * K-major operands as vtb_tc_gemm_bf16's, float32 row-major C_p with leading
@@ -483,9 +496,10 @@ int vtb_daxpy1(double* y, const double* x, int n, void* stream);
  * until the process exits; frames are processed in chunks that fit, so Nt is
  * unbounded but Ks * 16 bytes must be at most 4 MiB (Ks <= 262144), else
  * VTB_BAD_ARG.  The call allocates nothing (no cudaMalloc/cudaFree, no
- * allocating library).  The first call on a device looks up the array's
- * device address with that device current; make that first call before any
- * stream capture.  All calls share the one array: calls that overlap on the
+ * allocating library).  Every call looks up the array's device address on
+ * the current device (so a device reset leaves no stale address); the first
+ * call on a device also loads the library's module there, so make that first
+ * call before any stream capture.  All calls share the one array: calls that overlap on the
  * GPU (other streams, other threads) race, so serialise them.  Output equals
  * vtb_coeff_synthesize's. */
 int vtb_coeff_synthesize_noalloc(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, double W,

@@ -67,3 +67,46 @@ def test_synthesis_matches_direct_sum(case, dtype):
     tol = 1e-12 if dtype == torch.float64 else 1e-6
     err = np.abs(got - ref).max() / np.abs(ref).max()
     assert err <= tol, err
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_rank_synthesis_matches_direct_sum(case, dtype):
+    """vtb_coeff_basis + vtb_synth_harmonics: the same video as a product of
+    the frames' temporal harmonics and per-pixel weights (non-Hermitian
+    coefficients, so the m / -m pairing is exercised), frame ranges rendered
+    separately as the chunked download does."""
+    Mx, My, Mt, Px, Py, Px1, Py1, Nt = case
+    rng = np.random.default_rng(Mx * 100 + My * 10 + Mt + 7)
+    smap = torch.as_tensor(ellipse_storage_index(Mx, My), device="cuda")
+    Ks, Kt = int(smap.numel()), 2 * Mt + 1
+    a = rng.standard_normal(Ks * Kt) + 1j * rng.standard_normal(Ks * Kt)
+    W, t0, dt = 2 * np.pi * 20 / Mt, 0.013, 1e-3
+    ad = torch.as_tensor(a, dtype=torch.complex128, device="cuda")
+    P = Px * Py
+    H = torch.empty((P, Kt), dtype=torch.float64, device="cuda")
+    lib = _abi.lib()
+    st = lib.vtb_coeff_basis(ad.data_ptr(), smap.data_ptr(), Ks, Mx, My, Mt, Px, Py, Px1, Py1, H.data_ptr(), Kt,
+                             _abi.stream_ptr())
+    assert st == 0, _abi.status_string(st)
+    u = torch.full((Nt, Py, Px), float("nan"), dtype=dtype, device="cuda")
+    half = Nt // 2
+    for f0, f1 in ((0, half), (half, Nt)):
+        st = lib.vtb_synth_harmonics(H.data_ptr(), Kt, P, Mt, W, t0 + f0 * dt, dt, f1 - f0, u[f0:f1].data_ptr(),
+                                     int(dtype == torch.float32), _abi.stream_ptr())
+        assert st == 0, _abi.status_string(st)
+    ref = _direct(a, Mx, My, Mt, W, t0, dt, Nt, Px, Py, Px1, Py1)
+    got = u.double().cpu().numpy()
+    assert np.isfinite(got).all()
+    tol = 1e-12 if dtype == torch.float64 else 1e-6
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    assert err <= tol, err
+
+
+def test_rank_synthesis_rejects_unsupported_orders():
+    lib = _abi.lib()
+    assert lib.vtb_synth_harmonics(None, 0, 10, 0, 1.0, 0.0, 1e-3, 5, None, 0, None) == _abi.VTB_BAD_ARG
+    x = torch.zeros(64, dtype=torch.float64, device="cuda")
+    # Mt = 11: 23 harmonics, beyond the kernel's 21
+    assert lib.vtb_synth_harmonics(x.data_ptr(), 23, 2, 11, 1.0, 0.0, 1e-3, 1, x.data_ptr(), 0,
+                                   _abi.stream_ptr()) == _abi.VTB_BAD_ARG

@@ -77,3 +77,31 @@ def test_noalloc_rejects_oversized_frames():
     st = lib.vtb_coeff_synthesize_noalloc(dummy.data_ptr(), dummy.data_ptr(), 262145, 6, 6, 8, 1.0, 0.0, 1e-4, 10,
                                           64, 64, 64, 64, dummy.data_ptr(), 0, _abi.stream_ptr())
     assert st == _abi.VTB_BAD_ARG
+
+
+def test_noalloc_allocates_no_device_memory():
+    """After a first call (which loads the library's module on the device),
+    further calls leave both the device's free memory and torch's allocator
+    untouched: the scratch is the library's own fixed array."""
+    p = _problem(3, Nt=3001)
+    u = torch.empty((p["Nt"], p["Py"], p["Px"]), dtype=torch.float64, device="cuda")
+    lib = _abi.lib()
+
+    def once():
+        st = lib.vtb_coeff_synthesize_noalloc(p["a"].data_ptr(), p["smap"].data_ptr(), p["Ks"], p["Mx"], p["My"],
+                                              p["Mt"], p["W"], p["t0"], p["dt"], p["Nt"], p["Px"], p["Py"], p["Px1"],
+                                              p["Py1"], u.data_ptr(), 0, _abi.stream_ptr())
+        assert st == 0, _abi.status_string(st)
+
+    once()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    for _ in range(4):
+        once()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_allocated() == alloc0
+    ref = _reference(p, torch.float64)
+    assert ((u - ref).abs().max() / ref.abs().max()).item() <= 1e-13

@@ -55,6 +55,8 @@ SIGNATURES = {
     "vtb_herm_solve_workspace": [I, I, P],
     "vtb_herm_solve": [P, L, P, P, I, D, I, I, P, L, P, P, P],
     "vtb_coeff_synthesize": [P, P, I, I, I, I, D, D, D, I, I, I, I, I, P, P, I, P],
+    "vtb_coeff_basis": [P, P, I, I, I, I, I, I, I, I, P, I, P],
+    "vtb_synth_harmonics": [P, I, I, I, D, D, D, I, P, I, P],
     "vtb_coeff_synthesize_noalloc": [P, P, I, I, I, I, D, D, D, I, I, I, I, I, P, I, P],
     "vtb_split_bf16x3": [P, I, I, I, L, L, D, I, P, P],
     "vtb_tc_gemm_bf16": [P, I, P, I, I, P, L, L, I, D, I, P, P],

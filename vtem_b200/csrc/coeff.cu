@@ -1083,27 +1083,20 @@ __global__ void temporal_expand_chunk_kernel(const double2* __restrict__ a, int 
     }
 }
 
-// Device address of the scratch array, looked up once per device with that
-// device current (in host code the array's name is only a host-side stand-in).
-static double2* noalloc_scratch(int dev, int* status) {
-    static std::mutex mu;
-    static double2* addr[64] = {nullptr};
-    if (dev < 0 || dev >= 64) {
-        *status = VTB_BAD_ARG;
+// Device address of the scratch array on the current device (in host code
+// the array's name is only a host-side stand-in).  Looked up on every call,
+// not cached: after a device reset the module is loaded again and an older
+// address would point at freed memory.  Only the first lookup on a device
+// loads the module; later ones are a table lookup.
+static double2* noalloc_scratch(int* status) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_synth_scratch);
+    if (e != cudaSuccess || !p) {
+        set_last_cuda_error(e);
+        *status = VTB_CUDA_ERR;
         return nullptr;
     }
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_synth_scratch);
-        if (e != cudaSuccess || !p) {
-            set_last_cuda_error(e);
-            *status = VTB_CUDA_ERR;
-            return nullptr;
-        }
-        addr[dev] = reinterpret_cast<double2*>(p);
-    }
-    return addr[dev];
+    return reinterpret_cast<double2*>(p);
 }
 
 }  // namespace vtb
@@ -1117,10 +1110,8 @@ VTB_API int vtb_coeff_synthesize_noalloc(const double* a, const int32_t* smap, i
     VTB_CHECK_ARG((int64_t)Ks <= kNoAllocScratchElems);
     if (Nt == 0) return VTB_OK;
     VTB_CHECK_ARG(a && smap && u);
-    int dev = 0;
-    VTB_CUDA_TRY(cudaGetDevice(&dev));
     int st = VTB_OK;
-    double2* scratch = noalloc_scratch(dev, &st);
+    double2* scratch = noalloc_scratch(&st);
     if (!scratch) return st;
     cudaStream_t s = as_stream(stream);
     const int Kt = 2 * Mt + 1;

@@ -1,0 +1,232 @@
+// Synthesis as a rank-(2Mt+1) product of temporal harmonics and per-pixel
+// weights.
+//
+// The reconstruction of one window is (vtem/dirichlet.py:165-189 rewritten
+// in the coefficient space, as csrc/coeff.cu derives it)
+//     u(t, p) = Re sum_{s, m} a[s][m] phi_s(p) e^{j m W t},
+// phi_s the spatial Dirichlet function of ellipse entry s on the decode grid.
+// Gathering the spatial sum first, B_m(p) = sum_s a[s][m] phi_s(p), and
+// pairing m with -m,
+//     u(t, p) = Re B_0(p) + sum_{m=1}^{Mt} [cos(mWt) Re P_m(p) - sin(mWt) Im P_m(p)],
+//     P_m = B_m + conj(B_{-m})
+// (exact for any coefficients; P_m = 2 B_m for the Hermitian-symmetric ones
+// of a real video).  So the video is U = C H^T with C[t] = [1, cos Wt,
+// sin Wt, ..., cos MtWt, sin MtWt] (Nt x Kt) and H (P x Kt) the per-pixel
+// weights: 2Mt+1 = 17 float64 FMAs per voxel at the GPU configuration,
+// against the 8 bytes the voxel costs in HBM.
+//
+//   basis_kernel: H, one thread per pixel and block per m (Ks complex MACs
+//     per pixel and m; ex/ey of the period grid in shared memory, with the
+//     (-1)^(mx+my) signs and crop offsets of the decode grid).
+//   harmonics_kernel: U.  A block owns 256 * kHPix consecutive pixels and a
+//     range of frames; each thread keeps its kHPix pixels' Kt weights in
+//     registers, the block's frames' harmonics C (by powers of e^{jWt}) sit
+//     in shared memory and are read as broadcasts, and each warp writes 32
+//     consecutive voxels per store (streaming stores, the video exceeds L2).
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace vtb {
+
+constexpr int kHMaxKt = 33;       // Mt <= 16
+constexpr int kHPix = 2;          // pixels per thread
+constexpr int kHThreads = 256;
+constexpr int kHFrames = 64;      // frames per pass of a block
+
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// H[p * ldh + k]: k = 0 -> Re B_0, k = 2m-1 -> Re P_m, k = 2m -> -Im P_m
+__global__ void __launch_bounds__(256) basis_kernel(const double2* __restrict__ a, const int32_t* __restrict__ smap,
+                                                    int Ks, int Mx, int My, int Mt, int Px, int Py, int Px1, int Py1,
+                                                    double* __restrict__ H, int ldh) {
+    extern __shared__ double2 bs[];
+    const int Kx = 2 * Mx + 1, Ky = 2 * My + 1, Kt = 2 * Mt + 1;
+    const int m = blockIdx.y;                       // 0..Mt
+    double2* ex = bs;                               // Kx x Px
+    double2* ey = ex + Kx * Px;                     // Ky x Py
+    double2* am = ey + Ky * Py;                     // Ks: a[s][m]
+    double2* an = am + Ks;                          // Ks: conj a[s][-m]
+    const int xd = (Px1 - Px) / 2, yd = (Py1 - Py) / 2;
+    for (int e = threadIdx.x; e < Kx * Px; e += blockDim.x) {
+        const int c = e / Px, px = e % Px, mx = c - Mx;
+        const int64_t r = ((((int64_t)mx * (px + xd)) % Px1) + Px1) % Px1;
+        double s, co;
+        sincospi(2.0 * r / Px1, &s, &co);
+        const double sg = (mx & 1) ? -1.0 : 1.0;
+        ex[e] = make_double2(sg * co, sg * s);
+    }
+    for (int e = threadIdx.x; e < Ky * Py; e += blockDim.x) {
+        const int rr = e / Py, py = e % Py, my = My - rr;   // storage row rr holds my = My - rr
+        const int64_t r = ((((int64_t)my * (py + yd)) % Py1) + Py1) % Py1;
+        double s, co;
+        sincospi(2.0 * r / Py1, &s, &co);
+        const double sg = (my & 1) ? -1.0 : 1.0;
+        ey[e] = make_double2(sg * co, sg * s);
+    }
+    for (int s = threadIdx.x; s < Ks; s += blockDim.x) {
+        am[s] = a[(int64_t)s * Kt + Mt + m];
+        const double2 v = a[(int64_t)s * Kt + Mt - m];
+        an[s] = make_double2(v.x, -v.y);
+    }
+    __syncthreads();
+    const int P = Px * Py;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        const int px = p % Px, py = p / Px;
+        // P_m(p) = sum_s (a[s][m] phi_s + conj(a[s][-m] phi_s)); for m = 0 only B_0
+        double2 acc = make_double2(0.0, 0.0);
+        for (int s = 0; s < Ks; ++s) {
+            const int g = __ldg(smap + s), rr = g / Kx, c = g - rr * Kx;
+            const double2 phi = c_mul(ey[rr * Py + py], ex[c * Px + px]);
+            const double2 t1 = c_mul(am[s], phi);
+            acc.x += t1.x;
+            acc.y += t1.y;
+            if (m > 0) {
+                const double2 t2 = c_mul(an[s], make_double2(phi.x, -phi.y));
+                acc.x += t2.x;
+                acc.y += t2.y;
+            }
+        }
+        double* h = H + (int64_t)p * ldh;
+        if (m == 0) {
+            h[0] = acc.x;
+        } else {
+            h[2 * m - 1] = acc.x;
+            h[2 * m] = -acc.y;
+        }
+    }
+}
+
+template <typename OutT>
+__device__ __forceinline__ void stream_store(OutT* p, double v) {
+    __stcs(p, (OutT)v);
+}
+
+// U[f][p] = sum_k C[f][k] H[p][k], f = fb..fe of this block, pixels
+// pbase + t + 256 j (j < kHPix)
+template <typename OutT, int KT>
+__global__ void __launch_bounds__(kHThreads) harmonics_kernel(const double* __restrict__ H, int ldh, int P,
+                                                              double W, double t0, double dt, int Nt, int fchunks,
+                                                              OutT* __restrict__ u) {
+    __shared__ __align__(16) double Cs[kHFrames][KT + 1];
+    constexpr int MT = (KT - 1) / 2;
+    const int tid = threadIdx.x;
+    const int ptile = blockIdx.x / fchunks, fc = blockIdx.x % fchunks;
+    const int fb = (int)((int64_t)fc * Nt / fchunks), fe = (int)((int64_t)(fc + 1) * Nt / fchunks);
+    const int pbase = ptile * kHThreads * kHPix;
+    double h[kHPix][KT];
+#pragma unroll
+    for (int j = 0; j < kHPix; ++j) {
+        const int p = pbase + tid + kHThreads * j;
+#pragma unroll
+        for (int k = 0; k < KT; ++k) h[j][k] = p < P ? __ldg(H + (int64_t)p * ldh + k) : 0.0;
+    }
+    for (int f0 = fb; f0 < fe; f0 += kHFrames) {
+        const int nf = min(kHFrames, fe - f0);
+        __syncthreads();
+        if (tid < nf) {
+            double sn, co;
+            sincos(W * (t0 + (f0 + tid) * dt), &sn, &co);
+            const double2 base = make_double2(co, sn);
+            double2 pw = make_double2(1.0, 0.0);
+            Cs[tid][0] = 1.0;
+#pragma unroll
+            for (int m = 1; m <= MT; ++m) {
+                pw = c_mul(pw, base);
+                Cs[tid][2 * m - 1] = pw.x;
+                Cs[tid][2 * m] = pw.y;
+            }
+        }
+        __syncthreads();
+        for (int q = 0; q < nf; ++q) {
+            double acc[kHPix];
+#pragma unroll
+            for (int j = 0; j < kHPix; ++j) acc[j] = 0.0;
+#pragma unroll
+            for (int k = 0; k < KT; ++k) {
+                const double cv = Cs[q][k];
+#pragma unroll
+                for (int j = 0; j < kHPix; ++j) acc[j] = fma(cv, h[j][k], acc[j]);
+            }
+            OutT* uf = u + (int64_t)(f0 + q) * P;
+#pragma unroll
+            for (int j = 0; j < kHPix; ++j) {
+                const int p = pbase + tid + kHThreads * j;
+                if (p < P) stream_store(uf + p, acc[j]);
+            }
+        }
+    }
+}
+
+template <typename OutT, int KT>
+static void launch_harm(const double* H, int ldh, int P, double W, double t0, double dt, int Nt, OutT* u,
+                        cudaStream_t s) {
+    const int ptiles = ceil_div(P, kHThreads * kHPix);
+    // about four blocks per SM in all, at least one frame block per pass
+    int fchunks = std::max(1, std::min(ceil_div(Nt, 8), ceil_div(4 * kNumSMs, ptiles)));
+    harmonics_kernel<OutT, KT><<<ptiles * fchunks, kHThreads, 0, s>>>(H, ldh, P, W, t0, dt, Nt, fchunks, u);
+}
+
+template <typename OutT>
+static int dispatch_harm(int Kt, const double* H, int ldh, int P, double W, double t0, double dt, int Nt, OutT* u,
+                         cudaStream_t s) {
+    switch (Kt) {
+        case 3: launch_harm<OutT, 3>(H, ldh, P, W, t0, dt, Nt, u, s); break;
+        case 5: launch_harm<OutT, 5>(H, ldh, P, W, t0, dt, Nt, u, s); break;
+        case 7: launch_harm<OutT, 7>(H, ldh, P, W, t0, dt, Nt, u, s); break;
+        case 9: launch_harm<OutT, 9>(H, ldh, P, W, t0, dt, Nt, u, s); break;
+        case 11: launch_harm<OutT, 11>(H, ldh, P, W, t0, dt, Nt, u, s); break;
+        case 13: launch_harm<OutT, 13>(H, ldh, P, W, t0, dt, Nt, u, s); break;
+        case 15: launch_harm<OutT, 15>(H, ldh, P, W, t0, dt, Nt, u, s); break;
+        case 17: launch_harm<OutT, 17>(H, ldh, P, W, t0, dt, Nt, u, s); break;
+        case 19: launch_harm<OutT, 19>(H, ldh, P, W, t0, dt, Nt, u, s); break;
+        case 21: launch_harm<OutT, 21>(H, ldh, P, W, t0, dt, Nt, u, s); break;
+        default: return VTB_BAD_ARG;
+    }
+    return launch_status();
+}
+
+}  // namespace vtb
+
+using namespace vtb;
+
+// Per-pixel weights H (P x ldh doubles, P = Px*Py pixels in row-major frame
+// order, ldh >= 2Mt+1) of the coefficients a[s][m] (Ks x (2Mt+1) complex,
+// the decoder's layout; smap: storage index of each ellipse entry s in the
+// (2My+1) x (2Mx+1) grid): column 0 = Re B_0, 2m-1 = Re P_m, 2m = -Im P_m.
+// Replaces the spatial half of reconstruct_Kernel (vtem/dirichlet.py:354-420)
+// on the coefficient space: B_m(p) = sum_s a[s][m] phi_s(p), phi_s the
+// decode-grid Dirichlet functions of compute_dirich_space_fft
+// (vtem/vrf.py:437-499, period Px1 x Py1 cropped to Px x Py).
+VTB_API int vtb_coeff_basis(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, int Px, int Py,
+                            int Px1, int Py1, double* H, int ldh, void* stream) {
+    VTB_CHECK_ARG(Ks > 0 && Mx >= 0 && My >= 0 && Mt >= 0 && Px > 0 && Py > 0 && Px1 >= Px && Py1 >= Py);
+    VTB_CHECK_ARG(a && smap && H && ldh >= 2 * Mt + 1 && 2 * Mt + 1 <= kHMaxKt);
+    const int Kx = 2 * Mx + 1, Ky = 2 * My + 1;
+    const size_t sm = (size_t)(Kx * Px + Ky * Py + 2 * Ks) * sizeof(double2);
+    VTB_CHECK_ARG(sm <= 200 * 1024);
+    if (sm > 48 * 1024)
+        VTB_CUDA_TRY(cudaFuncSetAttribute(basis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int P = Px * Py;
+    dim3 grid(ceil_div(P, 256), Mt + 1);
+    basis_kernel<<<grid, 256, sm, as_stream(stream)>>>(reinterpret_cast<const double2*>(a), smap, Ks, Mx, My, Mt, Px,
+                                                      Py, Px1, Py1, H, ldh);
+    return launch_status();
+}
+
+// Video u[f][p] (Nt frames of P pixels, float64 or float32 when out_f32) at
+// t = t0 + f dt from the weights H of vtb_coeff_basis: u[f][p] = H[p][0] +
+// sum_{m=1}^{Mt} (cos(mWt) H[p][2m-1] + sin(mWt) H[p][2m]).  2Mt+1 in
+// {3, 5, ..., 21}.  Replaces the temporal half of reconstruct_Kernel
+// (vtem/dirichlet.py:354-420) as the coefficient space writes it.
+VTB_API int vtb_synth_harmonics(const double* H, int ldh, int P, int Mt, double W, double t0, double dt, int Nt,
+                                void* u, int out_f32, void* stream) {
+    VTB_CHECK_ARG(P > 0 && Mt >= 1 && Nt >= 0 && ldh >= 2 * Mt + 1);
+    if (Nt == 0) return VTB_OK;
+    VTB_CHECK_ARG(H && u);
+    cudaStream_t s = as_stream(stream);
+    if (out_f32) return dispatch_harm<float>(2 * Mt + 1, H, ldh, P, W, t0, dt, Nt, reinterpret_cast<float*>(u), s);
+    return dispatch_harm<double>(2 * Mt + 1, H, ldh, P, W, t0, dt, Nt, reinterpret_cast<double*>(u), s);
+}

@@ -73,7 +73,7 @@ def coefficient_count(Mx, My, Mt):
 
 class CoeffDecoder(object):
     def __init__(self, Ds, h_norm, Mx, My, Wt, Mt, decPx, decPy, Px1, Py1, rcond=1e-8, solver="auto", refine=0,
-                 device="cuda", mixed_sweeps=2, mixed_factor="tiles"):
+                 device="cuda", mixed_sweeps=2, mixed_factor="tiles", synth="harmonics"):
         self.Mx, self.My, self.Mt = int(Mx), int(My), int(Mt)
         self.Wt = float(Wt)
         self.W = self.Wt / self.Mt
@@ -116,6 +116,9 @@ class CoeffDecoder(object):
         if mixed_factor not in ("tiles", "cusolver"):
             raise ValueError("mixed_factor must be 'tiles' or 'cusolver'")
         self.mixed_factor = mixed_factor
+        if synth not in ("harmonics", "fused"):
+            raise ValueError("synth must be 'harmonics' or 'fused'")
+        self.synth = synth
         self.last_residual = None
         self.last_status = {}
         if solver == "mixed":
@@ -431,12 +434,30 @@ class CoeffDecoder(object):
         self.last_solver = "rnn"
         return self.a, float(dt_alpha)
 
+    def _harmonic_weights(self, a, s):
+        """Per-pixel weights H (P x Kt) of the coefficients a for the
+        rank-Kt synthesis (vtb_coeff_basis), or None when the fused kernel
+        serves this decoder (synth="fused", or Kt beyond 21)."""
+        if self.synth != "harmonics" or self.Kt > 21:
+            return None
+        P = self.decPx * self.decPy
+        if getattr(self, "_H", None) is None or self._H.shape[0] != P:
+            self._H = torch.empty((P, self.Kt), dtype=F64, device=self.M.device)
+        call("vtb_coeff_basis", dptr(a), dptr(self.smap), self.Ks, self.Mx, self.My, self.Mt, self.decPx, self.decPy,
+             self.Px1, self.Py1, dptr(self._H), self.Kt, s)
+        return self._H
+
     def synthesize(self, a, T, dt, t0=0.0, out=None, out_dtype=F64):
         """Video (Nt, decPy, decPx) at t = t0 + arange(0, T, dt)."""
         Nt = len(np.arange(0, T, dt))
         dev = self.M.device
         if out is None:
             out = torch.empty((Nt, self.decPy, self.decPx), dtype=out_dtype, device=dev)
+        H = self._harmonic_weights(a, stream_ptr())
+        if H is not None:
+            call("vtb_synth_harmonics", dptr(H), self.Kt, self.decPx * self.decPy, self.Mt, self.W, float(t0),
+                 float(dt), Nt, dptr(out), int(out.dtype == torch.float32), stream_ptr())
+            return out
         # the fused kernel (2My+1 <= 13) needs no expansion buffer
         A = None if 2 * self.My + 1 <= 13 else torch.empty((Nt, self.Ks), dtype=C128, device=dev)
         call("vtb_coeff_synthesize", dptr(a), dptr(self.smap), self.Ks, self.Mx, self.My, self.Mt, self.W, float(t0),
@@ -474,13 +495,18 @@ class CoeffDecoder(object):
         main = torch.cuda.current_stream(dev)
         cs = self._copy_stream
         bounds = np.linspace(0, Nt, max(1, int(chunks)) + 1).astype(np.int64)
-        A = None if 2 * self.My + 1 <= 13 else torch.empty((Nt, self.Ks), dtype=C128, device=dev)
+        H = self._harmonic_weights(a, main.cuda_stream)
+        A = None if H is not None or 2 * self.My + 1 <= 13 else torch.empty((Nt, self.Ks), dtype=C128, device=dev)
         for f0, f1 in zip(bounds[:-1], bounds[1:]):
             if f1 <= f0:
                 continue
-            call("vtb_coeff_synthesize", dptr(a), dptr(self.smap), self.Ks, self.Mx, self.My, self.Mt, self.W,
-                 float(f0 * dt), float(dt), int(f1 - f0), self.decPx, self.decPy, self.Px1, self.Py1, dptr(A),
-                 dptr(out[f0:f1]), int(f32), main.cuda_stream)
+            if H is not None:
+                call("vtb_synth_harmonics", dptr(H), self.Kt, self.decPx * self.decPy, self.Mt, self.W,
+                     float(f0 * dt), float(dt), int(f1 - f0), dptr(out[f0:f1]), int(f32), main.cuda_stream)
+            else:
+                call("vtb_coeff_synthesize", dptr(a), dptr(self.smap), self.Ks, self.Mx, self.My, self.Mt, self.W,
+                     float(f0 * dt), float(dt), int(f1 - f0), self.decPx, self.decPy, self.Px1, self.Py1, dptr(A),
+                     dptr(out[f0:f1]), int(f32), main.cuda_stream)
             ev = torch.cuda.Event()
             ev.record(main)
             cs.wait_event(ev)
@@ -492,8 +518,9 @@ class CoeffDecoder(object):
         return host_out
 
 
-def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=0, mixed_sweeps=2, mixed_factor="tiles"):
+def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=0, mixed_sweeps=2, mixed_factor="tiles",
+              synth="harmonics"):
     """A :class:`CoeffDecoder` on the output of ``vtdm.VTDM_prep``."""
     return CoeffDecoder(prep.Ds, prep.h_norm, prep.Mx, prep.My, Wt, Mt, prep.decPx, prep.decPy, prep.Px1, prep.Py1,
                         rcond=rcond, solver=solver, refine=refine, mixed_sweeps=mixed_sweeps,
-                        mixed_factor=mixed_factor)
+                        mixed_factor=mixed_factor, synth=synth)
