@@ -7,19 +7,22 @@
 // 64 x 64 tiles (T = ceil(K/64) tile rows) as a data-flow graph:
 //
 //   CTA 0 ("diagonal") walks the critical path, step k = 0..T-1:
-//     POTRF + inverse of the diagonal tile (k,k) (two 32 x 32 register
-//     factorisations in one warp each, the rest as small shared-memory
-//     products), publishes L_kk^-1 (Dinv) and L_kk;
-//     TRSM of the sub-diagonal tile L_{k+1,k} = A_{k+1,k} L_kk^-T;
+//     POTRF of the diagonal tile (k,k) with all its warps (8-column blocks:
+//     warp 0 factorises each 8 x 8 diagonal block while the others apply the
+//     previous block's update), publishes L_kk;
+//     TRSM of the sub-diagonal tile L_{k+1,k} = A_{k+1,k} L_kk^-T by blocked
+//     substitution;
 //     SYRK of the next diagonal tile A_{k+1,k+1} -= L_{k+1,k} L_{k+1,k}^T,
 //     which it keeps in shared memory for step k+1.
 //   CTAs 1.. ("workers") run every other piece: for tile (I,J) the updates
 //     A_IJ -= sum_{k'} L_Ik' L_Jk'^T (the 4 x 4 register block of each thread
 //     stays in registers across all of them), then for I >= J+2 the TRSM
-//     with the published Dinv_J.  Diagonal and sub-diagonal tiles receive
+//     with the published L_JJ.  Diagonal and sub-diagonal tiles receive
 //     from the workers all updates but the last (the diagonal CTA applies
 //     that one), so the diagonal CTA never waits on a round trip through a
 //     worker for data its own previous step produced.
+//   A second, small kernel then forms the inverses of the diagonal tiles
+//   (Dinv, for the triangular solves), one block per tile.
 //
 // Worker tasks are ordered by the step whose outputs they need ("group" g:
 // the TRSM tiles (I, g) for I >= g+2, then the sub-diagonal (g+2, g+1), then
@@ -40,7 +43,7 @@
 // on it), so K needs no padding.  The factor L is written over the lower
 // triangle of A (column-major, element (i, j) at j*ld + i, as spotrf leaves
 // it); Dinv receives T tiles of 64 x 64 (column-major, tile k at k*4096)
-// holding L_kk^-1 for the triangular solves.  A failed pivot (<= 0 or not a
+// holding L_kk^-1 for the triangular solves (second kernel, same stream).  A failed pivot (<= 0 or not a
 // number) or a spread of the squared pivots max/min >= 1/rcond sets the
 // status word to 1 or 2, as vtb_sym_factor's pivot test does.
 #include <cooperative_groups.h>
@@ -192,146 +195,154 @@ __device__ __forceinline__ void acc_to(const float (&acc)[4][4], float* s, int t
         for (int j = 0; j < 4; ++j) s[(4 * tc + j) * kCT + 4 * tr + i] = acc[i][j];
 }
 
-// X = X L^-T in place: X (column-major 64 x 64, shared), Li = L^-1 (lower,
-// column-major: Li[t*64 + c] = (L^-1)[c][t], zero for t > c)
-__device__ void trsm_right(float* X, const float* Li) {
-    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
-    float acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-    // acc = -(sum_t X[r][t] Li[c][t]) with t <= c
-    sub_ptq(acc, X, Li, tr, tc, 0, 4 * tc + 4);
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = -acc[i][j];
-    acc_to(acc, X, tr, tc);
-    __syncthreads();
-}
-
-// ---------------------------------------------------------------- 32 x 32 in one warp
-// Lane r holds row r of the symmetric positive definite block in a[0..31]
-// (a[c] = A[r][c]).  On return a[c] = L[r][c] and x[c] = (L^-1)[r][c] for
-// c <= r (zero above the diagonal).  Right-looking: at step j the pivot is
-// broadcast from lane j, column j of L is formed, the trailing columns and
-// the rows of the inverse (Gauss-Jordan on [L | I]) are updated.  pmin/pmax
-// track the pivots (squared diagonal of L) of the first nvalid rows (the
-// rest are the identity's padding beyond K); a pivot <= 0 or NaN sets bad.
-__device__ __forceinline__ void potrf_inv32(float (&a)[32], float (&x)[32], float& pmin, float& pmax, int& bad,
+// ---------------------------------------------------------------- 64 x 64 POTRF
+// The 8 x 8 diagonal block at (8bb, 8bb) of the column-major 64 x 64 tile S,
+// in one warp: lane i < 8 holds row i; right-looking, the pivot broadcast by
+// shuffle.  Writes L (zeros above the diagonal) and rinv[8bb + j] = 1/L_jj.
+// Pivots of rows beyond K (nvalid: rows of the tile below K) do not enter
+// pmin/pmax; a pivot <= 0 or NaN sets bad.
+__device__ __forceinline__ void potrf8_warp(float* S, float* rinv, int bb, float& pmin, float& pmax, int& bad,
                                             int nvalid) {
-    const int r = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, i = lane & 7, o = 8 * bb;
+    float a[8];
 #pragma unroll
-    for (int c = 0; c < 32; ++c) x[c] = c == r ? 1.f : 0.f;
+    for (int j = 0; j < 8; ++j) a[j] = S[(o + j) * kCT + o + i];
+    float rs_own = 0.f;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
+    for (int j = 0; j < 8; ++j) {
         float p = __shfl_sync(0xffffffffu, a[j], j);
         if (!(p > 0.f)) {
             bad = 1;
             p = 1.f;
         }
-        if (j < nvalid) {
+        if (o + j < nvalid) {
             pmin = fminf(pmin, p);
             pmax = fmaxf(pmax, p);
         }
         const float rs = rsqrtf(p);
-        const float l = r >= j ? a[j] * rs : 0.f;
+        if (i == j) rs_own = rs;
+        const float l = i >= j ? a[j] * rs : 0.f;
         a[j] = l;
 #pragma unroll
-        for (int c = j + 1; c < 32; ++c) a[c] = fmaf(-l, __shfl_sync(0xffffffffu, l, c), a[c]);
-#pragma unroll
-        for (int c = 0; c <= j; ++c) {
-            const float xj = __shfl_sync(0xffffffffu, x[c] * rs, j);
-            x[c] = r == j ? xj : fmaf(-l, xj, x[c]);
-        }
+        for (int c = j + 1; c < 8; ++c) a[c] = fmaf(-l, __shfl_sync(0xffffffffu, l, c), a[c]);
     }
+    if (lane < 8) {
 #pragma unroll
-    for (int c = 0; c < 32; ++c)
-        if (c > r) a[c] = 0.f;
-}
-
-// The 32 x 32 block at (o, o) of the column-major 64 x 64 tile S: lane r
-// reads row r; writes L into S and L^-1 into the same block of Li.
-__device__ __forceinline__ void warp_block_potrf(float* S, float* Li, int o, float& pmin, float& pmax, int& bad,
-                                                 int nvalid) {
-    const int r = threadIdx.x & 31;
-    float a[32], x[32];
-#pragma unroll
-    for (int c = 0; c < 32; ++c) a[c] = S[(o + c) * kCT + o + r];
-    potrf_inv32(a, x, pmin, pmax, bad, nvalid - o);
-#pragma unroll
-    for (int c = 0; c < 32; ++c) {
-        S[(o + c) * kCT + o + r] = a[c];
-        Li[(o + c) * kCT + o + r] = c <= r ? x[c] : 0.f;
+        for (int j = 0; j < 8; ++j) S[(o + j) * kCT + o + i] = j <= i ? a[j] : 0.f;
+        rinv[o + i] = rs_own;
     }
 }
 
-// POTRF + inverse of the 64 x 64 tile S (column-major, symmetric positive
-// definite) by 2 x 2 blocks of 32: S <- L (upper triangle zeroed), Li <-
-// L^-1 (lower, upper zero).  Tmp: 32 x 32 scratch (column-major, ld 32).
-// nvalid: rows of the tile below K.
-__device__ void potrf_inv64(float* S, float* Li, float* Tmp, float& pmin, float& pmax, int& bad, int nvalid) {
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // (1) L11, L11^-1
-    if (w == 0) warp_block_potrf(S, Li, 0, pmin, pmax, bad, nvalid);
+// row r of column block bb: x <- x L_bb^-T by substitution (x the row's 8
+// entries in that block, already updated by every earlier block)
+__device__ __forceinline__ void subst_row8(float* X, const float* L, const float* rinv, int bb, int r) {
+    const int o = 8 * bb;
+    float x[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) x[c] = X[(o + c) * kCT + r];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        float v = x[c];
+#pragma unroll
+        for (int t = 0; t < c; ++t) v = fmaf(-x[t], L[(o + t) * kCT + o + c], v);
+        x[c] = v * rinv[o + c];
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) X[(o + c) * kCT + r] = x[c];
+}
+
+// Cholesky of the symmetric positive definite 64 x 64 tile S (column-major,
+// lower triangle read) in place: S <- L (zeros above the diagonal), rinv <-
+// 1/diag(L).  Blocks of 8 columns, all 8 warps: after the column block bb is
+// solved (one thread per row below it), warp 0 updates and factorises the
+// next diagonal block while warps 1-7 apply the rank-8 update to the rest of
+// the trailing triangle in 4 x 4 register patches.  The chain is 8 block
+// factorisations and 8 row substitutions; nothing else waits on them.
+__device__ void potrf64(float* S, float* rinv, float& pmin, float& pmax, int& bad, int nvalid) {
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    if (w == 0) potrf8_warp(S, rinv, 0, pmin, pmax, bad, nvalid);
     __syncthreads();
-    // (2) L21 = A21 L11^-T: lane = row r (32 + r), warp w: columns 4w..4w+3
-    {
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int t = 0; t < 32; ++t) {
-            const float av = S[t * kCT + 32 + lane];
+    for (int bb = 0; bb < 8; ++bb) {
+        const int o = 8 * bb, c0 = o + 8;
+        if (tid >= c0 && tid < kCT) subst_row8(S, S, rinv, bb, tid);
+        __syncthreads();
+        if (bb == 7) break;
+        if (w == 0) {
+            // next diagonal block: S[c0+i][c0+j] -= sum_t L[c0+i][o+t] L[c0+j][o+t], two entries per lane
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc[j] = fmaf(av, Li[t * kCT + 4 * w + j], acc[j]);   // Li[c][t], t <= c
+            for (int h = 0; h < 2; ++h) {
+                const int e = lane + 32 * h, i = e & 7, j = e >> 3;
+                float v = S[(c0 + j) * kCT + c0 + i];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) v = fmaf(-S[(o + t) * kCT + c0 + i], S[(o + t) * kCT + c0 + j], v);
+                S[(c0 + j) * kCT + c0 + i] = v;
+            }
+            __syncwarp();
+            potrf8_warp(S, rinv, bb + 1, pmin, pmax, bad, nvalid);
+        } else {
+            // 4 x 4 patches of rows and columns [c0, 64), lower triangle, without the next diagonal block
+            const int m = (kCT - c0) / 4;
+            for (int q = tid - 32; q < m * m; q += kCThreads - 32) {
+                const int pr = q / m, pc = q % m;
+                if (pr < pc || (pr < 2 && pc < 2)) continue;
+                const int r0 = c0 + 4 * pr, cc0 = c0 + 4 * pc;
+                float acc[4][4];
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) {
+                    const float4 v = *reinterpret_cast<const float4*>(S + (cc0 + jj) * kCT + r0);
+                    acc[0][jj] = v.x;
+                    acc[1][jj] = v.y;
+                    acc[2][jj] = v.z;
+                    acc[3][jj] = v.w;
+                }
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    const float4 pv = *reinterpret_cast<const float4*>(S + (o + t) * kCT + r0);
+                    const float4 qv = *reinterpret_cast<const float4*>(S + (o + t) * kCT + cc0);
+                    const float pa[4] = {pv.x, pv.y, pv.z, pv.w};
+                    const float qa[4] = {qv.x, qv.y, qv.z, qv.w};
+#pragma unroll
+                    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+                        for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fmaf(-pa[ii], qa[jj], acc[ii][jj]);
+                }
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj)
+                    *reinterpret_cast<float4*>(S + (cc0 + jj) * kCT + r0) =
+                        make_float4(acc[0][jj], acc[1][jj], acc[2][jj], acc[3][jj]);
+            }
         }
         __syncthreads();
-#pragma unroll
-        for (int j = 0; j < 4; ++j) S[(4 * w + j) * kCT + 32 + lane] = acc[j];
     }
-    __syncthreads();
-    // (3) A22 -= L21 L21^T
-    {
-        float acc[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[j] = S[(32 + 4 * w + j) * kCT + 32 + lane];
-        for (int t = 0; t < 32; ++t) {
-            const float lv = S[t * kCT + 32 + lane];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[j] = fmaf(-lv, S[t * kCT + 32 + 4 * w + j], acc[j]);
+}
+
+// X = X L^-T in place (X column-major 64 x 64, L the column-major lower
+// factor tile, rinv = 1/diag(L)): for each block of 8 columns, the product
+// with the solved blocks (two entries per thread), then the substitution
+// inside the block (one thread per row).
+__device__ void trsm_subst(float* X, const float* L, const float* rinv) {
+    const int tid = threadIdx.x, r = tid & 63, cp = tid >> 6;   // cp: column pair 0..3
+    for (int bb = 0; bb < 8; ++bb) {
+        const int o = 8 * bb;
+        if (bb > 0) {
+            float v0 = X[(o + 2 * cp) * kCT + r], v1 = X[(o + 2 * cp + 1) * kCT + r];
+            for (int t = 0; t < o; ++t) {
+                const float xt = X[t * kCT + r];
+                v0 = fmaf(-xt, L[t * kCT + o + 2 * cp], v0);
+                v1 = fmaf(-xt, L[t * kCT + o + 2 * cp + 1], v1);
+            }
+            X[(o + 2 * cp) * kCT + r] = v0;
+            X[(o + 2 * cp + 1) * kCT + r] = v1;
+            __syncthreads();
         }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) S[(32 + 4 * w + j) * kCT + 32 + lane] = acc[j];
+        if (tid < kCT) subst_row8(X, L, rinv, bb, tid);
+        __syncthreads();
     }
-    __syncthreads();
-    // (4) warp 0: L22, L22^-1; warps 1..7 meanwhile: Tmp = L21 L11^-1
-    if (w == 0) {
-        warp_block_potrf(S, Li, 32, pmin, pmax, bad, nvalid);
-    } else {
-        for (int e = threadIdx.x - 32; e < 1024; e += kCThreads - 32) {
-            const int rr = e & 31, cc = e >> 5;
-            float s = 0.f;
-            for (int t = cc; t < 32; ++t) s = fmaf(S[t * kCT + 32 + rr], Li[cc * kCT + t], s);   // L21[rr][t] Li11[t][cc]
-            Tmp[cc * 32 + rr] = s;
-        }
-    }
-    __syncthreads();
-    // (5) Li21 = -L22^-1 Tmp: lane = row r, warp w: columns 4w..4w+3
-    {
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int t = 0; t <= lane; ++t) {
-            const float lv = Li[(32 + t) * kCT + 32 + lane];   // Li22[lane][t]
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[j] = fmaf(-lv, Tmp[(4 * w + j) * 32 + t], acc[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            Li[(4 * w + j) * kCT + 32 + lane] = acc[j];
-            S[(32 + 4 * w + j) * kCT + lane] = 0.f;            // upper block of L
-            Li[(32 + 4 * w + j) * kCT + lane] = 0.f;           // upper block of L^-1
-        }
-    }
-    __syncthreads();
+}
+
+// rinv = 1/diag(L) of a factor tile held in shared memory
+__device__ __forceinline__ void diag_recip(const float* L, float* rinv) {
+    if (threadIdx.x < kCT) rinv[threadIdx.x] = 1.0f / L[threadIdx.x * kCT + threadIdx.x];
 }
 
 // ---------------------------------------------------------------- worker tasks
@@ -361,9 +372,9 @@ __device__ __forceinline__ void task_of(int T, int t, int& I, int& J, int& type)
 
 struct CholSmem {
     float a[2][kCTE];     // worker: operand L_Ik' (double buffer); diagonal CTA: current and next diagonal tile
-    float b[2][kCTE];     // worker: operand L_Jk' (double buffer); diagonal CTA: L_kk^-1, sub-diagonal tile
+    float b[2][kCTE];     // worker: operand L_Jk' (double buffer), then L_JJ; diagonal CTA: sub-diagonal tile
     float x[kCTE];        // worker: the task's tile (staging)
-    float tmp[1024];
+    float rinv[kCT];
     int ok;
 };
 
@@ -417,15 +428,18 @@ __device__ void worker(const CholCtx& c, CholSmem& sm) {
                 if (I != J) load_tile(c, sm.b[nb], J, k + 1);
             }
         }
+        __syncthreads();
+        acc_to(acc, sm.x, tr, tc);
         if (type == 0) {
+            // TRSM with the published diagonal factor L_JJ
             if (!cta_wait(c, c.tflag + J * T + J, 2u, &sm.ok)) return;
-            for (int e = threadIdx.x; e < kCTE; e += kCThreads) sm.b[0][e] = __ldcg(c.Dinv + (int64_t)J * kCTE + e);
-            acc_to(acc, sm.x, tr, tc);
+            load_tile(c, sm.b[0], J, J);
+            cp_async_wait_all();
             __syncthreads();
-            trsm_right(sm.x, sm.b[0]);
+            diag_recip(sm.b[0], sm.rinv);
+            __syncthreads();
+            trsm_subst(sm.x, sm.b[0], sm.rinv);
         } else {
-            __syncthreads();
-            acc_to(acc, sm.x, tr, tc);
             __syncthreads();
         }
         store_tile(c, sm.x, I, J);
@@ -440,7 +454,6 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
     float pmin = 3.4e38f, pmax = 0.f;
     int bad = 0;
     int cur = 0;                         // sm.a[cur]: the diagonal tile of this step
-    float* Li = sm.b[0];
     float* X = sm.b[1];
     load_tile(c, sm.a[0], 0, 0);
     cp_async_wait_all();
@@ -457,8 +470,7 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
             hy = k < 1 || cta_ready(c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok);
             if (hy) load_tile(c, Y, k + 1, k + 1);
         }
-        potrf_inv64(D, Li, sm.tmp, pmin, pmax, bad, c.K - k * kCT);
-        for (int e = threadIdx.x; e < kCTE; e += kCThreads) __stcg(c.Dinv + (int64_t)k * kCTE + e, Li[e]);
+        potrf64(D, sm.rinv, pmin, pmax, bad, c.K - k * kCT);
         store_tile(c, D, k, k);
         cta_publish(c.tflag + k * T + k, 2u);
         if (k + 1 >= T) break;
@@ -469,7 +481,7 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
         }
         cp_async_wait_all();
         __syncthreads();
-        trsm_right(X, Li);
+        trsm_subst(X, D, sm.rinv);
         store_tile(c, X, k + 1, k);
         cta_publish(c.tflag + (k + 1) * T + k, 2u);
         // next diagonal tile: the workers applied updates k' < k; this CTA applies k
@@ -487,7 +499,7 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
         __syncthreads();
         cur ^= 1;
     }
-    // pivot test (pivots of warp 0, which ran every 32 x 32 factorisation)
+    // pivot test (pivots of warp 0, which ran every 8 x 8 factorisation)
     if (w == 0 && lane == 0) {
         int f = 0;
         if (bad) f = 1;
@@ -505,6 +517,31 @@ __global__ void __launch_bounds__(kCThreads, 1) chol_tiles_kernel(CholCtx c) {
     CholSmem& sm = *reinterpret_cast<CholSmem*>(chol_smem);
     if (blockIdx.x == 0) diagonal(c, sm);
     else worker(c, sm);
+}
+
+// Dinv tile k = L_kk^-1 (column-major) for the triangular solves, one block
+// per diagonal tile: X = I, X <- X L^-T = L^-T, stored transposed.
+__global__ void __launch_bounds__(kCThreads) chol_dinv_kernel(const float* __restrict__ A, int64_t ld, int K,
+                                                             float* __restrict__ Dinv) {
+    __shared__ __align__(16) float L[kCTE];
+    __shared__ __align__(16) float X[kCTE];
+    __shared__ float rinv[kCT];
+    const int k = blockIdx.x;
+    for (int e = threadIdx.x; e < kCTE; e += kCThreads) {
+        const int cc = e >> 6, r = e & 63;
+        const int gr = k * kCT + r, gc = k * kCT + cc;
+        L[e] = (gr < K && gc < K) ? (r >= cc ? A[(int64_t)gc * ld + gr] : 0.f) : (gr == gc ? 1.f : 0.f);
+        X[e] = r == cc ? 1.f : 0.f;
+    }
+    __syncthreads();
+    diag_recip(L, rinv);
+    __syncthreads();
+    trsm_subst(X, L, rinv);
+    // X = L^-T: (L^-1)[r][c] = X[c][r]; Dinv column-major: Dinv[c*64 + r] = (L^-1)[r][c] = X[r*64 + c]
+    for (int e = threadIdx.x; e < kCTE; e += kCThreads) {
+        const int cc = e >> 6, r = e & 63;
+        Dinv[(int64_t)k * kCTE + e] = X[r * kCT + cc];
+    }
 }
 
 static int chol_tiles(int K) { return (K + kCT - 1) / kCT; }
@@ -567,6 +604,7 @@ VTB_API int vtb_chol_factor(float* A, int64_t ld, int K, float* Dinv, void* work
     c.limit = wait_limit(kCholSpin);
     void* args[] = {(void*)&c};
     VTB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)chol_tiles_kernel, dim3(grid), dim3(kCThreads), args, sm, s));
+    chol_dinv_kernel<<<T, kCThreads, 0, s>>>(A, ld, K, Dinv);
     return launch_status();
 }
 
@@ -583,20 +621,22 @@ namespace vtb {
 //   every CTA: s_k += L_{k,j-1} y_{j-1} for its rows k > j
 // (s_k: the running sum of the already solved blocks), so the chain between
 // two barriers is one 64 x 64 product and one application of Dinv.  The
-// backward pass is the mirror image with L^T.  Each step's tiles are loaded
-// into registers BEFORE the barrier that releases the previous block, so
-// their L2 latency overlaps the wait.  No spin-wait: the cluster barrier is
-// the hardware's, and every CTA takes every step.
+// backward pass is the mirror image with L^T.  Four threads share a row
+// (forward) or a column (backward: columns of the column-major factor are
+// contiguous) of a tile, 16 elements each, and combine with warp shuffles.
+// Every tile a step needs is loaded into registers BEFORE the barrier that
+// releases the previous block, so its L2 latency overlaps the wait.  No
+// spin-wait: the cluster barrier is the hardware's, and every CTA takes every
+// step.
 constexpr int kSThreads = 256;
 constexpr int kSPre = 4;          // own tiles per step loaded ahead in registers
 constexpr int kSMaxT = 160;       // K <= 10240
+constexpr int kSMaxOwn = 24;      // ceil(T / C) for C >= 8
 
 struct SolveSmem {
     float v[kSMaxT * kCT];        // y (forward), then x (backward)
-    float s[24][kCT];             // running sums of own rows (ceil(T/C) <= 24)
-    float red[kSPre + 1][4][kCT]; // partial products of one step
-    float t[kCT + 1];             // the owner's block before Dinv
-    float tile[kCT * (kCT + 1)];  // padded tile for the transposed products
+    float s[kSMaxOwn][kCT];       // running sums of own rows
+    float t[kCT];                 // the owner's block before Dinv
 };
 
 __device__ __forceinline__ void dsm_store(float* local_addr, unsigned rank, float v) {
@@ -610,15 +650,44 @@ __device__ __forceinline__ void cluster_sync_all() {
     asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
-// this thread's 16 elements of tile (I, J): rows r = t & 63, columns 16q..16q+15
-__device__ __forceinline__ void load16(const float* A, int64_t ld, int K, int I, int J, float (&v)[16]) {
-    const int r = threadIdx.x & 63, q = threadIdx.x >> 6;
+// row mapping: thread (r = tid >> 2, part = tid & 3) holds M[r][16 part + i]
+// of tile (I, J) of the column-major A; entries beyond K are the identity's
+__device__ __forceinline__ void load_rows(const float* A, int64_t ld, int K, int I, int J, float (&v)[16]) {
+    const int r = threadIdx.x >> 2, part = threadIdx.x & 3;
     const int gr = I * kCT + r;
 #pragma unroll
-    for (int c = 0; c < 16; ++c) {
-        const int gc = J * kCT + 16 * q + c;
-        v[c] = (gr < K && gc < K) ? __ldcg(A + (int64_t)gc * ld + gr) : (gr == gc ? 1.f : 0.f);
+    for (int i = 0; i < 16; ++i) {
+        const int gc = J * kCT + 16 * part + i;
+        v[i] = (gr < K && gc < K) ? __ldcg(A + (int64_t)gc * ld + gr) : (gr == gc ? 1.f : 0.f);
     }
+}
+
+// column mapping: thread (c = tid >> 2, part = tid & 3) holds M[16 part + i][c]
+__device__ __forceinline__ void load_cols(const float* A, int64_t ld, int K, int I, int J, float (&v)[16]) {
+    const int c = threadIdx.x >> 2, part = threadIdx.x & 3;
+    const int gc = J * kCT + c;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int gr = I * kCT + 16 * part + i;
+        v[i] = (gr < K && gc < K) ? __ldcg(A + (int64_t)gc * ld + gr) : (gr == gc ? 1.f : 0.f);
+    }
+}
+
+// sum over the four threads of a row / column, every one of them gets it
+__device__ __forceinline__ float quad_sum(float x) {
+    x += __shfl_xor_sync(0xffffffffu, x, 1);
+    x += __shfl_xor_sync(0xffffffffu, x, 2);
+    return x;
+}
+
+__device__ __forceinline__ float dot16(const float (&w)[16], const float* v) {
+    float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+    for (int i = 0; i < 16; i += 2) {
+        a0 = fmaf(w[i], v[i], a0);
+        a1 = fmaf(w[i + 1], v[i + 1], a1);
+    }
+    return a0 + a1;
 }
 
 __global__ void __launch_bounds__(kSThreads, 1) chol_solve_kernel(const float* __restrict__ A, int64_t ld,
@@ -629,161 +698,106 @@ __global__ void __launch_bounds__(kSThreads, 1) chol_solve_kernel(const float* _
     unsigned C, q;
     asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(C));
     asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(q));
-    const int tid = threadIdx.x, r = tid & 63, qq = tid >> 6;
+    const int tid = threadIdx.x, rc = tid >> 2, part = tid & 3;
     const int nown = ((int)T - (int)q + (int)C - 1) / (int)C;   // own rows k = q + C m
-    for (int e = tid; e < 24 * kCT; e += kSThreads) (&sm.s[0][0])[e] = 0.f;
+    for (int e = tid; e < kSMaxOwn * kCT; e += kSThreads) (&sm.s[0][0])[e] = 0.f;
     cluster_sync_all();
 
     // ------------------------------------------------ forward: L y = b
     for (int j = 0; j < T; ++j) {
         const bool own = (j % (int)C) == (int)q;
-        // own rows k > j with a term from block j-1, in order: the first kSPre
-        // tiles ahead in registers
         float crit[16], dv[16], pre[kSPre][16];
-        if (own && j >= 1) load16(A, ld, K, j, j - 1, crit);
         if (own) {
+            if (j >= 1) load_rows(A, ld, K, j, j - 1, crit);
 #pragma unroll
-            for (int c = 0; c < 16; ++c) dv[c] = __ldcg(Dinv + (int64_t)j * kCTE + (16 * qq + c) * kCT + r);
+            for (int i = 0; i < 16; ++i) dv[i] = __ldcg(Dinv + (int64_t)j * kCTE + (16 * part + i) * kCT + rc);
         }
-        const int m0 = (j + 1 - (int)q + (int)C - 1) / (int)C;    // first own row index k = q + C m > j
-        const int mstart = m0 < 0 ? 0 : m0;
+        const int mstart = (j + 1 - (int)q + (int)C - 1) / (int)C;  // first own row k = q + C m > j
+        if (j >= 1) {
+#pragma unroll
+            for (int p = 0; p < kSPre; ++p)
+                if (mstart + p < nown) load_rows(A, ld, K, (int)q + (int)C * (mstart + p), j - 1, pre[p]);
+        }
+        cluster_sync_all();                     // y_{j-1} is in every CTA's v
+        const float* yp = sm.v + (j - 1) * kCT + 16 * part;
+        if (own) {
+            const int mj = (j - (int)q) / (int)C;
+            float lv = j >= 1 ? quad_sum(dot16(crit, yp)) : 0.f;
+            if (part == 0) {
+                const int gr = j * kCT + rc;
+                const float b = gr < K ? (float)x[gr] : 0.f;
+                sm.t[rc] = b - sm.s[mj][rc] - lv;
+            }
+            __syncthreads();
+            const float yj = quad_sum(dot16(dv, sm.t + 16 * part));
+            if (part == 0)
+                for (unsigned d = 0; d < C; ++d) dsm_store(sm.v + j * kCT + rc, d, yj);
+        }
+        // non-critical: s_k += L_{k,j-1} y_{j-1} for own k > j (row rc owned by its part-0 thread)
         if (j >= 1) {
 #pragma unroll
             for (int p = 0; p < kSPre; ++p) {
-                const int m = mstart + p;
-                if (m < nown) load16(A, ld, K, (int)q + (int)C * m, j - 1, pre[p]);
-            }
-        }
-        cluster_sync_all();                     // y_{j-1} is in every CTA's v
-        const float* yp = sm.v + (j - 1) * kCT;
-        if (own) {
-            float acc = 0.f;
-            if (j >= 1) {
-#pragma unroll
-                for (int c = 0; c < 16; ++c) acc = fmaf(crit[c], yp[16 * qq + c], acc);
-            }
-            sm.red[kSPre][qq][r] = acc;
-            __syncthreads();
-            if (tid < kCT) {
-                const int gr = j * kCT + tid;
-                const float b = gr < K ? (float)x[gr] : 0.f;
-                const int mj = (j - (int)q) / (int)C;
-                sm.t[tid] = b - sm.s[mj][tid] - ((sm.red[kSPre][0][tid] + sm.red[kSPre][1][tid]) +
-                                                 (sm.red[kSPre][2][tid] + sm.red[kSPre][3][tid]));
-            }
-            __syncthreads();
-            float y = 0.f;
-#pragma unroll
-            for (int c = 0; c < 16; ++c) y = fmaf(dv[c], sm.t[16 * qq + c], y);   // Dinv[r][16qq+c]
-            sm.red[kSPre][qq][r] = y;
-            __syncthreads();
-            if (tid < kCT) {
-                const float yj = (sm.red[kSPre][0][tid] + sm.red[kSPre][1][tid]) +
-                                 (sm.red[kSPre][2][tid] + sm.red[kSPre][3][tid]);
-                for (unsigned d = 0; d < C; ++d) dsm_store(sm.v + j * kCT + tid, d, yj);
-            }
-        }
-        // non-critical: s_k += L_{k,j-1} y_{j-1} for own k > j
-        if (j >= 1) {
-            for (int m = mstart; m < nown; m += kSPre) {
-#pragma unroll
-                for (int p = 0; p < kSPre; ++p) {
-                    const int mm = m + p;
-                    float acc = 0.f;
-                    if (mm < nown) {
-                        float w[16];
-                        if (m == mstart) {
-#pragma unroll
-                            for (int c = 0; c < 16; ++c) w[c] = pre[p][c];
-                        } else {
-                            load16(A, ld, K, (int)q + (int)C * mm, j - 1, w);
-                        }
-#pragma unroll
-                        for (int c = 0; c < 16; ++c) acc = fmaf(w[c], yp[16 * qq + c], acc);
-                    }
-                    sm.red[p][qq][r] = acc;
+                if (mstart + p < nown) {
+                    const float lv = quad_sum(dot16(pre[p], yp));
+                    if (part == 0) sm.s[mstart + p][rc] += lv;
                 }
-                __syncthreads();
-                if (tid < kCT) {
-                    for (int p = 0; p < kSPre && m + p < nown; ++p)
-                        sm.s[m + p][tid] += (sm.red[p][0][tid] + sm.red[p][1][tid]) +
-                                            (sm.red[p][2][tid] + sm.red[p][3][tid]);
-                }
-                __syncthreads();
+            }
+            for (int m = mstart + kSPre; m < nown; ++m) {
+                float w[16];
+                load_rows(A, ld, K, (int)q + (int)C * m, j - 1, w);
+                const float lv = quad_sum(dot16(w, yp));
+                if (part == 0) sm.s[m][rc] += lv;
             }
         }
     }
     cluster_sync_all();                         // y complete everywhere
-    for (int e = tid; e < 24 * kCT; e += kSThreads) (&sm.s[0][0])[e] = 0.f;
+    for (int e = tid; e < kSMaxOwn * kCT; e += kSThreads) (&sm.s[0][0])[e] = 0.f;
     __syncthreads();
 
     // ------------------------------------------------ backward: L^T x = y
     // step j = T-1 .. 0: owner(j): x_j = Dinv_j^T (y_j - s_j - L_{j+1,j}^T x_{j+1});
-    // every CTA: s_k += L_{j+1,k}^T x_{j+1} for own k < j
+    // every CTA: s_k += L_{j+1,k}^T x_{j+1} for own k < j (column rc owned by its part-0 thread)
     for (int j = T - 1; j >= 0; --j) {
         const bool own = (j % (int)C) == (int)q;
-        float crit[16], dv[16];
-        if (own && j + 1 < T) load16(A, ld, K, j + 1, j, crit);
+        const bool has = j + 1 < T;
+        float crit[16], dv[16], pre[kSPre][16];
         if (own) {
+            if (has) load_cols(A, ld, K, j + 1, j, crit);
 #pragma unroll
-            for (int c = 0; c < 16; ++c) dv[c] = __ldcg(Dinv + (int64_t)j * kCTE + (16 * qq + c) * kCT + r);
+            for (int i = 0; i < 16; ++i) dv[i] = __ldcg(Dinv + (int64_t)j * kCTE + rc * kCT + 16 * part + i);
+        }
+        // own rows k < j, in increasing k: k = q + C m for m < mend
+        const int mend = (j - (int)q + (int)C - 1) / (int)C;         // own k < j  <=>  m < mend
+        const int mlim = mend < 0 ? 0 : (mend < nown ? mend : nown);
+        if (has) {
+#pragma unroll
+            for (int p = 0; p < kSPre; ++p)
+                if (p < mlim) load_cols(A, ld, K, j + 1, (int)q + (int)C * p, pre[p]);
         }
         cluster_sync_all();                     // x_{j+1} is in every CTA's v
-        const float* xp = sm.v + (j + 1) * kCT;
+        const float* xp = sm.v + (j + 1) * kCT + 16 * part;
         if (own) {
             const int mj = (j - (int)q) / (int)C;
-            // tile L_{j+1,j} (rows of block j+1, columns of block j) transposed: padded shared copy
-            if (j + 1 < T) {
-#pragma unroll
-                for (int c = 0; c < 16; ++c) sm.tile[(16 * qq + c) * (kCT + 1) + r] = crit[c];
-            }
+            const float lv = has ? quad_sum(dot16(crit, xp)) : 0.f;
+            if (part == 0) sm.t[rc] = sm.v[j * kCT + rc] - sm.s[mj][rc] - lv;
             __syncthreads();
-            // thread (r, qq): column c = r of the tile, rows 16qq..16qq+15
-            float acc = 0.f;
-            if (j + 1 < T) {
-#pragma unroll
-                for (int k = 0; k < 16; ++k) acc = fmaf(sm.tile[r * (kCT + 1) + 16 * qq + k], xp[16 * qq + k], acc);
-            }
-            sm.red[kSPre][qq][r] = acc;
-            __syncthreads();
-            if (tid < kCT)
-                sm.t[tid] = sm.v[j * kCT + tid] - sm.s[mj][tid] -
-                            ((sm.red[kSPre][0][tid] + sm.red[kSPre][1][tid]) +
-                             (sm.red[kSPre][2][tid] + sm.red[kSPre][3][tid]));
-            // Dinv_j^T: x[c] = sum_{r >= c} Dinv[r][c] t[r]
-#pragma unroll
-            for (int c = 0; c < 16; ++c) sm.tile[(16 * qq + c) * (kCT + 1) + r] = dv[c];
-            __syncthreads();
-            float xv = 0.f;
-#pragma unroll
-            for (int k = 0; k < 16; ++k) xv = fmaf(sm.tile[r * (kCT + 1) + 16 * qq + k], sm.t[16 * qq + k], xv);
-            sm.red[kSPre][qq][r] = xv;
-            __syncthreads();
-            if (tid < kCT) {
-                const float xj = (sm.red[kSPre][0][tid] + sm.red[kSPre][1][tid]) +
-                                 (sm.red[kSPre][2][tid] + sm.red[kSPre][3][tid]);
-                for (unsigned d = 0; d < C; ++d) dsm_store(sm.v + j * kCT + tid, d, xj);
-            }
+            const float xj = quad_sum(dot16(dv, sm.t + 16 * part));
+            if (part == 0)
+                for (unsigned d = 0; d < C; ++d) dsm_store(sm.v + j * kCT + rc, d, xj);
         }
-        // non-critical: s_k += L_{j+1,k}^T x_{j+1} for own k < j
-        if (j + 1 < T) {
-            for (int m = 0; m < nown; ++m) {
-                const int k = (int)q + (int)C * m;
-                if (k >= j) break;
+        if (has) {
+#pragma unroll
+            for (int p = 0; p < kSPre; ++p) {
+                if (p < mlim) {
+                    const float lv = quad_sum(dot16(pre[p], xp));
+                    if (part == 0) sm.s[p][rc] += lv;
+                }
+            }
+            for (int m = kSPre; m < mlim; ++m) {
                 float w[16];
-                load16(A, ld, K, j + 1, k, w);
-                __syncthreads();
-#pragma unroll
-                for (int c = 0; c < 16; ++c) sm.tile[(16 * qq + c) * (kCT + 1) + r] = w[c];
-                __syncthreads();
-                float acc = 0.f;
-#pragma unroll
-                for (int kk = 0; kk < 16; ++kk)
-                    acc = fmaf(sm.tile[r * (kCT + 1) + 16 * qq + kk], xp[16 * qq + kk], acc);
-                sm.red[0][qq][r] = acc;
-                __syncthreads();
-                if (tid < kCT)
-                    sm.s[m][tid] += (sm.red[0][0][tid] + sm.red[0][1][tid]) + (sm.red[0][2][tid] + sm.red[0][3][tid]);
+                load_cols(A, ld, K, j + 1, (int)q + (int)C * m, w);
+                const float lv = quad_sum(dot16(w, xp));
+                if (part == 0) sm.s[m][rc] += lv;
             }
         }
     }

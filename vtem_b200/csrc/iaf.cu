@@ -14,7 +14,8 @@
 // reference kernel.
 //
 // Work split: one warp per neuron.  For each chunk of 32 steps the lanes load
-// 32 samples (coalesced when the input is neuron-major), form y = (x+b)/kappa
+// 32 samples (coalesced when the input is neuron-major; the loads run
+// kIafAhead chunks ahead of their use, in registers), form y = (x+b)/kappa
 // and the trapezoid area of their own step in parallel, and stage them in
 // shared memory; the warp then walks the 32 steps in order (the membrane
 // recursion is a strict sequential FP64 chain that no reordering may touch).
@@ -54,6 +55,7 @@ struct IafArgs {
 };
 
 constexpr int kIafWarps = 4;
+constexpr int kIafAhead = 8;   // chunks of 32 samples prefetched ahead
 
 template <bool RT>
 __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
@@ -97,9 +99,17 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
 
     double ycur = (ld(lane) + bia) / kap;
     double ynext = (ld(32 + lane) + bia) / kap;
+    // input samples kIafAhead chunks beyond ynext, in flight while the chain
+    // walks the current chunk (one chunk takes far less than an HBM round trip)
+    double ahead[kIafAhead];
+#pragma unroll
+    for (int i = 0; i < kIafAhead; ++i) ahead[i] = ld(64 + 32 * i + lane);
 
     for (int t0 = 0; t0 < steps && !stop; t0 += 32) {
-        const double xpre = ld(t0 + 64 + lane);
+        const double xpre = ahead[0];
+#pragma unroll
+        for (int i = 0; i + 1 < kIafAhead; ++i) ahead[i] = ahead[i + 1];
+        ahead[kIafAhead - 1] = ld(t0 + 64 + 32 * kIafAhead + lane);
         double y2l = __shfl_down_sync(full, ycur, 1);
         const double yn0 = __shfl_sync(full, ynext, 0);
         if (lane == 31) y2l = yn0;
