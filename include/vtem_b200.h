@@ -429,6 +429,22 @@ int vtb_chol_factor(float* A, int64_t ld, int K, float* Dinv, void* work, int64_
  * cluster size in use (0 before the first call). */
 int vtb_chol_solve(const float* L, int64_t ld, const float* Dinv, int K, double* x, void* stream);
 int vtb_chol_solve_cluster(void);
+/* vtb_chol_factor that also forms X = L^-1 in the same launch: the CTAs
+ * that are not busy with the factorisation compute X_ii = L_ii^-1 and
+ * X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj as soon as their operands are
+ * published.  Linv (vtb_chol_inverse_floats(K) floats, 16-byte aligned)
+ * receives the tiles (i, j), i >= j, of X, each 64 x 64 row-major, tile
+ * (i, j) at offset (i(i+1)/2 + j) * 4096.  Dinv is filled as by
+ * vtb_chol_factor. */
+int64_t vtb_chol_inverse_floats(int K);
+int vtb_chol_factor_inverse(float* A, int64_t ld, int K, float* Dinv, float* Linv, void* work, int64_t work_bytes,
+                            int32_t* status, double* pivots, double rcond, void* stream);
+/* x = L^-T L^-1 x (x float64 in and out, float32 arithmetic) with the packed
+ * inverse of vtb_chol_factor_inverse: two triangular matrix-vector products
+ * (y = X b, then x = X^T y), every tile read once; no step waits on another
+ * CTA.  y_work: ceil(K/64)*64 floats.  K <= 10240.  Replaces spotrs in the
+ * solve of linalg.py:591-631. */
+int vtb_chol_solve_inverse(const float* Linv, int K, double* x, float* y_work, void* stream);
 /* Pseudoinverse solve x = V diag(1/w if |w| > rcond*max|w| else 0) V^T b of
  * a float64 symmetric M (destroyed), the rule of solve_eq_sym
  * (vtem/utils/linalg.py:591-631, sq_Kernel :791-833).  kept (device) the

@@ -1,7 +1,9 @@
 """The float32 tile Cholesky and cluster solves of the mixed decoder, and the
 bounded device waits of every kernel that waits on another CTA (GPU).
 
-vtb_chol_factor / vtb_chol_solve replace cuSOLVER's spotrf / spotrs in the
+vtb_chol_factor / vtb_chol_solve (and vtb_chol_factor_inverse /
+vtb_chol_solve_inverse, which form L^-1 during the factorisation and solve
+by two matrix-vector products) replace cuSOLVER's spotrf / spotrs in the
 solve of the coefficient system (vtem/utils/linalg.py:591-631 as called at
 vtem/vtdm.py:645-648): checked against float64 NumPy on random symmetric
 positive definite matrices of sizes that exercise one tile, ragged tiles and
@@ -69,6 +71,73 @@ def test_chol_factor_and_solve_match_float64(K):
         xref = np.linalg.solve(A, b)
         assert np.linalg.norm(x.cpu().numpy() - xref) / np.linalg.norm(xref) < 1e-3
     assert lib().vtb_chol_solve_cluster() in (8, 16)
+
+
+def factor_inverse(A32, rcond=1e-12):
+    K = A32.shape[0]
+    dinv = torch.empty(int(lib().vtb_chol_dinv_floats(K)), dtype=torch.float32, device="cuda")
+    linv = torch.full((int(lib().vtb_chol_inverse_floats(K)),), float("nan"), dtype=torch.float32, device="cuda")
+    work = torch.empty(int(lib().vtb_chol_work_bytes(K)), dtype=torch.uint8, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    piv = torch.zeros(2, dtype=torch.float64, device="cuda")
+    call("vtb_chol_factor_inverse", dptr(A32), K, K, dptr(dinv), dptr(linv), dptr(work), work.numel(), dptr(status),
+         dptr(piv), rcond, stream_ptr())
+    torch.cuda.synchronize()
+    return dinv, linv, int(status.item()), piv.cpu().numpy()
+
+
+def unpack_inverse(linv, K):
+    T = (K + 63) // 64
+    X = np.zeros((64 * T, 64 * T))
+    t = linv.cpu().numpy().astype(np.float64).reshape(-1, 64, 64)
+    for i in range(T):
+        for j in range(i + 1):
+            X[64 * i:64 * i + 64, 64 * j:64 * j + 64] = t[i * (i + 1) // 2 + j]              # row-major tiles
+    return X[:K, :K]
+
+
+@pytest.mark.parametrize("K", [40, 100, 130, 257, 1921])
+def test_chol_factor_inverse_and_product_solve(K):
+    """The factor formed with L^-1 equals the plain factor bit for bit (same
+    task arithmetic), L^-1 matches float64 NumPy, and the two-product solve
+    x = L^-T L^-1 b solves A x = b."""
+    A = spd(K, 1e3, K + 1)
+    A32 = torch.as_tensor(A.astype(np.float32), device="cuda").contiguous()
+    A32b = A32.clone()
+    dinv0, status0, piv0 = factor(A32b)
+    dinv, linv, status, piv = factor_inverse(A32)
+    assert status == 0 and status0 == 0
+    assert torch.equal(torch.tril(A32.T), torch.tril(A32b.T))
+    assert np.array_equal(piv, piv0)
+    assert torch.equal(dinv, dinv0)
+    Lref = np.linalg.cholesky(A)
+    X = unpack_inverse(linv, K)
+    Xref = np.linalg.inv(Lref)
+    assert np.isfinite(X).all()
+    assert np.linalg.norm(X - Xref) / np.linalg.norm(Xref) < 1e-3
+    assert np.abs(np.triu(X, 1)).max() == 0.0                                     # exact zeros above
+    y = torch.empty(((K + 63) // 64) * 64, dtype=torch.float32, device="cuda")
+    rng = np.random.default_rng(2)
+    for _ in range(2):
+        b = rng.standard_normal(K)
+        x = torch.as_tensor(b, device="cuda")
+        call("vtb_chol_solve_inverse", dptr(linv), K, dptr(x), dptr(y), stream_ptr())
+        torch.cuda.synchronize()
+        xref = np.linalg.solve(A, b)
+        assert np.linalg.norm(x.cpu().numpy() - xref) / np.linalg.norm(xref) < 1e-3
+
+
+def test_chol_factor_inverse_wait_limit_runs_out():
+    K = 1921
+    A = spd(K, 1e2, 8)
+    A32 = torch.as_tensor(A.astype(np.float32), device="cuda").contiguous()
+    with _abi.wait_limit(1):
+        _, _, status, _ = factor_inverse(A32.clone())
+    assert status == 3
+    _, linv, status, _ = factor_inverse(A32)
+    assert status == 0
+    X = unpack_inverse(linv, K)
+    assert np.linalg.norm(X @ np.linalg.cholesky(A) - np.eye(K)) / np.sqrt(K) < 1e-4
 
 
 def test_chol_flags_bad_pivot_and_spread():
@@ -191,7 +260,7 @@ def _small_window():
 def test_mixed_decoder_tiles_match_cusolver_and_f64():
     w, prep, (tk1, tk2, ind, kap, dl, bia, sig) = _small_window()
     ref = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="eig").decode(tk1, tk2, ind, kap, dl, bia, w.T, w.dt)
-    for factor_kind in ("tiles", "cusolver"):
+    for factor_kind in ("inverse", "tiles", "cusolver"):
         dec = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="mixed", mixed_sweeps=3,
                              mixed_factor=factor_kind)
         u = dec.decode(tk1, tk2, ind, kap, dl, bia, w.T, w.dt)

@@ -57,6 +57,7 @@ namespace vtb {
 constexpr int kCT = 64;               // tile
 constexpr int kCTE = kCT * kCT;       // tile elements
 constexpr int kCThreads = 256;
+constexpr int kSMaxT = 160;           // solves: K <= 10240
 constexpr unsigned kCholSpin = 1u << 20;
 
 __device__ __forceinline__ unsigned c_ld_acquire(const unsigned* p) {
@@ -80,6 +81,8 @@ struct CholCtx {
     double* piv;         // caller's [min, max] squared pivots (may be null)
     double rcond;
     unsigned limit;
+    float* Xinv;         // packed L^-1 tiles, row-major (null: no inverse)
+    unsigned* xflag;     // T*T flags: 1 = X tile (i, j) published
 };
 
 // thread 0 waits until *f >= v; every thread learns the outcome
@@ -197,20 +200,26 @@ __device__ __forceinline__ void acc_to(const float (&acc)[4][4], float* s, int t
 
 // ---------------------------------------------------------------- 64 x 64 POTRF
 // The 8 x 8 diagonal block at (8bb, 8bb) of the column-major 64 x 64 tile S,
-// in one warp: lane i < 8 holds row i; right-looking, the pivot broadcast by
-// shuffle.  Writes L (zeros above the diagonal) and rinv[8bb + j] = 1/L_jj.
-// Pivots of rows beyond K (nvalid: rows of the tile below K) do not enter
-// pmin/pmax; a pivot <= 0 or NaN sets bad.
+// in one warp: every lane loads the whole block (broadcast reads) and
+// factorises it in its registers, so no step waits on another lane; lanes
+// 0..7 then write column `lane` of L (zeros above the diagonal) and lane 0
+// writes rinv[8bb + j] = 1/L_jj.  Pivots of rows beyond K (nvalid: rows of
+// the tile below K) do not enter pmin/pmax; a pivot <= 0 or NaN sets bad.
 __device__ __forceinline__ void potrf8_warp(float* S, float* rinv, int bb, float& pmin, float& pmax, int& bad,
                                             int nvalid) {
-    const int lane = threadIdx.x & 31, i = lane & 7, o = 8 * bb;
-    float a[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) a[j] = S[(o + j) * kCT + o + i];
-    float rs_own = 0.f;
+    const int lane = threadIdx.x & 31, o = 8 * bb;
+    float a[8][8];     // a[i][j]: row i, column j (lower part used)
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        float p = __shfl_sync(0xffffffffu, a[j], j);
+        const float4 lo = *reinterpret_cast<const float4*>(S + (o + j) * kCT + o);
+        const float4 hi = *reinterpret_cast<const float4*>(S + (o + j) * kCT + o + 4);
+        a[0][j] = lo.x; a[1][j] = lo.y; a[2][j] = lo.z; a[3][j] = lo.w;
+        a[4][j] = hi.x; a[5][j] = hi.y; a[6][j] = hi.z; a[7][j] = hi.w;
+    }
+    float rs[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        float p = a[j][j];
         if (!(p > 0.f)) {
             bad = 1;
             p = 1.f;
@@ -219,17 +228,24 @@ __device__ __forceinline__ void potrf8_warp(float* S, float* rinv, int bb, float
             pmin = fminf(pmin, p);
             pmax = fmaxf(pmax, p);
         }
-        const float rs = rsqrtf(p);
-        if (i == j) rs_own = rs;
-        const float l = i >= j ? a[j] * rs : 0.f;
-        a[j] = l;
+        rs[j] = rsqrtf(p);
 #pragma unroll
-        for (int c = j + 1; c < 8; ++c) a[c] = fmaf(-l, __shfl_sync(0xffffffffu, l, c), a[c]);
+        for (int i = j; i < 8; ++i) a[i][j] *= rs[j];
+#pragma unroll
+        for (int c = j + 1; c < 8; ++c)
+#pragma unroll
+            for (int i = c; i < 8; ++i) a[i][c] = fmaf(-a[i][j], a[c][j], a[i][c]);
     }
-    if (lane < 8) {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) S[(o + j) * kCT + o + i] = j <= i ? a[j] : 0.f;
-        rinv[o + i] = rs_own;
+    for (int c = 0; c < 8; ++c) {
+        if (lane == c) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) S[(o + c) * kCT + o + i] = i >= c ? a[i][c] : 0.f;
+        }
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) rinv[o + j] = rs[j];
     }
 }
 
@@ -346,29 +362,45 @@ __device__ __forceinline__ void diag_recip(const float* L, float* rinv) {
 }
 
 // ---------------------------------------------------------------- worker tasks
-// Group g (0 <= g <= T-3) holds T-g tasks: (I, g) for I = g+2..T-1 (type 0),
-// then (g+2, g+1) (type 1), then (g+2, g+2) (type 2).
-__device__ __forceinline__ void task_of(int T, int t, int& I, int& J, int& type) {
-    int g = 0, base = 0;
-    while (base + (T - g) <= t) {
-        base += T - g;
-        ++g;
+// Factorisation tasks, group g (0 <= g <= T-3), T-g of them: the TRSM tiles
+// (I, g) for I = g+2..T-1 (type 0), then the sub-diagonal (g+2, g+1) (type 1)
+// and the diagonal (g+2, g+2) (type 2), pre-updated through g.
+// Inverse tasks (when L^-1 is asked for): X_ii = L_ii^-1 (type 3, row i)
+// and X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj for j < i (type 4).
+// Global order, slot s = 0..T-1: [type 3 of row s][type 4 (s, j), j < s]
+// [factorisation group s].  A factorisation group s needs the diagonal
+// steps <= s and earlier groups; the diagonal step s needs groups <= s-1; a
+// row-s inverse task needs the diagonal step s, earlier rows of its column
+// and L tiles of row s, all from earlier slots: with every CTA resident,
+// no task waits on one behind it.
+__device__ __forceinline__ void task_of(int T, bool inv, int t, int& I, int& J, int& type) {
+    for (int sl = 0; sl < T; ++sl) {
+        if (inv) {
+            if (t == 0) { I = sl; J = sl; type = 3; return; }
+            --t;
+            if (t < sl) { I = sl; J = t; type = 4; return; }
+            t -= sl;
+        }
+        if (sl <= T - 3) {
+            const int n = T - sl, n0 = T - sl - 2;
+            if (t < n) {
+                if (t < n0) { I = sl + 2 + t; J = sl; type = 0; }
+                else if (t == n0) { I = sl + 2; J = sl + 1; type = 1; }
+                else { I = sl + 2; J = sl + 2; type = 2; }
+                return;
+            }
+            t -= n;
+        }
     }
-    const int o = t - base, n0 = T - g - 2;
-    if (o < n0) {
-        I = g + 2 + o;
-        J = g;
-        type = 0;
-    } else if (o == n0) {
-        I = g + 2;
-        J = g + 1;
-        type = 1;
-    } else {
-        I = g + 2;
-        J = g + 2;
-        type = 2;
-    }
+    I = J = type = -1;
 }
+
+__device__ __forceinline__ int task_count(int T, bool inv) {
+    return (T >= 3 ? T * (T + 1) / 2 - 3 : 0) + (inv ? T + T * (T - 1) / 2 : 0);
+}
+
+// packed lower-triangular tile index of (i, j), i >= j
+__device__ __forceinline__ int64_t packed_tile(int i, int j) { return (int64_t)i * (i + 1) / 2 + j; }
 
 struct CholSmem {
     float a[2][kCTE];     // worker: operand L_Ik' (double buffer); diagonal CTA: current and next diagonal tile
@@ -378,14 +410,121 @@ struct CholSmem {
     int ok;
 };
 
+// packed tile (i, j) of L^-1 (row-major) into shared memory, one cp.async group
+__device__ __forceinline__ void load_packed(const CholCtx& c, float* s, int i, int j) {
+    const float* src = c.Xinv + packed_tile(i, j) * kCTE;
+    for (int e = threadIdx.x; e < kCTE / 4; e += kCThreads) cp_async16(s + 4 * e, src + 4 * e);
+    cp_async_commit();
+}
+
+// shared tile s (row-major 64 x 64) into packed tile (i, j)
+__device__ __forceinline__ void store_packed(const CholCtx& c, const float* s, int i, int j) {
+    float* dst = c.Xinv + packed_tile(i, j) * kCTE;
+    for (int e = threadIdx.x; e < kCTE / 4; e += kCThreads)
+        __stcg(reinterpret_cast<float4*>(dst) + e, reinterpret_cast<const float4*>(s)[e]);
+}
+
+// Type 3: X_ii = L_ii^-1 into the packed inverse (row-major) and Dinv
+// (column-major).  X <- I L^-T = L^-T column-major, which is L^-1 row-major.
+__device__ bool task_diag_inverse(const CholCtx& c, CholSmem& sm, int i) {
+    if (!cta_wait(c, c.tflag + i * c.T + i, 2u, &sm.ok)) return false;
+    load_tile(c, sm.b[0], i, i);
+    for (int e = threadIdx.x; e < kCTE; e += kCThreads) sm.x[e] = (e >> 6) == (e & 63) ? 1.f : 0.f;
+    cp_async_wait_all();
+    __syncthreads();
+    diag_recip(sm.b[0], sm.rinv);
+    __syncthreads();
+    trsm_subst(sm.x, sm.b[0], sm.rinv);
+    store_packed(c, sm.x, i, i);
+    for (int e = threadIdx.x; e < kCTE; e += kCThreads) {
+        const int cc = e >> 6, r = e & 63;
+        __stcg(c.Dinv + (int64_t)i * kCTE + e, sm.x[r * kCT + cc]);
+    }
+    cta_publish(c.xflag + i * c.T + i, 1u);
+    return true;
+}
+
+// Type 4: X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj, operands double-buffered as
+// in the factorisation updates
+__device__ bool task_offdiag_inverse(const CholCtx& c, CholSmem& sm, int i, int j) {
+    const int T = c.T;
+    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+    float acc[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = 0.f;
+    const int n = i - j;     // k = j .. i-1
+    if (!cta_wait(c, c.tflag + i * T + j, 2u, &sm.ok)) return false;
+    if (!cta_wait(c, c.xflag + j * T + j, 1u, &sm.ok)) return false;
+    __syncthreads();
+    load_tile(c, sm.a[0], i, j);
+    load_packed(c, sm.b[0], j, j);
+    for (int q = 0; q < n; ++q) {
+        const int k = j + q, nb = (q + 1) & 1;
+        bool next = false;
+        if (q + 1 < n) {
+            next = cta_ready(c.tflag + i * T + k + 1, 2u, &sm.ok) && cta_ready(c.xflag + (k + 1) * T + j, 1u, &sm.ok);
+            if (next) {
+                load_tile(c, sm.a[nb], i, k + 1);
+                load_packed(c, sm.b[nb], k + 1, j);
+            }
+        }
+        if (next) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+        else cp_async_wait_all();
+        __syncthreads();
+        // acc -= L_ik X_kj: P = L_ik column-major, Q = X_kj row-major
+        sub_ptq(acc, sm.a[q & 1], sm.b[q & 1], tr, tc, 0, kCT);
+        if (q + 1 < n && !next) {
+            if (!cta_wait(c, c.tflag + i * T + k + 1, 2u, &sm.ok)) return false;
+            if (!cta_wait(c, c.xflag + (k + 1) * T + j, 1u, &sm.ok)) return false;
+            load_tile(c, sm.a[nb], i, k + 1);
+            load_packed(c, sm.b[nb], k + 1, j);
+        }
+    }
+    // acc = -S; X_ij = -X_ii S: with P = Dinv_i (column-major) and Q = acc
+    // (row-major), sub_ptq gives -Dinv_i (-S) ... negated below
+    if (!cta_wait(c, c.xflag + i * T + i, 1u, &sm.ok)) return false;
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) sm.x[(4 * tr + p) * kCT + 4 * tc + q] = acc[p][q];
+    for (int e = threadIdx.x; e < kCTE; e += kCThreads) sm.b[0][e] = __ldcg(c.Dinv + (int64_t)i * kCTE + e);
+    __syncthreads();
+    float out[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[p][q] = 0.f;
+    sub_ptq(out, sm.b[0], sm.x, tr, tc, 0, kCT);     // out = -Dinv_i (-S) = Dinv_i S
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) sm.x[(4 * tr + p) * kCT + 4 * tc + q] = -out[p][q];
+    __syncthreads();
+    store_packed(c, sm.x, i, j);
+    cta_publish(c.xflag + i * T + j, 1u);
+    return true;
+}
+
 __device__ void worker(const CholCtx& c, CholSmem& sm) {
     const int W = gridDim.x - 1, wid = blockIdx.x - 1;
     const int T = c.T;
-    const int ntask = T >= 3 ? T * (T + 1) / 2 - 3 : 0;
+    const bool inv = c.Xinv != nullptr;
+    const int ntask = task_count(T, inv);
     const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
     for (int t = wid; t < ntask; t += W) {
         int I, J, type;
-        task_of(T, t, I, J, type);
+        task_of(T, inv, t, I, J, type);
+        if (type == 3) {
+            if (!task_diag_inverse(c, sm, I)) return;
+            continue;
+        }
+        if (type == 4) {
+            if (!task_offdiag_inverse(c, sm, I, J)) return;
+            continue;
+        }
         // updates k' < kend, kend = J for type 0, I-1 for types 1 and 2
         const int kend = type == 0 ? J : I - 1;
         __syncthreads();
@@ -491,11 +630,14 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
         }
         cp_async_wait_all();
         __syncthreads();
+        // lower 4 x 4 patches only (the factorisation reads the lower triangle)
         float acc[4][4];
-        acc_from(acc, Y, tr, tc);
-        sub_ptq(acc, X, X, tr, tc, 0, kCT);
+        if (tc <= tr) {
+            acc_from(acc, Y, tr, tc);
+            sub_ptq(acc, X, X, tr, tc, 0, kCT);
+        }
         __syncthreads();
-        acc_to(acc, Y, tr, tc);
+        if (tc <= tr) acc_to(acc, Y, tr, tc);
         __syncthreads();
         cur ^= 1;
     }
@@ -555,7 +697,56 @@ VTB_API int64_t vtb_chol_dinv_floats(int K) { return K > 0 ? (int64_t)chol_tiles
 VTB_API int64_t vtb_chol_work_bytes(int K) {
     if (K <= 0) return 0;
     const int64_t T = chol_tiles(K);
-    return ((T * T * 4 + 255) & ~(int64_t)255) + 256;
+    return 2 * ((T * T * 4 + 255) & ~(int64_t)255) + 256;
+}
+
+VTB_API int64_t vtb_chol_inverse_floats(int K) {
+    if (K <= 0) return 0;
+    const int64_t T = chol_tiles(K);
+    return T * (T + 1) / 2 * kCTE;
+}
+
+static int chol_launch(float* A, int64_t ld, int K, float* Dinv, float* Linv, void* work, int64_t work_bytes,
+                       int32_t* status, double* pivots, double rcond, void* stream) {
+    VTB_CHECK_ARG(K > 0 && ld >= K && A && Dinv && work && status);
+    VTB_CHECK_ARG(work_bytes >= vtb_chol_work_bytes(K) && ((uintptr_t)work & 255) == 0);
+    VTB_CHECK_ARG(((uintptr_t)Linv & 15) == 0);
+    int dev = 0;
+    VTB_CUDA_TRY(cudaGetDevice(&dev));
+    int coop = 0, nsm = 0;
+    VTB_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    VTB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (!coop) return VTB_CUDA_ERR;
+    const size_t sm = sizeof(CholSmem);
+    VTB_CUDA_TRY(cudaFuncSetAttribute(chol_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int per_sm = 0;
+    VTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chol_tiles_kernel, kCThreads, sm));
+    if (per_sm < 1) return VTB_CUDA_ERR;
+    const int T = chol_tiles(K);
+    const int ntask = (T >= 3 ? T * (T + 1) / 2 - 3 : 0) + (Linv ? T + T * (T - 1) / 2 : 0);
+    const int grid = 1 + std::max(1, std::min(nsm - 1, ntask));
+    cudaStream_t s = as_stream(stream);
+    const int64_t fbytes = ((int64_t)T * T * 4 + 255) & ~(int64_t)255;
+    VTB_CUDA_TRY(cudaMemsetAsync(work, 0, (size_t)(2 * fbytes + 256), s));
+    CholCtx c;
+    c.A = A;
+    c.ld = ld;
+    c.K = K;
+    c.T = T;
+    c.Dinv = Dinv;
+    c.tflag = reinterpret_cast<unsigned*>(work);
+    c.xflag = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(work) + fbytes);
+    c.abort_word = reinterpret_cast<int*>(reinterpret_cast<char*>(work) + 2 * fbytes);
+    c.status = status;
+    c.piv = pivots;
+    c.rcond = rcond;
+    c.limit = wait_limit(kCholSpin);
+    c.Xinv = Linv;
+    void* args[] = {(void*)&c};
+    VTB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)chol_tiles_kernel, dim3(grid), dim3(kCThreads), args, sm, s));
+    // without the inverse tasks, the diagonal-tile inverses come from a second kernel
+    if (!Linv) chol_dinv_kernel<<<T, kCThreads, 0, s>>>(A, ld, K, Dinv);
+    return launch_status();
 }
 
 // Float32 Cholesky of the symmetric positive definite K x K matrix A
@@ -571,40 +762,100 @@ VTB_API int64_t vtb_chol_work_bytes(int K) {
 // vtem/vtdm.py:645-648).  Stream-ordered; does not synchronise.
 VTB_API int vtb_chol_factor(float* A, int64_t ld, int K, float* Dinv, void* work, int64_t work_bytes, int32_t* status,
                             double* pivots, double rcond, void* stream) {
-    VTB_CHECK_ARG(K > 0 && ld >= K && A && Dinv && work && status);
-    VTB_CHECK_ARG(work_bytes >= vtb_chol_work_bytes(K) && ((uintptr_t)work & 255) == 0);
-    int dev = 0;
-    VTB_CUDA_TRY(cudaGetDevice(&dev));
-    int coop = 0, nsm = 0;
-    VTB_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-    VTB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    if (!coop) return VTB_CUDA_ERR;
-    const size_t sm = sizeof(CholSmem);
-    VTB_CUDA_TRY(cudaFuncSetAttribute(chol_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    int per_sm = 0;
-    VTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chol_tiles_kernel, kCThreads, sm));
-    if (per_sm < 1) return VTB_CUDA_ERR;
-    const int T = chol_tiles(K);
-    const int ntask = T >= 3 ? T * (T + 1) / 2 - 3 : 0;
-    const int grid = 1 + std::max(1, std::min(nsm - 1, ntask));
+    return chol_launch(A, ld, K, Dinv, nullptr, work, work_bytes, status, pivots, rcond, stream);
+}
+
+// vtb_chol_factor that also forms L^-1 in the same launch: Linv
+// (vtb_chol_inverse_floats(K) floats, 16-byte aligned) receives the tiles
+// (i, j), i >= j, of L^-1, row-major, tile (i, j) at (i(i+1)/2 + j) * 4096.
+VTB_API int vtb_chol_factor_inverse(float* A, int64_t ld, int K, float* Dinv, float* Linv, void* work,
+                                    int64_t work_bytes, int32_t* status, double* pivots, double rcond, void* stream) {
+    VTB_CHECK_ARG(Linv);
+    return chol_launch(A, ld, K, Dinv, Linv, work, work_bytes, status, pivots, rcond, stream);
+}
+
+namespace vtb {
+
+// y = L^-1 b and x = L^-T y with the packed inverse: block row i of y is
+// sum_{j <= i} X_ij b_j, block column j of x is sum_{i >= j} X_ij^T y_i.
+// Each block handles the pair of block rows (columns) b and T-1-b, so every
+// block streams about T/2 tiles; four threads share a row (column).
+constexpr int kGThreads = 256;
+
+__global__ void __launch_bounds__(kGThreads) inv_lower_kernel(const float* __restrict__ X, int K,
+                                                              const double* __restrict__ b, float* __restrict__ y) {
+    __shared__ __align__(16) float bs[kSMaxT * kCT];
+    const int T = (K + kCT - 1) / kCT;
+    for (int e = threadIdx.x; e < T * kCT; e += kGThreads) bs[e] = e < K ? (float)b[e] : 0.f;
+    __syncthreads();
+    const int r = threadIdx.x >> 2, part = threadIdx.x & 3;
+    for (int h = 0; h < 2; ++h) {
+        const int i = h == 0 ? (int)blockIdx.x : T - 1 - (int)blockIdx.x;
+        if (h == 1 && i == (int)blockIdx.x) break;
+        float a0 = 0.f, a1 = 0.f;
+        for (int j = 0; j <= i; ++j) {
+            const float4* row = reinterpret_cast<const float4*>(X + packed_tile(i, j) * kCTE + r * kCT + 16 * part);
+            const float* bj = bs + j * kCT + 16 * part;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 v = __ldg(row + q);
+                a0 = fmaf(v.x, bj[4 * q], a0);
+                a1 = fmaf(v.y, bj[4 * q + 1], a1);
+                a0 = fmaf(v.z, bj[4 * q + 2], a0);
+                a1 = fmaf(v.w, bj[4 * q + 3], a1);
+            }
+        }
+        float acc = a0 + a1;
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        if (part == 0) y[i * kCT + r] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(kGThreads) inv_upper_kernel(const float* __restrict__ X, int K,
+                                                              const float* __restrict__ y, double* __restrict__ x) {
+    __shared__ __align__(16) float ys[kSMaxT * kCT];
+    const int T = (K + kCT - 1) / kCT;
+    for (int e = threadIdx.x; e < T * kCT; e += kGThreads) ys[e] = y[e];
+    __syncthreads();
+    const int cc = threadIdx.x >> 2, part = threadIdx.x & 3;
+    for (int h = 0; h < 2; ++h) {
+        const int j = h == 0 ? (int)blockIdx.x : T - 1 - (int)blockIdx.x;
+        if (h == 1 && j == (int)blockIdx.x) break;
+        float a0 = 0.f, a1 = 0.f;
+        for (int i = j; i < T; ++i) {
+            const float* col = X + packed_tile(i, j) * kCTE + (16 * part) * kCT + cc;
+            const float* yi = ys + i * kCT + 16 * part;
+#pragma unroll
+            for (int t = 0; t < 16; t += 2) {
+                a0 = fmaf(__ldg(col + t * kCT), yi[t], a0);
+                a1 = fmaf(__ldg(col + (t + 1) * kCT), yi[t + 1], a1);
+            }
+        }
+        float acc = a0 + a1;
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        const int g = j * kCT + cc;
+        if (part == 0 && g < K) x[g] = (double)acc;
+    }
+}
+
+}  // namespace vtb
+
+// x = L^-T L^-1 x (x float64 in and out, float32 arithmetic) with the packed
+// inverse of vtb_chol_factor_inverse: two triangular matrix-vector products
+// over the tiles, each read once (L2-resident at the GPU configuration).
+// y_work: ceil(K/64)*64 floats of scratch.  K <= 10240.  Replaces spotrs
+// in the mixed decoder's solve (linalg.py:591-631).  Stream-ordered.
+VTB_API int vtb_chol_solve_inverse(const float* Linv, int K, double* x, float* y_work, void* stream) {
+    VTB_CHECK_ARG(K > 0 && K <= kSMaxT * kCT && Linv && x && y_work && ((uintptr_t)Linv & 15) == 0);
+    const int T = (K + kCT - 1) / kCT;
     cudaStream_t s = as_stream(stream);
-    const int64_t fbytes = ((int64_t)T * T * 4 + 255) & ~(int64_t)255;
-    VTB_CUDA_TRY(cudaMemsetAsync(work, 0, (size_t)(fbytes + 256), s));
-    CholCtx c;
-    c.A = A;
-    c.ld = ld;
-    c.K = K;
-    c.T = T;
-    c.Dinv = Dinv;
-    c.tflag = reinterpret_cast<unsigned*>(work);
-    c.abort_word = reinterpret_cast<int*>(reinterpret_cast<char*>(work) + fbytes);
-    c.status = status;
-    c.piv = pivots;
-    c.rcond = rcond;
-    c.limit = wait_limit(kCholSpin);
-    void* args[] = {(void*)&c};
-    VTB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)chol_tiles_kernel, dim3(grid), dim3(kCThreads), args, sm, s));
-    chol_dinv_kernel<<<T, kCThreads, 0, s>>>(A, ld, K, Dinv);
+    const int grid = (T + 1) / 2;
+    inv_lower_kernel<<<grid, kGThreads, 0, s>>>(Linv, K, x, y_work);
+    int st = launch_status();
+    if (st) return st;
+    inv_upper_kernel<<<grid, kGThreads, 0, s>>>(Linv, K, y_work, x);
     return launch_status();
 }
 
@@ -630,7 +881,6 @@ namespace vtb {
 // step.
 constexpr int kSThreads = 256;
 constexpr int kSPre = 4;          // own tiles per step loaded ahead in registers
-constexpr int kSMaxT = 160;       // K <= 10240
 constexpr int kSMaxOwn = 24;      // ceil(T / C) for C >= 8
 
 struct SolveSmem {

@@ -24,8 +24,10 @@ underestimate it by orders of magnitude on badly sampled windows, must stay
 below 1 / (rcond * CHOL_MARGIN); otherwise the eigen-pseudoinverse runs.
 ``"mixed"`` builds M on the tensor cores from split-bf16 operands (fp32
 accumulation), factorises it by float32 Cholesky (this library's tile
-Cholesky, ``mixed_factor="tiles"``, or cuSOLVER's spotrf, ``"cusolver"``),
-and recovers float64
+Cholesky, which by default, ``mixed_factor="inverse"``, also forms L^-1 in
+the same launch so that every solve is two matrix-vector products;
+``"tiles"``: the factor alone and block substitutions; ``"cusolver"``:
+cuSOLVER's spotrf), and recovers float64
 accuracy with ``mixed_sweeps`` refinement sweeps against the exact float64
 residual Phi^H (q - Phi a), applied through the Kronecker factors without
 forming M in float64.  A mixed solve is accepted when the factorisation
@@ -73,7 +75,7 @@ def coefficient_count(Mx, My, Mt):
 
 class CoeffDecoder(object):
     def __init__(self, Ds, h_norm, Mx, My, Wt, Mt, decPx, decPy, Px1, Py1, rcond=1e-8, solver="auto", refine=0,
-                 device="cuda", mixed_sweeps=2, mixed_factor="tiles", synth="harmonics"):
+                 device="cuda", mixed_sweeps=2, mixed_factor="inverse", synth="harmonics"):
         self.Mx, self.My, self.Mt = int(Mx), int(My), int(Mt)
         self.Wt = float(Wt)
         self.W = self.Wt / self.Mt
@@ -113,8 +115,8 @@ class CoeffDecoder(object):
         self.last_solver = None
         self.last_pivots = (0.0, 0.0)
         self.mixed_sweeps = int(mixed_sweeps)
-        if mixed_factor not in ("tiles", "cusolver"):
-            raise ValueError("mixed_factor must be 'tiles' or 'cusolver'")
+        if mixed_factor not in ("inverse", "tiles", "cusolver"):
+            raise ValueError("mixed_factor must be 'inverse', 'tiles' or 'cusolver'")
         self.mixed_factor = mixed_factor
         if synth not in ("harmonics", "fused"):
             raise ValueError("synth must be 'harmonics' or 'fused'")
@@ -146,6 +148,9 @@ class CoeffDecoder(object):
         # the tile Cholesky's diagonal-tile inverses and flag scratch
         self._cdinv = torch.empty(int(lib().vtb_chol_dinv_floats(self.K)), dtype=torch.float32, device=device)
         self._cwork = torch.empty(int(lib().vtb_chol_work_bytes(self.K)), dtype=torch.uint8, device=device)
+        if self.mixed_factor == "inverse":
+            self._clinv = torch.empty(int(lib().vtb_chol_inverse_floats(self.K)), dtype=torch.float32, device=device)
+            self._cy = torch.empty(((self.K + 63) // 64) * 64, dtype=torch.float32, device=device)
 
     def set_norm(self, h_norm):
         """Per-neuron weights norm (vtem/vtdm.py:634-638, 1/(kappa sigma) for
@@ -239,7 +244,13 @@ class CoeffDecoder(object):
                                  0, 1.0, 0, self._stat_ptr(7), s)
         ld = self.ld32
         call("vtb_coeff_real_scatter", dptr(self.C), KK, self.Ks, self.Kt, dptr(self.Mr32), ld, 0, s)
-        if self.mixed_factor == "tiles":
+        if self.mixed_factor == "inverse":
+            # float32 tile Cholesky and L^-1 (one cooperative launch), solves by two products
+            call("vtb_chol_factor_inverse", dptr(self.Mr32), ld, K, dptr(self._cdinv), dptr(self._clinv),
+                 dptr(self._cwork), self._cwork.numel(), self._stat_ptr(0), self._stat_ptr(1),
+                 self.rcond * CHOL_MARGIN, s)
+            solve = lambda x: call("vtb_chol_solve_inverse", dptr(self._clinv), K, dptr(x), dptr(self._cy), s)
+        elif self.mixed_factor == "tiles":
             # float32 tile Cholesky (one cooperative launch) and cluster solves
             call("vtb_chol_factor", dptr(self.Mr32), ld, K, dptr(self._cdinv), dptr(self._cwork),
                  self._cwork.numel(), self._stat_ptr(0), self._stat_ptr(1), self.rcond * CHOL_MARGIN, s)
@@ -518,7 +529,7 @@ class CoeffDecoder(object):
         return host_out
 
 
-def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=0, mixed_sweeps=2, mixed_factor="tiles",
+def from_prep(prep, Wt, Mt, rcond=1e-8, solver="auto", refine=0, mixed_sweeps=2, mixed_factor="inverse",
               synth="harmonics"):
     """A :class:`CoeffDecoder` on the output of ``vtdm.VTDM_prep``."""
     return CoeffDecoder(prep.Ds, prep.h_norm, prep.Mx, prep.My, Wt, Mt, prep.decPx, prep.decPy, prep.Px1, prep.Py1,
