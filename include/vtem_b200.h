@@ -403,12 +403,14 @@ int vtb_sym_potrs_flags(const float* L, int64_t ld, const float* Dinv, int K, do
 /* Float32 Cholesky of ONE symmetric positive definite K x K matrix A
  * (column-major, leading dimension ld; the factor L overwrites the lower
  * triangle), written for the B200: one cooperative launch, 64 x 64 tiles as
- * a data-flow graph (one CTA walks the diagonal: POTRF, inverse, TRSM of the
- * sub-diagonal tile, SYRK of the next diagonal tile; every other CTA
- * accumulates the trailing updates of its tiles in registers and runs their
- * TRSMs), release/acquire flags between CTAs with bounded waits.  Dinv
- * (vtb_chol_dinv_floats(K) floats) receives the inverses of the 64 x 64
- * diagonal tiles of L; work: vtb_chol_work_bytes(K) bytes, 256-byte aligned.
+ * a data-flow graph (one CTA walks the diagonal: the panel [A_kk; I] ->
+ * [L_kk; L_kk^-T], the sub-diagonal tile as a product with L_kk^-T, SYRK of
+ * the next diagonal tile; every other CTA accumulates the trailing updates
+ * of its tiles in registers and runs their TRSMs as products with the
+ * published L_JJ^-T), release/acquire flags between CTAs with bounded
+ * waits.  Dinv (vtb_chol_dinv_floats(K) floats, 16-byte aligned) receives
+ * the inverses of the 64 x 64 diagonal tiles of L, each ROW-major (tile k
+ * at k*4096); work: vtb_chol_work_bytes(K) bytes, 256-byte aligned.
  * status (device int32, zeroed by the caller) receives 1 (a pivot <= 0), 2
  * (max/min squared pivot times rcond >= 1: the pseudoinverse might truncate)
  * or 3 (a wait between CTAs ran out; the factor is then invalid); pivots
@@ -441,10 +443,13 @@ int vtb_chol_factor_inverse(float* A, int64_t ld, int K, float* Dinv, float* Lin
                             int32_t* status, double* pivots, double rcond, void* stream);
 /* x = L^-T L^-1 x (x float64 in and out, float32 arithmetic) with the packed
  * inverse of vtb_chol_factor_inverse: two triangular matrix-vector products
- * (y = X b, then x = X^T y), every tile read once; no step waits on another
- * CTA.  y_work: ceil(K/64)*64 floats.  K <= 10240.  Replaces spotrs in the
- * solve of linalg.py:591-631. */
-int vtb_chol_solve_inverse(const float* Linv, int K, double* x, float* y_work, void* stream);
+ * (y = X b, then x = X^T y), one block per tile, every tile read once; the
+ * last block of each block row (column), found by an atomic ticket, sums
+ * the partials in a fixed order.  work: vtb_chol_solve_inverse_bytes(K)
+ * bytes, zeroed before the first call and left zeroed by every call.
+ * Replaces spotrs in the solve of linalg.py:591-631. */
+int64_t vtb_chol_solve_inverse_bytes(int K);
+int vtb_chol_solve_inverse(const float* Linv, int K, double* x, void* work, int64_t work_bytes, void* stream);
 /* Pseudoinverse solve x = V diag(1/w if |w| > rcond*max|w| else 0) V^T b of
  * a float64 symmetric M (destroyed), the rule of solve_eq_sym
  * (vtem/utils/linalg.py:591-631, sq_Kernel :791-833).  kept (device) the

@@ -96,7 +96,8 @@ def test_chol_and_wait_limit_entry_points_without_gpu():
     assert lib.vtb_chol_solve(None, 0, None, 0, None, None) == _abi.VTB_BAD_ARG
     assert lib.vtb_chol_inverse_floats(0) == 0 and lib.vtb_chol_inverse_floats(1921) == 31 * 32 // 2 * 4096
     assert lib.vtb_chol_factor_inverse(None, 0, 0, None, None, None, 0, None, None, 1e-8, None) == _abi.VTB_BAD_ARG
-    assert lib.vtb_chol_solve_inverse(None, 0, None, None, None) == _abi.VTB_BAD_ARG
+    assert lib.vtb_chol_solve_inverse(None, 0, None, None, 0, None) == _abi.VTB_BAD_ARG
+    assert lib.vtb_chol_solve_inverse_bytes(1921) == (31 * 32 // 2 * 64 + 31 * 64) * 4 + 2 * 31 * 4
     assert lib.vtb_set_wait_limit(-1, None) == _abi.VTB_BAD_ARG
     with _abi.wait_limit(7):
         import numpy as np

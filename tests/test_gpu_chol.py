@@ -58,7 +58,7 @@ def test_chol_factor_and_solve_match_float64(K):
     D = dinv.cpu().numpy().reshape(T, 64, 64)
     for k in range(T):
         r0, r1 = 64 * k, min(K, 64 * k + 64)
-        Dk = D[k].T[: r1 - r0, : r1 - r0]                                         # column-major tile
+        Dk = D[k][: r1 - r0, : r1 - r0]                                           # row-major tile
         ref = np.linalg.inv(Lref[r0:r1, r0:r1])
         assert np.linalg.norm(Dk - ref) / np.linalg.norm(ref) < 1e-3
     # solves: x = A^-1 b to float32 accuracy times the condition number
@@ -116,15 +116,21 @@ def test_chol_factor_inverse_and_product_solve(K):
     assert np.isfinite(X).all()
     assert np.linalg.norm(X - Xref) / np.linalg.norm(Xref) < 1e-3
     assert np.abs(np.triu(X, 1)).max() == 0.0                                     # exact zeros above
-    y = torch.empty(((K + 63) // 64) * 64, dtype=torch.float32, device="cuda")
+    work = torch.zeros(int(lib().vtb_chol_solve_inverse_bytes(K)), dtype=torch.uint8, device="cuda")
     rng = np.random.default_rng(2)
-    for _ in range(2):
-        b = rng.standard_normal(K)
+    bs = [rng.standard_normal(K), rng.standard_normal(K)]
+    outs = []
+    for b in bs + [bs[0]]:
         x = torch.as_tensor(b, device="cuda")
-        call("vtb_chol_solve_inverse", dptr(linv), K, dptr(x), dptr(y), stream_ptr())
+        call("vtb_chol_solve_inverse", dptr(linv), K, dptr(x), dptr(work), work.numel(), stream_ptr())
         torch.cuda.synchronize()
         xref = np.linalg.solve(A, b)
         assert np.linalg.norm(x.cpu().numpy() - xref) / np.linalg.norm(xref) < 1e-3
+        outs.append(x.cpu().numpy())
+    assert np.array_equal(outs[0], outs[2])                                       # fixed summation order
+    T = (K + 63) // 64
+    tickets = work[-8 * T:].view(torch.int32)
+    assert int(tickets.abs().sum().item()) == 0                                   # left zeroed
 
 
 def test_chol_factor_inverse_wait_limit_runs_out():

@@ -101,7 +101,8 @@ SIGNATURES = {
     "vtb_chol_solve_cluster": [],
     "vtb_chol_inverse_floats": [I],  # restype int64, set in lib()
     "vtb_chol_factor_inverse": [P, L, I, P, P, P, L, P, P, D, P],
-    "vtb_chol_solve_inverse": [P, I, P, P, P],
+    "vtb_chol_solve_inverse_bytes": [I],  # restype int64, set in lib()
+    "vtb_chol_solve_inverse": [P, I, P, P, L, P],
 }
 
 _lib = None
@@ -129,7 +130,7 @@ def lib():
             f.argtypes = args
             f.restype = ctypes.c_int
         for name in ("vtb_sym_dinv_floats", "vtb_tc_group_bytes", "vtb_sym_potrs_flags_bytes", "vtb_chol_dinv_floats",
-                     "vtb_chol_work_bytes", "vtb_chol_inverse_floats"):
+                     "vtb_chol_work_bytes", "vtb_chol_inverse_floats", "vtb_chol_solve_inverse_bytes"):
             getattr(l, name).argtypes = [ctypes.c_int]
             getattr(l, name).restype = ctypes.c_int64
         l.vtb_status_string.argtypes = [ctypes.c_int]

@@ -1,49 +1,51 @@
 // Float32 Cholesky factorisation of ONE symmetric positive definite system
 // (the mixed decoder's real-form coefficient system, K = 1921 at the GPU
-// configuration), written for the B200 instead of cuSOLVER's spotrf.
+// configuration), written for the B200 instead of cuSOLVER's spotrf, with the
+// inverse of the factor formed in the same launch when asked for.
 //
-// spotrf at K = 1921 is latency-bound (a chain of dependent panel steps, 0.67
+// spotrf at K = 1921 is latency-bound (a chain of dependent panel steps, 0.65
 // ms for 2.4 GFLOP).  Here one cooperative launch factorises the matrix in
 // 64 x 64 tiles (T = ceil(K/64) tile rows) as a data-flow graph:
 //
 //   CTA 0 ("diagonal") walks the critical path, step k = 0..T-1:
-//     POTRF of the diagonal tile (k,k) with all its warps (8-column blocks:
-//     warp 0 factorises each 8 x 8 diagonal block while the others apply the
-//     previous block's update), publishes L_kk;
-//     TRSM of the sub-diagonal tile L_{k+1,k} = A_{k+1,k} L_kk^-T by blocked
-//     substitution;
+//     one panel factorisation [A_kk; I] -> [L_kk; L_kk^-T] with all its warps
+//     (8-column blocks: warp 0 factorises each 8 x 8 diagonal block while the
+//     others apply the previous block's update); publishes L_kk and
+//     L_kk^-1 (Dinv) together;
+//     the sub-diagonal tile L_{k+1,k} = A_{k+1,k} L_kk^-T as a product;
 //     SYRK of the next diagonal tile A_{k+1,k+1} -= L_{k+1,k} L_{k+1,k}^T,
 //     which it keeps in shared memory for step k+1.
 //   CTAs 1.. ("workers") run every other piece: for tile (I,J) the updates
 //     A_IJ -= sum_{k'} L_Ik' L_Jk'^T (the 4 x 4 register block of each thread
-//     stays in registers across all of them), then for I >= J+2 the TRSM
-//     with the published L_JJ.  Diagonal and sub-diagonal tiles receive
-//     from the workers all updates but the last (the diagonal CTA applies
-//     that one), so the diagonal CTA never waits on a round trip through a
-//     worker for data its own previous step produced.
-//   A second, small kernel then forms the inverses of the diagonal tiles
-//   (Dinv, for the triangular solves), one block per tile.
+//     stays in registers across all of them), then for I >= J+2 the TRSM as
+//     the product with the published L_JJ^-T.  Diagonal and sub-diagonal
+//     tiles receive from the workers all updates but the last (the diagonal
+//     CTA applies that one), so the diagonal CTA never waits on a round trip
+//     through a worker for data its own previous step produced.  With the
+//     inverse asked for, the workers also form X = L^-1 tile by tile,
+//     X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj, as soon as its operands are
+//     published; the solves are then two matrix-vector products.
 //
 // Worker tasks are ordered by the step whose outputs they need ("group" g:
 // the TRSM tiles (I, g) for I >= g+2, then the sub-diagonal (g+2, g+1), then
-// the diagonal (g+2, g+2), pre-updated through g) and dealt round-robin; each
-// worker runs its tasks in that order.  Every dependency of a task lies in
-// an earlier position or in a diagonal step that depends only on earlier
-// groups, so with all CTAs co-resident (cooperative launch) the graph cannot
-// deadlock.
+// the diagonal (g+2, g+2), pre-updated through g; the inverse tiles of row s
+// before group s) and dealt round-robin; each worker runs its tasks in that
+// order.  Every dependency of a task lies in an earlier position or in a
+// diagonal step that depends only on earlier groups, so with all CTAs
+// co-resident (cooperative launch) the graph cannot deadlock.
 //
 // Hand-offs: a tile's producer stores it, then (after a CTA barrier) thread
-// 0 makes the stores visible (__threadfence) and release-stores the tile's
-// flag; a consumer's thread 0 acquire-polls the flag, the CTA barrier
-// follows, and the tile is read through L2 (ld.global.cg).  Every wait is
-// bounded: after the limit the CTA marks the call aborted (status 3) and all
-// CTAs stop waiting and return.
+// 0 release-stores the tile's flag (release is cumulative: the barrier
+// orders the other threads' stores before it); a consumer's thread 0 acquire-polls the flag, the CTA barrier
+// follows, and the tile is read through L2 (ld.global.cg / cp.async.cg).
+// Every wait is bounded: after the limit the CTA marks the call aborted
+// (status 3) and all CTAs stop waiting and return.
 //
 // Rows and columns beyond K behave as the identity (0 off the diagonal, 1
 // on it), so K needs no padding.  The factor L is written over the lower
 // triangle of A (column-major, element (i, j) at j*ld + i, as spotrf leaves
-// it); Dinv receives T tiles of 64 x 64 (column-major, tile k at k*4096)
-// holding L_kk^-1 for the triangular solves (second kernel, same stream).  A failed pivot (<= 0 or not a
+// it); Dinv receives T tiles of 64 x 64 holding L_kk^-1 ROW-major (tile k at
+// k*4096, element (r, c) at r*64 + c).  A failed pivot (<= 0 or not a
 // number) or a spread of the squared pivots max/min >= 1/rcond sets the
 // status word to 1 or 2, as vtb_sym_factor's pivot test does.
 #include <cooperative_groups.h>
@@ -105,12 +107,11 @@ __device__ bool cta_wait(const CholCtx& c, const unsigned* f, unsigned v, int* s
     return *s_ok != 0;
 }
 
+// the CTA barrier orders every thread's stores before thread 0's release
+// store, whose release semantics are cumulative at GPU scope
 __device__ __forceinline__ void cta_publish(unsigned* f, unsigned v) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        c_st_release(f, v);
-    }
+    if (threadIdx.x == 0) c_st_release(f, v);
 }
 
 // tile (I, J) of A into shared memory s (column-major, 64 x 64); entries
@@ -184,6 +185,29 @@ __device__ __forceinline__ void sub_ptq(float (&acc)[4][4], const float* P, cons
     }
 }
 
+// acc[i][j] -= sum_t P[t][4tr+i] Q[4tc+j][t]  (P column-major 64 x 64; Q with the t index contiguous: Q[c][t]
+// at Q + c*64 + t).  The Q reads of a quarter-warp are one address (same tc): broadcasts.
+__device__ __forceinline__ void sub_pq_rowq(float (&acc)[4][4], const float* P, const float* Q, int tr, int tc) {
+#pragma unroll 2
+    for (int t = 0; t < kCT; t += 4) {
+        float4 q[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) q[j] = *reinterpret_cast<const float4*>(Q + (4 * tc + j) * kCT + t);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float4 p = *reinterpret_cast<const float4*>(P + (t + u) * kCT + 4 * tr);
+            const float pv[4] = {p.x, p.y, p.z, p.w};
+            float qv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) qv[j] = u == 0 ? q[j].x : u == 1 ? q[j].y : u == 2 ? q[j].z : q[j].w;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(-pv[i], qv[j], acc[i][j]);
+        }
+    }
+}
+
 __device__ __forceinline__ void acc_from(float (&acc)[4][4], const float* s, int tr, int tc) {
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -201,10 +225,10 @@ __device__ __forceinline__ void acc_to(const float (&acc)[4][4], float* s, int t
 // ---------------------------------------------------------------- 64 x 64 POTRF
 // The 8 x 8 diagonal block at (8bb, 8bb) of the column-major 64 x 64 tile S,
 // in one warp: every lane loads the whole block (broadcast reads) and
-// factorises it in its registers, so no step waits on another lane; lanes
-// 0..7 then write column `lane` of L (zeros above the diagonal) and lane 0
-// writes rinv[8bb + j] = 1/L_jj.  Pivots of rows beyond K (nvalid: rows of
-// the tile below K) do not enter pmin/pmax; a pivot <= 0 or NaN sets bad.
+// factorises it in its registers, so no step waits on another lane; the
+// warp then writes L (zeros above the diagonal) and rinv[8bb + j] = 1/L_jj.
+// Pivots of rows beyond K (nvalid: rows of the tile below K) do not enter
+// pmin/pmax; a pivot <= 0 or NaN sets bad.
 __device__ __forceinline__ void potrf8_warp(float* S, float* rinv, int bb, float& pmin, float& pmax, int& bad,
                                             int nvalid) {
     const int lane = threadIdx.x & 31, o = 8 * bb;
@@ -236,17 +260,18 @@ __device__ __forceinline__ void potrf8_warp(float* S, float* rinv, int bb, float
 #pragma unroll
             for (int i = c; i < 8; ++i) a[i][c] = fmaf(-a[i][j], a[c][j], a[i][c]);
     }
+    // every lane holds the same values: warp-wide stores to one address each
+    // (no divergent branch, one shared-memory wavefront per store)
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        if (lane == c) {
+        float col[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) S[(o + c) * kCT + o + i] = i >= c ? a[i][c] : 0.f;
-        }
+        for (int i = 0; i < 8; ++i) col[i] = i >= c ? a[i][c] : 0.f;
+        *reinterpret_cast<float4*>(S + (o + c) * kCT + o) = make_float4(col[0], col[1], col[2], col[3]);
+        *reinterpret_cast<float4*>(S + (o + c) * kCT + o + 4) = make_float4(col[4], col[5], col[6], col[7]);
     }
-    if (lane == 0) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) rinv[o + j] = rs[j];
-    }
+    *reinterpret_cast<float4*>(rinv + o) = make_float4(rs[0], rs[1], rs[2], rs[3]);
+    *reinterpret_cast<float4*>(rinv + o + 4) = make_float4(rs[4], rs[5], rs[6], rs[7]);
 }
 
 // row r of column block bb: x <- x L_bb^-T by substitution (x the row's 8
@@ -267,20 +292,64 @@ __device__ __forceinline__ void subst_row8(float* X, const float* L, const float
     for (int c = 0; c < 8; ++c) X[(o + c) * kCT + r] = x[c];
 }
 
-// Cholesky of the symmetric positive definite 64 x 64 tile S (column-major,
-// lower triangle read) in place: S <- L (zeros above the diagonal), rinv <-
-// 1/diag(L).  Blocks of 8 columns, all 8 warps: after the column block bb is
-// solved (one thread per row below it), warp 0 updates and factorises the
-// next diagonal block while warps 1-7 apply the rank-8 update to the rest of
-// the trailing triangle in 4 x 4 register patches.  The chain is 8 block
-// factorisations and 8 row substitutions; nothing else waits on them.
-__device__ void potrf64(float* S, float* rinv, float& pmin, float& pmax, int& bad, int nvalid) {
+// X[r0..r0+3][c0..c0+3] -= sum_{t<8} X[r0..][o+t] L[c0..][o+t]: one 4 x 4 patch of
+// a rank-8 update (X, L column-major 64 x 64 in shared memory)
+__device__ __forceinline__ void patch_update(float* X, const float* L, int r0, int c0, int o) {
+    float acc[4][4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+        const float4 v = *reinterpret_cast<const float4*>(X + (c0 + jj) * kCT + r0);
+        acc[0][jj] = v.x;
+        acc[1][jj] = v.y;
+        acc[2][jj] = v.z;
+        acc[3][jj] = v.w;
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const float4 pv = *reinterpret_cast<const float4*>(X + (o + t) * kCT + r0);
+        const float4 qv = *reinterpret_cast<const float4*>(L + (o + t) * kCT + c0);
+        const float pa[4] = {pv.x, pv.y, pv.z, pv.w};
+        const float qa[4] = {qv.x, qv.y, qv.z, qv.w};
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fmaf(-pa[ii], qa[jj], acc[ii][jj]);
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+        *reinterpret_cast<float4*>(X + (c0 + jj) * kCT + r0) = make_float4(acc[0][jj], acc[1][jj], acc[2][jj], acc[3][jj]);
+}
+
+// Cholesky and inverse of the symmetric positive definite 64 x 64 tile S
+// (column-major, lower triangle read), as ONE panel [S; E] with E = I:
+// S <- L (zeros above the diagonal), E <- I L^-T = L^-T (column-major, i.e.
+// L^-1 row-major), rinv <- 1/diag(L).  Blocks of 8 columns, all 8 warps:
+// after the column block bb is solved (one thread per panel row that is not
+// zero in it: the rows of S below the block and rows 0..8bb+7 of E, 64 in
+// all), warp 0 updates and factorises the next diagonal block while warps 1-7
+// apply the rank-8 update to the rest of the panel in 4 x 4 register patches
+// (consecutive threads on consecutive row patches of one column patch:
+// conflict-free rows, broadcast column operand).  Rows 8bb+8.. of E are
+// still the identity's in the columns of block bb and need no work.
+__device__ void potrf_inv64(float* S, float* E, float* rinv, float& pmin, float& pmax, int& bad, int nvalid) {
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-    if (w == 0) potrf8_warp(S, rinv, 0, pmin, pmax, bad, nvalid);
+    if (w == 0) {
+        potrf8_warp(S, rinv, 0, pmin, pmax, bad, nvalid);
+    } else {
+        for (int e = tid - 32; e < kCTE / 4; e += kCThreads - 32) {
+            const int col = e >> 4, r = (e & 15) * 4;
+            *reinterpret_cast<float4*>(E + 4 * e) =
+                make_float4(r == col ? 1.f : 0.f, r + 1 == col ? 1.f : 0.f, r + 2 == col ? 1.f : 0.f,
+                            r + 3 == col ? 1.f : 0.f);
+        }
+    }
     __syncthreads();
     for (int bb = 0; bb < 8; ++bb) {
-        const int o = 8 * bb, c0 = o + 8;
-        if (tid >= c0 && tid < kCT) subst_row8(S, S, rinv, bb, tid);
+        const int o = 8 * bb, c0 = o + 8, nd = kCT - c0;
+        if (tid < kCT) {
+            if (tid < nd) subst_row8(S, S, rinv, bb, c0 + tid);
+            else subst_row8(E, S, rinv, bb, tid - nd);
+        }
         __syncthreads();
         if (bb == 7) break;
         if (w == 0) {
@@ -296,88 +365,38 @@ __device__ void potrf64(float* S, float* rinv, float& pmin, float& pmax, int& ba
             __syncwarp();
             potrf8_warp(S, rinv, bb + 1, pmin, pmax, bad, nvalid);
         } else {
-            // 4 x 4 patches of rows and columns [c0, 64), lower triangle, without the next diagonal block
-            const int m = (kCT - c0) / 4;
-            for (int q = tid - 32; q < m * m; q += kCThreads - 32) {
-                const int pr = q / m, pc = q % m;
-                if (pr < pc || (pr < 2 && pc < 2)) continue;
-                const int r0 = c0 + 4 * pr, cc0 = c0 + 4 * pc;
-                float acc[4][4];
-#pragma unroll
-                for (int jj = 0; jj < 4; ++jj) {
-                    const float4 v = *reinterpret_cast<const float4*>(S + (cc0 + jj) * kCT + r0);
-                    acc[0][jj] = v.x;
-                    acc[1][jj] = v.y;
-                    acc[2][jj] = v.z;
-                    acc[3][jj] = v.w;
+            // E rows 0..c0-1 (2bb+2 row patches) x columns [c0, 64); then the lower triangle of S's
+            // rows and columns [c0, 64) without the next diagonal block
+            const int m = nd / 4, me = 2 * bb + 2, ne = me * m;
+            for (int q = tid - 32; q < ne + m * m; q += kCThreads - 32) {
+                if (q < ne) {
+                    patch_update(E, S, 4 * (q % me), c0 + 4 * (q / me), o);
+                } else {
+                    const int q2 = q - ne, pc = q2 / m, pr = q2 % m;
+                    if (pr < pc || (pr < 2 && pc < 2)) continue;
+                    patch_update(S, S, c0 + 4 * pr, c0 + 4 * pc, o);
                 }
-#pragma unroll
-                for (int t = 0; t < 8; ++t) {
-                    const float4 pv = *reinterpret_cast<const float4*>(S + (o + t) * kCT + r0);
-                    const float4 qv = *reinterpret_cast<const float4*>(S + (o + t) * kCT + cc0);
-                    const float pa[4] = {pv.x, pv.y, pv.z, pv.w};
-                    const float qa[4] = {qv.x, qv.y, qv.z, qv.w};
-#pragma unroll
-                    for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-                        for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fmaf(-pa[ii], qa[jj], acc[ii][jj]);
-                }
-#pragma unroll
-                for (int jj = 0; jj < 4; ++jj)
-                    *reinterpret_cast<float4*>(S + (cc0 + jj) * kCT + r0) =
-                        make_float4(acc[0][jj], acc[1][jj], acc[2][jj], acc[3][jj]);
             }
         }
         __syncthreads();
     }
-}
-
-// X = X L^-T in place (X column-major 64 x 64, L the column-major lower
-// factor tile, rinv = 1/diag(L)): for each block of 8 columns, the product
-// with the solved blocks (two entries per thread), then the substitution
-// inside the block (one thread per row).
-__device__ void trsm_subst(float* X, const float* L, const float* rinv) {
-    const int tid = threadIdx.x, r = tid & 63, cp = tid >> 6;   // cp: column pair 0..3
-    for (int bb = 0; bb < 8; ++bb) {
-        const int o = 8 * bb;
-        if (bb > 0) {
-            float v0 = X[(o + 2 * cp) * kCT + r], v1 = X[(o + 2 * cp + 1) * kCT + r];
-            for (int t = 0; t < o; ++t) {
-                const float xt = X[t * kCT + r];
-                v0 = fmaf(-xt, L[t * kCT + o + 2 * cp], v0);
-                v1 = fmaf(-xt, L[t * kCT + o + 2 * cp + 1], v1);
-            }
-            X[(o + 2 * cp) * kCT + r] = v0;
-            X[(o + 2 * cp + 1) * kCT + r] = v1;
-            __syncthreads();
-        }
-        if (tid < kCT) subst_row8(X, L, rinv, bb, tid);
-        __syncthreads();
-    }
-}
-
-// rinv = 1/diag(L) of a factor tile held in shared memory
-__device__ __forceinline__ void diag_recip(const float* L, float* rinv) {
-    if (threadIdx.x < kCT) rinv[threadIdx.x] = 1.0f / L[threadIdx.x * kCT + threadIdx.x];
 }
 
 // ---------------------------------------------------------------- worker tasks
 // Factorisation tasks, group g (0 <= g <= T-3), T-g of them: the TRSM tiles
 // (I, g) for I = g+2..T-1 (type 0), then the sub-diagonal (g+2, g+1) (type 1)
 // and the diagonal (g+2, g+2) (type 2), pre-updated through g.
-// Inverse tasks (when L^-1 is asked for): X_ii = L_ii^-1 (type 3, row i)
-// and X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj for j < i (type 4).
-// Global order, slot s = 0..T-1: [type 3 of row s][type 4 (s, j), j < s]
-// [factorisation group s].  A factorisation group s needs the diagonal
-// steps <= s and earlier groups; the diagonal step s needs groups <= s-1; a
-// row-s inverse task needs the diagonal step s, earlier rows of its column
-// and L tiles of row s, all from earlier slots: with every CTA resident,
-// no task waits on one behind it.
+// Inverse tasks (when L^-1 is asked for): X_ij = -X_ii sum_{k=j}^{i-1} L_ik
+// X_kj for j < i (type 4); the diagonal CTA forms X_ii = L_ii^-1.
+// Global order, slot s = 0..T-1: [type 4 (s, j), j < s][factorisation group
+// s].  A factorisation group s needs the diagonal steps <= s and earlier
+// groups; the diagonal step s needs groups <= s-1; a row-s inverse task
+// needs the diagonal step s, earlier rows of its column and L tiles of row
+// s, all from earlier slots: with every CTA resident, no task waits on one
+// behind it.
 __device__ __forceinline__ void task_of(int T, bool inv, int t, int& I, int& J, int& type) {
     for (int sl = 0; sl < T; ++sl) {
         if (inv) {
-            if (t == 0) { I = sl; J = sl; type = 3; return; }
-            --t;
             if (t < sl) { I = sl; J = t; type = 4; return; }
             t -= sl;
         }
@@ -396,7 +415,7 @@ __device__ __forceinline__ void task_of(int T, bool inv, int t, int& I, int& J, 
 }
 
 __device__ __forceinline__ int task_count(int T, bool inv) {
-    return (T >= 3 ? T * (T + 1) / 2 - 3 : 0) + (inv ? T + T * (T - 1) / 2 : 0);
+    return (T >= 3 ? T * (T + 1) / 2 - 3 : 0) + (inv ? T * (T - 1) / 2 : 0);
 }
 
 // packed lower-triangular tile index of (i, j), i >= j
@@ -404,44 +423,36 @@ __device__ __forceinline__ int64_t packed_tile(int i, int j) { return (int64_t)i
 
 struct CholSmem {
     float a[2][kCTE];     // worker: operand L_Ik' (double buffer); diagonal CTA: current and next diagonal tile
-    float b[2][kCTE];     // worker: operand L_Jk' (double buffer), then L_JJ; diagonal CTA: sub-diagonal tile
-    float x[kCTE];        // worker: the task's tile (staging)
+    float b[2][kCTE];     // worker: operand L_Jk' (double buffer), then L_JJ^-1; diagonal CTA: sub-diagonal tile
+    float x[kCTE];        // worker: the task's tile (staging); diagonal CTA: L_kk^-T
     float rinv[kCT];
     int ok;
 };
 
-// packed tile (i, j) of L^-1 (row-major) into shared memory, one cp.async group
-__device__ __forceinline__ void load_packed(const CholCtx& c, float* s, int i, int j) {
-    const float* src = c.Xinv + packed_tile(i, j) * kCTE;
+// 64 x 64 floats at src (16-byte aligned) into shared memory, one cp.async group
+__device__ __forceinline__ void load_flat(float* s, const float* src) {
     for (int e = threadIdx.x; e < kCTE / 4; e += kCThreads) cp_async16(s + 4 * e, src + 4 * e);
     cp_async_commit();
 }
 
-// shared tile s (row-major 64 x 64) into packed tile (i, j)
-__device__ __forceinline__ void store_packed(const CholCtx& c, const float* s, int i, int j) {
-    float* dst = c.Xinv + packed_tile(i, j) * kCTE;
+// shared 64 x 64 floats to global dst (16-byte aligned)
+__device__ __forceinline__ void store_flat(float* dst, const float* s) {
     for (int e = threadIdx.x; e < kCTE / 4; e += kCThreads)
         __stcg(reinterpret_cast<float4*>(dst) + e, reinterpret_cast<const float4*>(s)[e]);
 }
 
-// Type 3: X_ii = L_ii^-1 into the packed inverse (row-major) and Dinv
-// (column-major).  X <- I L^-T = L^-T column-major, which is L^-1 row-major.
-__device__ bool task_diag_inverse(const CholCtx& c, CholSmem& sm, int i) {
-    if (!cta_wait(c, c.tflag + i * c.T + i, 2u, &sm.ok)) return false;
-    load_tile(c, sm.b[0], i, i);
-    for (int e = threadIdx.x; e < kCTE; e += kCThreads) sm.x[e] = (e >> 6) == (e & 63) ? 1.f : 0.f;
-    cp_async_wait_all();
-    __syncthreads();
-    diag_recip(sm.b[0], sm.rinv);
-    __syncthreads();
-    trsm_subst(sm.x, sm.b[0], sm.rinv);
-    store_packed(c, sm.x, i, i);
-    for (int e = threadIdx.x; e < kCTE; e += kCThreads) {
-        const int cc = e >> 6, r = e & 63;
-        __stcg(c.Dinv + (int64_t)i * kCTE + e, sm.x[r * kCT + cc]);
-    }
-    cta_publish(c.xflag + i * c.T + i, 1u);
-    return true;
+__device__ __forceinline__ void acc_zero(float (&acc)[4][4]) {
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = 0.f;
+}
+
+__device__ __forceinline__ void acc_neg(float (&acc)[4][4]) {
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = -acc[p][q];
 }
 
 // Type 4: X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj, operands double-buffered as
@@ -450,16 +461,12 @@ __device__ bool task_offdiag_inverse(const CholCtx& c, CholSmem& sm, int i, int 
     const int T = c.T;
     const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
     float acc[4][4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[p][q] = 0.f;
+    acc_zero(acc);
     const int n = i - j;     // k = j .. i-1
     if (!cta_wait(c, c.tflag + i * T + j, 2u, &sm.ok)) return false;
     if (!cta_wait(c, c.xflag + j * T + j, 1u, &sm.ok)) return false;
-    __syncthreads();
     load_tile(c, sm.a[0], i, j);
-    load_packed(c, sm.b[0], j, j);
+    load_flat(sm.b[0], c.Xinv + packed_tile(j, j) * kCTE);
     for (int q = 0; q < n; ++q) {
         const int k = j + q, nb = (q + 1) & 1;
         bool next = false;
@@ -467,7 +474,7 @@ __device__ bool task_offdiag_inverse(const CholCtx& c, CholSmem& sm, int i, int 
             next = cta_ready(c.tflag + i * T + k + 1, 2u, &sm.ok) && cta_ready(c.xflag + (k + 1) * T + j, 1u, &sm.ok);
             if (next) {
                 load_tile(c, sm.a[nb], i, k + 1);
-                load_packed(c, sm.b[nb], k + 1, j);
+                load_flat(sm.b[nb], c.Xinv + packed_tile(k + 1, j) * kCTE);
             }
         }
         if (next) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
@@ -479,31 +486,27 @@ __device__ bool task_offdiag_inverse(const CholCtx& c, CholSmem& sm, int i, int 
             if (!cta_wait(c, c.tflag + i * T + k + 1, 2u, &sm.ok)) return false;
             if (!cta_wait(c, c.xflag + (k + 1) * T + j, 1u, &sm.ok)) return false;
             load_tile(c, sm.a[nb], i, k + 1);
-            load_packed(c, sm.b[nb], k + 1, j);
+            load_flat(sm.b[nb], c.Xinv + packed_tile(k + 1, j) * kCTE);
         }
     }
-    // acc = -S; X_ij = -X_ii S: with P = Dinv_i (column-major) and Q = acc
-    // (row-major), sub_ptq gives -Dinv_i (-S) ... negated below
+    // acc = -S.  With P = -S row-major and Q = X_ii row-major, sub_pq_rowq
+    // gives out[a][b] = sum_t S[t][a] X_ii[b][t] = (X_ii S)[b][a]; X_ij = -(X_ii S)
     if (!cta_wait(c, c.xflag + i * T + i, 1u, &sm.ok)) return false;
+    load_flat(sm.b[0], c.Xinv + packed_tile(i, i) * kCTE);
 #pragma unroll
     for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) sm.x[(4 * tr + p) * kCT + 4 * tc + q] = acc[p][q];
-    for (int e = threadIdx.x; e < kCTE; e += kCThreads) sm.b[0][e] = __ldcg(c.Dinv + (int64_t)i * kCTE + e);
+        *reinterpret_cast<float4*>(sm.x + (4 * tr + p) * kCT + 4 * tc) =
+            make_float4(acc[p][0], acc[p][1], acc[p][2], acc[p][3]);
+    cp_async_wait_all();
     __syncthreads();
     float out[4][4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) out[p][q] = 0.f;
-    sub_ptq(out, sm.b[0], sm.x, tr, tc, 0, kCT);     // out = -Dinv_i (-S) = Dinv_i S
+    acc_zero(out);
+    sub_pq_rowq(out, sm.x, sm.b[0], tr, tc);
     __syncthreads();
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) sm.x[(4 * tr + p) * kCT + 4 * tc + q] = -out[p][q];
+    acc_neg(out);
+    acc_to(out, sm.x, tr, tc);     // X_ij[4tc+q][4tr+p] at (4tc+q)*64 + 4tr+p: row-major
     __syncthreads();
-    store_packed(c, sm.x, i, j);
+    store_flat(c.Xinv + packed_tile(i, j) * kCTE, sm.x);
     cta_publish(c.xflag + i * T + j, 1u);
     return true;
 }
@@ -517,10 +520,6 @@ __device__ void worker(const CholCtx& c, CholSmem& sm) {
     for (int t = wid; t < ntask; t += W) {
         int I, J, type;
         task_of(T, inv, t, I, J, type);
-        if (type == 3) {
-            if (!task_diag_inverse(c, sm, I)) return;
-            continue;
-        }
         if (type == 4) {
             if (!task_offdiag_inverse(c, sm, I, J)) return;
             continue;
@@ -570,30 +569,37 @@ __device__ void worker(const CholCtx& c, CholSmem& sm) {
         __syncthreads();
         acc_to(acc, sm.x, tr, tc);
         if (type == 0) {
-            // TRSM with the published diagonal factor L_JJ
+            // TRSM as a product with the published L_JJ^-T: L_IJ = A_IJ L_JJ^-T
             if (!cta_wait(c, c.tflag + J * T + J, 2u, &sm.ok)) return;
-            load_tile(c, sm.b[0], J, J);
+            load_flat(sm.b[0], c.Dinv + (int64_t)J * kCTE);
             cp_async_wait_all();
             __syncthreads();
-            diag_recip(sm.b[0], sm.rinv);
+            float out[4][4];
+            acc_zero(out);
+            sub_pq_rowq(out, sm.x, sm.b[0], tr, tc);
             __syncthreads();
-            trsm_subst(sm.x, sm.b[0], sm.rinv);
-        } else {
-            __syncthreads();
+            acc_neg(out);
+            acc_to(out, sm.x, tr, tc);
         }
+        __syncthreads();
         store_tile(c, sm.x, I, J);
         cta_publish(c.tflag + I * T + J, type == 0 ? 2u : 1u);
     }
 }
 
+// Step k: the panel factorisation of the diagonal tile (L_kk and its
+// inverse, published together), the sub-diagonal tile as a product with
+// L_kk^-T, and the next diagonal tile's last update.
 __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
     const int T = c.T;
     const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool inv = c.Xinv != nullptr;
     float pmin = 3.4e38f, pmax = 0.f;
     int bad = 0;
     int cur = 0;                         // sm.a[cur]: the diagonal tile of this step
     float* X = sm.b[1];
+    float* E = sm.x;
     load_tile(c, sm.a[0], 0, 0);
     cp_async_wait_all();
     __syncthreads();
@@ -609,18 +615,30 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
             hy = k < 1 || cta_ready(c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok);
             if (hy) load_tile(c, Y, k + 1, k + 1);
         }
-        potrf64(D, sm.rinv, pmin, pmax, bad, c.K - k * kCT);
+        potrf_inv64(D, E, sm.rinv, pmin, pmax, bad, c.K - k * kCT);
         store_tile(c, D, k, k);
+        store_flat(c.Dinv + (int64_t)k * kCTE, E);
+        if (inv) store_flat(c.Xinv + packed_tile(k, k) * kCTE, E);
         cta_publish(c.tflag + k * T + k, 2u);
+        if (inv && threadIdx.x == 0) c_st_release(c.xflag + k * T + k, 1u);
         if (k + 1 >= T) break;
-        // sub-diagonal tile: the workers applied updates k' < k (none when k = 0)
+        // sub-diagonal tile: the workers applied updates k' < k (none when k = 0);
+        // L_{k+1,k} = X L_kk^-T
         if (!hx) {
             if (!cta_wait(c, c.tflag + (k + 1) * T + k, 1u, &sm.ok)) return;
             load_tile(c, X, k + 1, k);
         }
         cp_async_wait_all();
         __syncthreads();
-        trsm_subst(X, D, sm.rinv);
+        {
+            float out[4][4];
+            acc_zero(out);
+            sub_pq_rowq(out, X, E, tr, tc);
+            __syncthreads();
+            acc_neg(out);
+            acc_to(out, X, tr, tc);
+        }
+        __syncthreads();
         store_tile(c, X, k + 1, k);
         cta_publish(c.tflag + (k + 1) * T + k, 2u);
         // next diagonal tile: the workers applied updates k' < k; this CTA applies k
@@ -661,31 +679,6 @@ __global__ void __launch_bounds__(kCThreads, 1) chol_tiles_kernel(CholCtx c) {
     else worker(c, sm);
 }
 
-// Dinv tile k = L_kk^-1 (column-major) for the triangular solves, one block
-// per diagonal tile: X = I, X <- X L^-T = L^-T, stored transposed.
-__global__ void __launch_bounds__(kCThreads) chol_dinv_kernel(const float* __restrict__ A, int64_t ld, int K,
-                                                             float* __restrict__ Dinv) {
-    __shared__ __align__(16) float L[kCTE];
-    __shared__ __align__(16) float X[kCTE];
-    __shared__ float rinv[kCT];
-    const int k = blockIdx.x;
-    for (int e = threadIdx.x; e < kCTE; e += kCThreads) {
-        const int cc = e >> 6, r = e & 63;
-        const int gr = k * kCT + r, gc = k * kCT + cc;
-        L[e] = (gr < K && gc < K) ? (r >= cc ? A[(int64_t)gc * ld + gr] : 0.f) : (gr == gc ? 1.f : 0.f);
-        X[e] = r == cc ? 1.f : 0.f;
-    }
-    __syncthreads();
-    diag_recip(L, rinv);
-    __syncthreads();
-    trsm_subst(X, L, rinv);
-    // X = L^-T: (L^-1)[r][c] = X[c][r]; Dinv column-major: Dinv[c*64 + r] = (L^-1)[r][c] = X[r*64 + c]
-    for (int e = threadIdx.x; e < kCTE; e += kCThreads) {
-        const int cc = e >> 6, r = e & 63;
-        Dinv[(int64_t)k * kCTE + e] = X[r * kCT + cc];
-    }
-}
-
 static int chol_tiles(int K) { return (K + kCT - 1) / kCT; }
 
 }  // namespace vtb
@@ -710,7 +703,7 @@ static int chol_launch(float* A, int64_t ld, int K, float* Dinv, float* Linv, vo
                        int32_t* status, double* pivots, double rcond, void* stream) {
     VTB_CHECK_ARG(K > 0 && ld >= K && A && Dinv && work && status);
     VTB_CHECK_ARG(work_bytes >= vtb_chol_work_bytes(K) && ((uintptr_t)work & 255) == 0);
-    VTB_CHECK_ARG(((uintptr_t)Linv & 15) == 0);
+    VTB_CHECK_ARG(((uintptr_t)Linv & 15) == 0 && ((uintptr_t)Dinv & 15) == 0);
     int dev = 0;
     VTB_CUDA_TRY(cudaGetDevice(&dev));
     int coop = 0, nsm = 0;
@@ -723,7 +716,7 @@ static int chol_launch(float* A, int64_t ld, int K, float* Dinv, float* Linv, vo
     VTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chol_tiles_kernel, kCThreads, sm));
     if (per_sm < 1) return VTB_CUDA_ERR;
     const int T = chol_tiles(K);
-    const int ntask = (T >= 3 ? T * (T + 1) / 2 - 3 : 0) + (Linv ? T + T * (T - 1) / 2 : 0);
+    const int ntask = (T >= 3 ? T * (T + 1) / 2 - 3 : 0) + (Linv ? T * (T - 1) / 2 : 0);
     const int grid = 1 + std::max(1, std::min(nsm - 1, ntask));
     cudaStream_t s = as_stream(stream);
     const int64_t fbytes = ((int64_t)T * T * 4 + 255) & ~(int64_t)255;
@@ -744,16 +737,14 @@ static int chol_launch(float* A, int64_t ld, int K, float* Dinv, float* Linv, vo
     c.Xinv = Linv;
     void* args[] = {(void*)&c};
     VTB_CUDA_TRY(cudaLaunchCooperativeKernel((void*)chol_tiles_kernel, dim3(grid), dim3(kCThreads), args, sm, s));
-    // without the inverse tasks, the diagonal-tile inverses come from a second kernel
-    if (!Linv) chol_dinv_kernel<<<T, kCThreads, 0, s>>>(A, ld, K, Dinv);
     return launch_status();
 }
 
 // Float32 Cholesky of the symmetric positive definite K x K matrix A
 // (column-major, leading dimension ld; only the lower triangle is written:
 // A = L L^T with L over the lower triangle).  Dinv (vtb_chol_dinv_floats(K)
-// floats) receives the inverses of the 64 x 64 diagonal tiles of L for
-// vtb_chol_solve.  work: vtb_chol_work_bytes(K) bytes of scratch (cleared
+// floats, 16-byte aligned) receives the inverses of the 64 x 64 diagonal
+// tiles of L, row-major, for vtb_chol_solve.  work: vtb_chol_work_bytes(K) bytes of scratch (cleared
 // here).  status (device int32, cleared by the caller) receives 1 when a
 // pivot fails, 2 when max/min of the squared pivots reaches 1/rcond, 3 when
 // a wait between CTAs ran out; pivots (device, may be NULL) receives [min,
@@ -776,86 +767,134 @@ VTB_API int vtb_chol_factor_inverse(float* A, int64_t ld, int K, float* Dinv, fl
 
 namespace vtb {
 
-// y = L^-1 b and x = L^-T y with the packed inverse: block row i of y is
-// sum_{j <= i} X_ij b_j, block column j of x is sum_{i >= j} X_ij^T y_i.
-// Each block handles the pair of block rows (columns) b and T-1-b, so every
-// block streams about T/2 tiles; four threads share a row (column).
+// y = L^-1 b and x = L^-T y with the packed inverse X, one block per tile:
+// block (i, j) forms its tile's product with the vector (X_ij b_j forward,
+// X_ij^T y_i backward) into a partial, and the last block of a block row
+// (column) to finish -- counted by an atomic ticket -- adds the partials in
+// a fixed order, so the result does not depend on the block schedule.
 constexpr int kGThreads = 256;
 
-__global__ void __launch_bounds__(kGThreads) inv_lower_kernel(const float* __restrict__ X, int K,
-                                                              const double* __restrict__ b, float* __restrict__ y) {
-    __shared__ __align__(16) float bs[kSMaxT * kCT];
-    const int T = (K + kCT - 1) / kCT;
-    for (int e = threadIdx.x; e < T * kCT; e += kGThreads) bs[e] = e < K ? (float)b[e] : 0.f;
-    __syncthreads();
-    const int r = threadIdx.x >> 2, part = threadIdx.x & 3;
-    for (int h = 0; h < 2; ++h) {
-        const int i = h == 0 ? (int)blockIdx.x : T - 1 - (int)blockIdx.x;
-        if (h == 1 && i == (int)blockIdx.x) break;
-        float a0 = 0.f, a1 = 0.f;
-        for (int j = 0; j <= i; ++j) {
-            const float4* row = reinterpret_cast<const float4*>(X + packed_tile(i, j) * kCTE + r * kCT + 16 * part);
-            const float* bj = bs + j * kCT + 16 * part;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float4 v = __ldg(row + q);
-                a0 = fmaf(v.x, bj[4 * q], a0);
-                a1 = fmaf(v.y, bj[4 * q + 1], a1);
-                a0 = fmaf(v.z, bj[4 * q + 2], a0);
-                a1 = fmaf(v.w, bj[4 * q + 3], a1);
-            }
-        }
-        float acc = a0 + a1;
-        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        if (part == 0) y[i * kCT + r] = acc;
-    }
+__device__ __forceinline__ void unpack_tile(int t, int& i, int& j) {
+    i = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
+    while ((int64_t)i * (i + 1) / 2 > t) --i;
+    while ((int64_t)(i + 1) * (i + 2) / 2 <= t) ++i;
+    j = t - i * (i + 1) / 2;
 }
 
-__global__ void __launch_bounds__(kGThreads) inv_upper_kernel(const float* __restrict__ X, int K,
-                                                              const float* __restrict__ y, double* __restrict__ x) {
-    __shared__ __align__(16) float ys[kSMaxT * kCT];
-    const int T = (K + kCT - 1) / kCT;
-    for (int e = threadIdx.x; e < T * kCT; e += kGThreads) ys[e] = y[e];
-    __syncthreads();
-    const int cc = threadIdx.x >> 2, part = threadIdx.x & 3;
-    for (int h = 0; h < 2; ++h) {
-        const int j = h == 0 ? (int)blockIdx.x : T - 1 - (int)blockIdx.x;
-        if (h == 1 && j == (int)blockIdx.x) break;
-        float a0 = 0.f, a1 = 0.f;
-        for (int i = j; i < T; ++i) {
-            const float* col = X + packed_tile(i, j) * kCTE + (16 * part) * kCT + cc;
-            const float* yi = ys + i * kCT + 16 * part;
-#pragma unroll
-            for (int t = 0; t < 16; t += 2) {
-                a0 = fmaf(__ldg(col + t * kCT), yi[t], a0);
-                a1 = fmaf(__ldg(col + (t + 1) * kCT), yi[t + 1], a1);
-            }
-        }
-        float acc = a0 + a1;
-        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        const int g = j * kCT + cc;
-        if (part == 0 && g < K) x[g] = (double)acc;
+__global__ void __launch_bounds__(kGThreads) inv_fwd_kernel(const float* __restrict__ X, int K,
+                                                            const double* __restrict__ b, float* __restrict__ part,
+                                                            float* __restrict__ y, unsigned* __restrict__ cnt) {
+    __shared__ float bs[kCT];
+    __shared__ int last;
+    const int t = blockIdx.x, tid = threadIdx.x;
+    int i, j;
+    unpack_tile(t, i, j);
+    if (tid < kCT) {
+        const int g = j * kCT + tid;
+        bs[tid] = g < K ? (float)b[g] : 0.f;
     }
+    __syncthreads();
+    const int r = tid >> 2, q = tid & 3;
+    const float4* row = reinterpret_cast<const float4*>(X + (int64_t)t * kCTE + r * kCT + 16 * q);
+    float4 v[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) v[e] = __ldg(row + e);
+    float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const float* bq = bs + 16 * q + 4 * e;
+        a0 = fmaf(v[e].x, bq[0], a0);
+        a1 = fmaf(v[e].y, bq[1], a1);
+        a0 = fmaf(v[e].z, bq[2], a0);
+        a1 = fmaf(v[e].w, bq[3], a1);
+    }
+    float acc = a0 + a1;
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    if (q == 0) part[(int64_t)t * kCT + r] = acc;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(cnt + i, 1u) == (unsigned)i;      // row i has i + 1 tiles
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (tid < kCT) {
+        float sum = 0.f;
+        for (int jj = 0; jj <= i; ++jj) sum += __ldcg(part + ((int64_t)i * (i + 1) / 2 + jj) * kCT + tid);
+        y[i * kCT + tid] = sum;
+    }
+    if (tid == 0) cnt[i] = 0u;
+}
+
+__global__ void __launch_bounds__(kGThreads) inv_bwd_kernel(const float* __restrict__ X, int K, int T,
+                                                            const float* __restrict__ y, float* __restrict__ part,
+                                                            double* __restrict__ x, unsigned* __restrict__ cnt) {
+    __shared__ float ys[kCT];
+    __shared__ float red[4][kCT];
+    __shared__ int last;
+    const int t = blockIdx.x, tid = threadIdx.x;
+    int i, j;
+    unpack_tile(t, i, j);
+    if (tid < kCT) ys[tid] = y[i * kCT + tid];
+    __syncthreads();
+    const int c = tid & 63, rq = tid >> 6;
+    const float* col = X + (int64_t)t * kCTE + (16 * rq) * kCT + c;
+    float v[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) v[e] = __ldg(col + e * kCT);
+    float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+    for (int e = 0; e < 16; e += 2) {
+        a0 = fmaf(v[e], ys[16 * rq + e], a0);
+        a1 = fmaf(v[e + 1], ys[16 * rq + e + 1], a1);
+    }
+    red[rq][c] = a0 + a1;
+    __syncthreads();
+    if (tid < kCT) part[(int64_t)t * kCT + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(cnt + T + j, 1u) == (unsigned)(T - 1 - j);   // column j has T - j tiles
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (tid < kCT) {
+        float sum = 0.f;
+        for (int ii = j; ii < T; ++ii) sum += __ldcg(part + ((int64_t)ii * (ii + 1) / 2 + j) * kCT + tid);
+        const int g = j * kCT + tid;
+        if (g < K) x[g] = (double)sum;
+    }
+    if (tid == 0) cnt[T + j] = 0u;
 }
 
 }  // namespace vtb
 
+VTB_API int64_t vtb_chol_solve_inverse_bytes(int K) {
+    if (K <= 0) return 0;
+    const int64_t T = chol_tiles(K);
+    return (T * (T + 1) / 2 * kCT + T * kCT) * 4 + 2 * T * 4;
+}
+
 // x = L^-T L^-1 x (x float64 in and out, float32 arithmetic) with the packed
-// inverse of vtb_chol_factor_inverse: two triangular matrix-vector products
-// over the tiles, each read once (L2-resident at the GPU configuration).
-// y_work: ceil(K/64)*64 floats of scratch.  K <= 10240.  Replaces spotrs
-// in the mixed decoder's solve (linalg.py:591-631).  Stream-ordered.
-VTB_API int vtb_chol_solve_inverse(const float* Linv, int K, double* x, float* y_work, void* stream) {
-    VTB_CHECK_ARG(K > 0 && K <= kSMaxT * kCT && Linv && x && y_work && ((uintptr_t)Linv & 15) == 0);
-    const int T = (K + kCT - 1) / kCT;
+// inverse of vtb_chol_factor_inverse: two triangular matrix-vector products,
+// one block per tile of X, every tile read once.  work:
+// vtb_chol_solve_inverse_bytes(K) bytes, 4-byte aligned, ZEROED before the
+// first call (each call leaves its counters zeroed again); calls sharing a
+// work buffer must be stream-ordered.  Replaces spotrs in the mixed
+// decoder's solve (linalg.py:591-631).  Stream-ordered.
+VTB_API int vtb_chol_solve_inverse(const float* Linv, int K, double* x, void* work, int64_t work_bytes,
+                                   void* stream) {
+    VTB_CHECK_ARG(K > 0 && Linv && x && work && ((uintptr_t)Linv & 15) == 0 && ((uintptr_t)work & 3) == 0);
+    VTB_CHECK_ARG(work_bytes >= vtb_chol_solve_inverse_bytes(K));
+    const int T = chol_tiles(K);
+    const int nt = T * (T + 1) / 2;
+    float* part = reinterpret_cast<float*>(work);
+    float* y = part + (int64_t)nt * kCT;
+    unsigned* cnt = reinterpret_cast<unsigned*>(y + T * kCT);
     cudaStream_t s = as_stream(stream);
-    const int grid = (T + 1) / 2;
-    inv_lower_kernel<<<grid, kGThreads, 0, s>>>(Linv, K, x, y_work);
+    inv_fwd_kernel<<<nt, kGThreads, 0, s>>>(Linv, K, x, part, y, cnt);
     int st = launch_status();
     if (st) return st;
-    inv_upper_kernel<<<grid, kGThreads, 0, s>>>(Linv, K, y_work, x);
+    inv_bwd_kernel<<<nt, kGThreads, 0, s>>>(Linv, K, T, y, part, x, cnt);
     return launch_status();
 }
 
@@ -960,7 +999,7 @@ __global__ void __launch_bounds__(kSThreads, 1) chol_solve_kernel(const float* _
         if (own) {
             if (j >= 1) load_rows(A, ld, K, j, j - 1, crit);
 #pragma unroll
-            for (int i = 0; i < 16; ++i) dv[i] = __ldcg(Dinv + (int64_t)j * kCTE + (16 * part + i) * kCT + rc);
+            for (int i = 0; i < 16; ++i) dv[i] = __ldcg(Dinv + (int64_t)j * kCTE + rc * kCT + 16 * part + i);
         }
         const int mstart = (j + 1 - (int)q + (int)C - 1) / (int)C;  // first own row k = q + C m > j
         if (j >= 1) {
@@ -1014,7 +1053,7 @@ __global__ void __launch_bounds__(kSThreads, 1) chol_solve_kernel(const float* _
         if (own) {
             if (has) load_cols(A, ld, K, j + 1, j, crit);
 #pragma unroll
-            for (int i = 0; i < 16; ++i) dv[i] = __ldcg(Dinv + (int64_t)j * kCTE + rc * kCT + 16 * part + i);
+            for (int i = 0; i < 16; ++i) dv[i] = __ldcg(Dinv + (int64_t)j * kCTE + (16 * part + i) * kCT + rc);
         }
         // own rows k < j, in increasing k: k = q + C m for m < mend
         const int mend = (j - (int)q + (int)C - 1) / (int)C;         // own k < j  <=>  m < mend

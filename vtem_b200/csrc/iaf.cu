@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
     __shared__ double s_area[kIafWarps][32];
     __shared__ double s_y1[kIafWarps][32];
     __shared__ double s_y2[kIafWarps][32];
+    __shared__ double s_v[kIafWarps][32];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -122,43 +123,61 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
         __syncwarp();
         const int nst = min(32, steps - t0);
         // Fast chunk: every step of the 32 has the positive-slope form and at
-        // most one frame-block boundary falls inside.  All lanes run the
+        // most one frame-block boundary falls inside.  The warp runs the
         // membrane and time recursions v += area_j, tc += dt in the
-        // reference's order as one register chain (the areas arrive by
-        // shuffle, off the chain's critical path), lane j keeping the value
-        // after step j; a ballot then finds the first crossing.  Steps before
-        // it are final as computed (the same float64 operations in the same
-        // order as the step loop below); the crossing step and the rest of
-        // the chunk run through the step loop from the exact state.
+        // reference's order as one register chain (uniform across lanes: the
+        // areas are shared-memory broadcasts, off the chain's critical path),
+        // storing the membrane value after each step; lane j then tests step
+        // j's value and a ballot finds the first crossing.  Steps before it
+        // are final as computed (the same float64 operations in the same
+        // order as the step loop below); tc at the step before the crossing
+        // is recomputed by the same additions, and the crossing step and the
+        // rest of the chunk run through the step loop from the exact state.
         int jstart = 0;
         if (nst == 32 && posmask == full && (bstep >= 32 || bstep <= 0)) {
             const int rpos = (next_reset >= t0 && next_reset < t0 + 32) ? next_reset - t0 : -1;
-            double v = v0, tt = tc, s_l = 0.0, t_l = 0.0;
+            double v = v0, tt = tc;
+            if (rpos < 0) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const double aj = __shfl_sync(full, areal, j);
-                if (j == rpos) tt = 0.0;
-                v = v + aj;
-                tt = tt + dt;
-                if (lane == j) {
-                    s_l = v;
-                    t_l = tt;
+                for (int j = 0; j < 32; ++j) {
+                    v = v + s_area[w][j];
+                    tt = tt + dt;
+                    s_v[w][j] = v;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    if (j == rpos) tt = 0.0;
+                    v = v + s_area[w][j];
+                    tt = tt + dt;
+                    s_v[w][j] = v;
                 }
             }
+            __syncwarp();
+            const double s_l = s_v[w][lane];
             const unsigned cross = __ballot_sync(full, s_l >= delta);
             const unsigned nearm = __ballot_sync(full, fabs(s_l - delta) < p.near_eps);
             const int f = cross ? __ffs(cross) - 1 : 32;
             near += (unsigned long long)__popc(f < 32 ? (nearm & ((1u << f) - 1u)) : nearm);
-            if (f > 0) {
-                v0 = __shfl_sync(full, s_l, f - 1);
-                tc = __shfl_sync(full, t_l, f - 1);
-                if (rpos >= 0 && rpos < f) {
-                    cnt_block = 0;
-                    ++block;
-                    next_reset += bstep;
-                    lim_block = block_limit(block);
+            if (f == 32) {
+                v0 = v;
+                tc = tt;
+            } else if (f > 0) {
+                v0 = s_v[w][f - 1];
+                double t2 = tc;
+                for (int j = 0; j < f; ++j) {
+                    if (j == rpos) t2 = 0.0;
+                    t2 = t2 + dt;
                 }
+                tc = t2;
             }
+            if (f > 0 && rpos >= 0 && rpos < f) {
+                cnt_block = 0;
+                ++block;
+                next_reset += bstep;
+                lim_block = block_limit(block);
+            }
+            __syncwarp();
             jstart = f;
         }
         for (int j = jstart; j < nst; ++j) {

@@ -15,8 +15,9 @@
 // weights: 2Mt+1 = 17 float64 FMAs per voxel at the GPU configuration,
 // against the 8 bytes the voxel costs in HBM.
 //
-//   basis_kernel: H, one thread per pixel and block per m (Ks complex MACs
-//     per pixel and m; ex/ey of the period grid in shared memory, with the
+//   basis_kernel: H, a block per m and 64 x 4 pixel tile: the row sums of
+//     the coefficient grid over the tile's columns, then 2(2My+1) complex
+//     MACs per pixel (ex/ey of the period grid in shared memory, with the
 //     (-1)^(mx+my) signs and crop offsets of the decode grid).
 //   harmonics_kernel: U.  A block owns 256 * kHPix consecutive pixels and a
 //     range of frames; each thread keeps its kHPix pixels' Kt weights in
@@ -38,64 +39,111 @@ __device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// H[p * ldh + k]: k = 0 -> Re B_0, k = 2m-1 -> Re P_m, k = 2m -> -Im P_m
-__global__ void __launch_bounds__(256) basis_kernel(const double2* __restrict__ a, const int32_t* __restrict__ smap,
-                                                    int Ks, int Mx, int My, int Mt, int Px, int Py, int Px1, int Py1,
-                                                    double* __restrict__ H, int ldh) {
+// H[p * ldh + k]: k = 0 -> Re B_0, k = 2m-1 -> Re P_m, k = 2m -> -Im P_m.
+// The spatial sum is separable over the rows of the coefficient grid:
+//   P_m(px, py) = sum_rr [ey[rr][py] Gp[rr][px] + conj(ey[rr][py]) Gn[rr][px]],
+//   Gp[rr][px] = sum_{s in row rr} a[s][m] ex[c(s)][px],
+//   Gn[rr][px] = sum_{s in row rr} conj(a[s][-m]) conj(ex[c(s)][px]),
+// so a block (one m, a tile of kBX x kBY pixels) first forms the row sums of
+// its columns, then two complex MACs per pixel and row.
+constexpr int kBX = 64;           // pixel columns per block
+constexpr int kBY = 4;            // pixel rows per block
+
+__global__ void __launch_bounds__(kBX * kBY) basis_kernel(const double2* __restrict__ a,
+                                                          const int32_t* __restrict__ smap, int Ks, int Mx, int My,
+                                                          int Mt, int Px, int Py, int Px1, int Py1,
+                                                          double* __restrict__ H, int ldh) {
     extern __shared__ double2 bs[];
     const int Kx = 2 * Mx + 1, Ky = 2 * My + 1, Kt = 2 * Mt + 1;
     const int m = blockIdx.y;                       // 0..Mt
-    double2* ex = bs;                               // Kx x Px
-    double2* ey = ex + Kx * Px;                     // Ky x Py
-    double2* am = ey + Ky * Py;                     // Ks: a[s][m]
+    const int tilesx = (Px + kBX - 1) / kBX;
+    const int x0 = (blockIdx.x % tilesx) * kBX, y0 = (blockIdx.x / tilesx) * kBY;
+    double2* ex = bs;                               // Kx x kBX
+    double2* gp = ex + Kx * kBX;                    // Ky x kBX
+    double2* gn = gp + Ky * kBX;                    // Ky x kBX
+    double2* ey = gn + Ky * kBX;                    // Ky x kBY
+    double2* am = ey + Ky * kBY;                    // Ks: a[s][m]
     double2* an = am + Ks;                          // Ks: conj a[s][-m]
+    int* srow = reinterpret_cast<int*>(an + Ks);    // Ks: row of entry s
+    int* scol = srow + Ks;                          // Ks: column of entry s
+    int* rlo = scol + Ks;                           // Ky: first / last entry of each row
+    int* rhi = rlo + Ky;
+    const int tid = threadIdx.x, nt = blockDim.x;
     const int xd = (Px1 - Px) / 2, yd = (Py1 - Py) / 2;
-    for (int e = threadIdx.x; e < Kx * Px; e += blockDim.x) {
-        const int c = e / Px, px = e % Px, mx = c - Mx;
-        const int64_t r = ((((int64_t)mx * (px + xd)) % Px1) + Px1) % Px1;
-        double s, co;
-        sincospi(2.0 * r / Px1, &s, &co);
+    for (int r = tid; r < Ky; r += nt) {
+        rlo[r] = Ks;
+        rhi[r] = -1;
+    }
+    for (int e = tid; e < Kx * kBX; e += nt) {
+        const int c = e / kBX, px = x0 + e % kBX, mx = c - Mx;
+        const int r = (((mx * (px + xd)) % Px1) + Px1) % Px1;
+        double sn, co;
+        sincospi(2.0 * r / Px1, &sn, &co);
         const double sg = (mx & 1) ? -1.0 : 1.0;
-        ex[e] = make_double2(sg * co, sg * s);
+        ex[e] = make_double2(sg * co, sg * sn);
     }
-    for (int e = threadIdx.x; e < Ky * Py; e += blockDim.x) {
-        const int rr = e / Py, py = e % Py, my = My - rr;   // storage row rr holds my = My - rr
-        const int64_t r = ((((int64_t)my * (py + yd)) % Py1) + Py1) % Py1;
-        double s, co;
-        sincospi(2.0 * r / Py1, &s, &co);
+    for (int e = tid; e < Ky * kBY; e += nt) {
+        const int rr = e / kBY, py = y0 + e % kBY, my = My - rr;   // storage row rr holds my = My - rr
+        const int r = (((my * (py + yd)) % Py1) + Py1) % Py1;
+        double sn, co;
+        sincospi(2.0 * r / Py1, &sn, &co);
         const double sg = (my & 1) ? -1.0 : 1.0;
-        ey[e] = make_double2(sg * co, sg * s);
+        ey[e] = make_double2(sg * co, sg * sn);
     }
-    for (int s = threadIdx.x; s < Ks; s += blockDim.x) {
+    __syncthreads();
+    for (int s = tid; s < Ks; s += nt) {
         am[s] = a[(int64_t)s * Kt + Mt + m];
         const double2 v = a[(int64_t)s * Kt + Mt - m];
         an[s] = make_double2(v.x, -v.y);
+        const int g = __ldg(smap + s), rr = g / Kx;
+        const bool ok = g >= 0 && rr < Ky;          // an index outside the grid contributes nothing
+        srow[s] = ok ? rr : -1;
+        scol[s] = ok ? g - rr * Kx : 0;
+        if (ok) {
+            atomicMin(rlo + rr, s);
+            atomicMax(rhi + rr, s);
+        }
     }
     __syncthreads();
-    const int P = Px * Py;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-        const int px = p % Px, py = p / Px;
-        // P_m(p) = sum_s (a[s][m] phi_s + conj(a[s][-m] phi_s)); for m = 0 only B_0
-        double2 acc = make_double2(0.0, 0.0);
-        for (int s = 0; s < Ks; ++s) {
-            const int g = __ldg(smap + s), rr = g / Kx, c = g - rr * Kx;
-            const double2 phi = c_mul(ey[rr * Py + py], ex[c * Px + px]);
-            const double2 t1 = c_mul(am[s], phi);
-            acc.x += t1.x;
-            acc.y += t1.y;
-            if (m > 0) {
-                const double2 t2 = c_mul(an[s], make_double2(phi.x, -phi.y));
-                acc.x += t2.x;
-                acc.y += t2.y;
-            }
+    // row sums of this block's columns
+    for (int e = tid; e < Ky * kBX; e += nt) {
+        const int rr = e / kBX, x = e % kBX;
+        double2 sp = make_double2(0.0, 0.0), sq = make_double2(0.0, 0.0);
+        for (int s = rlo[rr]; s <= rhi[rr]; ++s) {
+            if (srow[s] != rr) continue;
+            const double2 e1 = ex[scol[s] * kBX + x];
+            const double2 t1 = c_mul(am[s], e1);
+            sp.x += t1.x;
+            sp.y += t1.y;
+            const double2 t2 = c_mul(an[s], make_double2(e1.x, -e1.y));
+            sq.x += t2.x;
+            sq.y += t2.y;
         }
-        double* h = H + (int64_t)p * ldh;
-        if (m == 0) {
-            h[0] = acc.x;
-        } else {
-            h[2 * m - 1] = acc.x;
-            h[2 * m] = -acc.y;
+        gp[e] = sp;
+        gn[e] = sq;
+    }
+    __syncthreads();
+    const int x = tid % kBX, y = tid / kBX;
+    const int px = x0 + x, py = y0 + y;
+    if (px >= Px || py >= Py) return;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int rr = 0; rr < Ky; ++rr) {
+        const double2 e2 = ey[rr * kBY + y];
+        const double2 t1 = c_mul(e2, gp[rr * kBX + x]);
+        acc.x += t1.x;
+        acc.y += t1.y;
+        if (m > 0) {
+            const double2 t2 = c_mul(make_double2(e2.x, -e2.y), gn[rr * kBX + x]);
+            acc.x += t2.x;
+            acc.y += t2.y;
         }
+    }
+    double* h = H + ((int64_t)py * Px + px) * ldh;
+    if (m == 0) {
+        h[0] = acc.x;
+    } else {
+        h[2 * m - 1] = acc.x;
+        h[2 * m] = -acc.y;
     }
 }
 
@@ -204,15 +252,16 @@ VTB_API int vtb_coeff_basis(const double* a, const int32_t* smap, int Ks, int Mx
                             int Px1, int Py1, double* H, int ldh, void* stream) {
     VTB_CHECK_ARG(Ks > 0 && Mx >= 0 && My >= 0 && Mt >= 0 && Px > 0 && Py > 0 && Px1 >= Px && Py1 >= Py);
     VTB_CHECK_ARG(a && smap && H && ldh >= 2 * Mt + 1 && 2 * Mt + 1 <= kHMaxKt);
+    VTB_CHECK_ARG((int64_t)Mx * Px1 < (1LL << 30) && (int64_t)My * Py1 < (1LL << 30));
     const int Kx = 2 * Mx + 1, Ky = 2 * My + 1;
-    const size_t sm = (size_t)(Kx * Px + Ky * Py + 2 * Ks) * sizeof(double2);
+    const size_t sm = (size_t)(Kx * kBX + 2 * Ky * kBX + Ky * kBY + 2 * Ks) * sizeof(double2) +
+                      (size_t)(2 * Ks + 2 * Ky) * sizeof(int);
     VTB_CHECK_ARG(sm <= 200 * 1024);
     if (sm > 48 * 1024)
         VTB_CUDA_TRY(cudaFuncSetAttribute(basis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    const int P = Px * Py;
-    dim3 grid(ceil_div(P, 256), Mt + 1);
-    basis_kernel<<<grid, 256, sm, as_stream(stream)>>>(reinterpret_cast<const double2*>(a), smap, Ks, Mx, My, Mt, Px,
-                                                      Py, Px1, Py1, H, ldh);
+    dim3 grid(ceil_div(Px, kBX) * ceil_div(Py, kBY), Mt + 1);
+    basis_kernel<<<grid, kBX * kBY, sm, as_stream(stream)>>>(reinterpret_cast<const double2*>(a), smap, Ks, Mx, My, Mt,
+                                                            Px, Py, Px1, Py1, H, ldh);
     return launch_status();
 }
 

@@ -150,7 +150,8 @@ class CoeffDecoder(object):
         self._cwork = torch.empty(int(lib().vtb_chol_work_bytes(self.K)), dtype=torch.uint8, device=device)
         if self.mixed_factor == "inverse":
             self._clinv = torch.empty(int(lib().vtb_chol_inverse_floats(self.K)), dtype=torch.float32, device=device)
-            self._cy = torch.empty(((self.K + 63) // 64) * 64, dtype=torch.float32, device=device)
+            # product-solve scratch: partial sums and tickets (zeroed once; every solve leaves it zeroed)
+            self._cy = torch.zeros(int(lib().vtb_chol_solve_inverse_bytes(self.K)), dtype=torch.uint8, device=device)
 
     def set_norm(self, h_norm):
         """Per-neuron weights norm (vtem/vtdm.py:634-638, 1/(kappa sigma) for
@@ -249,7 +250,8 @@ class CoeffDecoder(object):
             call("vtb_chol_factor_inverse", dptr(self.Mr32), ld, K, dptr(self._cdinv), dptr(self._clinv),
                  dptr(self._cwork), self._cwork.numel(), self._stat_ptr(0), self._stat_ptr(1),
                  self.rcond * CHOL_MARGIN, s)
-            solve = lambda x: call("vtb_chol_solve_inverse", dptr(self._clinv), K, dptr(x), dptr(self._cy), s)
+            solve = lambda x: call("vtb_chol_solve_inverse", dptr(self._clinv), K, dptr(x), dptr(self._cy),
+                                   self._cy.numel(), s)
         elif self.mixed_factor == "tiles":
             # float32 tile Cholesky (one cooperative launch) and cluster solves
             call("vtb_chol_factor", dptr(self.Mr32), ld, K, dptr(self._cdinv), dptr(self._cwork),
