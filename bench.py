@@ -348,8 +348,9 @@ def gram_gemm_roofline(dec, peaks, reps=20):
     """The mixed decoder's tensor-core Kronecker Gram (the decode's tensor-
     bound kernel) timed alone with CUDA events on its own operands, at its
     autotuned tile width, against the measured bf16 peak.  Tensor work counts
-    the three split-bf16 products; the 158 MB RF-bank operand exceeds L2, so
-    repeated launches read it from HBM as a decode does."""
+    the three split-bf16 products (issued from [hi | lo] operand tiles); the
+    105 MB RF-bank operand exceeds L2, so repeated launches read it from HBM
+    as a decode does."""
     import torch
     from vtem_b200 import autotune
     from vtem_b200._abi import dptr, stream_ptr
@@ -357,8 +358,8 @@ def gram_gemm_roofline(dec, peaks, reps=20):
     s = stream_ptr()
 
     def once():
-        return autotune.gemm_bf16_tuned(dptr(dec.L3), M, dptr(dec.R3), KK, K, dptr(dec.C), KK, 1, 0, 1.0, 0,
-                                        dec._stat_ptr(7), s)
+        return autotune.gemm_bf16_tuned(dptr(dec.Lsplit), M, dptr(dec.Rsplit), KK, dec.Kp2, dptr(dec.C), KK, 1, 0, 1.0,
+                                        0, dec._stat_ptr(7), s, x3=True)
     bn = once()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -370,10 +371,10 @@ def gram_gemm_roofline(dec, peaks, reps=20):
     ms = e0.elapsed_time(e1) / reps
     flop = 2.0 * M * KK * K
     achieved = flop / (ms / 1e3) / 1e12
-    return {"bound": "tensor", "kernel": "tc_gemm_kernel<%d, float> (Kronecker Gram, split-bf16)" % bn,
+    return {"bound": "tensor", "kernel": "tc_gemm_kernel<%d, float, x3> (Kronecker Gram, three split-bf16 products)" % bn,
             "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
             "frac": achieved / peaks["bf16_tflops"], "peak_source": peaks["source"], "avg_ms": ms,
-            "tensor_flop": flop, "shape": [M, KK, K], "operand_bytes": M * K * 2 + KK * K * 2}
+            "tensor_flop": flop, "shape": [M, KK, K], "operand_bytes": (M + KK) * 2 * dec.Kp2 * 2}
 
 
 def serve_short(dev, requests=64, rate=200.0, seed=3):
@@ -689,12 +690,23 @@ def run_encode(w, V, dev, reps=5):
     Ltc, ttc = timed(lambda: bank.filter(V, out_layout="neuron", precision="bf16x3"))
     flop = 2.0 * w.F * w.Px * w.Py * w.N
 
-    def scan(L):
+    def encoder():
         iaf = ensemble_encode.IAF_encode(w.N, w.dt)
         iaf.load_parameters(h_kappa=w.kappa, h_bias=w.bias, h_delta=w.delta, h_v0=w.v0)
-        return iaf.encode_blocks(L, block_frames=min(101, w.F + 1), layout="neuron")
+        return iaf
 
-    sp64, tscan = timed(lambda: scan(L64))
+    def scan(L):
+        return encoder().encode_blocks(L, block_frames=min(101, w.F + 1), layout="neuron")
+
+    # the public call (overflow checks included) and the scan kernel alone, on one
+    # encoder whose state carries from call to call as the reference's does
+    enc = encoder()
+    bf = min(101, w.F + 1)
+    _, tscan = timed(lambda: enc.encode_blocks(L64, block_frames=bf, layout="neuron"))
+    # the scan kernel alone: one launch with the first-try spike buffer, no host check
+    cap0 = 64 + -(-w.F // ensemble_encode.SMALL_CAP_STRIDE)
+    _, tkernel = timed(lambda: enc._launch(L64, 1, w.F, w.N, w.F, bf, cap0, 0, block_rate=0.1))
+    sp64 = scan(L64)
     sptc = scan(Ltc)
     n64, ntc = int(sp64.count.sum()), int(sptc.count.sum())
     peaks = load_peaks()
@@ -702,7 +714,9 @@ def run_encode(w, V, dev, reps=5):
                               "f64_tflops": flop / t64 / 1e9, "tensor_core_tflops": flop / ttc / 1e9,
                               "tensor_core_frac_of_bf16_peak": 3 * flop / ttc / 1e9 / peaks["bf16_tflops"],
                               "tensor_core_rel_err": float((Ltc - L64).norm() / L64.norm())},
-            "iaf_scan": {"ms": tscan, "bytes_read": 8 * w.F * w.N, "gbs": 8.0 * w.F * w.N / tscan / 1e6,
+            "iaf_scan": {"ms": tscan, "kernel_ms": tkernel,
+                         "chain_floor_ms": w.F * 8.0 / (peaks.get("sm_max_mhz", 1965.0) * 1e3),
+                         "bytes_read": 8 * w.F * w.N, "gbs": 8.0 * w.F * w.N / tscan / 1e6,
                          "frac_of_hbm": 8.0 * w.F * w.N / tscan / 1e6 / peaks["hbm_gbs"],
                          "spikes": n64, "near_threshold": int(sp64.near_threshold)},
             "spikes_tensor_core_projection": ntc}

@@ -113,6 +113,18 @@ int vtb_tc_gemm_bf16(const void* A, int M, const void* B, int N, int K, void* C,
  * shape.  VTB_BAD_ARG for any other bn. */
 int vtb_tc_gemm_bf16_bn(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
                         int out_f64, double alpha, int accumulate, int32_t* err, int bn, void* stream);
+/* Split-bf16 operands of the three-product mode: dst[r][0:2Kp] = [hi | lo],
+ * Kp = K rounded up to 64, zero padded. */
+int vtb_split_bf16x2(const void* src, int src_f32, int rows, int K, int64_t ld, int64_t k_stride, double scale,
+                     void* dst, void* stream);
+/* Three-product split-bf16 GEMM: A (M x 2K) = [A_hi | A_lo], B (N x 2K) =
+ * [B_hi | B_lo] (vtb_split_bf16x2; K, the width of one part, a multiple of
+ * 64); C = alpha (A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T), every k-block's
+ * three products issued from the same shared-memory tiles: the result of
+ * vtb_tc_gemm_bf16_bn on the three-part layouts with two thirds of their
+ * operand bytes (the fp32 sums run in another order).  Same tile widths. */
+int vtb_tc_gemm_bf16x3_bn(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
+                          int out_f64, double alpha, int accumulate, int32_t* err, int bn, void* stream);
 
 /* ------------------------------------------------------------ IAF encoder */
 
@@ -293,6 +305,11 @@ int vtb_tc_group_build(void* host_desc, int nprob, const uint64_t* A, const int*
                        const int* K, const uint64_t* C, const int64_t* ldc, const uint64_t* err, int bn,
                        int* total_tiles);
 int vtb_tc_gemm_grouped(const void* dev_desc, int nprob, int total_tiles, int bn, void* stream);
+/* The same for the three-product mode (K_p the width of one operand part). */
+int vtb_tc_group_build_x3(void* host_desc, int nprob, const uint64_t* A, const int* M, const uint64_t* B,
+                          const int* N, const int* K, const uint64_t* C, const int64_t* ldc, const uint64_t* err,
+                          int bn, int* total_tiles);
+int vtb_tc_gemm_grouped_x3(const void* dev_desc, int nprob, int total_tiles, int bn, void* stream);
 
 /* Mixed-precision Kronecker Gram (tensor cores).  ps/ps2 list the npairs
  * spatial index pairs s <= s'.  L3 receives the RF-bank operand (2*npairs
@@ -303,6 +320,11 @@ int vtb_tc_gemm_grouped(const void* dev_desc, int nprob, int total_tiles, int bn
 int vtb_coeff_lhs_split(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs, void* L3,
                         void* stream);
 int vtb_coeff_wn_split(const double* Wn, int N, int Kt, void* R3, void* stream);
+/* The same operands as [hi | lo] (2*npairs x 2Kp and Kt*Kt x 2Kp) for
+ * vtb_tc_gemm_bf16x3_bn over K = Kp: the decoder's Gram. */
+int vtb_coeff_lhs_split2(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs, void* L2,
+                         void* stream);
+int vtb_coeff_wn_split2(const double* Wn, int N, int Kt, void* R2, void* stream);
 int vtb_coeff_scatter(const float* C, int64_t ldc, const int32_t* ps, const int32_t* ps2, int npairs, int Kt, double* M,
                       int64_t ldm, void* stream);
 

@@ -171,9 +171,9 @@ def test_real_form_matches_hermitian_system():
     call("vtb_coeff_unrealify_vec", dptr(x), K, 1, dptr(dec.a), 0, s)
     assert np.abs(dec.a.cpu().numpy() - a).max() <= 1e-9 * np.abs(a).max()
     # tensor-core Gram -> real form in float32
-    call("vtb_coeff_wn_split", dptr(dec.Wn), N, dec.Kt, dptr(dec.R3), s)
-    call("vtb_tc_gemm_bf16", dptr(dec.L3), 2 * dec.npairs, dptr(dec.R3), KK, 3 * dec.Kp2, dptr(dec.C), KK, 1, 0, 1.0,
-         0, dec._stat_ptr(7), s)
+    call("vtb_coeff_wn_split2", dptr(dec.Wn), N, dec.Kt, dptr(dec.Rsplit), s)
+    call("vtb_tc_gemm_bf16x3_bn", dptr(dec.Lsplit), 2 * dec.npairs, dptr(dec.Rsplit), KK, dec.Kp2, dptr(dec.C), KK, 1,
+         0, 1.0, 0, dec._stat_ptr(7), 128, s)
     ld = dec.ld32
     call("vtb_coeff_real_scatter", dptr(dec.C), KK, dec.Ks, dec.Kt, dptr(dec.Mr32), ld, 0, s)
     M32 = dec.Mr32[:, :K].double().cpu().numpy()

@@ -84,30 +84,33 @@ def test_autotuner_picks_a_candidate_and_caches_it():
     A = torch.as_tensor(rng.standard_normal((513, 200)), device="cuda")
     B = torch.as_tensor(rng.standard_normal((289, 200)), device="cuda")
     C1 = tc.gemm_split_bf16(A, B)
-    key = autotune._key(513, 289, tc.padded_k(200) * 3, True)
+    key = autotune._key(513, 289, tc.padded_k(200), True, x3=True)
     assert autotune._cache[key] in autotune.CANDIDATES
     C2 = tc.gemm_split_bf16(A, B)           # cached choice: same result
     assert torch.equal(C1, C2)
 
 
+@pytest.mark.parametrize("x3", [False, True])
 @pytest.mark.parametrize("bn", [64, 128, 256])
-def test_grouped_gemm_equals_single_launches(bn):
+def test_grouped_gemm_equals_single_launches(bn, x3):
     """One grouped launch over problems of uneven sizes gives each problem's
-    single-launch result bit for bit (same tiles, same accumulation order)."""
+    single-launch result bit for bit (same tiles, same accumulation order),
+    in the plain and the three-product mode."""
     from vtem_b200._abi import call, dptr, lib, stream_ptr
     rng = np.random.default_rng(bn + 1)
     shapes = [(300, 289, 384), (97, 49, 128), (513, 121, 192), (128, 225, 64), (40, 81, 256)]
+    parts = 2 if x3 else 1
+    single = "vtb_tc_gemm_bf16x3_bn" if x3 else "vtb_tc_gemm_bf16_bn"
     As, Bs, Cs, Cref, errs = [], [], [], [], []
     for (M, N, K) in shapes:
-        A = torch.as_tensor(rng.standard_normal((M, K)), device="cuda").to(torch.bfloat16).contiguous()
-        B = torch.as_tensor(rng.standard_normal((N, K)), device="cuda").to(torch.bfloat16).contiguous()
+        A = torch.as_tensor(rng.standard_normal((M, parts * K)), device="cuda").to(torch.bfloat16).contiguous()
+        B = torch.as_tensor(rng.standard_normal((N, parts * K)), device="cuda").to(torch.bfloat16).contiguous()
         As.append(A)
         Bs.append(B)
         Cs.append(torch.full((M, N), float("nan"), dtype=torch.float32, device="cuda"))
         Cref.append(torch.zeros((M, N), dtype=torch.float32, device="cuda"))
         errs.append(torch.zeros(1, dtype=torch.int32, device="cuda"))
-        call("vtb_tc_gemm_bf16_bn", dptr(A), M, dptr(B), N, K, dptr(Cref[-1]), N, 1, 0, 1.0, 0, dptr(errs[-1]), bn,
-             stream_ptr())
+        call(single, dptr(A), M, dptr(B), N, K, dptr(Cref[-1]), N, 1, 0, 1.0, 0, dptr(errs[-1]), bn, stream_ptr())
     n = len(shapes)
     u64 = np.uint64
     arr = [np.array([a.data_ptr() for a in As], u64), np.array([s[0] for s in shapes], np.int32),
@@ -116,10 +119,41 @@ def test_grouped_gemm_equals_single_launches(bn):
            np.array([s[1] for s in shapes], np.int64), np.array([e.data_ptr() for e in errs], u64)]
     host = np.zeros(int(lib().vtb_tc_group_bytes(n)), np.uint8)
     tiles = np.zeros(1, np.int32)
-    call("vtb_tc_group_build", host.ctypes.data, n, *[a.ctypes.data for a in arr], bn, tiles.ctypes.data)
+    call("vtb_tc_group_build_x3" if x3 else "vtb_tc_group_build", host.ctypes.data, n, *[a.ctypes.data for a in arr],
+         bn, tiles.ctypes.data)
     desc = torch.as_tensor(host).cuda()
-    call("vtb_tc_gemm_grouped", dptr(desc), n, int(tiles[0]), bn, stream_ptr())
+    call("vtb_tc_gemm_grouped_x3" if x3 else "vtb_tc_gemm_grouped", dptr(desc), n, int(tiles[0]), bn, stream_ptr())
     torch.cuda.synchronize()
     assert all(int(e.item()) == 0 for e in errs)
     for C, R in zip(Cs, Cref):
         assert torch.equal(C, R)
+
+
+@pytest.mark.parametrize("bn", [64, 96, 128, 160, 192, 256])
+def test_three_product_mode_every_tile_width(bn):
+    """vtb_tc_gemm_bf16x3_bn on [hi | lo] operands: the split-bf16 product
+    to the same accuracy as the three-part layout, and equal to it up to the
+    order of the fp32 sums, for every tile width (partial edge tiles in both
+    directions, several k-blocks)."""
+    from vtem_b200._abi import call, dptr, stream_ptr
+    rng = np.random.default_rng(100 + bn)
+    M, N, K = 300, 289, 320
+    A = torch.as_tensor(rng.standard_normal((M, K)), device="cuda")
+    B = torch.as_tensor(rng.standard_normal((N, K)), device="cuda")
+    A2, B2 = tc.split_bf16x2(A), tc.split_bf16x2(B)
+    A3, B3 = tc.split_bf16x3(A, 0), tc.split_bf16x3(B, 1)
+    Kp = tc.padded_k(K)
+    assert A2.shape == (M, 2 * Kp) and A3.shape == (M, 3 * Kp)
+    out2 = torch.zeros((M, N), dtype=torch.float32, device="cuda")
+    out3 = torch.zeros((M, N), dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    call("vtb_tc_gemm_bf16x3_bn", dptr(A2), M, dptr(B2), N, Kp, dptr(out2), N, 1, 0, 1.0, 0, dptr(err), bn,
+         stream_ptr())
+    call("vtb_tc_gemm_bf16_bn", dptr(A3), M, dptr(B3), N, 3 * Kp, dptr(out3), N, 1, 0, 1.0, 0, dptr(err), bn,
+         stream_ptr())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref = A @ B.T
+    rel = ((out2.double() - ref).norm() / ref.norm()).item()
+    assert rel < 5e-5, rel
+    assert (out2 - out3).abs().max().item() <= 1e-5 * ref.abs().max().item()

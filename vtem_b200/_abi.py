@@ -61,8 +61,12 @@ SIGNATURES = {
     "vtb_split_bf16x3": [P, I, I, I, L, L, D, I, P, P],
     "vtb_tc_gemm_bf16": [P, I, P, I, I, P, L, L, I, D, I, P, P],
     "vtb_tc_gemm_bf16_bn": [P, I, P, I, I, P, L, L, I, D, I, P, I, P],
+    "vtb_tc_gemm_bf16x3_bn": [P, I, P, I, I, P, L, L, I, D, I, P, I, P],
+    "vtb_split_bf16x2": [P, I, I, I, L, L, D, P, P],
     "vtb_coeff_lhs_split": [P, I, I, P, P, I, P, P],
     "vtb_coeff_wn_split": [P, I, I, P, P],
+    "vtb_coeff_lhs_split2": [P, I, I, P, P, I, P, P],
+    "vtb_coeff_wn_split2": [P, I, I, P, P],
     "vtb_coeff_scatter": [P, L, P, P, I, I, P, L, P],
     "vtb_coeff_rhs": [P, I, I, P, I, P, P],
     "vtb_coeff_residual": [P, P, P, I, I, P, P, P, P, I, D, P, I, P, P, P, P],
@@ -93,6 +97,8 @@ SIGNATURES = {
     "vtb_tc_group_bytes": [I],  # restype int64, set in lib()
     "vtb_tc_group_build": [P, I, P, P, P, P, P, P, P, P, I, P],
     "vtb_tc_gemm_grouped": [P, I, I, I, P],
+    "vtb_tc_group_build_x3": [P, I, P, P, P, P, P, P, P, P, I, P],
+    "vtb_tc_gemm_grouped_x3": [P, I, I, I, P],
     "vtb_sym_dinv_floats": [I],  # restype int64, set in lib()
     "vtb_chol_dinv_floats": [I],  # restype int64, set in lib()
     "vtb_chol_work_bytes": [I],  # restype int64, set in lib()

@@ -36,10 +36,12 @@ def _bucket(x):
     return max(0, int(x - 1).bit_length())
 
 
-def _key(M, N, K, out_f64):
+def _key(M, N, K, out_f64, x3=False):
     """Shape class: the exact column count (the tile waste depends on it) and
-    the row and reduction lengths rounded up to powers of two."""
-    return "%d,%d,%d,%d" % (_bucket(M), N, _bucket(K), int(bool(out_f64)))
+    the row and reduction lengths rounded up to powers of two; the
+    three-product mode is its own class."""
+    k = "%d,%d,%d,%d" % (_bucket(M), N, _bucket(K), int(bool(out_f64)))
+    return k + ",x3" if x3 else k
 
 
 _frozen = threading.local()
@@ -86,12 +88,12 @@ def _save():
         pass
 
 
-def tile_for(M, N, K, out_f64, launch, reps=3):
+def tile_for(M, N, K, out_f64, launch, reps=3, x3=False):
     """BN for the GEMM (M x K) @ (N x K)^T; ``launch(bn)`` issues one GEMM
     with tile width bn on the current stream (raising on a bad status)."""
     if os.environ.get("VTB_AUTOTUNE", "1") == "0":
         return DEFAULT_BN
-    key = _key(M, N, K, out_f64)
+    key = _key(M, N, K, out_f64, x3)
     with _lock:
         _load()
         if key in _cache:
@@ -118,18 +120,21 @@ def tile_for(M, N, K, out_f64, launch, reps=3):
     return best
 
 
-def gemm_bf16_tuned(A3, M, B3, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err_ptr, stream):
-    """vtb_tc_gemm_bf16_bn with the tuned tile width for this shape."""
+def gemm_bf16_tuned(A3, M, B3, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err_ptr, stream, x3=False):
+    """vtb_tc_gemm_bf16_bn (or, with ``x3``, the three-product
+    vtb_tc_gemm_bf16x3_bn on [hi | lo] operands, K the width of one part)
+    with the tuned tile width for this shape."""
+    name = "vtb_tc_gemm_bf16x3_bn" if x3 else "vtb_tc_gemm_bf16_bn"
+
     def launch(bn):
-        call("vtb_tc_gemm_bf16_bn", A3, M, B3, N, K, C, c_m, c_n, int(out_f64), float(alpha), int(accumulate),
-             err_ptr, int(bn), stream)
+        call(name, A3, M, B3, N, K, C, c_m, c_n, int(out_f64), float(alpha), int(accumulate), err_ptr, int(bn), stream)
 
     if accumulate:
         # tuning launches repeatedly: only a non-accumulating GEMM may be tuned
         with _lock:
             _load()
-            bn = _cache.get(_key(M, N, K, out_f64), DEFAULT_BN)
+            bn = _cache.get(_key(M, N, K, out_f64, x3), DEFAULT_BN)
     else:
-        bn = tile_for(M, N, K, out_f64, launch)
+        bn = tile_for(M, N, K, out_f64, launch, x3=x3)
     launch(bn)
     return bn

@@ -65,9 +65,9 @@ class ClipProblem(object):
 
 class GroupedGram(object):
     """The tensor-core Kronecker Gram GEMMs of many mixed decoders
-    (C_p = L3_p R3_p^T, uneven sizes) as ONE grouped launch
-    (``vtb_tc_gemm_grouped``); its tile width is chosen by timing the
-    candidates on the first eager run (``autotune``)."""
+    (C_p = the three split-bf16 products of L_p and R_p, uneven sizes) as
+    ONE grouped launch (``vtb_tc_gemm_grouped_x3``); its tile width is
+    chosen by timing the candidates on the first eager run (``autotune``)."""
 
     WIDTHS = (64, 128, 256)
 
@@ -77,9 +77,9 @@ class GroupedGram(object):
         dev = self.decs[0].M.device
         u64 = np.uint64
         self.args = [
-            np.array([d.L3.data_ptr() for d in self.decs], u64), np.array([2 * d.npairs for d in self.decs], np.int32),
-            np.array([d.R3.data_ptr() for d in self.decs], u64), np.array([d.Kt * d.Kt for d in self.decs], np.int32),
-            np.array([3 * d.Kp2 for d in self.decs], np.int32), np.array([d.C.data_ptr() for d in self.decs], u64),
+            np.array([d.Lsplit.data_ptr() for d in self.decs], u64), np.array([2 * d.npairs for d in self.decs], np.int32),
+            np.array([d.Rsplit.data_ptr() for d in self.decs], u64), np.array([d.Kt * d.Kt for d in self.decs], np.int32),
+            np.array([d.Kp2 for d in self.decs], np.int32), np.array([d.C.data_ptr() for d in self.decs], u64),
             np.array([d.Kt * d.Kt for d in self.decs], np.int64),
             np.array([d._stat_ptr(7) for d in self.decs], u64)]
         self.desc = {}
@@ -89,7 +89,7 @@ class GroupedGram(object):
             host = np.zeros(nbytes, np.uint8)
             tiles = np.zeros(1, np.int32)
             a = self.args
-            call("vtb_tc_group_build", host.ctypes.data, self.n, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data,
+            call("vtb_tc_group_build_x3", host.ctypes.data, self.n, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data,
                  a[3].ctypes.data, a[4].ctypes.data, a[5].ctypes.data, a[6].ctypes.data, a[7].ctypes.data, bn,
                  tiles.ctypes.data)
             self.desc[bn] = torch.as_tensor(host).to(dev)
@@ -97,7 +97,7 @@ class GroupedGram(object):
         self.bn = None
 
     def _launch(self, bn, s):
-        call("vtb_tc_gemm_grouped", dptr(self.desc[bn]), self.n, self.tiles[bn], bn, s)
+        call("vtb_tc_gemm_grouped_x3", dptr(self.desc[bn]), self.n, self.tiles[bn], bn, s)
 
     def launch(self, s):
         if self.bn is None:
@@ -128,7 +128,7 @@ def stage_mixed_pre(d, p, s):
          dptr(d.norm), d.Mt, d.W, dptr(d.Wn), dptr(d.gn), s)
     call("vtb_coeff_rhs", dptr(d.d), d.N, d.Ks, dptr(d.gn), d.Kt, dptr(d.b), s)
     call("vtb_coeff_realify_vec", dptr(d.b), d.K, 1, dptr(d.br), s)
-    call("vtb_coeff_wn_split", dptr(d.Wn), d.N, d.Kt, dptr(d.R3), s)
+    call("vtb_coeff_wn_split2", dptr(d.Wn), d.N, d.Kt, dptr(d.Rsplit), s)
 
 
 def stage_mixed_post(d, s):
@@ -149,9 +149,9 @@ def stage_mixed(d, p, s):
          dptr(d.norm), d.Mt, d.W, dptr(d.Wn), dptr(d.gn), s)
     call("vtb_coeff_rhs", dptr(d.d), d.N, d.Ks, dptr(d.gn), d.Kt, dptr(d.b), s)
     call("vtb_coeff_realify_vec", dptr(d.b), K, 1, dptr(d.br), s)
-    call("vtb_coeff_wn_split", dptr(d.Wn), d.N, d.Kt, dptr(d.R3), s)
-    autotune.gemm_bf16_tuned(dptr(d.L3), 2 * d.npairs, dptr(d.R3), KK, 3 * d.Kp2, dptr(d.C), KK, 1, 0, 1.0, 0,
-                             d._stat_ptr(7), s)
+    call("vtb_coeff_wn_split2", dptr(d.Wn), d.N, d.Kt, dptr(d.Rsplit), s)
+    autotune.gemm_bf16_tuned(dptr(d.Lsplit), 2 * d.npairs, dptr(d.Rsplit), KK, d.Kp2, dptr(d.C), KK, 1, 0, 1.0, 0,
+                             d._stat_ptr(7), s, x3=True)
     call("vtb_coeff_real_scatter", dptr(d.C), KK, d.Ks, d.Kt, dptr(d.Mr32), d.ld32, 0, s)
     d.xr.copy_(d.br)
 

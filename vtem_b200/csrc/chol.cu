@@ -9,9 +9,10 @@
 //
 //   CTA 0 ("diagonal") walks the critical path, step k = 0..T-1:
 //     one panel factorisation [A_kk; I] -> [L_kk; L_kk^-T] with all its warps
-//     (8-column blocks: warp 0 factorises each 8 x 8 diagonal block while the
-//     others apply the previous block's update); publishes L_kk and
-//     L_kk^-1 (Dinv) together;
+//     (8-column blocks: warp 0 factorises and inverts each 8 x 8 diagonal
+//     block while the others apply the previous block's update; the panel's
+//     rows below a block are multiplied by its inverse); publishes L_kk^-1
+//     (Dinv) first, then L_kk and the packed X_kk after the sub-diagonal;
 //     the sub-diagonal tile L_{k+1,k} = A_{k+1,k} L_kk^-T as a product;
 //     SYRK of the next diagonal tile A_{k+1,k+1} -= L_{k+1,k} L_{k+1,k}^T,
 //     which it keeps in shared memory for step k+1.
@@ -85,6 +86,7 @@ struct CholCtx {
     unsigned limit;
     float* Xinv;         // packed L^-1 tiles, row-major (null: no inverse)
     unsigned* xflag;     // T*T flags: 1 = X tile (i, j) published
+    unsigned* pflag;     // T*T counts of the partial chunks of X tile (i, j) done
 };
 
 // thread 0 waits until *f >= v; every thread learns the outcome
@@ -231,7 +233,7 @@ __device__ __forceinline__ void acc_to(const float (&acc)[4][4], float* s, int t
 // pmin/pmax; a pivot <= 0 or NaN sets bad.
 __device__ __forceinline__ void potrf8_warp(float* S, float* rinv, int bb, float& pmin, float& pmax, int& bad,
                                             int nvalid) {
-    const int lane = threadIdx.x & 31, o = 8 * bb;
+    const int o = 8 * bb;
     float a[8][8];     // a[i][j]: row i, column j (lower part used)
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -386,36 +388,109 @@ __device__ void potrf_inv64(float* S, float* E, float* rinv, float& pmin, float&
 // Factorisation tasks, group g (0 <= g <= T-3), T-g of them: the TRSM tiles
 // (I, g) for I = g+2..T-1 (type 0), then the sub-diagonal (g+2, g+1) (type 1)
 // and the diagonal (g+2, g+2) (type 2), pre-updated through g.
-// Inverse tasks (when L^-1 is asked for): X_ij = -X_ii sum_{k=j}^{i-1} L_ik
-// X_kj for j < i (type 4); the diagonal CTA forms X_ii = L_ii^-1.
-// Global order, slot s = 0..T-1: [type 4 (s, j), j < s][factorisation group
-// s].  A factorisation group s needs the diagonal steps <= s and earlier
-// groups; the diagonal step s needs groups <= s-1; a row-s inverse task
-// needs the diagonal step s, earlier rows of its column and L tiles of row
-// s, all from earlier slots: with every CTA resident, no task waits on one
-// behind it.
-__device__ __forceinline__ void task_of(int T, bool inv, int t, int& I, int& J, int& type) {
-    for (int sl = 0; sl < T; ++sl) {
-        if (inv) {
-            if (t < sl) { I = sl; J = t; type = 4; return; }
-            t -= sl;
+//
+// Inverse tasks (when L^-1 is asked for), X_ij = -X_ii S_ij with
+// S_ij = sum_{k=j}^{i-1} L_ik X_kj (the diagonal CTA forms X_ii = L_ii^-1):
+// the terms k = j..i-2 are summed in chunks of kXChunk consecutive k
+// (type 4, the chunk ending at k1 runs as soon as L_{i,k1} and X_{k1,j}
+// exist), each chunk adding to the running partial -S_ij kept in X_ij's own
+// storage; the last term k = i-1 and the product with X_ii are the final
+// task (type 5), so after the last diagonal step only one product per tile
+// of the last row remains.
+//
+// The workers form two pools (half each when the inverse is asked for): one
+// runs the factorisation tasks in group order, the other the inverse tasks
+// in slot order, s = 0..T-1: the chunks ending at k1 = s-1 (rows i >= s+1),
+// then the final tasks of row s.  A factorisation group s needs the
+// diagonal steps <= s and earlier groups; the diagonal step s needs groups
+// <= s-1; a chunk ending at s-1 needs L_{i,s-1} (group s-1 or step s-1),
+// rows <= s-1 of X and the row's earlier chunks; a final task of row s needs
+// step s and row s-1 of X.  The factorisation never waits on the inverse,
+// and within each pool every dependency lies earlier in its order (or in the
+// other pool, or on the diagonal), so with every CTA resident no task waits
+// on one behind it.
+constexpr int kXChunk = 8;
+
+// factorisation task t in group order
+__device__ __forceinline__ void factor_task(int T, int t, int& I, int& J, int& type) {
+    for (int g = 0; g <= T - 3; ++g) {
+        const int n = T - g, n0 = T - g - 2;
+        if (t < n) {
+            if (t < n0) { I = g + 2 + t; J = g; type = 0; }
+            else if (t == n0) { I = g + 2; J = g + 1; type = 1; }
+            else { I = g + 2; J = g + 2; type = 2; }
+            return;
         }
-        if (sl <= T - 3) {
-            const int n = T - sl, n0 = T - sl - 2;
-            if (t < n) {
-                if (t < n0) { I = sl + 2 + t; J = sl; type = 0; }
-                else if (t == n0) { I = sl + 2; J = sl + 1; type = 1; }
-                else { I = sl + 2; J = sl + 2; type = 2; }
-                return;
-            }
-            t -= n;
-        }
+        t -= n;
     }
     I = J = type = -1;
 }
 
-__device__ __forceinline__ int task_count(int T, bool inv) {
-    return (T >= 3 ? T * (T + 1) / 2 - 3 : 0) + (inv ? T * (T - 1) / 2 : 0);
+__host__ __device__ __forceinline__ int factor_count(int T) { return T >= 3 ? T * (T + 1) / 2 - 3 : 0; }
+
+// inverse task t in slot order
+__device__ __forceinline__ void inverse_task(int T, int t, int& I, int& J, int& type, int& k0, int& k1) {
+    for (int sl = 0; sl < T; ++sl) {
+        // chunks of row sl+1 ending at its last non-final term k = sl-1 (possibly short)
+        if (sl >= 1 && sl + 1 <= T - 1) {
+            if (t < sl) {
+                I = sl + 1;
+                J = t;
+                k1 = sl - 1;
+                k0 = J + ((k1 - J) / kXChunk) * kXChunk;
+                type = 4;
+                return;
+            }
+            t -= sl;
+        }
+        // full chunks [sl-kXChunk, sl-1] of rows sl+2..T-1
+        const int nb = sl / kXChunk;
+        if (nb > 0 && T - 1 >= sl + 2) {
+            const int cnt = (T - 2 - sl) * nb;
+            if (t < cnt) {
+                I = sl + 2 + t / nb;
+                J = sl - kXChunk - kXChunk * (t % nb);
+                k0 = sl - kXChunk;
+                k1 = sl - 1;
+                type = 4;
+                return;
+            }
+            t -= cnt;
+        }
+        // final tasks of row sl
+        if (t < sl) {
+            I = sl;
+            J = t;
+            k0 = k1 = sl - 1;
+            type = 5;
+            return;
+        }
+        t -= sl;
+    }
+    I = J = type = k0 = k1 = -1;
+}
+
+__host__ __device__ __forceinline__ int inverse_count(int T) {
+    int n = 0;
+    for (int sl = 0; sl < T; ++sl) {
+        if (sl >= 1 && sl + 1 <= T - 1) n += sl;
+        if (T - 1 >= sl + 2) n += (T - 2 - sl) * (sl / kXChunk);
+        n += sl;
+    }
+    return n;
+}
+
+__host__ __device__ __forceinline__ int task_count(int T, bool inv) {
+    return factor_count(T) + (inv ? inverse_count(T) : 0);
+}
+
+// workers of the factorisation when the inverse is formed too (the rest form
+// the inverse); all of them without it
+__host__ __device__ __forceinline__ int factor_workers(int W, int T, bool inv) {
+    if (!inv || inverse_count(T) == 0) return W;
+    if (factor_count(T) == 0) return 0;
+    const int wf = W / 2;
+    return wf < 1 ? 1 : wf;
 }
 
 // packed lower-triangular tile index of (i, j), i >= j
@@ -455,20 +530,37 @@ __device__ __forceinline__ void acc_neg(float (&acc)[4][4]) {
         for (int q = 0; q < 4; ++q) acc[p][q] = -acc[p][q];
 }
 
-// Type 4: X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj, operands double-buffered as
-// in the factorisation updates
-__device__ bool task_offdiag_inverse(const CholCtx& c, CholSmem& sm, int i, int j) {
+// the running partial -S_ij of an inverse tile (row-major in X_ij's storage)
+__device__ __forceinline__ void partial_load(const float* X, float (&acc)[4][4], int tr, int tc) {
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const float4 v = __ldcg(reinterpret_cast<const float4*>(X + (4 * tr + p) * kCT + 4 * tc));
+        acc[p][0] = v.x;
+        acc[p][1] = v.y;
+        acc[p][2] = v.z;
+        acc[p][3] = v.w;
+    }
+}
+
+__device__ __forceinline__ void partial_store(float* X, const float (&acc)[4][4], int tr, int tc) {
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+        __stcg(reinterpret_cast<float4*>(X + (4 * tr + p) * kCT + 4 * tc),
+               make_float4(acc[p][0], acc[p][1], acc[p][2], acc[p][3]));
+}
+
+// acc -= sum_{k=k0}^{k1} L_ik X_kj, operands double-buffered as in the
+// factorisation updates (P = L_ik column-major, Q = X_kj row-major)
+__device__ bool inv_accumulate(const CholCtx& c, CholSmem& sm, int i, int j, int k0, int k1, float (&acc)[4][4]) {
     const int T = c.T;
     const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
-    float acc[4][4];
-    acc_zero(acc);
-    const int n = i - j;     // k = j .. i-1
-    if (!cta_wait(c, c.tflag + i * T + j, 2u, &sm.ok)) return false;
-    if (!cta_wait(c, c.xflag + j * T + j, 1u, &sm.ok)) return false;
-    load_tile(c, sm.a[0], i, j);
-    load_flat(sm.b[0], c.Xinv + packed_tile(j, j) * kCTE);
+    const int n = k1 - k0 + 1;
+    if (!cta_wait(c, c.tflag + i * T + k0, 2u, &sm.ok)) return false;
+    if (!cta_wait(c, c.xflag + k0 * T + j, 1u, &sm.ok)) return false;
+    load_tile(c, sm.a[0], i, k0);
+    load_flat(sm.b[0], c.Xinv + packed_tile(k0, j) * kCTE);
     for (int q = 0; q < n; ++q) {
-        const int k = j + q, nb = (q + 1) & 1;
+        const int k = k0 + q, nb = (q + 1) & 1;
         bool next = false;
         if (q + 1 < n) {
             next = cta_ready(c.tflag + i * T + k + 1, 2u, &sm.ok) && cta_ready(c.xflag + (k + 1) * T + j, 1u, &sm.ok);
@@ -480,7 +572,6 @@ __device__ bool task_offdiag_inverse(const CholCtx& c, CholSmem& sm, int i, int 
         if (next) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
         else cp_async_wait_all();
         __syncthreads();
-        // acc -= L_ik X_kj: P = L_ik column-major, Q = X_kj row-major
         sub_ptq(acc, sm.a[q & 1], sm.b[q & 1], tr, tc, 0, kCT);
         if (q + 1 < n && !next) {
             if (!cta_wait(c, c.tflag + i * T + k + 1, 2u, &sm.ok)) return false;
@@ -489,6 +580,42 @@ __device__ bool task_offdiag_inverse(const CholCtx& c, CholSmem& sm, int i, int 
             load_flat(sm.b[nb], c.Xinv + packed_tile(k + 1, j) * kCTE);
         }
     }
+    return true;
+}
+
+// Type 4: one chunk k0..k1 of the partial of X_ij
+__device__ bool task_inverse_chunk(const CholCtx& c, CholSmem& sm, int i, int j, int k0, int k1) {
+    const int T = c.T;
+    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+    const int ch = (k0 - j) / kXChunk;
+    float* X = c.Xinv + packed_tile(i, j) * kCTE;
+    float acc[4][4];
+    if (ch > 0) {
+        if (!cta_wait(c, c.pflag + i * T + j, (unsigned)ch, &sm.ok)) return false;
+        partial_load(X, acc, tr, tc);
+    } else {
+        acc_zero(acc);
+    }
+    if (!inv_accumulate(c, sm, i, j, k0, k1, acc)) return false;
+    partial_store(X, acc, tr, tc);
+    cta_publish(c.pflag + i * T + j, (unsigned)ch + 1u);
+    return true;
+}
+
+// Type 5: the last term k = i-1, then X_ij = -X_ii S_ij
+__device__ bool task_inverse_final(const CholCtx& c, CholSmem& sm, int i, int j) {
+    const int T = c.T;
+    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+    const int nch = (i - 1 - j + kXChunk - 1) / kXChunk;     // chunks of k = j..i-2
+    float* X = c.Xinv + packed_tile(i, j) * kCTE;
+    float acc[4][4];
+    if (nch > 0) {
+        if (!cta_wait(c, c.pflag + i * T + j, (unsigned)nch, &sm.ok)) return false;
+        partial_load(X, acc, tr, tc);
+    } else {
+        acc_zero(acc);
+    }
+    if (!inv_accumulate(c, sm, i, j, i - 1, i - 1, acc)) return false;
     // acc = -S.  With P = -S row-major and Q = X_ii row-major, sub_pq_rowq
     // gives out[a][b] = sum_t S[t][a] X_ii[b][t] = (X_ii S)[b][a]; X_ij = -(X_ii S)
     if (!cta_wait(c, c.xflag + i * T + i, 1u, &sm.ok)) return false;
@@ -506,85 +633,102 @@ __device__ bool task_offdiag_inverse(const CholCtx& c, CholSmem& sm, int i, int 
     acc_neg(out);
     acc_to(out, sm.x, tr, tc);     // X_ij[4tc+q][4tr+p] at (4tc+q)*64 + 4tr+p: row-major
     __syncthreads();
-    store_flat(c.Xinv + packed_tile(i, j) * kCTE, sm.x);
+    store_flat(X, sm.x);
     cta_publish(c.xflag + i * T + j, 1u);
     return true;
 }
 
+__device__ bool worker_task(const CholCtx& c, CholSmem& sm, int t);
+
+// Each pool deals its tasks round-robin (pool worker w runs tasks w, w + Wp,
+// ...) in its order.
 __device__ void worker(const CholCtx& c, CholSmem& sm) {
     const int W = gridDim.x - 1, wid = blockIdx.x - 1;
     const int T = c.T;
     const bool inv = c.Xinv != nullptr;
-    const int ntask = task_count(T, inv);
+    const int wf = factor_workers(W, T, inv);
+    if (wid < wf) {
+        const int n = factor_count(T);
+        for (int t = wid; t < n; t += wf)
+            if (!worker_task(c, sm, t)) return;
+    } else {
+        const int n = inverse_count(T), wi = W - wf;
+        for (int t = wid - wf; t < n; t += wi) {
+            int I, J, type, k0, k1;
+            inverse_task(T, t, I, J, type, k0, k1);
+            if (type == 4 && !task_inverse_chunk(c, sm, I, J, k0, k1)) return;
+            if (type == 5 && !task_inverse_final(c, sm, I, J)) return;
+        }
+    }
+}
+
+// factorisation task t
+__device__ bool worker_task(const CholCtx& c, CholSmem& sm, int t) {
+    const int T = c.T;
     const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
-    for (int t = wid; t < ntask; t += W) {
-        int I, J, type;
-        task_of(T, inv, t, I, J, type);
-        if (type == 4) {
-            if (!task_offdiag_inverse(c, sm, I, J)) return;
-            continue;
-        }
-        // updates k' < kend, kend = J for type 0, I-1 for types 1 and 2
-        const int kend = type == 0 ? J : I - 1;
-        __syncthreads();
-        load_tile(c, sm.x, I, J);
-        cp_async_wait_all();
-        __syncthreads();
-        float acc[4][4];
-        acc_from(acc, sm.x, tr, tc);
-        // operands of update k in buffer k & 1; the next update's operands are
-        // requested before this one's product when their flags are already set
-        if (kend > 0) {
-            if (!cta_wait(c, c.tflag + I * T + 0, 2u, &sm.ok)) return;
-            if (I != J && !cta_wait(c, c.tflag + J * T + 0, 2u, &sm.ok)) return;
-            load_tile(c, sm.a[0], I, 0);
-            if (I != J) load_tile(c, sm.b[0], J, 0);
-        }
-        for (int k = 0; k < kend; ++k) {
-            const int nb = (k + 1) & 1;
-            bool next = false;
-            if (k + 1 < kend) {
-                next = cta_ready(c.tflag + I * T + k + 1, 2u, &sm.ok) &&
-                       (I == J || cta_ready(c.tflag + J * T + k + 1, 2u, &sm.ok));
-                if (next) {
-                    // the buffers of update k-1 are free: every thread passed the barriers above
-                    load_tile(c, sm.a[nb], I, k + 1);
-                    if (I != J) load_tile(c, sm.b[nb], J, k + 1);
-                }
-            }
-            // this update's groups complete; the next update's (one per operand) may stay in flight
-            if (next && I != J) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
-            else if (next) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-            else cp_async_wait_all();
-            __syncthreads();
-            const float* pa = sm.a[k & 1];
-            sub_ptq(acc, pa, I != J ? sm.b[k & 1] : pa, tr, tc, 0, kCT);
-            if (k + 1 < kend && !next) {
-                if (!cta_wait(c, c.tflag + I * T + k + 1, 2u, &sm.ok)) return;
-                if (I != J && !cta_wait(c, c.tflag + J * T + k + 1, 2u, &sm.ok)) return;
+    int I, J, type;
+    factor_task(T, t, I, J, type);
+    // updates k' < kend, kend = J for type 0, I-1 for types 1 and 2
+    const int kend = type == 0 ? J : I - 1;
+    __syncthreads();
+    load_tile(c, sm.x, I, J);
+    cp_async_wait_all();
+    __syncthreads();
+    float acc[4][4];
+    acc_from(acc, sm.x, tr, tc);
+    // operands of update k in buffer k & 1; the next update's operands are
+    // requested before this one's product when their flags are already set
+    if (kend > 0) {
+        if (!cta_wait(c, c.tflag + I * T + 0, 2u, &sm.ok)) return false;
+        if (I != J && !cta_wait(c, c.tflag + J * T + 0, 2u, &sm.ok)) return false;
+        load_tile(c, sm.a[0], I, 0);
+        if (I != J) load_tile(c, sm.b[0], J, 0);
+    }
+    for (int k = 0; k < kend; ++k) {
+        const int nb = (k + 1) & 1;
+        bool next = false;
+        if (k + 1 < kend) {
+            next = cta_ready(c.tflag + I * T + k + 1, 2u, &sm.ok) &&
+                   (I == J || cta_ready(c.tflag + J * T + k + 1, 2u, &sm.ok));
+            if (next) {
+                // the buffers of update k-1 are free: every thread passed the barriers above
                 load_tile(c, sm.a[nb], I, k + 1);
                 if (I != J) load_tile(c, sm.b[nb], J, k + 1);
             }
         }
+        // this update's groups complete; the next update's (one per operand) may stay in flight
+        if (next && I != J) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+        else if (next) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        else cp_async_wait_all();
         __syncthreads();
-        acc_to(acc, sm.x, tr, tc);
-        if (type == 0) {
-            // TRSM as a product with the published L_JJ^-T: L_IJ = A_IJ L_JJ^-T
-            if (!cta_wait(c, c.tflag + J * T + J, 2u, &sm.ok)) return;
-            load_flat(sm.b[0], c.Dinv + (int64_t)J * kCTE);
-            cp_async_wait_all();
-            __syncthreads();
-            float out[4][4];
-            acc_zero(out);
-            sub_pq_rowq(out, sm.x, sm.b[0], tr, tc);
-            __syncthreads();
-            acc_neg(out);
-            acc_to(out, sm.x, tr, tc);
+        const float* pa = sm.a[k & 1];
+        sub_ptq(acc, pa, I != J ? sm.b[k & 1] : pa, tr, tc, 0, kCT);
+        if (k + 1 < kend && !next) {
+            if (!cta_wait(c, c.tflag + I * T + k + 1, 2u, &sm.ok)) return false;
+            if (I != J && !cta_wait(c, c.tflag + J * T + k + 1, 2u, &sm.ok)) return false;
+            load_tile(c, sm.a[nb], I, k + 1);
+            if (I != J) load_tile(c, sm.b[nb], J, k + 1);
         }
-        __syncthreads();
-        store_tile(c, sm.x, I, J);
-        cta_publish(c.tflag + I * T + J, type == 0 ? 2u : 1u);
     }
+    __syncthreads();
+    acc_to(acc, sm.x, tr, tc);
+    if (type == 0) {
+        // TRSM as a product with the published L_JJ^-T: L_IJ = A_IJ L_JJ^-T
+        if (!cta_wait(c, c.tflag + J * T + J, 2u, &sm.ok)) return false;
+        load_flat(sm.b[0], c.Dinv + (int64_t)J * kCTE);
+        cp_async_wait_all();
+        __syncthreads();
+        float out[4][4];
+        acc_zero(out);
+        sub_pq_rowq(out, sm.x, sm.b[0], tr, tc);
+        __syncthreads();
+        acc_neg(out);
+        acc_to(out, sm.x, tr, tc);
+    }
+    __syncthreads();
+    store_tile(c, sm.x, I, J);
+    cta_publish(c.tflag + I * T + J, type == 0 ? 2u : 1u);
+    return true;
 }
 
 // Step k: the panel factorisation of the diagonal tile (L_kk and its
@@ -616,12 +760,21 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
             if (hy) load_tile(c, Y, k + 1, k + 1);
         }
         potrf_inv64(D, E, sm.rinv, pmin, pmax, bad, c.K - k * kCT);
-        store_tile(c, D, k, k);
+        // the workers need L_kk^-T first (their TRSMs); L_kk itself and the
+        // packed X_kk are written after the sub-diagonal tile is out, so the
+        // release stores on this CTA's path wait for as few stores as possible
         store_flat(c.Dinv + (int64_t)k * kCTE, E);
-        if (inv) store_flat(c.Xinv + packed_tile(k, k) * kCTE, E);
         cta_publish(c.tflag + k * T + k, 2u);
-        if (inv && threadIdx.x == 0) c_st_release(c.xflag + k * T + k, 1u);
-        if (k + 1 >= T) break;
+        // X_{k-1,k-1} was stored during the previous step: this release covers it
+        if (inv && k > 0 && threadIdx.x == 0) c_st_release(c.xflag + (k - 1) * T + k - 1, 1u);
+        if (k + 1 >= T) {
+            store_tile(c, D, k, k);
+            if (inv) {
+                store_flat(c.Xinv + packed_tile(k, k) * kCTE, E);
+                cta_publish(c.xflag + k * T + k, 1u);
+            }
+            break;
+        }
         // sub-diagonal tile: the workers applied updates k' < k (none when k = 0);
         // L_{k+1,k} = X L_kk^-T
         if (!hx) {
@@ -641,6 +794,8 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
         __syncthreads();
         store_tile(c, X, k + 1, k);
         cta_publish(c.tflag + (k + 1) * T + k, 2u);
+        store_tile(c, D, k, k);
+        if (inv) store_flat(c.Xinv + packed_tile(k, k) * kCTE, E);     // flag set with the next step's release
         // next diagonal tile: the workers applied updates k' < k; this CTA applies k
         if (!hy) {
             if (!cta_wait(c, c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok)) return;
@@ -690,7 +845,7 @@ VTB_API int64_t vtb_chol_dinv_floats(int K) { return K > 0 ? (int64_t)chol_tiles
 VTB_API int64_t vtb_chol_work_bytes(int K) {
     if (K <= 0) return 0;
     const int64_t T = chol_tiles(K);
-    return 2 * ((T * T * 4 + 255) & ~(int64_t)255) + 256;
+    return 3 * ((T * T * 4 + 255) & ~(int64_t)255) + 256;
 }
 
 VTB_API int64_t vtb_chol_inverse_floats(int K) {
@@ -716,11 +871,13 @@ static int chol_launch(float* A, int64_t ld, int K, float* Dinv, float* Linv, vo
     VTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chol_tiles_kernel, kCThreads, sm));
     if (per_sm < 1) return VTB_CUDA_ERR;
     const int T = chol_tiles(K);
-    const int ntask = (T >= 3 ? T * (T + 1) / 2 - 3 : 0) + (Linv ? T * (T - 1) / 2 : 0);
-    const int grid = 1 + std::max(1, std::min(nsm - 1, ntask));
+    const bool inv = Linv != nullptr;
+    const int ntask = task_count(T, inv);
+    const int need = (inv && factor_count(T) > 0 && inverse_count(T) > 0) ? 2 : 1;
+    const int grid = 1 + std::max(need, std::min(nsm - 1, ntask));
     cudaStream_t s = as_stream(stream);
     const int64_t fbytes = ((int64_t)T * T * 4 + 255) & ~(int64_t)255;
-    VTB_CUDA_TRY(cudaMemsetAsync(work, 0, (size_t)(2 * fbytes + 256), s));
+    VTB_CUDA_TRY(cudaMemsetAsync(work, 0, (size_t)(3 * fbytes + 256), s));
     CholCtx c;
     c.A = A;
     c.ld = ld;
@@ -729,7 +886,8 @@ static int chol_launch(float* A, int64_t ld, int K, float* Dinv, float* Linv, vo
     c.Dinv = Dinv;
     c.tflag = reinterpret_cast<unsigned*>(work);
     c.xflag = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(work) + fbytes);
-    c.abort_word = reinterpret_cast<int*>(reinterpret_cast<char*>(work) + 2 * fbytes);
+    c.pflag = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(work) + 2 * fbytes);
+    c.abort_word = reinterpret_cast<int*>(reinterpret_cast<char*>(work) + 3 * fbytes);
     c.status = status;
     c.piv = pivots;
     c.rcond = rcond;
@@ -785,6 +943,7 @@ __global__ void __launch_bounds__(kGThreads) inv_fwd_kernel(const float* __restr
                                                             const double* __restrict__ b, float* __restrict__ part,
                                                             float* __restrict__ y, unsigned* __restrict__ cnt) {
     __shared__ float bs[kCT];
+    __shared__ float red[4][kCT];
     __shared__ int last;
     const int t = blockIdx.x, tid = threadIdx.x;
     int i, j;
@@ -818,11 +977,16 @@ __global__ void __launch_bounds__(kGThreads) inv_fwd_kernel(const float* __restr
     __syncthreads();
     if (!last) return;
     __threadfence();
-    if (tid < kCT) {
+    {
+        // four threads per row, each over every fourth partial, then a fixed-order combine
+        const int rr = tid & 63, qq = tid >> 6;
         float sum = 0.f;
-        for (int jj = 0; jj <= i; ++jj) sum += __ldcg(part + ((int64_t)i * (i + 1) / 2 + jj) * kCT + tid);
-        y[i * kCT + tid] = sum;
+#pragma unroll 4
+        for (int jj = qq; jj <= i; jj += 4) sum += __ldcg(part + ((int64_t)i * (i + 1) / 2 + jj) * kCT + rr);
+        red[qq][rr] = sum;
     }
+    __syncthreads();
+    if (tid < kCT) y[i * kCT + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
     if (tid == 0) cnt[i] = 0u;
 }
 
@@ -857,11 +1021,18 @@ __global__ void __launch_bounds__(kGThreads) inv_bwd_kernel(const float* __restr
     __syncthreads();
     if (!last) return;
     __threadfence();
-    if (tid < kCT) {
+    {
+        const int cc2 = tid & 63, qq = tid >> 6;
         float sum = 0.f;
-        for (int ii = j; ii < T; ++ii) sum += __ldcg(part + ((int64_t)ii * (ii + 1) / 2 + j) * kCT + tid);
+#pragma unroll 4
+        for (int ii = j + qq; ii < T; ii += 4) sum += __ldcg(part + ((int64_t)ii * (ii + 1) / 2 + j) * kCT + cc2);
+        __syncthreads();       // every thread has read red[][] above
+        red[qq][cc2] = sum;
+    }
+    __syncthreads();
+    if (tid < kCT) {
         const int g = j * kCT + tid;
-        if (g < K) x[g] = (double)sum;
+        if (g < K) x[g] = (double)((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
     }
     if (tid == 0) cnt[T + j] = 0u;
 }

@@ -1161,6 +1161,9 @@ VTB_API int vtb_coeff_synthesize_noalloc(const double* a, const int32_t* smap, i
 namespace vtb {
 
 // L3[row][seg*Kp + k], row = 2*pair + part, k = 2n + q, Kp = 2N rounded up to 64
+// PARTS = 3: [hi | hi | lo] (the plain GEMM's layout); PARTS = 2: [hi | lo]
+// (the three-product mode's)
+template <int PARTS>
 __global__ void kron_lhs_split_kernel(const double2* __restrict__ d, int N, int Ks, const int32_t* __restrict__ ps,
                                       const int32_t* __restrict__ ps2, int npairs, int Kp,
                                       __nv_bfloat16* __restrict__ L3) {
@@ -1177,14 +1180,20 @@ __global__ void kron_lhs_split_kernel(const double2* __restrict__ d, int N, int 
         }
         const __nv_bfloat16 hi = __float2bfloat16_rn((float)x);
         const __nv_bfloat16 lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
-        __nv_bfloat16* dst = L3 + (int64_t)row * 3 * Kp + k;
+        __nv_bfloat16* dst = L3 + (int64_t)row * PARTS * Kp + k;
         dst[0] = hi;
-        dst[Kp] = hi;
-        dst[2 * Kp] = lo;
+        if (PARTS == 3) {
+            dst[Kp] = hi;
+            dst[2 * Kp] = lo;
+        } else {
+            dst[Kp] = lo;
+        }
     }
 }
 
 // R3[e][seg*Kp + k] with e = (m, m'), k = 2n + q: pattern [hi | lo | hi]
+// (PARTS = 3) or [hi | lo] (PARTS = 2)
+template <int PARTS>
 __global__ void kron_rhs_split_kernel(const double2* __restrict__ Wn, int N, int KK, int Kp,
                                       __nv_bfloat16* __restrict__ R3) {
     const int64_t total = (int64_t)KK * Kp;
@@ -1197,10 +1206,10 @@ __global__ void kron_rhs_split_kernel(const double2* __restrict__ Wn, int N, int
         }
         const __nv_bfloat16 hi = __float2bfloat16_rn((float)x);
         const __nv_bfloat16 lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
-        __nv_bfloat16* dst = R3 + (int64_t)e * 3 * Kp + k;
+        __nv_bfloat16* dst = R3 + (int64_t)e * PARTS * Kp + k;
         dst[0] = hi;
         dst[Kp] = lo;
-        dst[2 * Kp] = hi;
+        if (PARTS == 3) dst[2 * Kp] = hi;
     }
 }
 
@@ -1290,23 +1299,56 @@ __global__ void zadd_kernel(double2* __restrict__ a, const double2* __restrict__
 
 }  // namespace vtb
 
-VTB_API int vtb_coeff_lhs_split(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs,
-                                void* L3, void* stream) {
-    VTB_CHECK_ARG(N > 0 && Ks > 0 && npairs > 0 && d && ps && ps2 && L3 && ((uintptr_t)L3 & 15) == 0);
+static int lhs_split(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs, void* L,
+                     int parts, void* stream) {
+    VTB_CHECK_ARG(N > 0 && Ks > 0 && npairs > 0 && d && ps && ps2 && L && ((uintptr_t)L & 15) == 0);
     const int Kp = ceil_div(2 * N, 64) * 64;
     const int64_t total = (int64_t)npairs * 2 * Kp;
-    kron_lhs_split_kernel<<<(int)std::min<int64_t>(ceil_div(total, 256), 32 * kNumSMs), 256, 0, as_stream(stream)>>>(
-        reinterpret_cast<const double2*>(d), N, Ks, ps, ps2, npairs, Kp, reinterpret_cast<__nv_bfloat16*>(L3));
+    const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 32 * kNumSMs);
+    if (parts == 3)
+        kron_lhs_split_kernel<3><<<blocks, 256, 0, as_stream(stream)>>>(
+            reinterpret_cast<const double2*>(d), N, Ks, ps, ps2, npairs, Kp, reinterpret_cast<__nv_bfloat16*>(L));
+    else
+        kron_lhs_split_kernel<2><<<blocks, 256, 0, as_stream(stream)>>>(
+            reinterpret_cast<const double2*>(d), N, Ks, ps, ps2, npairs, Kp, reinterpret_cast<__nv_bfloat16*>(L));
     return launch_status();
 }
 
-VTB_API int vtb_coeff_wn_split(const double* Wn, int N, int Kt, void* R3, void* stream) {
-    VTB_CHECK_ARG(N > 0 && Kt > 0 && Wn && R3 && ((uintptr_t)R3 & 15) == 0);
+static int wn_split(const double* Wn, int N, int Kt, void* R, int parts, void* stream) {
+    VTB_CHECK_ARG(N > 0 && Kt > 0 && Wn && R && ((uintptr_t)R & 15) == 0);
     const int Kp = ceil_div(2 * N, 64) * 64;
     const int64_t total = (int64_t)Kt * Kt * Kp;
-    kron_rhs_split_kernel<<<(int)std::min<int64_t>(ceil_div(total, 256), 32 * kNumSMs), 256, 0, as_stream(stream)>>>(
-        reinterpret_cast<const double2*>(Wn), N, Kt * Kt, Kp, reinterpret_cast<__nv_bfloat16*>(R3));
+    const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 32 * kNumSMs);
+    if (parts == 3)
+        kron_rhs_split_kernel<3><<<blocks, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(Wn), N,
+                                                                         Kt * Kt, Kp,
+                                                                         reinterpret_cast<__nv_bfloat16*>(R));
+    else
+        kron_rhs_split_kernel<2><<<blocks, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(Wn), N,
+                                                                         Kt * Kt, Kp,
+                                                                         reinterpret_cast<__nv_bfloat16*>(R));
     return launch_status();
+}
+
+VTB_API int vtb_coeff_lhs_split(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs,
+                                void* L3, void* stream) {
+    return lhs_split(d, N, Ks, ps, ps2, npairs, L3, 3, stream);
+}
+
+VTB_API int vtb_coeff_wn_split(const double* Wn, int N, int Kt, void* R3, void* stream) {
+    return wn_split(Wn, N, Kt, R3, 3, stream);
+}
+
+// [hi | lo] operands (2 * npairs x 2Kp and Kt^2 x 2Kp bf16, Kp = 2N rounded up
+// to 64) for vtb_tc_gemm_bf16x3_bn: the same Gram with two thirds of the
+// operand bytes of the [hi | hi | lo] / [hi | lo | hi] layouts.
+VTB_API int vtb_coeff_lhs_split2(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs,
+                                 void* L2, void* stream) {
+    return lhs_split(d, N, Ks, ps, ps2, npairs, L2, 2, stream);
+}
+
+VTB_API int vtb_coeff_wn_split2(const double* Wn, int N, int Kt, void* R2, void* stream) {
+    return wn_split(Wn, N, Kt, R2, 2, stream);
 }
 
 VTB_API int vtb_coeff_scatter(const float* C, int64_t ldc, const int32_t* ps, const int32_t* ps2, int npairs, int Kt,

@@ -58,11 +58,11 @@ constexpr int kIafWarps = 4;
 constexpr int kIafAhead = 8;   // chunks of 32 samples prefetched ahead
 
 template <bool RT>
-__global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
-    __shared__ double s_area[kIafWarps][32];
+__global__ void __launch_bounds__(kIafWarps * 32, 1) iaf_scan_kernel(IafArgs p) {
+    __shared__ __align__(16) double s_area[kIafWarps][32];
     __shared__ double s_y1[kIafWarps][32];
     __shared__ double s_y2[kIafWarps][32];
-    __shared__ double s_v[kIafWarps][32];
+    __shared__ __align__(16) double s_v[kIafWarps][32];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -122,65 +122,20 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
         s_y2[w][lane] = y2l;
         __syncwarp();
         const int nst = min(32, steps - t0);
-        // Fast chunk: every step of the 32 has the positive-slope form and at
-        // most one frame-block boundary falls inside.  The warp runs the
-        // membrane and time recursions v += area_j, tc += dt in the
-        // reference's order as one register chain (uniform across lanes: the
-        // areas are shared-memory broadcasts, off the chain's critical path),
-        // storing the membrane value after each step; lane j then tests step
-        // j's value and a ballot finds the first crossing.  Steps before it
-        // are final as computed (the same float64 operations in the same
-        // order as the step loop below); tc at the step before the crossing
-        // is recomputed by the same additions, and the crossing step and the
-        // rest of the chunk run through the step loop from the exact state.
-        int jstart = 0;
-        if (nst == 32 && posmask == full && (bstep >= 32 || bstep <= 0)) {
-            const int rpos = (next_reset >= t0 && next_reset < t0 + 32) ? next_reset - t0 : -1;
-            double v = v0, tt = tc;
-            if (rpos < 0) {
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    v = v + s_area[w][j];
-                    tt = tt + dt;
-                    s_v[w][j] = v;
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    if (j == rpos) tt = 0.0;
-                    v = v + s_area[w][j];
-                    tt = tt + dt;
-                    s_v[w][j] = v;
-                }
-            }
-            __syncwarp();
-            const double s_l = s_v[w][lane];
-            const unsigned cross = __ballot_sync(full, s_l >= delta);
-            const unsigned nearm = __ballot_sync(full, fabs(s_l - delta) < p.near_eps);
-            const int f = cross ? __ffs(cross) - 1 : 32;
-            near += (unsigned long long)__popc(f < 32 ? (nearm & ((1u << f) - 1u)) : nearm);
-            if (f == 32) {
-                v0 = v;
-                tc = tt;
-            } else if (f > 0) {
-                v0 = s_v[w][f - 1];
-                double t2 = tc;
-                for (int j = 0; j < f; ++j) {
-                    if (j == rpos) t2 = 0.0;
-                    t2 = t2 + dt;
-                }
-                tc = t2;
-            }
-            if (f > 0 && rpos >= 0 && rpos < f) {
-                cnt_block = 0;
-                ++block;
-                next_reset += bstep;
-                lim_block = block_limit(block);
-            }
-            __syncwarp();
-            jstart = f;
-        }
-        for (int j = jstart; j < nst; ++j) {
+        // The chunk is walked as register chains between slow steps.  A
+        // chain covers the steps j0.. of the positive-slope form: the warp
+        // runs the membrane and time recursions v += area_j, tc += dt in the
+        // reference's order (uniform across lanes: the 32 areas are loaded
+        // from shared memory into registers first, so the chain is nothing
+        // but dependent adds) and stores the membrane value after each step;
+        // lane j tests step j's value and ballots find the first step that is
+        // a crossing or not of the positive-slope form.  Steps before it are
+        // final as computed (the same float64 operations in the same order as
+        // the reference's step loop); tc before it is recomputed by the same
+        // additions.  That step runs the reference's full loop (slow_step)
+        // from the exact state, and the next chain starts after it.  With
+        // frame blocks shorter than 32 steps every step takes the full loop.
+        auto slow_step = [&](int j) {
             const int g = t0 + j;
             if (g == next_reset) {  // start of the next frame block
                 tc = 0.0;
@@ -197,7 +152,7 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
                 if (!(s >= delta)) {  // the common step: no crossing
                     v0 = s;
                     tc += dt;
-                    continue;
+                    return;
                 }
                 // crossing(s) inside this step: the reference's loop
                 double y1 = s_y1[w][j];
@@ -229,7 +184,7 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
                     near += (fabs(s2 - delta) < p.near_eps) ? 1ull : 0ull;
                     if (!(s2 >= delta)) break;
                 }
-                if (stop) break;
+                if (stop) return;
                 v0 += area;
                 tc += ddt;
             } else {
@@ -262,14 +217,90 @@ __global__ void __launch_bounds__(kIafWarps * 32) iaf_scan_kernel(IafArgs p) {
                     a = ((y2 - y1) / ddt);
                     if (count >= p.cap) { stop = true; break; }
                 }
-                if (stop) break;
+                if (stop) return;
                 v0 += (y1 + y2) / 2 * ddt;
                 tc += ddt;
             }
+        };
+        // the next chunk's inputs, issued before the walk so the division overlaps it
+        const double ynn = (xpre + bia) / kap;
+        const bool fastok = bstep >= 32 || bstep <= 0;
+        int j0 = 0;
+        while (j0 < nst && !stop) {
+            int f = j0;
+            if (fastok) {
+                const int rpos = (next_reset >= t0 + j0 && next_reset < t0 + nst) ? next_reset - t0 : -1;
+                double ar[32];
+#pragma unroll
+                for (int j = 0; j < 32; j += 2) {
+                    const double2 q = *reinterpret_cast<const double2*>(&s_area[w][j]);
+                    ar[j] = q.x;
+                    ar[j + 1] = q.y;
+                }
+                double v = v0, tt = tc;
+                if (j0 == 0 && nst == 32 && rpos < 0) {
+#pragma unroll
+                    for (int j = 0; j < 32; j += 2) {
+                        v = v + ar[j];
+                        tt = tt + dt;
+                        const double va = v;
+                        v = v + ar[j + 1];
+                        tt = tt + dt;
+                        *reinterpret_cast<double2*>(&s_v[w][j]) = make_double2(va, v);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; j += 2) {
+                        if (j >= j0 && j < nst) {
+                            if (j == rpos) tt = 0.0;
+                            v = v + ar[j];
+                            tt = tt + dt;
+                        }
+                        const double va = v;
+                        if (j + 1 >= j0 && j + 1 < nst) {
+                            if (j + 1 == rpos) tt = 0.0;
+                            v = v + ar[j + 1];
+                            tt = tt + dt;
+                        }
+                        *reinterpret_cast<double2*>(&s_v[w][j]) = make_double2(va, v);
+                    }
+                }
+                __syncwarp();
+                const double s_l = s_v[w][lane];
+                const bool inseg = lane >= j0 && lane < nst;
+                const unsigned npos = __ballot_sync(full, inseg && !((posmask >> lane) & 1u));
+                const unsigned cross = __ballot_sync(full, inseg && s_l >= delta);
+                const unsigned nearm = __ballot_sync(full, inseg && fabs(s_l - delta) < p.near_eps);
+                const unsigned stopm = npos | cross;
+                f = stopm ? __ffs(stopm) - 1 : nst;
+                near += (unsigned long long)__popc(f < 32 ? (nearm & ((1u << f) - 1u)) : nearm);
+                if (f == nst) {
+                    v0 = v;
+                    tc = tt;
+                } else if (f > j0) {
+                    v0 = s_v[w][f - 1];
+                    double t2 = tc;
+                    for (int j = j0; j < f; ++j) {
+                        if (j == rpos) t2 = 0.0;
+                        t2 = t2 + dt;
+                    }
+                    tc = t2;
+                }
+                if (rpos >= j0 && rpos < f) {
+                    cnt_block = 0;
+                    ++block;
+                    next_reset += bstep;
+                    lim_block = block_limit(block);
+                }
+                __syncwarp();
+                if (f >= nst) break;
+            }
+            slow_step(f);
+            j0 = f + 1;
         }
         __syncwarp();
         ycur = ynext;
-        ynext = (xpre + bia) / kap;
+        ynext = ynn;
     }
     if (lane == 0) {
         p.v0[n] = v0;

@@ -74,22 +74,29 @@ __device__ __forceinline__ double2 gram_from_pairs(const float* __restrict__ C, 
     return make_double2(re, conj ? -im : im);
 }
 
+// Mr from the tensor-core Gram: one block row of threads per real row R,
+// one thread per complex column k <= h, which reads M[j][k] and M[j][K-1-k]
+// once and writes both real columns they feed (k and h+1+k).
 template <typename OutT>
 __global__ void __launch_bounds__(256) real_scatter_kernel(const float* __restrict__ C, int64_t ldc, int Ks, int Kt,
                                                            OutT* __restrict__ Mr, int64_t ldr) {
     const int K = Ks * Kt, h = (K - 1) / 2;
-    const int64_t total = (int64_t)K * K;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int R = (int)(i / K), Q = (int)(i - (int64_t)R * K);
-        int j, p, k, q;
-        real_split(R, h, j, p);
-        real_split(Q, h, k, q);
+    const int R = blockIdx.y;
+    int j, p;
+    real_split(R, h, j, p);
+    OutT* row = Mr + (int64_t)R * ldr;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= h; k += gridDim.x * blockDim.x) {
         const double2 A = gram_from_pairs(C, ldc, Ks, Kt, j, k);
         const double2 B = gram_from_pairs(C, ldc, Ks, Kt, j, K - 1 - k);
-        double v = real_entry(A, B, p, q);
-        if (R == h) v *= kInvSqrt2;
-        if (Q == h) v *= kInvSqrt2;
-        Mr[(int64_t)R * ldr + Q] = (OutT)v;
+        double v0 = real_entry(A, B, p, 0);
+        if (R == h) v0 *= kInvSqrt2;
+        if (k == h) v0 *= kInvSqrt2;
+        row[k] = (OutT)v0;
+        if (k < h) {
+            double v1 = real_entry(A, B, p, 1);
+            if (R == h) v1 *= kInvSqrt2;
+            row[h + 1 + k] = (OutT)v1;
+        }
     }
 }
 
@@ -762,14 +769,15 @@ using namespace vtb;
 VTB_API int vtb_coeff_real_scatter(const float* C, int64_t ldc, int Ks, int Kt, void* Mr, int64_t ldr, int out_f64,
                                    void* stream) {
     VTB_CHECK_ARG(Ks > 0 && (Ks & 1) && Kt > 0 && (Kt & 1) && C && Mr && ldr >= (int64_t)Ks * Kt);
-    const int64_t total = (int64_t)Ks * Kt * Ks * Kt;
-    const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 16 * kNumSMs);
+    const int K = Ks * Kt, h = (K - 1) / 2;
+    VTB_CHECK_ARG(K <= 65535);
+    const dim3 grid(ceil_div(h + 1, 256), K);
     if (out_f64)
-        real_scatter_kernel<double><<<blocks, 256, 0, as_stream(stream)>>>(C, ldc, Ks, Kt,
-                                                                           reinterpret_cast<double*>(Mr), ldr);
+        real_scatter_kernel<double><<<grid, 256, 0, as_stream(stream)>>>(C, ldc, Ks, Kt, reinterpret_cast<double*>(Mr),
+                                                                         ldr);
     else
-        real_scatter_kernel<float><<<blocks, 256, 0, as_stream(stream)>>>(C, ldc, Ks, Kt, reinterpret_cast<float*>(Mr),
-                                                                          ldr);
+        real_scatter_kernel<float><<<grid, 256, 0, as_stream(stream)>>>(C, ldc, Ks, Kt, reinterpret_cast<float*>(Mr),
+                                                                        ldr);
     return launch_status();
 }
 

@@ -158,7 +158,7 @@ template <typename OutT, int KT>
 __global__ void __launch_bounds__(kHThreads) harmonics_kernel(const double* __restrict__ H, int ldh, int P,
                                                               double W, double t0, double dt, int Nt, int fchunks,
                                                               OutT* __restrict__ u) {
-    __shared__ __align__(16) double Cs[kHFrames][KT + 1];
+    __shared__ __align__(16) double Cs[kHFrames + 1][KT + 1];   // one spare row for an odd frame count
     constexpr int MT = (KT - 1) / 2;
     const int tid = threadIdx.x;
     const int ptile = blockIdx.x / fchunks, fc = blockIdx.x % fchunks;
@@ -188,21 +188,29 @@ __global__ void __launch_bounds__(kHThreads) harmonics_kernel(const double* __re
             }
         }
         __syncthreads();
-        for (int q = 0; q < nf; ++q) {
-            double acc[kHPix];
+        // two frames at a time: 2 x kHPix independent FMA chains per thread
+        for (int q = 0; q < nf; q += 2) {
+            const bool two = q + 1 < nf;
+            double acc0[kHPix], acc1[kHPix];
 #pragma unroll
-            for (int j = 0; j < kHPix; ++j) acc[j] = 0.0;
+            for (int j = 0; j < kHPix; ++j) acc0[j] = acc1[j] = 0.0;
 #pragma unroll
             for (int k = 0; k < KT; ++k) {
-                const double cv = Cs[q][k];
+                const double c0 = Cs[q][k], c1 = Cs[q + 1][k];
 #pragma unroll
-                for (int j = 0; j < kHPix; ++j) acc[j] = fma(cv, h[j][k], acc[j]);
+                for (int j = 0; j < kHPix; ++j) {
+                    acc0[j] = fma(c0, h[j][k], acc0[j]);
+                    acc1[j] = fma(c1, h[j][k], acc1[j]);
+                }
             }
             OutT* uf = u + (int64_t)(f0 + q) * P;
 #pragma unroll
             for (int j = 0; j < kHPix; ++j) {
                 const int p = pbase + tid + kHThreads * j;
-                if (p < P) stream_store(uf + p, acc[j]);
+                if (p < P) {
+                    stream_store(uf + p, acc0[j]);
+                    if (two) stream_store(uf + P + p, acc1[j]);
+                }
             }
         }
     }

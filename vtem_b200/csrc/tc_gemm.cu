@@ -86,32 +86,48 @@ struct TcIdesc {
                                       ((uint32_t)(kTcBM >> 4) << 24);
 };
 
-template <int BN>
+// X3 (three-product mode): the operands are [hi | lo] along K (2K columns)
+// and every k-block issues hi*hi, hi*lo and lo*hi from the same
+// shared-memory tiles, so no operand part is stored or loaded twice.
+template <int BN, bool X3>
+struct TcCfg {
+    static constexpr int kParts = X3 ? 2 : 1;
+    static constexpr int kStageBytes = kParts * (kTcBM + BN) * kTcBK * 2;
+    static constexpr int kFit = (220 * 1024) / kStageBytes;
+    static constexpr int kStages = kFit < kTcStages ? kFit : kTcStages;
+};
+
+template <int BN, bool X3 = false>
 struct TcSmem {
-    __nv_bfloat16 a[kTcStages][kTcBM * kTcBK];
-    __nv_bfloat16 b[kTcStages][BN * kTcBK];
-    uint64_t full[kTcStages];
-    uint64_t empty[kTcStages];
+    using Cfg = TcCfg<BN, X3>;
+    __nv_bfloat16 a[Cfg::kStages][Cfg::kParts][kTcBM * kTcBK];
+    __nv_bfloat16 b[Cfg::kStages][Cfg::kParts][BN * kTcBK];
+    uint64_t full[Cfg::kStages];
+    uint64_t empty[Cfg::kStages];
     uint64_t done;
     uint32_t tmem_base;
 };
 
 // One 128 x BN output tile (rows m0.., columns n0..) of C = alpha A B^T; the
-// tensor maps may live in kernel parameters or in global memory.
-template <int BN, typename OutT>
+// tensor maps may live in kernel parameters or in global memory.  With X3,
+// K is the width of one operand part and C = A_hi B_hi^T + A_hi B_lo^T +
+// A_lo B_hi^T.
+template <int BN, typename OutT, bool X3 = false>
 __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMap* tmB, int M, int N, int K, int m0,
                                         int n0, OutT* __restrict__ C, int64_t c_m, int64_t c_n, double alpha,
                                         int accumulate, int32_t* __restrict__ err, uint32_t limit,
                                         uint8_t* smem_raw) {
+    using Sm = TcSmem<BN, X3>;
+    constexpr int S = Sm::Cfg::kStages;
     // 1024-byte alignment of the stage buffers (the swizzle atoms)
-    TcSmem<BN>& sm = *reinterpret_cast<TcSmem<BN>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    Sm& sm = *reinterpret_cast<Sm*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int nk = K / kTcBK;
     constexpr uint32_t kTmemCols = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
 
     if (tid == 0) {
-        for (int s = 0; s < kTcStages; ++s) {
+        for (int s = 0; s < S; ++s) {
             mbar_init(&sm.full[s], 1);
             mbar_init(&sm.empty[s], 1);
         }
@@ -133,14 +149,18 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
     int issued = 0;   // TMA stages the producer issued
     if (tid == 0) {
         // producer
-        constexpr uint32_t bytes = (kTcBM + BN) * kTcBK * 2;
+        constexpr uint32_t bytes = Sm::Cfg::kStageBytes;
         for (int kb = 0; kb < nk && ok; ++kb) {
-            const int s = kb % kTcStages;
-            if (kb >= kTcStages) ok = mbar_wait(&sm.empty[s], ((kb / kTcStages) + 1) & 1, limit);
+            const int s = kb % S;
+            if (kb >= S) ok = mbar_wait(&sm.empty[s], ((kb / S) + 1) & 1, limit);
             if (!ok) break;
             mbar_expect_tx(&sm.full[s], bytes);
-            tma_load_2d(sm.a[s], tmA, &sm.full[s], kb * kTcBK, m0);
-            tma_load_2d(sm.b[s], tmB, &sm.full[s], kb * kTcBK, n0);
+            tma_load_2d(sm.a[s][0], tmA, &sm.full[s], kb * kTcBK, m0);
+            tma_load_2d(sm.b[s][0], tmB, &sm.full[s], kb * kTcBK, n0);
+            if (X3) {
+                tma_load_2d(sm.a[s][Sm::Cfg::kParts - 1], tmA, &sm.full[s], K + kb * kTcBK, m0);
+                tma_load_2d(sm.b[s][Sm::Cfg::kParts - 1], tmB, &sm.full[s], K + kb * kTcBK, n0);
+            }
             issued = kb + 1;
         }
         if (!ok) atomicExch(err, VTB_TIMEOUT);
@@ -148,23 +168,27 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
         // MMA issuer
         constexpr uint32_t idesc = TcIdesc<BN>::value;
         for (int kb = 0; kb < nk && ok; ++kb) {
-            const int s = kb % kTcStages;
-            ok = mbar_wait(&sm.full[s], (kb / kTcStages) & 1, limit);
+            const int s = kb % S;
+            ok = mbar_wait(&sm.full[s], (kb / S) & 1, limit);
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint64_t da = smem_desc_sw128(sm.a[s]);
-            const uint64_t db = smem_desc_sw128(sm.b[s]);
+            // products of this k-block: (A part, B part) = (0,0); with X3 also (0,1) and (1,0)
 #pragma unroll
-            for (int j = 0; j < kTcBK / 16; ++j) {
-                // advance 16 bf16 (32 bytes) along K inside the swizzle row
-                const uint64_t adv = (uint64_t)(j * 2);
-                const uint32_t acc = (kb > 0 || j > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                    "l"(da + adv), "l"(db + adv), "r"(idesc), "r"(acc)
-                    : "memory");
+            for (int pr = 0; pr < (X3 ? 3 : 1); ++pr) {
+                const uint64_t da = smem_desc_sw128(sm.a[s][pr == 2 ? Sm::Cfg::kParts - 1 : 0]);
+                const uint64_t db = smem_desc_sw128(sm.b[s][pr == 1 ? Sm::Cfg::kParts - 1 : 0]);
+#pragma unroll
+                for (int j = 0; j < kTcBK / 16; ++j) {
+                    // advance 16 bf16 (32 bytes) along K inside the swizzle row
+                    const uint64_t adv = (uint64_t)(j * 2);
+                    const uint32_t acc = (kb > 0 || pr > 0 || j > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                        "l"(da + adv), "l"(db + adv), "r"(idesc), "r"(acc)
+                        : "memory");
+                }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                              smem_u32(&sm.empty[s]))
@@ -212,8 +236,8 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
     }
     // a CTA that gave up drains its producer's issued TMA loads before it exits
     if (tid == 0)
-        for (int kb = issued > kTcStages ? issued - kTcStages : 0; kb < issued; ++kb)
-            mbar_wait(&sm.full[kb % kTcStages], (kb / kTcStages) & 1, kDrainLimit);
+        for (int kb = issued > S ? issued - S : 0; kb < issued; ++kb)
+            mbar_wait(&sm.full[kb % S], (kb / S) & 1, kDrainLimit);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
@@ -221,14 +245,14 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
     }
 }
 
-template <int BN, typename OutT>
+template <int BN, typename OutT, bool X3>
 __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
                                                          const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
                                                          OutT* __restrict__ C, int64_t c_m, int64_t c_n, double alpha,
                                                          int accumulate, int32_t* __restrict__ err, uint32_t limit) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    tc_tile<BN, OutT>(&tmA, &tmB, M, N, K, blockIdx.y * kTcBM, blockIdx.x * BN, C, c_m, c_n, alpha, accumulate, err,
-                      limit, smem_raw);
+    tc_tile<BN, OutT, X3>(&tmA, &tmB, M, N, K, blockIdx.y * kTcBM, blockIdx.x * BN, C, c_m, c_n, alpha, accumulate,
+                          err, limit, smem_raw);
 }
 
 // Grouped GEMM: many independent problems C_p = A_p B_p^T (float32 output,
@@ -246,7 +270,7 @@ struct TcGroupProblem {
     int pad[6];
 };
 
-template <int BN>
+template <int BN, bool X3>
 __global__ void __launch_bounds__(128, 1) tc_gemm_grouped_kernel(const TcGroupProblem* __restrict__ probs, int nprob,
                                                                   uint32_t limit) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -266,8 +290,8 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_grouped_kernel(const TcGroupPr
     }
     const int ntn = (p->N + BN - 1) / BN;
     const int t = tile - p->tile_start;
-    tc_tile<BN, float>(&p->ma, &p->mb, p->M, p->N, p->K, (t / ntn) * kTcBM, (t % ntn) * BN, p->C, p->ldc, 1, 1.0, 0,
-                       p->err, limit, smem_raw);
+    tc_tile<BN, float, X3>(&p->ma, &p->mb, p->M, p->N, p->K, (t / ntn) * kTcBM, (t % ntn) * BN, p->C, p->ldc, 1, 1.0,
+                           0, p->err, limit, smem_raw);
 }
 
 // ------------------------------------------------------------------ split-bf16 operands
@@ -287,6 +311,30 @@ __global__ void split_bf16x3_kernel(const InT* __restrict__ src, int rows, int K
         d[0] = hi;
         d[Kp] = pattern == 0 ? hi : lo;
         d[2 * Kp] = pattern == 0 ? lo : hi;
+    }
+}
+
+// dst[r][seg*Kp + k]: seg 0 = hi, seg 1 = lo (the three-product mode's
+// layout).  A thread converts 8 consecutive k and writes 16 bytes per part.
+template <typename InT>
+__global__ void split_bf16x2_kernel(const InT* __restrict__ src, int rows, int K, int64_t ld, int64_t ks,
+                                    double scale, int Kp, __nv_bfloat16* __restrict__ dst) {
+    const int gpr = Kp / 8;     // groups of 8 per row
+    const int64_t total = (int64_t)rows * gpr;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(g / gpr), k0 = (int)(g % gpr) * 8;
+        const InT* row = src + (int64_t)r * ld;
+        __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int k = k0 + i;
+            const double x = k < K ? (double)__ldg(row + (int64_t)k * ks) * scale : 0.0;
+            hi[i] = __float2bfloat16_rn((float)x);
+            lo[i] = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi[i])));
+        }
+        __nv_bfloat16* d = dst + (int64_t)r * 2 * Kp + k0;
+        *reinterpret_cast<uint4*>(d) = *reinterpret_cast<const uint4*>(hi);
+        *reinterpret_cast<uint4*>(d + Kp) = *reinterpret_cast<const uint4*>(lo);
     }
 }
 
@@ -318,22 +366,23 @@ static int make_map(CUtensorMap* map, const void* base, int rows, int K, int64_t
     return r == CUDA_SUCCESS ? VTB_OK : VTB_BAD_ARG;
 }
 
-template <int BN, typename OutT>
+template <int BN, typename OutT, bool X3>
 static int launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, OutT* C, int64_t c_m,
                      int64_t c_n, double alpha, int accumulate, int32_t* err, cudaStream_t s) {
-    const size_t sm = sizeof(TcSmem<BN>) + 1024;
+    const size_t sm = sizeof(TcSmem<BN, X3>) + 1024;
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [&]() {
-        attr = cudaFuncSetAttribute(tc_gemm_kernel<BN, OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        attr = cudaFuncSetAttribute(tc_gemm_kernel<BN, OutT, X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sm);
     });
     if (attr != cudaSuccess) {
         set_last_cuda_error(attr);
         return VTB_CUDA_ERR;
     }
     dim3 grid(ceil_div(N, BN), ceil_div(M, kTcBM));
-    tc_gemm_kernel<BN, OutT><<<grid, 128, sm, s>>>(ma, mb, M, N, K, C, c_m, c_n, alpha, accumulate, err,
-                                                   wait_limit(kWaitLimit));
+    tc_gemm_kernel<BN, OutT, X3><<<grid, 128, sm, s>>>(ma, mb, M, N, K, C, c_m, c_n, alpha, accumulate, err,
+                                                       wait_limit(kWaitLimit));
     return launch_status();
 }
 
@@ -360,37 +409,75 @@ VTB_API int vtb_split_bf16x3(const void* src, int src_f32, int rows, int K, int6
     return launch_status();
 }
 
-template <int BN>
+VTB_API int vtb_split_bf16x2(const void* src, int src_f32, int rows, int K, int64_t ld, int64_t k_stride,
+                             double scale, void* dst, void* stream) {
+    VTB_CHECK_ARG(rows >= 0 && K >= 0);
+    if (rows == 0) return VTB_OK;
+    VTB_CHECK_ARG(src && dst && ((uintptr_t)dst & 15) == 0);
+    const int Kp = ceil_div(K, kTcBK) * kTcBK;
+    const int64_t total = (int64_t)rows * (Kp / 8);
+    const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 16 * kNumSMs);
+    if (src_f32)
+        split_bf16x2_kernel<float><<<blocks, 256, 0, as_stream(stream)>>>(
+            reinterpret_cast<const float*>(src), rows, K, ld, k_stride, scale, Kp,
+            reinterpret_cast<__nv_bfloat16*>(dst));
+    else
+        split_bf16x2_kernel<double><<<blocks, 256, 0, as_stream(stream)>>>(
+            reinterpret_cast<const double*>(src), rows, K, ld, k_stride, scale, Kp,
+            reinterpret_cast<__nv_bfloat16*>(dst));
+    return launch_status();
+}
+
+template <int BN, bool X3>
 static int tc_dispatch(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
                        int out_f64, double alpha, int accumulate, int32_t* err, cudaStream_t s) {
     CUtensorMap ma, mb;
-    int st = make_map(&ma, A, M, K, K, kTcBM);
+    const int Kw = X3 ? 2 * K : K;     // columns of the operand arrays
+    int st = make_map(&ma, A, M, Kw, Kw, kTcBM);
     if (st) return st;
-    st = make_map(&mb, B, N, K, K, BN);
+    st = make_map(&mb, B, N, Kw, Kw, BN);
     if (st) return st;
     if (out_f64)
-        return launch_tc<BN, double>(ma, mb, M, N, K, reinterpret_cast<double*>(C), c_m, c_n, alpha, accumulate, err, s);
-    return launch_tc<BN, float>(ma, mb, M, N, K, reinterpret_cast<float*>(C), c_m, c_n, alpha, accumulate, err, s);
+        return launch_tc<BN, double, X3>(ma, mb, M, N, K, reinterpret_cast<double*>(C), c_m, c_n, alpha, accumulate,
+                                         err, s);
+    return launch_tc<BN, float, X3>(ma, mb, M, N, K, reinterpret_cast<float*>(C), c_m, c_n, alpha, accumulate, err,
+                                    s);
 }
 
-// Output tile widths the kernel is built for (M tile = 128): the autotuner
-// of vtem_b200.autotune picks one per problem shape.
-VTB_API int vtb_tc_gemm_bf16_bn(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
-                                int out_f64, double alpha, int accumulate, int32_t* err, int bn, void* stream) {
+template <bool X3>
+static int tc_gemm_bn(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
+                      int out_f64, double alpha, int accumulate, int32_t* err, int bn, void* stream) {
     VTB_CHECK_ARG(M >= 0 && N >= 0 && K > 0 && (K % kTcBK) == 0);
     if (M == 0 || N == 0) return VTB_OK;
     VTB_CHECK_ARG(A && B && C && err && ((uintptr_t)A & 15) == 0 && ((uintptr_t)B & 15) == 0);
     VTB_CHECK_ARG(ceil_div(M, kTcBM) <= 65535);
     cudaStream_t s = as_stream(stream);
     switch (bn) {
-        case 64: return tc_dispatch<64>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
-        case 96: return tc_dispatch<96>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
-        case 128: return tc_dispatch<128>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
-        case 160: return tc_dispatch<160>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
-        case 192: return tc_dispatch<192>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
-        case 256: return tc_dispatch<256>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 64: return tc_dispatch<64, X3>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 96: return tc_dispatch<96, X3>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 128: return tc_dispatch<128, X3>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 160: return tc_dispatch<160, X3>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 192: return tc_dispatch<192, X3>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        case 256: return tc_dispatch<256, X3>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
         default: return VTB_BAD_ARG;
     }
+}
+
+// Output tile widths the kernel is built for (M tile = 128): the autotuner
+// of vtem_b200.autotune picks one per problem shape.
+VTB_API int vtb_tc_gemm_bf16_bn(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
+                                int out_f64, double alpha, int accumulate, int32_t* err, int bn, void* stream) {
+    return tc_gemm_bn<false>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, bn, stream);
+}
+
+// Three-product split-bf16 GEMM: A (M x 2K) = [A_hi | A_lo] and B (N x 2K) =
+// [B_hi | B_lo] (vtb_split_bf16x2), C = alpha (A_hi B_hi^T + A_hi B_lo^T +
+// A_lo B_hi^T): the products of the three-part layout of vtb_split_bf16x3
+// with two thirds of its operand bytes.
+VTB_API int vtb_tc_gemm_bf16x3_bn(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m,
+                                  int64_t c_n, int out_f64, double alpha, int accumulate, int32_t* err, int bn,
+                                  void* stream) {
+    return tc_gemm_bn<true>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, bn, stream);
 }
 
 VTB_API int vtb_tc_gemm_bf16(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
@@ -406,9 +493,9 @@ VTB_API int64_t vtb_tc_group_bytes(int nprob) { return nprob > 0 ? (int64_t)npro
 // problems' device pointers and sizes); *total_tiles receives the grid size.
 // The caller copies the array to device memory (vtb_tc_group_bytes bytes,
 // 64-byte aligned) before vtb_tc_gemm_grouped.
-VTB_API int vtb_tc_group_build(void* host_desc, int nprob, const uint64_t* A, const int* M, const uint64_t* B,
-                               const int* N, const int* K, const uint64_t* C, const int64_t* ldc, const uint64_t* err,
-                               int bn, int* total_tiles) {
+static int group_build(void* host_desc, int nprob, const uint64_t* A, const int* M, const uint64_t* B, const int* N,
+                       const int* K, const uint64_t* C, const int64_t* ldc, const uint64_t* err, int bn, int parts,
+                       int* total_tiles) {
     VTB_CHECK_ARG(host_desc && nprob > 0 && A && M && B && N && K && C && ldc && err && total_tiles);
     VTB_CHECK_ARG(bn == 64 || bn == 128 || bn == 256);
     TcGroupProblem* d = reinterpret_cast<TcGroupProblem*>(host_desc);
@@ -417,9 +504,10 @@ VTB_API int vtb_tc_group_build(void* host_desc, int nprob, const uint64_t* A, co
         VTB_CHECK_ARG(M[p] > 0 && N[p] > 0 && K[p] > 0 && (K[p] % kTcBK) == 0 && A[p] && B[p] && C[p] && err[p]);
         VTB_CHECK_ARG((A[p] & 15) == 0 && (B[p] & 15) == 0);
         memset(&d[p], 0, sizeof(TcGroupProblem));
-        int st = make_map(&d[p].ma, reinterpret_cast<const void*>(A[p]), M[p], K[p], K[p], kTcBM);
+        const int Kw = parts * K[p];
+        int st = make_map(&d[p].ma, reinterpret_cast<const void*>(A[p]), M[p], Kw, Kw, kTcBM);
         if (st) return st;
-        st = make_map(&d[p].mb, reinterpret_cast<const void*>(B[p]), N[p], K[p], K[p], bn);
+        st = make_map(&d[p].mb, reinterpret_cast<const void*>(B[p]), N[p], Kw, Kw, bn);
         if (st) return st;
         d[p].C = reinterpret_cast<float*>(C[p]);
         d[p].ldc = ldc[p];
@@ -434,31 +522,56 @@ VTB_API int vtb_tc_group_build(void* host_desc, int nprob, const uint64_t* A, co
     return VTB_OK;
 }
 
-template <int BN>
+VTB_API int vtb_tc_group_build(void* host_desc, int nprob, const uint64_t* A, const int* M, const uint64_t* B,
+                               const int* N, const int* K, const uint64_t* C, const int64_t* ldc, const uint64_t* err,
+                               int bn, int* total_tiles) {
+    return group_build(host_desc, nprob, A, M, B, N, K, C, ldc, err, bn, 1, total_tiles);
+}
+
+// The same for the three-product mode: A_p (M_p x 2K_p) = [hi | lo], B_p
+// (N_p x 2K_p) = [hi | lo], K_p the width of one part.
+VTB_API int vtb_tc_group_build_x3(void* host_desc, int nprob, const uint64_t* A, const int* M, const uint64_t* B,
+                                  const int* N, const int* K, const uint64_t* C, const int64_t* ldc,
+                                  const uint64_t* err, int bn, int* total_tiles) {
+    return group_build(host_desc, nprob, A, M, B, N, K, C, ldc, err, bn, 2, total_tiles);
+}
+
+template <int BN, bool X3>
 static int launch_grouped(const void* desc, int nprob, int tiles, cudaStream_t s) {
-    const size_t sm = sizeof(TcSmem<BN>) + 1024;
+    const size_t sm = sizeof(TcSmem<BN, X3>) + 1024;
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [&]() {
-        attr = cudaFuncSetAttribute(tc_gemm_grouped_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        attr = cudaFuncSetAttribute(tc_gemm_grouped_kernel<BN, X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sm);
     });
     if (attr != cudaSuccess) {
         set_last_cuda_error(attr);
         return VTB_CUDA_ERR;
     }
-    tc_gemm_grouped_kernel<BN><<<tiles, 128, sm, s>>>(reinterpret_cast<const TcGroupProblem*>(desc), nprob,
-                                                       wait_limit(kWaitLimit));
+    tc_gemm_grouped_kernel<BN, X3><<<tiles, 128, sm, s>>>(reinterpret_cast<const TcGroupProblem*>(desc), nprob,
+                                                           wait_limit(kWaitLimit));
     return launch_status();
+}
+
+template <bool X3>
+static int grouped(const void* dev_desc, int nprob, int total_tiles, int bn, void* stream) {
+    VTB_CHECK_ARG(dev_desc && nprob > 0 && total_tiles > 0 && ((uintptr_t)dev_desc & 63) == 0);
+    cudaStream_t s = as_stream(stream);
+    switch (bn) {
+        case 64: return launch_grouped<64, X3>(dev_desc, nprob, total_tiles, s);
+        case 128: return launch_grouped<128, X3>(dev_desc, nprob, total_tiles, s);
+        case 256: return launch_grouped<256, X3>(dev_desc, nprob, total_tiles, s);
+        default: return VTB_BAD_ARG;
+    }
 }
 
 // One launch over all problems of a descriptor array built with the same bn.
 VTB_API int vtb_tc_gemm_grouped(const void* dev_desc, int nprob, int total_tiles, int bn, void* stream) {
-    VTB_CHECK_ARG(dev_desc && nprob > 0 && total_tiles > 0 && ((uintptr_t)dev_desc & 63) == 0);
-    cudaStream_t s = as_stream(stream);
-    switch (bn) {
-        case 64: return launch_grouped<64>(dev_desc, nprob, total_tiles, s);
-        case 128: return launch_grouped<128>(dev_desc, nprob, total_tiles, s);
-        case 256: return launch_grouped<256>(dev_desc, nprob, total_tiles, s);
-        default: return VTB_BAD_ARG;
-    }
+    return grouped<false>(dev_desc, nprob, total_tiles, bn, stream);
+}
+
+// One launch over a descriptor array of vtb_tc_group_build_x3.
+VTB_API int vtb_tc_gemm_grouped_x3(const void* dev_desc, int nprob, int total_tiles, int bn, void* stream) {
+    return grouped<true>(dev_desc, nprob, total_tiles, bn, stream);
 }

@@ -125,8 +125,12 @@ class IAF_encode(pop_encode):
         st = torch.empty((N, cap), dtype=F64, device=x.device)
         ss = torch.empty((N, cap), dtype=torch.int32, device=x.device)
         cnt = torch.empty(N, dtype=torch.int32, device=x.device)
-        near = torch.zeros(1, dtype=torch.int64, device=x.device)
-        status = torch.zeros(1, dtype=torch.int32, device=x.device)
+        # one buffer for the near-threshold count (int64) and the status word
+        # (int32 in the low half of the second word): one read returns both
+        flags = torch.zeros(2, dtype=torch.int64, device=x.device)
+        near = flags[0:1]
+        status = flags[1:2].view(torch.int32)[0:1]
+        self._flags = flags
         if randn is not None:
             rb, rs, rn = randn.stride()
             rargs = (dptr(randn), rb, rs, rn, block_cap, dptr(self.d_sigma[sl]), dptr(self.d_delta_value[sl]))
@@ -203,7 +207,7 @@ class IAF_encode(pop_encode):
                                                      block_rate=avg_rate if check else 0.0)
             if not check:
                 break
-            code = int(status.item())
+            near_h, code = _read_flags(self._flags)
             if code == VTB_BLOCK_LIMIT or (code == VTB_OVERFLOW and i + 1 == len(caps)):
                 self.reset_timer()
                 raise ValueError("number of spikes exceeded the limit of buffer")
@@ -216,11 +220,18 @@ class IAF_encode(pop_encode):
                 self.d_delta_value.copy_(saved[2])
         self.reset_timer()
         out = DeviceSpikes(st, ss, cnt, block_frames, self.dt)
-        out.near_threshold = int(near.item()) if check else near
+        out.near_threshold = near_h if check else near
         return out
 
     def _draw_randn(self, nblocks, block_cap, N):
         return None
+
+
+def _read_flags(flags):
+    """(near-threshold count, status word) of a launch, one host read."""
+    near, word = flags.cpu().tolist()
+    code = ((int(word) + (1 << 31)) % (1 << 32)) - (1 << 31)      # the low 32 bits, signed
+    return int(near), code
 
 
 class IAF_encode_rt(IAF_encode):

@@ -134,11 +134,11 @@ class CoeffDecoder(object):
         self.npairs = int(self.ps.numel())
         from . import tc
         self.Kp2 = tc.padded_k(2 * self.N)
-        self.L3 = torch.empty((2 * self.npairs, 3 * self.Kp2), dtype=torch.bfloat16, device=device)
-        call("vtb_coeff_lhs_split", dptr(self.d), self.N, self.Ks, dptr(self.ps), dptr(self.ps2), self.npairs,
-             dptr(self.L3), stream_ptr())
+        self.Lsplit = torch.empty((2 * self.npairs, 2 * self.Kp2), dtype=torch.bfloat16, device=device)
+        call("vtb_coeff_lhs_split2", dptr(self.d), self.N, self.Ks, dptr(self.ps), dptr(self.ps2), self.npairs,
+             dptr(self.Lsplit), stream_ptr())
         KK = self.Kt * self.Kt
-        self.R3 = torch.empty((KK, 3 * self.Kp2), dtype=torch.bfloat16, device=device)
+        self.Rsplit = torch.empty((KK, 2 * self.Kp2), dtype=torch.bfloat16, device=device)
         self.C = torch.empty((2 * self.npairs, KK), dtype=torch.float32, device=device)
         self.gres = torch.empty((self.N, self.Kt), dtype=C128, device=device)
         self.r = torch.empty((self.K,), dtype=C128, device=device)
@@ -163,8 +163,8 @@ class CoeffDecoder(object):
              dptr(self.d), stream_ptr())
         self._dsw = None
         if self.solver == "mixed":
-            call("vtb_coeff_lhs_split", dptr(self.d), self.N, self.Ks, dptr(self.ps), dptr(self.ps2), self.npairs,
-                 dptr(self.L3), stream_ptr())
+            call("vtb_coeff_lhs_split2", dptr(self.d), self.N, self.Ks, dptr(self.ps), dptr(self.ps2), self.npairs,
+                 dptr(self.Lsplit), stream_ptr())
 
     def _workspace(self, mode):
         """Workspace of the real-form solver: mode 0 eigen, 1 float64
@@ -240,9 +240,9 @@ class CoeffDecoder(object):
         self.stat.zero_()
         call("vtb_coeff_rhs", dptr(self.d), self.N, self.Ks, dptr(self.gn), self.Kt, dptr(self.b), s)
         call("vtb_coeff_realify_vec", dptr(self.b), K, 1, dptr(self.br), s)
-        call("vtb_coeff_wn_split", dptr(self.Wn), self.N, self.Kt, dptr(self.R3), s)
-        autotune.gemm_bf16_tuned(dptr(self.L3), 2 * self.npairs, dptr(self.R3), KK, 3 * self.Kp2, dptr(self.C), KK, 1,
-                                 0, 1.0, 0, self._stat_ptr(7), s)
+        call("vtb_coeff_wn_split2", dptr(self.Wn), self.N, self.Kt, dptr(self.Rsplit), s)
+        autotune.gemm_bf16_tuned(dptr(self.Lsplit), 2 * self.npairs, dptr(self.Rsplit), KK, self.Kp2, dptr(self.C), KK,
+                                 1, 0, 1.0, 0, self._stat_ptr(7), s, x3=True)
         ld = self.ld32
         call("vtb_coeff_real_scatter", dptr(self.C), KK, self.Ks, self.Kt, dptr(self.Mr32), ld, 0, s)
         if self.mixed_factor == "inverse":

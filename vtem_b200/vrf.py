@@ -66,29 +66,7 @@ class vrf(object):
         ``precision="bf16x3"`` (extension) computes it on the tensor cores
         from split-bf16 operands (relative error ~1e-5) instead of float64.
         """
-        V = _dev(V).reshape(V.shape[0], -1)
-        F, P = V.shape
-        if P != self.Pxall * self.Pyall:
-            raise ValueError("video frame size does not match the RF grid")
-        rf = self._rf_full()
-        N = rf.shape[0]
-        if precision == "bf16x3":
-            from . import tc
-            return tc.gemm_split_bf16(V, rf, alpha=self.dx * self.dy,
-                                      out_layout="row" if out_layout == "time" else "col")
-        if precision != "f64":
-            raise ValueError("precision must be 'f64' or 'bf16x3'")
-        if V.dtype != F64:
-            V = V.to(F64)
-        if out_layout == "time":
-            out = torch.empty((F, N), dtype=F64, device=V.device)
-            ts, ns = N, 1
-        else:
-            out = torch.empty((N, F), dtype=F64, device=V.device)
-            ts, ns = 1, F
-        call("vtb_rf_filter", dptr(V), F, P, P, dptr(rf), N, P, self.dx * self.dy, dptr(out), ts, ns,
-             stream_ptr())
-        return out
+        return _project(V, self._rf_full(), self.dx * self.dy, self.Pxall * self.Pyall, out_layout, precision)
 
     def _rf_full(self):
         if getattr(self, "_rf_cache", None) is None or self._rf_cache.shape[0] != self.num_neurons:
@@ -280,6 +258,30 @@ class vrf_cs(vrf):
         return self.filters
 
 
+def _project(V, rf, alpha, P_expected, out_layout, precision):
+    """alpha * V rf^T, (frames, N) or (N, frames) (vrf.py:264-292)."""
+    V = _dev(V).reshape(V.shape[0], -1)
+    F, P = V.shape
+    if P != P_expected:
+        raise ValueError("video frame size does not match the RF grid")
+    N = rf.shape[0]
+    if precision == "bf16x3":
+        from . import tc
+        return tc.gemm_split_bf16(V, rf, alpha=alpha, out_layout="row" if out_layout == "time" else "col")
+    if precision != "f64":
+        raise ValueError("precision must be 'f64' or 'bf16x3'")
+    if V.dtype != F64:
+        V = V.to(F64)
+    if out_layout == "time":
+        out = torch.empty((F, N), dtype=F64, device=V.device)
+        ts, ns = N, 1
+    else:
+        out = torch.empty((N, F), dtype=F64, device=V.device)
+        ts, ns = 1, F
+    call("vtb_rf_filter", dptr(V), F, P, P, dptr(rf), N, P, alpha, dptr(out), ts, ns, stream_ptr())
+    return out
+
+
 class vrf_bank(object):
     """Concatenation of several RF objects sharing one pixel grid, seen as
     one encoder of ``sum(num_neurons)`` neurons (extension: the reference
@@ -296,5 +298,19 @@ class vrf_bank(object):
         self.num_neurons = sum(b.num_neurons for b in self.banks)
 
     def filter(self, V, out_layout="time", precision="f64"):
-        outs = [b.filter(V, out_layout, precision) for b in self.banks]
-        return torch.cat(outs, dim=1 if out_layout == "time" else 0)
+        """Every bank's projection, in bank order, as ONE product of the video
+        with the banks' stacked RFs (one pass over the video, no
+        concatenation of outputs) when the banks share the pixel area."""
+        b0 = self.banks[0]
+        if any((b.dx, b.dy) != (b0.dx, b0.dy) for b in self.banks):
+            outs = [b.filter(V, out_layout, precision) for b in self.banks]
+            return torch.cat(outs, dim=1 if out_layout == "time" else 0)
+        parts = [b._rf_full() for b in self.banks]
+        # the stacked RFs are rebuilt when any bank regenerated its RFs (the
+        # held references keep a regenerated array from reusing an address)
+        src = [b._rf_cache for b in self.banks]
+        held = getattr(self, "_rf_src", None)
+        if held is None or len(held) != len(src) or any(a is not b for a, b in zip(held, src)):
+            self._rf_all = torch.cat(parts, dim=0).contiguous()
+            self._rf_src = src
+        return _project(V, self._rf_all, b0.dx * b0.dy, self.Pxall * self.Pyall, out_layout, precision)
