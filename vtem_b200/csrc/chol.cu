@@ -109,6 +109,31 @@ __device__ bool cta_wait(const CholCtx& c, const unsigned* f, unsigned v, int* s
     return *s_ok != 0;
 }
 
+// cta_wait on two flags at once (f2 may be null): thread 0 issues both loads
+// per poll, so two flags that are already set cost one round trip
+__device__ bool cta_wait2(const CholCtx& c, const unsigned* f1, unsigned v1, const unsigned* f2, unsigned v2,
+                          int* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned it = 0;
+        for (;;) {
+            const unsigned a = c_ld_acquire(f1);
+            const unsigned b = f2 ? c_ld_acquire(f2) : v2;
+            if (a >= v1 && b >= v2) break;
+            if (++it > c.limit || *(volatile int*)c.abort_word != 0) {
+                atomicExch(c.abort_word, 1);
+                atomicMax(c.status, 3);
+                ok = 0;
+                break;
+            }
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
 // the CTA barrier orders every thread's stores before thread 0's release
 // store, whose release semantics are cumulative at GPU scope
 __device__ __forceinline__ void cta_publish(unsigned* f, unsigned v) {
@@ -158,6 +183,18 @@ __device__ bool cta_ready(const unsigned* f, unsigned v, int* s_ok) {
     if (threadIdx.x == 0) *s_ok = c_ld_acquire(f) >= v;
     __syncthreads();
     return *s_ok != 0;
+}
+
+// two such checks in one round trip (thread 0 issues both loads before
+// using either); bit 0 of the result for f1, bit 1 for f2
+__device__ int cta_ready2(const unsigned* f1, unsigned v1, const unsigned* f2, unsigned v2, int* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned a = c_ld_acquire(f1), b = c_ld_acquire(f2);
+        *s_ok = (a >= v1 ? 1 : 0) | (b >= v2 ? 2 : 0);
+    }
+    __syncthreads();
+    return *s_ok;
 }
 
 // shared tile s into tile (I, J) of A (rows and columns below K; for a
@@ -555,15 +592,14 @@ __device__ bool inv_accumulate(const CholCtx& c, CholSmem& sm, int i, int j, int
     const int T = c.T;
     const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
     const int n = k1 - k0 + 1;
-    if (!cta_wait(c, c.tflag + i * T + k0, 2u, &sm.ok)) return false;
-    if (!cta_wait(c, c.xflag + k0 * T + j, 1u, &sm.ok)) return false;
+    if (!cta_wait2(c, c.tflag + i * T + k0, 2u, c.xflag + k0 * T + j, 1u, &sm.ok)) return false;
     load_tile(c, sm.a[0], i, k0);
     load_flat(sm.b[0], c.Xinv + packed_tile(k0, j) * kCTE);
     for (int q = 0; q < n; ++q) {
         const int k = k0 + q, nb = (q + 1) & 1;
         bool next = false;
         if (q + 1 < n) {
-            next = cta_ready(c.tflag + i * T + k + 1, 2u, &sm.ok) && cta_ready(c.xflag + (k + 1) * T + j, 1u, &sm.ok);
+            next = cta_ready2(c.tflag + i * T + k + 1, 2u, c.xflag + (k + 1) * T + j, 1u, &sm.ok) == 3;
             if (next) {
                 load_tile(c, sm.a[nb], i, k + 1);
                 load_flat(sm.b[nb], c.Xinv + packed_tile(k + 1, j) * kCTE);
@@ -574,8 +610,7 @@ __device__ bool inv_accumulate(const CholCtx& c, CholSmem& sm, int i, int j, int
         __syncthreads();
         sub_ptq(acc, sm.a[q & 1], sm.b[q & 1], tr, tc, 0, kCT);
         if (q + 1 < n && !next) {
-            if (!cta_wait(c, c.tflag + i * T + k + 1, 2u, &sm.ok)) return false;
-            if (!cta_wait(c, c.xflag + (k + 1) * T + j, 1u, &sm.ok)) return false;
+            if (!cta_wait2(c, c.tflag + i * T + k + 1, 2u, c.xflag + (k + 1) * T + j, 1u, &sm.ok)) return false;
             load_tile(c, sm.a[nb], i, k + 1);
             load_flat(sm.b[nb], c.Xinv + packed_tile(k + 1, j) * kCTE);
         }
@@ -679,8 +714,8 @@ __device__ bool worker_task(const CholCtx& c, CholSmem& sm, int t) {
     // operands of update k in buffer k & 1; the next update's operands are
     // requested before this one's product when their flags are already set
     if (kend > 0) {
-        if (!cta_wait(c, c.tflag + I * T + 0, 2u, &sm.ok)) return false;
-        if (I != J && !cta_wait(c, c.tflag + J * T + 0, 2u, &sm.ok)) return false;
+        if (!cta_wait2(c, c.tflag + I * T + 0, 2u, I != J ? c.tflag + J * T + 0 : nullptr, 2u, &sm.ok))
+            return false;
         load_tile(c, sm.a[0], I, 0);
         if (I != J) load_tile(c, sm.b[0], J, 0);
     }
@@ -688,8 +723,8 @@ __device__ bool worker_task(const CholCtx& c, CholSmem& sm, int t) {
         const int nb = (k + 1) & 1;
         bool next = false;
         if (k + 1 < kend) {
-            next = cta_ready(c.tflag + I * T + k + 1, 2u, &sm.ok) &&
-                   (I == J || cta_ready(c.tflag + J * T + k + 1, 2u, &sm.ok));
+            next = I == J ? cta_ready(c.tflag + I * T + k + 1, 2u, &sm.ok)
+                          : cta_ready2(c.tflag + I * T + k + 1, 2u, c.tflag + J * T + k + 1, 2u, &sm.ok) == 3;
             if (next) {
                 // the buffers of update k-1 are free: every thread passed the barriers above
                 load_tile(c, sm.a[nb], I, k + 1);
@@ -704,8 +739,8 @@ __device__ bool worker_task(const CholCtx& c, CholSmem& sm, int t) {
         const float* pa = sm.a[k & 1];
         sub_ptq(acc, pa, I != J ? sm.b[k & 1] : pa, tr, tc, 0, kCT);
         if (k + 1 < kend && !next) {
-            if (!cta_wait(c, c.tflag + I * T + k + 1, 2u, &sm.ok)) return false;
-            if (I != J && !cta_wait(c, c.tflag + J * T + k + 1, 2u, &sm.ok)) return false;
+            if (!cta_wait2(c, c.tflag + I * T + k + 1, 2u, I != J ? c.tflag + J * T + k + 1 : nullptr, 2u, &sm.ok))
+                return false;
             load_tile(c, sm.a[nb], I, k + 1);
             if (I != J) load_tile(c, sm.b[nb], J, k + 1);
         }
@@ -754,9 +789,10 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
         // them, arrive during the factorisation of this one
         bool hx = false, hy = false;
         if (k + 1 < T) {
-            hx = k < 1 || cta_ready(c.tflag + (k + 1) * T + k, 1u, &sm.ok);
+            const int r = k < 1 ? 3 : cta_ready2(c.tflag + (k + 1) * T + k, 1u, c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok);
+            hx = (r & 1) != 0;
+            hy = (r & 2) != 0;
             if (hx) load_tile(c, X, k + 1, k);
-            hy = k < 1 || cta_ready(c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok);
             if (hy) load_tile(c, Y, k + 1, k + 1);
         }
         potrf_inv64(D, E, sm.rinv, pmin, pmax, bad, c.K - k * kCT);
@@ -792,8 +828,11 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
             acc_to(out, X, tr, tc);
         }
         __syncthreads();
+        // L_{k+1,k}, L_kk and the packed X_kk go out now and drain during the
+        // SYRK; L_{k+1,k}'s flag is released after it (the workers need that
+        // tile several microseconds later), by a thread outside warp 0 so
+        // that the next block factorisation does not wait on the release
         store_tile(c, X, k + 1, k);
-        cta_publish(c.tflag + (k + 1) * T + k, 2u);
         store_tile(c, D, k, k);
         if (inv) store_flat(c.Xinv + packed_tile(k, k) * kCTE, E);     // flag set with the next step's release
         // next diagonal tile: the workers applied updates k' < k; this CTA applies k
@@ -812,6 +851,7 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
         __syncthreads();
         if (tc <= tr) acc_to(acc, Y, tr, tc);
         __syncthreads();
+        if (threadIdx.x == kCThreads - 32) c_st_release(c.tflag + (k + 1) * T + k, 2u);
         cur ^= 1;
     }
     // pivot test (pivots of warp 0, which ran every 8 x 8 factorisation)

@@ -74,34 +74,47 @@ __global__ void __launch_bounds__(kBX * kBY) basis_kernel(const double2* __restr
         rlo[r] = Ks;
         rhi[r] = -1;
     }
-    for (int e = tid; e < Kx * kBX; e += nt) {
-        const int c = e / kBX, px = x0 + e % kBX, mx = c - Mx;
-        const int r = (((mx * (px + xd)) % Px1) + Px1) % Px1;
-        double sn, co;
-        sincospi(2.0 * r / Px1, &sn, &co);
-        const double sg = (mx & 1) ? -1.0 : 1.0;
-        ex[e] = make_double2(sg * co, sg * sn);
-    }
-    for (int e = tid; e < Ky * kBY; e += nt) {
-        const int rr = e / kBY, py = y0 + e % kBY, my = My - rr;   // storage row rr holds my = My - rr
-        const int r = (((my * (py + yd)) % Py1) + Py1) % Py1;
-        double sn, co;
-        sincospi(2.0 * r / Py1, &sn, &co);
-        const double sg = (my & 1) ? -1.0 : 1.0;
-        ey[e] = make_double2(sg * co, sg * sn);
-    }
     __syncthreads();
-    for (int s = tid; s < Ks; s += nt) {
-        am[s] = a[(int64_t)s * Kt + Mt + m];
-        const double2 v = a[(int64_t)s * Kt + Mt - m];
-        an[s] = make_double2(v.x, -v.y);
-        const int g = __ldg(smap + s), rr = g / Kx;
-        const bool ok = g >= 0 && rr < Ky;          // an index outside the grid contributes nothing
-        srow[s] = ok ? rr : -1;
-        scol[s] = ok ? g - rr * Kx : 0;
-        if (ok) {
-            atomicMin(rlo + rr, s);
-            atomicMax(rhi + rr, s);
+    // threads 0..kBX-1: one pixel column each, ex[Mx +- m] = (-1)^m (e^{2 pi i (px+xd)/Px1})^(+-m)
+    // by powers of one sincospi; threads kBX..kBX+kBY-1: the same for the rows (ey); threads
+    // from 128: the coefficients of this m and the grid row / column of every entry
+    if (tid < kBX) {
+        const int px = x0 + tid;
+        double sn, co;
+        sincospi(2.0 * (double)(((px + xd) % Px1 + Px1) % Px1) / Px1, &sn, &co);
+        const double2 base = make_double2(co, sn);
+        double2 pw = make_double2(1.0, 0.0);
+        for (int mm = 0; mm <= Mx; ++mm) {
+            const double sg = (mm & 1) ? -1.0 : 1.0;
+            ex[(Mx + mm) * kBX + tid] = make_double2(sg * pw.x, sg * pw.y);
+            ex[(Mx - mm) * kBX + tid] = make_double2(sg * pw.x, -sg * pw.y);
+            pw = c_mul(pw, base);
+        }
+    } else if (tid < kBX + kBY) {
+        const int y = tid - kBX, py = y0 + y;
+        double sn, co;
+        sincospi(2.0 * (double)(((py + yd) % Py1 + Py1) % Py1) / Py1, &sn, &co);
+        const double2 base = make_double2(co, sn);
+        double2 pw = make_double2(1.0, 0.0);
+        for (int mm = 0; mm <= My; ++mm) {       // storage row rr holds my = My - rr
+            const double sg = (mm & 1) ? -1.0 : 1.0;
+            ey[(My - mm) * kBY + y] = make_double2(sg * pw.x, sg * pw.y);
+            ey[(My + mm) * kBY + y] = make_double2(sg * pw.x, -sg * pw.y);
+            pw = c_mul(pw, base);
+        }
+    } else if (tid >= 128) {
+        for (int s = tid - 128; s < Ks; s += nt - 128) {
+            am[s] = a[(int64_t)s * Kt + Mt + m];
+            const double2 v = a[(int64_t)s * Kt + Mt - m];
+            an[s] = make_double2(v.x, -v.y);
+            const int g = __ldg(smap + s), rr = g / Kx;
+            const bool ok = g >= 0 && rr < Ky;          // an index outside the grid contributes nothing
+            srow[s] = ok ? rr : -1;
+            scol[s] = ok ? g - rr * Kx : 0;
+            if (ok) {
+                atomicMin(rlo + rr, s);
+                atomicMax(rhi + rr, s);
+            }
         }
     }
     __syncthreads();
