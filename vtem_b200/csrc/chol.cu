@@ -177,6 +177,56 @@ __device__ void load_tile(const CholCtx& c, float* s, int I, int J) {
     cp_async_commit();   // an empty group: every call commits exactly one
 }
 
+__device__ __forceinline__ unsigned c_ld_relaxed(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// The diagonal CTA's look-ahead copies: during the panel factorisation of
+// step k, warp 7 polls (non-blocking relaxed loads, each read one block
+// later) the flags of the next sub-diagonal and diagonal tiles, and when one
+// is published it orders the load after the flag (fence) and copies the
+// tile with its own cp.async groups.  Only full, 16-byte-aligned tiles are
+// copied this way; the others take the CTA-wide path.
+struct LookAhead {
+    const unsigned* f[2];
+    float* dst[2];
+    int I[2], J[2];
+    unsigned seen[2];
+    bool on[2], issued[2];
+};
+
+__device__ __forceinline__ void look_ahead_poll(const CholCtx& c, LookAhead& la) {
+    const int lane = threadIdx.x & 31;
+    // tiles whose flag the previous poll saw set: one fence orders all their copies after the flags
+    bool go[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) go[t] = la.on[t] && !la.issued[t] && la.seen[t] >= 1u;
+    if (go[0] || go[1]) {
+        asm volatile("fence.acq_rel.gpu;\n" ::: "memory");
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            if (!go[t]) continue;
+            const int r0 = la.I[t] * kCT, c0 = la.J[t] * kCT;
+            for (int e = lane; e < kCTE / 4; e += 32) {
+                const int cc = e >> 4, r = (e & 15) * 4;
+                const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(la.dst[t] + cc * kCT + r));
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d),
+                             "l"(c.A + (int64_t)(c0 + cc) * c.ld + r0 + r)
+                             : "memory");
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            la.issued[t] = true;
+        }
+    }
+    // new looks at the flags not yet seen set, read at the next poll
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+        if (la.on[t] && !la.issued[t]) la.seen[t] = c_ld_relaxed(la.f[t]);
+}
+
 // thread 0 checks *f >= v once (no wait); every thread learns the answer
 __device__ bool cta_ready(const unsigned* f, unsigned v, int* s_ok) {
     __syncthreads();
@@ -370,7 +420,8 @@ __device__ __forceinline__ void patch_update(float* X, const float* L, int r0, i
 // (consecutive threads on consecutive row patches of one column patch:
 // conflict-free rows, broadcast column operand).  Rows 8bb+8.. of E are
 // still the identity's in the columns of block bb and need no work.
-__device__ void potrf_inv64(float* S, float* E, float* rinv, float& pmin, float& pmax, int& bad, int nvalid) {
+__device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, float& pmin, float& pmax, int& bad,
+                            int nvalid, LookAhead& la) {
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     if (w == 0) {
         potrf8_warp(S, rinv, 0, pmin, pmax, bad, nvalid);
@@ -385,9 +436,13 @@ __device__ void potrf_inv64(float* S, float* E, float* rinv, float& pmin, float&
     __syncthreads();
     for (int bb = 0; bb < 8; ++bb) {
         const int o = 8 * bb, c0 = o + 8, nd = kCT - c0;
+        // warp 7 takes no part in the row substitution below (nor, after block 0, in the
+        // trailing update): it polls the look-ahead tiles
+        if (w == kCThreads / 32 - 1 && bb > 0) look_ahead_poll(c, la);
         if (tid < kCT) {
-            if (tid < nd) subst_row8(S, S, rinv, bb, c0 + tid);
-            else subst_row8(E, S, rinv, bb, tid - nd);
+            // one code path for both kinds of row (no divergence inside a warp)
+            const bool srow = tid < nd;
+            subst_row8(srow ? S : E, S, rinv, bb, srow ? c0 + tid : tid - nd);
         }
         __syncthreads();
         if (bb == 7) break;
@@ -408,13 +463,11 @@ __device__ void potrf_inv64(float* S, float* E, float* rinv, float& pmin, float&
             // rows and columns [c0, 64) without the next diagonal block
             const int m = nd / 4, me = 2 * bb + 2, ne = me * m;
             for (int q = tid - 32; q < ne + m * m; q += kCThreads - 32) {
-                if (q < ne) {
-                    patch_update(E, S, 4 * (q % me), c0 + 4 * (q / me), o);
-                } else {
-                    const int q2 = q - ne, pc = q2 / m, pr = q2 % m;
-                    if (pr < pc || (pr < 2 && pc < 2)) continue;
-                    patch_update(S, S, c0 + 4 * pr, c0 + 4 * pc, o);
-                }
+                // one code path for E and S patches (no divergence inside a warp)
+                const bool ep = q < ne;
+                const int q2 = q - ne, pc = q2 / m, pr = q2 % m;
+                if (!ep && (pr < pc || (pr < 2 && pc < 2))) continue;
+                patch_update(ep ? E : S, S, ep ? 4 * (q % me) : c0 + 4 * pr, c0 + 4 * (ep ? q / me : pc), o);
             }
         }
         __syncthreads();
@@ -539,6 +592,7 @@ struct CholSmem {
     float x[kCTE];        // worker: the task's tile (staging); diagonal CTA: L_kk^-T
     float rinv[kCT];
     int ok;
+    int la;               // diagonal CTA: look-ahead copies done (bit 0 sub-diagonal, bit 1 diagonal tile)
 };
 
 // 64 x 64 floats at src (16-byte aligned) into shared memory, one cp.async group
@@ -787,15 +841,29 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
         float* Y = sm.a[cur ^ 1];
         // the next two tiles, requested now when the workers have published
         // them, arrive during the factorisation of this one
-        bool hx = false, hy = false;
+        // step 0's neighbours need no worker update: copied now; later ones are
+        // polled for and copied by warp 7 during the panel (look-ahead)
+        LookAhead la;
+        la.on[0] = la.on[1] = false;
+        la.issued[0] = la.issued[1] = false;
+        la.seen[0] = la.seen[1] = 0u;
         if (k + 1 < T) {
-            const int r = k < 1 ? 3 : cta_ready2(c.tflag + (k + 1) * T + k, 1u, c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok);
-            hx = (r & 1) != 0;
-            hy = (r & 2) != 0;
-            if (hx) load_tile(c, X, k + 1, k);
-            if (hy) load_tile(c, Y, k + 1, k + 1);
+            if (k < 1) {
+                load_tile(c, X, k + 1, k);
+                load_tile(c, Y, k + 1, k + 1);
+            } else if ((k + 2) * kCT <= c.K && (c.ld & 3) == 0 && ((uintptr_t)c.A & 15) == 0) {
+                la.f[0] = c.tflag + (k + 1) * T + k;
+                la.f[1] = c.tflag + (k + 1) * T + k + 1;
+                la.dst[0] = X;
+                la.dst[1] = Y;
+                la.I[0] = la.I[1] = k + 1;
+                la.J[0] = k;
+                la.J[1] = k + 1;
+                la.on[0] = la.on[1] = true;
+            }
         }
-        potrf_inv64(D, E, sm.rinv, pmin, pmax, bad, c.K - k * kCT);
+        const bool hx = k < 1, hy = k < 1;
+        potrf_inv64(c, D, E, sm.rinv, pmin, pmax, bad, c.K - k * kCT, la);
         // the workers need L_kk^-T first (their TRSMs); L_kk itself and the
         // packed X_kk are written after the sub-diagonal tile is out, so the
         // release stores on this CTA's path wait for as few stores as possible
@@ -811,9 +879,17 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
             }
             break;
         }
+        // the look-ahead copies warp 7 issued are complete for everyone after this barrier
+        if (threadIdx.x >= kCThreads - 32) {
+            look_ahead_poll(c, la);
+            cp_async_wait_all();
+            if (threadIdx.x == kCThreads - 32) sm.la = (la.issued[0] ? 1 : 0) | (la.issued[1] ? 2 : 0);
+        }
+        __syncthreads();
+        const int pre = sm.la;
         // sub-diagonal tile: the workers applied updates k' < k (none when k = 0);
         // L_{k+1,k} = X L_kk^-T
-        if (!hx) {
+        if (!hx && !(pre & 1)) {
             if (!cta_wait(c, c.tflag + (k + 1) * T + k, 1u, &sm.ok)) return;
             load_tile(c, X, k + 1, k);
         }
@@ -836,7 +912,7 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
         store_tile(c, D, k, k);
         if (inv) store_flat(c.Xinv + packed_tile(k, k) * kCTE, E);     // flag set with the next step's release
         // next diagonal tile: the workers applied updates k' < k; this CTA applies k
-        if (!hy) {
+        if (!hy && !(pre & 2)) {
             if (!cta_wait(c, c.tflag + (k + 1) * T + k + 1, 1u, &sm.ok)) return;
             load_tile(c, Y, k + 1, k + 1);
         }
