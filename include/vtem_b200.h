@@ -312,21 +312,17 @@ int vtb_tc_group_build_x3(void* host_desc, int nprob, const uint64_t* A, const i
 int vtb_tc_gemm_grouped_x3(const void* dev_desc, int nprob, int total_tiles, int bn, void* stream);
 
 /* Mixed-precision Kronecker Gram (tensor cores).  ps/ps2 list the npairs
- * spatial index pairs s <= s'.  L3 receives the RF-bank operand (2*npairs
- * rows x 3*Kp bf16, Kp = 2N rounded up to 64; once per decoder), R3 the
- * per-decode operand from Wn (Kt*Kt rows x 3*Kp).  vtb_tc_gemm_bf16(L3, R3)
- * then gives C[(2p + part)][(m, m')], scattered into the column-major
- * Hermitian M by vtb_coeff_scatter. */
-int vtb_coeff_lhs_split(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs, void* L3,
-                        void* stream);
-int vtb_coeff_wn_split(const double* Wn, int N, int Kt, void* R3, void* stream);
-/* The same operands as [hi | lo] (2*npairs x 2Kp and Kt*Kt x 2Kp) for
- * vtb_tc_gemm_bf16x3_bn over K = Kp: the decoder's Gram. */
-int vtb_coeff_lhs_split2(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs, void* L2,
-                         void* stream);
-int vtb_coeff_wn_split2(const double* Wn, int N, int Kt, void* R2, void* stream);
-int vtb_coeff_scatter(const float* C, int64_t ldc, const int32_t* ps, const int32_t* ps2, int npairs, int Kt, double* M,
-                      int64_t ldm, void* stream);
+ * spatial index pairs s <= s'; Kh = N rounded up to 64.  L receives the
+ * RF-bank operand (2*npairs rows x 2Kh bf16, [hi | lo] of the real and the
+ * imaginary part of a_n[p] = d_n[s_p] conj(d_n[s'_p]) over n; once per
+ * decoder), R the per-decode operand (Kt(Kt+1) rows x 2Kh: the real and the
+ * imaginary part of W_n[m][m'] for m <= m').  vtb_tc_gemm_bf16x3_bn(L, R)
+ * over K = Kh gives the four real sums per (pair, (m, m')) from which
+ * vtb_coeff_real_scatter forms both M((s,m),(s',m')) and M((s,m'),(s',m)):
+ * half the products of the complex GEMM's real form (W_n is Hermitian). */
+int vtb_coeff_lhs_sym(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs, void* L,
+                      void* stream);
+int vtb_coeff_wn_sym(const double* Wn, int N, int Kt, void* R, void* stream);
 
 /* b[(s,m)] = sum_n d[n][s] gn[n][m] (the right-hand side Phi^H q). */
 int vtb_coeff_rhs(const double* d, int N, int Ks, const double* gn, int Kt, double* b, void* stream);
@@ -386,8 +382,8 @@ int vtb_zadd(double* a, const double* d, int n, void* stream);
  * Mr is written row-major and full (it is symmetric, so also column-major). */
 
 /* Mr (K x K, K = Ks*Kt, float32 or float64 when out_f64) from the tensor-core
- * Gram output C of vtb_coeff_lhs_split/vtb_coeff_wn_split/vtb_tc_gemm_bf16
- * (pairs s <= s' in row-major upper-triangular order). */
+ * Gram output C (2*npairs x Kt(Kt+1), leading dimension ldc) of
+ * vtb_coeff_lhs_sym/vtb_coeff_wn_sym/vtb_tc_gemm_bf16x3_bn. */
 int vtb_coeff_real_scatter(const float* C, int64_t ldc, int Ks, int Kt, void* Mr, int64_t ldr, int out_f64,
                            void* stream);
 /* Mr from the complex column-major M of vtb_coeff_gram. */

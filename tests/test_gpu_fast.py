@@ -152,7 +152,7 @@ def test_real_form_matches_hermitian_system():
                             Mt, 8, 8, 8, 8, solver="mixed")
     t1, t2, ii = (torch.as_tensor(x, device="cuda") for x in (tk1, tk2, ind))
     s = stream_ptr()
-    K, KK = dec.K, dec.Kt * dec.Kt
+    K, NE = dec.K, dec.NE
     call("vtb_coeff_temporal_gram", dptr(t1), dptr(t2), dptr(ii), n, N, dptr(kap), dptr(dl), dptr(bia),
          dptr(dec.norm), Mt, W, dptr(dec.Wn), dptr(dec.gn), s)
     dec._build_M(s)
@@ -171,11 +171,11 @@ def test_real_form_matches_hermitian_system():
     call("vtb_coeff_unrealify_vec", dptr(x), K, 1, dptr(dec.a), 0, s)
     assert np.abs(dec.a.cpu().numpy() - a).max() <= 1e-9 * np.abs(a).max()
     # tensor-core Gram -> real form in float32
-    call("vtb_coeff_wn_split2", dptr(dec.Wn), N, dec.Kt, dptr(dec.Rsplit), s)
-    call("vtb_tc_gemm_bf16x3_bn", dptr(dec.Lsplit), 2 * dec.npairs, dptr(dec.Rsplit), KK, dec.Kp2, dptr(dec.C), KK, 1,
-         0, 1.0, 0, dec._stat_ptr(7), 128, s)
+    call("vtb_coeff_wn_sym", dptr(dec.Wn), N, dec.Kt, dptr(dec.Rsplit), s)
+    call("vtb_tc_gemm_bf16x3_bn", dptr(dec.Lsplit), 2 * dec.npairs, dptr(dec.Rsplit), NE, dec.Kh, dptr(dec.C), dec.ldc,
+         1, 0, 1.0, 0, dec._stat_ptr(7), 128, s)
     ld = dec.ld32
-    call("vtb_coeff_real_scatter", dptr(dec.C), KK, dec.Ks, dec.Kt, dptr(dec.Mr32), ld, 0, s)
+    call("vtb_coeff_real_scatter", dptr(dec.C), dec.ldc, dec.Ks, dec.Kt, dptr(dec.Mr32), ld, 0, s)
     M32 = dec.Mr32[:, :K].double().cpu().numpy()
     assert np.abs(M32 - Mr).max() <= 2e-5 * np.abs(Mr).max()
     # float32 Cholesky + solve, then a float64 Cholesky solve, against numpy

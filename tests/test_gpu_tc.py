@@ -60,22 +60,27 @@ def test_rf_filter_split_bf16_matches_f64():
     assert rel < 5e-5, rel
 
 
-@pytest.mark.parametrize("bn", [64, 96, 128, 160, 192, 256])
-def test_every_tile_width_is_exact_on_bf16_inputs(bn):
+@pytest.mark.parametrize("bn", [64, 96, 128, 160, 192, 256, 320])
+@pytest.mark.parametrize("N,ldc,alpha", [(289, 289, 1.0), (289, 292, 1.0), (289, 292, 0.5), (306, 308, 1.0)])
+def test_every_tile_width_is_exact_on_bf16_inputs(bn, N, ldc, alpha):
     """Each tile width the autotuner may pick computes the same product
     (bf16-exact operands: fp32 accumulation is exact), with partial edge tiles
-    in both directions."""
+    in both directions.  Row pitch 289 takes the shared-memory staged stores,
+    292 and 308 (16-byte rows) the tensor stores, with the last N mod 4
+    columns by plain stores; the padding columns stay untouched."""
     from vtem_b200._abi import call, dptr, stream_ptr
     rng = np.random.default_rng(bn)
-    M, N, K = 300, 289, 256
+    M, K = 300, 256
     A = torch.as_tensor(rng.integers(-8, 9, (M, K)).astype(np.float32) / 8, device="cuda").to(torch.bfloat16)
     B = torch.as_tensor(rng.integers(-8, 9, (N, K)).astype(np.float32) / 8, device="cuda").to(torch.bfloat16)
-    out = torch.zeros((M, N), dtype=torch.float32, device="cuda")
+    out = torch.full((M, ldc), float("nan"), dtype=torch.float32, device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
-    call("vtb_tc_gemm_bf16_bn", dptr(A), M, dptr(B), N, K, dptr(out), N, 1, 0, 1.0, 0, dptr(err), bn, stream_ptr())
+    call("vtb_tc_gemm_bf16_bn", dptr(A), M, dptr(B), N, K, dptr(out), ldc, 1, 0, alpha, 0, dptr(err), bn,
+         stream_ptr())
     torch.cuda.synchronize()
     assert int(err.item()) == 0
-    assert torch.equal(out.double(), A.double() @ B.double().T)
+    assert torch.equal(out[:, :N].double(), alpha * (A.double() @ B.double().T))
+    assert torch.isnan(out[:, N:]).all()
 
 
 def test_autotuner_picks_a_candidate_and_caches_it():
@@ -129,7 +134,7 @@ def test_grouped_gemm_equals_single_launches(bn, x3):
         assert torch.equal(C, R)
 
 
-@pytest.mark.parametrize("bn", [64, 96, 128, 160, 192, 256])
+@pytest.mark.parametrize("bn", [64, 96, 128, 160, 192, 256, 320])
 def test_three_product_mode_every_tile_width(bn):
     """vtb_tc_gemm_bf16x3_bn on [hi | lo] operands: the split-bf16 product
     to the same accuracy as the three-part layout, and equal to it up to the

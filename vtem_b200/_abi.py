@@ -63,11 +63,8 @@ SIGNATURES = {
     "vtb_tc_gemm_bf16_bn": [P, I, P, I, I, P, L, L, I, D, I, P, I, P],
     "vtb_tc_gemm_bf16x3_bn": [P, I, P, I, I, P, L, L, I, D, I, P, I, P],
     "vtb_split_bf16x2": [P, I, I, I, L, L, D, P, P],
-    "vtb_coeff_lhs_split": [P, I, I, P, P, I, P, P],
-    "vtb_coeff_wn_split": [P, I, I, P, P],
-    "vtb_coeff_lhs_split2": [P, I, I, P, P, I, P, P],
-    "vtb_coeff_wn_split2": [P, I, I, P, P],
-    "vtb_coeff_scatter": [P, L, P, P, I, I, P, L, P],
+    "vtb_coeff_lhs_sym": [P, I, I, P, P, I, P, P],
+    "vtb_coeff_wn_sym": [P, I, I, P, P],
     "vtb_coeff_rhs": [P, I, I, P, I, P, P],
     "vtb_coeff_residual": [P, P, P, I, I, P, P, P, P, I, D, P, I, P, P, P, P],
     "vtb_herm_potrs": [P, L, P, I, P, L, P],

@@ -1,10 +1,11 @@
 """Autotuner for the tensor-core GEMM's output tile width.
 
 ``vtb_tc_gemm_bf16_bn`` is built for output tiles of 128 rows by BN columns
-with BN in :data:`CANDIDATES`.  The best BN depends on the problem: the
-Kronecker Gram of the decoder has only (2 Mt + 1)^2 columns (289 at Mt = 8),
-where a width that divides them evenly wastes no tensor-core work, while the
-RF projection has hundreds of RF columns and many rows.  ``tile_for`` times
+with BN in :data:`CANDIDATES` (320: two 160-column accumulators that share
+each A tile).  The best BN depends on the problem: the Kronecker Gram of the
+decoder has only (Mt + 1)(2 Mt + 1) * 2 columns (306 at Mt = 8), where one
+tile across all of them loads every A tile once, while the RF projection has
+hundreds of RF columns and many rows.  ``tile_for`` times
 every candidate on the caller's own operands (CUDA events, a few launches
 each) the first time a shape class (exact column count, row and reduction
 lengths rounded to powers of two) is seen, and reuses the choice afterwards;
@@ -23,7 +24,7 @@ import torch
 
 from ._abi import call
 
-CANDIDATES = (64, 96, 128, 160, 192, 256)
+CANDIDATES = (64, 96, 128, 160, 192, 256, 320)
 DEFAULT_BN = 128
 
 _lock = threading.Lock()

@@ -78,9 +78,9 @@ class GroupedGram(object):
         u64 = np.uint64
         self.args = [
             np.array([d.Lsplit.data_ptr() for d in self.decs], u64), np.array([2 * d.npairs for d in self.decs], np.int32),
-            np.array([d.Rsplit.data_ptr() for d in self.decs], u64), np.array([d.Kt * d.Kt for d in self.decs], np.int32),
-            np.array([d.Kp2 for d in self.decs], np.int32), np.array([d.C.data_ptr() for d in self.decs], u64),
-            np.array([d.Kt * d.Kt for d in self.decs], np.int64),
+            np.array([d.Rsplit.data_ptr() for d in self.decs], u64), np.array([d.NE for d in self.decs], np.int32),
+            np.array([d.Kh for d in self.decs], np.int32), np.array([d.C.data_ptr() for d in self.decs], u64),
+            np.array([d.ldc for d in self.decs], np.int64),
             np.array([d._stat_ptr(7) for d in self.decs], u64)]
         self.desc = {}
         self.tiles = {}
@@ -128,13 +128,12 @@ def stage_mixed_pre(d, p, s):
          dptr(d.norm), d.Mt, d.W, dptr(d.Wn), dptr(d.gn), s)
     call("vtb_coeff_rhs", dptr(d.d), d.N, d.Ks, dptr(d.gn), d.Kt, dptr(d.b), s)
     call("vtb_coeff_realify_vec", dptr(d.b), d.K, 1, dptr(d.br), s)
-    call("vtb_coeff_wn_split2", dptr(d.Wn), d.N, d.Kt, dptr(d.Rsplit), s)
+    call("vtb_coeff_wn_sym", dptr(d.Wn), d.N, d.Kt, dptr(d.Rsplit), s)
 
 
 def stage_mixed_post(d, s):
     """After the Gram GEMM: the float32 real system and xr = br."""
-    KK = d.Kt * d.Kt
-    call("vtb_coeff_real_scatter", dptr(d.C), KK, d.Ks, d.Kt, dptr(d.Mr32), d.ld32, 0, s)
+    call("vtb_coeff_real_scatter", dptr(d.C), d.ldc, d.Ks, d.Kt, dptr(d.Mr32), d.ld32, 0, s)
     d.xr.copy_(d.br)
 
 
@@ -143,16 +142,16 @@ def stage_mixed(d, p, s):
     W_n, g_n, b and its real form br, the tensor-core Gram scattered into the
     float32 real system Mr32, and xr = br."""
     tk1, tk2, ind, n, kap, dl, bi = p.spikes
-    K, KK = d.K, d.Kt * d.Kt
+    K = d.K
     d.stat.zero_()
     call("vtb_coeff_temporal_gram", dptr(tk1), dptr(tk2), dptr(ind), n, d.N, dptr(kap), dptr(dl), dptr(bi),
          dptr(d.norm), d.Mt, d.W, dptr(d.Wn), dptr(d.gn), s)
     call("vtb_coeff_rhs", dptr(d.d), d.N, d.Ks, dptr(d.gn), d.Kt, dptr(d.b), s)
     call("vtb_coeff_realify_vec", dptr(d.b), K, 1, dptr(d.br), s)
-    call("vtb_coeff_wn_split2", dptr(d.Wn), d.N, d.Kt, dptr(d.Rsplit), s)
-    autotune.gemm_bf16_tuned(dptr(d.Lsplit), 2 * d.npairs, dptr(d.Rsplit), KK, d.Kp2, dptr(d.C), KK, 1, 0, 1.0, 0,
+    call("vtb_coeff_wn_sym", dptr(d.Wn), d.N, d.Kt, dptr(d.Rsplit), s)
+    autotune.gemm_bf16_tuned(dptr(d.Lsplit), 2 * d.npairs, dptr(d.Rsplit), d.NE, d.Kh, dptr(d.C), d.ldc, 1, 0, 1.0, 0,
                              d._stat_ptr(7), s, x3=True)
-    call("vtb_coeff_real_scatter", dptr(d.C), KK, d.Ks, d.Kt, dptr(d.Mr32), d.ld32, 0, s)
+    call("vtb_coeff_real_scatter", dptr(d.C), d.ldc, d.Ks, d.Kt, dptr(d.Mr32), d.ld32, 0, s)
     d.xr.copy_(d.br)
 
 

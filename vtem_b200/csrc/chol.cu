@@ -185,46 +185,55 @@ __device__ __forceinline__ unsigned c_ld_relaxed(const unsigned* p) {
 
 // The diagonal CTA's look-ahead copies: during the panel factorisation of
 // step k, warp 7 polls (non-blocking relaxed loads, each read one block
-// later) the flags of the next sub-diagonal and diagonal tiles, and when one
-// is published it orders the load after the flag (fence) and copies the
-// tile with its own cp.async groups.  Only full, 16-byte-aligned tiles are
-// copied this way; the others take the CTA-wide path.
+// later) the flags of the next sub-diagonal and diagonal tiles; when one is
+// published it orders the copies after the flag (one fence, in warp 7 only)
+// and tells the CTA through a shared word, and after the next barrier warps
+// 1-7 issue the tile's 16-byte cp.async copies between them (warp 0, on the
+// panel's critical path, copies nothing).  Only full, 16-byte-aligned tiles
+// are copied this way; the others take the CTA-wide path.
 struct LookAhead {
     const unsigned* f[2];
     float* dst[2];
     int I[2], J[2];
-    unsigned seen[2];
-    bool on[2], issued[2];
+    unsigned seen[2];  // warp 7: the flag values its last poll read
+    bool on[2];
+    int fenced;        // warp 7: tiles whose copies are ordered after their flags (bits)
+    int issued;        // copying threads: tiles whose copies they issued (bits)
 };
 
-__device__ __forceinline__ void look_ahead_poll(const CholCtx& c, LookAhead& la) {
-    const int lane = threadIdx.x & 31;
-    // tiles whose flag the previous poll saw set: one fence orders all their copies after the flags
-    bool go[2];
-#pragma unroll
-    for (int t = 0; t < 2; ++t) go[t] = la.on[t] && !la.issued[t] && la.seen[t] >= 1u;
-    if (go[0] || go[1]) {
-        asm volatile("fence.acq_rel.gpu;\n" ::: "memory");
-        __syncwarp();
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-            if (!go[t]) continue;
-            const int r0 = la.I[t] * kCT, c0 = la.J[t] * kCT;
-            for (int e = lane; e < kCTE / 4; e += 32) {
-                const int cc = e >> 4, r = (e & 15) * 4;
-                const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(la.dst[t] + cc * kCT + r));
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d),
-                             "l"(c.A + (int64_t)(c0 + cc) * c.ld + r0 + r)
-                             : "memory");
-            }
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
-            la.issued[t] = true;
-        }
-    }
-    // new looks at the flags not yet seen set, read at the next poll
+// warp 7: one fence for the tiles whose flags the previous poll saw set,
+// published in *go; then new looks at the flags not yet seen set
+__device__ __forceinline__ void look_ahead_poll(LookAhead& la, int* go) {
+    int nb = 0;
 #pragma unroll
     for (int t = 0; t < 2; ++t)
-        if (la.on[t] && !la.issued[t]) la.seen[t] = c_ld_relaxed(la.f[t]);
+        if (la.on[t] && !((la.fenced >> t) & 1) && la.seen[t] >= 1u) nb |= 1 << t;
+    if (nb) {
+        asm volatile("fence.acq_rel.gpu;\n" ::: "memory");
+        la.fenced |= nb;
+        if ((threadIdx.x & 31) == 0) *go = la.fenced;
+    }
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+        if (la.on[t] && !((la.fenced >> t) & 1)) la.seen[t] = c_ld_relaxed(la.f[t]);
+}
+
+// threads [first, kCThreads): their share of the copies of the tiles in go
+// (read after a barrier that follows its write) not issued yet
+__device__ __forceinline__ void look_ahead_issue(const CholCtx& c, LookAhead& la, int go, int first) {
+    const int todo = go & ~la.issued;
+    if (!todo) return;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        if (!((todo >> t) & 1)) continue;
+        const int r0 = la.I[t] * kCT, c0 = la.J[t] * kCT;
+        for (int e = threadIdx.x - first; e < kCTE / 4; e += kCThreads - first) {
+            const int cc = e >> 4, r = (e & 15) * 4;
+            cp_async16(la.dst[t] + cc * kCT + r, c.A + (int64_t)(c0 + cc) * c.ld + r0 + r);
+        }
+    }
+    cp_async_commit();
+    la.issued |= todo;
 }
 
 // thread 0 checks *f >= v once (no wait); every thread learns the answer
@@ -421,7 +430,7 @@ __device__ __forceinline__ void patch_update(float* X, const float* L, int r0, i
 // conflict-free rows, broadcast column operand).  Rows 8bb+8.. of E are
 // still the identity's in the columns of block bb and need no work.
 __device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, float& pmin, float& pmax, int& bad,
-                            int nvalid, LookAhead& la) {
+                            int nvalid, LookAhead& la, int* go) {
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     if (w == 0) {
         potrf8_warp(S, rinv, 0, pmin, pmax, bad, nvalid);
@@ -436,9 +445,8 @@ __device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, f
     __syncthreads();
     for (int bb = 0; bb < 8; ++bb) {
         const int o = 8 * bb, c0 = o + 8, nd = kCT - c0;
-        // warp 7 takes no part in the row substitution below (nor, after block 0, in the
-        // trailing update): it polls the look-ahead tiles
-        if (w == kCThreads / 32 - 1 && bb > 0) look_ahead_poll(c, la);
+        // warp 7 takes no part in the row substitution below: it polls the look-ahead tiles
+        if (w == kCThreads / 32 - 1 && bb > 0) look_ahead_poll(la, go);
         if (tid < kCT) {
             // one code path for both kinds of row (no divergence inside a warp)
             const bool srow = tid < nd;
@@ -459,6 +467,7 @@ __device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, f
             __syncwarp();
             potrf8_warp(S, rinv, bb + 1, pmin, pmax, bad, nvalid);
         } else {
+            look_ahead_issue(c, la, *go, 32);
             // E rows 0..c0-1 (2bb+2 row patches) x columns [c0, 64); then the lower triangle of S's
             // rows and columns [c0, 64) without the next diagonal block
             const int m = nd / 4, me = 2 * bb + 2, ne = me * m;
@@ -592,7 +601,8 @@ struct CholSmem {
     float x[kCTE];        // worker: the task's tile (staging); diagonal CTA: L_kk^-T
     float rinv[kCT];
     int ok;
-    int la;               // diagonal CTA: look-ahead copies done (bit 0 sub-diagonal, bit 1 diagonal tile)
+    int la;               // diagonal CTA: look-ahead tiles ordered after their flags (bit 0 sub-diagonal,
+                          // bit 1 diagonal tile); complete after the post-panel barrier
 };
 
 // 64 x 64 floats at src (16-byte aligned) into shared memory, one cp.async group
@@ -845,8 +855,9 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
         // polled for and copied by warp 7 during the panel (look-ahead)
         LookAhead la;
         la.on[0] = la.on[1] = false;
-        la.issued[0] = la.issued[1] = false;
+        la.fenced = la.issued = 0;
         la.seen[0] = la.seen[1] = 0u;
+        if (threadIdx.x == 0) sm.la = 0;
         if (k + 1 < T) {
             if (k < 1) {
                 load_tile(c, X, k + 1, k);
@@ -863,7 +874,7 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
             }
         }
         const bool hx = k < 1, hy = k < 1;
-        potrf_inv64(c, D, E, sm.rinv, pmin, pmax, bad, c.K - k * kCT, la);
+        potrf_inv64(c, D, E, sm.rinv, pmin, pmax, bad, c.K - k * kCT, la, &sm.la);
         // the workers need L_kk^-T first (their TRSMs); L_kk itself and the
         // packed X_kk are written after the sub-diagonal tile is out, so the
         // release stores on this CTA's path wait for as few stores as possible
@@ -879,12 +890,12 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
             }
             break;
         }
-        // the look-ahead copies warp 7 issued are complete for everyone after this barrier
-        if (threadIdx.x >= kCThreads - 32) {
-            look_ahead_poll(c, la);
-            cp_async_wait_all();
-            if (threadIdx.x == kCThreads - 32) sm.la = (la.issued[0] ? 1 : 0) | (la.issued[1] ? 2 : 0);
-        }
+        // the last poll's fence, the copies not issued yet, and all look-ahead
+        // copies complete for everyone after the second barrier
+        if (threadIdx.x >= kCThreads - 32) look_ahead_poll(la, &sm.la);
+        __syncthreads();
+        if (threadIdx.x >= 32) look_ahead_issue(c, la, sm.la, 32);
+        cp_async_wait_all();
         __syncthreads();
         const int pre = sm.la;
         // sub-diagonal tile: the workers applied updates k' < k (none when k = 0);

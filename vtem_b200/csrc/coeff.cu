@@ -1149,84 +1149,65 @@ VTB_API int vtb_coeff_synthesize_noalloc(const double* a, const int32_t* smap, i
 // Mixed-precision pieces of the coefficient-space decoder.
 //
 // (1) The Kronecker Gram as one tensor-core GEMM.  For s <= s' (M is
-//     Hermitian) and a_n = d_n[s] conj(d_n[s']):
-//        Re M((s,m),(s',m')) = sum_n a_n.re W_n.re - a_n.im W_n.im
-//        Im M((s,m),(s',m')) = sum_n a_n.im W_n.re + a_n.re W_n.im
-//     i.e. C = L R^T with L[(pair, part), (n, q)] built from the RF bank
-//     only (split once per decoder) and R[(m, m'), (n, q)] = W_n[m, m'].q
-//     (split per decode).  Split-bf16 products, fp32 accumulation.
+//     Hermitian) and a_n = d_n[s] conj(d_n[s']),
+//        M((s,m),(s',m')) = sum_n a_n W_n[m][m'],
+//     and W_n is Hermitian, so the four real sums over n of
+//     {a.re, a.im} x {W.re, W.im}[m][m'] for m <= m' give both
+//     (m, m') (= sum a W) and (m', m) (= sum a conj W).  C = L R^T with
+//     L[(pair, part), n] built from the RF bank only (split once per decoder)
+//     and R[(u, part), n] for the Kt(Kt+1)/2 upper-triangular entries u of
+//     W_n (split per decode): half the products of the real form of the
+//     complex GEMM.  Split-bf16 products, fp32 accumulation.
 // (2) The exact float64 residual r = Phi^H (q - Phi a) through the same
 //     Kronecker factors (never forming M in float64), for refinement sweeps
 //     on top of a factorisation of the tensor-core M.
 namespace vtb {
 
-// L3[row][seg*Kp + k], row = 2*pair + part, k = 2n + q, Kp = 2N rounded up to 64
-// PARTS = 3: [hi | hi | lo] (the plain GEMM's layout); PARTS = 2: [hi | lo]
-// (the three-product mode's)
-template <int PARTS>
-__global__ void kron_lhs_split_kernel(const double2* __restrict__ d, int N, int Ks, const int32_t* __restrict__ ps,
-                                      const int32_t* __restrict__ ps2, int npairs, int Kp,
-                                      __nv_bfloat16* __restrict__ L3) {
-    const int64_t total = (int64_t)npairs * 2 * Kp;
+// x -> bf16 hi at dst[0] and the bf16 of the remainder x - hi at dst[seg]
+__device__ __forceinline__ void split_bf16_store(double x, __nv_bfloat16* dst, int seg) {
+    const __nv_bfloat16 hi = __float2bfloat16_rn((float)x);
+    dst[0] = hi;
+    dst[seg] = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
+}
+
+// L[row][seg * Kh + n], row = 2 * pair + part, Kh = N rounded up to 64,
+// segments [hi | lo]: part 0 the real, part 1 the imaginary part of
+// a_n[p] = d_n[s_p] conj(d_n[s'_p]) (zero for the padding n >= N).
+__global__ void kron_lhs_sym_kernel(const double2* __restrict__ d, int N, int Ks, const int32_t* __restrict__ ps,
+                                    const int32_t* __restrict__ ps2, int npairs, int Kh,
+                                    __nv_bfloat16* __restrict__ L) {
+    const int64_t total = (int64_t)npairs * Kh;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int row = (int)(e / Kp), k = (int)(e % Kp);
-        const int p = row >> 1, part = row & 1;
-        double x = 0.0;
-        if (k < 2 * N) {
-            const int n = k >> 1, q = k & 1;
-            const double2 a = cmulc(d[(int64_t)n * Ks + ps[p]], d[(int64_t)n * Ks + ps2[p]]);
-            // part 0 (real): [a.re, -a.im]; part 1 (imag): [a.im, a.re]
-            x = part == 0 ? (q == 0 ? a.x : -a.y) : (q == 0 ? a.y : a.x);
-        }
-        const __nv_bfloat16 hi = __float2bfloat16_rn((float)x);
-        const __nv_bfloat16 lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
-        __nv_bfloat16* dst = L3 + (int64_t)row * PARTS * Kp + k;
-        dst[0] = hi;
-        if (PARTS == 3) {
-            dst[Kp] = hi;
-            dst[2 * Kp] = lo;
-        } else {
-            dst[Kp] = lo;
-        }
+        const int p = (int)(e / Kh), n = (int)(e % Kh);
+        double2 a = make_double2(0.0, 0.0);
+        if (n < N) a = cmulc(d[(int64_t)n * Ks + ps[p]], d[(int64_t)n * Ks + ps2[p]]);
+        __nv_bfloat16* row = L + (int64_t)(2 * p) * 2 * Kh + n;
+        split_bf16_store(a.x, row, Kh);
+        split_bf16_store(a.y, row + 2 * Kh, Kh);
     }
 }
 
-// R3[e][seg*Kp + k] with e = (m, m'), k = 2n + q: pattern [hi | lo | hi]
-// (PARTS = 3) or [hi | lo] (PARTS = 2)
-template <int PARTS>
-__global__ void kron_rhs_split_kernel(const double2* __restrict__ Wn, int N, int KK, int Kp,
-                                      __nv_bfloat16* __restrict__ R3) {
-    const int64_t total = (int64_t)KK * Kp;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int e = (int)(i / Kp), k = (int)(i % Kp);
-        double x = 0.0;
-        if (k < 2 * N) {
-            const double2 w = Wn[(int64_t)(k >> 1) * KK + e];
-            x = (k & 1) ? w.y : w.x;
-        }
-        const __nv_bfloat16 hi = __float2bfloat16_rn((float)x);
-        const __nv_bfloat16 lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
-        __nv_bfloat16* dst = R3 + (int64_t)e * PARTS * Kp + k;
-        dst[0] = hi;
-        dst[Kp] = lo;
-        if (PARTS == 3) dst[2 * Kp] = hi;
-    }
-}
+constexpr int kWnChunk = 32;  // neurons per block of kron_rhs_sym_kernel
 
-// M (column-major, complex float64) from the GEMM result C[(2p + part) * ldc + e]
-__global__ void kron_scatter_kernel(const float* __restrict__ C, int64_t ldc, const int32_t* __restrict__ ps,
-                                    const int32_t* __restrict__ ps2, int npairs, int Kt,
-                                    double2* __restrict__ M, int64_t ldm) {
-    const int KK = Kt * Kt;
-    const int64_t total = (int64_t)npairs * KK;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int p = (int)(i / KK), e = (int)(i % KK);
-        const int m = e / Kt, mp = e % Kt;
-        const int s = ps[p], sp = ps2[p];
-        const double re = C[(int64_t)(2 * p) * ldc + e], im = C[(int64_t)(2 * p + 1) * ldc + e];
-        const int64_t row = (int64_t)s * Kt + m, col = (int64_t)sp * Kt + mp;
-        M[col * ldm + row] = make_double2(re, im);
-        if (s != sp) M[row * ldm + col] = make_double2(re, -im);
+// R[row][seg * Kh + n], row = 2u + part for the upper-triangular entries
+// u = (m, m'), m <= m' (row-major order) of the Hermitian W_n, segments
+// [hi | lo]: part 0 the real, part 1 the imaginary part of W_n[m][m'].
+// Block (neuron chunk, m): row m of 32 neurons' W_n read contiguously into
+// shared memory, then written as 32-neuron runs of each output row.
+__global__ void __launch_bounds__(256) kron_rhs_sym_kernel(const double2* __restrict__ Wn, int N, int Kt, int Kh,
+                                                           __nv_bfloat16* __restrict__ R) {
+    __shared__ double2 sw[kWnChunk * 32];
+    const int n0 = blockIdx.x * kWnChunk, m = blockIdx.y, nm = Kt - m, KK = Kt * Kt;
+    for (int e = threadIdx.x; e < kWnChunk * nm; e += blockDim.x) {
+        const int i = e / nm, j = e - i * nm;
+        sw[i * nm + j] = n0 + i < N ? Wn[(int64_t)(n0 + i) * KK + m * Kt + m + j] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const int u0 = m * Kt - m * (m - 1) / 2;
+    for (int e = threadIdx.x; e < nm * 2 * kWnChunk; e += blockDim.x) {
+        const int i = e & (kWnChunk - 1), part = (e / kWnChunk) & 1, j = e / (2 * kWnChunk);
+        const double2 w = sw[i * nm + j];
+        split_bf16_store(part ? w.y : w.x, R + (int64_t)(2 * (u0 + j) + part) * 2 * Kh + n0 + i, Kh);
     }
 }
 
@@ -1299,64 +1280,22 @@ __global__ void zadd_kernel(double2* __restrict__ a, const double2* __restrict__
 
 }  // namespace vtb
 
-static int lhs_split(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs, void* L,
-                     int parts, void* stream) {
+VTB_API int vtb_coeff_lhs_sym(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs,
+                              void* L, void* stream) {
     VTB_CHECK_ARG(N > 0 && Ks > 0 && npairs > 0 && d && ps && ps2 && L && ((uintptr_t)L & 15) == 0);
-    const int Kp = ceil_div(2 * N, 64) * 64;
-    const int64_t total = (int64_t)npairs * 2 * Kp;
+    const int Kh = ceil_div(N, 64) * 64;
+    const int64_t total = (int64_t)npairs * Kh;
     const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 32 * kNumSMs);
-    if (parts == 3)
-        kron_lhs_split_kernel<3><<<blocks, 256, 0, as_stream(stream)>>>(
-            reinterpret_cast<const double2*>(d), N, Ks, ps, ps2, npairs, Kp, reinterpret_cast<__nv_bfloat16*>(L));
-    else
-        kron_lhs_split_kernel<2><<<blocks, 256, 0, as_stream(stream)>>>(
-            reinterpret_cast<const double2*>(d), N, Ks, ps, ps2, npairs, Kp, reinterpret_cast<__nv_bfloat16*>(L));
+    kron_lhs_sym_kernel<<<blocks, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(d), N, Ks, ps, ps2,
+                                                               npairs, Kh, reinterpret_cast<__nv_bfloat16*>(L));
     return launch_status();
 }
 
-static int wn_split(const double* Wn, int N, int Kt, void* R, int parts, void* stream) {
-    VTB_CHECK_ARG(N > 0 && Kt > 0 && Wn && R && ((uintptr_t)R & 15) == 0);
-    const int Kp = ceil_div(2 * N, 64) * 64;
-    const int64_t total = (int64_t)Kt * Kt * Kp;
-    const int blocks = (int)std::min<int64_t>(ceil_div(total, 256), 32 * kNumSMs);
-    if (parts == 3)
-        kron_rhs_split_kernel<3><<<blocks, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(Wn), N,
-                                                                         Kt * Kt, Kp,
-                                                                         reinterpret_cast<__nv_bfloat16*>(R));
-    else
-        kron_rhs_split_kernel<2><<<blocks, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(Wn), N,
-                                                                         Kt * Kt, Kp,
-                                                                         reinterpret_cast<__nv_bfloat16*>(R));
-    return launch_status();
-}
-
-VTB_API int vtb_coeff_lhs_split(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs,
-                                void* L3, void* stream) {
-    return lhs_split(d, N, Ks, ps, ps2, npairs, L3, 3, stream);
-}
-
-VTB_API int vtb_coeff_wn_split(const double* Wn, int N, int Kt, void* R3, void* stream) {
-    return wn_split(Wn, N, Kt, R3, 3, stream);
-}
-
-// [hi | lo] operands (2 * npairs x 2Kp and Kt^2 x 2Kp bf16, Kp = 2N rounded up
-// to 64) for vtb_tc_gemm_bf16x3_bn: the same Gram with two thirds of the
-// operand bytes of the [hi | hi | lo] / [hi | lo | hi] layouts.
-VTB_API int vtb_coeff_lhs_split2(const double* d, int N, int Ks, const int32_t* ps, const int32_t* ps2, int npairs,
-                                 void* L2, void* stream) {
-    return lhs_split(d, N, Ks, ps, ps2, npairs, L2, 2, stream);
-}
-
-VTB_API int vtb_coeff_wn_split2(const double* Wn, int N, int Kt, void* R2, void* stream) {
-    return wn_split(Wn, N, Kt, R2, 2, stream);
-}
-
-VTB_API int vtb_coeff_scatter(const float* C, int64_t ldc, const int32_t* ps, const int32_t* ps2, int npairs, int Kt,
-                              double* M, int64_t ldm, void* stream) {
-    VTB_CHECK_ARG(npairs > 0 && Kt > 0 && C && ps && ps2 && M);
-    const int64_t total = (int64_t)npairs * Kt * Kt;
-    kron_scatter_kernel<<<(int)std::min<int64_t>(ceil_div(total, 256), 32 * kNumSMs), 256, 0, as_stream(stream)>>>(
-        C, ldc, ps, ps2, npairs, Kt, reinterpret_cast<double2*>(M), ldm);
+VTB_API int vtb_coeff_wn_sym(const double* Wn, int N, int Kt, void* R, void* stream) {
+    VTB_CHECK_ARG(N > 0 && Kt > 0 && Kt <= 32 && Wn && R && ((uintptr_t)R & 15) == 0);
+    const int Kh = ceil_div(N, 64) * 64;
+    kron_rhs_sym_kernel<<<dim3(Kh / kWnChunk, Kt), 256, 0, as_stream(stream)>>>(
+        reinterpret_cast<const double2*>(Wn), N, Kt, Kh, reinterpret_cast<__nv_bfloat16*>(R));
     return launch_status();
 }
 

@@ -57,8 +57,10 @@ __device__ __forceinline__ double real_entry(double2 A, double2 B, int p, int q)
 }
 
 // Element M[j][k] of the Hermitian M from the tensor-core Gram output
-// C[(2p + part) * ldc + m*Kt + m'] (pairs p of spatial indices s <= s' in
-// row-major upper-triangular order).
+// C[(2p + pa) * ldc + 2u + pw] = sum_n {a.re, a.im}[pa] {W.re, W.im}[pw] for
+// the pairs p of spatial indices s <= s' and the upper-triangular temporal
+// entries u = (m, m'), m <= m' (both in row-major upper-triangular order):
+// sum a W for m <= m', sum a conj(W[m'][m]) for m > m' (W_n is Hermitian).
 __device__ __forceinline__ double2 gram_from_pairs(const float* __restrict__ C, int64_t ldc, int Ks, int Kt, int j,
                                                    int k) {
     int s = j / Kt, m = j - s * Kt, s2 = k / Kt, m2 = k - s2 * Kt;
@@ -69,8 +71,13 @@ __device__ __forceinline__ double2 gram_from_pairs(const float* __restrict__ C, 
         conj = true;
     }
     const int64_t p = (int64_t)s * Ks - (int64_t)s * (s - 1) / 2 + (s2 - s);
-    const int e = m * Kt + m2;
-    const double re = C[(2 * p) * ldc + e], im = C[(2 * p + 1) * ldc + e];
+    const bool lower = m > m2;
+    const int ma = lower ? m2 : m, mb = lower ? m : m2;
+    const int u = ma * Kt - ma * (ma - 1) / 2 + (mb - ma);
+    const float* c = C + (2 * p) * ldc + 2 * u;
+    const double rr = c[0], ri = c[1], ir = c[ldc], ii = c[ldc + 1];
+    const double re = lower ? rr + ii : rr - ii;
+    const double im = lower ? ir - ri : ri + ir;
     return make_double2(re, conj ? -im : im);
 }
 
@@ -768,7 +775,8 @@ using namespace vtb;
 
 VTB_API int vtb_coeff_real_scatter(const float* C, int64_t ldc, int Ks, int Kt, void* Mr, int64_t ldr, int out_f64,
                                    void* stream) {
-    VTB_CHECK_ARG(Ks > 0 && (Ks & 1) && Kt > 0 && (Kt & 1) && C && Mr && ldr >= (int64_t)Ks * Kt);
+    VTB_CHECK_ARG(Ks > 0 && (Ks & 1) && Kt > 0 && (Kt & 1) && C && Mr && ldr >= (int64_t)Ks * Kt &&
+                  ldc >= (int64_t)Kt * (Kt + 1));
     const int K = Ks * Kt, h = (K - 1) / 2;
     VTB_CHECK_ARG(K <= 65535);
     const dim3 grid(ceil_div(h + 1, 256), K);

@@ -21,6 +21,7 @@
 #include <cudaTypedefs.h>
 
 #include <cstring>
+#include <type_traits>
 #include <mutex>
 
 #include "common.cuh"
@@ -74,9 +75,42 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
 }
 
 // K-major operand tile, 128-byte swizzle: 8-row atoms of 1024 bytes.
+template <int BK>
+__device__ __forceinline__ uint64_t smem_desc_k(const void* base);
+
+// K-major operand tile, 64-byte swizzle (BK = 32 bf16 per row): 8-row atoms of 512 bytes.
+template <>
+__device__ __forceinline__ uint64_t smem_desc_k<32>(const void* base) {
+    const uint64_t addr = smem_u32(base);
+    return ((addr >> 4) & 0x3FFFull) | (1ull << 16) | (32ull << 32) | (1ull << 46) | (4ull << 61);
+}
+
 __device__ __forceinline__ uint64_t smem_desc_sw128(const void* base) {
     const uint64_t addr = smem_u32(base);
     return ((addr >> 4) & 0x3FFFull) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+template <>
+__device__ __forceinline__ uint64_t smem_desc_k<64>(const void* base) {
+    return smem_desc_sw128(base);
+}
+
+// 16 consecutive fp32 accumulator columns of this warp's 32 TMEM lanes (one
+// row per thread); the registers are valid after tmem_ld_wait
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    tmem_ld16_async(taddr, v);
+    tmem_ld_wait();
 }
 
 template <int BN>
@@ -89,42 +123,68 @@ struct TcIdesc {
 // X3 (three-product mode): the operands are [hi | lo] along K (2K columns)
 // and every k-block issues hi*hi, hi*lo and lo*hi from the same
 // shared-memory tiles, so no operand part is stored or loaded twice.
-template <int BN, bool X3>
+// NS sub-tiles of BN columns share each A tile: a CTA computes a
+// 128 x (NS * BN) tile with NS accumulators side by side in tensor memory
+// (BN <= 256 is the largest N of one MMA), loading its A rows once.
+constexpr int kSmemRing = 225 * 1024;  // stage ring; barriers and 1 KB alignment slack fit in the rest of 227 KB
+
+// BK: the k-block (64 bf16 = 128-byte rows with the 128-byte swizzle, or
+// 32 = 64-byte rows with the 64-byte swizzle: half-size stages, twice as
+// many in the same ring, for tiles whose stage would otherwise leave only
+// two in flight)
+template <int BN, bool X3, int NS = 1, int BK = kTcBK>
 struct TcCfg {
+    static_assert(BK == 64 || BK == 32, "k-block of 64 or 32");
     static constexpr int kParts = X3 ? 2 : 1;
-    static constexpr int kStageBytes = kParts * (kTcBM + BN) * kTcBK * 2;
-    static constexpr int kFit = (220 * 1024) / kStageBytes;
-    static constexpr int kStages = kFit < kTcStages ? kFit : kTcStages;
+    static constexpr int kCols = NS * BN;
+    static constexpr int kStageBytes = kParts * (kTcBM + kCols) * BK * 2;
+    static constexpr int kFit = kSmemRing / kStageBytes;
+    static constexpr int kMaxStages = kTcStages * (kTcBK / BK);
+    static constexpr int kStages = kFit < kMaxStages ? kFit : kMaxStages;
+    static_assert(kStages >= 2, "at least two pipeline stages");
+    static constexpr uint32_t kTmemCols = kCols <= 32 ? 32 : kCols <= 64 ? 64 : kCols <= 128 ? 128
+                                                       : kCols <= 256 ? 256 : 512;
 };
 
-template <int BN, bool X3 = false>
+template <int BN, bool X3 = false, int NS = 1, int BK = kTcBK>
 struct TcSmem {
-    using Cfg = TcCfg<BN, X3>;
-    __nv_bfloat16 a[Cfg::kStages][Cfg::kParts][kTcBM * kTcBK];
-    __nv_bfloat16 b[Cfg::kStages][Cfg::kParts][BN * kTcBK];
+    using Cfg = TcCfg<BN, X3, NS, BK>;
+    __nv_bfloat16 a[Cfg::kStages][Cfg::kParts][kTcBM * BK];
+    __nv_bfloat16 b[Cfg::kStages][Cfg::kParts][Cfg::kCols * BK];
     uint64_t full[Cfg::kStages];
     uint64_t empty[Cfg::kStages];
     uint64_t done;
     uint32_t tmem_base;
 };
 
-// One 128 x BN output tile (rows m0.., columns n0..) of C = alpha A B^T; the
-// tensor maps may live in kernel parameters or in global memory.  With X3,
-// K is the width of one operand part and C = A_hi B_hi^T + A_hi B_lo^T +
-// A_lo B_hi^T.
-template <int BN, typename OutT, bool X3 = false>
-__device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMap* tmB, int M, int N, int K, int m0,
-                                        int n0, OutT* __restrict__ C, int64_t c_m, int64_t c_n, double alpha,
-                                        int accumulate, int32_t* __restrict__ err, uint32_t limit,
-                                        uint8_t* smem_raw) {
-    using Sm = TcSmem<BN, X3>;
-    constexpr int S = Sm::Cfg::kStages;
+// 2-D tiled store of a shared-memory box to global memory (bulk async group)
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(smem_u32(src)), "r"(x), "r"(y)
+                 : "memory");
+}
+
+// One 128 x (NS * BN) output tile (rows m0.., columns n0..) of C = alpha A B^T;
+// the tensor maps may live in kernel parameters or in global memory.  With
+// X3, K is the width of one operand part and C = A_hi B_hi^T + A_hi B_lo^T +
+// A_lo B_hi^T.  tmC (nullable): a float32 map of C (box 32 x 128, 128-byte
+// swizzle) for the tensor-store epilogue.
+template <int BN, typename OutT, bool X3 = false, int NS = 1, int BK = kTcBK>
+__device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMap* tmB, const CUtensorMap* tmC,
+                                        int M, int N, int K, int m0, int n0, OutT* __restrict__ C, int64_t c_m,
+                                        int64_t c_n, double alpha, int accumulate, int32_t* __restrict__ err,
+                                        uint32_t limit, uint8_t* smem_raw) {
+    using Sm = TcSmem<BN, X3, NS, BK>;
+    using Cfg = typename Sm::Cfg;
+    constexpr int S = Cfg::kStages;
+    constexpr int kCols = Cfg::kCols;
+    constexpr uint32_t kTmemCols = Cfg::kTmemCols;
     // 1024-byte alignment of the stage buffers (the swizzle atoms)
     Sm& sm = *reinterpret_cast<Sm*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
-    const int nk = K / kTcBK;
-    constexpr uint32_t kTmemCols = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+    const int nk = K / BK;
 
     if (tid == 0) {
         for (int s = 0; s < S; ++s) {
@@ -149,17 +209,19 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
     int issued = 0;   // TMA stages the producer issued
     if (tid == 0) {
         // producer
-        constexpr uint32_t bytes = Sm::Cfg::kStageBytes;
+        constexpr uint32_t bytes = Cfg::kStageBytes;
         for (int kb = 0; kb < nk && ok; ++kb) {
             const int s = kb % S;
             if (kb >= S) ok = mbar_wait(&sm.empty[s], ((kb / S) + 1) & 1, limit);
             if (!ok) break;
             mbar_expect_tx(&sm.full[s], bytes);
-            tma_load_2d(sm.a[s][0], tmA, &sm.full[s], kb * kTcBK, m0);
-            tma_load_2d(sm.b[s][0], tmB, &sm.full[s], kb * kTcBK, n0);
-            if (X3) {
-                tma_load_2d(sm.a[s][Sm::Cfg::kParts - 1], tmA, &sm.full[s], K + kb * kTcBK, m0);
-                tma_load_2d(sm.b[s][Sm::Cfg::kParts - 1], tmB, &sm.full[s], K + kb * kTcBK, n0);
+#pragma unroll
+            for (int part = 0; part < Cfg::kParts; ++part) {
+                tma_load_2d(sm.a[s][part], tmA, &sm.full[s], part * K + kb * BK, m0);
+#pragma unroll
+                for (int ns = 0; ns < NS; ++ns)
+                    tma_load_2d(sm.b[s][part] + ns * BN * BK, tmB, &sm.full[s], part * K + kb * BK,
+                                n0 + ns * BN);
             }
             issued = kb + 1;
         }
@@ -175,19 +237,22 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
             // products of this k-block: (A part, B part) = (0,0); with X3 also (0,1) and (1,0)
 #pragma unroll
             for (int pr = 0; pr < (X3 ? 3 : 1); ++pr) {
-                const uint64_t da = smem_desc_sw128(sm.a[s][pr == 2 ? Sm::Cfg::kParts - 1 : 0]);
-                const uint64_t db = smem_desc_sw128(sm.b[s][pr == 1 ? Sm::Cfg::kParts - 1 : 0]);
+                const uint64_t da = smem_desc_k<BK>(sm.a[s][pr == 2 ? Cfg::kParts - 1 : 0]);
 #pragma unroll
-                for (int j = 0; j < kTcBK / 16; ++j) {
-                    // advance 16 bf16 (32 bytes) along K inside the swizzle row
-                    const uint64_t adv = (uint64_t)(j * 2);
-                    const uint32_t acc = (kb > 0 || pr > 0 || j > 0) ? 1u : 0u;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                        "l"(da + adv), "l"(db + adv), "r"(idesc), "r"(acc)
-                        : "memory");
+                for (int ns = 0; ns < NS; ++ns) {
+                    const uint64_t db = smem_desc_k<BK>(sm.b[s][pr == 1 ? Cfg::kParts - 1 : 0] + ns * BN * BK);
+#pragma unroll
+                    for (int j = 0; j < BK / 16; ++j) {
+                        // advance 16 bf16 (32 bytes) along K inside the swizzle row
+                        const uint64_t adv = (uint64_t)(j * 2);
+                        const uint32_t acc = (kb > 0 || pr > 0 || j > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + ns * BN),
+                            "l"(da + adv), "l"(db + adv), "r"(idesc), "r"(acc)
+                            : "memory");
+                    }
                 }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -210,34 +275,146 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
         mbar_wait(&sm.done, 0, kDrainLimit);
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int row = m0 + warp * 32 + (tid & 31);
+    // a CTA that gave up drains its producer's issued TMA loads before the
+    // stage ring is reused or the CTA exits
+    if (tid == 0)
+        for (int kb = issued > S ? issued - S : 0; kb < issued; ++kb)
+            mbar_wait(&sm.full[kb % S], (kb / S) & 1, kDrainLimit);
+    const bool rowf = std::is_same<OutT, float>::value && c_n == 1 && !accumulate;
+    const bool unit = alpha == 1.0;
+    const int r = warp * 32 + (tid & 31);   // this thread's accumulator row (TMEM lane)
+    static_assert(kCols % 32 == 0, "32-column accumulator chunks");
+    if (rowf && tmC != nullptr) {
+        // row-major float output by tensor stores: 32-column slabs of 128 rows
+        // x 128 bytes in the C map's 128-byte swizzle, staged in the (now
+        // idle) stage ring
+        constexpr int kSlabBytes = kTcBM * 128;
+        static_assert(sizeof(sm.a) + sizeof(sm.b) >= (size_t)(kCols / 32) * kSlabBytes, "slabs fit the ring");
+        uint8_t* st = reinterpret_cast<uint8_t*>(&sm.a[0][0][0]);
+        __syncthreads();
 #pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 16) {
-        uint32_t v[16];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-            "%14, %15}, [%16];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (have && row < M) {
+        for (int c0 = 0; c0 < kCols; c0 += 32) {
+            uint32_t v[2][16];
+            tmem_ld16_async(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v[0]);
+            tmem_ld16_async(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c0 + 16), v[1]);
+            tmem_ld_wait();
+            uint8_t* row = st + (c0 / 32) * kSlabBytes + r * 128;
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int col = n0 + c0 + j;
-                if (col < N) {
-                    OutT* c = C + (int64_t)row * c_m + (int64_t)col * c_n;
-                    const double x = alpha * (double)__uint_as_float(v[j]);
-                    *c = accumulate ? (OutT)((double)*c + x) : (OutT)x;
+            for (int q = 0; q < 8; ++q) {
+                const uint32_t* w = &v[q >> 2][(q & 3) * 4];
+                float4 f;
+                if (unit) {
+                    f = make_float4(__uint_as_float(w[0]), __uint_as_float(w[1]), __uint_as_float(w[2]),
+                                    __uint_as_float(w[3]));
+                } else {
+                    f = make_float4((float)(alpha * (double)__uint_as_float(w[0])),
+                                    (float)(alpha * (double)__uint_as_float(w[1])),
+                                    (float)(alpha * (double)__uint_as_float(w[2])),
+                                    (float)(alpha * (double)__uint_as_float(w[3])));
+                }
+                *reinterpret_cast<float4*>(row + ((q ^ (r & 7)) << 4)) = f;
+            }
+        }
+        // the generic-proxy writes become visible to the tensor stores
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        // the map covers the first N4 = N rounded down to 4 columns (whole
+        // 16-byte chunks: the tensor store clips at chunk granularity); the
+        // last N - N4 columns are written from the slabs by plain stores
+        const int N4 = N & ~3;
+        if (tid == 0 && have) {
+            for (int j = 0; j < kCols / 32; ++j)
+                if (n0 + 32 * j < N4) tma_store_2d(tmC, st + j * kSlabBytes, n0 + 32 * j, m0);
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+        if (have && N4 < N && m0 + r < M) {
+            for (int col = max(N4, n0); col < min(N, n0 + kCols); ++col) {
+                const int cc = col - n0, q = (cc & 31) >> 2;
+                const float* src = reinterpret_cast<const float*>(st + (cc >> 5) * kSlabBytes + r * 128 +
+                                                                  ((q ^ (r & 7)) << 4)) + (cc & 3);
+                reinterpret_cast<float*>(C)[(int64_t)(m0 + r) * c_m + col] = *src;
+            }
+        }
+        // the slabs are read before the CTA exits
+        if (tid == 0 && have) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    } else if (rowf) {
+        // row-major float output without a map: the tile goes through the
+        // stage ring so that each warp's global stores run along a row (one
+        // thread per row would scatter every store over 32 rows)
+        constexpr int kLds = kCols + 4;  // rows 4 banks apart: conflict-free float4 stores
+        static_assert(sizeof(sm.a) + sizeof(sm.b) >= sizeof(float) * kTcBM * kLds, "staging tile fits the ring");
+        float* st = reinterpret_cast<float*>(&sm.a[0][0][0]);
+        __syncthreads();
+#pragma unroll 1
+        for (int c0 = 0; c0 < kCols; c0 += 32) {
+            uint32_t v[2][16];
+            tmem_ld16_async(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v[0]);
+            tmem_ld16_async(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c0 + 16), v[1]);
+            tmem_ld_wait();
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                float f[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    f[j] = unit ? __uint_as_float(v[h][j]) : (float)(alpha * (double)__uint_as_float(v[h][j]));
+                float4* dst = reinterpret_cast<float4*>(st + r * kLds + c0 + 16 * h);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    dst[q] = make_float4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
+            }
+        }
+        __syncthreads();
+        if (have) {
+            // warp w writes rows w, w + 4, ...: 8-byte pairs along the row when
+            // the row starts allow it, else single floats
+            const int rows = min(kTcBM, M - m0), cols = min(kCols, N - n0), lane = tid & 31;
+            float* Cf = reinterpret_cast<float*>(C) + (int64_t)m0 * c_m + n0;
+            const bool pairs = (c_m & 1) == 0 && (reinterpret_cast<uintptr_t>(Cf) & 7) == 0;
+            constexpr int kRowsPerIter = 4;
+#pragma unroll 1
+            for (int rr0 = warp; rr0 < rows; rr0 += 4 * kRowsPerIter) {
+#pragma unroll
+                for (int u = 0; u < kRowsPerIter; ++u) {
+                    const int rr = rr0 + 4 * u;
+                    if (rr >= rows) break;
+                    const float* srow = st + rr * kLds;
+                    float* grow = Cf + (int64_t)rr * c_m;
+                    if (pairs) {
+#pragma unroll
+                        for (int cc = 2 * lane; cc < kCols; cc += 64) {
+                            if (cc + 1 < cols) {
+                                *reinterpret_cast<float2*>(grow + cc) = *reinterpret_cast<const float2*>(srow + cc);
+                            } else if (cc < cols) {
+                                grow[cc] = srow[cc];
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int cc = lane; cc < kCols; cc += 32)
+                            if (cc < cols) grow[cc] = srow[cc];
+                    }
+                }
+            }
+        }
+    } else {
+        const int row = m0 + r;
+#pragma unroll 1
+        for (int c0 = 0; c0 < kCols; c0 += 16) {
+            uint32_t v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (have && row < M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = n0 + c0 + j;
+                    if (col < N) {
+                        OutT* c = C + (int64_t)row * c_m + (int64_t)col * c_n;
+                        const double x = alpha * (double)__uint_as_float(v[j]);
+                        *c = accumulate ? (OutT)((double)*c + x) : (OutT)x;
+                    }
                 }
             }
         }
     }
-    // a CTA that gave up drains its producer's issued TMA loads before it exits
-    if (tid == 0)
-        for (int kb = issued > S ? issued - S : 0; kb < issued; ++kb)
-            mbar_wait(&sm.full[kb % S], (kb / S) & 1, kDrainLimit);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
@@ -245,14 +422,16 @@ __device__ __forceinline__ void tc_tile(const CUtensorMap* tmA, const CUtensorMa
     }
 }
 
-template <int BN, typename OutT, bool X3>
+template <int BN, typename OutT, bool X3, int NS, int BK>
 __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
-                                                         const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
-                                                         OutT* __restrict__ C, int64_t c_m, int64_t c_n, double alpha,
-                                                         int accumulate, int32_t* __restrict__ err, uint32_t limit) {
+                                                         const __grid_constant__ CUtensorMap tmB,
+                                                         const __grid_constant__ CUtensorMap tmC, int use_c_map,
+                                                         int M, int N, int K, OutT* __restrict__ C, int64_t c_m,
+                                                         int64_t c_n, double alpha, int accumulate,
+                                                         int32_t* __restrict__ err, uint32_t limit) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    tc_tile<BN, OutT, X3>(&tmA, &tmB, M, N, K, blockIdx.y * kTcBM, blockIdx.x * BN, C, c_m, c_n, alpha, accumulate,
-                          err, limit, smem_raw);
+    tc_tile<BN, OutT, X3, NS, BK>(&tmA, &tmB, use_c_map ? &tmC : nullptr, M, N, K, blockIdx.y * kTcBM,
+                                  blockIdx.x * (NS * BN), C, c_m, c_n, alpha, accumulate, err, limit, smem_raw);
 }
 
 // Grouped GEMM: many independent problems C_p = A_p B_p^T (float32 output,
@@ -290,7 +469,7 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_grouped_kernel(const TcGroupPr
     }
     const int ntn = (p->N + BN - 1) / BN;
     const int t = tile - p->tile_start;
-    tc_tile<BN, float, X3>(&p->ma, &p->mb, p->M, p->N, p->K, (t / ntn) * kTcBM, (t % ntn) * BN, p->C, p->ldc, 1, 1.0,
+    tc_tile<BN, float, X3>(&p->ma, &p->mb, nullptr, p->M, p->N, p->K, (t / ntn) * kTcBM, (t % ntn) * BN, p->C, p->ldc, 1, 1.0,
                            0, p->err, limit, smem_raw);
 }
 
@@ -352,37 +531,61 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// rows x K bf16 row-major (row pitch ld elements), box = box_rows x 64
-static int make_map(CUtensorMap* map, const void* base, int rows, int K, int64_t ld, int box_rows) {
+// rows x K bf16 row-major (row pitch ld elements), box = box_rows x box_k
+// (64: 128-byte rows, 128-byte swizzle; 32: 64-byte rows, 64-byte swizzle)
+static int make_map(CUtensorMap* map, const void* base, int rows, int K, int64_t ld, int box_rows,
+                    int box_k = kTcBK) {
     auto fn = encode_fn();
     if (!fn) return VTB_CUDA_ERR;
     cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-    cuuint32_t box[2] = {(cuuint32_t)kTcBK, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)box_k, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, box_k == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? VTB_OK : VTB_BAD_ARG;
 }
 
-template <int BN, typename OutT, bool X3>
+// float32 C (rows x cols, row pitch ldc elements) for the tensor-store
+// epilogue: box 32 x 128, 128-byte swizzle, over the first cols rounded down
+// to 4 columns (the kernel writes the rest); false when the layout does not
+// allow a map (base not 16-byte aligned, pitch not a multiple of 16 bytes)
+static bool make_c_map(CUtensorMap* map, const float* C, int rows, int cols, int64_t ldc) {
+    auto fn = encode_fn();
+    const int cols4 = cols & ~3;
+    if (!fn || cols4 == 0 || ((uintptr_t)C & 15) != 0 || ((ldc * 4) & 15) != 0 || ldc < cols) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)cols4, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ldc * 4};
+    cuuint32_t box[2] = {32, (cuuint32_t)kTcBM};
+    cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(C), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN, typename OutT, bool X3, int NS, int BK>
 static int launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int K, OutT* C, int64_t c_m,
                      int64_t c_n, double alpha, int accumulate, int32_t* err, cudaStream_t s) {
-    const size_t sm = sizeof(TcSmem<BN, X3>) + 1024;
+    const size_t sm = sizeof(TcSmem<BN, X3, NS, BK>) + 1024;
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [&]() {
-        attr = cudaFuncSetAttribute(tc_gemm_kernel<BN, OutT, X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sm);
+        attr = cudaFuncSetAttribute(tc_gemm_kernel<BN, OutT, X3, NS, BK>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     });
     if (attr != cudaSuccess) {
         set_last_cuda_error(attr);
         return VTB_CUDA_ERR;
     }
-    dim3 grid(ceil_div(N, BN), ceil_div(M, kTcBM));
-    tc_gemm_kernel<BN, OutT, X3><<<grid, 128, sm, s>>>(ma, mb, M, N, K, C, c_m, c_n, alpha, accumulate, err,
-                                                       wait_limit(kWaitLimit));
+    CUtensorMap mc;
+    std::memset(&mc, 0, sizeof(mc));
+    int use_c = 0;
+    if (std::is_same<OutT, float>::value && c_n == 1 && !accumulate)
+        use_c = make_c_map(&mc, reinterpret_cast<const float*>(C), M, N, c_m) ? 1 : 0;
+    dim3 grid(ceil_div(N, NS * BN), ceil_div(M, kTcBM));
+    tc_gemm_kernel<BN, OutT, X3, NS, BK><<<grid, 128, sm, s>>>(ma, mb, mc, use_c, M, N, K, C, c_m, c_n, alpha,
+                                                               accumulate, err, wait_limit(kWaitLimit));
     return launch_status();
 }
 
@@ -428,20 +631,20 @@ VTB_API int vtb_split_bf16x2(const void* src, int src_f32, int rows, int K, int6
     return launch_status();
 }
 
-template <int BN, bool X3>
+template <int BN, bool X3, int NS = 1, int BK = kTcBK>
 static int tc_dispatch(const void* A, int M, const void* B, int N, int K, void* C, int64_t c_m, int64_t c_n,
                        int out_f64, double alpha, int accumulate, int32_t* err, cudaStream_t s) {
     CUtensorMap ma, mb;
     const int Kw = X3 ? 2 * K : K;     // columns of the operand arrays
-    int st = make_map(&ma, A, M, Kw, Kw, kTcBM);
+    int st = make_map(&ma, A, M, Kw, Kw, kTcBM, BK);
     if (st) return st;
-    st = make_map(&mb, B, N, Kw, Kw, BN);
+    st = make_map(&mb, B, N, Kw, Kw, BN, BK);
     if (st) return st;
     if (out_f64)
-        return launch_tc<BN, double, X3>(ma, mb, M, N, K, reinterpret_cast<double*>(C), c_m, c_n, alpha, accumulate,
-                                         err, s);
-    return launch_tc<BN, float, X3>(ma, mb, M, N, K, reinterpret_cast<float*>(C), c_m, c_n, alpha, accumulate, err,
-                                    s);
+        return launch_tc<BN, double, X3, NS, BK>(ma, mb, M, N, K, reinterpret_cast<double*>(C), c_m, c_n, alpha,
+                                                 accumulate, err, s);
+    return launch_tc<BN, float, X3, NS, BK>(ma, mb, M, N, K, reinterpret_cast<float*>(C), c_m, c_n, alpha,
+                                            accumulate, err, s);
 }
 
 template <bool X3>
@@ -459,6 +662,8 @@ static int tc_gemm_bn(const void* A, int M, const void* B, int N, int K, void* C
         case 160: return tc_dispatch<160, X3>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
         case 192: return tc_dispatch<192, X3>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
         case 256: return tc_dispatch<256, X3>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
+        // two 160-column accumulators sharing each A tile, 32-wide k-blocks
+        case 320: return tc_dispatch<160, X3, 2, 32>(A, M, B, N, K, C, c_m, c_n, out_f64, alpha, accumulate, err, s);
         default: return VTB_BAD_ARG;
     }
 }

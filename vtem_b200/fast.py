@@ -133,13 +133,16 @@ class CoeffDecoder(object):
         self.ps2 = torch.as_tensor(iu[1].astype(np.int32), device=device)
         self.npairs = int(self.ps.numel())
         from . import tc
-        self.Kp2 = tc.padded_k(2 * self.N)
-        self.Lsplit = torch.empty((2 * self.npairs, 2 * self.Kp2), dtype=torch.bfloat16, device=device)
-        call("vtb_coeff_lhs_split2", dptr(self.d), self.N, self.Ks, dptr(self.ps), dptr(self.ps2), self.npairs,
+        # Gram operands: [hi | lo] over the neurons (Kh = N padded to the
+        # GEMM's k-block), rows (pair, re/im) and (upper temporal entry, re/im)
+        self.Kh = tc.padded_k(self.N)
+        self.NE = self.Kt * (self.Kt + 1)
+        self.ldc = (self.NE + 3) // 4 * 4   # 16-byte rows: the GEMM stores C with tensor stores
+        self.Lsplit = torch.empty((2 * self.npairs, 2 * self.Kh), dtype=torch.bfloat16, device=device)
+        call("vtb_coeff_lhs_sym", dptr(self.d), self.N, self.Ks, dptr(self.ps), dptr(self.ps2), self.npairs,
              dptr(self.Lsplit), stream_ptr())
-        KK = self.Kt * self.Kt
-        self.Rsplit = torch.empty((KK, 2 * self.Kp2), dtype=torch.bfloat16, device=device)
-        self.C = torch.empty((2 * self.npairs, KK), dtype=torch.float32, device=device)
+        self.Rsplit = torch.empty((self.NE, 2 * self.Kh), dtype=torch.bfloat16, device=device)
+        self.C = torch.empty((2 * self.npairs, self.ldc), dtype=torch.float32, device=device)
         self.gres = torch.empty((self.N, self.Kt), dtype=C128, device=device)
         self.r = torch.empty((self.K,), dtype=C128, device=device)
         # float32 real system, rows padded to 16 bytes (the tile Cholesky copies 16-byte chunks)
@@ -163,7 +166,7 @@ class CoeffDecoder(object):
              dptr(self.d), stream_ptr())
         self._dsw = None
         if self.solver == "mixed":
-            call("vtb_coeff_lhs_split2", dptr(self.d), self.N, self.Ks, dptr(self.ps), dptr(self.ps2), self.npairs,
+            call("vtb_coeff_lhs_sym", dptr(self.d), self.N, self.Ks, dptr(self.ps), dptr(self.ps2), self.npairs,
                  dptr(self.Lsplit), stream_ptr())
 
     def _workspace(self, mode):
@@ -236,15 +239,15 @@ class CoeffDecoder(object):
 
     def _solve_mixed(self, s, spikes):
         tk1, tk2, ind, n, kap, dl, bi = spikes
-        K, KK = self.K, self.Kt * self.Kt
+        K, NE = self.K, self.NE
         self.stat.zero_()
         call("vtb_coeff_rhs", dptr(self.d), self.N, self.Ks, dptr(self.gn), self.Kt, dptr(self.b), s)
         call("vtb_coeff_realify_vec", dptr(self.b), K, 1, dptr(self.br), s)
-        call("vtb_coeff_wn_split2", dptr(self.Wn), self.N, self.Kt, dptr(self.Rsplit), s)
-        autotune.gemm_bf16_tuned(dptr(self.Lsplit), 2 * self.npairs, dptr(self.Rsplit), KK, self.Kp2, dptr(self.C), KK,
-                                 1, 0, 1.0, 0, self._stat_ptr(7), s, x3=True)
+        call("vtb_coeff_wn_sym", dptr(self.Wn), self.N, self.Kt, dptr(self.Rsplit), s)
+        autotune.gemm_bf16_tuned(dptr(self.Lsplit), 2 * self.npairs, dptr(self.Rsplit), NE, self.Kh, dptr(self.C),
+                                 self.ldc, 1, 0, 1.0, 0, self._stat_ptr(7), s, x3=True)
         ld = self.ld32
-        call("vtb_coeff_real_scatter", dptr(self.C), KK, self.Ks, self.Kt, dptr(self.Mr32), ld, 0, s)
+        call("vtb_coeff_real_scatter", dptr(self.C), self.ldc, self.Ks, self.Kt, dptr(self.Mr32), ld, 0, s)
         if self.mixed_factor == "inverse":
             # float32 tile Cholesky and L^-1 (one cooperative launch), solves by two products
             call("vtb_chol_factor_inverse", dptr(self.Mr32), ld, K, dptr(self._cdinv), dptr(self._clinv),
@@ -274,6 +277,11 @@ class CoeffDecoder(object):
             call("vtb_norm_ratio", dptr(self.rr), dptr(self.xr), K, self._stat_ptr(3 + min(i, 3)), s)
             call("vtb_daxpy1", dptr(self.xr), dptr(self.rr), K, s)
         call("vtb_coeff_unrealify_vec", dptr(self.xr), K, 1, dptr(self.a), 0, s)
+        # work that uses the mixed solution is queued before the acceptance
+        # read, so the GPU keeps running while the host waits for the status
+        spec = getattr(self, "_speculate", None)
+        if spec is not None:
+            spec()
         flag, piv, ratios, tc_err = self._read_stat()
         self.last_pivots = piv
         self.last_ratios = ratios[:min(self.mixed_sweeps, 4)]
@@ -289,6 +297,7 @@ class CoeffDecoder(object):
             self.last_solver = "mixed->" + self.last_solver
             return
         self.last_solver = "mixed"
+        self._spec_valid = True
 
     def _mixed_solver(self, s, work):
         """The solve with the float32 factor in Mr32: the multi-CTA flag
@@ -351,9 +360,9 @@ class CoeffDecoder(object):
         if self.solver != "mixed":
             raise ValueError("gram_error needs the mixed decoder")
         s = stream_ptr()
-        K, KK = self.K, self.Kt * self.Kt
+        K = self.K
         mtc = torch.empty((K, K), dtype=torch.float32, device=self.M.device)
-        call("vtb_coeff_real_scatter", dptr(self.C), KK, self.Ks, self.Kt, dptr(mtc), K, 0, s)
+        call("vtb_coeff_real_scatter", dptr(self.C), self.ldc, self.Ks, self.Kt, dptr(mtc), K, 0, s)
         self._build_real(s)
         return float((mtc.double() - self.Mr).norm() / self.Mr.norm())
 
@@ -480,8 +489,23 @@ class CoeffDecoder(object):
 
     def decode(self, tk1, tk2, neuron_ind, kappa, delta, bias, T, dt, out=None, out_dtype=F64,
                assume_sorted=False):
-        """The window's video (Nt, decPy, decPx) at t = arange(0, T, dt)."""
-        a = self.coefficients(tk1, tk2, neuron_ind, kappa, delta, bias, assume_sorted=assume_sorted)
+        """The window's video (Nt, decPy, decPx) at t = arange(0, T, dt).
+        With the mixed solver the synthesis of the mixed solution is queued
+        before its acceptance is read and done again only if the window falls
+        back to float64."""
+        res = {}
+
+        def speculate():
+            res["u"] = self.synthesize(self.a, T, dt, out=out, out_dtype=out_dtype)
+
+        self._speculate = speculate
+        self._spec_valid = False
+        try:
+            a = self.coefficients(tk1, tk2, neuron_ind, kappa, delta, bias, assume_sorted=assume_sorted)
+        finally:
+            self._speculate = None
+        if self._spec_valid and "u" in res:
+            return res["u"]
         return self.synthesize(a, T, dt, out=out, out_dtype=out_dtype)
 
 
