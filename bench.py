@@ -666,7 +666,7 @@ def run_plain(w, prep, tk1, tk2, ind, u_fast_variants, dev, Nt):
     return out
 
 
-def run_encode(w, V, dev, reps=5):
+def run_encode(w, V, dev, reps=9):
     """Encoder stages on the clip, device-timed: the RF projection
     L = dx dy V RF^T in float64 and on the tensor cores (split-bf16 operands,
     fp32 accumulation), and the IAF block scan (float64) on the float64
@@ -689,15 +689,19 @@ def run_encode(w, V, dev, reps=5):
     bank = vrf.vrf_bank(banks) if len(banks) > 1 else banks[0]
 
     def timed(fn):
-        fn()
+        # median of per-call CUDA-event times after a warm-up call (one slow
+        # call, e.g. an allocation, does not move the figure)
+        out = fn()
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        ts = []
         for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
             out = fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return out, e0.elapsed_time(e1) / reps
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return out, float(np.median(ts))
 
     L64, t64 = timed(lambda: bank.filter(V, out_layout="neuron", precision="f64"))
     Ltc, ttc = timed(lambda: bank.filter(V, out_layout="neuron", precision="bf16x3"))

@@ -184,57 +184,58 @@ __device__ __forceinline__ unsigned c_ld_relaxed(const unsigned* p) {
 }
 
 // The diagonal CTA's look-ahead copies: during the panel factorisation of
-// step k, warp 7 polls (non-blocking relaxed loads, each read one block
-// later) the flags of the next sub-diagonal and diagonal tiles; when one is
-// published it orders the copies after the flag (one fence, in warp 7 only)
-// and tells the CTA through a shared word, and after the next barrier warps
-// 1-7 issue the tile's 16-byte cp.async copies between them (warp 0, on the
-// panel's critical path, copies nothing).  Only full, 16-byte-aligned tiles
-// are copied this way; the others take the CTA-wide path.
+// step k, warp 7 leaves the panel (whose barriers then count warps 0-6 only)
+// and polls the flags of the next sub-diagonal and diagonal tiles with
+// relaxed loads (each read one poll later); a tile whose flag it saw set is
+// ordered after the flag (one fence for all such tiles) and copied by warp
+// 7's own cp.async groups.  The fences and copies never hold up a panel
+// barrier.  Only full, 16-byte-aligned tiles are copied this way; the others
+// take the CTA-wide path.
 struct LookAhead {
     const unsigned* f[2];
     float* dst[2];
     int I[2], J[2];
-    unsigned seen[2];  // warp 7: the flag values its last poll read
+    unsigned seen[2];  // the flag values the last poll read
     bool on[2];
-    int fenced;        // warp 7: tiles whose copies are ordered after their flags (bits)
-    int issued;        // copying threads: tiles whose copies they issued (bits)
+    int issued;        // tiles whose copies were issued (bits)
 };
 
-// warp 7: one fence for the tiles whose flags the previous poll saw set,
-// published in *go; then new looks at the flags not yet seen set
-__device__ __forceinline__ void look_ahead_poll(LookAhead& la, int* go) {
+// one poll of warp 7: fence and copy the tiles whose flags the previous poll
+// saw set, then new relaxed looks at the other flags
+__device__ __forceinline__ void look_ahead_poll(const CholCtx& c, LookAhead& la) {
+    const int lane = threadIdx.x & 31;
     int nb = 0;
 #pragma unroll
     for (int t = 0; t < 2; ++t)
-        if (la.on[t] && !((la.fenced >> t) & 1) && la.seen[t] >= 1u) nb |= 1 << t;
+        if (la.on[t] && !((la.issued >> t) & 1) && la.seen[t] >= 1u) nb |= 1 << t;
     if (nb) {
         asm volatile("fence.acq_rel.gpu;\n" ::: "memory");
-        la.fenced |= nb;
-        if ((threadIdx.x & 31) == 0) *go = la.fenced;
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            if (!((nb >> t) & 1)) continue;
+            const int r0 = la.I[t] * kCT, c0 = la.J[t] * kCT;
+            for (int e = lane; e < kCTE / 4; e += 32) {
+                const int cc = e >> 4, r = (e & 15) * 4;
+                cp_async16(la.dst[t] + cc * kCT + r, c.A + (int64_t)(c0 + cc) * c.ld + r0 + r);
+            }
+        }
+        cp_async_commit();
+        la.issued |= nb;
     }
 #pragma unroll
     for (int t = 0; t < 2; ++t)
-        if (la.on[t] && !((la.fenced >> t) & 1)) la.seen[t] = c_ld_relaxed(la.f[t]);
+        if (la.on[t] && !((la.issued >> t) & 1)) la.seen[t] = c_ld_relaxed(la.f[t]);
 }
 
-// threads [first, kCThreads): their share of the copies of the tiles in go
-// (read after a barrier that follows its write) not issued yet
-__device__ __forceinline__ void look_ahead_issue(const CholCtx& c, LookAhead& la, int go, int first) {
-    const int todo = go & ~la.issued;
-    if (!todo) return;
-#pragma unroll
-    for (int t = 0; t < 2; ++t) {
-        if (!((todo >> t) & 1)) continue;
-        const int r0 = la.I[t] * kCT, c0 = la.J[t] * kCT;
-        for (int e = threadIdx.x - first; e < kCTE / 4; e += kCThreads - first) {
-            const int cc = e >> 4, r = (e & 15) * 4;
-            cp_async16(la.dst[t] + cc * kCT + r, c.A + (int64_t)(c0 + cc) * c.ld + r0 + r);
-        }
-    }
-    cp_async_commit();
-    la.issued |= todo;
+__device__ __forceinline__ bool look_ahead_open(const LookAhead& la) {
+    return (la.on[0] && !(la.issued & 1)) || (la.on[1] && !(la.issued & 2));
 }
+
+// barrier of the panel's warps 0-6 (warp 7 runs the look-ahead meanwhile)
+__device__ __forceinline__ void panel_sync() { asm volatile("bar.sync 1, 224;" ::: "memory"); }
+
+constexpr int kLookAheadPolls = 1 << 12;   // bound of warp 7's poll loop (a panel takes ~30 polls)
 
 // thread 0 checks *f >= v once (no wait); every thread learns the answer
 __device__ bool cta_ready(const unsigned* f, unsigned v, int* s_ok) {
@@ -260,10 +261,43 @@ __device__ int cta_ready2(const unsigned* f1, unsigned v1, const unsigned* f2, u
 // diagonal tile the lower triangle only)
 __device__ void store_tile(const CholCtx& c, const float* s, int I, int J) {
     const int r0 = I * kCT, c0 = J * kCT;
+    if (r0 + kCT <= c.K && c0 + kCT <= c.K && (c.ld & 3) == 0 && ((uintptr_t)c.A & 15) == 0) {
+        // full tile: 16-byte stores (4 rows of a column); a diagonal tile keeps
+        // the matrix's upper triangle (chunks across the diagonal entry by entry)
+        for (int e = threadIdx.x; e < kCTE / 4; e += kCThreads) {
+            const int cc = e >> 4, r = (e & 15) * 4;
+            float* g = c.A + (int64_t)(c0 + cc) * c.ld + r0 + r;
+            const float4 v = reinterpret_cast<const float4*>(s)[e];
+            if (I != J || r >= cc) {
+                __stcg(reinterpret_cast<float4*>(g), v);
+            } else if (r + 3 >= cc) {
+                if (r + 1 >= cc) __stcg(g + 1, v.y);
+                if (r + 2 >= cc) __stcg(g + 2, v.z);
+                __stcg(g + 3, v.w);
+            }
+        }
+        return;
+    }
     for (int e = threadIdx.x; e < kCTE; e += kCThreads) {
         const int cc = e >> 6, r = e & 63;
         const int gr = r0 + r, gc = c0 + cc;
         if (gr < c.K && gc < c.K && (I != J || r >= cc)) __stcg(c.A + (int64_t)gc * c.ld + gr, s[e]);
+    }
+}
+
+// acc[i][j] -= p_i q_j over a 4 x 4 patch with the packed FP32 FMA (rows in
+// pairs, two fma.rn per instruction: the same roundings as fmaf)
+__device__ __forceinline__ void rank1_sub(float (&acc)[4][4], float4 p, const float (&q)[4]) {
+    const float2 p01 = make_float2(p.x, p.y), p23 = make_float2(p.z, p.w);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float2 nq = make_float2(-q[j], -q[j]);
+        const float2 a01 = __ffma2_rn(p01, nq, make_float2(acc[0][j], acc[1][j]));
+        const float2 a23 = __ffma2_rn(p23, nq, make_float2(acc[2][j], acc[3][j]));
+        acc[0][j] = a01.x;
+        acc[1][j] = a01.y;
+        acc[2][j] = a23.x;
+        acc[3][j] = a23.y;
     }
 }
 
@@ -274,12 +308,8 @@ __device__ __forceinline__ void sub_ptq(float (&acc)[4][4], const float* P, cons
     for (int t = t0; t < t1; ++t) {
         const float4 p = *reinterpret_cast<const float4*>(P + t * kCT + 4 * tr);
         const float4 q = *reinterpret_cast<const float4*>(Q + t * kCT + 4 * tc);
-        const float pv[4] = {p.x, p.y, p.z, p.w};
         const float qv[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(-pv[i], qv[j], acc[i][j]);
+        rank1_sub(acc, p, qv);
     }
 }
 
@@ -294,14 +324,10 @@ __device__ __forceinline__ void sub_pq_rowq(float (&acc)[4][4], const float* P, 
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const float4 p = *reinterpret_cast<const float4*>(P + (t + u) * kCT + 4 * tr);
-            const float pv[4] = {p.x, p.y, p.z, p.w};
             float qv[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) qv[j] = u == 0 ? q[j].x : u == 1 ? q[j].y : u == 2 ? q[j].z : q[j].w;
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(-pv[i], qv[j], acc[i][j]);
+            rank1_sub(acc, p, qv);
         }
     }
 }
@@ -406,12 +432,8 @@ __device__ __forceinline__ void patch_update(float* X, const float* L, int r0, i
     for (int t = 0; t < 8; ++t) {
         const float4 pv = *reinterpret_cast<const float4*>(X + (o + t) * kCT + r0);
         const float4 qv = *reinterpret_cast<const float4*>(L + (o + t) * kCT + c0);
-        const float pa[4] = {pv.x, pv.y, pv.z, pv.w};
         const float qa[4] = {qv.x, qv.y, qv.z, qv.w};
-#pragma unroll
-        for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-            for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fmaf(-pa[ii], qa[jj], acc[ii][jj]);
+        rank1_sub(acc, pv, qa);
     }
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj)
@@ -430,7 +452,7 @@ __device__ __forceinline__ void patch_update(float* X, const float* L, int r0, i
 // conflict-free rows, broadcast column operand).  Rows 8bb+8.. of E are
 // still the identity's in the columns of block bb and need no work.
 __device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, float& pmin, float& pmax, int& bad,
-                            int nvalid, LookAhead& la, int* go) {
+                            int nvalid, LookAhead& la, volatile int* done) {
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     if (w == 0) {
         potrf8_warp(S, rinv, 0, pmin, pmax, bad, nvalid);
@@ -443,16 +465,20 @@ __device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, f
         }
     }
     __syncthreads();
+    if (w == kCThreads / 32 - 1) {
+        // warp 7: the look-ahead, until both tiles are on their way or the panel is done
+        for (int it = 0; it < kLookAheadPolls && look_ahead_open(la) && !*done; ++it) look_ahead_poll(c, la);
+        __syncthreads();
+        return;
+    }
     for (int bb = 0; bb < 8; ++bb) {
         const int o = 8 * bb, c0 = o + 8, nd = kCT - c0;
-        // warp 7 takes no part in the row substitution below: it polls the look-ahead tiles
-        if (w == kCThreads / 32 - 1 && bb > 0) look_ahead_poll(la, go);
         if (tid < kCT) {
             // one code path for both kinds of row (no divergence inside a warp)
             const bool srow = tid < nd;
             subst_row8(srow ? S : E, S, rinv, bb, srow ? c0 + tid : tid - nd);
         }
-        __syncthreads();
+        panel_sync();
         if (bb == 7) break;
         if (w == 0) {
             // next diagonal block: S[c0+i][c0+j] -= sum_t L[c0+i][o+t] L[c0+j][o+t], two entries per lane
@@ -467,11 +493,10 @@ __device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, f
             __syncwarp();
             potrf8_warp(S, rinv, bb + 1, pmin, pmax, bad, nvalid);
         } else {
-            look_ahead_issue(c, la, *go, 32);
-            // E rows 0..c0-1 (2bb+2 row patches) x columns [c0, 64); then the lower triangle of S's
-            // rows and columns [c0, 64) without the next diagonal block
+            // warps 1-6: E rows 0..c0-1 (2bb+2 row patches) x columns [c0, 64); then the lower
+            // triangle of S's rows and columns [c0, 64) without the next diagonal block
             const int m = nd / 4, me = 2 * bb + 2, ne = me * m;
-            for (int q = tid - 32; q < ne + m * m; q += kCThreads - 32) {
+            for (int q = tid - 32; q < ne + m * m; q += kCThreads - 64) {
                 // one code path for E and S patches (no divergence inside a warp)
                 const bool ep = q < ne;
                 const int q2 = q - ne, pc = q2 / m, pr = q2 % m;
@@ -479,8 +504,11 @@ __device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, f
                 patch_update(ep ? E : S, S, ep ? 4 * (q % me) : c0 + 4 * pr, c0 + 4 * (ep ? q / me : pc), o);
             }
         }
-        __syncthreads();
+        panel_sync();
     }
+    // the panel is done: warp 7 stops polling and joins
+    if (tid == 0) *done = 1;
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------- worker tasks
@@ -601,8 +629,8 @@ struct CholSmem {
     float x[kCTE];        // worker: the task's tile (staging); diagonal CTA: L_kk^-T
     float rinv[kCT];
     int ok;
-    int la;               // diagonal CTA: look-ahead tiles ordered after their flags (bit 0 sub-diagonal,
-                          // bit 1 diagonal tile); complete after the post-panel barrier
+    int la;               // diagonal CTA: look-ahead tiles copied in (bit 0 sub-diagonal, bit 1 diagonal)
+    int panel_done;       // diagonal CTA: set when the panel factorisation ends (warp 7 stops polling)
 };
 
 // 64 x 64 floats at src (16-byte aligned) into shared memory, one cp.async group
@@ -855,9 +883,12 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
         // polled for and copied by warp 7 during the panel (look-ahead)
         LookAhead la;
         la.on[0] = la.on[1] = false;
-        la.fenced = la.issued = 0;
+        la.issued = 0;
         la.seen[0] = la.seen[1] = 0u;
-        if (threadIdx.x == 0) sm.la = 0;
+        if (threadIdx.x == 0) {
+            sm.la = 0;
+            sm.panel_done = 0;
+        }
         if (k + 1 < T) {
             if (k < 1) {
                 load_tile(c, X, k + 1, k);
@@ -874,7 +905,7 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
             }
         }
         const bool hx = k < 1, hy = k < 1;
-        potrf_inv64(c, D, E, sm.rinv, pmin, pmax, bad, c.K - k * kCT, la, &sm.la);
+        potrf_inv64(c, D, E, sm.rinv, pmin, pmax, bad, c.K - k * kCT, la, &sm.panel_done);
         // the workers need L_kk^-T first (their TRSMs); L_kk itself and the
         // packed X_kk are written after the sub-diagonal tile is out, so the
         // release stores on this CTA's path wait for as few stores as possible
@@ -890,12 +921,13 @@ __device__ void diagonal(const CholCtx& c, CholSmem& sm) {
             }
             break;
         }
-        // the last poll's fence, the copies not issued yet, and all look-ahead
-        // copies complete for everyone after the second barrier
-        if (threadIdx.x >= kCThreads - 32) look_ahead_poll(la, &sm.la);
-        __syncthreads();
-        if (threadIdx.x >= 32) look_ahead_issue(c, la, sm.la, 32);
-        cp_async_wait_all();
+        // warp 7's last poll (tiles its previous poll saw set), then its
+        // copies are complete for everyone after this barrier
+        if (threadIdx.x >= kCThreads - 32) {
+            look_ahead_poll(c, la);
+            cp_async_wait_all();
+            if (threadIdx.x == kCThreads - 32) sm.la = la.issued;
+        }
         __syncthreads();
         const int pre = sm.la;
         // sub-diagonal tile: the workers applied updates k' < k (none when k = 0);

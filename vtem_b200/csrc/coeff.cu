@@ -174,6 +174,153 @@ __global__ void __launch_bounds__(256) temporal_gram_kernel(
     if (own_g) gn[(int64_t)nr * Kt + threadIdx.x] = gacc;
 }
 
+// ---- one warp per neuron (Kt(Kt+1)/2 <= 32 * kWarpEntries): no block-wide
+// barrier between the phases of a neuron, four neurons per block, so the
+// short per-neuron chains of many neurons overlap on each SM.
+constexpr int kNrWarps = 4;        // neurons (warps) per block
+constexpr int kWarpEntries = 8;    // upper W_n entries per lane: Kt(Kt+1)/2 <= 256, Mt <= 10
+
+static inline bool warp_per_neuron(int Kt) { return Kt * (Kt + 1) / 2 <= 32 * kWarpEntries; }
+
+// The temporal Gram W_n and g_n of one neuron per warp: lane l computes the
+// spike T_k(m) of the chunk's l-th spike into the warp's shared memory, then
+// owns the upper entries e = l, l + 32, ... and (l < Kt) g_n[l].  Chunks of
+// kTChunk spikes in order, the same sums in the same order as
+// temporal_gram_kernel.
+__global__ void __launch_bounds__(kNrWarps * 32) temporal_gram_warp_kernel(
+    const double* __restrict__ tk1, const double* __restrict__ tk2, const int32_t* __restrict__ ind, int nspk, int N,
+    const double* __restrict__ kappa, const double* __restrict__ delta, const double* __restrict__ bias,
+    const double* __restrict__ norm, int Mt, double W, double2* __restrict__ Wn, double2* __restrict__ gn) {
+    extern __shared__ double2 shw[];
+    const int Kt = 2 * Mt + 1, KK = Kt * Kt, nup = Kt * (Kt + 1) / 2;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nr = blockIdx.x * kNrWarps + w;
+    if (nr >= N) return;   // whole warps only; no block-wide barrier below
+    double2* T = shw + (size_t)w * kTChunk * (Kt + 1);
+    double* q = reinterpret_cast<double*>(T + kTChunk * Kt);
+    const int lo = warp_lower_bound(ind, nspk, nr), hi = warp_lower_bound(ind, nspk, nr + 1);
+    const double kd = kappa[nr] * delta[nr], bb = bias[nr], nn = norm[nr];
+    int em[kWarpEntries], emp[kWarpEntries];
+    double2 acc[kWarpEntries];
+#pragma unroll
+    for (int u = 0; u < kWarpEntries; ++u) {
+        int e = lane + 32 * u, m = 0;
+        em[u] = -1;
+        emp[u] = 0;
+        acc[u] = make_double2(0, 0);
+        if (e < nup) {
+            while (e >= Kt - m) {
+                e -= Kt - m;
+                ++m;
+            }
+            em[u] = m;
+            emp[u] = m + e;
+        }
+    }
+    double2 gacc = make_double2(0, 0);
+    for (int k0 = lo; k0 < hi; k0 += kTChunk) {
+        const int nk = min(kTChunk, hi - k0);
+        __syncwarp();
+        if (lane < nk) {
+            const double a = tk1[k0 + lane], b = tk2[k0 + lane];
+            spike_T(a, b, Mt, W, T + lane * Kt);
+            q[lane] = (kd - bb * (b - a)) * nn;   // q_k, compute_q_Kernel's formula
+        }
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < kWarpEntries; ++u) {
+            if (em[u] < 0) continue;
+            for (int kk = 0; kk < nk; ++kk) {
+                const double2 a = T[kk * Kt + em[u]], b = T[kk * Kt + emp[u]];
+                // conj(a) * b
+                acc[u].x += a.x * b.x + a.y * b.y;
+                acc[u].y += a.x * b.y - a.y * b.x;
+            }
+        }
+        if (lane < Kt) {
+            for (int kk = 0; kk < nk; ++kk) {
+                const double2 a = T[kk * Kt + lane];
+                const double qk = q[kk];
+                gacc.x += a.x * qk;
+                gacc.y -= a.y * qk;
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < kWarpEntries; ++u) {
+        if (em[u] < 0) continue;
+        const int m = em[u], mp = emp[u];
+        Wn[(int64_t)nr * KK + m * Kt + mp] = acc[u];
+        if (m != mp) Wn[(int64_t)nr * KK + mp * Kt + m] = make_double2(acc[u].x, -acc[u].y);
+    }
+    if (lane < Kt) gn[(int64_t)nr * Kt + lane] = gacc;
+}
+
+// The residual's per-neuron part, one neuron per warp: v(m) = sum_s
+// conj(d_n[s]) a(s, m) (lane m, two partial sums over s), then per chunk of
+// spikes y_k = q_k - Re sum_m T_k(m) v(m) (lane k) and g(m) += sum_k
+// conj(T_k(m)) y_k (lane m).
+__global__ void __launch_bounds__(kNrWarps * 32) coeff_residual_warp_kernel(
+    const double* __restrict__ tk1, const double* __restrict__ tk2, const int32_t* __restrict__ ind, int nspk, int N,
+    const double* __restrict__ kappa, const double* __restrict__ delta, const double* __restrict__ bias,
+    const double* __restrict__ norm, int Mt, double W, const double2* __restrict__ d, int Ks,
+    const double2* __restrict__ a, double2* __restrict__ gres) {
+    extern __shared__ double2 shw[];
+    const int Kt = 2 * Mt + 1;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nr = blockIdx.x * kNrWarps + w;
+    if (nr >= N) return;   // whole warps only; no block-wide barrier below
+    double2* T = shw + (size_t)w * (kTChunk * Kt + Kt + kTChunk);
+    double2* v = T + kTChunk * Kt;
+    double* y = reinterpret_cast<double*>(v + Kt);
+    const int lo = warp_lower_bound(ind, nspk, nr), hi = warp_lower_bound(ind, nspk, nr + 1);
+    const double kd = kappa[nr] * delta[nr], bb = bias[nr], nn = norm[nr];
+    if (lane < Kt) {
+        double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
+        const double2* dn = d + (int64_t)nr * Ks;
+        int s = 0;
+        for (; s + 1 < Ks; s += 2) {
+            const double2 d0 = dn[s], a0 = a[(int64_t)s * Kt + lane];
+            const double2 d1 = dn[s + 1], a1 = a[(int64_t)(s + 1) * Kt + lane];
+            sr0 += d0.x * a0.x + d0.y * a0.y;   // conj(d) * a
+            si0 += d0.x * a0.y - d0.y * a0.x;
+            sr1 += d1.x * a1.x + d1.y * a1.y;
+            si1 += d1.x * a1.y - d1.y * a1.x;
+        }
+        if (s < Ks) {
+            const double2 d0 = dn[s], a0 = a[(int64_t)s * Kt + lane];
+            sr0 += d0.x * a0.x + d0.y * a0.y;
+            si0 += d0.x * a0.y - d0.y * a0.x;
+        }
+        v[lane] = make_double2(sr0 + sr1, si0 + si1);
+    }
+    double2 gacc = make_double2(0, 0);
+    for (int k0 = lo; k0 < hi; k0 += kTChunk) {
+        const int nk = min(kTChunk, hi - k0);
+        __syncwarp();
+        if (lane < nk) spike_T(tk1[k0 + lane], tk2[k0 + lane], Mt, W, T + lane * Kt);
+        __syncwarp();
+        if (lane < nk) {
+            double acc = 0.0;
+            for (int m = 0; m < Kt; ++m) {
+                const double2 t = T[lane * Kt + m], vv = v[m];
+                acc += t.x * vv.x - t.y * vv.y;
+            }
+            const double qk = (kd - bb * (tk2[k0 + lane] - tk1[k0 + lane])) * nn;
+            y[lane] = qk - acc;
+        }
+        __syncwarp();
+        if (lane < Kt) {
+            for (int kk = 0; kk < nk; ++kk) {
+                const double2 t = T[kk * Kt + lane];
+                gacc.x += t.x * y[kk];
+                gacc.y -= t.y * y[kk];
+            }
+        }
+    }
+    if (lane < Kt) gres[(int64_t)nr * Kt + lane] = gacc;
+}
+
 // ------------------------------------------------------------------ M
 // Block = 4 x 4 tile of (s, s') pairs (s-tile <= s'-tile: M is Hermitian and
 // the mirror half is written from the same accumulators); threads own (m, m')
@@ -243,82 +390,77 @@ __global__ void __launch_bounds__(256) kron_gram_kernel(const double2* __restric
     }
 }
 
-// b[(s, m)] = sum_n d[n][s] g[n][m]: a cluster of kRhsSplit CTAs per spatial
-// index s, each summing a contiguous quarter of the neurons: warp w owns the
-// temporal indices m = w, w+8, ..., its lanes stride over the neurons (each
-// d[n][s] loaded once for all of the warp's m) with two partial sums per m,
-// then a warp reduction; the cluster's first CTA adds the others' partial
-// sums through distributed shared memory in rank order (deterministic).
-constexpr int kRhsMaxM = 4;   // m per warp per pass: 32 per pass
-constexpr int kRhsSplit = 4;  // CTAs per cluster (neuron quarters)
+// b[(s, m)] = sum_n d[n][s] g[n][m]: a cluster of kRhsSplit CTAs per group
+// of kRhsS spatial indices, each CTA summing a contiguous eighth of the
+// neurons.  The CTA stages up to `chunk` neurons' d[n][s0..s0+3] and
+// g[n][0..Kt) in shared memory (coalesced row reads; one chunk covers the
+// CTA's neurons at the usual sizes), and two threads per output (s, m) sum
+// the even and the odd neurons, added in that order; the cluster's first CTA
+// adds the others' partial sums through distributed shared memory in rank
+// order (deterministic).
+constexpr int kRhsS = 4;       // spatial indices per cluster
+constexpr int kRhsM = 32;      // temporal indices per pass
+constexpr int kRhsSplit = 8;   // CTAs per cluster (neuron eighths)
+
+static inline int rhs_grid(int Ks) { return ceil_div(Ks, kRhsS) * kRhsSplit; }
+
+// neurons staged per pass, so that the staging and the partial sums fit the
+// 48 KB a kernel gets without an opt-in
+static inline int rhs_chunk(int Kt) {
+    int c = 128;
+    while (c > 8 && (size_t)c * (kRhsS + Kt) * sizeof(double2) > 46 * 1024) c /= 2;
+    return c;
+}
+
+static inline size_t rhs_smem(int Kt) { return (size_t)rhs_chunk(Kt) * (kRhsS + Kt) * sizeof(double2); }
 
 __global__ void __cluster_dims__(kRhsSplit, 1, 1) __launch_bounds__(256)
     kron_rhs_kernel(const double2* __restrict__ d, int N, int Ks, const double2* __restrict__ gn, int Kt,
-                    double2* __restrict__ b) {
+                    double2* __restrict__ b, int chunk) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
-    __shared__ double2 part[32];
+    extern __shared__ double2 shr[];
+    double2* sd = shr;                  // chunk x kRhsS
+    double2* sg = shr + chunk * kRhsS;  // chunk x Kt
+    __shared__ double2 part[kRhsS * kRhsM];
     const int rank = (int)cluster.block_rank();
-    const int s = blockIdx.x / kRhsSplit;
+    const int s0 = (blockIdx.x / kRhsSplit) * kRhsS;
     const int nq = (N + kRhsSplit - 1) / kRhsSplit;
     const int n_lo = rank * nq, n_hi = min(N, n_lo + nq);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int mbase = 0; mbase < Kt; mbase += 8 * kRhsMaxM) {
-        double2 acc[kRhsMaxM][2];
-#pragma unroll
-        for (int q = 0; q < kRhsMaxM; ++q) acc[q][0] = acc[q][1] = make_double2(0, 0);
-        int n = n_lo + lane;
-        for (; n + 32 < n_hi; n += 64) {
-#pragma unroll
-            for (int u2 = 0; u2 < 2; ++u2) {
-                const int nu = n + 32 * u2;
-                const double2 dv = d[(int64_t)nu * Ks + s];
-#pragma unroll
-                for (int q = 0; q < kRhsMaxM; ++q) {
-                    const int m = mbase + w + 8 * q;
-                    if (m < Kt) {
-                        const double2 p = cmul(dv, gn[(int64_t)nu * Kt + m]);
-                        acc[q][u2].x += p.x;
-                        acc[q][u2].y += p.y;
-                    }
-                }
+    const int t = threadIdx.x, h = t & 1, o = t >> 1, si = o / kRhsM, mm = o % kRhsM;
+    for (int mb = 0; mb < Kt; mb += kRhsM) {
+        const int m = mb + mm;
+        double2 acc = make_double2(0, 0);
+        for (int c = n_lo; c < n_hi; c += chunk) {
+            const int nc = min(chunk, n_hi - c);
+            __syncthreads();
+            for (int e = t; e < nc * kRhsS; e += blockDim.x) {
+                const int n = e / kRhsS, j = e % kRhsS;
+                sd[e] = s0 + j < Ks ? d[(int64_t)(c + n) * Ks + s0 + j] : make_double2(0, 0);
             }
-        }
-        for (; n < n_hi; n += 32) {
-            const double2 dv = d[(int64_t)n * Ks + s];
-#pragma unroll
-            for (int q = 0; q < kRhsMaxM; ++q) {
-                const int m = mbase + w + 8 * q;
-                if (m < Kt) {
-                    const double2 p = cmul(dv, gn[(int64_t)n * Kt + m]);
-                    acc[q][0].x += p.x;
-                    acc[q][0].y += p.y;
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kRhsMaxM; ++q) {
-            double x = acc[q][0].x + acc[q][1].x, y = acc[q][0].y + acc[q][1].y;
-#pragma unroll
-            for (int o = 16; o; o >>= 1) {
-                x += __shfl_xor_sync(0xffffffffu, x, o);
-                y += __shfl_xor_sync(0xffffffffu, y, o);
-            }
-            if (lane == 0) part[w + 8 * q] = make_double2(x, y);
-        }
-        cluster.sync();
-        if (rank == 0 && threadIdx.x < 32) {
-            const int m = mbase + threadIdx.x;
+            for (int e = t; e < nc * Kt; e += blockDim.x) sg[e] = gn[(int64_t)c * Kt + e];
+            __syncthreads();
             if (m < Kt) {
-                double2 t = part[threadIdx.x];
-#pragma unroll
-                for (int r = 1; r < kRhsSplit; ++r) {
-                    const double2 o = cluster.map_shared_rank(part, r)[threadIdx.x];
-                    t.x += o.x;
-                    t.y += o.y;
+                for (int n = h; n < nc; n += 2) {
+                    const double2 p = cmul(sd[n * kRhsS + si], sg[n * Kt + m]);
+                    acc.x += p.x;
+                    acc.y += p.y;
                 }
-                b[(int64_t)s * Kt + m] = t;
             }
+        }
+        // even + odd neurons (lanes 2o and 2o + 1 of the same warp)
+        const double ox = __shfl_xor_sync(0xffffffffu, acc.x, 1), oy = __shfl_xor_sync(0xffffffffu, acc.y, 1);
+        if (h == 0) part[o] = make_double2(acc.x + ox, acc.y + oy);
+        cluster.sync();
+        if (rank == 0 && h == 0 && s0 + si < Ks && m < Kt) {
+            double2 v = part[o];
+#pragma unroll
+            for (int r = 1; r < kRhsSplit; ++r) {
+                const double2 w = cluster.map_shared_rank(part, r)[o];
+                v.x += w.x;
+                v.y += w.y;
+            }
+            b[(int64_t)(s0 + si) * Kt + m] = v;
         }
         cluster.sync();   // the partial sums stay valid until rank 0 has read them
     }
@@ -935,6 +1077,12 @@ VTB_API int vtb_coeff_temporal_gram(const double* tk1, const double* tk2, const 
     const int Kt = 2 * Mt + 1;
     const size_t sm = (size_t)kTChunk * (Kt + 1) * sizeof(double2);
     VTB_CHECK_ARG(Kt * (Kt + 1) / 2 <= 256 * kTgEntries);
+    if (warp_per_neuron(Kt)) {
+        temporal_gram_warp_kernel<<<ceil_div(N, kNrWarps), kNrWarps * 32, kNrWarps * sm, as_stream(stream)>>>(
+            tk1, tk2, ind, nspk, N, kappa, delta, bias, norm, Mt, W, reinterpret_cast<double2*>(Wn),
+            reinterpret_cast<double2*>(gn));
+        return launch_status();
+    }
     temporal_gram_kernel<<<N, 256, sm, as_stream(stream)>>>(tk1, tk2, ind, nspk, kappa, delta, bias, norm, Mt, W,
                                                            reinterpret_cast<double2*>(Wn),
                                                            reinterpret_cast<double2*>(gn));
@@ -959,9 +1107,9 @@ VTB_API int vtb_coeff_gram(const double* d, int N, int Ks, const double* Wn, con
                                                            reinterpret_cast<double2*>(M), ldm);
     int st = launch_status();
     if (st) return st;
-    kron_rhs_kernel<<<Ks * kRhsSplit, 256, 0, as_stream(stream)>>>(
+    kron_rhs_kernel<<<rhs_grid(Ks), 256, rhs_smem(Kt), as_stream(stream)>>>(
         reinterpret_cast<const double2*>(d), N, Ks, reinterpret_cast<const double2*>(gn), Kt,
-        reinterpret_cast<double2*>(b));
+        reinterpret_cast<double2*>(b), rhs_chunk(Kt));
     return launch_status();
 }
 
@@ -1301,9 +1449,9 @@ VTB_API int vtb_coeff_wn_sym(const double* Wn, int N, int Kt, void* R, void* str
 
 VTB_API int vtb_coeff_rhs(const double* d, int N, int Ks, const double* gn, int Kt, double* b, void* stream) {
     VTB_CHECK_ARG(N > 0 && Ks > 0 && Kt > 0 && d && gn && b);
-    kron_rhs_kernel<<<Ks * kRhsSplit, 256, 0, as_stream(stream)>>>(reinterpret_cast<const double2*>(d), N, Ks,
-                                                      reinterpret_cast<const double2*>(gn), Kt,
-                                                      reinterpret_cast<double2*>(b));
+    kron_rhs_kernel<<<rhs_grid(Ks), 256, rhs_smem(Kt), as_stream(stream)>>>(
+        reinterpret_cast<const double2*>(d), N, Ks, reinterpret_cast<const double2*>(gn), Kt,
+        reinterpret_cast<double2*>(b), rhs_chunk(Kt));
     return launch_status();
 }
 
@@ -1316,13 +1464,22 @@ VTB_API int vtb_coeff_residual(const double* tk1, const double* tk2, const int32
     const int Kt = 2 * Mt + 1;
     const size_t sm = (size_t)Kt * sizeof(double2) + (size_t)kTChunk * Kt * sizeof(double2) + kTChunk * sizeof(double);
     cudaStream_t s = as_stream(stream);
-    coeff_residual_kernel<<<N, 256, sm, s>>>(tk1, tk2, ind, nspk, kappa, delta, bias, norm, Mt, W,
-                                             reinterpret_cast<const double2*>(d), Ks,
-                                             reinterpret_cast<const double2*>(a), reinterpret_cast<double2*>(gres));
+    if (warp_per_neuron(Kt)) {
+        const size_t smw = (size_t)(kTChunk * Kt + Kt + kTChunk) * sizeof(double2);
+        coeff_residual_warp_kernel<<<ceil_div(N, kNrWarps), kNrWarps * 32, kNrWarps * smw, s>>>(
+            tk1, tk2, ind, nspk, N, kappa, delta, bias, norm, Mt, W, reinterpret_cast<const double2*>(d), Ks,
+            reinterpret_cast<const double2*>(a), reinterpret_cast<double2*>(gres));
+    } else {
+        coeff_residual_kernel<<<N, 256, sm, s>>>(tk1, tk2, ind, nspk, kappa, delta, bias, norm, Mt, W,
+                                                 reinterpret_cast<const double2*>(d), Ks,
+                                                 reinterpret_cast<const double2*>(a),
+                                                 reinterpret_cast<double2*>(gres));
+    }
     int st = launch_status();
     if (st) return st;
-    kron_rhs_kernel<<<Ks * kRhsSplit, 256, 0, s>>>(reinterpret_cast<const double2*>(d), N, Ks,
-                                       reinterpret_cast<const double2*>(gres), Kt, reinterpret_cast<double2*>(r));
+    kron_rhs_kernel<<<rhs_grid(Ks), 256, rhs_smem(Kt), s>>>(reinterpret_cast<const double2*>(d), N, Ks,
+                                                            reinterpret_cast<const double2*>(gres), Kt,
+                                                            reinterpret_cast<double2*>(r), rhs_chunk(Kt));
     return launch_status();
 }
 
@@ -1379,7 +1536,8 @@ VTB_API int vtb_coeff_from_spike_weights(const double* tk1, const double* tk2, c
     temporal_weighted_kernel<<<N, 64, 0, s>>>(tk1, tk2, ind, nspk, w, Mt, W, reinterpret_cast<double2*>(g));
     int st = launch_status();
     if (st) return st;
-    kron_rhs_kernel<<<Ks * kRhsSplit, 256, 0, s>>>(reinterpret_cast<const double2*>(d), N, Ks, reinterpret_cast<const double2*>(g),
-                                       Kt, reinterpret_cast<double2*>(a));
+    kron_rhs_kernel<<<rhs_grid(Ks), 256, rhs_smem(Kt), s>>>(reinterpret_cast<const double2*>(d), N, Ks,
+                                                            reinterpret_cast<const double2*>(g), Kt,
+                                                            reinterpret_cast<double2*>(a), rhs_chunk(Kt));
     return launch_status();
 }
