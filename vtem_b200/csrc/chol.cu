@@ -536,7 +536,7 @@ __device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, f
 // and within each pool every dependency lies earlier in its order (or in the
 // other pool, or on the diagonal), so with every CTA resident no task waits
 // on one behind it.
-constexpr int kXChunk = 8;
+constexpr int kXChunk = 4;
 
 // factorisation task t in group order
 __device__ __forceinline__ void factor_task(int T, int t, int& I, int& J, int& type) {
