@@ -471,6 +471,9 @@ __device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, f
         __syncthreads();
         return;
     }
+    // blocks past the last row inside K (the last tile of a K that is not a
+    // multiple of 64) hold the identity and stay as they are
+    const int nb = nvalid >= kCT ? 8 : max(1, (nvalid + 7) / 8);
     for (int bb = 0; bb < 8; ++bb) {
         const int o = 8 * bb, c0 = o + 8, nd = kCT - c0;
         if (tid < kCT) {
@@ -479,7 +482,7 @@ __device__ void potrf_inv64(const CholCtx& c, float* S, float* E, float* rinv, f
             subst_row8(srow ? S : E, S, rinv, bb, srow ? c0 + tid : tid - nd);
         }
         panel_sync();
-        if (bb == 7) break;
+        if (bb == nb - 1) break;
         if (w == 0) {
             // next diagonal block: S[c0+i][c0+j] -= sum_t L[c0+i][o+t] L[c0+j][o+t], two entries per lane
 #pragma unroll
