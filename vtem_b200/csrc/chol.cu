@@ -610,6 +610,21 @@ __host__ __device__ __forceinline__ int inverse_count(int T) {
     return n;
 }
 
+// Inverse tasks of the last kTailSlots slots go round-robin over ALL workers
+// (the factorisation pool runs out of work there while these chunks pile
+// up); the index of the first of them in slot order.
+constexpr int kTailSlots = 4;
+
+__host__ __device__ __forceinline__ int inverse_tail_start(int T) {
+    int n = 0;
+    for (int sl = 0; sl < T - kTailSlots; ++sl) {
+        if (sl >= 1 && sl + 1 <= T - 1) n += sl;
+        if (T - 1 >= sl + 2) n += (T - 2 - sl) * (sl / kXChunk);
+        n += sl;
+    }
+    return n;
+}
+
 __host__ __device__ __forceinline__ int task_count(int T, bool inv) {
     return factor_count(T) + (inv ? inverse_count(T) : 0);
 }
@@ -777,19 +792,28 @@ __device__ void worker(const CholCtx& c, CholSmem& sm) {
     const int T = c.T;
     const bool inv = c.Xinv != nullptr;
     const int wf = factor_workers(W, T, inv);
+    const int n_inv = inv ? inverse_count(T) : 0;
+    const int tail = (inv && wf > 0 && wf < W) ? min(inverse_tail_start(T), n_inv) : n_inv;
+    auto inverse = [&](int t) -> bool {
+        int I, J, type, k0, k1;
+        inverse_task(T, t, I, J, type, k0, k1);
+        if (type == 4) return task_inverse_chunk(c, sm, I, J, k0, k1);
+        if (type == 5) return task_inverse_final(c, sm, I, J);
+        return true;
+    };
     if (wid < wf) {
         const int n = factor_count(T);
         for (int t = wid; t < n; t += wf)
             if (!worker_task(c, sm, t)) return;
     } else {
-        const int n = inverse_count(T), wi = W - wf;
-        for (int t = wid - wf; t < n; t += wi) {
-            int I, J, type, k0, k1;
-            inverse_task(T, t, I, J, type, k0, k1);
-            if (type == 4 && !task_inverse_chunk(c, sm, I, J, k0, k1)) return;
-            if (type == 5 && !task_inverse_final(c, sm, I, J)) return;
-        }
+        const int wi = W - wf;
+        for (int t = wid - wf; t < tail; t += wi)
+            if (!inverse(t)) return;
     }
+    // the inverse's tail, every worker in slot order (each CTA's tasks stay
+    // in increasing global order: no task waits on one behind it)
+    for (int t = tail + wid; t < n_inv; t += W)
+        if (!inverse(t)) return;
 }
 
 // factorisation task t
