@@ -276,18 +276,27 @@ __global__ void __launch_bounds__(kNrWarps * 32) coeff_residual_warp_kernel(
     const int lo = warp_lower_bound(ind, nspk, nr), hi = warp_lower_bound(ind, nspk, nr + 1);
     const double kd = kappa[nr] * delta[nr], bb = bias[nr], nn = norm[nr];
     if (lane < Kt) {
+        // loads of 8 spatial indices are issued together (one L2 latency per 8)
+        constexpr int kU = 8;
         double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
         const double2* dn = d + (int64_t)nr * Ks;
         int s = 0;
-        for (; s + 1 < Ks; s += 2) {
-            const double2 d0 = dn[s], a0 = a[(int64_t)s * Kt + lane];
-            const double2 d1 = dn[s + 1], a1 = a[(int64_t)(s + 1) * Kt + lane];
-            sr0 += d0.x * a0.x + d0.y * a0.y;   // conj(d) * a
-            si0 += d0.x * a0.y - d0.y * a0.x;
-            sr1 += d1.x * a1.x + d1.y * a1.y;
-            si1 += d1.x * a1.y - d1.y * a1.x;
+        for (; s + kU <= Ks; s += kU) {
+            double2 dd[kU], aa[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                dd[u] = dn[s + u];
+                aa[u] = a[(int64_t)(s + u) * Kt + lane];
+            }
+#pragma unroll
+            for (int u = 0; u < kU; u += 2) {
+                sr0 += dd[u].x * aa[u].x + dd[u].y * aa[u].y;   // conj(d) * a
+                si0 += dd[u].x * aa[u].y - dd[u].y * aa[u].x;
+                sr1 += dd[u + 1].x * aa[u + 1].x + dd[u + 1].y * aa[u + 1].y;
+                si1 += dd[u + 1].x * aa[u + 1].y - dd[u + 1].y * aa[u + 1].x;
+            }
         }
-        if (s < Ks) {
+        for (; s < Ks; ++s) {
             const double2 d0 = dn[s], a0 = a[(int64_t)s * Kt + lane];
             sr0 += d0.x * a0.x + d0.y * a0.y;
             si0 += d0.x * a0.y - d0.y * a0.x;
