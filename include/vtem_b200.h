@@ -282,8 +282,9 @@ int vtb_coeff_synthesize(const double* a, const int32_t* smap, int Ks, int Mx, i
  * with C[f] = [1, cos(mWt), sin(mWt) for m = 1..Mt] at t = t0 + f dt and the
  * per-pixel weights H of vtb_coeff_basis (column 0 = Re B_0, 2m-1 = Re P_m,
  * 2m = -Im P_m, where B_m(p) = sum_s a[s][m] E_s(p) and P_m = B_m +
- * conj B_{-m}): 2Mt+1 float64 FMAs per voxel, the coefficients' spatial sum
- * done once per window instead of once per frame.  H: P x ldh doubles, P =
+ * conj B_{-m}): the frames are taken in pairs symmetric about each block's
+ * centre frame, 2Mt+1 float64 FMAs per pair of voxels, the coefficients'
+ * spatial sum done once per window instead of once per frame.  H: P x ldh doubles, P =
  * Px*Py pixels in row-major frame order, ldh >= 2Mt+1 <= 33 (basis) or <= 21
  * (harmonics).  Replaces reconstruct_Kernel (vtem/dirichlet.py:354-420) on
  * the coefficient space, as vtb_coeff_synthesize does. */
@@ -291,6 +292,13 @@ int vtb_coeff_basis(const double* a, const int32_t* smap, int Ks, int Mx, int My
                     int Py1, double* H, int ldh, void* stream);
 int vtb_synth_harmonics(const double* H, int ldh, int P, int Mt, double W, double t0, double dt, int Nt, void* u,
                         int out_f32, void* stream);
+/* vtb_coeff_basis followed by vtb_synth_harmonics in one call (Mt in
+ * 1..10), so that no host round trip separates the two kernels.
+ * H is caller-owned scratch of P x ldh doubles.  Replaces reconstruct_Kernel
+ * (vtem/dirichlet.py:354-420) on the coefficient space. */
+int vtb_coeff_synth_rank(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, int Px, int Py,
+                         int Px1, int Py1, double* H, int ldh, double W, double t0, double dt, int Nt, void* u,
+                         int out_f32, void* stream);
 
 /* Grouped tensor-core GEMM: nprob independent problems C_p = A_p B_p^T (bf16
  * K-major operands as vtb_tc_gemm_bf16's, float32 row-major C_p with leading

@@ -110,3 +110,56 @@ def test_rank_synthesis_rejects_unsupported_orders():
     # Mt = 11: 23 harmonics, beyond the kernel's 21
     assert lib.vtb_synth_harmonics(x.data_ptr(), 23, 2, 11, 1.0, 0.0, 1e-3, 1, x.data_ptr(), 0,
                                    _abi.stream_ptr()) == _abi.VTB_BAD_ARG
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_synth_rank_one_call_matches_direct_sum(case, dtype):
+    """vtb_coeff_synth_rank: weights and harmonics in one call, the harmonics
+    kernel launched programmatically behind the weights kernel."""
+    Mx, My, Mt, Px, Py, Px1, Py1, Nt = case
+    rng = np.random.default_rng(Mx * 100 + My * 10 + Mt + 11)
+    smap = torch.as_tensor(ellipse_storage_index(Mx, My), device="cuda")
+    Ks, Kt = int(smap.numel()), 2 * Mt + 1
+    a = rng.standard_normal(Ks * Kt) + 1j * rng.standard_normal(Ks * Kt)
+    W, t0, dt = 2 * np.pi * 20 / Mt, 0.021, 1e-3
+    ad = torch.as_tensor(a, dtype=torch.complex128, device="cuda")
+    H = torch.empty((Px * Py, Kt), dtype=torch.float64, device="cuda")
+    u = torch.full((Nt, Py, Px), float("nan"), dtype=dtype, device="cuda")
+    st = _abi.lib().vtb_coeff_synth_rank(ad.data_ptr(), smap.data_ptr(), Ks, Mx, My, Mt, Px, Py, Px1, Py1,
+                                         H.data_ptr(), Kt, W, t0, dt, Nt, u.data_ptr(), int(dtype == torch.float32),
+                                         _abi.stream_ptr())
+    assert st == 0, _abi.status_string(st)
+    ref = _direct(a, Mx, My, Mt, W, t0, dt, Nt, Px, Py, Px1, Py1)
+    got = u.double().cpu().numpy()
+    assert np.isfinite(got).all()
+    tol = 1e-12 if dtype == torch.float64 else 1e-6
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    assert err <= tol, err
+
+
+@pytest.mark.parametrize("Nt", [1100, 1101])
+def test_synth_rank_long_frame_ranges(Nt):
+    """Frame ranges longer than one pass of frame pairs (a wide frame, so few
+    ranges per pixel tile), even and odd range lengths: the same video as
+    the per-frame fused kernel."""
+    Mx, My, Mt, Px, Py = 3, 3, 4, 296, 256
+    rng = np.random.default_rng(Nt)
+    smap = torch.as_tensor(ellipse_storage_index(Mx, My), device="cuda")
+    Ks, Kt = int(smap.numel()), 2 * Mt + 1
+    a = rng.standard_normal(Ks * Kt) + 1j * rng.standard_normal(Ks * Kt)
+    W, t0, dt = 2 * np.pi * 20 / Mt, 0.37, 1e-4
+    ad = torch.as_tensor(a, dtype=torch.complex128, device="cuda")
+    H = torch.empty((Px * Py, Kt), dtype=torch.float64, device="cuda")
+    u = torch.full((Nt, Py, Px), float("nan"), dtype=torch.float64, device="cuda")
+    ref = torch.empty_like(u)
+    lib = _abi.lib()
+    st = lib.vtb_coeff_synth_rank(ad.data_ptr(), smap.data_ptr(), Ks, Mx, My, Mt, Px, Py, Px, Py, H.data_ptr(), Kt,
+                                  W, t0, dt, Nt, u.data_ptr(), 0, _abi.stream_ptr())
+    assert st == 0, _abi.status_string(st)
+    st = lib.vtb_coeff_synthesize(ad.data_ptr(), smap.data_ptr(), Ks, Mx, My, Mt, W, t0, dt, Nt, Px, Py, Px, Py,
+                                  None, ref.data_ptr(), 0, _abi.stream_ptr())
+    assert st == 0, _abi.status_string(st)
+    assert torch.isfinite(u).all()
+    err = float((u - ref).abs().max() / ref.abs().max())
+    assert err <= 1e-12, err

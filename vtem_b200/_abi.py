@@ -57,6 +57,7 @@ SIGNATURES = {
     "vtb_coeff_synthesize": [P, P, I, I, I, I, D, D, D, I, I, I, I, I, P, P, I, P],
     "vtb_coeff_basis": [P, P, I, I, I, I, I, I, I, I, P, I, P],
     "vtb_synth_harmonics": [P, I, I, I, D, D, D, I, P, I, P],
+    "vtb_coeff_synth_rank": [P, P, I, I, I, I, I, I, I, I, P, I, D, D, D, I, P, I, P],
     "vtb_coeff_synthesize_noalloc": [P, P, I, I, I, I, D, D, D, I, I, I, I, I, P, I, P],
     "vtb_split_bf16x3": [P, I, I, I, L, L, D, I, P, P],
     "vtb_tc_gemm_bf16": [P, I, P, I, I, P, L, L, I, D, I, P, P],

@@ -15,15 +15,20 @@
 // weights: 2Mt+1 = 17 float64 FMAs per voxel at the GPU configuration,
 // against the 8 bytes the voxel costs in HBM.
 //
-//   basis_kernel: H, a block per m and 64 x 4 pixel tile: the row sums of
-//     the coefficient grid over the tile's columns, then 2(2My+1) complex
-//     MACs per pixel (ex/ey of the period grid in shared memory, with the
-//     (-1)^(mx+my) signs and crop offsets of the decode grid).
-//   harmonics_kernel: U.  A block owns 256 * kHPix consecutive pixels and a
-//     range of frames; each thread keeps its kHPix pixels' Kt weights in
-//     registers, the block's frames' harmonics C (by powers of e^{jWt}) sit
-//     in shared memory and are read as broadcasts, and each warp writes 32
-//     consecutive voxels per store (streaming stores, the video exceeds L2).
+//   basis_kernel: H, a block per m and 64 x 4 pixel tile: the coefficients
+//     of m and -m placed on the dense (2My+1) x (2Mx+1) grid (zero outside
+//     the ellipse), the grid's row sums over the tile's columns, then
+//     2(2My+1) complex MACs per pixel (ex/ey of the period grid in shared
+//     memory, with the (-1)^(mx+my) signs and crop offsets of the decode
+//     grid).
+//   harmonics_kernel: U.  A block owns 256 consecutive pixels (one per
+//     thread; 64 registers, four blocks per SM) and a range of frames; each
+//     thread keeps its pixel's Kt weights in registers, rotated to the
+//     block's centre frame, and takes the frames in pairs symmetric about
+//     that centre (2Mt+1 FMAs per PAIR of voxels, see the kernel); the pair
+//     harmonics (by powers of e^{j W dt (j + 1/2)}) sit in shared memory and
+//     are read as broadcasts, and each warp writes 256 consecutive bytes per
+//     store (streaming stores, the video exceeds L2).
 #include <algorithm>
 
 #include "common.cuh"
@@ -31,9 +36,7 @@
 namespace vtb {
 
 constexpr int kHMaxKt = 33;       // Mt <= 16
-constexpr int kHPix = 2;          // pixels per thread
-constexpr int kHThreads = 256;
-constexpr int kHFrames = 64;      // frames per pass of a block
+constexpr int kHThreads = 256;    // two adjacent pixels per thread
 
 __device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -62,22 +65,18 @@ __global__ void __launch_bounds__(kBX * kBY) basis_kernel(const double2* __restr
     double2* gp = ex + Kx * kBX;                    // Ky x kBX
     double2* gn = gp + Ky * kBX;                    // Ky x kBX
     double2* ey = gn + Ky * kBX;                    // Ky x kBY
-    double2* am = ey + Ky * kBY;                    // Ks: a[s][m]
-    double2* an = am + Ks;                          // Ks: conj a[s][-m]
-    int* srow = reinterpret_cast<int*>(an + Ks);    // Ks: row of entry s
-    int* scol = srow + Ks;                          // Ks: column of entry s
-    int* rlo = scol + Ks;                           // Ky: first / last entry of each row
-    int* rhi = rlo + Ky;
+    double2* ap = ey + Ky * kBY;                    // Ky x Kx grid: a[s][m] at entry s's place, 0 elsewhere
+    double2* an = ap + Ky * Kx;                     // Ky x Kx grid: conj a[s][-m]
     const int tid = threadIdx.x, nt = blockDim.x;
     const int xd = (Px1 - Px) / 2, yd = (Py1 - Py) / 2;
-    for (int r = tid; r < Ky; r += nt) {
-        rlo[r] = Ks;
-        rhi[r] = -1;
+    for (int g = tid; g < Ky * Kx; g += nt) {
+        ap[g] = make_double2(0.0, 0.0);
+        an[g] = make_double2(0.0, 0.0);
     }
     __syncthreads();
     // threads 0..kBX-1: one pixel column each, ex[Mx +- m] = (-1)^m (e^{2 pi i (px+xd)/Px1})^(+-m)
     // by powers of one sincospi; threads kBX..kBX+kBY-1: the same for the rows (ey); threads
-    // from 128: the coefficients of this m and the grid row / column of every entry
+    // from 128: the coefficients of this m, placed on the grid
     if (tid < kBX) {
         const int px = x0 + tid;
         double sn, co;
@@ -104,36 +103,43 @@ __global__ void __launch_bounds__(kBX * kBY) basis_kernel(const double2* __restr
         }
     } else if (tid >= 128) {
         for (int s = tid - 128; s < Ks; s += nt - 128) {
-            am[s] = a[(int64_t)s * Kt + Mt + m];
+            const int g = __ldg(smap + s);
+            if (g < 0 || g >= Ky * Kx) continue;    // an index outside the grid contributes nothing
+            ap[g] = a[(int64_t)s * Kt + Mt + m];
             const double2 v = a[(int64_t)s * Kt + Mt - m];
-            an[s] = make_double2(v.x, -v.y);
-            const int g = __ldg(smap + s), rr = g / Kx;
-            const bool ok = g >= 0 && rr < Ky;          // an index outside the grid contributes nothing
-            srow[s] = ok ? rr : -1;
-            scol[s] = ok ? g - rr * Kx : 0;
-            if (ok) {
-                atomicMin(rlo + rr, s);
-                atomicMax(rhi + rr, s);
-            }
+            an[g] = make_double2(v.x, -v.y);
         }
     }
     __syncthreads();
-    // row sums of this block's columns
+    // row sums of this block's columns over the grid's columns (zero outside the ellipse);
+    // two partial sums per output halve the dependent chain
     for (int e = tid; e < Ky * kBX; e += nt) {
         const int rr = e / kBX, x = e % kBX;
-        double2 sp = make_double2(0.0, 0.0), sq = make_double2(0.0, 0.0);
-        for (int s = rlo[rr]; s <= rhi[rr]; ++s) {
-            if (srow[s] != rr) continue;
-            const double2 e1 = ex[scol[s] * kBX + x];
-            const double2 t1 = c_mul(am[s], e1);
-            sp.x += t1.x;
-            sp.y += t1.y;
-            const double2 t2 = c_mul(an[s], make_double2(e1.x, -e1.y));
-            sq.x += t2.x;
-            sq.y += t2.y;
+        const double2* apr = ap + rr * Kx;
+        const double2* anr = an + rr * Kx;
+        double2 sp0 = make_double2(0.0, 0.0), sq0 = sp0, sp1 = sp0, sq1 = sp0;
+        int c = 0;
+        for (; c + 1 < Kx; c += 2) {
+            const double2 e0 = ex[c * kBX + x], e1 = ex[(c + 1) * kBX + x];
+            const double2 p0 = apr[c], p1 = apr[c + 1], n0 = anr[c], n1 = anr[c + 1];
+            sp0.x = fma(p0.x, e0.x, fma(-p0.y, e0.y, sp0.x));
+            sp0.y = fma(p0.x, e0.y, fma(p0.y, e0.x, sp0.y));
+            sq0.x = fma(n0.x, e0.x, fma(n0.y, e0.y, sq0.x));      // n0 conj(e0)
+            sq0.y = fma(n0.y, e0.x, fma(-n0.x, e0.y, sq0.y));
+            sp1.x = fma(p1.x, e1.x, fma(-p1.y, e1.y, sp1.x));
+            sp1.y = fma(p1.x, e1.y, fma(p1.y, e1.x, sp1.y));
+            sq1.x = fma(n1.x, e1.x, fma(n1.y, e1.y, sq1.x));
+            sq1.y = fma(n1.y, e1.x, fma(-n1.x, e1.y, sq1.y));
         }
-        gp[e] = sp;
-        gn[e] = sq;
+        if (c < Kx) {
+            const double2 e0 = ex[c * kBX + x], p0 = apr[c], n0 = anr[c];
+            sp0.x = fma(p0.x, e0.x, fma(-p0.y, e0.y, sp0.x));
+            sp0.y = fma(p0.x, e0.y, fma(p0.y, e0.x, sp0.y));
+            sq0.x = fma(n0.x, e0.x, fma(n0.y, e0.y, sq0.x));
+            sq0.y = fma(n0.y, e0.x, fma(-n0.x, e0.y, sq0.y));
+        }
+        gp[e] = make_double2(sp0.x + sp1.x, sp0.y + sp1.y);
+        gn[e] = make_double2(sq0.x + sq1.x, sq0.y + sq1.y);
     }
     __syncthreads();
     const int x = tid % kBX, y = tid / kBX;
@@ -165,77 +171,170 @@ __device__ __forceinline__ void stream_store(OutT* p, double v) {
     __stcs(p, (OutT)v);
 }
 
-// U[f][p] = sum_k C[f][k] H[p][k], f = fb..fe of this block, pixels
-// pbase + t + 256 j (j < kHPix)
+// two adjacent pixels of one frame with one 16-byte (float64) or 8-byte
+// (float32) streaming store when the row allows it
+template <typename OutT>
+__device__ __forceinline__ void store_pair(OutT* row, int p, int P, bool vec, double v0, double v1) {
+    if (vec) {
+        if constexpr (sizeof(OutT) == 8) {
+            __stcs(reinterpret_cast<double2*>(row + p), make_double2(v0, v1));
+        } else {
+            __stcs(reinterpret_cast<float2*>(row + p), make_float2((float)v0, (float)v1));
+        }
+    } else {
+        if (p < P) stream_store(row + p, v0);
+        if (p + 1 < P) stream_store(row + p + 1, v1);
+    }
+}
+
+// U[f][p] = sum_k C[f][k] H[p][k] for the frames fb..fe-1 of this block and
+// the pixels pbase + 2 t + {0, 1}.  The frames are taken in pairs placed
+// symmetrically about the block's centre angle th_c = W (t0 + c dt): with
+// A_m = a_m cos(m th_c) + b_m sin(m th_c), B_m = b_m cos(m th_c) - a_m sin(m th_c)
+// (a_m = H[p][2m-1], b_m = H[p][2m], A_0 = H[p][0]), the two frames at th_c -+ phi are
+//     u = E -+ O,  E = sum_{m=0}^{Mt} A_m cos(m phi),  O = sum_{m=1}^{Mt} B_m sin(m phi),
+// so a pair of voxels costs 2Mt+1 FMAs and two adds instead of 2(2Mt+1) FMAs.
+// The rotation to A, B is done once per pixel and block.
+constexpr int kHPairs = 160;      // frame pairs per pass of a block (even)
+
+#ifndef VTB_HARM_PIX
+#define VTB_HARM_PIX 1            // pixels per thread (1, or 2 adjacent with vector stores)
+#endif
+#ifndef VTB_HARM_QP
+#define VTB_HARM_QP 2             // frame pairs per inner iteration
+#endif
+constexpr int kHPix = VTB_HARM_PIX;
+constexpr int kHQp = VTB_HARM_QP;
+static_assert(kHPix == 1 || kHPix == 2, "one or two pixels per thread");
+static_assert(kHPairs % kHQp == 0, "whole groups of pairs per pass");
+
 template <typename OutT, int KT>
 __global__ void __launch_bounds__(kHThreads) harmonics_kernel(const double* __restrict__ H, int ldh, int P,
                                                               double W, double t0, double dt, int Nt, int fchunks,
-                                                              OutT* __restrict__ u) {
-    __shared__ __align__(16) double Cs[kHFrames + 1][KT + 1];   // one spare row for an odd frame count
+                                                              int vec, OutT* __restrict__ u) {
     constexpr int MT = (KT - 1) / 2;
+    // (cos m phi_j, sin m phi_j), m = 1..MT; spare rows for a pass whose pair count is not a multiple of kHQp
+    __shared__ __align__(16) double2 Cs[kHPairs + kHQp][MT];
+    __shared__ __align__(16) double2 Rc[MT];                // (cos m th_c, sin m th_c)
     const int tid = threadIdx.x;
     const int ptile = blockIdx.x / fchunks, fc = blockIdx.x % fchunks;
     const int fb = (int)((int64_t)fc * Nt / fchunks), fe = (int)((int64_t)(fc + 1) * Nt / fchunks);
-    const int pbase = ptile * kHThreads * kHPix;
-    double h[kHPix][KT];
-#pragma unroll
-    for (int j = 0; j < kHPix; ++j) {
-        const int p = pbase + tid + kHThreads * j;
-#pragma unroll
-        for (int k = 0; k < KT; ++k) h[j][k] = p < P ? __ldg(H + (int64_t)p * ldh + k) : 0.0;
-    }
-    for (int f0 = fb; f0 < fe; f0 += kHFrames) {
-        const int nf = min(kHFrames, fe - f0);
-        __syncthreads();
-        if (tid < nf) {
+    const int nfr = fe - fb, half = nfr >> 1, odd = nfr & 1;
+    const int npairs = half + odd;
+    // pair j: frames lo = fb + half - 1 + odd - j and hi = fb + half + j, at th_c -+ (j + h) W dt
+    const double h = odd ? 0.0 : 0.5;
+    const double wdt = W * dt;
+    auto fill_pairs = [&](int j0) {
+        const int j = j0 + tid;
+        if (tid < kHPairs && j < npairs) {
             double sn, co;
-            sincos(W * (t0 + (f0 + tid) * dt), &sn, &co);
+            sincos(wdt * ((double)j + h), &sn, &co);
             const double2 base = make_double2(co, sn);
-            double2 pw = make_double2(1.0, 0.0);
-            Cs[tid][0] = 1.0;
+            double2 pw = base;
 #pragma unroll
-            for (int m = 1; m <= MT; ++m) {
+            for (int m = 0; m < MT; ++m) {
+                Cs[tid][m] = pw;
                 pw = c_mul(pw, base);
-                Cs[tid][2 * m - 1] = pw.x;
-                Cs[tid][2 * m] = pw.y;
             }
         }
-        __syncthreads();
-        // two frames at a time: 2 x kHPix independent FMA chains per thread
-        for (int q = 0; q < nf; q += 2) {
-            const bool two = q + 1 < nf;
-            double acc0[kHPix], acc1[kHPix];
+    };
+    if (nfr > 0) {
+        fill_pairs(0);
+        if (tid == kHThreads - 1) {
+            double sn, co;
+            sincos(W * (t0 + ((double)fb + 0.5 * (double)(nfr - 1)) * dt), &sn, &co);
+            const double2 base = make_double2(co, sn);
+            double2 pw = base;
 #pragma unroll
-            for (int j = 0; j < kHPix; ++j) acc0[j] = acc1[j] = 0.0;
-#pragma unroll
-            for (int k = 0; k < KT; ++k) {
-                const double c0 = Cs[q][k], c1 = Cs[q + 1][k];
-#pragma unroll
-                for (int j = 0; j < kHPix; ++j) {
-                    acc0[j] = fma(c0, h[j][k], acc0[j]);
-                    acc1[j] = fma(c1, h[j][k], acc1[j]);
-                }
+            for (int m = 0; m < MT; ++m) {
+                Rc[m] = pw;
+                pw = c_mul(pw, base);
             }
-            OutT* uf = u + (int64_t)(f0 + q) * P;
+        }
+    }
+    if (nfr <= 0) return;
+    __syncthreads();
+    const int p = ptile * kHThreads * kHPix + kHPix * tid;
+    double A[kHPix][MT + 1], B[kHPix][MT];
 #pragma unroll
-            for (int j = 0; j < kHPix; ++j) {
-                const int p = pbase + tid + kHThreads * j;
-                if (p < P) {
-                    stream_store(uf + p, acc0[j]);
-                    if (two) stream_store(uf + P + p, acc1[j]);
+    for (int i = 0; i < kHPix; ++i) {
+        const bool in = p + i < P;
+        const double* hp = H + (int64_t)(p + i) * ldh;
+        A[i][0] = in ? __ldg(hp) : 0.0;
+#pragma unroll
+        for (int m = 1; m <= MT; ++m) {
+            const double a = in ? __ldg(hp + 2 * m - 1) : 0.0, b = in ? __ldg(hp + 2 * m) : 0.0;
+            const double2 r = Rc[m - 1];
+            A[i][m] = fma(a, r.x, b * r.y);
+            B[i][m - 1] = fma(b, r.x, -(a * r.y));
+        }
+    }
+    const bool active = p < P;
+    for (int j0 = 0; j0 < npairs; j0 += kHPairs) {
+        const int np = min(kHPairs, npairs - j0);
+        if (j0 > 0) {
+            __syncthreads();
+            fill_pairs(j0);
+            __syncthreads();
+        }
+        if (active) {
+            // kHQp pairs at a time: kHQp x kHPix x (E, O) independent FMA chains
+            for (int q = 0; q < np; q += kHQp) {
+                double E[kHQp][kHPix], O[kHQp][kHPix];
+#pragma unroll
+                for (int k = 0; k < kHQp; ++k) {
+#pragma unroll
+                    for (int i = 0; i < kHPix; ++i) {
+                        E[k][i] = A[i][0];
+                        O[k][i] = 0.0;
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < MT; ++m) {
+#pragma unroll
+                    for (int k = 0; k < kHQp; ++k) {
+                        const double2 c = Cs[q + k][m];
+#pragma unroll
+                        for (int i = 0; i < kHPix; ++i) {
+                            E[k][i] = fma(c.x, A[i][m + 1], E[k][i]);
+                            O[k][i] = fma(c.y, B[i][m], O[k][i]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kHQp; ++k) {
+                    if (q + k >= np) break;
+                    const int j = j0 + q + k;
+                    const int lo = fb + half - 1 + odd - j, hi = fb + half + j;
+                    OutT* rh = u + (int64_t)hi * P;
+                    OutT* rl = u + (int64_t)lo * P;
+                    if constexpr (kHPix == 2) {
+                        store_pair(rh, p, P, vec, E[k][0] + O[k][0], E[k][1] + O[k][1]);
+                        if (lo != hi) store_pair(rl, p, P, vec, E[k][0] - O[k][0], E[k][1] - O[k][1]);
+                    } else {
+                        stream_store(rh + p, E[k][0] + O[k][0]);
+                        if (lo != hi) stream_store(rl + p, E[k][0] - O[k][0]);
+                    }
                 }
             }
         }
     }
 }
 
+// fchunks: frame ranges per pixel tile, about four blocks per SM in all and
+// at least two frames per range
+static int harm_fchunks(int P, int Nt) {
+    const int ptiles = ceil_div(P, kHThreads * kHPix);
+    return std::max(1, std::min(ceil_div(Nt, 8), ceil_div(4 * kNumSMs, ptiles)));
+}
+
 template <typename OutT, int KT>
 static void launch_harm(const double* H, int ldh, int P, double W, double t0, double dt, int Nt, OutT* u,
                         cudaStream_t s) {
     const int ptiles = ceil_div(P, kHThreads * kHPix);
-    // about four blocks per SM in all, at least one frame block per pass
-    int fchunks = std::max(1, std::min(ceil_div(Nt, 8), ceil_div(4 * kNumSMs, ptiles)));
-    harmonics_kernel<OutT, KT><<<ptiles * fchunks, kHThreads, 0, s>>>(H, ldh, P, W, t0, dt, Nt, fchunks, u);
+    const int fchunks = harm_fchunks(P, Nt);
+    const int vec = (P % 2 == 0 && reinterpret_cast<uintptr_t>(u) % (2 * sizeof(OutT)) == 0) ? 1 : 0;
+    harmonics_kernel<OutT, KT><<<ptiles * fchunks, kHThreads, 0, s>>>(H, ldh, P, W, t0, dt, Nt, fchunks, vec, u);
 }
 
 template <typename OutT>
@@ -269,21 +368,25 @@ using namespace vtb;
 // on the coefficient space: B_m(p) = sum_s a[s][m] phi_s(p), phi_s the
 // decode-grid Dirichlet functions of compute_dirich_space_fft
 // (vtem/vrf.py:437-499, period Px1 x Py1 cropped to Px x Py).
-VTB_API int vtb_coeff_basis(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, int Px, int Py,
-                            int Px1, int Py1, double* H, int ldh, void* stream) {
+static int launch_basis(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, int Px, int Py,
+                        int Px1, int Py1, double* H, int ldh, cudaStream_t stream) {
     VTB_CHECK_ARG(Ks > 0 && Mx >= 0 && My >= 0 && Mt >= 0 && Px > 0 && Py > 0 && Px1 >= Px && Py1 >= Py);
     VTB_CHECK_ARG(a && smap && H && ldh >= 2 * Mt + 1 && 2 * Mt + 1 <= kHMaxKt);
     VTB_CHECK_ARG((int64_t)Mx * Px1 < (1LL << 30) && (int64_t)My * Py1 < (1LL << 30));
     const int Kx = 2 * Mx + 1, Ky = 2 * My + 1;
-    const size_t sm = (size_t)(Kx * kBX + 2 * Ky * kBX + Ky * kBY + 2 * Ks) * sizeof(double2) +
-                      (size_t)(2 * Ks + 2 * Ky) * sizeof(int);
+    const size_t sm = (size_t)(Kx * kBX + 2 * Ky * kBX + Ky * kBY + 2 * Ky * Kx) * sizeof(double2);
     VTB_CHECK_ARG(sm <= 200 * 1024);
     if (sm > 48 * 1024)
         VTB_CUDA_TRY(cudaFuncSetAttribute(basis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     dim3 grid(ceil_div(Px, kBX) * ceil_div(Py, kBY), Mt + 1);
-    basis_kernel<<<grid, kBX * kBY, sm, as_stream(stream)>>>(reinterpret_cast<const double2*>(a), smap, Ks, Mx, My, Mt,
-                                                            Px, Py, Px1, Py1, H, ldh);
+    basis_kernel<<<grid, kBX * kBY, sm, stream>>>(reinterpret_cast<const double2*>(a), smap, Ks, Mx, My, Mt, Px, Py,
+                                                  Px1, Py1, H, ldh);
     return launch_status();
+}
+
+VTB_API int vtb_coeff_basis(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, int Px, int Py,
+                            int Px1, int Py1, double* H, int ldh, void* stream) {
+    return launch_basis(a, smap, Ks, Mx, My, Mt, Px, Py, Px1, Py1, H, ldh, as_stream(stream));
 }
 
 // Video u[f][p] (Nt frames of P pixels, float64 or float32 when out_f32) at
@@ -297,6 +400,25 @@ VTB_API int vtb_synth_harmonics(const double* H, int ldh, int P, int Mt, double 
     if (Nt == 0) return VTB_OK;
     VTB_CHECK_ARG(H && u);
     cudaStream_t s = as_stream(stream);
+    if (out_f32) return dispatch_harm<float>(2 * Mt + 1, H, ldh, P, W, t0, dt, Nt, reinterpret_cast<float*>(u), s);
+    return dispatch_harm<double>(2 * Mt + 1, H, ldh, P, W, t0, dt, Nt, reinterpret_cast<double*>(u), s);
+}
+
+// The whole rank-(2Mt+1) synthesis in one call: the weights H (P x ldh,
+// caller-owned scratch) of vtb_coeff_basis, then the video u as
+// vtb_synth_harmonics writes it, both kernels queued by this call so that no
+// host round trip separates them.  Mt in 1..10.  Replaces reconstruct_Kernel (vtem/dirichlet.py:354-420)
+// on the coefficient space.
+VTB_API int vtb_coeff_synth_rank(const double* a, const int32_t* smap, int Ks, int Mx, int My, int Mt, int Px, int Py,
+                                 int Px1, int Py1, double* H, int ldh, double W, double t0, double dt, int Nt, void* u,
+                                 int out_f32, void* stream) {
+    VTB_CHECK_ARG(Mt >= 1 && Nt >= 0 && (int64_t)Px * Py < (1LL << 31));
+    if (Nt == 0) return VTB_OK;
+    VTB_CHECK_ARG(u && 2 * Mt + 1 <= 21);
+    cudaStream_t s = as_stream(stream);
+    const int st = launch_basis(a, smap, Ks, Mx, My, Mt, Px, Py, Px1, Py1, H, ldh, s);
+    if (st != VTB_OK) return st;
+    const int P = Px * Py;
     if (out_f32) return dispatch_harm<float>(2 * Mt + 1, H, ldh, P, W, t0, dt, Nt, reinterpret_cast<float*>(u), s);
     return dispatch_harm<double>(2 * Mt + 1, H, ldh, P, W, t0, dt, Nt, reinterpret_cast<double*>(u), s);
 }

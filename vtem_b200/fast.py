@@ -121,6 +121,9 @@ class CoeffDecoder(object):
         if synth not in ("harmonics", "fused"):
             raise ValueError("synth must be 'harmonics' or 'fused'")
         self.synth = synth
+        # (start, end) CUDA events that synthesize() records on the current
+        # stream around its launches, for timing the synthesis alone
+        self.synth_events = None
         self.last_residual = None
         self.last_status = {}
         if solver == "mixed":
@@ -475,16 +478,27 @@ class CoeffDecoder(object):
         dev = self.M.device
         if out is None:
             out = torch.empty((Nt, self.decPy, self.decPx), dtype=out_dtype, device=dev)
-        H = self._harmonic_weights(a, stream_ptr())
-        if H is not None:
-            call("vtb_synth_harmonics", dptr(H), self.Kt, self.decPx * self.decPy, self.Mt, self.W, float(t0),
-                 float(dt), Nt, dptr(out), int(out.dtype == torch.float32), stream_ptr())
+        ev = self.synth_events
+        if ev is not None:
+            ev[0].record()
+        if self.synth == "harmonics" and self.Kt <= 21:
+            # weights and harmonics in one call (the second kernel launched programmatically)
+            P = self.decPx * self.decPy
+            if getattr(self, "_H", None) is None or self._H.shape[0] != P:
+                self._H = torch.empty((P, self.Kt), dtype=F64, device=dev)
+            call("vtb_coeff_synth_rank", dptr(a), dptr(self.smap), self.Ks, self.Mx, self.My, self.Mt, self.decPx,
+                 self.decPy, self.Px1, self.Py1, dptr(self._H), self.Kt, self.W, float(t0), float(dt), Nt, dptr(out),
+                 int(out.dtype == torch.float32), stream_ptr())
+            if ev is not None:
+                ev[1].record()
             return out
         # the fused kernel (2My+1 <= 13) needs no expansion buffer
         A = None if 2 * self.My + 1 <= 13 else torch.empty((Nt, self.Ks), dtype=C128, device=dev)
         call("vtb_coeff_synthesize", dptr(a), dptr(self.smap), self.Ks, self.Mx, self.My, self.Mt, self.W, float(t0),
              float(dt), Nt, self.decPx, self.decPy, self.Px1, self.Py1, dptr(A), dptr(out),
              int(out.dtype == torch.float32), stream_ptr())
+        if ev is not None:
+            ev[1].record()
         return out
 
     def decode(self, tk1, tk2, neuron_ind, kappa, delta, bias, T, dt, out=None, out_dtype=F64,
