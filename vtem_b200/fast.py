@@ -244,8 +244,17 @@ class CoeffDecoder(object):
         tk1, tk2, ind, n, kap, dl, bi = spikes
         K, NE = self.K, self.NE
         self.stat.zero_()
-        call("vtb_coeff_rhs", dptr(self.d), self.N, self.Ks, dptr(self.gn), self.Kt, dptr(self.b), s)
-        call("vtb_coeff_realify_vec", dptr(self.b), K, 1, dptr(self.br), s)
+        # the right-hand side runs on a side stream beside the Gram, the
+        # scatter and the factorisation, which it does not feed
+        main = torch.cuda.current_stream(self.M.device)
+        side = self._side_stream()
+        forked = torch.cuda.Event()
+        forked.record(main)
+        side.wait_event(forked)
+        call("vtb_coeff_rhs", dptr(self.d), self.N, self.Ks, dptr(self.gn), self.Kt, dptr(self.b), side.cuda_stream)
+        call("vtb_coeff_realify_vec", dptr(self.b), K, 1, dptr(self.br), side.cuda_stream)
+        rhs_done = torch.cuda.Event()
+        rhs_done.record(side)
         call("vtb_coeff_wn_sym", dptr(self.Wn), self.N, self.Kt, dptr(self.Rsplit), s)
         autotune.gemm_bf16_tuned(dptr(self.Lsplit), 2 * self.npairs, dptr(self.Rsplit), NE, self.Kh, dptr(self.C),
                                  self.ldc, 1, 0, 1.0, 0, self._stat_ptr(7), s, x3=True)
@@ -268,6 +277,7 @@ class CoeffDecoder(object):
             call("vtb_sym_factor", dptr(self.Mr32), ld, K, 2, self.rcond * CHOL_MARGIN, dptr(work), work.numel(),
                  self._stat_ptr(0), self._stat_ptr(1), s)
             solve = self._mixed_solver(s, work)
+        main.wait_event(rhs_done)
         self.xr.copy_(self.br)
         solve(self.xr)
         for i in range(self.mixed_sweeps):
@@ -301,6 +311,14 @@ class CoeffDecoder(object):
             return
         self.last_solver = "mixed"
         self._spec_valid = True
+
+    def _side_stream(self):
+        """A second stream on the decoder's device for work that overlaps
+        the main chain of a decode."""
+        st = getattr(self, "_side", None)
+        if st is None:
+            st = self._side = torch.cuda.Stream(device=self.M.device)
+        return st
 
     def _mixed_solver(self, s, work):
         """The solve with the float32 factor in Mr32: the multi-CTA flag
