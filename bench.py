@@ -340,6 +340,10 @@ def run_ours(args, rank, world, local):
         result["gram_rel_frobenius"] = gram_err
         if not args.no_serve:
             result["serving"] = serve_short(dev, args.serve_requests, args.rate)
+        if args.batch_clips > 0:
+            # many clips of uneven size decoded as one batch (grouped Grams and solves, CUDA graphs)
+            result["batch"] = batch_measure(dev, local, args.batch_clips, 2, args.sweeps, 3, 3, 2,
+                                            eig=args.batch_eig)[0]
         if not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(host_clip_from_device(w, prep, rd), windows=2, window=0.1)
     if world > 1:
@@ -429,33 +433,33 @@ def launches_mixed(dec):
     return 1 + 5 + 1 + 1 + 7 * dec.mixed_sweeps + 1 + 2
 
 
-def run_batch(args, rank, world, local):
-    """Many-clip workload: 256 independent clips of uneven size (seed 2).
-    One step = decoding every clip of the batch (mixed precision: grouped
-    float32 Cholesky, batched triangular solves and float64 refinement,
-    replayed as CUDA graphs; float64 fallbacks on worker threads); compared
-    with decoding the same clips one after another with the stand-alone
-    decoders (mixed, and float64)."""
+def batch_measure(dev, local, count, seed, sweeps, warmup, steps, plain_count, eig="bucketed"):
+    """Decode ``count`` independent clips of uneven size (batch_clips, seed
+    ``seed``) as one batch: ``steps`` timed runs of the BatchDecoder after
+    ``warmup`` (graph capture) runs, a 256 MB flush before each; the same
+    clips decoded one after another by the stand-alone decoders (mixed, and
+    float64); the plain float64 decode of the first ``plain_count`` clips for
+    the SNR.  ``eig``: how the BatchDecoder eigen-solves the systems that
+    both Cholesky factorisations refuse.  Returns (batch result dict, ms per
+    step, voxels per step)."""
     import torch
     from vtem_b200 import batch, fast, workloads
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    clips = workloads.batch_clips(count=args.clips, seed=2 + rank)
+    clips = workloads.batch_clips(count=count, seed=seed)
     t0 = time.perf_counter()
     probs = [batch.encode_clip_problem(c, device=dev) for c in clips]
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t0
     voxels = sum(p.voxels for p in probs)
     spikes = [int(p.tk1.numel()) for p in probs]
-    bd = batch.BatchDecoder(probs, streams=8, sweeps=args.sweeps, graph=True)
+    bd = batch.BatchDecoder(probs, streams=8, sweeps=sweeps, graph=True, eig=eig)
     flush = torch.zeros(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         bd.run()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
     ms, phases = 0.0, np.zeros(3)
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush_l2(flush)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -469,7 +473,7 @@ def run_batch(args, rank, world, local):
     solvers = bd.solver_counts()
 
     def sequential(solver):
-        decs = [fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver=solver, mixed_sweeps=args.sweeps)
+        decs = [fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver=solver, mixed_sweeps=sweeps)
                 for p in probs]
         for d, p in zip(decs, probs):
             d.decode(p.tk1, p.tk2, p.ind, p.kappa, p.delta, p.bias, p.T, p.dt, assume_sorted=True)
@@ -484,25 +488,45 @@ def run_batch(args, rank, world, local):
 
     seq_mixed = sequential("mixed")
     seq_f64 = sequential("auto")
-    step_ms = ms / args.steps
-    plain = plain_sample(clips, probs, bd.outs, dev, args.plain_sample)
-    return {"metric": METRIC + " [batch of %d clips]" % len(probs), "value": voxels * args.steps / (ms / 1e3),
-            "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 (split-bf16 tensor-core Gram, f32 Cholesky, f64 refinement)",
-            "data": "synthetic (seeded Dirichlet-bandlimited video)",
-            "config": {"workload": "batch: %d clips, side {16,32,48,64}, 0.05-0.5 s, Mt 3..8, M 2..6, 32..1024 RFs"
-                                   % len(probs), "voxels_per_step": voxels, "spikes_min": min(spikes),
-                       "spikes_max": max(spikes), "groups": len(bd.groups), "solvers": solvers,
-                       "cuda_graphs": bd.use_graph, "graph_error": bd.graph_error, "setup_s": t_setup,
-                       "l2": "256 MB flush between steps"},
-            "phases_ms": {"grouped_mixed_solve": phases[0] / args.steps, "f64_fallbacks": phases[1] / args.steps,
-                          "synthesis": phases[2] / args.steps},
-            "sequential_ms": {"mixed": seq_mixed, "f64": seq_f64},
-            "batched_speedup": {"vs_sequential_mixed": seq_mixed / step_ms, "vs_sequential_f64": seq_f64 / step_ms},
-            "clips_per_s": len(probs) * args.steps / (ms / 1e3), "clocks": clk,
-            "plain_fp64_sample": plain,
-            "vs_plain_fp64": (voxels * args.steps / (ms / 1e3)) / plain["voxels_per_s"] if plain else None}
+    step_ms = ms / steps
+    plain = plain_sample(clips, probs, bd.outs, dev, plain_count)
+    res = {"clips": len(probs), "voxels_per_s": voxels * steps / (ms / 1e3), "ms_per_step": step_ms,
+           "config": {"workload": "batch: %d clips, side {16,32,48,64}, 0.05-0.5 s, Mt 3..8, M 2..6, 32..1024 RFs"
+                                  % len(probs), "voxels_per_step": voxels, "spikes_min": min(spikes),
+                      "spikes_max": max(spikes), "groups": len(bd.groups), "solvers": solvers,
+                      "cuda_graphs": bd.use_graph, "graph_error": bd.graph_error, "setup_s": t_setup,
+                      "eig": eig, "l2": "256 MB flush between steps"},
+           "phases_ms": {"grouped_mixed_solve": phases[0] / steps, "f64_fallbacks": phases[1] / steps,
+                         "synthesis": phases[2] / steps},
+           "sequential_ms": {"mixed": seq_mixed, "f64": seq_f64},
+           "batched_speedup": {"vs_sequential_mixed": seq_mixed / step_ms, "vs_sequential_f64": seq_f64 / step_ms},
+           "clips_per_s": len(probs) * steps / (ms / 1e3), "clocks": clk,
+           "plain_fp64_sample": plain,
+           "vs_plain_fp64": (voxels * steps / (ms / 1e3)) / plain["voxels_per_s"] if plain else None}
+    del bd, probs, flush
+    torch.cuda.empty_cache()
+    return res, step_ms, voxels
+
+
+def run_batch(args, rank, world, local):
+    """Many-clip workload: 256 independent clips of uneven size (seed 2).
+    One step = decoding every clip of the batch (mixed precision: grouped
+    float32 Cholesky, batched triangular solves and float64 refinement,
+    replayed as CUDA graphs; float64 fallbacks on worker threads); compared
+    with decoding the same clips one after another with the stand-alone
+    decoders (mixed, and float64)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    res, step_ms, voxels = batch_measure(dev, local, args.clips, 2 + rank, args.sweeps, args.warmup, args.steps,
+                                         args.plain_sample, eig=args.batch_eig)
+    out = {"metric": METRIC + " [batch of %d clips]" % res["clips"], "value": res["voxels_per_s"],
+           "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64 (split-bf16 tensor-core Gram, f32 Cholesky, f64 refinement)",
+           "data": "synthetic (seeded Dirichlet-bandlimited video)"}
+    out.update({k: v for k, v in res.items() if k not in ("voxels_per_s", "ms_per_step", "clips")})
+    return out
 
 
 def plain_sample(clips, probs, outs, dev, count):
@@ -754,6 +778,62 @@ def run_encode_only(args, rank, world, local):
     res = run_encode(w, V, dev, reps=max(1, args.steps))
     res["config"] = {"workload": "encode: 64x64 px, %d samples, 768 Gabor + 256 centre-surround RFs" % w.F}
     return res
+
+
+def run_synth(args, rank, world, local):
+    """Synthesis kernels alone at the GPU configuration's decode shape
+    (Mx = My = 6, Mt = 8, 64 x 64 px, ``--frames`` frames) on seeded random
+    coefficients: vtb_coeff_synth_rank (weights + harmonics, one call),
+    vtb_synth_harmonics and vtb_coeff_basis, each timed ``--steps`` times
+    with CUDA events after ``--warmup`` calls, a 256 MB add queued before
+    each timed call (the host queues ahead of the device; the video, 328 MB,
+    exceeds L2); medians."""
+    import torch
+    from vtem_b200 import _abi
+    from vtem_b200.fast import ellipse_storage_index
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    Mx = My = 6
+    Mt, Px, Py, Nt = 8, 64, 64, args.frames
+    smap = torch.as_tensor(ellipse_storage_index(Mx, My), device=dev)
+    Ks, Kt = int(smap.numel()), 2 * Mt + 1
+    rng = np.random.default_rng(rank)
+    a = torch.as_tensor(rng.standard_normal(Ks * Kt) + 1j * rng.standard_normal(Ks * Kt), dtype=torch.complex128,
+                        device=dev)
+    H = torch.empty((Px * Py, Kt), dtype=torch.float64, device=dev)
+    u = torch.empty((Nt, Py, Px), dtype=torch.float64, device=dev)
+    flush = torch.zeros(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
+    lib, W, dt = _abi.lib(), 2 * np.pi * 20 / Mt, 1e-4
+
+    def rank_call():
+        return lib.vtb_coeff_synth_rank(a.data_ptr(), smap.data_ptr(), Ks, Mx, My, Mt, Px, Py, Px, Py, H.data_ptr(),
+                                        Kt, W, 0.0, dt, Nt, u.data_ptr(), 0, _abi.stream_ptr())
+
+    def harm_call():
+        return lib.vtb_synth_harmonics(H.data_ptr(), Kt, Px * Py, Mt, W, 0.0, dt, Nt, u.data_ptr(), 0,
+                                       _abi.stream_ptr())
+
+    def basis_call():
+        return lib.vtb_coeff_basis(a.data_ptr(), smap.data_ptr(), Ks, Mx, My, Mt, Px, Py, Px, Py, H.data_ptr(), Kt,
+                                   _abi.stream_ptr())
+
+    out = {}
+    for name, fn in (("synth_rank", rank_call), ("harmonics", harm_call), ("basis", basis_call)):
+        for _ in range(args.warmup):
+            assert fn() == 0
+        ts = []
+        for _ in range(args.steps):
+            flush.add_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            assert fn() == 0
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        med = float(np.median(ts))
+        out[name] = {"median_us": med * 1e3, "min_us": min(ts) * 1e3,
+                     "video_write_gbs": Nt * Px * Py * 8 / med / 1e6}
+    return {"workload": "synth: Mx=My=6, Mt=8, 64x64 px, %d frames, random coefficients" % Nt, "kernels": out}
 
 
 def run_stitch(args, rank, world, local):
@@ -1081,7 +1161,7 @@ def main():
     ap.add_argument("--no-rnn", action="store_true")
     ap.add_argument("--rnn-steps", type=int, default=2000)
     ap.add_argument("--sweeps", type=int, default=1)
-    ap.add_argument("--workload", default="gpu", choices=["gpu", "batch", "serve", "encode", "stitch", "cpu-full"])
+    ap.add_argument("--workload", default="gpu", choices=["gpu", "batch", "serve", "encode", "stitch", "synth", "cpu-full"])
     ap.add_argument("--tile", type=int, default=48)
     ap.add_argument("--window", type=float, default=0.5)
     ap.add_argument("--clips", type=int, default=256)
@@ -1093,6 +1173,10 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=8)
     ap.add_argument("--no-serve", action="store_true", help="skip the short serving run of the default line")
     ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--batch-clips", type=int, default=256,
+                    help="clips of the batch run in the default line (0: none)")
+    ap.add_argument("--batch-eig", default="bucketed", choices=["bucketed", "threads"],
+                    help="eigen-solves of the refused batch systems: padded batches or per worker thread")
     ap.add_argument("--ref-window", type=float, default=0.025,
                     help="decode window (s) of one reference-arm step")
     ap.add_argument("--cpu-frames", type=int, default=40,
@@ -1110,6 +1194,8 @@ def main():
         res = run_encode_only(args, rank, world, local)
     elif args.workload == "stitch":
         res = run_stitch(args, rank, world, local)
+    elif args.workload == "synth":
+        res = run_synth(args, rank, world, local) if rank == 0 else None
     elif args.workload == "cpu-full":
         res = run_cpu_full(args) if rank == 0 else None
     else:

@@ -26,11 +26,14 @@ def problems():
     return [batch.encode_clip_problem(c) for c in pick]
 
 
-def test_batch_equals_alone(problems):
+@pytest.mark.parametrize("eig", ["threads", "bucketed"])
+def test_batch_equals_alone(problems, eig):
     """Every clip of the grouped mixed-precision batch equals its stand-alone
     mixed decode, and both equal the reference's pseudoinverse semantics
-    (eigen path); replaying the captured graphs gives the same videos."""
-    bd = batch.BatchDecoder(problems, streams=4, sweeps=2, graph=True)
+    (eigen path), with the refused systems eigen-solved on the worker
+    threads or in padded batches; replaying the captured graphs gives the
+    same videos."""
+    bd = batch.BatchDecoder(problems, streams=4, sweeps=2, graph=True, eig=eig)
     outs = [o.clone() for o in bd.run()]
     torch.cuda.synchronize()
     assert bd.graph_error is None, bd.graph_error

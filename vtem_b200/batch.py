@@ -370,9 +370,17 @@ class BatchDecoder(object):
     graphs on the first run and replays them afterwards; inputs are read
     from the problems' device tensors, so new spikes of the same sizes are
     decoded by copying them into those tensors.  ``workers`` host threads
-    run the float64 fallbacks and spike-space solves concurrently."""
+    run the float64 fallbacks and spike-space solves concurrently.
+    ``eig`` chooses how refused systems that the float64 Cholesky refuses
+    too are eigen-solved: "bucketed" (batched eigensolver calls of one padded
+    size, after every float64 Cholesky has finished) or "threads" (each on
+    its worker thread, as a stand-alone decoder would, concurrently over the
+    workers' streams)."""
 
-    def __init__(self, problems, streams=8, sweeps=1, graph=True, workers=8):
+    def __init__(self, problems, streams=8, sweeps=1, graph=True, workers=8, eig="bucketed"):
+        if eig not in ("threads", "bucketed"):
+            raise ValueError("eig must be 'threads' or 'bucketed'")
+        self.eig = eig
         self.problems = list(problems)
         self.decs = [fast.from_prep(p.prep, p.Wt, p.Mt, rcond=p.rcond, solver="mixed", mixed_sweeps=sweeps)
                      for p in self.problems]
@@ -513,8 +521,10 @@ class BatchDecoder(object):
             ev[1].record(main)
             bad = [self.coeff[j] for j in self.plan.check()]
             # float64 Cholesky first (concurrently); the systems it refuses are
-            # eigen-solved together, grouped by padded size
-            chol = [(i, self._pool.submit(self._float64, i, ev[1], False)) for i in bad]
+            # eigen-solved on the same worker thread, or together, grouped by
+            # padded size
+            threads = self.eig == "threads"
+            chol = [(i, self._pool.submit(self._float64, i, ev[1], threads)) for i in bad]
         else:
             ev[1].record(main)
         rest = []

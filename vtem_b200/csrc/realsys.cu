@@ -61,8 +61,12 @@ __device__ __forceinline__ double real_entry(double2 A, double2 B, int p, int q)
 // the pairs p of spatial indices s <= s' and the upper-triangular temporal
 // entries u = (m, m'), m <= m' (both in row-major upper-triangular order):
 // sum a W for m <= m', sum a conj(W[m'][m]) for m > m' (W_n is Hermitian).
-__device__ __forceinline__ double2 gram_from_pairs(const float* __restrict__ C, int64_t ldc, int Ks, int Kt, int j,
+// KT > 0: the temporal order is a compile-time constant (the divisions by
+// Kt become multiply-shifts); KT == 0: Kt at run time
+template <int KT>
+__device__ __forceinline__ double2 gram_from_pairs(const float* __restrict__ C, int64_t ldc, int Ks, int Kt_rt, int j,
                                                    int k) {
+    const int Kt = KT > 0 ? KT : Kt_rt;
     int s = j / Kt, m = j - s * Kt, s2 = k / Kt, m2 = k - s2 * Kt;
     bool conj = false;
     if (s > s2) {
@@ -75,7 +79,7 @@ __device__ __forceinline__ double2 gram_from_pairs(const float* __restrict__ C, 
     const int ma = lower ? m2 : m, mb = lower ? m : m2;
     const int u = ma * Kt - ma * (ma - 1) / 2 + (mb - ma);
     const float* c = C + (2 * p) * ldc + 2 * u;
-    const double rr = c[0], ri = c[1], ir = c[ldc], ii = c[ldc + 1];
+    const double rr = __ldg(c), ri = __ldg(c + 1), ir = __ldg(c + ldc), ii = __ldg(c + ldc + 1);
     const double re = lower ? rr + ii : rr - ii;
     const double im = lower ? ir - ri : ri + ir;
     return make_double2(re, conj ? -im : im);
@@ -84,7 +88,7 @@ __device__ __forceinline__ double2 gram_from_pairs(const float* __restrict__ C, 
 // Mr from the tensor-core Gram: one block row of threads per real row R,
 // one thread per complex column k <= h, which reads M[j][k] and M[j][K-1-k]
 // once and writes both real columns they feed (k and h+1+k).
-template <typename OutT>
+template <typename OutT, int KT>
 __global__ void __launch_bounds__(256) real_scatter_kernel(const float* __restrict__ C, int64_t ldc, int Ks, int Kt,
                                                            OutT* __restrict__ Mr, int64_t ldr) {
     const int K = Ks * Kt, h = (K - 1) / 2;
@@ -93,8 +97,8 @@ __global__ void __launch_bounds__(256) real_scatter_kernel(const float* __restri
     real_split(R, h, j, p);
     OutT* row = Mr + (int64_t)R * ldr;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= h; k += gridDim.x * blockDim.x) {
-        const double2 A = gram_from_pairs(C, ldc, Ks, Kt, j, k);
-        const double2 B = gram_from_pairs(C, ldc, Ks, Kt, j, K - 1 - k);
+        const double2 A = gram_from_pairs<KT>(C, ldc, Ks, Kt, j, k);
+        const double2 B = gram_from_pairs<KT>(C, ldc, Ks, Kt, j, K - 1 - k);
         double v0 = real_entry(A, B, p, 0);
         if (R == h) v0 *= kInvSqrt2;
         if (k == h) v0 *= kInvSqrt2;
@@ -104,6 +108,20 @@ __global__ void __launch_bounds__(256) real_scatter_kernel(const float* __restri
             if (R == h) v1 *= kInvSqrt2;
             row[h + 1 + k] = (OutT)v1;
         }
+    }
+}
+
+template <typename OutT>
+static void launch_real_scatter(const float* C, int64_t ldc, int Ks, int Kt, OutT* Mr, int64_t ldr, dim3 grid,
+                                cudaStream_t s) {
+    switch (Kt) {
+        case 7: real_scatter_kernel<OutT, 7><<<grid, 256, 0, s>>>(C, ldc, Ks, Kt, Mr, ldr); break;
+        case 9: real_scatter_kernel<OutT, 9><<<grid, 256, 0, s>>>(C, ldc, Ks, Kt, Mr, ldr); break;
+        case 11: real_scatter_kernel<OutT, 11><<<grid, 256, 0, s>>>(C, ldc, Ks, Kt, Mr, ldr); break;
+        case 13: real_scatter_kernel<OutT, 13><<<grid, 256, 0, s>>>(C, ldc, Ks, Kt, Mr, ldr); break;
+        case 15: real_scatter_kernel<OutT, 15><<<grid, 256, 0, s>>>(C, ldc, Ks, Kt, Mr, ldr); break;
+        case 17: real_scatter_kernel<OutT, 17><<<grid, 256, 0, s>>>(C, ldc, Ks, Kt, Mr, ldr); break;
+        default: real_scatter_kernel<OutT, 0><<<grid, 256, 0, s>>>(C, ldc, Ks, Kt, Mr, ldr); break;
     }
 }
 
@@ -781,11 +799,9 @@ VTB_API int vtb_coeff_real_scatter(const float* C, int64_t ldc, int Ks, int Kt, 
     VTB_CHECK_ARG(K <= 65535);
     const dim3 grid(ceil_div(h + 1, 256), K);
     if (out_f64)
-        real_scatter_kernel<double><<<grid, 256, 0, as_stream(stream)>>>(C, ldc, Ks, Kt, reinterpret_cast<double*>(Mr),
-                                                                         ldr);
+        launch_real_scatter<double>(C, ldc, Ks, Kt, reinterpret_cast<double*>(Mr), ldr, grid, as_stream(stream));
     else
-        real_scatter_kernel<float><<<grid, 256, 0, as_stream(stream)>>>(C, ldc, Ks, Kt, reinterpret_cast<float*>(Mr),
-                                                                        ldr);
+        launch_real_scatter<float>(C, ldc, Ks, Kt, reinterpret_cast<float*>(Mr), ldr, grid, as_stream(stream));
     return launch_status();
 }
 
