@@ -105,3 +105,15 @@ def test_chol_and_wait_limit_entry_points_without_gpu():
         assert lib.vtb_set_wait_limit(7, prev.ctypes.data) == 0 and prev[0] == 7
     prev = np.zeros(1, np.int64)
     assert lib.vtb_set_wait_limit(0, prev.ctypes.data) == 0 and prev[0] == 0
+
+
+def test_synth_rank_rejects_unsupported_orders_without_gpu():
+    lib = _abi.lib()
+    # Mt = 0 and Mt = 11 (23 harmonics, beyond the kernel's 21) are refused before any launch
+    assert lib.vtb_coeff_synth_rank(None, None, 29, 3, 3, 0, 8, 8, 8, 8, None, 1, 1.0, 0.0, 1e-3, 4, None, 0,
+                                    None) == _abi.VTB_BAD_ARG
+    assert lib.vtb_coeff_synth_rank(None, None, 29, 3, 3, 11, 8, 8, 8, 8, None, 23, 1.0, 0.0, 1e-3, 4, 1, 0,
+                                    None) == _abi.VTB_BAD_ARG
+    # no frames: nothing to do
+    assert lib.vtb_coeff_synth_rank(None, None, 29, 3, 3, 4, 8, 8, 8, 8, None, 9, 1.0, 0.0, 1e-3, 0, None, 0,
+                                    None) == _abi.VTB_OK

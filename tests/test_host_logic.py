@@ -148,3 +148,36 @@ def test_spatial_tiles_match_oracle():
             np.testing.assert_array_equal(wa, wb)
             cover[r0:r1, c0:c1] += wa
         np.testing.assert_allclose(cover, 1.0, rtol=0, atol=1e-12)
+
+
+def test_frame_pair_synthesis_identity():
+    """The harmonics kernel's frame-pair form (csrc/synth_rank.cu): with the
+    weights rotated to a block's centre angle th_c, A_m = a_m cos(m th_c) +
+    b_m sin(m th_c) and B_m = b_m cos(m th_c) - a_m sin(m th_c), the frames
+    at th_c -+ phi are E -+ O (E = sum_m A_m cos(m phi), O = sum_m B_m
+    sin(m phi)).  Checked against u[f] = H_0 + sum_m (cos(m W t_f) a_m +
+    sin(m W t_f) b_m) for even and odd frame ranges, with the kernel's
+    pairing of frames lo = fb + half - 1 + odd - j and hi = fb + half + j."""
+    rng = np.random.default_rng(5)
+    Mt, W, t0, dt = 8, 2 * np.pi * 2.5, 0.013, 1e-4
+    H = rng.standard_normal((7, 2 * Mt + 1))
+    m = np.arange(1, Mt + 1)
+    for fb, nfr in ((0, 10), (3, 11), (17, 1), (5, 2)):
+        f = np.arange(fb, fb + nfr)
+        th = W * (t0 + f * dt)
+        direct = H[:, 0][None, :] + np.cos(np.outer(th, m)) @ H[:, 1::2].T + np.sin(np.outer(th, m)) @ H[:, 2::2].T
+        half, odd = nfr >> 1, nfr & 1
+        thc = W * (t0 + (fb + 0.5 * (nfr - 1)) * dt)
+        a, b = H[:, 1::2], H[:, 2::2]
+        A = a * np.cos(m * thc) + b * np.sin(m * thc)
+        B = b * np.cos(m * thc) - a * np.sin(m * thc)
+        got = np.full((nfr, H.shape[0]), np.nan)
+        for j in range(half + odd):
+            phi = W * dt * (j + (0.0 if odd else 0.5))
+            E = H[:, 0] + A @ np.cos(m * phi)
+            Od = B @ np.sin(m * phi)
+            lo, hi = fb + half - 1 + odd - j, fb + half + j
+            got[hi - fb] = E + Od
+            got[lo - fb] = E - Od
+        assert np.isfinite(got).all()
+        assert np.abs(got - direct).max() <= 1e-12 * np.abs(direct).max()
