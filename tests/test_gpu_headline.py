@@ -110,12 +110,12 @@ def test_coeff_f64_decode_matches_oracle(c1):
 
 def _bench_decode(c1, sweeps):
     """The decoder as the benchmark drives it: device-resident spikes sorted
-    by neuron, coefficients then synthesis."""
+    by neuron, one ``decode`` call (the synthesis queued before the
+    acceptance read, done again after a fallback)."""
     w, prep = c1["w"], c1["prep"]
     dec = fast.from_prep(prep, w.Wt, w.Mt, rcond=w.rcond, solver="mixed", mixed_sweeps=sweeps)
     d = tuple(torch.as_tensor(x, device="cuda") for x in c1["spikes"])
-    a = dec.coefficients(*d, assume_sorted=True)
-    u = dec.synthesize(a, w.T, w.dt)
+    u = dec.decode(*d, w.T, w.dt, assume_sorted=True)
     return dec, u
 
 
