@@ -181,3 +181,20 @@ def test_frame_pair_synthesis_identity():
             got[lo - fb] = E - Od
         assert np.isfinite(got).all()
         assert np.abs(got - direct).max() <= 1e-12 * np.abs(direct).max()
+
+
+def test_pinv_buckets_partition_sizes():
+    """Padded-size buckets of the batched eigen-pseudoinverse: every system
+    in exactly one bucket, padded to the bucket's largest size, and no
+    system smaller than PINV_BUCKET_RATIO of it (bounded padding work)."""
+    from vtem_b200 import batch
+    rng = np.random.default_rng(11)
+    for Ks in ([1921], [91, 91, 91], list(rng.integers(91, 1922, 97)), [100, 69, 70, 49, 48, 1000]):
+        out = batch.pinv_buckets(Ks)
+        seen = sorted(i for _, idx in out for i in idx)
+        assert seen == list(range(len(Ks)))
+        for top, idx in out:
+            assert top == max(Ks[i] for i in idx)
+            assert all(Ks[i] >= batch.PINV_BUCKET_RATIO * top for i in idx)
+        tops = [t for t, _ in out]
+        assert tops == sorted(tops, reverse=True)
