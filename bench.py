@@ -427,10 +427,12 @@ def serve_short(dev, requests=64, rate=200.0, seed=3):
 
 def launches_mixed(dec):
     # this library's kernels per decode: temporal Gram (1); right-hand side, realify, W_n split, tensor-core
-    # Gram, real scatter (5); tile Cholesky (1); initial solve (1); per sweep: unrealify, residual and its
-    # reduction (2), realify, solve, norm ratio, axpy (7); final unrealify (1); synthesis: per-pixel weights
-    # and the harmonics product (2).  With mixed_factor="cusolver", cuSOLVER's kernels are not counted.
-    return 1 + 5 + 1 + 1 + 7 * dec.mixed_sweeps + 1 + 2
+    # Gram, real scatter (5); tile Cholesky (1); initial solve (2 with the inverse: the two product kernels;
+    # 1 otherwise); per sweep: unrealify, residual and its reduction (2), realify, solve, norm ratio, axpy;
+    # final unrealify (1); synthesis: per-pixel weights and the harmonics product (2).  With
+    # mixed_factor="cusolver", cuSOLVER's kernels are not counted.
+    solve = 2 if dec.mixed_factor == "inverse" else 1
+    return 1 + 5 + 1 + solve + (6 + solve) * dec.mixed_sweeps + 1 + 2
 
 
 def batch_measure(dev, local, count, seed, sweeps, warmup, steps, plain_count, eig="bucketed"):
